@@ -1,0 +1,20 @@
+"""grasph_b200 — host-side mirror of Grasph.jl's SPH API over libgrasph_cuda.so.
+
+The per-timestep hot path (cell-key sort, CSR grid, ghosts, staged pair
+sweeps, state updaters, leapfrog update) runs as sm_100a CUDA kernels behind
+the C ABI in include/grasph_cuda.h; this package builds the model through
+that ABI and moves host arrays in and out.
+"""
+from . import consts
+from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, CauchyFluidPfn,
+                    CountingPfn, CubicSplineKernel, DynamicBoundarySystem, ElastoPlasticParticleSystem,
+                    ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn, GhostCopier, GhostEntry,
+                    GhostParticleSystem, HookeLawStressUpdater, HouseholderReflect, LeapFrogTimeIntegrator,
+                    LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
+                    StressParticleSystem, SystemInteraction, TaitEOSUpdater, WenlandC2Kernel,
+                    ZeroFieldUpdater, is_coupled)
+from .engine import (CudaBackend, GcError, Session, compile_instance, download_instance, load_library,
+                     time_integrate, upload_instance)
+
+PRECISION_FP64 = consts.GC_PRECISION_FP64
+PRECISION_FP32_COMPENSATED = consts.GC_PRECISION_FP32_COMPENSATED

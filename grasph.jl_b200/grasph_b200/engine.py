@@ -1,0 +1,517 @@
+"""Drive libgrasph_cuda.so from the host mirror of Grasph.jl's API.
+
+`compile_instance` walks a LeapFrogTimeIntegrator (systems, ghost entries,
+interactions, updaters) and issues the C-ABI model-building calls — the same
+sequence a Julia `ccall` shim issues.  `Device` owns one
+context; `time_integrate` is the drop-in for
+`time_integrate!(::LeapFrogTimeIntegrator, ...)` (src/TimeIntegration.jl:580).
+
+There is no CPU fallback: if the shared library is missing or the context
+cannot be created, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import consts as C
+from .model import (AbstractBoundarySystem, AbstractParticleSystem, ArgumentError,
+                    GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator,
+                    SystemInteraction, updater_chains, _pfn_kind, _pfn_params)
+
+PKG_DIR = Path(__file__).resolve().parents[1]
+LIB_PATH = PKG_DIR / "libgrasph_cuda.so"
+
+_dp = ct.POINTER(ct.c_double)
+_ip = ct.POINTER(ct.c_int)
+_i64p = ct.POINTER(ct.c_int64)
+_i32p = ct.POINTER(ct.c_int32)
+
+
+class GcError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"{C.STATUS_NAMES.get(status, status)}: {msg}")
+
+
+class GcStats(ct.Structure):
+    _fields_ = [("steps_done", ct.c_int64), ("pairs_last_step", ct.c_int64),
+                ("grid_inconsistent", ct.c_int64), ("resorts", ct.c_int64),
+                ("last_status", ct.c_int32), ("pad", ct.c_int32)]
+
+
+_LIB = None
+
+
+def load_library(path: os.PathLike | None = None):
+    """Load libgrasph_cuda.so (built in-tree by __graft_entry__.build())."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is not built; run `python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = ct.CDLL(str(p))
+    sig = {
+        "gc_ctx_create": (ct.c_int, [ct.c_int, ct.c_size_t, ct.POINTER(ct.c_void_p)]),
+        "gc_ctx_destroy": (ct.c_int, [ct.c_void_p]),
+        "gc_last_error": (ct.c_char_p, [ct.c_void_p]),
+        "gc_status_string": (ct.c_char_p, [ct.c_int]),
+        "gc_instance_add": (ct.c_int, [ct.c_void_p, _ip]),
+        "gc_add_system": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int64, ct.c_int, ct.c_int,
+                                     ct.c_double, ct.c_double, _dp, ct.c_double, _ip]),
+        "gc_add_boundary": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _dp, _dp, ct.c_double, _ip]),
+        "gc_add_ghost": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _ip, _ip, _ip, ct.c_int,
+                                    _dp, _dp, ct.c_double, ct.c_int64, _ip]),
+        "gc_add_interaction": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_double,
+                                          ct.c_int, _ip, _dp, _ip]),
+        "gc_set_updaters": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _ip, _ip, _dp]),
+        "gc_set_integrator": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double]),
+        "gc_finalize": (ct.c_int, [ct.c_void_p]),
+        "gc_upload_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
+        "gc_download_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
+        "gc_get_count": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _i64p]),
+        "gc_set_precision": (ct.c_int, [ct.c_void_p, ct.c_int]),
+        "gc_step": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double]),
+        "gc_get_stats": (ct.c_int, [ct.c_void_p, ct.POINTER(GcStats)]),
+        "gc_sort_system": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double, _i64p]),
+        "gc_build_grid": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _i64p, ct.c_int64, _dp, _i64p, _i64p]),
+        "gc_generate_ghosts": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
+        "gc_update_ghost_kinematics": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
+        "gc_update_ghost": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int]),
+        "gc_sweep": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int]),
+        "gc_update_state": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_double]),
+        "gc_neighbor_counts": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _i32p, ct.c_int64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def _arr(a, dtype, ptr):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, a.ctypes.data_as(ptr)
+
+
+class CudaBackend:
+    """C-ABI calls on one libgrasph_cuda.so context."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, lib=None):
+        self.lib = lib or load_library()
+        self.ctx = ct.c_void_p()
+        self._chk(self.lib.gc_ctx_create(device, hbm_budget, ct.byref(self.ctx)), where="gc_ctx_create")
+
+    # -- plumbing
+    def _chk(self, st, where=""):
+        if st != 0:
+            msg = ""
+            if self.ctx:
+                msg = (self.lib.gc_last_error(self.ctx) or b"").decode()
+            raise GcError(st, f"{where}: {msg}")
+
+    def close(self):
+        if self.ctx:
+            self.lib.gc_ctx_destroy(self.ctx)
+            self.ctx = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- model building
+    def instance_add(self):
+        out = ct.c_int()
+        self._chk(self.lib.gc_instance_add(self.ctx, ct.byref(out)), "gc_instance_add")
+        return out.value
+
+    def add_system(self, inst, kind, n, nd, ns, mass, c, source_v, source_rho):
+        sv, svp = _arr(source_v, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_system(self.ctx, inst, kind, n, nd, ns, mass, c, svp, source_rho,
+                                         ct.byref(out)), "gc_add_system")
+        return out.value
+
+    def add_boundary(self, inst, sys, kind, normal, point, beta_or_lj):
+        nrm, np_ = _arr(normal, np.float64, _dp)
+        pt, pp = _arr(point, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_boundary(self.ctx, inst, sys, kind, np_, pp, beta_or_lj, ct.byref(out)),
+                  "gc_add_boundary")
+        return out.value
+
+    def add_ghost(self, inst, src, copiers, normals, points, cutoff, capacity):
+        nf = np.array([len(c) for c in copiers] or [0], dtype=np.int32)
+        flds = np.array([f for c in copiers for f, _ in c] or [0], dtype=np.int32)
+        mds = np.array([m for c in copiers for _, m in c] or [0], dtype=np.int32)
+        nrm, nrmp = _arr(normals, np.float64, _dp)
+        pts, ptsp = _arr(points, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_ghost(self.ctx, inst, src, len(copiers), nf.ctypes.data_as(_ip),
+                                        flds.ctypes.data_as(_ip), mds.ctypes.data_as(_ip), nrm.shape[0],
+                                        nrmp, ptsp, cutoff, capacity, ct.byref(out)), "gc_add_ghost")
+        return out.value
+
+    def add_interaction(self, inst, a, b, kernel_kind, h, pfn_kinds, pfn_params):
+        k = np.asarray(pfn_kinds, dtype=np.int32)
+        p, pp = _arr(pfn_params, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_interaction(self.ctx, inst, a, b, kernel_kind, h, len(k),
+                                              k.ctypes.data_as(_ip), pp, ct.byref(out)), "gc_add_interaction")
+        return out.value
+
+    def set_updaters(self, inst, sys, chains):
+        cl = np.array([len(c) for c in chains] or [0], dtype=np.int32)
+        kinds = np.array([k for c in chains for k, _ in c] or [0], dtype=np.int32)
+        prm = np.array([p for c in chains for _, p in c] or [np.zeros(C.GC_UPD_NPARAM)], dtype=np.float64)
+        self._chk(self.lib.gc_set_updaters(self.ctx, inst, sys, len(chains), cl.ctypes.data_as(_ip),
+                                           kinds.ctypes.data_as(_ip), prm.ctypes.data_as(_dp)),
+                  "gc_set_updaters")
+
+    def set_integrator(self, inst, gamma):
+        self._chk(self.lib.gc_set_integrator(self.ctx, inst, gamma), "gc_set_integrator")
+
+    def finalize(self):
+        self._chk(self.lib.gc_finalize(self.ctx), "gc_finalize")
+
+    # -- state
+    def upload(self, inst, handle, field, array):
+        a = np.ascontiguousarray(array)
+        self._chk(self.lib.gc_upload_field(self.ctx, inst, handle, field, a.ctypes.data, a.nbytes),
+                  "gc_upload_field")
+
+    def download_into(self, inst, handle, field, out):
+        self._chk(self.lib.gc_download_field(self.ctx, inst, handle, field, out.ctypes.data, out.nbytes),
+                  "gc_download_field")
+        return out
+
+    def count(self, inst, handle):
+        n = ct.c_int64()
+        self._chk(self.lib.gc_get_count(self.ctx, inst, handle, ct.byref(n)), "gc_get_count")
+        return n.value
+
+    def set_precision(self, mode):
+        self._chk(self.lib.gc_set_precision(self.ctx, mode), "gc_set_precision")
+
+    def step(self, nsteps, cfl):
+        self._chk(self.lib.gc_step(self.ctx, nsteps, cfl), "gc_step")
+
+    def stats(self):
+        s = GcStats()
+        self._chk(self.lib.gc_get_stats(self.ctx, ct.byref(s)), "gc_get_stats")
+        return {f: getattr(s, f) for f, _ in GcStats._fields_ if f != "pad"}
+
+    # -- phase hooks
+    def sort(self, inst, handle, cutoff, n):
+        perm = np.zeros(n, dtype=np.int64)
+        self._chk(self.lib.gc_sort_system(self.ctx, inst, handle, cutoff, perm.ctypes.data_as(_i64p)),
+                  "gc_sort_system")
+        return perm
+
+    def build_grid(self, inst, inter, nd):
+        ming = np.zeros(nd)
+        ng = np.zeros(nd, dtype=np.int64)
+        ncells = ct.c_int64()
+        self._chk(self.lib.gc_build_grid(self.ctx, inst, inter, None, 0, ming.ctypes.data_as(_dp),
+                                         ng.ctypes.data_as(_i64p), ct.byref(ncells)), "gc_build_grid")
+        cs = np.zeros(ncells.value + 1, dtype=np.int64)
+        self._chk(self.lib.gc_build_grid(self.ctx, inst, inter, cs.ctypes.data_as(_i64p), cs.size, None,
+                                         None, None), "gc_build_grid")
+        return cs, ming, ng
+
+    def generate_ghosts(self, inst, ghost):
+        self._chk(self.lib.gc_generate_ghosts(self.ctx, inst, ghost), "gc_generate_ghosts")
+
+    def update_ghost_kinematics(self, inst, ghost):
+        self._chk(self.lib.gc_update_ghost_kinematics(self.ctx, inst, ghost), "gc_update_ghost_kinematics")
+
+    def update_ghost(self, inst, ghost, stage):
+        self._chk(self.lib.gc_update_ghost(self.ctx, inst, ghost, stage), "gc_update_ghost")
+
+    def sweep(self, inst, inter, stage):
+        self._chk(self.lib.gc_sweep(self.ctx, inst, inter, stage), "gc_sweep")
+
+    def update_state(self, inst, sys, stage, dt):
+        self._chk(self.lib.gc_update_state(self.ctx, inst, sys, stage, dt), "gc_update_state")
+
+    def neighbor_counts(self, inst, inter, n):
+        out = np.zeros(n, dtype=np.int32)
+        self._chk(self.lib.gc_neighbor_counts(self.ctx, inst, inter, out.ctypes.data_as(_i32p), n),
+                  "gc_neighbor_counts")
+        return out
+
+
+# ------------------------------------------------------------ compilation
+
+class InstanceMap:
+    """Object → handle map of one compiled instance."""
+
+    def __init__(self, inst):
+        self.inst = inst
+        self.handles = {}
+        self.inters = {}
+        self.systems = []
+        self.ghosts = []
+
+    def h(self, obj):
+        return self.handles[id(obj)]
+
+
+def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0) -> InstanceMap:
+    """Issue the model-building calls for one simulation (one instance)."""
+    m = InstanceMap(inst)
+    sys_ids = {id(ps) for ps in systems}
+    for ps in systems:
+        if not isinstance(ps, AbstractParticleSystem):
+            raise ArgumentError("systems must be particle systems (wrap boundaries only as system_b)")
+        m.handles[id(ps)] = backend.add_system(inst, ps.kind, ps.n, ps.ndims, ps.ns, ps.mass, ps.c,
+                                               ps.source_v, ps.source_rho)
+        m.systems.append(ps)
+    for ge in ghosts:
+        g = ge.ghost
+        if id(g.source) not in sys_ids:
+            raise ArgumentError("a ghost's source system must be in the integrator's systems")
+        copiers = []
+        for u in g.updaters:
+            copiers.append([] if u is None else
+                           [({"p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS, "rho": C.GC_FIELD_RHO}[f], md)
+                            for f, md in u.entries])
+        hnd = backend.add_ghost(inst, m.h(g.source), copiers, ge.normals, ge.points, ge.cutoff, ge.capacity)
+        m.handles[id(g)] = hnd
+        m.handles[id(ge)] = hnd
+        m.ghosts.append(ge)
+    for it in interactions:
+        a = it.system_a
+        if id(a) not in sys_ids:
+            raise ArgumentError("system_a must be in the integrator's systems")
+        b = it.system_b
+        if b is None:
+            bh = -1
+        elif isinstance(b, AbstractBoundarySystem):
+            if id(b) not in m.handles:
+                if id(b.inner) not in sys_ids:
+                    raise ArgumentError("a boundary's inner system must be in the integrator's systems")
+                if b.wrap_kind == C.GC_WRAP_DYNAMIC:
+                    m.handles[id(b)] = backend.add_boundary(inst, m.h(b.inner), b.wrap_kind, b.boundary_normal,
+                                                            b.boundary_point, b.boundary_beta)
+                else:
+                    nd = b.inner.ndims
+                    m.handles[id(b)] = backend.add_boundary(inst, m.h(b.inner), b.wrap_kind, np.zeros(nd),
+                                                            np.zeros(nd), b.lj_cutoff)
+            bh = m.h(b)
+        elif isinstance(b, GhostParticleSystem):
+            if id(b) not in m.handles:
+                raise ArgumentError("a ghost used as system_b must belong to a GhostEntry in `ghosts`")
+            bh = m.h(b)
+        else:
+            if id(b) not in sys_ids:
+                raise ArgumentError("system_b must be in the integrator's systems")
+            bh = m.h(b)
+        kinds = [_pfn_kind(p) for p in it.pfns]
+        params = np.array([_pfn_params(p) for p in it.pfns], dtype=np.float64)
+        m.inters[id(it)] = backend.add_interaction(inst, m.h(a), bh, it.kernel.kind, it.kernel.h, kinds, params)
+    for ps in systems:
+        chains = updater_chains(ps)
+        if chains:
+            backend.set_updaters(inst, m.h(ps), chains)
+    backend.set_integrator(inst, gamma)
+    return m
+
+
+def upload_instance(backend, m: InstanceMap):
+    for ps in m.systems:
+        h = m.h(ps)
+        for name, fid in ps.particle_fields():
+            backend.upload(m.inst, h, fid, getattr(ps, name))
+
+
+def download_instance(backend, m: InstanceMap, with_ghosts=True):
+    for ps in m.systems:
+        h = m.h(ps)
+        for name, fid in ps.particle_fields():
+            backend.download_into(m.inst, h, fid, getattr(ps, name))
+    if with_ghosts:
+        for ge in m.ghosts:
+            download_ghost(backend, m, ge)
+
+
+def download_ghost(backend, m: InstanceMap, ge: GhostEntry):
+    g = ge.ghost
+    h = m.h(g)
+    n = backend.count(m.inst, h)
+    nd = g.ndims
+    g.x = backend.download_into(m.inst, h, C.GC_FIELD_X, np.zeros((n, nd)))
+    g.v = backend.download_into(m.inst, h, C.GC_FIELD_V, np.zeros((n, nd)))
+    g.rho = backend.download_into(m.inst, h, C.GC_FIELD_RHO, np.zeros(n))
+    g.idx_original = backend.download_into(m.inst, h, C.GC_FIELD_IDX_ORIGINAL, np.zeros(n, dtype=np.int64))
+    g.idx_boundary = backend.download_into(m.inst, h, C.GC_FIELD_IDX_BOUNDARY, np.zeros(n, dtype=np.int64))
+    g.normals = backend.download_into(m.inst, h, C.GC_FIELD_NORMALS, np.zeros((n, nd)))
+    for f in g.extras_fields:
+        if f == "p":
+            g.extras["p"] = backend.download_into(m.inst, h, C.GC_FIELD_P, np.zeros(n))
+        elif f == "stress":
+            g.extras["stress"] = backend.download_into(m.inst, h, C.GC_FIELD_STRESS,
+                                                       np.zeros((n, g.source.ns)))
+
+
+# --------------------------------------------------------------- sessions
+
+class Session:
+    """A device context holding one or more simulations (instances).
+
+    ``Session([lf])`` is the single-rank drop-in; ``Session([lf1, lf2, ...])``
+    packs independent simulations of one model structure into one context
+    (batched stepping).  Per-phase methods mirror the reference's
+    per-phase entry points for a single instance.
+    """
+
+    def __init__(self, integrators, *, device=0, precision=C.GC_PRECISION_FP64, hbm_budget=0,
+                 backend=None):
+        if isinstance(integrators, LeapFrogTimeIntegrator):
+            integrators = [integrators]
+        self.integrators = list(integrators)
+        self.backend = backend or CudaBackend(device, hbm_budget)
+        self.maps = []
+        for lf in self.integrators:
+            inst = self.backend.instance_add()
+            self.maps.append(compile_instance(self.backend, inst, lf.systems, lf.interactions, lf.ghosts,
+                                              lf.gamma))
+        self.backend.finalize()
+        self.backend.set_precision(precision)
+        self.precision = precision
+
+    # -- state transfer
+    def push(self):
+        for m in self.maps:
+            upload_instance(self.backend, m)
+
+    def pull(self, with_ghosts=True):
+        for m in self.maps:
+            download_instance(self.backend, m, with_ghosts)
+
+    def step(self, nsteps, cfl):
+        self.backend.step(nsteps, cfl)
+
+    def stats(self):
+        return self.backend.stats()
+
+    # -- per-phase hooks (instance 0 unless given)
+    def _m(self, inst):
+        return self.maps[inst]
+
+    def sort_particles(self, ps, cutoff, inst=0):
+        m = self._m(inst)
+        n = ps.n if not isinstance(ps, GhostParticleSystem) else self.backend.count(m.inst, m.h(ps))
+        return self.backend.sort(m.inst, m.h(ps), cutoff, n)
+
+    def create_grid(self, si, inst=0):
+        m = self._m(inst)
+        return self.backend.build_grid(m.inst, m.inters[id(si)], si.ndims)
+
+    def generate_ghosts(self, ge, inst=0):
+        m = self._m(inst)
+        self.backend.generate_ghosts(m.inst, m.h(ge))
+
+    def update_ghost_kinematics(self, ge, inst=0):
+        m = self._m(inst)
+        self.backend.update_ghost_kinematics(m.inst, m.h(ge))
+
+    def update_ghost(self, ge, stage, inst=0):
+        m = self._m(inst)
+        self.backend.update_ghost(m.inst, m.h(ge), stage)
+
+    def sweep(self, si, stage=1, inst=0):
+        m = self._m(inst)
+        self.backend.sweep(m.inst, m.inters[id(si)], stage)
+
+    def update_state(self, ps, stage=1, dt=0.0, inst=0):
+        m = self._m(inst)
+        self.backend.update_state(m.inst, m.h(ps), stage, dt)
+
+    def neighbor_counts(self, si, inst=0):
+        m = self._m(inst)
+        return self.backend.neighbor_counts(m.inst, m.inters[id(si)], si.system_a.n)
+
+    def pull_ghost(self, ge, inst=0):
+        download_ghost(self.backend, self._m(inst), ge)
+
+    def close(self):
+        self.backend.close()
+
+
+def _summary(ps):
+    rows = []
+    for name in ("v", "rho", "p", "stress"):
+        if hasattr(ps, name):
+            a = np.asarray(getattr(ps, name))
+            rows.append(f"  {name:8s} min {a.min():.6g}  mean {a.mean():.6g}  max {a.max():.6g}")
+    return "\n".join(rows)
+
+
+def time_integrate(integrator: LeapFrogTimeIntegrator, num_timesteps: int, print_interval_step: int,
+                   save_interval_step: int, CFL: float, output_prefix=None, *, step_offset: int = 0,
+                   output_width=None, print_timer: bool = False, precision=C.GC_PRECISION_FP64,
+                   verbose: bool = False):
+    """Drop-in for ``time_integrate!`` (src/TimeIntegration.jl:580-697).
+
+    Host arrays are uploaded at entry and written back at exit (and at each
+    print/save boundary); all steps in between run on the device.  Snapshots
+    go to ``{prefix}_{step}.npz`` (the reference writes HDF5).
+    Returns a dict of wall-clock phase timings (the TimerOutputs stand-in).
+    """
+    t0 = time.perf_counter()
+    sess = integrator._device
+    if sess is None or sess.precision != precision:
+        sess = Session([integrator], precision=precision)
+        integrator._device = sess
+    sess.push()
+    t_up = time.perf_counter()
+    width = output_width if output_width is not None else len(str(step_offset + num_timesteps))
+    done = 0
+    while done < num_timesteps:
+        g = step_offset + done
+        nxt = num_timesteps - done
+        for interval in (print_interval_step, save_interval_step if output_prefix is not None else 0):
+            if interval and interval > 0:
+                nxt = min(nxt, interval - (g % interval))
+        sess.step(nxt, CFL)
+        done += nxt
+        g = step_offset + done
+        boundary_print = verbose and print_interval_step > 0 and g % print_interval_step == 0
+        boundary_save = output_prefix is not None and save_interval_step > 0 and g % save_interval_step == 0
+        if boundary_print or boundary_save:
+            sess.pull()
+            if boundary_print:
+                print(f"\nStep {g}")
+                for ps in integrator.systems:
+                    print(ps.name)
+                    print(_summary(ps))
+            if boundary_save:
+                path = f"{output_prefix}_{str(g).zfill(width)}.npz"
+                d = os.path.dirname(path)
+                if d:
+                    os.makedirs(d, exist_ok=True)
+                arrays = {}
+                for ps in integrator.systems:
+                    for name, _ in ps.particle_fields():
+                        arrays[f"{ps.name}/{name}"] = getattr(ps, name)
+                np.savez(path, step=g, **arrays)
+    t_run = time.perf_counter()
+    sess.pull()
+    t_down = time.perf_counter()
+    timer = {"upload_s": t_up - t0, "steps_s": t_run - t_up, "download_s": t_down - t_run,
+             "steps": num_timesteps}
+    if print_timer:
+        print(timer)
+    return timer

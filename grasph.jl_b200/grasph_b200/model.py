@@ -1,0 +1,573 @@
+"""Host-side mirror of Grasph.jl's model API.
+
+The classes below keep the names, constructor arguments, validation and
+error behaviour of the Julia API on the hot path, so code (and tests)
+written against Grasph.jl translate line for line.  They hold host state in
+numpy arrays shaped like Julia's ``Vector{SVector{K,Float64}}`` (``(n, K)``,
+row-major, i.e. the same bytes as Julia's AoS layout).  Numerical work is
+never done here: `grasph_b200.engine` ships the model to libgrasph_cuda.so.
+
+Reference counterparts (Grasph.jl source tree):
+  particle systems   src/Particles.jl:38,149,245,351
+  boundary wrappers  src/BoundaryParticles.jl:38,68
+  ghosts             src/GhostParticles.jl:53,174,300
+  kernels            src/Kernels.jl:18,92
+  pair functors      src/PairwiseFunctors.jl:18,78,136,252
+  state updaters     src/StateUpdaters.jl:30,108,131,202,356
+  interaction        src/Interaction.jl:23,61
+  integrator         src/TimeIntegration.jl:29,53
+"""
+from __future__ import annotations
+
+import math
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import consts as C
+
+
+class ArgumentError(ValueError):
+    """Mirror of Julia's ``ArgumentError`` for invalid constructor input."""
+
+
+# ---------------------------------------------------------------- systems
+
+class AbstractParticleSystem:
+    """Common base; concrete types mirror src/Particles.jl."""
+
+    kind = C.GC_SYS_BASIC
+    has_p = False
+    has_stress = False
+    is_ep = False
+
+    def __init__(self, name: str, n: int, ndims: int, mass: float, c: float, *,
+                 ns: int = 0, dtype=np.float64, source_v=None, source_rho: float = 0.0,
+                 state_updater=()):
+        n = int(n)
+        ndims = int(ndims)
+        if n <= 0:
+            raise ArgumentError(f"n must be positive, got {n}")
+        if ndims <= 0:
+            raise ArgumentError(f"ndims must be positive, got {ndims}")
+        if source_v is None:
+            source_v = np.zeros(ndims)
+        source_v = np.asarray(source_v, dtype=np.float64)
+        if source_v.shape != (ndims,):
+            raise ArgumentError(
+                f"length(source_v) = {source_v.size} must equal ndims = {ndims}")
+        if np.dtype(dtype) != np.float64:
+            raise ArgumentError("only Float64 particle systems are supported by the device library")
+        self.name = str(name)
+        self.n = n
+        self.ndims = ndims
+        self.ns = int(ns)
+        self.mass = float(mass)
+        self.c = float(c)
+        self.source_v = source_v
+        self.source_rho = float(source_rho)
+        self.id = np.arange(1, n + 1, dtype=np.int64)
+        self.x = np.zeros((n, ndims))
+        self.v = np.zeros((n, ndims))
+        self.v_adjustment = np.zeros((n, ndims))
+        self.rho = np.zeros(n)
+        self.dvdt = np.zeros((n, ndims))
+        self.drhodt = np.zeros(n)
+        ups = state_updater if isinstance(state_updater, tuple) else (state_updater,)
+        self.state_updater = ups
+
+    # Fields in the order of src/Sorting.jl:15-26 (the arrays a sort permutes).
+    def particle_fields(self):
+        f = [("x", C.GC_FIELD_X), ("id", C.GC_FIELD_ID), ("v", C.GC_FIELD_V),
+             ("v_adjustment", C.GC_FIELD_V_ADJUSTMENT), ("rho", C.GC_FIELD_RHO),
+             ("dvdt", C.GC_FIELD_DVDT), ("drhodt", C.GC_FIELD_DRHODT)]
+        if self.has_p:
+            f.append(("p", C.GC_FIELD_P))
+        if self.has_stress:
+            f += [("stress", C.GC_FIELD_STRESS), ("strain_rate", C.GC_FIELD_STRAIN_RATE)]
+        if self.is_ep:
+            f += [("vorticity", C.GC_FIELD_VORTICITY), ("strain", C.GC_FIELD_STRAIN),
+                  ("strain_p", C.GC_FIELD_STRAIN_P)]
+        return f
+
+    def __repr__(self):
+        return f"{type(self).__name__}({self.name!r}, n={self.n}, ndims={self.ndims})"
+
+
+class BasicParticleSystem(AbstractParticleSystem):
+    """src/Particles.jl:38-101."""
+
+    kind = C.GC_SYS_BASIC
+
+    def __init__(self, name, n, ndims, mass, c, **kw):
+        super().__init__(name, n, ndims, mass, c, **kw)
+
+
+class FluidParticleSystem(AbstractParticleSystem):
+    """src/Particles.jl:149-214 (Basic fields plus pressure ``p``)."""
+
+    kind = C.GC_SYS_FLUID
+    has_p = True
+
+    def __init__(self, name, n, ndims, mass, c, **kw):
+        super().__init__(name, n, ndims, mass, c, **kw)
+        self.p = np.zeros(self.n)
+
+
+class StressParticleSystem(AbstractParticleSystem):
+    """src/Particles.jl:245-317 (Fluid fields plus Voigt ``stress``, ``strain_rate``)."""
+
+    kind = C.GC_SYS_STRESS
+    has_p = True
+    has_stress = True
+
+    def __init__(self, name, n, ndims, ns, mass, c, **kw):
+        ns = int(ns)
+        if ns not in (3, 4, 6):
+            raise ArgumentError(f"ns must be 3, 4, or 6, got {ns}")
+        super().__init__(name, n, ndims, mass, c, ns=ns, **kw)
+        self.p = np.zeros(self.n)
+        self.stress = np.zeros((self.n, ns))
+        self.strain_rate = np.zeros((self.n, ns))
+
+
+class ElastoPlasticParticleSystem(StressParticleSystem):
+    """src/Particles.jl:351-430 (Stress fields plus vorticity, strain, strain_p).
+
+    2-D vorticity is a scalar per particle, 3-D a 3-vector (:401)."""
+
+    kind = C.GC_SYS_ELASTOPLASTIC
+    is_ep = True
+
+    def __init__(self, name, n, ndims, ns, mass, c, **kw):
+        super().__init__(name, n, ndims, ns, mass, c, **kw)
+        self.vorticity = np.zeros(self.n) if self.ndims == 2 else np.zeros((self.n, 3))
+        self.strain = np.zeros((self.n, self.ns))
+        self.strain_p = np.zeros((self.n, self.ns))
+
+
+# --------------------------------------------------------------- wrappers
+
+class AbstractBoundarySystem:
+    """Wrapper that forwards every field to ``inner`` (src/BoundaryParticles.jl:13-20)."""
+
+    wrap_kind = 0
+
+    def __getattr__(self, item):
+        return getattr(self.__dict__["inner"], item)
+
+
+class StaticBoundarySystem(AbstractBoundarySystem):
+    """Lennard-Jones repulsion boundary, src/BoundaryParticles.jl:38-49."""
+
+    wrap_kind = C.GC_WRAP_STATIC
+
+    def __init__(self, inner: AbstractParticleSystem, lj_cutoff: float):
+        self.inner = inner
+        self.lj_cutoff = float(lj_cutoff)
+
+
+class DynamicBoundarySystem(AbstractBoundarySystem):
+    """Distance-ratio velocity boundary, src/BoundaryParticles.jl:68-86."""
+
+    wrap_kind = C.GC_WRAP_DYNAMIC
+
+    def __init__(self, inner: AbstractParticleSystem, normal, point, beta: float):
+        nd = inner.ndims
+        self.inner = inner
+        self.boundary_normal = np.asarray(normal, dtype=np.float64).reshape(nd)
+        self.boundary_point = np.asarray(point, dtype=np.float64).reshape(nd)
+        self.boundary_beta = float(beta)
+
+
+# ----------------------------------------------------------------- ghosts
+
+class HouseholderReflect:
+    """Marker: reflect a Voigt tensor by H σ H (src/GhostParticles.jl:26)."""
+
+
+_FIELD_BY_NAME = {"p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS, "rho": C.GC_FIELD_RHO}
+
+
+class GhostCopier:
+    """Per-stage field copier, src/GhostParticles.jl:53-59.
+
+    Entries are field names, or ``(name, HouseholderReflect())`` pairs."""
+
+    def __init__(self, *entries):
+        self.entries = []
+        for e in entries:
+            if isinstance(e, tuple):
+                name, mode = e
+                if not isinstance(mode, HouseholderReflect):
+                    raise ArgumentError("copy mode must be HouseholderReflect()")
+                m = C.GC_COPY_HOUSEHOLDER
+            else:
+                name, m = e, C.GC_COPY_PLAIN
+            name = str(name).lstrip(":")
+            if name not in _FIELD_BY_NAME:
+                raise ArgumentError(f"unsupported ghost copier field :{name}")
+            self.entries.append((name, m))
+
+    @property
+    def fields(self):
+        return tuple(n for n, _ in self.entries)
+
+
+class GhostParticleSystem:
+    """Mirror particles owned per step, src/GhostParticles.jl:174-220."""
+
+    def __init__(self, ps: AbstractParticleSystem, *updaters, name=None):
+        for u in updaters:
+            if u is not None and not isinstance(u, GhostCopier):
+                raise ArgumentError("ghost updaters must be GhostCopier or nothing")
+        self.source = ps
+        self.name = f"ghost({ps.name})" if name is None else str(name)
+        self.updaters = tuple(updaters)
+        seen = []
+        for u in self.updaters:
+            if u is None:
+                continue
+            for f in u.fields:
+                if f not in seen:
+                    seen.append(f)
+        self.extras_fields = tuple(seen)
+        nd = ps.ndims
+        self.x = np.zeros((0, nd))
+        self.v = np.zeros((0, nd))
+        self.rho = np.zeros(0)
+        self.idx_original = np.zeros(0, dtype=np.int64)
+        self.idx_boundary = np.zeros(0, dtype=np.int64)
+        self.normals = np.zeros((0, nd))
+        self.extras = {f: (np.zeros(0) if f != "stress" else np.zeros((0, ps.ns)))
+                       for f in self.extras_fields}
+
+    @property
+    def n(self):
+        return self.x.shape[0]
+
+    @property
+    def ndims(self):
+        return self.source.ndims
+
+    @property
+    def mass(self):
+        return self.source.mass
+
+    @property
+    def c(self):
+        return self.source.c
+
+    def __getattr__(self, item):
+        ex = self.__dict__.get("extras", {})
+        if item in ex:
+            return ex[item]
+        return getattr(self.__dict__["source"], item)
+
+
+class GhostEntry:
+    """A ghost system plus its boundary planes, src/GhostParticles.jl:300-329."""
+
+    def __init__(self, ghost: GhostParticleSystem, cutoff: float, *boundary_pairs,
+                 capacity: int = 0):
+        if not boundary_pairs:
+            raise ArgumentError("at least one boundary (normal, point) pair is required")
+        nd = ghost.ndims
+        self.ghost = ghost
+        self.cutoff = float(cutoff)
+        self.normals = np.array([np.asarray(nrm, dtype=np.float64).reshape(nd)
+                                 for nrm, _ in boundary_pairs])
+        self.points = np.array([np.asarray(pt, dtype=np.float64).reshape(nd)
+                                for _, pt in boundary_pairs])
+        self.capacity = int(capacity)
+
+    @property
+    def boundaries(self):
+        return list(zip(self.normals, self.points))
+
+
+# ---------------------------------------------------------------- kernels
+
+class AbstractKernel:
+    kind = C.GC_KERNEL_CUBIC_SPLINE
+
+    def __init__(self, h: float, ndims: int = 3):
+        self.h = float(h)
+        self.ndims = int(ndims)
+
+    @property
+    def interaction_length(self):
+        return 2.0 * self.h
+
+
+class CubicSplineKernel(AbstractKernel):
+    """src/Kernels.jl:18-81."""
+
+    kind = C.GC_KERNEL_CUBIC_SPLINE
+
+    @property
+    def norm_coeff(self):
+        H = self.h
+        if self.ndims == 1:
+            return 2.0 / (3.0 * H)
+        if self.ndims == 2:
+            return 10.0 / ((7.0 * math.pi) * (H * H))
+        return 1.0 / (math.pi * (H * H * H))
+
+
+class WenlandC2Kernel(AbstractKernel):
+    """src/Kernels.jl:92-153."""
+
+    kind = C.GC_KERNEL_WENDLAND_C2
+
+    @property
+    def norm_coeff(self):
+        H = self.h
+        if self.ndims == 2:
+            return 7.0 / ((64.0 * math.pi) * (H * H))
+        return 21.0 / ((256.0 * math.pi) * (H * H * H))
+
+
+# ----------------------------------------------------------- pair functors
+
+class _Pfn:
+    kind = C.GC_PFN_NONE
+
+    def params(self):
+        p = np.zeros(C.GC_PFN_NPARAM)
+        p[4] = np.nan
+        p[5] = np.nan
+        return p
+
+
+class FluidPfn(_Pfn):
+    """Weakly-compressible momentum + continuity, src/PairwiseFunctors.jl:136-242."""
+
+    kind = C.GC_PFN_FLUID
+
+    def __init__(self, alpha, beta, h, *, sigma=2, delta=None, epsilon=None):
+        self.art_visc_alpha = float(alpha)
+        self.art_visc_beta = float(beta)
+        self.h = float(h)
+        self.sigma = int(sigma)
+        if self.sigma not in (1, 2):
+            raise ArgumentError("FluidPfn sigma must be 1 or 2 on the device path")
+        if epsilon is not None:
+            raise ArgumentError("surface tension (epsilon) belongs to the two-sided multiphase "
+                                "functor, which the device library does not implement")
+        self.delta = None if delta is None else float(delta)
+        self.epsilon = None
+
+    def params(self):
+        p = super().params()
+        p[0], p[1], p[2], p[3] = self.art_visc_alpha, self.art_visc_beta, self.h, self.sigma
+        if self.delta is not None:
+            p[4] = self.delta
+        return p
+
+
+class CauchyFluidPfn(_Pfn):
+    """Cauchy-stress momentum + continuity, src/PairwiseFunctors.jl:252-355."""
+
+    kind = C.GC_PFN_CAUCHY_FLUID
+
+    def __init__(self, alpha, beta, h, *, delta=None):
+        self.art_visc_alpha = float(alpha)
+        self.art_visc_beta = float(beta)
+        self.h = float(h)
+        self.delta = None if delta is None else float(delta)
+
+    def params(self):
+        p = super().params()
+        p[0], p[1], p[2], p[3] = self.art_visc_alpha, self.art_visc_beta, self.h, 2
+        if self.delta is not None:
+            p[4] = self.delta
+        return p
+
+
+class StrainRatePfn(_Pfn):
+    """src/PairwiseFunctors.jl:18-70."""
+
+    kind = C.GC_PFN_STRAIN_RATE
+
+
+class StrainRateVorticityPfn(_Pfn):
+    """src/PairwiseFunctors.jl:78-126."""
+
+    kind = C.GC_PFN_STRAIN_RATE_VORTICITY
+
+
+class CountingPfn(_Pfn):
+    """Adds 1 to ``dvdt[:,0]`` and ``drhodt`` of both pair endpoints: the
+    counting functor of the reference's sweep tests
+    (test/test_interaction_sweep.jl:14-30)."""
+
+    kind = C.GC_PFN_COUNT
+
+
+def _pfn_kind(p):
+    return C.GC_PFN_NONE if p is None else p.kind
+
+
+def _pfn_params(p):
+    return _Pfn().params() if p is None else p.params()
+
+
+# ---------------------------------------------------------- state updaters
+
+class _Updater:
+    kind = C.GC_UPD_NONE
+
+    def params(self):
+        return np.zeros(C.GC_UPD_NPARAM)
+
+
+class ZeroFieldUpdater(_Updater):
+    """src/StateUpdaters.jl:30-42."""
+
+    kind = C.GC_UPD_ZERO_FIELDS
+    _ok = {"strain_rate": C.GC_FIELD_STRAIN_RATE, "vorticity": C.GC_FIELD_VORTICITY,
+           "p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS, "dvdt": C.GC_FIELD_DVDT,
+           "drhodt": C.GC_FIELD_DRHODT}
+
+    def __init__(self, *fields):
+        names = [str(f).lstrip(":") for f in fields]
+        for n in names:
+            if n not in self._ok:
+                raise ArgumentError(f"ZeroFieldUpdater: unsupported field :{n}")
+        self.fields = tuple(names)
+
+    def params(self):
+        p = super().params()
+        mask = 0
+        for n in self.fields:
+            mask |= 1 << self._ok[n]
+        p[0] = float(mask)
+        return p
+
+
+class TaitEOSUpdater(_Updater):
+    """p = ρ0 c²/γ ((ρ/ρ0)^γ − 1), src/StateUpdaters.jl:108-118."""
+
+    kind = C.GC_UPD_TAIT_EOS
+
+    def __init__(self, rho0, *, gamma=7.0):
+        self.rho0 = float(rho0)
+        self.gamma = float(gamma)
+
+    def params(self):
+        p = super().params()
+        p[0], p[1] = self.rho0, self.gamma
+        return p
+
+
+class LinearEOSUpdater(_Updater):
+    """p = c² (ρ − ρ0), src/StateUpdaters.jl:131-140."""
+
+    kind = C.GC_UPD_LINEAR_EOS
+
+    def __init__(self, rho0):
+        self.rho0 = float(rho0)
+
+    def params(self):
+        p = super().params()
+        p[0] = self.rho0
+        return p
+
+
+class ElastoPlasticStressUpdater(_Updater):
+    """Jaumann + Drucker–Prager return mapping, src/StateUpdaters.jl:202-335."""
+
+    kind = C.GC_UPD_ELASTOPLASTIC
+
+    def __init__(self, E, nu, phi, psi, cohesion):
+        self.E, self.nu, self.phi, self.psi, self.cohesion = map(float, (E, nu, phi, psi, cohesion))
+
+    def params(self):
+        p = super().params()
+        p[:5] = [self.E, self.nu, self.phi, self.psi, self.cohesion]
+        return p
+
+
+class HookeLawStressUpdater(_Updater):
+    """Plane-strain Hooke update, src/StateUpdaters.jl:356-405."""
+
+    kind = C.GC_UPD_HOOKE
+
+    def __init__(self, E, nu):
+        self.E, self.nu = float(E), float(nu)
+
+    def params(self):
+        p = super().params()
+        p[0], p[1] = self.E, self.nu
+        return p
+
+
+def updater_chains(ps: AbstractParticleSystem):
+    """The state_updater tuple as per-stage chains of (kind, params)."""
+    chains = []
+    for entry in ps.state_updater:
+        if entry is None:
+            chains.append([])
+        elif isinstance(entry, tuple):
+            chains.append([(u.kind, u.params()) for u in entry if u is not None])
+        elif isinstance(entry, _Updater):
+            chains.append([(entry.kind, entry.params())])
+        else:
+            raise ArgumentError(f"unsupported state updater {type(entry).__name__}")
+    return chains
+
+
+# ------------------------------------------------------------ interaction
+
+class SystemInteraction:
+    """src/Interaction.jl:23-92."""
+
+    def __init__(self, kernel: AbstractKernel, pairwise_fn, system_a, system_b=None):
+        nd = system_a.ndims
+        if kernel.ndims != nd:
+            raise ArgumentError(f"kernel.ndims ({kernel.ndims}) must match system_a.ndims ({nd})")
+        if system_b is not None and system_b.ndims != nd:
+            raise ArgumentError(
+                f"system_b.ndims ({system_b.ndims}) must match system_a.ndims ({nd})")
+        if not isinstance(system_a, AbstractParticleSystem):
+            raise ArgumentError("system_a must be a particle system")
+        self.kernel = kernel
+        self.pfns = pairwise_fn if isinstance(pairwise_fn, tuple) else (pairwise_fn,)
+        self.system_a = system_a
+        self.system_b = system_b
+        self.ndims = nd
+        self._cell_size = 2.0 * kernel.h
+
+    def is_coupled(self):
+        return self.system_b is not None
+
+
+def is_coupled(si: SystemInteraction) -> bool:
+    return si.is_coupled()
+
+
+# ------------------------------------------------------------- integrator
+
+class LeapFrogTimeIntegrator:
+    """src/TimeIntegration.jl:29-67."""
+
+    def __init__(self, systems, interactions, *, ghosts=(), gamma=0.0, **kw):
+        if "Γ" in kw:
+            gamma = kw.pop("Γ")
+        if kw:
+            raise ArgumentError(f"unsupported integrator options {sorted(kw)}")
+        sys_ = (systems,) if isinstance(systems, AbstractParticleSystem) else tuple(systems)
+        ints = (interactions,) if isinstance(interactions, SystemInteraction) else tuple(interactions)
+        gsts = (ghosts,) if isinstance(ghosts, GhostEntry) else tuple(ghosts)
+        if not sys_:
+            raise ArgumentError("systems must not be empty")
+        if not ints:
+            raise ArgumentError("interactions must not be empty")
+        self.systems = sys_
+        self.interactions = ints
+        self.ghosts = gsts
+        self.c = max(ps.c for ps in sys_)
+        self.h = min(it.kernel.h for it in ints)
+        self.gamma = float(gamma)
+        self._device = None

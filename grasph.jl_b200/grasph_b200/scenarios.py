@@ -1,0 +1,208 @@
+"""Synthetic scenario builders with the shapes of the benchmark workloads.
+
+Every builder returns a `LeapFrogTimeIntegrator` assembled from the
+reference-API mirror plus a dict of metadata (dt inputs, counts).  Geometry
+follows the reference's example scripts: lattice fluid at (i+½)dx, boundary
+walls as 3-layer `DynamicBoundarySystem`s (DambreakWall.jl:107-172 pattern),
+the elasto-plastic column with a dynamic bottom and a ghost-mirrored left
+wall (EP_ColumnCollapse.jl:13-129).  Inputs the reference scripts do not
+build themselves are constructed here:
+  * hydrostatic initial density (inverse of the Tait EOS,
+    src/StateUpdaters.jl:117) for the dam breaks;
+  * geostatic K0 initial stress for the columns (the reference starts EP
+    stress at zero, src/Particles.jl:410).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, DynamicBoundarySystem,
+                    ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
+                    GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator,
+                    StrainRateVorticityPfn, SystemInteraction, TaitEOSUpdater, ZeroFieldUpdater)
+
+G = 9.81
+
+
+def _tait_pressure(rho, rho0, c, gamma):
+    return rho0 * c * c / gamma * ((rho / rho0) ** gamma - 1.0)
+
+
+def _wall(name, pts, mass, c, rho0):
+    ps = BasicParticleSystem(name, len(pts), pts.shape[1], mass, c)
+    ps.x[:] = pts
+    ps.rho[:] = rho0
+    return ps
+
+
+# ------------------------------------------------------------ dam break 2-D
+
+def dambreak_2d(nx=50, ny=100, dx=0.02, tank=(4.0, 4.0), layers=3, rho0=1000.0, gamma=7.0,
+                alpha=0.01, beta=0.0, hfac=1.2, cfl=0.2, wall_beta=3.0):
+    """2-D weakly-compressible dam break (FP64 plain single instance).
+
+    Water column nx×ny at spacing dx in the lower-left corner of a tank of
+    `tank` metres with `layers` rows of boundary particles per wall."""
+    W, H = tank
+    col_h = ny * dx
+    c0 = 10.0 * math.sqrt(2.0 * G * col_h)
+    h = hfac * dx
+    mass = rho0 * dx * dx
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    x = np.stack([(ii.ravel() + 0.5) * dx, (jj.ravel() + 0.5) * dx], axis=1)
+    fluid = FluidParticleSystem("fluid", len(x), 2, mass, c0, source_v=[0.0, -G],
+                                state_updater=TaitEOSUpdater(rho0, gamma=gamma))
+    fluid.x[:] = x
+    fluid.rho[:] = rho0 * (1.0 + gamma * G * (col_h - x[:, 1]) / (c0 * c0)) ** (1.0 / gamma)
+    fluid.p[:] = _tait_pressure(fluid.rho, rho0, c0, gamma)
+
+    nwx = int(round(W / dx)) + 6
+    nwy = int(round(H / dx))
+    lay = np.arange(layers)
+    xs = -2.5 * dx + np.arange(nwx) * dx
+    ys = (np.arange(nwy) + 0.5) * dx
+    floor = np.array([(xv, -(l + 0.5) * dx) for l in lay for xv in xs])
+    top = np.array([(xv, H + (l + 0.5) * dx) for l in lay for xv in xs])
+    left = np.array([(-(l + 0.5) * dx, yv) for l in lay for yv in ys])
+    right = np.array([(W + (l + 0.5) * dx, yv) for l in lay for yv in ys])
+    walls = [("floor", floor, (0.0, 1.0), (0.0, 0.0)), ("left", left, (1.0, 0.0), (0.0, 0.0)),
+             ("right", right, (-1.0, 0.0), (W, 0.0)), ("top", top, (0.0, -1.0), (0.0, H))]
+    kernel = CubicSplineKernel(h, ndims=2)
+    pfn = FluidPfn(alpha, beta, h)
+    systems = [fluid]
+    inters = [SystemInteraction(kernel, pfn, fluid)]
+    for name, pts, nrm, pt in walls:
+        inner = _wall(name, pts, mass, c0, rho0)
+        systems.append(inner)
+        inters.append(SystemInteraction(kernel, pfn, fluid, DynamicBoundarySystem(inner, nrm, pt, wall_beta)))
+    lf = LeapFrogTimeIntegrator(systems, inters)
+    meta = dict(workload="dambreak_2d", n_fluid=fluid.n, n_boundary=sum(s.n for s in systems[1:]),
+                h=h, c0=c0, cfl=cfl, dt=cfl * h / c0, ndims=2)
+    return lf, meta
+
+
+# ------------------------------------------------------------ dam break 3-D
+
+def dambreak_3d(nx=100, ny=50, nz=200, dx=0.01, tank=(4.0, 1.0, 4.0), layers=3, rho0=1000.0, gamma=7.0,
+                alpha=0.01, beta=0.0, hfac=1.2, cfl=0.2, wall_beta=3.0):
+    """3-D dam break: fluid block nx×ny×nz (z vertical, as dambreak_3d.jl)
+    in a tank of `tank` metres with 3-layer dynamic walls on all six faces."""
+    X, Y, Z = tank
+    col_h = nz * dx
+    c0 = 10.0 * math.sqrt(2.0 * G * col_h)
+    h = hfac * dx
+    mass = rho0 * dx ** 3
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    x = np.stack([(ii.ravel() + 0.5) * dx, (jj.ravel() + 0.5) * dx, (kk.ravel() + 0.5) * dx], axis=1)
+    fluid = FluidParticleSystem("fluid", len(x), 3, mass, c0, source_v=[0.0, 0.0, -G],
+                                state_updater=TaitEOSUpdater(rho0, gamma=gamma))
+    fluid.x[:] = x
+    fluid.rho[:] = rho0 * (1.0 + gamma * G * (col_h - x[:, 2]) / (c0 * c0)) ** (1.0 / gamma)
+    fluid.p[:] = _tait_pressure(fluid.rho, rho0, c0, gamma)
+
+    nX, nY, nZ = (int(round(v / dx)) for v in (X, Y, Z))
+    ext_x = -2.5 * dx + np.arange(nX + 6) * dx
+    ext_y = -2.5 * dx + np.arange(nY + 6) * dx
+    in_y = (np.arange(nY) + 0.5) * dx
+    in_z = (np.arange(nZ) + 0.5) * dx
+    ext_x_l = ext_x
+    layers_off = [(l + 0.5) * dx for l in range(layers)]
+
+    def plane(a, b, fixed_axis, fixed_vals):
+        A, B = np.meshgrid(a, b, indexing="ij")
+        out = []
+        for f in fixed_vals:
+            cols = [None, None, None]
+            free = [ax for ax in range(3) if ax != fixed_axis]
+            cols[free[0]] = A.ravel()
+            cols[free[1]] = B.ravel()
+            cols[fixed_axis] = np.full(A.size, f)
+            out.append(np.stack(cols, axis=1))
+        return np.concatenate(out)
+
+    walls = [
+        ("floor", plane(ext_x, ext_y, 2, [-o for o in layers_off]), (0, 0, 1.0), (0, 0, 0.0)),
+        ("ceiling", plane(ext_x, ext_y, 2, [Z + o for o in layers_off]), (0, 0, -1.0), (0, 0, Z)),
+        ("left", plane(in_y, in_z, 0, [-o for o in layers_off]), (1.0, 0, 0), (0.0, 0, 0)),
+        ("right", plane(in_y, in_z, 0, [X + o for o in layers_off]), (-1.0, 0, 0), (X, 0, 0)),
+        ("front", plane(ext_x_l, in_z, 1, [-o for o in layers_off]), (0, 1.0, 0), (0, 0.0, 0)),
+        ("back", plane(ext_x_l, in_z, 1, [Y + o for o in layers_off]), (0, -1.0, 0), (0, Y, 0)),
+    ]
+    kernel = CubicSplineKernel(h, ndims=3)
+    pfn = FluidPfn(alpha, beta, h)
+    systems = [fluid]
+    inters = [SystemInteraction(kernel, pfn, fluid)]
+    for name, pts, nrm, pt in walls:
+        inner = _wall(name, pts, mass, c0, rho0)
+        systems.append(inner)
+        inters.append(SystemInteraction(kernel, pfn, fluid, DynamicBoundarySystem(inner, nrm, pt, wall_beta)))
+    lf = LeapFrogTimeIntegrator(systems, inters)
+    meta = dict(workload="dambreak_3d", n_fluid=fluid.n, n_boundary=sum(s.n for s in systems[1:]),
+                h=h, c0=c0, cfl=cfl, dt=cfl * h / c0, ndims=3)
+    return lf, meta
+
+
+# ---------------------------------------------------------- column collapse
+
+def column_collapse(nx=400, ny=200, dx=0.0005, rho0=2650.0, E=0.84e6, nu=0.3, phi_deg=19.8, psi=0.0,
+                    cohesion=0.0, alpha=0.1, beta=0.1, hfac=1.5, cfl=0.1, bottom_len=None, layers=3,
+                    wall_beta=3.0, geostatic=True):
+    """2-D granular column collapse with the elasto-plastic Drucker–Prager
+    updater (EP_ColumnCollapse.jl layout): column nx×ny, dynamic bottom of
+    `layers` rows, ghost-mirrored left wall at x=0 (cutoff 3h, stress copied
+    at stage 1), stages (StrainRateVorticityPfn, CauchyFluidPfn)."""
+    phi = phi_deg * math.pi / 180.0
+    c = math.sqrt(E * (1 - nu) / (rho0 * (1 + nu) * (1 - 2 * nu)))
+    h = hfac * dx
+    mass = rho0 * dx * dx
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    x = np.stack([(ii.ravel() + 0.5) * dx, (jj.ravel() + 0.5) * dx], axis=1)
+    fluid = ElastoPlasticParticleSystem(
+        "soil", len(x), 2, 4, mass, c, source_v=[0.0, -G],
+        state_updater=(ZeroFieldUpdater("strain_rate", "vorticity"),
+                       ElastoPlasticStressUpdater(E, nu, phi, psi, cohesion)))
+    fluid.x[:] = x
+    fluid.rho[:] = rho0
+    if geostatic:
+        Hc = ny * dx
+        K0 = 1.0 - math.sin(phi)
+        syy = -rho0 * G * (Hc - x[:, 1])
+        fluid.stress[:, 0] = K0 * syy
+        fluid.stress[:, 1] = syy
+        fluid.stress[:, 2] = K0 * syy
+    if bottom_len is None:
+        bottom_len = max(2.5 * nx * dx, nx * dx + 20 * dx)
+    nbx = int(round(bottom_len / dx))
+    bx = np.array([((i - 3.5) * dx, -(j - 0.5) * dx) for i in range(1, nbx + 4) for j in range(1, layers + 1)])
+    bottom = _wall("bottom", bx, mass, c, rho0)
+    ghost = GhostParticleSystem(fluid, GhostCopier("stress"))
+    gentry = GhostEntry(ghost, 3.0 * h, ((1.0, 0.0), (0.0, 0.0)), capacity=int(fluid.n))
+    kernel = CubicSplineKernel(h, ndims=2)
+    srv = StrainRateVorticityPfn()
+    cau = CauchyFluidPfn(alpha, beta, h)
+    dyn = DynamicBoundarySystem(bottom, (0.0, 1.0), (0.0, 0.0), wall_beta)
+    inters = [SystemInteraction(kernel, (srv, cau), fluid),
+              SystemInteraction(kernel, (srv, cau), fluid, dyn),
+              SystemInteraction(kernel, (srv, cau), fluid, ghost)]
+    lf = LeapFrogTimeIntegrator([fluid, bottom], inters, ghosts=(gentry,))
+    meta = dict(workload="column_collapse", n_fluid=fluid.n, n_boundary=bottom.n, h=h, c0=c, cfl=cfl,
+                dt=cfl * h / c, ndims=2, phi=phi, E=E)
+    return lf, meta
+
+
+def batched_columns(count=256, seed=20261203, nmin=2000, nmax=60000, dx=0.0005, **kw):
+    """`count` column collapses with log-uniform particle counts, aspect
+    ratio H/W ~ U[0.5, 4], friction angle ~ U[25°, 40°], E ~ U[0.5, 5] MPa."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        N = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
+        ar = rng.uniform(0.5, 4.0)
+        nx = max(2, int(round(math.sqrt(N / ar))))
+        ny = max(2, int(round(N / nx)))
+        phi = rng.uniform(25.0, 40.0)
+        E = rng.uniform(0.5e6, 5.0e6)
+        out.append(column_collapse(nx=nx, ny=ny, dx=dx, phi_deg=phi, E=E, **kw))
+    return out

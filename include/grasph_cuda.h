@@ -1,0 +1,254 @@
+/*
+ * grasph_cuda.h — C ABI of libgrasph_cuda.so, the sm_100a implementation of
+ * Grasph.jl's per-timestep SPH hot path (sort → grid → ghosts → staged sweeps
+ * → leapfrog update).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (GC_OK == 0).  A failed call leaves a message that
+ * gc_last_error() returns.  Host arrays use the memory layout Julia gives a
+ * `Vector{SVector{K,Float64}}`: particle-major, K consecutive doubles per
+ * particle (`pointer(ps.x)` under `GC.@preserve`).  Integer fields (`id`,
+ * ghost `idx_original`/`idx_boundary`) are int64 and 1-based as in Julia.
+ *
+ * Each declaration names the Grasph.jl function or constructor it replaces
+ * (file:line in the Grasph.jl source tree).
+ *
+ * Objects live in a context (one CUDA device, one stream).  A context holds
+ * one or more *instances*: independent simulations that share one model
+ * structure (the same kinds of systems, interactions, functors and updaters
+ * in the same order) but may differ in particle counts and parameters.  A
+ * single-rank Grasph.jl run is one instance; batched runs pack many.
+ */
+#ifndef GRASPH_CUDA_H
+#define GRASPH_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    GC_OK = 0,
+    GC_ERR_ARG = 1,               /* invalid argument (Julia ArgumentError)        */
+    GC_ERR_OOM = 2,               /* device allocation failed / budget exceeded     */
+    GC_ERR_CAPACITY = 3,          /* ghost, cell or neighbour capacity overflow     */
+    GC_ERR_NONFINITE = 4,         /* NaN/Inf or out-of-Int64 position (InexactError)*/
+    GC_ERR_GRID_INCONSISTENT = 5, /* sort-key order disagrees with grid-cell order  */
+    GC_ERR_TIMEOUT = 6,           /* a bounded device wait ran out                  */
+    GC_ERR_CUDA = 7,              /* CUDA runtime error                             */
+    GC_ERR_STATE = 8,             /* call made in the wrong lifecycle state         */
+    GC_ERR_UNSUPPORTED = 9        /* functor/system combination not implemented     */
+};
+
+/* ---------------------------------------------------------- system kinds */
+/* src/Particles.jl:38 (Basic), :149 (Fluid), :245 (Stress), :351 (ElastoPlastic) */
+enum {
+    GC_SYS_BASIC = 0,
+    GC_SYS_FLUID = 1,
+    GC_SYS_STRESS = 2,
+    GC_SYS_ELASTOPLASTIC = 3
+};
+
+/* ------------------------------------------------------------- field ids */
+/* Per-particle arrays of src/Sorting.jl:15-26 plus ghost bookkeeping.      */
+enum {
+    GC_FIELD_X = 0,            /* ND doubles                                  */
+    GC_FIELD_V = 1,            /* ND doubles                                  */
+    GC_FIELD_RHO = 2,          /* 1 double                                    */
+    GC_FIELD_DVDT = 3,         /* ND doubles                                  */
+    GC_FIELD_DRHODT = 4,       /* 1 double                                    */
+    GC_FIELD_P = 5,            /* 1 double   (Fluid, Stress, ElastoPlastic)   */
+    GC_FIELD_STRESS = 6,       /* NS doubles (Stress, ElastoPlastic)          */
+    GC_FIELD_STRAIN_RATE = 7,  /* NS doubles (Stress, ElastoPlastic)          */
+    GC_FIELD_VORTICITY = 8,    /* 1 double in 2-D, 3 in 3-D (ElastoPlastic)   */
+    GC_FIELD_STRAIN = 9,       /* NS doubles (ElastoPlastic)                  */
+    GC_FIELD_STRAIN_P = 10,    /* NS doubles (ElastoPlastic)                  */
+    GC_FIELD_ID = 11,          /* int64, 1-based                              */
+    GC_FIELD_V_ADJUSTMENT = 12,/* ND doubles (always zero without XSPH)       */
+    GC_FIELD_IDX_ORIGINAL = 13,/* ghosts: int64 source index, 1-based         */
+    GC_FIELD_IDX_BOUNDARY = 14,/* ghosts: int64 plane index, 1-based          */
+    GC_FIELD_NORMALS = 15,     /* ghosts: ND doubles                          */
+    GC_NFIELDS = 16
+};
+
+/* ------------------------------------------------------ boundary wrappers */
+/* src/BoundaryParticles.jl:38 (StaticBoundarySystem), :68 (DynamicBoundarySystem) */
+enum { GC_WRAP_DYNAMIC = 1, GC_WRAP_STATIC = 2 };
+
+/* ---------------------------------------------------------- kernel kinds */
+/* src/Kernels.jl:18 (CubicSplineKernel), :92 (WenlandC2Kernel)             */
+enum { GC_KERNEL_CUBIC_SPLINE = 0, GC_KERNEL_WENDLAND_C2 = 1 };
+
+/* ------------------------------------------------- pairwise functor kinds */
+/* src/PairwiseFunctors.jl.  GC_PFN_COUNT is the counting functor the
+ * reference's sweep tests use (test/test_interaction_sweep.jl:14-30): each
+ * accepted pair adds 1 to dvdt[.][1] and drhodt of both endpoints.          */
+enum {
+    GC_PFN_NONE = 0,                    /* `nothing` stage                     */
+    GC_PFN_FLUID = 1,                   /* FluidPfn :136                       */
+    GC_PFN_CAUCHY_FLUID = 2,            /* CauchyFluidPfn :252                 */
+    GC_PFN_STRAIN_RATE = 3,             /* StrainRatePfn :18                   */
+    GC_PFN_STRAIN_RATE_VORTICITY = 4,   /* StrainRateVorticityPfn :78          */
+    GC_PFN_COUNT = 5
+};
+/* Per-stage functor parameters, GC_PFN_NPARAM doubles each:
+ *   [0] art_visc_alpha  [1] art_visc_beta  [2] h
+ *   [3] sigma S (FluidPfn; 2 = Monaghan form)  [4] delta (NaN = nothing)
+ *   [5] epsilon (NaN = nothing)                                            */
+#define GC_PFN_NPARAM 6
+
+/* ---------------------------------------------------------- updater kinds */
+/* src/StateUpdaters.jl                                                     */
+enum {
+    GC_UPD_NONE = 0,          /* `nothing`                                  */
+    GC_UPD_ZERO_FIELDS = 1,   /* ZeroFieldUpdater :30; param[0] = bitmask of 1<<GC_FIELD_* */
+    GC_UPD_TAIT_EOS = 2,      /* TaitEOSUpdater :108; [0] rho0 [1] gamma    */
+    GC_UPD_LINEAR_EOS = 3,    /* LinearEOSUpdater :131; [0] rho0            */
+    GC_UPD_ELASTOPLASTIC = 4, /* ElastoPlasticStressUpdater :202; [0] E [1] nu [2] phi [3] psi [4] cohesion */
+    GC_UPD_HOOKE = 5          /* HookeLawStressUpdater :356; [0] E [1] nu   */
+};
+#define GC_UPD_NPARAM 6
+/* At most this many updaters may be chained in one stage (a Julia tuple of
+ * functors inside the per-stage tuple).                                    */
+#define GC_UPD_MAX_CHAIN 4
+
+/* ------------------------------------------------------- ghost copy modes */
+/* src/GhostParticles.jl:53 (GhostCopier), :26 (HouseholderReflect)          */
+enum { GC_COPY_PLAIN = 0, GC_COPY_HOUSEHOLDER = 1 };
+
+/* ------------------------------------------------------------- precision */
+enum {
+    GC_PRECISION_FP64 = 0,             /* reference arithmetic, FP64 throughout    */
+    GC_PRECISION_FP32_COMPENSATED = 1  /* FP32 pair sweep, Kahan sums, FP64 state  */
+};
+
+typedef struct gc_ctx gc_ctx;
+
+typedef struct gc_stats {
+    int64_t steps_done;          /* leapfrog steps completed in this context      */
+    int64_t pairs_last_step;     /* accepted pairs of the last step, all stages   */
+    int64_t grid_inconsistent;   /* cells where key order and cell order disagreed */
+    int64_t resorts;             /* steps whose sort took the slow (permuting) path */
+    int32_t last_status;         /* device error word of the last step            */
+    int32_t pad;
+} gc_stats;
+
+/* ============================================================ lifecycle */
+/* Create a context on `device`; `hbm_budget_bytes` caps device allocations
+ * (0 = no cap).                                                           */
+int gc_ctx_create(int device, size_t hbm_budget_bytes, gc_ctx** out);
+int gc_ctx_destroy(gc_ctx* ctx);
+const char* gc_last_error(gc_ctx* ctx);
+const char* gc_status_string(int status);
+
+/* Add an instance (an independent simulation).                            */
+int gc_instance_add(gc_ctx* ctx, int* inst_out);
+
+/* ====================================================== model building */
+/* BasicParticleSystem / FluidParticleSystem / StressParticleSystem /
+ * ElastoPlasticParticleSystem constructors, src/Particles.jl:61,173,272,381.
+ * `ns` is ignored for Basic/Fluid.  Returns a handle in *sys_out.          */
+int gc_add_system(gc_ctx* ctx, int inst, int kind, int64_t n, int ndims, int ns,
+                  double mass, double c, const double* source_v, double source_rho,
+                  int* sys_out);
+
+/* DynamicBoundarySystem(inner, normal, point, beta) src/BoundaryParticles.jl:79
+ * or StaticBoundarySystem(inner, lj_cutoff) :47.  `normal`/`point` are
+ * ignored for the static kind.  Returns a handle usable as system_b.       */
+int gc_add_boundary(gc_ctx* ctx, int inst, int sys, int kind, const double* normal,
+                    const double* point, double beta_or_lj_cutoff, int* handle_out);
+
+/* GhostParticleSystem(ps, copiers...) src/GhostParticles.jl:199 together with
+ * GhostEntry(ghost, cutoff, (normal, point)...) :317.
+ * Copier k (stage k+1) lists copier_nfields[k] (field, mode) entries, taken
+ * consecutively from copier_fields/copier_modes; 0 entries = `nothing`.
+ * `normals`/`points` hold nplanes×ndims doubles.  `capacity` bounds the ghost
+ * count (0 = the source's particle count × nplanes).                        */
+int gc_add_ghost(gc_ctx* ctx, int inst, int src_sys, int ncopiers,
+                 const int* copier_nfields, const int* copier_fields, const int* copier_modes,
+                 int nplanes, const double* normals, const double* points, double cutoff,
+                 int64_t capacity, int* handle_out);
+
+/* SystemInteraction(kernel, pfns, system_a[, system_b]) src/Interaction.jl:61,
+ * with CubicSplineKernel(h; ndims) src/Kernels.jl:34 or WenlandC2Kernel :108.
+ * b_handle = -1 for a self interaction.  pfn_params holds
+ * nstages×GC_PFN_NPARAM doubles.                                           */
+int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kernel_kind,
+                       double h, int nstages, const int* pfn_kinds, const double* pfn_params,
+                       int* inter_out);
+
+/* The `state_updater` tuple of a system (src/Particles.jl:200): nstages
+ * entries, each a chain of `chain_len[s]` updaters (kinds / GC_UPD_NPARAM
+ * params taken consecutively).                                            */
+int gc_set_updaters(gc_ctx* ctx, int inst, int sys, int nstages, const int* chain_len,
+                    const int* kinds, const double* params);
+
+/* LeapFrogTimeIntegrator(systems, interactions; ghosts, Γ)
+ * src/TimeIntegration.jl:53.  The systems list is every system added to
+ * the instance in order; the ghosts list every ghost handle.              */
+int gc_set_integrator(gc_ctx* ctx, int inst, double damping_gamma);
+
+/* Validate every instance against instance 0's structure and allocate the
+ * device state.  Model-building calls are refused afterwards.              */
+int gc_finalize(gc_ctx* ctx);
+
+/* ============================================================ state I/O */
+/* Copy one per-particle field between host (Julia AoS layout) and device.
+ * `bytes` must equal n×components×8.  Ghost handles accept the ghost fields
+ * (x, v, rho, p, stress, idx_original, idx_boundary, normals).              */
+int gc_upload_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes);
+int gc_download_field(gc_ctx* ctx, int inst, int handle, int field, void* host, size_t bytes);
+/* Current particle count of a handle (ghost counts change every step).    */
+int gc_get_count(gc_ctx* ctx, int inst, int handle, int64_t* n_out);
+
+/* ============================================================ stepping */
+int gc_set_precision(gc_ctx* ctx, int mode);
+
+/* time_integrate!(::LeapFrogTimeIntegrator, nsteps, ...) loop body
+ * src/TimeIntegration.jl:645-693 for every instance, dt = CFL·h_min/c_max
+ * per instance (:598).  Printing and HDF5 output stay on the Julia side.   */
+int gc_step(gc_ctx* ctx, int nsteps, double cfl);
+
+int gc_get_stats(gc_ctx* ctx, gc_stats* out);
+
+/* ======================================================== phase hooks */
+/* The same device kernels, one reference phase at a time (parity tests and
+ * the per-phase Julia entry points).                                      */
+
+/* sort_particles!(ps, cutoff, ...) src/Sorting.jl:157.  perm_out (may be
+ * NULL) receives n 1-based source indices: new position k holds old
+ * particle perm_out[k].                                                   */
+int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* perm_out);
+
+/* create_grid!(si) src/Interaction.jl:123.  Outputs (each may be NULL):
+ * cell_start (1-based, length ncells+1, `cap` entries available),
+ * mingridx (ND doubles), ngridx (ND int64), ncells.                        */
+int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int64_t cap,
+                  double* mingridx_out, int64_t* ngridx_out, int64_t* ncells_out);
+
+/* generate_ghosts!(ge) src/GhostParticles.jl:344 (unsorted, generation order) */
+int gc_generate_ghosts(gc_ctx* ctx, int inst, int ghost);
+/* update_ghost_kinematics!(ge) src/GhostParticles.jl:404                  */
+int gc_update_ghost_kinematics(gc_ctx* ctx, int inst, int ghost);
+/* update_ghost!(ge, stage) src/GhostParticles.jl:277,423 (stage is 1-based) */
+int gc_update_ghost(gc_ctx* ctx, int inst, int ghost, int stage);
+
+/* sweep!(si, stage) src/Interaction.jl:292 — adds this interaction's pair
+ * terms of `stage` (1-based) into the current accumulators.  Requires a
+ * grid from gc_build_grid.                                                */
+int gc_sweep(gc_ctx* ctx, int inst, int inter, int stage);
+
+/* update_state!(ps, stage, dt) src/Particles.jl:542 (stage 1-based).     */
+int gc_update_state(gc_ctx* ctx, int inst, int sys, int stage, double dt);
+
+/* Accepted-pair count per system_a particle of an interaction, from the
+ * grid of the last gc_build_grid / gc_step (n_a int32 values).             */
+int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRASPH_CUDA_H */

@@ -1,0 +1,1755 @@
+// grasph_oracle.cpp — TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+//
+// A plain C++17 restatement of Grasph.jl's per-timestep SPH path, used as the
+// parity checker for libgrasph_cuda.so.  Only tests/, __graft_entry__.smoke()
+// and bench.py's CPU-baseline leg may load it.  The product library never
+// links, loads or falls back to it.
+//
+// Every routine follows the reference's own loop order and expression trees
+// (file:line cited per function), compiled with -ffp-contract=off and no
+// fast-math so the FP64 arithmetic is the reference's arithmetic:
+//   * SVector operations are per component, dot products are left-to-right
+//     sums of products (StaticArrays 1.9 `_vecdot`);
+//   * `x^3` is x*x*x (Julia literal_pow), `x^2` is x*x;
+//   * `@fastmath` axpy on scalar fields (src/Utils.jl:19-29) is taken as a
+//     fused multiply-add, on SVector fields as separate multiply and add
+//     (Base.FastMath falls back to plain operators for non-scalar types);
+//   * `x^y` with an integer-valued Float64 y and `x^n` with an Int n use a
+//     compensated power-by-squaring (Graillat, Langlois & Louvet, "Algorithms
+//     for accurate, validated and fast polynomial evaluation", 2009 — the
+//     compensated-power scheme), which is the method Julia 1.12 applies to
+//     these cases; other real powers call std::pow.
+// The coloured sweeps can run on OpenMP threads; colours make every thread's
+// writes disjoint, so threaded results equal serial results bit for bit.
+//
+// Parity status: the sort, grid, neighbour sets and per-pair arithmetic are
+// pinned by the reference's known-answer tests (ported under tests/).  Tait
+// EOS, artificial-viscosity, Lennard-Jones, dynamic-boundary and continuity
+// magnitudes have no known-answer test in the reference and are pinned only
+// by this restatement (Julia is not available to run the reference itself).
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <array>
+#include <numeric>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/grasph_cuda.h"
+
+namespace {
+
+// ------------------------------------------------------------------ helpers
+
+// Julia `min`/`max` on Float64: NaN propagates; min(-0.0, 0.0) == -0.0.
+inline double jmin(double a, double b) {
+    if (std::isnan(a) || std::isnan(b)) return a - b;  // NaN
+    if (a < b) return a;
+    if (b < a) return b;
+    return std::signbit(a) ? a : b;
+}
+inline double jmax(double a, double b) {
+    if (std::isnan(a) || std::isnan(b)) return a - b;
+    if (a > b) return a;
+    if (b > a) return b;
+    return std::signbit(a) ? b : a;
+}
+
+// Julia floor(Int, v): InexactError when v is not representable.
+inline bool floor_int(double v, int64_t* out) {
+    double f = std::floor(v);
+    if (!(f >= -9.2233720368547758e18 && f < 9.2233720368547758e18)) return false;
+    *out = (int64_t)f;
+    return true;
+}
+
+// Error-free product a*b = p + e (exact with a correctly rounded fma).
+inline void two_prod(double a, double b, double* p, double* e) {
+    *p = a * b;
+    *e = std::fma(a, b, -*p);
+}
+
+// Compensated x^n for integer n (power by squaring with the rounding error of
+// each product carried in a second word).
+double comp_powi(double x, int64_t n) {
+    if (n == 0) return 1.0;
+    if (n == 3) return x * x * x;
+    double xl = 0.0;
+    if (n < 0) {
+        double rx = 1.0 / x;
+        if (n == -2) return rx * rx;
+        if (std::isfinite(x)) xl = -std::fma(x, rx, -1.0) * rx;
+        x = rx;
+        n = -n;
+    }
+    double y = 1.0, yl = 0.0;
+    while (n > 1) {
+        if (n & 1) {
+            double err = y * xl + x * yl;
+            double p, e;
+            two_prod(x, y, &p, &e);
+            y = p;
+            yl = e + err;
+        }
+        double err = x * 2.0 * xl;
+        double p, e;
+        two_prod(x, x, &p, &e);
+        x = p;
+        xl = e + err;
+        n >>= 1;
+    }
+    double err = y * xl + x * yl;
+    if (std::isfinite(x) && std::isfinite(err)) return std::fma(x, y, err);
+    return x * y;
+}
+
+double jpow(double x, double y) {
+    if (y == std::trunc(y) && std::fabs(y) < 9.0e15) return comp_powi(x, (int64_t)y);
+    return std::pow(x, y);
+}
+
+// ------------------------------------------------------------------ model
+
+struct Upd {
+    int kind;
+    double prm[GC_UPD_NPARAM];
+};
+
+struct Sys {
+    int kind = GC_SYS_BASIC, nd = 2, ns = 0, nvort = 0;
+    int64_t n = 0;
+    double mass = 0, c = 0, srcv[3] = {0, 0, 0}, srcrho = 0;
+    std::vector<double> x, v, vadj, rho, dvdt, drhodt, p, stress, sr, vort, strain, strainp;
+    std::vector<int64_t> id;
+    bool upd_set = false;
+    std::vector<std::vector<Upd>> upd;  // one chain per updater-tuple entry
+    std::vector<double> q0v, q0rho;
+    bool has_p() const { return kind >= GC_SYS_FLUID; }
+    bool has_stress() const { return kind >= GC_SYS_STRESS; }
+    bool is_ep() const { return kind == GC_SYS_ELASTOPLASTIC; }
+};
+
+struct Copier {
+    std::vector<std::pair<int, int>> entries;  // (field, mode)
+};
+
+struct Ghost {
+    int src = 0;
+    double cutoff = 0;
+    int nplanes = 0;
+    std::vector<double> pn, pp;
+    std::vector<Copier> copiers;
+    bool ex_p = false, ex_stress = false;
+    int64_t n = 0;
+    std::vector<double> x, v, rho, normals, p, stress;
+    std::vector<int64_t> io, ib;
+};
+
+enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3 };
+struct Handle {
+    int type = H_SYS;
+    int idx = 0;  // system index (H_SYS, wrappers) or ghost index
+    double normal[3] = {0, 0, 0}, point[3] = {0, 0, 0};
+    double beta = 0, ljcut = 0;
+};
+
+struct Inter {
+    int a = 0;      // system index
+    int b = -1;     // handle index or -1
+    int kk = GC_KERNEL_CUBIC_SPLINE;
+    double H = 0;
+    int nstages = 0;
+    std::vector<int> pk;
+    std::vector<std::array<double, GC_PFN_NPARAM>> pp;
+    double cell = 0;
+    double ming[3] = {0, 0, 0};
+    int64_t ng[3] = {1, 1, 1};
+    std::vector<int64_t> cs, csa;
+    double mina[3] = {0, 0, 0}, maxa[3] = {0, 0, 0};
+    bool grid = false;
+};
+
+}  // namespace
+
+struct oracle_ctx {
+    std::vector<Sys> sys;
+    std::vector<Ghost> ghosts;
+    std::vector<Handle> handles;
+    std::vector<int> sys_handle;  // handle of each system
+    std::vector<Inter> inters;
+    double gamma = 0;
+    int threads = 1;
+    int64_t steps = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(oracle_ctx* c, int code, const char* msg) {
+    c->err = msg;
+    return code;
+}
+
+// ------------------------------------------------------------------ kernels
+// src/Kernels.jl:42-81 (cubic spline), :116-153 (Wendland C2)
+struct Kern {
+    int kind, nd;
+    double H, norm;
+};
+
+Kern make_kernel(int kind, int nd, double H) {
+    Kern k{kind, nd, H, 0.0};
+    const double pi = 3.141592653589793;
+    if (kind == GC_KERNEL_CUBIC_SPLINE) {
+        if (nd == 1) k.norm = 2.0 / (3.0 * H);
+        else if (nd == 2) k.norm = 10.0 / ((7.0 * pi) * (H * H));
+        else k.norm = 1.0 / (pi * (H * H * H));
+    } else {
+        if (nd == 2) k.norm = 7.0 / ((64.0 * pi) * (H * H));
+        else k.norm = 21.0 / ((256.0 * pi) * (H * H * H));
+    }
+    return k;
+}
+
+inline double kernel_w(const Kern& k, double q) {
+    if (k.kind == GC_KERNEL_CUBIC_SPLINE) {
+        double a = jmax(0.0, 2.0 - q), b = jmax(0.0, 1.0 - q);
+        return k.norm * (0.25 * (a * a * a) - (b * b * b));
+    }
+    double a = jmax(0.0, 2.0 - q);
+    double a2 = a * a;
+    return (k.norm * (a2 * a2)) * (2.0 * q + 1.0);
+}
+
+inline double kernel_dw_dq(const Kern& k, double q) {
+    if (k.kind == GC_KERNEL_CUBIC_SPLINE) {
+        double a = jmax(0.0, 2.0 - q), b = jmax(0.0, 1.0 - q);
+        return k.norm * (-3.0 * (0.25 * (a * a) - (b * b)));
+    }
+    double a = jmax(0.0, 2.0 - q);
+    return ((-k.norm * 10.0) * q) * (a * a * a);
+}
+
+// ------------------------------------------------------------- primitives
+// src/PairwisePhysics.jl
+
+template <int ND>
+inline double dot(const double* a, const double* b) {
+    double s = a[0] * b[0];
+    for (int d = 1; d < ND; ++d) s = s + a[d] * b[d];
+    return s;
+}
+
+// :29-34
+template <int ND>
+inline double art_visc(const double* dx, const double* dv, double h, double ri, double rj,
+                       double alpha, double beta, double ci, double cj) {
+    double vr = jmin(dot<ND>(dx, dv), 0.0);
+    double muv = (h * vr) / (dot<ND>(dx, dx) + (h * h) * 0.01);
+    double mc = 0.5 * (ci + cj);
+    return ((beta * muv - alpha * mc) * muv) / ((0.5 * ri) * rj);
+}
+
+// :58-69
+inline double pressure_coeff(double pi_, double pj, double ri, double rj, int S) {
+    if (S == 1) return -(pi_ + pj) / (ri * rj);
+    return -(pi_ / (ri * ri) + pj / (rj * rj));
+}
+
+// :99-105
+inline double cont_coeff(double ri, double rj, int S) { return S == 1 ? ri / rj : 1.0; }
+
+// :238-243 (the nine-argument form every functor calls)
+template <int ND>
+inline double diffusion(const double* dx, double ri, double rj, double ci, double cj, double hi,
+                        double hj, const double* gx, double delta, bool on) {
+    if (!on) return 0.0;
+    double rr = dot<ND>(dx, dx);
+    double c = 0.5 * (ci + cj);
+    double h = 0.5 * (hi + hj);
+    return (((((2.0 * delta) * c) * h) * (ri - rj)) * dot<ND>(dx, gx)) / rr;
+}
+
+// :258-263
+template <int ND>
+inline double lennard_jones(const double* dx, double cutoff, double c) {
+    double rr = dot<ND>(dx, dx);
+    double r = std::sqrt(rr);
+    double ind = r < cutoff ? 1.0 : 0.0;
+    double f = (ind * (comp_powi(cutoff / r, 12) - comp_powi(cutoff / r, 6))) / rr;
+    return ((0.01 * c) * c) * f;
+}
+
+// :125-151; out has ND components
+template <int ND>
+inline void cauchy(const double* si, const double* sj, int ns, double ri, double rj, const double* g,
+                   double* out) {
+    double ci = 1.0 / (ri * ri);
+    double cj = 1.0 / (rj * rj);
+    if (ND == 2) {
+        int xy = ns == 3 ? 2 : 3;
+        out[0] = (si[0] * g[0] + si[xy] * g[1]) * ci + (sj[0] * g[0] + sj[xy] * g[1]) * cj;
+        out[1] = (si[xy] * g[0] + si[1] * g[1]) * ci + (sj[xy] * g[0] + sj[1] * g[1]) * cj;
+    } else {
+        out[0] = (si[0] * g[0] + si[3] * g[1] + si[4] * g[2]) * ci +
+                 (sj[0] * g[0] + sj[3] * g[1] + sj[4] * g[2]) * cj;
+        out[1] = (si[3] * g[0] + si[1] * g[1] + si[5] * g[2]) * ci +
+                 (sj[3] * g[0] + sj[1] * g[1] + sj[5] * g[2]) * cj;
+        out[2] = (si[4] * g[0] + si[5] * g[1] + si[2] * g[2]) * ci +
+                 (sj[4] * g[0] + sj[5] * g[1] + sj[2] * g[2]) * cj;
+    }
+}
+
+// :169-195
+template <int ND>
+inline void strain_rate_t(const double* dv, const double* g, int ns, double* sr) {
+    if (ND == 2) {
+        sr[0] = dv[0] * g[0];
+        sr[1] = dv[1] * g[1];
+        if (ns == 4) {
+            sr[2] = 0.0;
+            sr[3] = 0.5 * (dv[0] * g[1] + dv[1] * g[0]);
+        } else {
+            sr[2] = 0.5 * (dv[0] * g[1] + dv[1] * g[0]);
+        }
+    } else {
+        sr[0] = dv[0] * g[0];
+        sr[1] = dv[1] * g[1];
+        sr[2] = dv[2] * g[2];
+        sr[3] = 0.5 * (dv[0] * g[1] + dv[1] * g[0]);
+        sr[4] = 0.5 * (dv[0] * g[2] + dv[2] * g[0]);
+        sr[5] = 0.5 * (dv[1] * g[2] + dv[2] * g[1]);
+    }
+}
+
+// :210-220
+template <int ND>
+inline void vorticity_t(const double* dv, const double* g, double* w) {
+    if (ND == 2) {
+        w[0] = 0.5 * (dv[0] * g[1] - dv[1] * g[0]);
+    } else {
+        w[0] = 0.5 * (dv[0] * g[1] - dv[1] * g[0]);
+        w[1] = 0.5 * (dv[0] * g[2] - dv[2] * g[0]);
+        w[2] = 0.5 * (dv[1] * g[2] - dv[2] * g[1]);
+    }
+}
+
+// ---------------------------------------------------------------- b views
+
+struct BView {
+    int type;  // H_SYS / H_DYN / H_STATIC / H_GHOST
+    int64_t n;
+    const double* x;
+    const double* v;
+    const double* rho;
+    const double* p;
+    const double* stress;
+    double mass, c;
+    int ns;
+    Sys* sys;  // backing system for two-sided writes (H_SYS and wrappers)
+    const double* normal;
+    const double* point;
+    double beta, ljcut;
+};
+
+struct Pfn {
+    int kind;
+    double alpha, beta, h;
+    int S;
+    double delta;
+    bool has_delta;
+};
+
+Pfn make_pfn(int kind, const double* prm) {
+    Pfn f;
+    f.kind = kind;
+    f.alpha = prm[0];
+    f.beta = prm[1];
+    f.h = prm[2];
+    f.S = (int)prm[3];
+    f.delta = prm[4];
+    f.has_delta = !std::isnan(prm[4]);
+    return f;
+}
+
+// --------------------------------------------------------- self functors
+// src/PairwiseFunctors.jl :20 (SR), :80 (SRV), :151 (Fluid), :265 (Cauchy)
+template <int ND>
+void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, const double* gx) {
+    const int ns = ps.ns;
+    switch (f.kind) {
+        case GC_PFN_FLUID: {
+            const double* vi = &ps.v[i * ND];
+            const double* vj = &ps.v[j * ND];
+            double ri = ps.rho[i], rj = ps.rho[j], pi_ = ps.p[i], pj = ps.p[j];
+            double mass = ps.mass;
+            double dv[ND];
+            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, ps.c, ps.c);
+            double dh = pressure_coeff(pi_, pj, ri, rj, f.S);
+            double s = mass * (dh - piv);
+            for (int d = 0; d < ND; ++d) {
+                double t = s * gx[d];
+                ps.dvdt[i * ND + d] = ps.dvdt[i * ND + d] + t;
+                ps.dvdt[j * ND + d] = ps.dvdt[j * ND + d] - t;
+            }
+            double dr = dot<ND>(dv, gx);
+            double psi = diffusion<ND>(dx, ri, rj, ps.c, ps.c, f.h, f.h, gx, f.delta, f.has_delta);
+            ps.drhodt[i] = ps.drhodt[i] + mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
+            ps.drhodt[j] = ps.drhodt[j] + mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri);
+            break;
+        }
+        case GC_PFN_CAUCHY_FLUID: {
+            const double* vi = &ps.v[i * ND];
+            const double* vj = &ps.v[j * ND];
+            double ri = ps.rho[i], rj = ps.rho[j];
+            double mass = ps.mass;
+            double dv[ND], hv[ND];
+            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, ps.c, ps.c);
+            cauchy<ND>(&ps.stress[i * ns], &ps.stress[j * ns], ns, ri, rj, gx, hv);
+            for (int d = 0; d < ND; ++d) {
+                double t = mass * (hv[d] - piv * gx[d]);
+                ps.dvdt[i * ND + d] = ps.dvdt[i * ND + d] + t;
+                ps.dvdt[j * ND + d] = ps.dvdt[j * ND + d] - t;
+            }
+            double dr = dot<ND>(dv, gx);
+            double psi = diffusion<ND>(dx, ri, rj, ps.c, ps.c, f.h, f.h, gx, f.delta, f.has_delta);
+            ps.drhodt[i] = ps.drhodt[i] + mass * (dr + psi / rj);
+            ps.drhodt[j] = ps.drhodt[j] + mass * (dr - psi / ri);
+            break;
+        }
+        case GC_PFN_STRAIN_RATE:
+        case GC_PFN_STRAIN_RATE_VORTICITY: {
+            double ri = ps.rho[i], rj = ps.rho[j];
+            double mass = ps.mass;
+            double dv[ND], sr[6], w[3];
+            for (int d = 0; d < ND; ++d) dv[d] = ps.v[j * ND + d] - ps.v[i * ND + d];
+            strain_rate_t<ND>(dv, gx, ns, sr);
+            double fi = mass / rj, fj = mass / ri;
+            for (int k = 0; k < ns; ++k) {
+                ps.sr[i * ns + k] = ps.sr[i * ns + k] + sr[k] * fi;
+                ps.sr[j * ns + k] = ps.sr[j * ns + k] + sr[k] * fj;
+            }
+            if (f.kind == GC_PFN_STRAIN_RATE_VORTICITY) {
+                vorticity_t<ND>(dv, gx, w);
+                const int nv = ps.nvort;
+                for (int k = 0; k < nv; ++k) {
+                    ps.vort[i * nv + k] = ps.vort[i * nv + k] + w[k] * fi;
+                    ps.vort[j * nv + k] = ps.vort[j * nv + k] + w[k] * fj;
+                }
+            }
+            break;
+        }
+        case GC_PFN_COUNT: {
+            ps.dvdt[i * ND] += 1.0;
+            ps.dvdt[j * ND] += 1.0;
+            ps.drhodt[i] += 1.0;
+            ps.drhodt[j] += 1.0;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// ------------------------------------------------------ coupled functors
+// src/PairwiseFunctors.jl: generic one-sided :37/:97/:193; dynamic
+// :53/:111/:222/:334; static :210/:322; ghost Cauchy :286; counting (tests).
+template <int ND>
+void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, const double* dx,
+                 const double* gx) {
+    const int ns = a.ns;
+    const double* vi = &a.v[i * ND];
+    if (f.kind == GC_PFN_COUNT) {
+        a.dvdt[i * ND] += 1.0;
+        a.drhodt[i] += 1.0;
+        b.sys->dvdt[j * ND] += 1.0;
+        b.sys->drhodt[j] += 1.0;
+        return;
+    }
+    if (b.type == H_DYN) {
+        double tmp[ND];
+        for (int d = 0; d < ND; ++d) tmp[d] = a.x[i * ND + d] - b.point[d];
+        double da = dot<ND>(tmp, b.normal);
+        for (int d = 0; d < ND; ++d) tmp[d] = b.x[j * ND + d] - b.point[d];
+        double db = dot<ND>(tmp, b.normal);
+        double m = -jmin(b.beta, std::fabs(db / da));
+        double vj[ND];
+        for (int d = 0; d < ND; ++d) vj[d] = m * vi[d];
+        double ri = a.rho[i];
+        double mass = a.mass;
+        switch (f.kind) {
+            case GC_PFN_FLUID: {
+                double pi_ = a.p[i];
+                double dv[ND];
+                for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+                double piv = art_visc<ND>(dx, dv, f.h, ri, ri, f.alpha, f.beta, a.c, a.c);
+                double dh = pressure_coeff(pi_, pi_, ri, ri, f.S);
+                double s = mass * (dh - piv);
+                for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + s * gx[d];
+                double dr = dot<ND>(dv, gx);
+                double psi = diffusion<ND>(dx, ri, ri, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
+                a.drhodt[i] = a.drhodt[i] + mass * (dr * cont_coeff(ri, ri, f.S) + psi / ri);
+                break;
+            }
+            case GC_PFN_CAUCHY_FLUID: {
+                double dv[ND], hv[ND];
+                for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+                double piv = art_visc<ND>(dx, dv, f.h, ri, ri, f.alpha, f.beta, a.c, a.c);
+                const double* si = &a.stress[i * ns];
+                cauchy<ND>(si, si, ns, ri, ri, gx, hv);
+                for (int d = 0; d < ND; ++d)
+                    a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + mass * (hv[d] - piv * gx[d]);
+                double dr = dot<ND>(dv, gx);
+                double psi = diffusion<ND>(dx, ri, ri, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
+                a.drhodt[i] = a.drhodt[i] + mass * (dr + psi / ri);
+                break;
+            }
+            case GC_PFN_STRAIN_RATE:
+            case GC_PFN_STRAIN_RATE_VORTICITY: {
+                double dv[ND], sr[6], w[3];
+                for (int d = 0; d < ND; ++d) dv[d] = vj[d] - vi[d];
+                strain_rate_t<ND>(dv, gx, ns, sr);
+                double fi = mass / ri;
+                for (int k = 0; k < ns; ++k) a.sr[i * ns + k] = a.sr[i * ns + k] + sr[k] * fi;
+                if (f.kind == GC_PFN_STRAIN_RATE_VORTICITY) {
+                    vorticity_t<ND>(dv, gx, w);
+                    for (int k = 0; k < a.nvort; ++k)
+                        a.vort[i * a.nvort + k] = a.vort[i * a.nvort + k] + w[k] * fi;
+                }
+                break;
+            }
+        }
+        return;
+    }
+    const double* vj = &b.v[j * ND];
+    double ri = a.rho[i], rj = b.rho[j];
+    if (b.type == H_STATIC && (f.kind == GC_PFN_FLUID || f.kind == GC_PFN_CAUCHY_FLUID)) {
+        double dv[ND];
+        for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+        double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, a.c);
+        double rf = lennard_jones<ND>(dx, b.ljcut, a.c);
+        double s = (-b.mass) * piv;
+        for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + (s * gx[d] + rf * dx[d]);
+        return;
+    }
+    switch (f.kind) {
+        case GC_PFN_FLUID: {  // generic one-sided :193
+            double pi_ = a.p[i], pj = b.p[j];
+            double dv[ND];
+            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, a.c);
+            double dh = pressure_coeff(pi_, pj, ri, rj, f.S);
+            double s = b.mass * (dh - piv);
+            for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + s * gx[d];
+            double dr = dot<ND>(dv, gx);
+            double psi = diffusion<ND>(dx, ri, rj, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
+            a.drhodt[i] = a.drhodt[i] + b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
+            break;
+        }
+        case GC_PFN_CAUCHY_FLUID: {  // ghost one-sided :286
+            double dv[ND], hv[ND];
+            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, b.c);
+            cauchy<ND>(&a.stress[i * ns], &b.stress[j * ns], ns, ri, rj, gx, hv);
+            for (int d = 0; d < ND; ++d)
+                a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + b.mass * (hv[d] - piv * gx[d]);
+            double dr = dot<ND>(dv, gx);
+            double psi = diffusion<ND>(dx, ri, rj, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
+            a.drhodt[i] = a.drhodt[i] + b.mass * (dr + psi / rj);
+            break;
+        }
+        case GC_PFN_STRAIN_RATE:
+        case GC_PFN_STRAIN_RATE_VORTICITY: {  // generic one-sided :37/:97
+            double dv[ND], sr[6], w[3];
+            for (int d = 0; d < ND; ++d) dv[d] = vj[d] - vi[d];
+            strain_rate_t<ND>(dv, gx, ns, sr);
+            double fi = b.mass / rj;
+            for (int k = 0; k < ns; ++k) a.sr[i * ns + k] = a.sr[i * ns + k] + sr[k] * fi;
+            if (f.kind == GC_PFN_STRAIN_RATE_VORTICITY) {
+                vorticity_t<ND>(dv, gx, w);
+                for (int k = 0; k < a.nvort; ++k)
+                    a.vort[i * a.nvort + k] = a.vort[i * a.nvort + k] + w[k] * fi;
+            }
+            break;
+        }
+    }
+}
+
+// ----------------------------------------------------------------- pairs
+// src/Interaction.jl:543-557 (_pair_self!) and :717-732 (_pair_coupled!)
+template <int ND>
+inline void pair_self(const Pfn& f, const Kern& k, Sys& ps, int64_t i, int64_t j, double h,
+                      double cutoff_sq) {
+    double dx[ND];
+    for (int d = 0; d < ND; ++d) dx[d] = ps.x[i * ND + d] - ps.x[j * ND + d];
+    double r_sq = dot<ND>(dx, dx);
+    if (r_sq < cutoff_sq) {
+        double r = std::sqrt(r_sq);
+        double q = r / h;
+        double gc = kernel_dw_dq(k, q) / (r * h);
+        double gx[ND];
+        for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
+        pfn_self<ND>(f, ps, i, j, dx, gx);
+    }
+}
+
+template <int ND>
+inline void pair_coupled(const Pfn& f, const Kern& k, Sys& a, const BView& b, int64_t i, int64_t j,
+                         double h, double cutoff_sq) {
+    double dx[ND];
+    for (int d = 0; d < ND; ++d) dx[d] = a.x[i * ND + d] - b.x[j * ND + d];
+    double r_sq = dot<ND>(dx, dx);
+    if (r_sq < cutoff_sq) {
+        double r = std::sqrt(r_sq);
+        double q = r / h;
+        double gc = kernel_dw_dq(k, q) / (r * h);
+        double gx[ND];
+        for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
+        pfn_coupled<ND>(f, a, b, i, j, dx, gx);
+    }
+}
+
+// Cell-range helper: cs is 1-based CSR (cs[c] for c in 1..ncells+1 stored at cs[c-1]).
+inline int64_t CS(const std::vector<int64_t>& cs, int64_t c1) { return cs[(size_t)(c1 - 1)]; }
+
+// ---------------------------------------------------------------- sweeps
+// src/Interaction.jl:393-439 (2-D self, 6 colours), :477-541 (3-D, 18 colours)
+template <int ND>
+void sweep_self(oracle_ctx* ctx, Inter& it, const Pfn& f) {
+    Sys& ps = ctx->sys[it.a];
+    Kern k = make_kernel(it.kk, ND, it.H);
+    const double h = it.H;
+    const double cutoff_sq = it.cell * it.cell;
+    const std::vector<int64_t>& cs = it.cs;
+    if (ND == 2) {
+        const int64_t ny = it.ng[1], nx = it.ng[0];
+        for (int colour = 0; colour < 6; ++colour) {
+            int64_t bx = colour / 3 + 2, by = colour % 3 + 2;
+            int64_t nax = bx <= nx - 1 ? (nx - 1 - bx) / 2 + 1 : 0;
+            int64_t nay = by <= ny - 1 ? (ny - 1 - by) / 3 + 1 : 0;
+            int64_t total = nax * nay;
+#pragma omp parallel for schedule(static) num_threads(ctx->threads)
+            for (int64_t flat = 1; flat <= total; ++flat) {
+                int64_t sx = (flat - 1) / nay, sy = (flat - 1) % nay;
+                int64_t cx = bx + sx * 2, cy = by + sy * 3;
+                int64_t cell = (cx - 1) * ny + cy;
+                int64_t pstart = CS(cs, cell), pend_same = CS(cs, cell + 1), pend_next = CS(cs, cell + 2);
+                int64_t nb = cell + ny - 1;
+                int64_t nps = CS(cs, nb), npe = CS(cs, nb + 3);
+                for (int64_t pi_ = pstart; pi_ <= pend_same - 1; ++pi_) {
+                    for (int64_t pj = pi_ + 1; pj <= pend_next - 1; ++pj)
+                        pair_self<ND>(f, k, ps, pi_ - 1, pj - 1, h, cutoff_sq);
+                    for (int64_t pj = nps; pj <= npe - 1; ++pj)
+                        pair_self<ND>(f, k, ps, pi_ - 1, pj - 1, h, cutoff_sq);
+                }
+            }
+        }
+    } else {
+        const int64_t nz = it.ng[2], ny = it.ng[1], nx = it.ng[0], nyz = ny * nz;
+        const int64_t off[4] = {nz - 1, nyz - nz - 1, nyz - 1, nyz + nz - 1};
+        for (int colour = 0; colour < 18; ++colour) {
+            int64_t bx = colour / 9 + 2, by = (colour % 9) / 3 + 2, bz = colour % 3 + 2;
+            int64_t nax = bx <= nx - 1 ? (nx - 1 - bx) / 2 + 1 : 0;
+            int64_t nay = by <= ny - 1 ? (ny - 1 - by) / 3 + 1 : 0;
+            int64_t naz = bz <= nz - 1 ? (nz - 1 - bz) / 3 + 1 : 0;
+            int64_t nayz = nay * naz, total = nax * nayz;
+#pragma omp parallel for schedule(static) num_threads(ctx->threads)
+            for (int64_t flat = 1; flat <= total; ++flat) {
+                int64_t sx = (flat - 1) / nayz, rem = (flat - 1) % nayz;
+                int64_t sy = rem / naz, sz = rem % naz;
+                int64_t cx = bx + sx * 2, cy = by + sy * 3, cz = bz + sz * 3;
+                int64_t cell = (cx - 1) * nyz + (cy - 1) * nz + cz;
+                int64_t pstart = CS(cs, cell), pend = CS(cs, cell + 1), pend_next = CS(cs, cell + 2);
+                for (int64_t pi_ = pstart; pi_ <= pend - 1; ++pi_)
+                    for (int64_t pj = pi_ + 1; pj <= pend_next - 1; ++pj)
+                        pair_self<ND>(f, k, ps, pi_ - 1, pj - 1, h, cutoff_sq);
+                for (int dir = 0; dir < 4; ++dir) {
+                    int64_t nb = cell + off[dir];
+                    int64_t nps = CS(cs, nb), npe = CS(cs, nb + 3);
+                    for (int64_t pi_ = pstart; pi_ <= pend - 1; ++pi_)
+                        for (int64_t pj = nps; pj <= npe - 1; ++pj)
+                            pair_self<ND>(f, k, ps, pi_ - 1, pj - 1, h, cutoff_sq);
+                }
+            }
+        }
+    }
+}
+
+int make_view(oracle_ctx* ctx, int handle, BView* out);
+
+// src/Interaction.jl:600-645 (2-D coupled, 9 colours), :660-715 (3-D, 27 colours)
+template <int ND>
+void sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
+    Sys& a = ctx->sys[it.a];
+    Kern k = make_kernel(it.kk, ND, it.H);
+    const double h = it.H, cutoff = it.cell;
+    const double cutoff_sq = it.cell * it.cell;
+    const std::vector<int64_t>& cs = it.cs;
+    const std::vector<int64_t>& csa = it.csa;
+    int64_t cmin[3], cmax[3];
+    for (int d = 0; d < ND; ++d) {
+        floor_int((it.mina[d] - it.ming[d]) / cutoff, &cmin[d]);
+        floor_int((it.maxa[d] - it.ming[d]) / cutoff, &cmax[d]);
+        cmin[d] += 1;
+        cmax[d] += 1;
+    }
+    if (ND == 2) {
+        const int64_t ny = it.ng[1];
+        for (int colour = 0; colour < 9; ++colour) {
+            int64_t bx = colour / 3 + cmin[0], by = colour % 3 + cmin[1];
+            int64_t nax = bx <= cmax[0] ? (cmax[0] - bx) / 3 + 1 : 0;
+            int64_t nay = by <= cmax[1] ? (cmax[1] - by) / 3 + 1 : 0;
+            int64_t total = nax * nay;
+#pragma omp parallel for schedule(static) num_threads(ctx->threads)
+            for (int64_t flat = 1; flat <= total; ++flat) {
+                int64_t sx = (flat - 1) / nay, sy = (flat - 1) % nay;
+                int64_t cx = bx + sx * 3, cy = by + sy * 3;
+                int64_t cell = (cx - 1) * ny + cy;
+                int64_t as = CS(csa, cell), ae = CS(csa, cell + 1);
+                for (int64_t pi_ = as; pi_ <= ae - 1; ++pi_)
+                    for (int64_t dcx = -1; dcx <= 1; ++dcx) {
+                        int64_t nb = cell + dcx * ny - 1;
+                        int64_t bs = CS(cs, nb), be = CS(cs, nb + 3);
+                        for (int64_t pj = bs; pj <= be - 1; ++pj)
+                            pair_coupled<ND>(f, k, a, b, pi_ - 1, pj - 1, h, cutoff_sq);
+                    }
+            }
+        }
+    } else {
+        const int64_t nz = it.ng[2], ny = it.ng[1], nyz = ny * nz;
+        for (int colour = 0; colour < 27; ++colour) {
+            int64_t bx = colour / 9 + cmin[0], by = (colour % 9) / 3 + cmin[1], bz = colour % 3 + cmin[2];
+            int64_t nax = bx <= cmax[0] ? (cmax[0] - bx) / 3 + 1 : 0;
+            int64_t nay = by <= cmax[1] ? (cmax[1] - by) / 3 + 1 : 0;
+            int64_t naz = bz <= cmax[2] ? (cmax[2] - bz) / 3 + 1 : 0;
+            int64_t nayz = nay * naz, total = nax * nayz;
+#pragma omp parallel for schedule(static) num_threads(ctx->threads)
+            for (int64_t flat = 1; flat <= total; ++flat) {
+                int64_t sx = (flat - 1) / nayz, rem = (flat - 1) % nayz;
+                int64_t sy = rem / naz, sz = rem % naz;
+                int64_t cx = bx + sx * 3, cy = by + sy * 3, cz = bz + sz * 3;
+                int64_t cell = (cx - 1) * nyz + (cy - 1) * nz + cz;
+                int64_t as = CS(csa, cell), ae = CS(csa, cell + 1);
+                for (int64_t pi_ = as; pi_ <= ae - 1; ++pi_)
+                    for (int64_t dcx = -1; dcx <= 1; ++dcx)
+                        for (int64_t dcy = -1; dcy <= 1; ++dcy) {
+                            int64_t nb = cell + dcx * nyz + dcy * nz - 1;
+                            int64_t bs = CS(cs, nb), be = CS(cs, nb + 3);
+                            for (int64_t pj = bs; pj <= be - 1; ++pj)
+                                pair_coupled<ND>(f, k, a, b, pi_ - 1, pj - 1, h, cutoff_sq);
+                        }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------- grid
+// src/Interaction.jl:131-251
+int cell_1idx(const double* x, int nd, const double* ming, double dcell, const int64_t* ng,
+              int64_t* out) {
+    int64_t flat = 0, stride = 1;
+    for (int d = nd - 1; d >= 0; --d) {
+        int64_t cd;
+        if (!floor_int((x[d] - ming[d]) / dcell, &cd)) return GC_ERR_NONFINITE;
+        flat += cd * stride;
+        stride *= ng[d];
+    }
+    *out = flat + 1;
+    return GC_OK;
+}
+
+int populate_sorted(std::vector<int64_t>& cs, const double* x, int64_t n, int nd, const double* ming,
+                    double cutoff, const int64_t* ng) {
+    int64_t ncells = (int64_t)cs.size() - 1;
+    int64_t prev = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t cell;
+        int st = cell_1idx(&x[i * nd], nd, ming, cutoff, ng, &cell);
+        if (st) return st;
+        if (cell != prev) {
+            if (cell < 1 || cell > ncells) return GC_ERR_CAPACITY;
+            cs[(size_t)(cell - 1)] = i + 1;
+            prev = cell;
+        }
+    }
+    cs[(size_t)ncells] = n + 1;
+    for (int64_t c = ncells; c >= 1; --c)
+        if (cs[(size_t)(c - 1)] == 0) cs[(size_t)(c - 1)] = cs[(size_t)c];
+    return GC_OK;
+}
+
+void bbox(const double* x, int64_t n, int nd, double* mn, double* mx, bool init) {
+    int64_t start = 0;
+    if (init) {
+        for (int d = 0; d < nd; ++d) mn[d] = mx[d] = x[d];
+        start = 1;
+    }
+    for (int64_t i = start; i < n; ++i)
+        for (int d = 0; d < nd; ++d) {
+            mn[d] = jmin(mn[d], x[i * nd + d]);
+            mx[d] = jmax(mx[d], x[i * nd + d]);
+        }
+}
+
+int create_grid(oracle_ctx* ctx, Inter& it) {
+    Sys& a = ctx->sys[it.a];
+    const int nd = a.nd;
+    const double cutoff = it.cell;
+    double mn[3], mx[3];
+    bbox(a.x.data(), a.n, nd, mn, mx, true);
+    BView b{};
+    if (it.b >= 0) {
+        int st = make_view(ctx, it.b, &b);
+        if (st) return st;
+        for (int d = 0; d < nd; ++d) {
+            it.mina[d] = mn[d];
+            it.maxa[d] = mx[d];
+        }
+        bbox(b.x, b.n, nd, mn, mx, false);
+    }
+    for (int d = 0; d < nd; ++d) {
+        double raw = mn[d] - 2.0 * cutoff;
+        it.ming[d] = std::floor(raw / cutoff) * cutoff;
+        double maxg = mx[d] + 2.0 * cutoff;
+        int64_t ngd;
+        if (!floor_int((maxg - it.ming[d]) / cutoff, &ngd)) return fail(ctx, GC_ERR_NONFINITE, "non-finite grid extent");
+        it.ng[d] = ngd + 1;
+    }
+    int64_t ncells = 1;
+    for (int d = 0; d < nd; ++d) ncells *= it.ng[d];
+    if (ncells > (int64_t)1 << 34) return fail(ctx, GC_ERR_CAPACITY, "grid too large");
+    it.cs.assign((size_t)ncells + 1, 0);
+    int st;
+    if (it.b < 0) {
+        st = populate_sorted(it.cs, a.x.data(), a.n, nd, it.ming, cutoff, it.ng);
+    } else {
+        it.csa.assign((size_t)ncells + 1, 0);
+        st = populate_sorted(it.csa, a.x.data(), a.n, nd, it.ming, cutoff, it.ng);
+        if (!st) st = populate_sorted(it.cs, b.x, b.n, nd, it.ming, cutoff, it.ng);
+    }
+    if (st) return fail(ctx, st, "grid population failed (non-finite position or cell outside grid)");
+    it.grid = true;
+    return GC_OK;
+}
+
+// ------------------------------------------------------------------- sort
+// src/Sorting.jl:157-195; stable lexicographic order of floor(x/cutoff).
+int sort_keys(const double* x, int64_t n, int nd, double cutoff, std::vector<int64_t>& keys) {
+    keys.resize((size_t)n * nd);
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < nd; ++d)
+            if (!floor_int(x[i * nd + d] / cutoff, &keys[(size_t)(i * nd + d)])) return GC_ERR_NONFINITE;
+    return GC_OK;
+}
+
+inline bool lt_key(const int64_t* a, const int64_t* b, int nd) {
+    for (int d = 0; d < nd; ++d)
+        if (a[d] != b[d]) return a[d] < b[d];
+    return false;
+}
+
+template <class T>
+void apply_perm(std::vector<T>& arr, const std::vector<int64_t>& perm, int comps) {
+    if (arr.empty() || comps == 0) return;
+    std::vector<T> scratch(arr.size());
+    int64_t n = (int64_t)perm.size();
+    for (int64_t i = 0; i < n; ++i)
+        for (int k = 0; k < comps; ++k) scratch[(size_t)(i * comps + k)] = arr[(size_t)(perm[i] * comps + k)];
+    for (int64_t i = 0; i < n * comps; ++i) arr[(size_t)i] = scratch[(size_t)i];
+}
+
+// Returns 1 if a permutation was applied, 0 for the fast path; <0 on error.
+int sort_order(const double* x, int64_t n, int nd, double cutoff, std::vector<int64_t>& perm) {
+    perm.resize((size_t)n);
+    std::iota(perm.begin(), perm.end(), 0);
+    if (n <= 1) return 0;
+    std::vector<int64_t> keys;
+    if (sort_keys(x, n, nd, cutoff, keys)) return -GC_ERR_NONFINITE;
+    bool sorted = true;
+    for (int64_t i = 0; i + 1 < n; ++i)
+        if (lt_key(&keys[(size_t)((i + 1) * nd)], &keys[(size_t)(i * nd)], nd)) {
+            sorted = false;
+            break;
+        }
+    if (sorted) return 0;
+    std::stable_sort(perm.begin(), perm.end(), [&](int64_t p, int64_t q) {
+        return lt_key(&keys[(size_t)(p * nd)], &keys[(size_t)(q * nd)], nd);
+    });
+    return 1;
+}
+
+int sort_system(Sys& s, double cutoff, std::vector<int64_t>* perm_out) {
+    std::vector<int64_t> perm;
+    int r = sort_order(s.x.data(), s.n, s.nd, cutoff, perm);
+    if (r < 0) return -r;
+    if (r == 1) {
+        const int nd = s.nd, ns = s.ns;
+        apply_perm(s.x, perm, nd);
+        apply_perm(s.id, perm, 1);
+        apply_perm(s.v, perm, nd);
+        apply_perm(s.vadj, perm, nd);
+        apply_perm(s.rho, perm, 1);
+        apply_perm(s.dvdt, perm, nd);
+        apply_perm(s.drhodt, perm, 1);
+        if (s.has_p()) apply_perm(s.p, perm, 1);
+        if (s.has_stress()) {
+            apply_perm(s.stress, perm, ns);
+            apply_perm(s.sr, perm, ns);
+        }
+        if (s.is_ep()) {
+            apply_perm(s.vort, perm, s.nvort);
+            apply_perm(s.strain, perm, ns);
+            apply_perm(s.strainp, perm, ns);
+        }
+    }
+    if (perm_out) *perm_out = perm;
+    return GC_OK;
+}
+
+// Ghost sort: permutes (x, v, rho, idx_original, idx_boundary, extras); the
+// cached normals are not in the reference's permuted-array list
+// (src/Sorting.jl:33-40) and stay in generation order.
+int sort_ghost(Ghost& g, int nd, int ns, double cutoff, std::vector<int64_t>* perm_out) {
+    std::vector<int64_t> perm;
+    int r = sort_order(g.x.data(), g.n, nd, cutoff, perm);
+    if (r < 0) return -r;
+    if (r == 1) {
+        apply_perm(g.x, perm, nd);
+        apply_perm(g.v, perm, nd);
+        apply_perm(g.rho, perm, 1);
+        apply_perm(g.io, perm, 1);
+        apply_perm(g.ib, perm, 1);
+        if (g.ex_p) apply_perm(g.p, perm, 1);
+        if (g.ex_stress) apply_perm(g.stress, perm, ns);
+    }
+    if (perm_out) *perm_out = perm;
+    return GC_OK;
+}
+
+// ----------------------------------------------------------------- ghosts
+// src/GhostParticles.jl:344-392
+void generate_ghosts(oracle_ctx* ctx, Ghost& g) {
+    Sys& ps = ctx->sys[g.src];
+    const int nd = ps.nd;
+    int64_t total = 0;
+    for (int b = 0; b < g.nplanes; ++b)
+        for (int64_t i = 0; i < ps.n; ++i) {
+            double tmp[3];
+            for (int d = 0; d < nd; ++d) tmp[d] = ps.x[i * nd + d] - g.pp[b * nd + d];
+            double da = nd == 2 ? dot<2>(tmp, &g.pn[b * nd]) : dot<3>(tmp, &g.pn[b * nd]);
+            if (std::fabs(da) <= g.cutoff && da > 0.0) ++total;
+        }
+    g.n = total;
+    g.x.assign((size_t)total * nd, 0.0);
+    g.v.resize((size_t)total * nd);
+    g.rho.resize((size_t)total);
+    g.io.assign((size_t)total, 0);
+    g.ib.assign((size_t)total, 0);
+    g.normals.assign((size_t)total * nd, 0.0);
+    if (g.ex_p) g.p.resize((size_t)total);
+    if (g.ex_stress) g.stress.resize((size_t)total * ps.ns);
+    int64_t cur = 0;
+    for (int b = 0; b < g.nplanes; ++b)
+        for (int64_t i = 0; i < ps.n; ++i) {
+            double tmp[3];
+            for (int d = 0; d < nd; ++d) tmp[d] = ps.x[i * nd + d] - g.pp[b * nd + d];
+            double da = nd == 2 ? dot<2>(tmp, &g.pn[b * nd]) : dot<3>(tmp, &g.pn[b * nd]);
+            if (std::fabs(da) <= g.cutoff && da > 0.0) {
+                for (int d = 0; d < nd; ++d) g.x[cur * nd + d] = ps.x[i * nd + d] - (2.0 * da) * g.pn[b * nd + d];
+                g.io[cur] = i + 1;
+                g.ib[cur] = b + 1;
+                for (int d = 0; d < nd; ++d) g.normals[cur * nd + d] = g.pn[b * nd + d];
+                ++cur;
+            }
+        }
+}
+
+// src/GhostParticles.jl:404-421
+void ghost_kinematics(oracle_ctx* ctx, Ghost& g) {
+    Sys& ps = ctx->sys[g.src];
+    const int nd = ps.nd;
+    for (int64_t k = 0; k < g.n; ++k) {
+        const double* nrm = &g.normals[k * nd];
+        int64_t o = g.io[k] - 1;
+        const double* vr = &ps.v[o * nd];
+        double dvn = nd == 2 ? dot<2>(vr, nrm) : dot<3>(vr, nrm);
+        double s = 2.0 * dvn;
+        for (int d = 0; d < nd; ++d) g.v[k * nd + d] = vr[d] - s * nrm[d];
+        g.rho[k] = ps.rho[o];
+    }
+}
+
+// src/GhostParticles.jl:66-110
+void householder(const double* s, int ns, const double* n, int nd, double* out) {
+    if (ns == 3 || ns == 4) {
+        double nx = n[0], ny = n[1];
+        int xy = ns == 3 ? 2 : 3;
+        double tx = s[0] * nx + s[xy] * ny;
+        double ty = s[xy] * nx + s[1] * ny;
+        double sc = tx * nx + ty * ny;
+        out[0] = s[0] - 4.0 * tx * nx + 4.0 * sc * nx * nx;
+        out[1] = s[1] - 4.0 * ty * ny + 4.0 * sc * ny * ny;
+        if (ns == 4) out[2] = s[2];
+        out[xy] = s[xy] - 2.0 * (tx * ny + nx * ty) + 4.0 * sc * nx * ny;
+    } else {
+        double nx = n[0], ny = n[1], nz = n[2];
+        double tx = s[0] * nx + s[3] * ny + s[4] * nz;
+        double ty = s[3] * nx + s[1] * ny + s[5] * nz;
+        double tz = s[4] * nx + s[5] * ny + s[2] * nz;
+        double sc = tx * nx + ty * ny + tz * nz;
+        out[0] = s[0] - 4.0 * tx * nx + 4.0 * sc * nx * nx;
+        out[1] = s[1] - 4.0 * ty * ny + 4.0 * sc * ny * ny;
+        out[2] = s[2] - 4.0 * tz * nz + 4.0 * sc * nz * nz;
+        out[3] = s[3] - 2.0 * (tx * ny + nx * ty) + 4.0 * sc * nx * ny;
+        out[4] = s[4] - 2.0 * (tx * nz + nx * tz) + 4.0 * sc * nx * nz;
+        out[5] = s[5] - 2.0 * (ty * nz + ny * tz) + 4.0 * sc * ny * nz;
+    }
+    (void)nd;
+}
+
+// src/GhostParticles.jl:112-129,261-278
+void update_ghost(oracle_ctx* ctx, Ghost& g, int stage) {
+    if (stage < 1 || stage > (int)g.copiers.size()) return;
+    Sys& ps = ctx->sys[g.src];
+    const int nd = ps.nd, ns = ps.ns;
+    for (auto& e : g.copiers[stage - 1].entries) {
+        int field = e.first, mode = e.second;
+        for (int64_t k = 0; k < g.n; ++k) {
+            int64_t o = g.io[k] - 1;
+            if (field == GC_FIELD_P) {
+                g.p[k] = ps.p[o];
+            } else if (field == GC_FIELD_STRESS) {
+                if (mode == GC_COPY_HOUSEHOLDER)
+                    householder(&ps.stress[o * ns], ns, &g.normals[k * nd], nd, &g.stress[k * ns]);
+                else
+                    for (int q = 0; q < ns; ++q) g.stress[k * ns + q] = ps.stress[o * ns + q];
+            }
+            // A :rho copier writes the extras copy, which the first-class rho shadows.
+        }
+    }
+}
+
+// --------------------------------------------------------------- updaters
+// src/StateUpdaters.jl
+void ep_update(Sys& ps, int64_t i, const Upd& u, double dt) {
+    const double E = u.prm[0], nu = u.prm[1], phi = u.prm[2], psi = u.prm[3], coh = u.prm[4];
+    double* s = &ps.stress[i * 4];
+    const double* er = &ps.sr[i * 4];
+    double w = ps.vort[i * ps.nvort];
+    double sxx = s[0], syy = s[1], szz = s[2], sxy = s[3];
+    double dexx = er[0] * dt, deyy = er[1] * dt, dezz = er[2] * dt, dexy = er[3] * dt;
+    double D0 = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    double dsxx = D0 * ((1.0 - nu) * dexx + nu * deyy + nu * dezz);
+    double dsyy = D0 * (nu * dexx + (1.0 - nu) * deyy + nu * dezz);
+    double dszz = D0 * (nu * dexx + nu * deyy + (1.0 - nu) * dezz);
+    double dsxy = D0 * (1.0 - 2.0 * nu) * dexy;
+    double wdt = w * dt;
+    dsxx = dsxx - 2.0 * sxy * wdt;
+    dsyy = dsyy + 2.0 * sxy * wdt;
+    dsxy = dsxy + (sxx - syy) * wdt;
+    double txx = sxx + dsxx, tyy = syy + dsyy, tzz = szz + dszz, txy = sxy + dsxy;
+    double sqrt3 = std::sqrt(3.0);
+    double sphi = std::sin(phi), cphi = std::cos(phi);
+    double a_phi = 2.0 * sphi / (sqrt3 * (3.0 - sphi));
+    double k_c = 6.0 * coh * cphi / (sqrt3 * (3.0 - sphi));
+    double I1 = txx + tyy + tzz;
+    double p3 = I1 / 3.0;
+    double s_xx = txx - p3, s_yy = tyy - p3, s_zz = tzz - p3, s_xy = txy;
+    double J2 = 0.5 * (s_xx * s_xx + s_yy * s_yy + s_zz * s_zz + 2.0 * (s_xy * s_xy));
+    double sqJ2 = std::sqrt(J2);
+    double f = a_phi * I1 + sqJ2 - k_c;
+    double depxx = 0.0, depyy = 0.0, depzz = 0.0, depxy = 0.0;
+    if (f > 0.0) {
+        double spsi = std::sin(psi);
+        double a_psi = 2.0 * spsi / (sqrt3 * (3.0 - spsi));
+        double inv2 = 1.0 / (2.0 * sqJ2);
+        double dfxx = a_phi + s_xx * inv2, dfyy = a_phi + s_yy * inv2, dfzz = a_phi + s_zz * inv2;
+        double dfxy = s_xy * inv2;
+        double dgxx = a_psi + s_xx * inv2, dgyy = a_psi + s_yy * inv2, dgzz = a_psi + s_zz * inv2;
+        double dgxy = s_xy * inv2;
+        double Dxx = D0 * ((1.0 - nu) * dgxx + nu * dgyy + nu * dgzz);
+        double Dyy = D0 * (nu * dgxx + (1.0 - nu) * dgyy + nu * dgzz);
+        double Dzz = D0 * (nu * dgxx + nu * dgyy + (1.0 - nu) * dgzz);
+        double Dxy = D0 * (1.0 - 2.0 * nu) * dgxy;
+        double denom = dfxx * Dxx + dfyy * Dyy + dfzz * Dzz + 2.0 * dfxy * Dxy;
+        double dl = f / denom;
+        depxx = dl * dgxx;
+        depyy = dl * dgyy;
+        depzz = dl * dgzz;
+        depxy = dl * dgxy;
+        dsxx = dsxx - D0 * ((1.0 - nu) * depxx + nu * depyy + nu * depzz);
+        dsyy = dsyy - D0 * (nu * depxx + (1.0 - nu) * depyy + nu * depzz);
+        dszz = dszz - D0 * (nu * depxx + nu * depyy + (1.0 - nu) * depzz);
+        dsxy = dsxy - D0 * (1.0 - 2.0 * nu) * depxy;
+    }
+    s[0] = sxx + dsxx;
+    s[1] = syy + dsyy;
+    s[2] = szz + dszz;
+    s[3] = sxy + dsxy;
+    if (sxx + dsxx + syy + dsyy + szz + dszz > k_c / a_phi) {
+        double apex = k_c / a_phi / 3.0;
+        s[0] = apex;
+        s[1] = apex;
+        s[2] = apex;
+        s[3] = 0.0;
+    }
+    double* e = &ps.strain[i * 4];
+    double* ep = &ps.strainp[i * 4];
+    e[0] = e[0] + dexx;
+    e[1] = e[1] + deyy;
+    e[2] = e[2] + dezz;
+    e[3] = e[3] + dexy;
+    ep[0] = ep[0] + depxx;
+    ep[1] = ep[1] + depyy;
+    ep[2] = ep[2] + depzz;
+    ep[3] = ep[3] + depxy;
+}
+
+void hooke_update(Sys& ps, int64_t i, const Upd& u, double dt) {
+    const double E = u.prm[0], nu = u.prm[1];
+    double* s = &ps.stress[i * 4];
+    const double* er = &ps.sr[i * 4];
+    double w = ps.vort[i * ps.nvort];
+    double sxx = s[0], syy = s[1], szz = s[2], sxy = s[3];
+    double dexx = er[0] * dt, deyy = er[1] * dt, dezz = er[2] * dt, dexy = er[3] * dt;
+    double D0 = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    double dsxx = D0 * ((1.0 - nu) * dexx + nu * deyy + nu * dezz);
+    double dsyy = D0 * (nu * dexx + (1.0 - nu) * deyy + nu * dezz);
+    double dszz = D0 * (nu * dexx + nu * deyy + (1.0 - nu) * dezz);
+    double dsxy = D0 * (1.0 - 2.0 * nu) * dexy;
+    double wdt = w * dt;
+    dsxx = dsxx - 2.0 * sxy * wdt;
+    dsyy = dsyy + 2.0 * sxy * wdt;
+    dsxy = dsxy + (sxx - syy) * wdt;
+    double nxx = sxx + dsxx, nyy = syy + dsyy, nzz = szz + dszz, nxy = sxy + dsxy;
+    s[0] = nxx;
+    s[1] = nyy;
+    s[2] = nzz;
+    s[3] = nxy;
+    ps.p[i] = -(nxx + nyy + nzz) / 3.0;
+}
+
+void apply_updater(Sys& ps, const Upd& u, double dt) {
+    const int64_t n = ps.n;
+    switch (u.kind) {
+        case GC_UPD_ZERO_FIELDS: {
+            uint64_t mask = (uint64_t)u.prm[0];
+            for (int64_t i = 0; i < n; ++i) {
+                if (mask & (1u << GC_FIELD_STRAIN_RATE))
+                    for (int k = 0; k < ps.ns; ++k) ps.sr[i * ps.ns + k] = 0.0;
+                if (mask & (1u << GC_FIELD_VORTICITY))
+                    for (int k = 0; k < ps.nvort; ++k) ps.vort[i * ps.nvort + k] = 0.0;
+                if (mask & (1u << GC_FIELD_P)) ps.p[i] = 0.0;
+                if (mask & (1u << GC_FIELD_STRESS))
+                    for (int k = 0; k < ps.ns; ++k) ps.stress[i * ps.ns + k] = 0.0;
+                if (mask & (1u << GC_FIELD_DVDT))
+                    for (int d = 0; d < ps.nd; ++d) ps.dvdt[i * ps.nd + d] = 0.0;
+                if (mask & (1u << GC_FIELD_DRHODT)) ps.drhodt[i] = 0.0;
+            }
+            break;
+        }
+        case GC_UPD_TAIT_EOS: {
+            const double rho0 = u.prm[0], gam = u.prm[1];
+            const double pre = rho0 * ps.c * ps.c / gam;
+            for (int64_t i = 0; i < n; ++i) ps.p[i] = pre * (jpow(ps.rho[i] / rho0, gam) - 1.0);
+            break;
+        }
+        case GC_UPD_LINEAR_EOS: {
+            const double rho0 = u.prm[0];
+            for (int64_t i = 0; i < n; ++i) ps.p[i] = ps.c * ps.c * (ps.rho[i] - rho0);
+            break;
+        }
+        case GC_UPD_ELASTOPLASTIC:
+            for (int64_t i = 0; i < n; ++i) ep_update(ps, i, u, dt);
+            break;
+        case GC_UPD_HOOKE:
+            for (int64_t i = 0; i < n; ++i) hooke_update(ps, i, u, dt);
+            break;
+        default:
+            break;
+    }
+}
+
+// src/Particles.jl:542-570
+void update_state(Sys& ps, int stage, double dt) {
+    if (stage < 1 || stage > (int)ps.upd.size()) return;
+    for (const Upd& u : ps.upd[stage - 1]) apply_updater(ps, u, dt);
+}
+
+// ------------------------------------------------------------------ views
+int make_view(oracle_ctx* ctx, int handle, BView* out) {
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return GC_ERR_ARG;
+    const Handle& h = ctx->handles[handle];
+    BView b{};
+    b.type = h.type;
+    if (h.type == H_GHOST) {
+        Ghost& g = ctx->ghosts[h.idx];
+        Sys& src = ctx->sys[g.src];
+        b.n = g.n;
+        b.x = g.x.data();
+        b.v = g.v.data();
+        b.rho = g.rho.data();
+        b.p = g.ex_p ? g.p.data() : nullptr;
+        b.stress = g.ex_stress ? g.stress.data() : nullptr;
+        b.mass = src.mass;
+        b.c = src.c;
+        b.ns = src.ns;
+        b.sys = nullptr;
+    } else {
+        Sys& s = ctx->sys[h.idx];
+        b.n = s.n;
+        b.x = s.x.data();
+        b.v = s.v.data();
+        b.rho = s.rho.data();
+        b.p = s.has_p() ? s.p.data() : nullptr;
+        b.stress = s.has_stress() ? s.stress.data() : nullptr;
+        b.mass = s.mass;
+        b.c = s.c;
+        b.ns = s.ns;
+        b.sys = &s;
+        b.normal = h.normal;
+        b.point = h.point;
+        b.beta = h.beta;
+        b.ljcut = h.ljcut;
+    }
+    *out = b;
+    return GC_OK;
+}
+
+// Which functor/system_b combinations the restatement (and the device
+// library) implement; the rest are refused instead of guessed.
+int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
+    const Sys& a = ctx->sys[it.a];
+    if (pk == GC_PFN_NONE) return GC_OK;
+    if (pk == GC_PFN_FLUID && !a.has_p()) return GC_ERR_ARG;
+    if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE) && !a.has_stress()) return GC_ERR_ARG;
+    if (pk == GC_PFN_STRAIN_RATE_VORTICITY && !a.is_ep()) return GC_ERR_ARG;
+    if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE || pk == GC_PFN_STRAIN_RATE_VORTICITY)) {
+        if (a.nd == 2 && !(a.ns == 3 || a.ns == 4)) return GC_ERR_UNSUPPORTED;
+        if (a.nd == 3 && a.ns != 6) return GC_ERR_UNSUPPORTED;
+    }
+    if (it.b < 0) return GC_OK;
+    const Handle& h = ctx->handles[it.b];
+    if (pk == GC_PFN_COUNT) return h.type == H_GHOST ? GC_ERR_UNSUPPORTED : GC_OK;
+    if (h.type == H_DYN) return GC_OK;
+    if (h.type == H_STATIC) return GC_OK;
+    if (h.type == H_GHOST) {
+        const Ghost& g = ctx->ghosts[h.idx];
+        if (pk == GC_PFN_FLUID && !g.ex_p) return GC_ERR_UNSUPPORTED;
+        if (pk == GC_PFN_CAUCHY_FLUID && !g.ex_stress) return GC_ERR_UNSUPPORTED;
+        return GC_OK;
+    }
+    // plain real system_b: one-sided generic functors only
+    const Sys& b = ctx->sys[h.idx];
+    if (pk == GC_PFN_FLUID) {
+        if (a.kind == GC_SYS_FLUID && b.kind == GC_SYS_FLUID) return GC_ERR_UNSUPPORTED;  // two-sided multiphase
+        return b.has_p() ? GC_OK : GC_ERR_ARG;
+    }
+    if (pk == GC_PFN_CAUCHY_FLUID) return GC_ERR_UNSUPPORTED;  // two-sided real-real
+    return GC_OK;
+}
+
+int sweep(oracle_ctx* ctx, Inter& it, int stage) {
+    if (stage < 1 || stage > it.nstages) return GC_OK;
+    int pk = it.pk[stage - 1];
+    if (pk == GC_PFN_NONE) return GC_OK;
+    if (!it.grid) return fail(ctx, GC_ERR_STATE, "sweep before create_grid");
+    Pfn f = make_pfn(pk, it.pp[stage - 1].data());
+    const int nd = ctx->sys[it.a].nd;
+    if (it.b < 0) {
+        if (nd == 2) sweep_self<2>(ctx, it, f);
+        else sweep_self<3>(ctx, it, f);
+    } else {
+        BView b;
+        int st = make_view(ctx, it.b, &b);
+        if (st) return st;
+        if (nd == 2) sweep_coupled<2>(ctx, it, f, b);
+        else sweep_coupled<3>(ctx, it, f, b);
+    }
+    return GC_OK;
+}
+
+// ------------------------------------------------------------- integrator
+// src/TimeIntegration.jl:580-697 (LeapFrog)
+int num_stages(oracle_ctx* ctx) { return ctx->inters.empty() ? 0 : ctx->inters[0].nstages; }
+
+int step_once(oracle_ctx* ctx, double dt) {
+    const int nst = num_stages(ctx);
+    double hmin = 1e300;
+    for (auto& it : ctx->inters) hmin = std::min(hmin, it.H);
+    const double sort_cutoff = 2.0 * hmin;
+    // 1. sort every real system
+    for (auto& s : ctx->sys) {
+        int st = sort_system(s, sort_cutoff, nullptr);
+        if (st) return fail(ctx, st, "sort: non-finite position");
+    }
+    // 2. save q0
+    for (auto& s : ctx->sys) {
+        s.q0v = s.v;
+        s.q0rho = s.rho;
+    }
+    // 3-5. ghosts, ghost sort, grids
+    for (auto& g : ctx->ghosts) generate_ghosts(ctx, g);
+    for (auto& g : ctx->ghosts) {
+        const Sys& src = ctx->sys[g.src];
+        int st = sort_ghost(g, src.nd, src.ns, sort_cutoff, nullptr);
+        if (st) return fail(ctx, st, "ghost sort: non-finite position");
+    }
+    for (auto& it : ctx->inters) {
+        int st = create_grid(ctx, it);
+        if (st) return st;
+    }
+    // 6. half-step: q += dt/2 * dqdt, dqdt <- source
+    const double half = dt / 2.0;
+    for (auto& s : ctx->sys) {
+        const int nd = s.nd;
+        for (int64_t i = 0; i < s.n * nd; ++i) s.v[i] = s.v[i] + half * s.dvdt[i];
+        for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(half, s.drhodt[i], s.rho[i]);
+        for (int64_t i = 0; i < s.n; ++i)
+            for (int d = 0; d < nd; ++d) s.dvdt[i * nd + d] = s.srcv[d];
+        for (int64_t i = 0; i < s.n; ++i) s.drhodt[i] = s.srcrho;
+    }
+    // 7. ghost kinematics
+    for (auto& g : ctx->ghosts) ghost_kinematics(ctx, g);
+    // 8. stages
+    for (int stage = 1; stage <= nst; ++stage) {
+        for (auto& s : ctx->sys)
+            if (s.upd_set && (int)s.upd.size() == nst) update_state(s, stage, dt);
+        for (auto& g : ctx->ghosts) update_ghost(ctx, g, stage);
+        for (auto& it : ctx->inters) {
+            int st = sweep(ctx, it, stage);
+            if (st) return st;
+        }
+    }
+    // 8b. damping
+    if (ctx->gamma != 0.0) {
+        const double gdt = ctx->gamma / dt;
+        for (auto& s : ctx->sys)
+            for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
+    }
+    // 9. full step: q = q0 + dt * dqdt
+    for (auto& s : ctx->sys) {
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.dvdt[i];
+        for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.drhodt[i], s.q0rho[i]);
+    }
+    // 10. XSPH correction with a zero adjustment: v += -1*0; v += 1*0
+    for (auto& s : ctx->sys)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = (s.v[i] + (-1.0 * s.vadj[i])) + 1.0 * s.vadj[i];
+    // 11. positions
+    for (auto& s : ctx->sys)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+    ctx->steps += 1;
+    return GC_OK;
+}
+
+double compute_dt(oracle_ctx* ctx, double cfl) {
+    double c = -1e300, h = 1e300;
+    for (auto& s : ctx->sys) c = std::max(c, s.c);
+    for (auto& it : ctx->inters) h = std::min(h, it.H);
+    return cfl * h / c;
+}
+
+// field access
+int field_comps(const Sys& s, int field) {
+    switch (field) {
+        case GC_FIELD_X: case GC_FIELD_V: case GC_FIELD_DVDT: case GC_FIELD_V_ADJUSTMENT: return s.nd;
+        case GC_FIELD_RHO: case GC_FIELD_DRHODT: case GC_FIELD_ID: return 1;
+        case GC_FIELD_P: return s.has_p() ? 1 : -1;
+        case GC_FIELD_STRESS: case GC_FIELD_STRAIN_RATE: return s.has_stress() ? s.ns : -1;
+        case GC_FIELD_VORTICITY: return s.is_ep() ? s.nvort : -1;
+        case GC_FIELD_STRAIN: case GC_FIELD_STRAIN_P: return s.is_ep() ? s.ns : -1;
+        default: return -1;
+    }
+}
+
+std::vector<double>* field_vec(Sys& s, int field) {
+    switch (field) {
+        case GC_FIELD_X: return &s.x;
+        case GC_FIELD_V: return &s.v;
+        case GC_FIELD_RHO: return &s.rho;
+        case GC_FIELD_DVDT: return &s.dvdt;
+        case GC_FIELD_DRHODT: return &s.drhodt;
+        case GC_FIELD_P: return &s.p;
+        case GC_FIELD_STRESS: return &s.stress;
+        case GC_FIELD_STRAIN_RATE: return &s.sr;
+        case GC_FIELD_VORTICITY: return &s.vort;
+        case GC_FIELD_STRAIN: return &s.strain;
+        case GC_FIELD_STRAIN_P: return &s.strainp;
+        case GC_FIELD_V_ADJUSTMENT: return &s.vadj;
+        default: return nullptr;
+    }
+}
+
+}  // namespace
+
+// =================================================================== C API
+extern "C" {
+
+int oracle_create(oracle_ctx** out) {
+    *out = new oracle_ctx();
+    return GC_OK;
+}
+
+int oracle_destroy(oracle_ctx* ctx) {
+    delete ctx;
+    return GC_OK;
+}
+
+const char* oracle_last_error(oracle_ctx* ctx) { return ctx->err.c_str(); }
+
+int oracle_set_threads(oracle_ctx* ctx, int threads) {
+    ctx->threads = threads < 1 ? 1 : threads;
+    return GC_OK;
+}
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int oracle_add_system(oracle_ctx* ctx, int kind, int64_t n, int nd, int ns, double mass, double c,
+                      const double* source_v, double source_rho, int* sys_out) {
+    if (n <= 0) return fail(ctx, GC_ERR_ARG, "n must be positive");
+    if (nd < 2 || nd > 3) return fail(ctx, GC_ERR_UNSUPPORTED, "ndims must be 2 or 3");
+    if (kind < GC_SYS_BASIC || kind > GC_SYS_ELASTOPLASTIC) return fail(ctx, GC_ERR_ARG, "bad system kind");
+    Sys s;
+    s.kind = kind;
+    s.n = n;
+    s.nd = nd;
+    s.ns = kind >= GC_SYS_STRESS ? ns : 0;
+    if (kind >= GC_SYS_STRESS && !(ns == 3 || ns == 4 || ns == 6)) return fail(ctx, GC_ERR_ARG, "ns must be 3, 4, or 6");
+    s.nvort = kind == GC_SYS_ELASTOPLASTIC ? (nd == 2 ? 1 : 3) : 0;
+    s.mass = mass;
+    s.c = c;
+    for (int d = 0; d < nd; ++d) s.srcv[d] = source_v ? source_v[d] : 0.0;
+    s.srcrho = source_rho;
+    s.x.assign((size_t)n * nd, 0.0);
+    s.v.assign((size_t)n * nd, 0.0);
+    s.vadj.assign((size_t)n * nd, 0.0);
+    s.rho.assign((size_t)n, 0.0);
+    s.dvdt.assign((size_t)n * nd, 0.0);
+    s.drhodt.assign((size_t)n, 0.0);
+    s.id.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) s.id[i] = i + 1;
+    if (s.has_p()) s.p.assign((size_t)n, 0.0);
+    if (s.has_stress()) {
+        s.stress.assign((size_t)n * s.ns, 0.0);
+        s.sr.assign((size_t)n * s.ns, 0.0);
+    }
+    if (s.is_ep()) {
+        s.vort.assign((size_t)n * s.nvort, 0.0);
+        s.strain.assign((size_t)n * s.ns, 0.0);
+        s.strainp.assign((size_t)n * s.ns, 0.0);
+    }
+    ctx->sys.push_back(std::move(s));
+    Handle h;
+    h.type = H_SYS;
+    h.idx = (int)ctx->sys.size() - 1;
+    ctx->handles.push_back(h);
+    ctx->sys_handle.push_back((int)ctx->handles.size() - 1);
+    *sys_out = (int)ctx->handles.size() - 1;
+    return GC_OK;
+}
+
+static int sys_index(oracle_ctx* ctx, int handle) {
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return -1;
+    if (ctx->handles[handle].type != H_SYS) return -1;
+    return ctx->handles[handle].idx;
+}
+
+int oracle_add_boundary(oracle_ctx* ctx, int sys, int kind, const double* normal, const double* point,
+                        double beta_or_lj, int* handle_out) {
+    int si = sys_index(ctx, sys);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "boundary inner must be a system");
+    Handle h;
+    h.type = kind == GC_WRAP_DYNAMIC ? H_DYN : H_STATIC;
+    h.idx = si;
+    const int nd = ctx->sys[si].nd;
+    if (kind == GC_WRAP_DYNAMIC) {
+        for (int d = 0; d < nd; ++d) {
+            h.normal[d] = normal[d];
+            h.point[d] = point[d];
+        }
+        h.beta = beta_or_lj;
+    } else if (kind == GC_WRAP_STATIC) {
+        h.ljcut = beta_or_lj;
+    } else {
+        return fail(ctx, GC_ERR_ARG, "bad boundary kind");
+    }
+    ctx->handles.push_back(h);
+    *handle_out = (int)ctx->handles.size() - 1;
+    return GC_OK;
+}
+
+int oracle_add_ghost(oracle_ctx* ctx, int src_sys, int ncopiers, const int* copier_nfields,
+                     const int* copier_fields, const int* copier_modes, int nplanes, const double* normals,
+                     const double* points, double cutoff, int* handle_out) {
+    int si = sys_index(ctx, src_sys);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "ghost source must be a system");
+    if (nplanes < 1) return fail(ctx, GC_ERR_ARG, "at least one boundary (normal, point) pair is required");
+    const Sys& s = ctx->sys[si];
+    Ghost g;
+    g.src = si;
+    g.cutoff = cutoff;
+    g.nplanes = nplanes;
+    g.pn.assign(normals, normals + nplanes * s.nd);
+    g.pp.assign(points, points + nplanes * s.nd);
+    int pos = 0;
+    for (int k = 0; k < ncopiers; ++k) {
+        Copier cp;
+        for (int e = 0; e < copier_nfields[k]; ++e, ++pos) {
+            int fld = copier_fields[pos], mode = copier_modes[pos];
+            if (fld == GC_FIELD_P) {
+                if (!s.has_p()) return fail(ctx, GC_ERR_ARG, "copier field p missing on source");
+                g.ex_p = true;
+            } else if (fld == GC_FIELD_STRESS) {
+                if (!s.has_stress()) return fail(ctx, GC_ERR_ARG, "copier field stress missing on source");
+                g.ex_stress = true;
+            } else if (fld != GC_FIELD_RHO) {
+                return fail(ctx, GC_ERR_UNSUPPORTED, "copier field not supported");
+            }
+            cp.entries.push_back({fld, mode});
+        }
+        g.copiers.push_back(cp);
+    }
+    ctx->ghosts.push_back(std::move(g));
+    Handle h;
+    h.type = H_GHOST;
+    h.idx = (int)ctx->ghosts.size() - 1;
+    ctx->handles.push_back(h);
+    *handle_out = (int)ctx->handles.size() - 1;
+    return GC_OK;
+}
+
+int oracle_add_interaction(oracle_ctx* ctx, int sys_a, int b_handle, int kernel_kind, double h, int nstages,
+                           const int* pfn_kinds, const double* pfn_params, int* inter_out) {
+    int si = sys_index(ctx, sys_a);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "system_a must be a system");
+    if (b_handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad system_b handle");
+    Inter it;
+    it.a = si;
+    it.b = b_handle;
+    it.kk = kernel_kind;
+    it.H = h;
+    it.nstages = nstages;
+    it.cell = 2.0 * h;
+    for (int s = 0; s < nstages; ++s) {
+        it.pk.push_back(pfn_kinds[s]);
+        std::array<double, GC_PFN_NPARAM> a;
+        for (int k = 0; k < GC_PFN_NPARAM; ++k) a[k] = pfn_params[s * GC_PFN_NPARAM + k];
+        it.pp.push_back(a);
+        int st = check_combo(ctx, it, pfn_kinds[s]);
+        if (st) return fail(ctx, st, "unsupported pairwise functor / system combination");
+    }
+    ctx->inters.push_back(std::move(it));
+    *inter_out = (int)ctx->inters.size() - 1;
+    return GC_OK;
+}
+
+int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_len, const int* kinds,
+                        const double* params) {
+    int si = sys_index(ctx, sys);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "updaters need a system");
+    Sys& s = ctx->sys[si];
+    s.upd.clear();
+    s.upd_set = true;
+    int pos = 0;
+    for (int st = 0; st < nstages; ++st) {
+        std::vector<Upd> chain;
+        for (int k = 0; k < chain_len[st]; ++k, ++pos) {
+            Upd u;
+            u.kind = kinds[pos];
+            for (int q = 0; q < GC_UPD_NPARAM; ++q) u.prm[q] = params[pos * GC_UPD_NPARAM + q];
+            if ((u.kind == GC_UPD_ELASTOPLASTIC || u.kind == GC_UPD_HOOKE) && !(s.is_ep() && s.ns == 4))
+                return fail(ctx, GC_ERR_ARG, "ElastoPlasticStressUpdater requires NS=4 (plane-strain Voigt)");
+            if ((u.kind == GC_UPD_TAIT_EOS || u.kind == GC_UPD_LINEAR_EOS) && !s.has_p())
+                return fail(ctx, GC_ERR_ARG, "EOS updater needs a pressure field");
+            chain.push_back(u);
+        }
+        s.upd.push_back(chain);
+    }
+    return GC_OK;
+}
+
+int oracle_set_integrator(oracle_ctx* ctx, double gamma) {
+    ctx->gamma = gamma;
+    return GC_OK;
+}
+
+int oracle_set_field(oracle_ctx* ctx, int handle, int field, const void* host, size_t bytes) {
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
+    const Handle& h = ctx->handles[handle];
+    if (h.type == H_GHOST) return fail(ctx, GC_ERR_ARG, "ghost fields are generated, not set");
+    Sys& s = ctx->sys[h.idx];
+    int comps = field_comps(s, field);
+    if (comps < 0) return fail(ctx, GC_ERR_ARG, "field not present on this system");
+    if (bytes != (size_t)s.n * comps * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+    if (field == GC_FIELD_ID) {
+        std::memcpy(s.id.data(), host, bytes);
+        return GC_OK;
+    }
+    std::vector<double>* vec = field_vec(s, field);
+    std::memcpy(vec->data(), host, bytes);
+    return GC_OK;
+}
+
+int oracle_get_count(oracle_ctx* ctx, int handle, int64_t* n_out) {
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
+    const Handle& h = ctx->handles[handle];
+    *n_out = h.type == H_GHOST ? ctx->ghosts[h.idx].n : ctx->sys[h.idx].n;
+    return GC_OK;
+}
+
+int oracle_get_field(oracle_ctx* ctx, int handle, int field, void* host, size_t bytes) {
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
+    const Handle& h = ctx->handles[handle];
+    if (h.type == H_GHOST) {
+        Ghost& g = ctx->ghosts[h.idx];
+        const Sys& s = ctx->sys[g.src];
+        const void* src = nullptr;
+        size_t need = 0;
+        switch (field) {
+            case GC_FIELD_X: src = g.x.data(); need = g.n * s.nd * 8; break;
+            case GC_FIELD_V: src = g.v.data(); need = g.n * s.nd * 8; break;
+            case GC_FIELD_RHO: src = g.rho.data(); need = g.n * 8; break;
+            case GC_FIELD_P: if (!g.ex_p) return fail(ctx, GC_ERR_ARG, "ghost has no p"); src = g.p.data(); need = g.n * 8; break;
+            case GC_FIELD_STRESS: if (!g.ex_stress) return fail(ctx, GC_ERR_ARG, "ghost has no stress"); src = g.stress.data(); need = g.n * s.ns * 8; break;
+            case GC_FIELD_IDX_ORIGINAL: src = g.io.data(); need = g.n * 8; break;
+            case GC_FIELD_IDX_BOUNDARY: src = g.ib.data(); need = g.n * 8; break;
+            case GC_FIELD_NORMALS: src = g.normals.data(); need = g.n * s.nd * 8; break;
+            default: return fail(ctx, GC_ERR_ARG, "field not present on ghosts");
+        }
+        if (bytes != need) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+        if (need) std::memcpy(host, src, need);
+        return GC_OK;
+    }
+    Sys& s = ctx->sys[h.idx];
+    int comps = field_comps(s, field);
+    if (comps < 0) return fail(ctx, GC_ERR_ARG, "field not present on this system");
+    if (bytes != (size_t)s.n * comps * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+    if (field == GC_FIELD_ID) {
+        std::memcpy(host, s.id.data(), bytes);
+        return GC_OK;
+    }
+    std::memcpy(host, field_vec(s, field)->data(), bytes);
+    return GC_OK;
+}
+
+int oracle_step(oracle_ctx* ctx, int nsteps, double cfl) {
+    if (ctx->inters.empty()) return fail(ctx, GC_ERR_ARG, "interactions must not be empty");
+    const int nst = num_stages(ctx);
+    for (auto& it : ctx->inters)
+        if (it.nstages != nst) return fail(ctx, GC_ERR_ARG, "All interactions must have the same number of stages");
+    double dt = compute_dt(ctx, cfl);
+    for (int s = 0; s < nsteps; ++s) {
+        int st = step_once(ctx, dt);
+        if (st) return st;
+    }
+    return GC_OK;
+}
+
+int oracle_sort_system(oracle_ctx* ctx, int handle, double cutoff, int64_t* perm_out) {
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
+    const Handle& h = ctx->handles[handle];
+    std::vector<int64_t> perm;
+    int st;
+    int64_t n;
+    if (h.type == H_GHOST) {
+        Ghost& g = ctx->ghosts[h.idx];
+        st = sort_ghost(g, ctx->sys[g.src].nd, ctx->sys[g.src].ns, cutoff, &perm);
+        n = g.n;
+    } else {
+        st = sort_system(ctx->sys[h.idx], cutoff, &perm);
+        n = ctx->sys[h.idx].n;
+    }
+    if (st) return fail(ctx, st, "sort failed: non-finite position");
+    if (perm_out)
+        for (int64_t i = 0; i < n; ++i) perm_out[i] = perm[i] + 1;
+    return GC_OK;
+}
+
+int oracle_build_grid(oracle_ctx* ctx, int inter, int64_t* cell_start_out, int64_t cap, double* mingridx_out,
+                      int64_t* ngridx_out, int64_t* ncells_out) {
+    if (inter < 0 || inter >= (int)ctx->inters.size()) return fail(ctx, GC_ERR_ARG, "bad interaction");
+    Inter& it = ctx->inters[inter];
+    int st = create_grid(ctx, it);
+    if (st) return st;
+    const int nd = ctx->sys[it.a].nd;
+    int64_t ncells = (int64_t)it.cs.size() - 1;
+    if (ncells_out) *ncells_out = ncells;
+    if (mingridx_out)
+        for (int d = 0; d < nd; ++d) mingridx_out[d] = it.ming[d];
+    if (ngridx_out)
+        for (int d = 0; d < nd; ++d) ngridx_out[d] = it.ng[d];
+    if (cell_start_out) {
+        if (cap < ncells + 1) return fail(ctx, GC_ERR_CAPACITY, "cell_start buffer too small");
+        std::memcpy(cell_start_out, it.cs.data(), (size_t)(ncells + 1) * 8);
+    }
+    return GC_OK;
+}
+
+// Coupled grids also carry system_a's CSR (src/Interaction.jl:168-172).
+int oracle_grid_cell_start_a(oracle_ctx* ctx, int inter, int64_t* out, int64_t cap) {
+    Inter& it = ctx->inters[inter];
+    if (it.csa.empty()) return fail(ctx, GC_ERR_STATE, "no system_a grid");
+    if (cap < (int64_t)it.csa.size()) return fail(ctx, GC_ERR_CAPACITY, "buffer too small");
+    std::memcpy(out, it.csa.data(), it.csa.size() * 8);
+    return GC_OK;
+}
+
+int oracle_generate_ghosts(oracle_ctx* ctx, int ghost) {
+    if (ghost < 0 || ghost >= (int)ctx->handles.size() || ctx->handles[ghost].type != H_GHOST)
+        return fail(ctx, GC_ERR_ARG, "not a ghost handle");
+    generate_ghosts(ctx, ctx->ghosts[ctx->handles[ghost].idx]);
+    return GC_OK;
+}
+
+int oracle_update_ghost_kinematics(oracle_ctx* ctx, int ghost) {
+    if (ghost < 0 || ghost >= (int)ctx->handles.size() || ctx->handles[ghost].type != H_GHOST)
+        return fail(ctx, GC_ERR_ARG, "not a ghost handle");
+    ghost_kinematics(ctx, ctx->ghosts[ctx->handles[ghost].idx]);
+    return GC_OK;
+}
+
+int oracle_update_ghost(oracle_ctx* ctx, int ghost, int stage) {
+    if (ghost < 0 || ghost >= (int)ctx->handles.size() || ctx->handles[ghost].type != H_GHOST)
+        return fail(ctx, GC_ERR_ARG, "not a ghost handle");
+    update_ghost(ctx, ctx->ghosts[ctx->handles[ghost].idx], stage);
+    return GC_OK;
+}
+
+int oracle_sweep(oracle_ctx* ctx, int inter, int stage) {
+    if (inter < 0 || inter >= (int)ctx->inters.size()) return fail(ctx, GC_ERR_ARG, "bad interaction");
+    return sweep(ctx, ctx->inters[inter], stage);
+}
+
+int oracle_update_state(oracle_ctx* ctx, int sys, int stage, double dt) {
+    int si = sys_index(ctx, sys);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "not a system handle");
+    update_state(ctx->sys[si], stage, dt);
+    return GC_OK;
+}
+
+// Kernel primitives for the known-answer tests (src/Kernels.jl).
+double oracle_kernel_norm(int kind, int nd, double H) { return make_kernel(kind, nd, H).norm; }
+double oracle_kernel_w(int kind, int nd, double H, double q) { return kernel_w(make_kernel(kind, nd, H), q); }
+double oracle_kernel_dw_dq(int kind, int nd, double H, double q) {
+    return kernel_dw_dq(make_kernel(kind, nd, H), q);
+}
+double oracle_powi(double x, int64_t n) { return comp_powi(x, n); }
+
+// Number of leapfrog steps done.
+int64_t oracle_steps(oracle_ctx* ctx) { return ctx->steps; }
+
+}  // extern "C"
