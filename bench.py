@@ -1,0 +1,333 @@
+"""Benchmark of the per-timestep SPH hot path (one leapfrog step = one step).
+
+Default workload: the 3-D dam break of 1,000,000 fluid particles (100×50×200
+at dx = 0.01 m) in a 4.0×1.0×4.0 m tank with 3-layer dynamic walls on all
+six faces (1,472,616 boundary particles), FP64, synthetic inputs generated
+by grasph_b200.scenarios (hydrostatic initial density).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` counts fluid particle-steps per
+second over all ranks with state resident in HBM; `e2e` measures the same
+through the host API (upload of every field from pinned host memory, one
+step, download of every field) per step.  With N > 1 every rank advances
+its own replica ("replicas only": the reference path does not shard a
+single simulation).  The state (≈ 330 MB) exceeds the 126 MB L2, so no
+flush is needed between steps.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "grasph.jl_b200"))
+
+METRIC = "particle-steps/s & pair-interactions/s vs plain FP64 GPU; p50/p99 sim latency"
+
+# Algorithmic model of the dominant kernel (the fused pair sweep), per fluid
+# particle and launch: read x, v, rho, p once and write dvdt, drhodt once.
+SWEEP_BYTES_PER_PARTICLE = {2: 16 + 16 + 8 + 8 + 16 + 8, 3: 24 + 24 + 8 + 8 + 24 + 8}
+# FLOPs of one accepted FluidPfn pair as the reference evaluates it
+# (kernel + geometry ≈ 20, artificial viscosity, pressure, momentum and
+# continuity terms; FMA counted as 2, division and sqrt as 1).
+FLUID_PAIR_FLOPS = {2: 70, 3: 86}
+
+
+def build_workload(name, scale):
+    from grasph_b200 import scenarios
+    if name == "dambreak_3d":
+        if scale == "full":
+            return scenarios.dambreak_3d()
+        return scenarios.dambreak_3d(nx=40, ny=20, nz=80, dx=0.025)
+    if name == "dambreak_2d":
+        return scenarios.dambreak_2d()
+    if name == "column":
+        if scale == "full":
+            return scenarios.column_collapse()
+        return scenarios.column_collapse(nx=100, ny=50, dx=0.002)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_desc(meta):
+    return {k: meta[k] for k in ("workload", "n_fluid", "n_boundary", "ndims") if k in meta}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path).read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = sorted(r[0] for r in rows)
+        out["sm_mhz"] = sm[len(sm) // 2]
+        out["sm_max_mhz"] = max(r[1] for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, flags in rows:
+            for nm, fl in zip(names, flags):
+                if fl.lower() == "active":
+                    reasons.add(nm)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+def pin_arrays(lf):
+    """Move every host field into page-locked memory (the e2e host buffers)."""
+    import torch
+    for ps in lf.systems:
+        for name, _ in ps.particle_fields():
+            a = getattr(ps, name)
+            t = torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.int64,
+                            pin_memory=True)
+            v = t.numpy()
+            v[...] = a
+            setattr(ps, name, v)
+            ps.__dict__.setdefault("_pinned", []).append(t)
+
+
+def field_bytes(lf):
+    return sum(getattr(ps, n).nbytes for ps in lf.systems for n, _ in ps.particle_fields())
+
+
+def cpu_sample(workload, scale, steps, threads):
+    """Time the CPU restatement of the reference on a bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import grasph_b200 as G
+    from pyoracle import OracleBackend
+    lf, meta = build_workload(workload, scale)
+    be = OracleBackend(threads=threads)
+    s = G.Session([lf], backend=be)
+    s.push()
+    s.step(1, meta["cfl"])  # first step sorts every system from scratch
+    t0 = time.perf_counter()
+    s.step(steps, meta["cfl"])
+    dt = time.perf_counter() - t0
+    return meta["n_fluid"] * steps / dt, dt, meta
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    pyoracle.build()
+    steps = max(1, min(args.steps, 3))
+    value, secs, meta = cpu_sample(args.workload, args.scale, steps, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": secs / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": dict(workload_desc(meta), parallelism="cpu threads"),
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full steps after 1 warm-up step on {threads} threads; "
+                                   "the reference's Julia is not available on this box, so the CPU "
+                                   "restatement of its algorithm (coloured sweeps, OpenMP) is timed"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import grasph_b200 as G
+    from grasph_b200 import engine
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+    lf, meta = build_workload(args.workload, args.scale)
+    nd = meta["ndims"]
+    prec = G.PRECISION_FP64 if args.precision == "fp64" else G.PRECISION_FP32_COMPENSATED
+    sess = G.Session([lf], device=local_rank, precision=prec)
+    be = sess.backend
+    lib = be.lib
+    sess.push()
+    peak = engine.ct.c_double()
+    lib.gc_measure_fp64_peak.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_double)]
+    lib.gc_measure_fp64_peak(be.ctx, engine.ct.byref(peak))
+    sess.step(args.warmup, meta["cfl"])
+    sptr = engine.ct.c_void_p()
+    lib.gc_stream.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_void_p)]
+    lib.gc_stream(be.ctx, engine.ct.byref(sptr))
+    stream = torch.cuda.ExternalStream(sptr.value)
+    lib.gc_set_profiling.argtypes = [engine.ct.c_void_p, engine.ct.c_int]
+    lib.gc_set_profiling(be.ctx, 1)
+    st0 = be.stats()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sess.step(args.steps, meta["cfl"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    st1 = be.stats()
+    lib.gc_set_profiling(be.ctx, 0)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+    sweep_ms = st1["sweep_ms"]
+    sweep_launches = max(1, st1["sweep_launches"])
+    pairs = st1["pairs_last_step"]
+    n_fluid = meta["n_fluid"]
+    value = n_fluid * args.steps / (ms / 1e3) * world
+    pair_rate = pairs * args.steps / (ms / 1e3) * world
+
+    # end to end through the host API: pinned host buffers in and out per step
+    e2e = None
+    if not args.no_e2e:
+        pin_arrays(lf)
+        nb = field_bytes(lf)
+        e2e_steps = max(1, min(args.steps, 5))
+        sess.push()
+        sess.step(1, meta["cfl"])
+        sess.pull()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sess.push()
+            sess.step(1, meta["cfl"])
+            sess.pull()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": n_fluid * e2e_steps / el * world, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
+               "ms_per_step": el / e2e_steps * 1e3}
+
+    # roofline of the dominant kernel (the fused pair sweep)
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    hbm_peak, src = 6650.0, "fallback"
+    if peaks_file.exists():
+        hbm_peak, src = json.loads(peaks_file.read_text())["hbm_gbs"], "measured"
+    sweep_avg_s = sweep_ms / sweep_launches / 1e3
+    per_launch_bytes = SWEEP_BYTES_PER_PARTICLE[nd] * n_fluid
+    achieved_gbs = per_launch_bytes / sweep_avg_s / 1e9
+    flops_per_launch = pairs * FLUID_PAIR_FLOPS[nd]
+    achieved_tflops = flops_per_launch / sweep_avg_s / 1e12
+    roof = {"kernel": "k_force (fused FP64 pair sweep)", "bound": "hbm", "achieved": achieved_gbs,
+            "peak": hbm_peak, "peak_source": src, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+            "traffic": None, "bytes_per_launch": per_launch_bytes,
+            "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": (sweep_ms / args.steps) / (ms / args.steps),
+            "compute": {"bound": "fp64", "achieved": achieved_tflops, "peak": peak.value,
+                        "peak_source": "measured FP64 FMA issue rate (gc_measure_fp64_peak)",
+                        "unit": "TFLOP/s", "frac": achieved_tflops / peak.value,
+                        "flops_per_launch": flops_per_launch}}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        v, secs, _ = cpu_sample(args.workload, args.scale, 1, threads)
+        cpu = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"1 full step after 1 warm-up step of the same workload on {threads} threads "
+                         f"({secs:.1f} s); CPU restatement of the reference algorithm"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == G.PRECISION_FP64 else "f32-compensated",
+        "data": "synthetic",
+        "config": dict(workload_desc(meta), parallelism=f"replicas x{world}", l2="state larger than L2",
+                       precision=args.precision),
+        "pair_interactions_per_s": pair_rate, "pairs_per_step": pairs,
+        "gpu_launches": launches, "clocks": clk, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sess.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column"])
+    ap.add_argument("--scale", default="full", choices=["full", "small"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1944 @@
+// gc_context.cu — host runtime of libgrasph_cuda.so: model building, device
+// memory, the per-step schedule and the C ABI of include/grasph_cuda.h.
+//
+// One step (src/TimeIntegration.jl:645-693) is issued as:
+//   plan    bounding boxes → sort/grid/ghost plans → one host read of the
+//           required cell counts (buffers grow here, before any mutation)
+//   sort    stable counting sort of every moving system (key, histogram,
+//           scan, scatter, per-cell fix-up, gather into the other buffer)
+//   ghosts  flag → scan → fill (generation order) → sort
+//   grids   cell histogram of every system_b → scan = CSR cell_start
+//   half    v += dt/2·dvdt, rho += dt/2·drhodt, q0 snapshot, reset to source
+//   stages  updaters → ghost copiers → one fused sweep per (system, stage)
+//   full    damping, q = q0 + dt·dqdt, x += dt·v
+// All launches go to the context's stream; the host reads device memory
+// once per step (the plan) and once per gc_step call (the error word).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gc_force.h"
+#include "gc_internal.h"
+#include "gc_kernels.h"
+#include "gc_update.h"
+
+using namespace gc;
+
+namespace {
+
+// ------------------------------------------------------------ host model
+struct HUpd {
+    int kind;
+    double prm[GC_UPD_NPARAM];
+};
+struct HSys {
+    int kind = 0, nd = 2, ns = 0, nvort = 0;
+    int64_t n = 0;
+    double mass = 0, c = 0, srcv[3] = {0, 0, 0}, srcrho = 0;
+    bool upd_set = false;
+    std::vector<std::vector<HUpd>> upd;
+};
+enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3 };
+struct HHandle {
+    int type = H_SYS, idx = 0;
+    double normal[3] = {0, 0, 0}, point[3] = {0, 0, 0}, beta = 0, ljcut = 0;
+};
+struct HGhost {
+    int src = 0;
+    double cutoff = 0;
+    int nplanes = 0;
+    double normals[4][3] = {}, points[4][3] = {};
+    std::vector<std::vector<std::pair<int, int>>> copiers;
+    bool ex_p = false, ex_stress = false;
+};
+struct HInter {
+    int a = 0, b = -1, kk = 0, nstages = 0;
+    double H = 0;
+    std::vector<int> pk;
+    std::vector<std::array<double, GC_PFN_NPARAM>> pp;
+};
+struct HInst {
+    std::vector<HSys> sys;
+    std::vector<HHandle> handles;
+    std::vector<int> sys_handle;
+    std::vector<HGhost> ghosts;
+    std::vector<HInter> inters;
+    double gamma = 0;
+};
+
+// ---------------------------------------------------------- device state
+enum { F_X = 0, F_V, F_RHO, F_DVDT, F_DRHODT, F_P, F_STRESS, F_SR, F_VORT, F_STRAIN, F_STRAINP, NF };
+
+struct DSlot {
+    int64_t N = 0;
+    int nd = 2, ns = 0, nvort = 0, kind = 0;
+    int ncomp[NF] = {};
+    double* f[2][NF] = {};
+    int32_t* id[2] = {};
+    int cur = 0;
+    double *q0v = nullptr, *q0rho = nullptr, *aux = nullptr;
+    int32_t* inst_of = nullptr;
+    SysInst* d_inst = nullptr;
+    std::vector<SysInst> h_inst;
+    double *d_mass = nullptr, *d_c = nullptr;
+    bool written = false;      // some functor writes this system
+    bool moving = true;        // sorted and integrated every step
+    bool sorted_once = false;  // static systems: sorted since the last upload
+    std::vector<int64_t> nonzero_kin;  // per instance: uploaded v/dvdt/drhodt nonzero
+    // updaters: [stage][chain] -> per-instance UpdInst device array
+    std::vector<std::vector<UpdInst*>> d_upd;
+    std::vector<std::vector<int>> upd_kind;
+    bool upd_set = false;
+    int nupd = 0;
+    double* F(int k) { return f[cur][k]; }
+    double* A(int k) { return f[cur ^ 1][k]; }
+};
+
+struct DGhost {
+    int src = 0, nplanes = 0, nd = 2, ns = 0;
+    int64_t CAP = 0;
+    double* x[2] = {};
+    int32_t *io[2] = {}, *ib[2] = {}, *ginst[2] = {};
+    int cur = 0;
+    double *normals = nullptr, *v = nullptr, *rho = nullptr, *p = nullptr, *stress = nullptr, *aux = nullptr;
+    int32_t *flags = nullptr, *pos = nullptr;
+    int64_t* d_count = nullptr;
+    GhostInst* d_gh = nullptr;
+    std::vector<GhostInst> h_gh;
+    SysInst* d_inst = nullptr;
+    std::vector<SysInst> h_inst;
+    double *d_mass = nullptr, *d_c = nullptr;
+    std::vector<std::vector<std::pair<int, int>>> copiers;
+    bool ex_p = false, ex_stress = false;
+    int64_t need_slot = -1;  // index into need[] for its sort cells
+};
+
+struct DInter {
+    int a = 0, btype = BT_SELF, bslot = -1, bghost = -1, kk = 0, nstages = 0;
+    bool two_sided = false;
+    std::vector<int> pk;
+    GridInst* d_gi = nullptr;
+    std::vector<GridInst> h_gi;
+    std::vector<PfnInst*> d_pi;
+    int32_t* cs = nullptr;     // CSR over system_b
+    int32_t* cs_a = nullptr;   // CSR over system_a (two-sided)
+    int32_t* counts = nullptr; // per system_a particle
+    int64_t cap_cells = 0;
+    int64_t need_slot = -1;
+    bool grid_valid = false;
+};
+
+}  // namespace
+
+struct gc_ctx {
+    int device = 0;
+    size_t budget = 0, allocated = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<HInst> inst;
+    bool finalized = false;
+    int precision = GC_PRECISION_FP64;
+    // structure
+    std::vector<DSlot> slots;
+    std::vector<DGhost> ghosts;
+    std::vector<DInter> inters;
+    int nstages = 0;
+    // scratch
+    int32_t *key = nullptr, *perm = nullptr, *hist = nullptr, *start = nullptr, *fill = nullptr, *scan_tmp = nullptr;
+    int64_t cap_keyN = 0, cap_cells = 0, cap_scan = 0;
+    unsigned long long* bbox_scratch = nullptr;
+    int* d_err = nullptr;
+    unsigned long long* d_incons = nullptr;
+    int64_t* d_need = nullptr;
+    int64_t* h_need = nullptr;  // pinned
+    int nneed = 0;
+    int64_t* d_total_cells = nullptr;  // device copy of the current sort's cell total
+    // host I/O staging (device side of AoS <-> planar transposes)
+    double* staging = nullptr;
+    int64_t cap_staging = 0;  // doubles
+    // stats / profiling
+    int64_t steps_done = 0, resorts = 0;
+    int last_status = 0;
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    size_t ev_used = 0;
+    double sweep_ms = 0;
+    int64_t sweep_launches = 0;
+    unsigned long long* d_pairs = nullptr;
+};
+
+namespace {
+
+// ---------------------------------------------------------------- errors
+int seterr(gc_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+    return code;
+}
+
+#define CU(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return seterr(ctx, GC_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                          __FILE__, __LINE__);                                                 \
+    } while (0)
+
+#define TRY(expr)            \
+    do {                     \
+        int st_ = (expr);    \
+        if (st_) return st_; \
+    } while (0)
+
+template <class T>
+int dalloc(gc_ctx* ctx, T** p, size_t count) {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    if (ctx->budget && ctx->allocated + bytes > ctx->budget)
+        return seterr(ctx, GC_ERR_OOM, "device budget of %zu bytes exceeded", ctx->budget);
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return seterr(ctx, GC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    CU(cudaMemsetAsync(q, 0, bytes, ctx->stream));
+    ctx->allocated += bytes;
+    *p = (T*)q;
+    return GC_OK;
+}
+
+template <class T>
+void dfree(gc_ctx* ctx, T*& p, size_t count) {
+    if (p) {
+        cudaFree(p);
+        size_t bytes = count * sizeof(T);
+        ctx->allocated -= std::min(ctx->allocated, bytes ? bytes : 16);
+        p = nullptr;
+    }
+}
+
+int sys_comps(const HSys& s, int field) {
+    switch (field) {
+        case GC_FIELD_X: case GC_FIELD_V: case GC_FIELD_DVDT: case GC_FIELD_V_ADJUSTMENT: return s.nd;
+        case GC_FIELD_RHO: case GC_FIELD_DRHODT: case GC_FIELD_ID: return 1;
+        case GC_FIELD_P: return s.kind >= GC_SYS_FLUID ? 1 : -1;
+        case GC_FIELD_STRESS: case GC_FIELD_STRAIN_RATE: return s.kind >= GC_SYS_STRESS ? s.ns : -1;
+        case GC_FIELD_VORTICITY: return s.kind == GC_SYS_ELASTOPLASTIC ? s.nvort : -1;
+        case GC_FIELD_STRAIN: case GC_FIELD_STRAIN_P: return s.kind == GC_SYS_ELASTOPLASTIC ? s.ns : -1;
+        default: return -1;
+    }
+}
+
+int field_slot(int field) {
+    switch (field) {
+        case GC_FIELD_X: return F_X;
+        case GC_FIELD_V: return F_V;
+        case GC_FIELD_RHO: return F_RHO;
+        case GC_FIELD_DVDT: return F_DVDT;
+        case GC_FIELD_DRHODT: return F_DRHODT;
+        case GC_FIELD_P: return F_P;
+        case GC_FIELD_STRESS: return F_STRESS;
+        case GC_FIELD_STRAIN_RATE: return F_SR;
+        case GC_FIELD_VORTICITY: return F_VORT;
+        case GC_FIELD_STRAIN: return F_STRAIN;
+        case GC_FIELD_STRAIN_P: return F_STRAINP;
+        default: return -1;
+    }
+}
+
+double kernel_norm(int kind, int nd, double H) {
+    const double pi = 3.141592653589793;
+    if (kind == GC_KERNEL_CUBIC_SPLINE) {
+        if (nd == 1) return 2.0 / (3.0 * H);
+        if (nd == 2) return 10.0 / ((7.0 * pi) * (H * H));
+        return 1.0 / (pi * (H * H * H));
+    }
+    if (nd == 2) return 7.0 / ((64.0 * pi) * (H * H));
+    return 21.0 / ((256.0 * pi) * (H * H * H));
+}
+
+// Functor/system_b combinations implemented (the CPU oracle refuses the same).
+int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
+    const HSys& a = I.sys[it.a];
+    if (pk == GC_PFN_NONE) return GC_OK;
+    if (pk == GC_PFN_FLUID && a.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "FluidPfn needs a pressure field");
+    if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE) && a.kind < GC_SYS_STRESS)
+        return seterr(ctx, GC_ERR_ARG, "functor needs a stress system");
+    if (pk == GC_PFN_STRAIN_RATE_VORTICITY && a.kind != GC_SYS_ELASTOPLASTIC)
+        return seterr(ctx, GC_ERR_ARG, "StrainRateVorticityPfn needs an elasto-plastic system");
+    if (pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE || pk == GC_PFN_STRAIN_RATE_VORTICITY) {
+        if (a.nd == 2 && !(a.ns == 3 || a.ns == 4)) return seterr(ctx, GC_ERR_UNSUPPORTED, "2-D stress needs NS 3 or 4");
+        if (a.nd == 3 && a.ns != 6) return seterr(ctx, GC_ERR_UNSUPPORTED, "3-D stress needs NS 6");
+    }
+    if (it.b < 0) return GC_OK;
+    const HHandle& h = I.handles[it.b];
+    if (pk == GC_PFN_COUNT) return h.type == H_GHOST ? seterr(ctx, GC_ERR_UNSUPPORTED, "counting functor with ghosts") : GC_OK;
+    if (h.type == H_DYN || h.type == H_STATIC) return GC_OK;
+    if (h.type == H_GHOST) {
+        const HGhost& g = I.ghosts[h.idx];
+        if (pk == GC_PFN_FLUID && !g.ex_p) return seterr(ctx, GC_ERR_UNSUPPORTED, "FluidPfn with ghosts needs a :p copier");
+        if (pk == GC_PFN_CAUCHY_FLUID && !g.ex_stress)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "CauchyFluidPfn with ghosts needs a :stress copier");
+        return GC_OK;
+    }
+    const HSys& b = I.sys[h.idx];
+    if (pk == GC_PFN_FLUID) {
+        if (a.kind == GC_SYS_FLUID && b.kind == GC_SYS_FLUID)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "two-sided Fluid×Fluid functor not implemented");
+        return b.kind >= GC_SYS_FLUID ? GC_OK : seterr(ctx, GC_ERR_ARG, "system_b has no pressure field");
+    }
+    if (pk == GC_PFN_CAUCHY_FLUID) return seterr(ctx, GC_ERR_UNSUPPORTED, "two-sided CauchyFluidPfn not implemented");
+    return GC_OK;
+}
+
+// ------------------------------------------------------------- finalize
+bool same_structure(const HInst& a, const HInst& b, std::string& why) {
+    if (a.sys.size() != b.sys.size()) return why = "system count", false;
+    for (size_t s = 0; s < a.sys.size(); ++s) {
+        const HSys &x = a.sys[s], &y = b.sys[s];
+        if (x.kind != y.kind || x.nd != y.nd || x.ns != y.ns) return why = "system kinds", false;
+        if (x.upd_set != y.upd_set || x.upd.size() != y.upd.size()) return why = "updater tuples", false;
+        for (size_t t = 0; t < x.upd.size(); ++t) {
+            if (x.upd[t].size() != y.upd[t].size()) return why = "updater chains", false;
+            for (size_t q = 0; q < x.upd[t].size(); ++q)
+                if (x.upd[t][q].kind != y.upd[t][q].kind) return why = "updater kinds", false;
+        }
+    }
+    if (a.handles.size() != b.handles.size()) return why = "handles", false;
+    for (size_t h = 0; h < a.handles.size(); ++h)
+        if (a.handles[h].type != b.handles[h].type || a.handles[h].idx != b.handles[h].idx)
+            return why = "wrapper/ghost handles", false;
+    if (a.ghosts.size() != b.ghosts.size()) return why = "ghost entries", false;
+    for (size_t g = 0; g < a.ghosts.size(); ++g) {
+        const HGhost &x = a.ghosts[g], &y = b.ghosts[g];
+        if (x.src != y.src || x.nplanes != y.nplanes || x.copiers != y.copiers) return why = "ghost entries", false;
+    }
+    if (a.inters.size() != b.inters.size()) return why = "interactions", false;
+    for (size_t i = 0; i < a.inters.size(); ++i) {
+        const HInter &x = a.inters[i], &y = b.inters[i];
+        if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk)
+            return why = "interactions", false;
+        for (int s = 0; s < x.nstages; ++s)
+            if (x.pp[s][3] != y.pp[s][3] || std::isnan(x.pp[s][4]) != std::isnan(y.pp[s][4]))
+                return why = "functor variants", false;
+    }
+    return true;
+}
+
+UpdInst make_upd(const HUpd& u, const HSys& s) {
+    UpdInst d{};
+    d.kind = u.kind;
+    for (int q = 0; q < GC_UPD_NPARAM; ++q) d.prm[q] = u.prm[q];
+    if (u.kind == GC_UPD_ZERO_FIELDS) d.zmask = (uint32_t)u.prm[0];
+    if (u.kind == GC_UPD_TAIT_EOS) {
+        double rho0 = u.prm[0], gam = u.prm[1];
+        d.pre = rho0 * s.c * s.c / gam;
+        d.gamma_int = (gam == std::trunc(gam) && std::fabs(gam) < 9.0e15) ? 1 : 0;
+    }
+    if (u.kind == GC_UPD_ELASTOPLASTIC || u.kind == GC_UPD_HOOKE) {
+        double E = u.prm[0], nu = u.prm[1], phi = u.prm[2], psi = u.prm[3], coh = u.prm[4];
+        d.D0 = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        d.omn = 1.0 - nu;
+        d.om2n = 1.0 - 2.0 * nu;
+        double sqrt3 = std::sqrt(3.0);
+        double sphi = std::sin(phi), cphi = std::cos(phi), spsi = std::sin(psi);
+        d.a_phi = 2.0 * sphi / (sqrt3 * (3.0 - sphi));
+        d.k_c = 6.0 * coh * cphi / (sqrt3 * (3.0 - sphi));
+        d.a_psi = 2.0 * spsi / (sqrt3 * (3.0 - spsi));
+        d.apex_thr = d.k_c / d.a_phi;
+        d.apex = d.k_c / d.a_phi / 3.0;
+    }
+    return d;
+}
+
+int finalize(gc_ctx* ctx) {
+    if (ctx->inst.empty()) return seterr(ctx, GC_ERR_STATE, "no instance");
+    const HInst& I0 = ctx->inst[0];
+    if (I0.sys.empty()) return seterr(ctx, GC_ERR_ARG, "systems must not be empty");
+    if (I0.inters.empty()) return seterr(ctx, GC_ERR_ARG, "interactions must not be empty");
+    for (size_t k = 1; k < ctx->inst.size(); ++k) {
+        std::string why;
+        if (!same_structure(I0, ctx->inst[k], why))
+            return seterr(ctx, GC_ERR_ARG, "instance %zu differs from instance 0 in %s", k, why.c_str());
+    }
+    ctx->nstages = I0.inters[0].nstages;
+    for (auto& it : I0.inters)
+        if (it.nstages != ctx->nstages)
+            return seterr(ctx, GC_ERR_ARG, "All interactions must have the same number of stages (pfns length)");
+    if (ctx->nstages > MAX_STAGES) return seterr(ctx, GC_ERR_UNSUPPORTED, "too many stages");
+    const int ninst = (int)ctx->inst.size();
+
+    // per-instance dt inputs
+    std::vector<double> hmin(ninst, 1e300), cmax(ninst, -1e300);
+    for (int k = 0; k < ninst; ++k) {
+        for (auto& it : ctx->inst[k].inters) hmin[k] = std::min(hmin[k], it.H);
+        for (auto& s : ctx->inst[k].sys) cmax[k] = std::max(cmax[k], s.c);
+    }
+
+    // ---- system slots
+    ctx->slots.resize(I0.sys.size());
+    int64_t maxN = 0;
+    for (size_t s = 0; s < I0.sys.size(); ++s) {
+        DSlot& D = ctx->slots[s];
+        const HSys& h0 = I0.sys[s];
+        D.nd = h0.nd;
+        D.ns = h0.ns;
+        D.nvort = h0.nvort;
+        D.kind = h0.kind;
+        D.h_inst.resize(ninst);
+        D.nonzero_kin.assign(ninst, 0);
+        int64_t base = 0;
+        for (int k = 0; k < ninst; ++k) {
+            const HSys& h = ctx->inst[k].sys[s];
+            SysInst& S = D.h_inst[k];
+            memset(&S, 0, sizeof S);
+            S.base = base;
+            S.n = h.n;
+            S.mass = h.mass;
+            S.c = h.c;
+            for (int d = 0; d < 3; ++d) S.srcv[d] = h.srcv[d];
+            S.srcrho = h.srcrho;
+            S.sort_cutoff = 2.0 * hmin[k];
+            base += h.n;
+        }
+        D.N = base;
+        if (D.N >= (int64_t)1 << 31) return seterr(ctx, GC_ERR_CAPACITY, "more than 2^31 particles in one system slot");
+        maxN = std::max(maxN, D.N);
+        D.ncomp[F_X] = D.ncomp[F_V] = D.ncomp[F_DVDT] = D.nd;
+        D.ncomp[F_RHO] = D.ncomp[F_DRHODT] = 1;
+        D.ncomp[F_P] = D.kind >= GC_SYS_FLUID ? 1 : 0;
+        D.ncomp[F_STRESS] = D.ncomp[F_SR] = D.kind >= GC_SYS_STRESS ? D.ns : 0;
+        D.ncomp[F_VORT] = D.kind == GC_SYS_ELASTOPLASTIC ? D.nvort : 0;
+        D.ncomp[F_STRAIN] = D.ncomp[F_STRAINP] = D.kind == GC_SYS_ELASTOPLASTIC ? D.ns : 0;
+        for (int b = 0; b < 2; ++b) {
+            for (int f = 0; f < NF; ++f)
+                if (D.ncomp[f]) TRY(dalloc(ctx, &D.f[b][f], (size_t)D.ncomp[f] * D.N));
+            TRY(dalloc(ctx, &D.id[b], (size_t)D.N));
+        }
+        TRY(dalloc(ctx, &D.q0v, (size_t)D.nd * D.N));
+        TRY(dalloc(ctx, &D.q0rho, (size_t)D.N));
+        TRY(dalloc(ctx, &D.aux, (size_t)D.N));
+        TRY(dalloc(ctx, &D.inst_of, (size_t)D.N));
+        std::vector<int32_t> io(D.N);
+        for (int k = 0; k < ninst; ++k)
+            for (int64_t i = 0; i < D.h_inst[k].n; ++i) io[D.h_inst[k].base + i] = k;
+        CU(cudaMemcpyAsync(D.inst_of, io.data(), io.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        TRY(dalloc(ctx, &D.d_inst, (size_t)ninst));
+        TRY(dalloc(ctx, &D.d_mass, (size_t)ninst));
+        TRY(dalloc(ctx, &D.d_c, (size_t)ninst));
+        std::vector<double> m(ninst), c(ninst);
+        for (int k = 0; k < ninst; ++k) {
+            m[k] = D.h_inst[k].mass;
+            c[k] = D.h_inst[k].c;
+        }
+        CU(cudaMemcpyAsync(D.d_mass, m.data(), ninst * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(D.d_c, c.data(), ninst * 8, cudaMemcpyHostToDevice, ctx->stream));
+        // ids default to 1..n per instance
+        std::vector<int32_t> ids(D.N);
+        for (int k = 0; k < ninst; ++k)
+            for (int64_t i = 0; i < D.h_inst[k].n; ++i) ids[D.h_inst[k].base + i] = (int32_t)(i + 1);
+        CU(cudaMemcpyAsync(D.id[0], ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        // updaters
+        D.upd_set = h0.upd_set;
+        D.nupd = (int)h0.upd.size();
+        D.d_upd.resize(h0.upd.size());
+        D.upd_kind.resize(h0.upd.size());
+        for (size_t t = 0; t < h0.upd.size(); ++t) {
+            for (size_t q = 0; q < h0.upd[t].size(); ++q) {
+                std::vector<UpdInst> per(ninst);
+                for (int k = 0; k < ninst; ++k) per[k] = make_upd(ctx->inst[k].sys[s].upd[t][q], ctx->inst[k].sys[s]);
+                UpdInst* d = nullptr;
+                TRY(dalloc(ctx, &d, (size_t)ninst));
+                CU(cudaMemcpyAsync(d, per.data(), ninst * sizeof(UpdInst), cudaMemcpyHostToDevice, ctx->stream));
+                D.d_upd[t].push_back(d);
+                D.upd_kind[t].push_back(h0.upd[t][q].kind);
+            }
+        }
+        // Host-side copies must outlive the async copies above.
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+
+    // ---- ghosts
+    ctx->ghosts.resize(I0.ghosts.size());
+    for (size_t g = 0; g < I0.ghosts.size(); ++g) {
+        DGhost& G = ctx->ghosts[g];
+        const HGhost& h0 = I0.ghosts[g];
+        DSlot& S = ctx->slots[h0.src];
+        G.src = h0.src;
+        G.nplanes = h0.nplanes;
+        G.nd = S.nd;
+        G.ns = S.ns;
+        G.copiers = h0.copiers;
+        G.ex_p = h0.ex_p;
+        G.ex_stress = h0.ex_stress;
+        G.CAP = S.N * G.nplanes;
+        if (G.CAP >= (int64_t)1 << 31) return seterr(ctx, GC_ERR_CAPACITY, "ghost capacity beyond 2^31");
+        maxN = std::max(maxN, G.CAP);
+        for (int b = 0; b < 2; ++b) {
+            TRY(dalloc(ctx, &G.x[b], (size_t)G.nd * G.CAP));
+            TRY(dalloc(ctx, &G.io[b], (size_t)G.CAP));
+            TRY(dalloc(ctx, &G.ib[b], (size_t)G.CAP));
+            TRY(dalloc(ctx, &G.ginst[b], (size_t)G.CAP));
+        }
+        TRY(dalloc(ctx, &G.normals, (size_t)G.nd * G.CAP));
+        TRY(dalloc(ctx, &G.v, (size_t)G.nd * G.CAP));
+        TRY(dalloc(ctx, &G.rho, (size_t)G.CAP));
+        TRY(dalloc(ctx, &G.aux, (size_t)G.CAP));
+        if (G.ex_p) TRY(dalloc(ctx, &G.p, (size_t)G.CAP));
+        if (G.ex_stress) TRY(dalloc(ctx, &G.stress, (size_t)G.ns * G.CAP));
+        TRY(dalloc(ctx, &G.flags, (size_t)G.CAP));
+        TRY(dalloc(ctx, &G.pos, (size_t)G.CAP + 1));
+        TRY(dalloc(ctx, &G.d_count, 1));
+        G.h_gh.resize(ninst);
+        G.h_inst.resize(ninst);
+        std::vector<double> m(ninst), c(ninst);
+        for (int k = 0; k < ninst; ++k) {
+            const HGhost& h = ctx->inst[k].ghosts[g];
+            const HSys& src = ctx->inst[k].sys[h.src];
+            GhostInst& H = G.h_gh[k];
+            memset(&H, 0, sizeof H);
+            for (int b = 0; b < h.nplanes; ++b)
+                for (int d = 0; d < 3; ++d) {
+                    H.normals[b][d] = h.normals[b][d];
+                    H.points[b][d] = h.points[b][d];
+                }
+            H.cutoff = h.cutoff;
+            H.src_base = S.h_inst[k].base;
+            H.src_n = S.h_inst[k].n;
+            H.mass = src.mass;
+            H.c = src.c;
+            SysInst& GI = G.h_inst[k];
+            memset(&GI, 0, sizeof GI);
+            GI.mass = src.mass;
+            GI.c = src.c;
+            GI.sort_cutoff = 2.0 * hmin[k];
+            m[k] = src.mass;
+            c[k] = src.c;
+        }
+        TRY(dalloc(ctx, &G.d_gh, (size_t)ninst));
+        TRY(dalloc(ctx, &G.d_inst, (size_t)ninst));
+        TRY(dalloc(ctx, &G.d_mass, (size_t)ninst));
+        TRY(dalloc(ctx, &G.d_c, (size_t)ninst));
+        CU(cudaMemcpyAsync(G.d_gh, G.h_gh.data(), ninst * sizeof(GhostInst), cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(G.d_inst, G.h_inst.data(), ninst * sizeof(SysInst), cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(G.d_mass, m.data(), ninst * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(G.d_c, c.data(), ninst * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+
+    // ---- interactions
+    ctx->inters.resize(I0.inters.size());
+    for (size_t i = 0; i < I0.inters.size(); ++i) {
+        DInter& D = ctx->inters[i];
+        const HInter& h0 = I0.inters[i];
+        D.a = h0.a;
+        D.kk = h0.kk;
+        D.nstages = h0.nstages;
+        D.pk = h0.pk;
+        if (h0.b < 0) {
+            D.btype = BT_SELF;
+            D.bslot = h0.a;
+        } else {
+            const HHandle& hh = I0.handles[h0.b];
+            if (hh.type == H_GHOST) {
+                D.btype = BT_GHOST;
+                D.bghost = hh.idx;
+            } else {
+                D.btype = hh.type == H_DYN ? BT_DYNAMIC : hh.type == H_STATIC ? BT_STATIC : BT_SYSTEM;
+                D.bslot = hh.idx;
+            }
+        }
+        for (int s = 0; s < D.nstages; ++s)
+            if (D.pk[s] == GC_PFN_COUNT && D.btype != BT_SELF && D.btype != BT_GHOST) D.two_sided = true;
+        D.h_gi.resize(ninst);
+        for (int k = 0; k < ninst; ++k) {
+            const HInst& I = ctx->inst[k];
+            const HInter& h = I.inters[i];
+            GridInst& G = D.h_gi[k];
+            memset(&G, 0, sizeof G);
+            G.H = h.H;
+            G.cell = 2.0 * h.H;
+            G.cutoff_sq = G.cell * G.cell;
+            G.knorm = kernel_norm(h.kk, I.sys[h.a].nd, h.H);
+            if (h.b >= 0) {
+                const HHandle& hh = I.handles[h.b];
+                for (int d = 0; d < 3; ++d) {
+                    G.normal[d] = hh.normal[d];
+                    G.point[d] = hh.point[d];
+                }
+                G.beta = hh.beta;
+                G.ljcut = hh.ljcut;
+                if (hh.type == H_GHOST) {
+                    const HSys& src = I.sys[I.ghosts[hh.idx].src];
+                    G.bmass = src.mass;
+                    G.bc = src.c;
+                } else {
+                    G.bmass = I.sys[hh.idx].mass;
+                    G.bc = I.sys[hh.idx].c;
+                }
+            }
+        }
+        TRY(dalloc(ctx, &D.d_gi, (size_t)ninst));
+        CU(cudaMemcpyAsync(D.d_gi, D.h_gi.data(), ninst * sizeof(GridInst), cudaMemcpyHostToDevice, ctx->stream));
+        D.d_pi.resize(D.nstages, nullptr);
+        for (int s = 0; s < D.nstages; ++s) {
+            std::vector<PfnInst> per(ninst);
+            for (int k = 0; k < ninst; ++k) {
+                const auto& p = ctx->inst[k].inters[i].pp[s];
+                per[k].alpha = p[0];
+                per[k].beta = p[1];
+                per[k].h = p[2];
+                per[k].S = (int)p[3];
+                per[k].delta = std::isnan(p[4]) ? 0.0 : p[4];
+                per[k].has_delta = std::isnan(p[4]) ? 0 : 1;
+            }
+            TRY(dalloc(ctx, &D.d_pi[s], (size_t)ninst));
+            CU(cudaMemcpyAsync(D.d_pi[s], per.data(), ninst * sizeof(PfnInst), cudaMemcpyHostToDevice, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+        }
+        TRY(dalloc(ctx, &D.counts, (size_t)ctx->slots[D.a].N));
+        // writers
+        bool writes = false;
+        for (int s = 0; s < D.nstages; ++s) writes |= D.pk[s] != GC_PFN_NONE;
+        if (writes) ctx->slots[D.a].written = true;
+        if (D.two_sided && D.bslot >= 0) ctx->slots[D.bslot].written = true;
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+
+    // ---- shared scratch
+    ctx->cap_keyN = std::max<int64_t>(maxN, 1);
+    TRY(dalloc(ctx, &ctx->key, (size_t)ctx->cap_keyN));
+    TRY(dalloc(ctx, &ctx->perm, (size_t)ctx->cap_keyN));
+    TRY(dalloc(ctx, &ctx->bbox_scratch, (size_t)ninst * 2 * MAXD));
+    TRY(dalloc(ctx, &ctx->d_err, 1));
+    TRY(dalloc(ctx, &ctx->d_incons, 1));
+    TRY(dalloc(ctx, &ctx->d_total_cells, 1));
+    ctx->nneed = (int)(ctx->slots.size() + ctx->ghosts.size() + ctx->inters.size());
+    TRY(dalloc(ctx, &ctx->d_need, (size_t)ctx->nneed));
+    CU(cudaMallocHost(&ctx->h_need, sizeof(int64_t) * ctx->nneed));
+    for (size_t g = 0; g < ctx->ghosts.size(); ++g) ctx->ghosts[g].need_slot = (int64_t)(ctx->slots.size() + g);
+    for (size_t i = 0; i < ctx->inters.size(); ++i)
+        ctx->inters[i].need_slot = (int64_t)(ctx->slots.size() + ctx->ghosts.size() + i);
+    ctx->finalized = true;
+    return GC_OK;
+}
+
+// ------------------------------------------------------------- capacity
+int ensure_cells(gc_ctx* ctx, int64_t cells) {
+    if (cells + 1 > ctx->cap_cells) {
+        int64_t cap = std::max<int64_t>(cells + 1 + cells / 4, 1024);
+        CU(cudaStreamSynchronize(ctx->stream));  // in-flight kernels may use the old buffers
+        dfree(ctx, ctx->hist, ctx->cap_cells);
+        dfree(ctx, ctx->start, ctx->cap_cells);
+        dfree(ctx, ctx->fill, ctx->cap_cells);
+        TRY(dalloc(ctx, &ctx->hist, (size_t)cap));
+        TRY(dalloc(ctx, &ctx->start, (size_t)cap));
+        TRY(dalloc(ctx, &ctx->fill, (size_t)cap));
+        ctx->cap_cells = cap;
+    }
+    int64_t st = scan_tmp_elems(ctx->cap_cells) + 16;
+    if (st > ctx->cap_scan) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, ctx->scan_tmp, ctx->cap_scan);
+        TRY(dalloc(ctx, &ctx->scan_tmp, (size_t)st));
+        ctx->cap_scan = st;
+    }
+    return GC_OK;
+}
+
+int ensure_inter_cells(gc_ctx* ctx, DInter& D, int64_t cells) {
+    if (cells + 1 > D.cap_cells) {
+        int64_t cap = std::max<int64_t>(cells + 1 + cells / 4, 1024);
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, D.cs, D.cap_cells);
+        dfree(ctx, D.cs_a, D.cap_cells);
+        TRY(dalloc(ctx, &D.cs, (size_t)cap));
+        if (D.two_sided) TRY(dalloc(ctx, &D.cs_a, (size_t)cap));
+        D.cap_cells = cap;
+    }
+    return ensure_cells(ctx, cells);
+}
+
+// ------------------------------------------------------------- phases
+int check_launch(gc_ctx* ctx, const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return seterr(ctx, GC_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+    return GC_OK;
+}
+
+int ninst(gc_ctx* ctx) { return (int)ctx->inst.size(); }
+
+int bbox_slot(gc_ctx* ctx, DSlot& S) {
+    launch_bbox(S.F(F_X), S.N, S.nd, S.inst_of, nullptr, S.d_inst, ctx->bbox_scratch, ninst(ctx), ctx->d_err,
+                ctx->stream);
+    return check_launch(ctx, "bbox");
+}
+
+// Conservative ghost extent before generation: the reflection of the source
+// bounding box's corners across every plane, padded by one cell.
+__global__ void k_ghost_bound(GhostInst* gh, const SysInst* src, SysInst* gi, int ninst, int nd, int nplanes) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ninst) return;
+    const SysInst& S = src[k];
+    double lo[MAXD], hi[MAXD];
+    for (int d = 0; d < nd; ++d) {
+        lo[d] = 1e300;
+        hi[d] = -1e300;
+    }
+    int ncorner = 1 << nd;
+    for (int b = 0; b < nplanes; ++b)
+        for (int cI = 0; cI < ncorner; ++cI) {
+            double x[MAXD], da = 0.0;
+            for (int d = 0; d < nd; ++d) x[d] = (cI >> d) & 1 ? S.bbmax[d] : S.bbmin[d];
+            for (int d = 0; d < nd; ++d) da += (x[d] - gh[k].points[b][d]) * gh[k].normals[b][d];
+            for (int d = 0; d < nd; ++d) {
+                double r = x[d] - 2.0 * da * gh[k].normals[b][d];
+                lo[d] = fmin(lo[d], fmin(r, x[d]));
+                hi[d] = fmax(hi[d], fmax(r, x[d]));
+            }
+        }
+    double pad = 2.0 * S.sort_cutoff;
+    for (int d = 0; d < nd; ++d) {
+        gi[k].bbmin[d] = lo[d] - pad;
+        gi[k].bbmax[d] = hi[d] + pad;
+    }
+    gi[k].n = S.n;  // upper bound on the count, used only for planning
+}
+
+// Stable counting sort of `S` (or of a ghost set when G != nullptr).
+int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells) {
+    const int ni = ninst(ctx);
+    TRY(ensure_cells(ctx, cells));
+    CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
+    CU(cudaMemsetAsync(ctx->fill, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
+    int64_t tc = cells;
+    CU(cudaMemcpyAsync(ctx->d_total_cells, &tc, 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (S) {
+        launch_sort_keys(S->F(F_X), S->N, S->nd, S->inst_of, nullptr, S->d_inst, ctx->key, ctx->hist, ctx->cap_cells,
+                         ctx->d_err, ctx->stream);
+        scan_exclusive(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
+        launch_sort_scatter(ctx->key, S->N, nullptr, ctx->start, ctx->fill, ctx->perm, ctx->stream);
+        launch_sort_fixup(ctx->start, cells, ctx->d_total_cells, ctx->perm, ctx->stream);
+        for (int f = 0; f < NF; ++f)
+            if (S->ncomp[f]) launch_gather(S->F(f), S->A(f), S->ncomp[f], S->N, ctx->perm, nullptr, ctx->stream);
+        launch_gather_i32(S->id[S->cur], S->id[S->cur ^ 1], S->N, ctx->perm, nullptr, ctx->stream);
+        S->cur ^= 1;
+    } else {
+        launch_sort_keys(G->x[G->cur], G->CAP, G->nd, G->ginst[G->cur], G->d_count, G->d_inst, ctx->key, ctx->hist,
+                         ctx->cap_cells, ctx->d_err, ctx->stream);
+        scan_exclusive(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
+        launch_sort_scatter(ctx->key, G->CAP, G->d_count, ctx->start, ctx->fill, ctx->perm, ctx->stream);
+        launch_sort_fixup(ctx->start, cells, ctx->d_total_cells, ctx->perm, ctx->stream);
+        const int c = G->cur, a = c ^ 1;
+        launch_gather(G->x[c], G->x[a], G->nd, G->CAP, ctx->perm, G->d_count, ctx->stream);
+        launch_gather_i32(G->io[c], G->io[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
+        launch_gather_i32(G->ib[c], G->ib[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
+        launch_gather_i32(G->ginst[c], G->ginst[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
+        G->cur = a;
+    }
+    (void)ni;
+    return check_launch(ctx, "sort");
+}
+
+int collect_profile(gc_ctx* ctx);
+
+int read_need(gc_ctx* ctx) {
+    CU(cudaMemcpyAsync(ctx->h_need, ctx->d_need, sizeof(int64_t) * ctx->nneed, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    TRY(collect_profile(ctx));
+    int e = 0;
+    CU(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e & ERR_NONFINITE) return seterr(ctx, GC_ERR_NONFINITE, "non-finite or out-of-range particle position");
+    if (e & ERR_CAPACITY) return seterr(ctx, GC_ERR_CAPACITY, "grid or key range exceeds 2^31 cells");
+    return GC_OK;
+}
+
+GridPlanArgs grid_plan_args(gc_ctx* ctx, DInter& D) {
+    GridPlanArgs g{};
+    g.gi = D.d_gi;
+    g.ninst = ninst(ctx);
+    g.nd = ctx->slots[D.a].nd;
+    g.a = ctx->slots[D.a].d_inst;
+    if (D.btype == BT_GHOST) g.b = ctx->ghosts[D.bghost].d_inst;
+    else if (D.btype != BT_SELF) g.b = ctx->slots[D.bslot].d_inst;
+    g.need = ctx->d_need + D.need_slot;
+    g.err = ctx->d_err;
+    return g;
+}
+
+// Ghost generation into the current buffers (generation order).
+int generate_ghosts(gc_ctx* ctx, DGhost& G) {
+    DSlot& S = ctx->slots[G.src];
+    GhostGenArgs a{};
+    a.src_x = S.F(F_X);
+    a.Nsrc = S.N;
+    a.src_inst_of = S.inst_of;
+    a.gh = G.d_gh;
+    a.ninst = ninst(ctx);
+    a.nd = G.nd;
+    a.nplanes = G.nplanes;
+    a.flags = G.flags;
+    a.pos = G.pos;
+    a.gx = G.x[G.cur];
+    a.gio = G.io[G.cur];
+    a.gib = G.ib[G.cur];
+    a.ginst = G.ginst[G.cur];
+    a.gnormals = G.normals;
+    a.count = G.d_count;
+    a.ginst_params = G.d_inst;
+    launch_ghost_flags(a, ctx->stream);
+    int64_t n = G.CAP;
+    int64_t st = scan_tmp_elems(n) + 16;
+    if (st > ctx->cap_scan) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, ctx->scan_tmp, ctx->cap_scan);
+        TRY(dalloc(ctx, &ctx->scan_tmp, (size_t)st));
+        ctx->cap_scan = st;
+    }
+    scan_exclusive(G.flags, G.pos, n, ctx->scan_tmp, ctx->stream);
+    launch_ghost_fill(a, ctx->stream);
+    return check_launch(ctx, "ghost generation");
+}
+
+int ghost_bbox_and_plan(gc_ctx* ctx, DGhost& G) {
+    launch_bbox(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
+                ctx->d_err, ctx->stream);
+    launch_sort_plan(G.d_inst, ninst(ctx), G.nd, ctx->d_need + G.need_slot, ctx->d_err, ctx->stream);
+    return check_launch(ctx, "ghost plan");
+}
+
+int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
+    TRY(ensure_inter_cells(ctx, D, cells));
+    DSlot& A = ctx->slots[D.a];
+    const double* bx;
+    const int32_t* binst;
+    const int64_t* bcount = nullptr;
+    int64_t bN;
+    if (D.btype == BT_GHOST) {
+        DGhost& G = ctx->ghosts[D.bghost];
+        bx = G.x[G.cur];
+        binst = G.ginst[G.cur];
+        bcount = G.d_count;
+        bN = G.CAP;
+    } else {
+        DSlot& B = ctx->slots[D.bslot];
+        bx = B.F(F_X);
+        binst = B.inst_of;
+        bN = B.N;
+    }
+    CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
+    launch_grid_count(bx, bN, A.nd, binst, bcount, D.d_gi, ctx->hist, cells, ctx->d_err, ctx->d_incons, ctx->stream);
+    scan_exclusive(ctx->hist, D.cs, cells, ctx->scan_tmp, ctx->stream);
+    if (D.two_sided) {
+        CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
+        launch_grid_count(A.F(F_X), A.N, A.nd, A.inst_of, nullptr, D.d_gi, ctx->hist, cells, ctx->d_err,
+                          ctx->d_incons, ctx->stream);
+        scan_exclusive(ctx->hist, D.cs_a, cells, ctx->scan_tmp, ctx->stream);
+    }
+    D.grid_valid = true;
+    return check_launch(ctx, "grid");
+}
+
+// Full prepare phase: sorts, ghosts and grids.  `sort_mask` selects which
+// system slots are sorted.
+int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
+    const int ni = ninst(ctx);
+    CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
+    // bounding boxes of every real system (positions are current)
+    for (auto& S : ctx->slots) TRY(bbox_slot(ctx, S));
+    for (size_t s = 0; s < ctx->slots.size(); ++s)
+        if (sort_mask[s])
+            launch_sort_plan(ctx->slots[s].d_inst, ni, ctx->slots[s].nd, ctx->d_need + s, ctx->d_err, ctx->stream);
+    for (auto& G : ctx->ghosts) {
+        k_ghost_bound<<<(ni + 127) / 128, 128, 0, ctx->stream>>>(G.d_gh, ctx->slots[G.src].d_inst, G.d_inst, ni, G.nd,
+                                                                 G.nplanes);
+        launch_sort_plan(G.d_inst, ni, G.nd, ctx->d_need + G.need_slot, ctx->d_err, ctx->stream);
+    }
+    for (auto& D : ctx->inters) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
+    TRY(check_launch(ctx, "plan"));
+    TRY(read_need(ctx));
+    std::vector<int64_t> need(ctx->h_need, ctx->h_need + ctx->nneed);
+    // sorts
+    for (size_t s = 0; s < ctx->slots.size(); ++s)
+        if (sort_mask[s]) TRY(sort_particles_slot(ctx, &ctx->slots[s], nullptr, need[s]));
+    // ghosts: generate, bound-checked plan, sort
+    for (auto& G : ctx->ghosts) {
+        TRY(generate_ghosts(ctx, G));
+        TRY(ghost_bbox_and_plan(ctx, G));
+        TRY(sort_particles_slot(ctx, nullptr, &G, need[G.need_slot]));
+    }
+    // grids (ghost-b plans are recomputed from the exact ghost boxes; the
+    // cell count cannot exceed the planned bound)
+    for (auto& D : ctx->inters) {
+        if (D.btype == BT_GHOST) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
+        TRY(build_grid(ctx, D, need[D.need_slot]));
+    }
+    return GC_OK;
+}
+
+StepArgs step_args(DSlot& S) {
+    StepArgs a{};
+    a.N = S.N;
+    a.nd = S.nd;
+    a.inst_of = S.inst_of;
+    a.inst = S.d_inst;
+    a.x = S.F(F_X);
+    a.v = S.F(F_V);
+    a.rho = S.F(F_RHO);
+    a.dvdt = S.F(F_DVDT);
+    a.drhodt = S.F(F_DRHODT);
+    a.q0v = S.q0v;
+    a.q0rho = S.q0rho;
+    return a;
+}
+
+int run_updaters(gc_ctx* ctx, DSlot& S, int stage, double dt_override) {
+    if (stage < 1 || stage > (int)S.d_upd.size()) return GC_OK;
+    for (size_t q = 0; q < S.d_upd[stage - 1].size(); ++q) {
+        UpdArgs a{};
+        a.N = S.N;
+        a.nd = S.nd;
+        a.ns = S.ns;
+        a.nvort = S.nvort;
+        a.inst_of = S.inst_of;
+        a.inst = S.d_inst;
+        a.u = S.d_upd[stage - 1][q];
+        a.dt = dt_override;
+        a.rho = S.F(F_RHO);
+        a.p = S.F(F_P);
+        a.stress = S.F(F_STRESS);
+        a.sr = S.F(F_SR);
+        a.vort = S.F(F_VORT);
+        a.strain = S.F(F_STRAIN);
+        a.strainp = S.F(F_STRAINP);
+        a.dvdt = S.F(F_DVDT);
+        a.drhodt = S.F(F_DRHODT);
+        launch_update(a, ctx->stream);
+    }
+    return check_launch(ctx, "updater");
+}
+
+int ghost_kinematics(gc_ctx* ctx, DGhost& G) {
+    DSlot& S = ctx->slots[G.src];
+    launch_ghost_kinematics(G.CAP, G.d_count, G.nd, G.io[G.cur], G.ginst[G.cur], G.normals, G.d_gh, S.F(F_V),
+                            S.F(F_RHO), S.N, G.v, G.rho, ctx->stream);
+    return check_launch(ctx, "ghost kinematics");
+}
+
+int ghost_copy(gc_ctx* ctx, DGhost& G, int stage) {
+    if (stage < 1 || stage > (int)G.copiers.size()) return GC_OK;
+    DSlot& S = ctx->slots[G.src];
+    for (auto& e : G.copiers[stage - 1]) {
+        int field = e.first, mode = e.second;
+        if (field == GC_FIELD_P)
+            launch_ghost_copy(G.CAP, G.d_count, G.nd, 1, G.io[G.cur], G.ginst[G.cur], G.normals, G.d_gh, field, mode,
+                              S.F(F_P), S.N, G.p, ctx->stream);
+        else if (field == GC_FIELD_STRESS)
+            launch_ghost_copy(G.CAP, G.d_count, G.nd, G.ns, G.io[G.cur], G.ginst[G.cur], G.normals, G.d_gh, field,
+                              mode, S.F(F_STRESS), S.N, G.stress, ctx->stream);
+    }
+    return check_launch(ctx, "ghost copy");
+}
+
+int aux_mode_for(int pfn) {
+    if (pfn == GC_PFN_FLUID) return AUX_P_OVER_RHO2;
+    if (pfn == GC_PFN_CAUCHY_FLUID) return AUX_INV_RHO2;
+    return AUX_MASS_OVER_RHO;
+}
+
+// Fused sweep of the interactions `ids` (same system_a, same functor kind).
+int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
+    DSlot& S = ctx->slots[a];
+    int pfn = ctx->inters[ids[0]].pk[stage - 1];
+    const int mode = aux_mode_for(pfn);
+    if (pfn != GC_PFN_COUNT) {
+        launch_aux(mode, S.N, nullptr, S.F(F_RHO), S.F(F_P), S.inst_of, S.d_mass, S.aux, ctx->stream);
+    }
+    ForceArgs A{};
+    A.nd = S.nd;
+    A.ns = S.ns;
+    A.pfn = pfn;
+    A.kk = ctx->inters[ids[0]].kk;
+    A.aN = S.N;
+    A.a_inst_of = S.inst_of;
+    A.ax = S.F(F_X);
+    A.av = S.F(F_V);
+    A.arho = S.F(F_RHO);
+    A.aaux = S.aux;
+    A.astress = S.F(F_STRESS);
+    A.a_p = S.F(F_P);
+    A.advdt = S.F(F_DVDT);
+    A.adrhodt = S.F(F_DRHODT);
+    A.asr = S.F(F_SR);
+    A.avort = S.F(F_VORT);
+    A.a_c = S.d_c;
+    A.a_mass = S.d_mass;
+    A.err = ctx->d_err;
+    A.nref = 0;
+    for (int id : ids) {
+        DInter& D = ctx->inters[id];
+        if (!D.grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
+        if (A.nref == MAX_REFS) return seterr(ctx, GC_ERR_UNSUPPORTED, "too many interactions on one system");
+        InterRef& r = A.ref[A.nref++];
+        r.btype = D.btype;
+        r.gi = D.d_gi;
+        r.pi = D.d_pi[stage - 1];
+        r.cs = D.cs;
+        r.counts = D.counts;
+        if (D.btype == BT_GHOST) {
+            DGhost& G = ctx->ghosts[D.bghost];
+            r.bx = G.x[G.cur];
+            r.bv = G.v;
+            r.brho = G.rho;
+            r.bp = G.p;
+            r.bstress = G.stress;
+            r.bN = G.CAP;
+            if (pfn != GC_PFN_COUNT)
+                launch_aux(mode, G.CAP, G.d_count, G.rho, G.p, G.ginst[G.cur], G.d_mass, G.aux, ctx->stream);
+            r.baux = G.aux;
+        } else {
+            DSlot& B = ctx->slots[D.bslot];
+            r.bx = B.F(F_X);
+            r.bv = B.F(F_V);
+            r.brho = B.F(F_RHO);
+            r.bp = B.F(F_P);
+            r.bstress = B.F(F_STRESS);
+            r.bN = B.N;
+            if (D.btype == BT_SELF) {
+                r.baux = S.aux;
+            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT) {
+                launch_aux(mode, B.N, nullptr, B.F(F_RHO), B.F(F_P), B.inst_of, B.d_mass, B.aux, ctx->stream);
+                r.baux = B.aux;
+            } else {
+                r.baux = B.aux;
+            }
+        }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->profiling && !count_only) {
+        if (ctx->ev_used == ctx->ev_pool.size()) {
+            cudaEvent_t a, b;
+            CU(cudaEventCreate(&a));
+            CU(cudaEventCreate(&b));
+            ctx->ev_pool.push_back({a, b});
+        }
+        e0 = ctx->ev_pool[ctx->ev_used].first;
+        e1 = ctx->ev_pool[ctx->ev_used].second;
+        ctx->ev_used++;
+        CU(cudaEventRecord(e0, ctx->stream));
+    }
+    int st = launch_force_f64(A, count_only, ctx->stream);
+    if (st) return seterr(ctx, st, "functor/system combination not implemented on the device");
+    if (e1) CU(cudaEventRecord(e1, ctx->stream));
+    TRY(check_launch(ctx, "sweep"));
+    // b side of two-sided (counting) coupled interactions
+    for (int id : ids) {
+        DInter& D = ctx->inters[id];
+        if (!D.two_sided || count_only) continue;
+        DSlot& B = ctx->slots[D.bslot];
+        ForceArgs R = A;
+        R.nd = B.nd;
+        R.ns = B.ns;
+        R.aN = B.N;
+        R.a_inst_of = B.inst_of;
+        R.ax = B.F(F_X);
+        R.av = B.F(F_V);
+        R.arho = B.F(F_RHO);
+        R.aaux = B.aux;
+        R.advdt = B.F(F_DVDT);
+        R.adrhodt = B.F(F_DRHODT);
+        R.a_c = B.d_c;
+        R.a_mass = B.d_mass;
+        R.nref = 1;
+        InterRef& r = R.ref[0];
+        r.btype = BT_SYSTEM;
+        r.gi = D.d_gi;
+        r.pi = D.d_pi[stage - 1];
+        r.cs = D.cs_a;
+        r.counts = nullptr;
+        r.bx = S.F(F_X);
+        r.bv = S.F(F_V);
+        r.brho = S.F(F_RHO);
+        r.bp = S.F(F_P);
+        r.bstress = S.F(F_STRESS);
+        r.baux = S.aux;
+        r.bN = S.N;
+        st = launch_force_f64(R, false, ctx->stream);
+        if (st) return seterr(ctx, st, "two-sided functor not implemented on the device");
+        TRY(check_launch(ctx, "sweep (system_b side)"));
+    }
+    return GC_OK;
+}
+
+int sweep_stage(gc_ctx* ctx, int stage) {
+    for (size_t a = 0; a < ctx->slots.size(); ++a) {
+        // group this system's interactions by functor kind
+        std::vector<int> kinds;
+        for (size_t i = 0; i < ctx->inters.size(); ++i) {
+            DInter& D = ctx->inters[i];
+            int pk = D.pk[stage - 1];
+            if (D.a != (int)a || pk == GC_PFN_NONE) continue;
+            if (std::find(kinds.begin(), kinds.end(), pk) == kinds.end()) kinds.push_back(pk);
+        }
+        for (int pk : kinds) {
+            std::vector<int> ids;
+            for (size_t i = 0; i < ctx->inters.size(); ++i)
+                if (ctx->inters[i].a == (int)a && ctx->inters[i].pk[stage - 1] == pk) ids.push_back((int)i);
+            for (size_t off = 0; off < ids.size(); off += MAX_REFS) {
+                std::vector<int> chunk(ids.begin() + off, ids.begin() + std::min(ids.size(), off + MAX_REFS));
+                TRY(sweep_group(ctx, (int)a, chunk, stage, false));
+            }
+        }
+    }
+    return GC_OK;
+}
+
+void upload_inst_params(gc_ctx* ctx, double cfl) {
+    const int ni = ninst(ctx);
+    for (int k = 0; k < ni; ++k) {
+        const HInst& I = ctx->inst[k];
+        double h = 1e300, c = -1e300;
+        for (auto& it : I.inters) h = std::min(h, it.H);
+        for (auto& s : I.sys) c = std::max(c, s.c);
+        double dt = cfl * h / c;
+        for (auto& S : ctx->slots) {
+            S.h_inst[k].dt = dt;
+            S.h_inst[k].half_dt = dt / 2.0;
+            S.h_inst[k].gamma_dt = I.gamma != 0.0 ? I.gamma / dt : 0.0;
+            S.h_inst[k].sort_cutoff = 2.0 * h;
+        }
+    }
+}
+
+int push_slot_params(gc_ctx* ctx, DSlot& S) {
+    // Only the host-owned members; bbox/plan members are device-written.
+    const int ni = ninst(ctx);
+    std::vector<SysInst> cur(ni);
+    CU(cudaMemcpy(cur.data(), S.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < ni; ++k) {
+        cur[k].base = S.h_inst[k].base;
+        cur[k].n = S.h_inst[k].n;
+        cur[k].mass = S.h_inst[k].mass;
+        cur[k].c = S.h_inst[k].c;
+        for (int d = 0; d < 3; ++d) cur[k].srcv[d] = S.h_inst[k].srcv[d];
+        cur[k].srcrho = S.h_inst[k].srcrho;
+        cur[k].sort_cutoff = S.h_inst[k].sort_cutoff;
+        cur[k].dt = S.h_inst[k].dt;
+        cur[k].half_dt = S.h_inst[k].half_dt;
+        cur[k].gamma_dt = S.h_inst[k].gamma_dt;
+    }
+    CU(cudaMemcpy(S.d_inst, cur.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
+    return GC_OK;
+}
+
+void decide_motion(gc_ctx* ctx) {
+    for (auto& S : ctx->slots) {
+        bool src_zero = true;
+        for (auto& h : S.h_inst) {
+            for (int d = 0; d < S.nd; ++d) src_zero &= h.srcv[d] == 0.0;
+            src_zero &= h.srcrho == 0.0;
+        }
+        bool kin_zero = true;
+        for (auto v : S.nonzero_kin) kin_zero &= v == 0;
+        S.moving = S.written || !src_zero || !kin_zero;
+    }
+}
+
+int one_step(gc_ctx* ctx) {
+    std::vector<char> mask(ctx->slots.size());
+    for (size_t s = 0; s < ctx->slots.size(); ++s) {
+        DSlot& S = ctx->slots[s];
+        mask[s] = S.moving || !S.sorted_once;
+    }
+    TRY(prepare(ctx, mask));
+    for (size_t s = 0; s < ctx->slots.size(); ++s)
+        if (mask[s]) ctx->slots[s].sorted_once = true;
+    ctx->resorts += 1;
+    for (auto& S : ctx->slots)
+        if (S.moving) launch_halfstep(step_args(S), ctx->stream);
+    TRY(check_launch(ctx, "half step"));
+    for (auto& G : ctx->ghosts) TRY(ghost_kinematics(ctx, G));
+    for (int stage = 1; stage <= ctx->nstages; ++stage) {
+        for (auto& S : ctx->slots)
+            if (S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
+        for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
+        TRY(sweep_stage(ctx, stage));
+    }
+    for (auto& S : ctx->slots)
+        if (S.moving) launch_fullstep(step_args(S), ctx->stream);
+    TRY(check_launch(ctx, "full step"));
+    ctx->steps_done += 1;
+    return GC_OK;
+}
+
+int collect_profile(gc_ctx* ctx) {
+    for (size_t i = 0; i < ctx->ev_used; ++i) {
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, ctx->ev_pool[i].first, ctx->ev_pool[i].second));
+        ctx->sweep_ms += ms;
+        ctx->sweep_launches += 1;
+    }
+    ctx->ev_used = 0;
+    return GC_OK;
+}
+
+int finish_status(gc_ctx* ctx) {
+    CU(cudaStreamSynchronize(ctx->stream));
+    TRY(collect_profile(ctx));
+    int e = 0;
+    CU(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    ctx->last_status = e;
+    if (e & ERR_NONFINITE) return seterr(ctx, GC_ERR_NONFINITE, "non-finite or out-of-range particle position");
+    if (e & ERR_CAPACITY) return seterr(ctx, GC_ERR_CAPACITY, "a particle fell outside its grid or key range");
+    return GC_OK;
+}
+
+bool valid_inst(gc_ctx* ctx, int inst) { return inst >= 0 && inst < (int)ctx->inst.size(); }
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+const char* gc_status_string(int st) {
+    switch (st) {
+        case GC_OK: return "GC_OK";
+        case GC_ERR_ARG: return "GC_ERR_ARG";
+        case GC_ERR_OOM: return "GC_ERR_OOM";
+        case GC_ERR_CAPACITY: return "GC_ERR_CAPACITY";
+        case GC_ERR_NONFINITE: return "GC_ERR_NONFINITE";
+        case GC_ERR_GRID_INCONSISTENT: return "GC_ERR_GRID_INCONSISTENT";
+        case GC_ERR_TIMEOUT: return "GC_ERR_TIMEOUT";
+        case GC_ERR_CUDA: return "GC_ERR_CUDA";
+        case GC_ERR_STATE: return "GC_ERR_STATE";
+        case GC_ERR_UNSUPPORTED: return "GC_ERR_UNSUPPORTED";
+    }
+    return "unknown status";
+}
+
+int gc_ctx_create(int device, size_t hbm_budget_bytes, gc_ctx** out) {
+    if (!out) return GC_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return GC_ERR_CUDA;
+    if (device < 0 || device >= n) return GC_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return GC_ERR_CUDA;
+    gc_ctx* ctx = new gc_ctx();
+    ctx->device = device;
+    ctx->budget = hbm_budget_bytes;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return GC_ERR_CUDA;
+    }
+    *out = ctx;
+    return GC_OK;
+}
+
+int gc_ctx_destroy(gc_ctx* ctx) {
+    if (!ctx) return GC_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& S : ctx->slots) {
+        for (int b = 0; b < 2; ++b) {
+            for (int f = 0; f < NF; ++f) cudaFree(S.f[b][f]);
+            cudaFree(S.id[b]);
+        }
+        cudaFree(S.q0v);
+        cudaFree(S.q0rho);
+        cudaFree(S.aux);
+        cudaFree(S.inst_of);
+        cudaFree(S.d_inst);
+        cudaFree(S.d_mass);
+        cudaFree(S.d_c);
+        for (auto& ch : S.d_upd)
+            for (auto* p : ch) cudaFree(p);
+    }
+    for (auto& G : ctx->ghosts) {
+        for (int b = 0; b < 2; ++b) {
+            cudaFree(G.x[b]);
+            cudaFree(G.io[b]);
+            cudaFree(G.ib[b]);
+            cudaFree(G.ginst[b]);
+        }
+        cudaFree(G.normals);
+        cudaFree(G.v);
+        cudaFree(G.rho);
+        cudaFree(G.p);
+        cudaFree(G.stress);
+        cudaFree(G.aux);
+        cudaFree(G.flags);
+        cudaFree(G.pos);
+        cudaFree(G.d_count);
+        cudaFree(G.d_gh);
+        cudaFree(G.d_inst);
+        cudaFree(G.d_mass);
+        cudaFree(G.d_c);
+    }
+    for (auto& D : ctx->inters) {
+        cudaFree(D.d_gi);
+        for (auto* p : D.d_pi) cudaFree(p);
+        cudaFree(D.cs);
+        cudaFree(D.cs_a);
+        cudaFree(D.counts);
+    }
+    cudaFree(ctx->key);
+    cudaFree(ctx->perm);
+    cudaFree(ctx->hist);
+    cudaFree(ctx->start);
+    cudaFree(ctx->fill);
+    cudaFree(ctx->scan_tmp);
+    cudaFree(ctx->bbox_scratch);
+    cudaFree(ctx->d_err);
+    cudaFree(ctx->d_incons);
+    cudaFree(ctx->d_need);
+    cudaFree(ctx->d_total_cells);
+    if (ctx->h_need) cudaFreeHost(ctx->h_need);
+    cudaFree(ctx->staging);
+    cudaFree(ctx->d_pairs);
+    for (auto& e : ctx->ev_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GC_OK;
+}
+
+const char* gc_last_error(gc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int gc_instance_add(gc_ctx* ctx, int* inst_out) {
+    if (!ctx || !inst_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    ctx->inst.emplace_back();
+    *inst_out = (int)ctx->inst.size() - 1;
+    return GC_OK;
+}
+
+int gc_add_system(gc_ctx* ctx, int inst, int kind, int64_t n, int ndims, int ns, double mass, double c,
+                  const double* source_v, double source_rho, int* sys_out) {
+    if (!ctx || !sys_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance %d", inst);
+    if (n <= 0) return seterr(ctx, GC_ERR_ARG, "n must be positive, got %lld", (long long)n);
+    if (ndims < 2 || ndims > 3) return seterr(ctx, GC_ERR_UNSUPPORTED, "ndims must be 2 or 3, got %d", ndims);
+    if (kind < GC_SYS_BASIC || kind > GC_SYS_ELASTOPLASTIC) return seterr(ctx, GC_ERR_ARG, "bad system kind");
+    if (kind >= GC_SYS_STRESS && !(ns == 3 || ns == 4 || ns == 6))
+        return seterr(ctx, GC_ERR_ARG, "ns must be 3, 4, or 6, got %d", ns);
+    HInst& I = ctx->inst[inst];
+    HSys s;
+    s.kind = kind;
+    s.n = n;
+    s.nd = ndims;
+    s.ns = kind >= GC_SYS_STRESS ? ns : 0;
+    s.nvort = kind == GC_SYS_ELASTOPLASTIC ? (ndims == 2 ? 1 : 3) : 0;
+    s.mass = mass;
+    s.c = c;
+    for (int d = 0; d < ndims; ++d) s.srcv[d] = source_v ? source_v[d] : 0.0;
+    s.srcrho = source_rho;
+    I.sys.push_back(s);
+    HHandle h;
+    h.type = H_SYS;
+    h.idx = (int)I.sys.size() - 1;
+    I.handles.push_back(h);
+    I.sys_handle.push_back((int)I.handles.size() - 1);
+    *sys_out = (int)I.handles.size() - 1;
+    return GC_OK;
+}
+
+static int sys_of(gc_ctx* ctx, int inst, int handle) {
+    if (!valid_inst(ctx, inst)) return -1;
+    HInst& I = ctx->inst[inst];
+    if (handle < 0 || handle >= (int)I.handles.size() || I.handles[handle].type != H_SYS) return -1;
+    return I.handles[handle].idx;
+}
+
+int gc_add_boundary(gc_ctx* ctx, int inst, int sys, int kind, const double* normal, const double* point,
+                    double beta_or_lj_cutoff, int* handle_out) {
+    if (!ctx || !handle_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    int si = sys_of(ctx, inst, sys);
+    if (si < 0) return seterr(ctx, GC_ERR_ARG, "boundary inner must be a system handle");
+    HInst& I = ctx->inst[inst];
+    HHandle h;
+    h.idx = si;
+    const int nd = I.sys[si].nd;
+    if (kind == GC_WRAP_DYNAMIC) {
+        if (!normal || !point) return seterr(ctx, GC_ERR_ARG, "dynamic boundary needs normal and point");
+        h.type = H_DYN;
+        for (int d = 0; d < nd; ++d) {
+            h.normal[d] = normal[d];
+            h.point[d] = point[d];
+        }
+        h.beta = beta_or_lj_cutoff;
+    } else if (kind == GC_WRAP_STATIC) {
+        h.type = H_STATIC;
+        h.ljcut = beta_or_lj_cutoff;
+    } else {
+        return seterr(ctx, GC_ERR_ARG, "bad boundary kind %d", kind);
+    }
+    I.handles.push_back(h);
+    *handle_out = (int)I.handles.size() - 1;
+    return GC_OK;
+}
+
+int gc_add_ghost(gc_ctx* ctx, int inst, int src_sys, int ncopiers, const int* copier_nfields,
+                 const int* copier_fields, const int* copier_modes, int nplanes, const double* normals,
+                 const double* points, double cutoff, int64_t capacity, int* handle_out) {
+    if (!ctx || !handle_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    int si = sys_of(ctx, inst, src_sys);
+    if (si < 0) return seterr(ctx, GC_ERR_ARG, "ghost source must be a system handle");
+    if (nplanes < 1) return seterr(ctx, GC_ERR_ARG, "at least one boundary (normal, point) pair is required");
+    if (nplanes > 4) return seterr(ctx, GC_ERR_UNSUPPORTED, "at most 4 planes per ghost entry");
+    HInst& I = ctx->inst[inst];
+    const HSys& s = I.sys[si];
+    HGhost g;
+    g.src = si;
+    g.cutoff = cutoff;
+    g.nplanes = nplanes;
+    for (int b = 0; b < nplanes; ++b)
+        for (int d = 0; d < s.nd; ++d) {
+            g.normals[b][d] = normals[b * s.nd + d];
+            g.points[b][d] = points[b * s.nd + d];
+        }
+    int pos = 0;
+    for (int k = 0; k < ncopiers; ++k) {
+        std::vector<std::pair<int, int>> cp;
+        for (int e = 0; e < copier_nfields[k]; ++e, ++pos) {
+            int fld = copier_fields[pos], mode = copier_modes[pos];
+            if (fld == GC_FIELD_P) {
+                if (s.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "copier field p missing on source");
+                g.ex_p = true;
+            } else if (fld == GC_FIELD_STRESS) {
+                if (s.kind < GC_SYS_STRESS) return seterr(ctx, GC_ERR_ARG, "copier field stress missing on source");
+                g.ex_stress = true;
+            } else if (fld != GC_FIELD_RHO) {
+                return seterr(ctx, GC_ERR_UNSUPPORTED, "copier field %d not supported", fld);
+            }
+            cp.push_back({fld, mode});
+        }
+        g.copiers.push_back(cp);
+    }
+    (void)capacity;
+    I.ghosts.push_back(g);
+    HHandle h;
+    h.type = H_GHOST;
+    h.idx = (int)I.ghosts.size() - 1;
+    I.handles.push_back(h);
+    *handle_out = (int)I.handles.size() - 1;
+    return GC_OK;
+}
+
+int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kernel_kind, double h, int nstages,
+                       const int* pfn_kinds, const double* pfn_params, int* inter_out) {
+    if (!ctx || !inter_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    int si = sys_of(ctx, inst, sys_a);
+    if (si < 0) return seterr(ctx, GC_ERR_ARG, "system_a must be a system handle");
+    HInst& I = ctx->inst[inst];
+    if (b_handle >= (int)I.handles.size()) return seterr(ctx, GC_ERR_ARG, "bad system_b handle");
+    if (nstages < 1 || nstages > MAX_STAGES) return seterr(ctx, GC_ERR_ARG, "bad stage count");
+    if (kernel_kind != GC_KERNEL_CUBIC_SPLINE && kernel_kind != GC_KERNEL_WENDLAND_C2)
+        return seterr(ctx, GC_ERR_ARG, "bad kernel kind");
+    HInter it;
+    it.a = si;
+    it.b = b_handle;
+    it.kk = kernel_kind;
+    it.H = h;
+    it.nstages = nstages;
+    for (int s = 0; s < nstages; ++s) {
+        it.pk.push_back(pfn_kinds[s]);
+        std::array<double, GC_PFN_NPARAM> a;
+        for (int k = 0; k < GC_PFN_NPARAM; ++k) a[k] = pfn_params[s * GC_PFN_NPARAM + k];
+        if (pfn_kinds[s] == GC_PFN_FLUID && !(a[3] == 1.0 || a[3] == 2.0))
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "FluidPfn sigma must be 1 or 2");
+        it.pp.push_back(a);
+        int st = check_combo(ctx, I, it, pfn_kinds[s]);
+        if (st) return st;
+    }
+    I.inters.push_back(it);
+    *inter_out = (int)I.inters.size() - 1;
+    return GC_OK;
+}
+
+int gc_set_updaters(gc_ctx* ctx, int inst, int sys, int nstages, const int* chain_len, const int* kinds,
+                    const double* params) {
+    if (!ctx) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    int si = sys_of(ctx, inst, sys);
+    if (si < 0) return seterr(ctx, GC_ERR_ARG, "updaters need a system handle");
+    HSys& s = ctx->inst[inst].sys[si];
+    s.upd.clear();
+    s.upd_set = true;
+    int pos = 0;
+    for (int st = 0; st < nstages; ++st) {
+        if (chain_len[st] > GC_UPD_MAX_CHAIN) return seterr(ctx, GC_ERR_UNSUPPORTED, "updater chain too long");
+        std::vector<HUpd> chain;
+        for (int k = 0; k < chain_len[st]; ++k, ++pos) {
+            HUpd u;
+            u.kind = kinds[pos];
+            for (int q = 0; q < GC_UPD_NPARAM; ++q) u.prm[q] = params[pos * GC_UPD_NPARAM + q];
+            if ((u.kind == GC_UPD_ELASTOPLASTIC || u.kind == GC_UPD_HOOKE) &&
+                !(s.kind == GC_SYS_ELASTOPLASTIC && s.ns == 4))
+                return seterr(ctx, GC_ERR_ARG, "ElastoPlasticStressUpdater requires NS=4 (plane-strain Voigt)");
+            if ((u.kind == GC_UPD_TAIT_EOS || u.kind == GC_UPD_LINEAR_EOS) && s.kind < GC_SYS_FLUID)
+                return seterr(ctx, GC_ERR_ARG, "EOS updater needs a pressure field");
+            if (u.kind < GC_UPD_NONE || u.kind > GC_UPD_HOOKE) return seterr(ctx, GC_ERR_ARG, "bad updater kind");
+            if (u.kind != GC_UPD_NONE) chain.push_back(u);
+        }
+        s.upd.push_back(chain);
+    }
+    return GC_OK;
+}
+
+int gc_set_integrator(gc_ctx* ctx, int inst, double damping_gamma) {
+    if (!ctx) return GC_ERR_ARG;
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
+    ctx->inst[inst].gamma = damping_gamma;
+    return GC_OK;
+}
+
+int gc_finalize(gc_ctx* ctx) {
+    if (!ctx) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    cudaSetDevice(ctx->device);
+    int st = finalize(ctx);
+    if (st) return st;
+    upload_inst_params(ctx, 0.0);
+    for (auto& S : ctx->slots) TRY(push_slot_params(ctx, S));
+    return GC_OK;
+}
+
+// ---------------------------------------------------------------- state I/O
+static int ensure_staging(gc_ctx* ctx, int64_t doubles) {
+    if (doubles > ctx->cap_staging) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, ctx->staging, ctx->cap_staging);
+        int64_t cap = std::max<int64_t>(doubles, 1 << 16);
+        TRY(dalloc(ctx, &ctx->staging, (size_t)cap));
+        ctx->cap_staging = cap;
+    }
+    return GC_OK;
+}
+
+static int ghost_field_io(gc_ctx* ctx, int inst, DGhost& G, int field, void* host, size_t bytes) {
+    const GhostInst* hg = nullptr;
+    std::vector<GhostInst> gh(ninst(ctx));
+    CU(cudaMemcpy(gh.data(), G.d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
+    hg = &gh[inst];
+    const int64_t n = hg->n, base = hg->base;
+    auto get_planar = [&](const double* src, int ncomp, int64_t stride) -> int {
+        if (bytes != (size_t)(n * ncomp * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
+        std::vector<double> tmp((size_t)ncomp * n);
+        for (int c = 0; c < ncomp; ++c)
+            if (n) CU(cudaMemcpy(&tmp[(size_t)c * n], src + c * stride + base, n * 8, cudaMemcpyDeviceToHost));
+        double* out = (double*)host;
+        for (int64_t i = 0; i < n; ++i)
+            for (int c = 0; c < ncomp; ++c) out[i * ncomp + c] = tmp[(size_t)c * n + i];
+        return GC_OK;
+    };
+    auto get_i32 = [&](const int32_t* src) -> int {
+        if (bytes != (size_t)(n * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
+        std::vector<int32_t> tmp(n);
+        if (n) CU(cudaMemcpy(tmp.data(), src + base, n * 4, cudaMemcpyDeviceToHost));
+        int64_t* out = (int64_t*)host;
+        for (int64_t i = 0; i < n; ++i) out[i] = tmp[i];
+        return GC_OK;
+    };
+    switch (field) {
+        case GC_FIELD_X: return get_planar(G.x[G.cur], G.nd, G.CAP);
+        case GC_FIELD_V: return get_planar(G.v, G.nd, G.CAP);
+        case GC_FIELD_RHO: return get_planar(G.rho, 1, G.CAP);
+        case GC_FIELD_NORMALS: return get_planar(G.normals, G.nd, G.CAP);
+        case GC_FIELD_P:
+            if (!G.ex_p) return seterr(ctx, GC_ERR_ARG, "ghost has no p");
+            return get_planar(G.p, 1, G.CAP);
+        case GC_FIELD_STRESS:
+            if (!G.ex_stress) return seterr(ctx, GC_ERR_ARG, "ghost has no stress");
+            return get_planar(G.stress, G.ns, G.CAP);
+        case GC_FIELD_IDX_ORIGINAL: return get_i32(G.io[G.cur]);
+        case GC_FIELD_IDX_BOUNDARY: return get_i32(G.ib[G.cur]);
+    }
+    return seterr(ctx, GC_ERR_ARG, "field not present on ghosts");
+}
+
+struct HandleRef {
+    DSlot* slot = nullptr;
+    DGhost* ghost = nullptr;
+    int sys = -1;
+};
+
+static int resolve(gc_ctx* ctx, int inst, int handle, HandleRef* r) {
+    if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
+    HInst& I = ctx->inst[inst];
+    if (handle < 0 || handle >= (int)I.handles.size()) return seterr(ctx, GC_ERR_ARG, "bad handle");
+    const HHandle& h = I.handles[handle];
+    if (h.type == H_GHOST) r->ghost = &ctx->ghosts[h.idx];
+    else {
+        r->slot = &ctx->slots[h.idx];
+        r->sys = h.idx;
+    }
+    return GC_OK;
+}
+
+int gc_upload_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes) {
+    if (!ctx || !host) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, handle, &r));
+    if (r.ghost) return seterr(ctx, GC_ERR_ARG, "ghost fields are generated on the device");
+    DSlot& S = *r.slot;
+    const HSys& hs = ctx->inst[inst].sys[r.sys];
+    int comps = sys_comps(hs, field);
+    if (comps < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", field);
+    const int64_t n = hs.n, base = S.h_inst[inst].base;
+    if (bytes != (size_t)(n * comps * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
+    if (field == GC_FIELD_V_ADJUSTMENT) {
+        const double* in = (const double*)host;
+        for (int64_t i = 0; i < n * comps; ++i)
+            if (in[i] != 0.0) return seterr(ctx, GC_ERR_UNSUPPORTED, "non-zero v_adjustment (XSPH) is not supported");
+        return GC_OK;
+    }
+    if (field == GC_FIELD_ID) {
+        TRY(ensure_staging(ctx, n));
+        CU(cudaMemcpyAsync(ctx->staging, host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        launch_i64_to_i32((const int64_t*)ctx->staging, S.id[S.cur] + base, n, ctx->stream);
+        CU(cudaStreamSynchronize(ctx->stream));
+        return check_launch(ctx, "upload");
+    }
+    int fs = field_slot(field);
+    const double* in = (const double*)host;
+    bool nz = false;
+    if (field == GC_FIELD_V || field == GC_FIELD_DVDT || field == GC_FIELD_DRHODT)
+        for (int64_t i = 0; i < n * comps && !nz; ++i) nz = in[i] != 0.0;
+    TRY(ensure_staging(ctx, n * comps));
+    CU(cudaMemcpyAsync(ctx->staging, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    launch_aos_to_planar(ctx->staging, S.F(fs), n, comps, S.N, base, ctx->stream);
+    CU(cudaStreamSynchronize(ctx->stream));
+    TRY(check_launch(ctx, "upload"));
+    if (field == GC_FIELD_X) S.sorted_once = false;
+    if (field == GC_FIELD_V || field == GC_FIELD_DVDT || field == GC_FIELD_DRHODT) {
+        int64_t bit = field == GC_FIELD_V ? 1 : field == GC_FIELD_DVDT ? 2 : 4;
+        if (nz) S.nonzero_kin[inst] |= bit;
+        else S.nonzero_kin[inst] &= ~bit;
+    }
+    for (auto& D : ctx->inters) D.grid_valid = false;
+    return GC_OK;
+}
+
+int gc_download_field(gc_ctx* ctx, int inst, int handle, int field, void* host, size_t bytes) {
+    if (!ctx || !host) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, handle, &r));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (r.ghost) return ghost_field_io(ctx, inst, *r.ghost, field, host, bytes);
+    DSlot& S = *r.slot;
+    const HSys& hs = ctx->inst[inst].sys[r.sys];
+    int comps = sys_comps(hs, field);
+    if (comps < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", field);
+    const int64_t n = hs.n, base = S.h_inst[inst].base;
+    if (bytes != (size_t)(n * comps * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
+    if (field == GC_FIELD_V_ADJUSTMENT) {
+        memset(host, 0, bytes);
+        return GC_OK;
+    }
+    if (field == GC_FIELD_ID) {
+        TRY(ensure_staging(ctx, n));
+        launch_i32_to_i64(S.id[S.cur] + base, (int64_t*)ctx->staging, n, ctx->stream);
+        CU(cudaMemcpyAsync(host, ctx->staging, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        return check_launch(ctx, "download");
+    }
+    int fs = field_slot(field);
+    TRY(ensure_staging(ctx, n * comps));
+    launch_planar_to_aos(S.F(fs), ctx->staging, n, comps, S.N, base, ctx->stream);
+    CU(cudaMemcpyAsync(host, ctx->staging, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return check_launch(ctx, "download");
+}
+
+int gc_get_count(gc_ctx* ctx, int inst, int handle, int64_t* n_out) {
+    if (!ctx || !n_out) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, handle, &r));
+    if (r.ghost) {
+        std::vector<GhostInst> gh(ninst(ctx));
+        CU(cudaStreamSynchronize(ctx->stream));
+        CU(cudaMemcpy(gh.data(), r.ghost->d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
+        *n_out = gh[inst].n;
+    } else {
+        *n_out = ctx->inst[inst].sys[r.sys].n;
+    }
+    return GC_OK;
+}
+
+int gc_set_precision(gc_ctx* ctx, int mode) {
+    if (!ctx) return GC_ERR_ARG;
+    if (mode != GC_PRECISION_FP64 && mode != GC_PRECISION_FP32_COMPENSATED)
+        return seterr(ctx, GC_ERR_ARG, "bad precision mode");
+    ctx->precision = mode;
+    return GC_OK;
+}
+
+int gc_step(gc_ctx* ctx, int nsteps, double cfl) {
+    if (!ctx) return GC_ERR_ARG;
+    if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
+    if (nsteps < 0) return seterr(ctx, GC_ERR_ARG, "negative step count");
+    cudaSetDevice(ctx->device);
+    upload_inst_params(ctx, cfl);
+    for (auto& S : ctx->slots) TRY(push_slot_params(ctx, S));
+    decide_motion(ctx);
+    CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    for (int s = 0; s < nsteps; ++s) TRY(one_step(ctx));
+    return finish_status(ctx);
+}
+
+int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
+    if (!ctx || !out) return GC_ERR_ARG;
+    memset(out, 0, sizeof *out);
+    out->steps_done = ctx->steps_done;
+    out->last_status = ctx->last_status;
+    out->kernel_launches = (int64_t)g_launches.load();
+    out->sweep_launches = ctx->sweep_launches;
+    out->sweep_ms = ctx->sweep_ms;
+    if (ctx->finalized && ctx->steps_done > 0) {
+        if (!ctx->d_pairs) TRY(dalloc(ctx, &ctx->d_pairs, 1));
+        int64_t pairs = 0;
+        for (auto& D : ctx->inters) {
+            bool active = false;
+            for (int p : D.pk) active |= p != GC_PFN_NONE;
+            if (!active) continue;
+            CU(cudaMemsetAsync(ctx->d_pairs, 0, 8, ctx->stream));
+            launch_sum_counts(D.counts, ctx->slots[D.a].N, ctx->d_pairs, ctx->stream);
+            unsigned long long v = 0;
+            CU(cudaMemcpyAsync(&v, ctx->d_pairs, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            pairs += D.btype == BT_SELF ? (int64_t)(v / 2) : (int64_t)v;
+        }
+        out->pairs_last_step = pairs;
+    }
+    if (ctx->d_incons) {
+        unsigned long long v = 0;
+        CU(cudaMemcpy(&v, ctx->d_incons, sizeof v, cudaMemcpyDeviceToHost));
+        out->grid_inconsistent = (int64_t)v;
+    }
+    return GC_OK;
+}
+
+// ------------------------------------------------------------- phase hooks
+int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* perm_out) {
+    if (!ctx) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, handle, &r));
+    const int ni = ninst(ctx);
+    CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
+    if (r.ghost) {
+        DGhost& G = *r.ghost;
+        std::vector<SysInst> gi(ni);
+        CU(cudaMemcpy(gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
+        for (auto& g : gi) g.sort_cutoff = cutoff;
+        CU(cudaMemcpy(G.d_inst, gi.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
+        TRY(ghost_bbox_and_plan(ctx, G));
+        TRY(read_need(ctx));
+        TRY(sort_particles_slot(ctx, nullptr, &G, ctx->h_need[G.need_slot]));
+        if (perm_out) {
+            CU(cudaMemcpy(gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
+            const int64_t n = gi[inst].n, base = gi[inst].base;
+            std::vector<int32_t> p(n);
+            if (n) CU(cudaMemcpy(p.data(), ctx->perm + base, n * 4, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < n; ++i) perm_out[i] = p[i] - base + 1;
+        }
+        return finish_status(ctx);
+    }
+    DSlot& S = *r.slot;
+    for (auto& h : S.h_inst) h.sort_cutoff = cutoff;
+    TRY(push_slot_params(ctx, S));
+    TRY(bbox_slot(ctx, S));
+    launch_sort_plan(S.d_inst, ni, S.nd, ctx->d_need + r.sys, ctx->d_err, ctx->stream);
+    TRY(read_need(ctx));
+    TRY(sort_particles_slot(ctx, &S, nullptr, ctx->h_need[r.sys]));
+    if (perm_out) {
+        const int64_t n = S.h_inst[inst].n, base = S.h_inst[inst].base;
+        std::vector<int32_t> p(n);
+        CU(cudaMemcpy(p.data(), ctx->perm + base, n * 4, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; ++i) perm_out[i] = p[i] - base + 1;
+    }
+    for (auto& D : ctx->inters) D.grid_valid = false;
+    return finish_status(ctx);
+}
+
+int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int64_t cap, double* mingridx_out,
+                  int64_t* ngridx_out, int64_t* ncells_out) {
+    if (!ctx) return GC_ERR_ARG;
+    if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
+    if (!valid_inst(ctx, inst) || inter < 0 || inter >= (int)ctx->inters.size())
+        return seterr(ctx, GC_ERR_ARG, "bad interaction");
+    DInter& D = ctx->inters[inter];
+    CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
+    TRY(bbox_slot(ctx, ctx->slots[D.a]));
+    if (D.btype == BT_GHOST) {
+        DGhost& G = ctx->ghosts[D.bghost];
+        launch_bbox(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
+                    ctx->d_err, ctx->stream);
+    } else if (D.btype != BT_SELF) {
+        TRY(bbox_slot(ctx, ctx->slots[D.bslot]));
+    }
+    launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
+    TRY(read_need(ctx));
+    TRY(build_grid(ctx, D, ctx->h_need[D.need_slot]));
+    TRY(finish_status(ctx));
+    std::vector<GridInst> gi(ninst(ctx));
+    CU(cudaMemcpy(gi.data(), D.d_gi, gi.size() * sizeof(GridInst), cudaMemcpyDeviceToHost));
+    const GridInst& G = gi[inst];
+    const int nd = ctx->slots[D.a].nd;
+    if (ncells_out) *ncells_out = G.ncells;
+    if (mingridx_out)
+        for (int d = 0; d < nd; ++d) mingridx_out[d] = G.ming[d];
+    if (ngridx_out)
+        for (int d = 0; d < nd; ++d) ngridx_out[d] = G.ng[d];
+    if (cell_start_out) {
+        if (cap < G.ncells + 1) return seterr(ctx, GC_ERR_CAPACITY, "cell_start buffer too small");
+        std::vector<int32_t> cs(G.ncells + 1);
+        CU(cudaMemcpy(cs.data(), D.cs + G.cellbase, cs.size() * 4, cudaMemcpyDeviceToHost));
+        int64_t bbase;
+        if (D.btype == BT_GHOST) {
+            std::vector<GhostInst> gh(ninst(ctx));
+            CU(cudaMemcpy(gh.data(), ctx->ghosts[D.bghost].d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
+            bbase = gh[inst].base;
+        } else {
+            bbase = ctx->slots[D.bslot].h_inst[inst].base;
+        }
+        for (int64_t c = 0; c <= G.ncells; ++c) cell_start_out[c] = cs[c] - bbase + 1;
+    }
+    return GC_OK;
+}
+
+int gc_generate_ghosts(gc_ctx* ctx, int inst, int ghost) {
+    if (!ctx) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, ghost, &r));
+    if (!r.ghost) return seterr(ctx, GC_ERR_ARG, "not a ghost handle");
+    CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    TRY(generate_ghosts(ctx, *r.ghost));
+    for (auto& D : ctx->inters) D.grid_valid = false;
+    return finish_status(ctx);
+}
+
+int gc_update_ghost_kinematics(gc_ctx* ctx, int inst, int ghost) {
+    if (!ctx) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, ghost, &r));
+    if (!r.ghost) return seterr(ctx, GC_ERR_ARG, "not a ghost handle");
+    TRY(ghost_kinematics(ctx, *r.ghost));
+    return finish_status(ctx);
+}
+
+int gc_update_ghost(gc_ctx* ctx, int inst, int ghost, int stage) {
+    if (!ctx) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, ghost, &r));
+    if (!r.ghost) return seterr(ctx, GC_ERR_ARG, "not a ghost handle");
+    TRY(ghost_copy(ctx, *r.ghost, stage));
+    return finish_status(ctx);
+}
+
+int gc_sweep(gc_ctx* ctx, int inst, int inter, int stage) {
+    if (!ctx) return GC_ERR_ARG;
+    if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
+    if (!valid_inst(ctx, inst) || inter < 0 || inter >= (int)ctx->inters.size())
+        return seterr(ctx, GC_ERR_ARG, "bad interaction");
+    DInter& D = ctx->inters[inter];
+    if (stage < 1 || stage > D.nstages || D.pk[stage - 1] == GC_PFN_NONE) return GC_OK;
+    CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    TRY(sweep_group(ctx, D.a, std::vector<int>{inter}, stage, false));
+    return finish_status(ctx);
+}
+
+int gc_update_state(gc_ctx* ctx, int inst, int sys, int stage, double dt) {
+    if (!ctx) return GC_ERR_ARG;
+    HandleRef r;
+    TRY(resolve(ctx, inst, sys, &r));
+    if (!r.slot) return seterr(ctx, GC_ERR_ARG, "not a system handle");
+    TRY(run_updaters(ctx, *r.slot, stage, dt));
+    return finish_status(ctx);
+}
+
+int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, int64_t n) {
+    if (!ctx || !counts_out) return GC_ERR_ARG;
+    if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
+    if (!valid_inst(ctx, inst) || inter < 0 || inter >= (int)ctx->inters.size())
+        return seterr(ctx, GC_ERR_ARG, "bad interaction");
+    DInter& D = ctx->inters[inter];
+    DSlot& S = ctx->slots[D.a];
+    if (n != S.h_inst[inst].n) return seterr(ctx, GC_ERR_ARG, "count buffer length mismatch");
+    // A counting sweep: the first non-`nothing` stage's functor kind decides
+    // the launch; counts do not depend on it.
+    int stage = 1;
+    for (int s = 1; s <= D.nstages; ++s)
+        if (D.pk[s - 1] != GC_PFN_NONE) {
+            stage = s;
+            break;
+        }
+    std::vector<int> ids{inter};
+    std::vector<int> saved = D.pk;
+    for (auto& p : D.pk) p = GC_PFN_COUNT;
+    int st = sweep_group(ctx, D.a, ids, stage, true);
+    D.pk = saved;
+    TRY(st);
+    TRY(finish_status(ctx));
+    CU(cudaMemcpy(counts_out, D.counts + S.h_inst[inst].base, n * 4, cudaMemcpyDeviceToHost));
+    return GC_OK;
+}
+
+int gc_stream(gc_ctx* ctx, void** stream_out) {
+    if (!ctx || !stream_out) return GC_ERR_ARG;
+    *stream_out = (void*)ctx->stream;
+    return GC_OK;
+}
+
+int gc_set_profiling(gc_ctx* ctx, int on) {
+    if (!ctx) return GC_ERR_ARG;
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->ev_used = 0;
+    ctx->profiling = on != 0;
+    ctx->sweep_ms = 0;
+    ctx->sweep_launches = 0;
+    return GC_OK;
+}
+
+int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out) {
+    if (!ctx || !tflops_out) return GC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    double* out = nullptr;
+    TRY(dalloc(ctx, &out, 1));
+    const int threads = 256, blocks = sms * 8, iters = 1 << 16;
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    launch_fp64_peak(out, blocks, threads, 1024, ctx->stream);  // warm-up
+    CU(cudaEventRecord(a, ctx->stream));
+    launch_fp64_peak(out, blocks, threads, iters, ctx->stream);
+    CU(cudaEventRecord(b, ctx->stream));
+    CU(cudaEventSynchronize(b));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    dfree(ctx, out, 1);
+    double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+    *tflops_out = flops / (ms * 1e-3) / 1e12;
+    return GC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// gc_force.h — arguments of the fused pair-sweep kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gc_internal.h"
+
+namespace gc {
+
+constexpr int FORCE_TPB = 128;  // threads per block of the sweep
+constexpr int FORCE_BUF = 32;   // staged neighbours per thread (shared memory)
+constexpr int MAX_REFS = 8;     // interactions fused into one launch
+
+// system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)
+enum { BT_SELF = 0, BT_DYNAMIC = 1, BT_STATIC = 2, BT_GHOST = 3, BT_SYSTEM = 4 };
+
+// per-particle divisor caches (one per slot, refreshed before each sweep)
+enum { AUX_P_OVER_RHO2 = 0, AUX_INV_RHO2 = 1, AUX_MASS_OVER_RHO = 2 };
+
+struct InterRef {
+    int btype;
+    const GridInst* gi;   // per instance
+    const PfnInst* pi;    // per instance, this stage
+    const int32_t* cs;    // packed CSR over system_b (global b indices)
+    const double *bx, *bv, *brho, *bp, *bstress, *baux;
+    int64_t bN;           // planar stride of system_b's arrays
+    int32_t* counts;      // optional per-particle accepted-pair counts
+};
+
+struct ForceArgs {
+    int nd, ns, pfn, kk;
+    int64_t aN;
+    const int32_t* a_inst_of;
+    const double *ax, *av, *arho, *aaux, *astress, *a_p;
+    double *advdt, *adrhodt, *asr, *avort;
+    const double* a_c;     // per-instance sound speed
+    const double* a_mass;  // per-instance particle mass
+    int* err;
+    int nref;
+    InterRef ref[MAX_REFS];
+};
+
+int launch_force_f64(const ForceArgs& A, bool count_only, cudaStream_t s);
+void launch_aux(int mode, int64_t N, const int64_t* count, const double* rho, const double* p,
+                const int32_t* inst_of, const double* mass, double* aux, cudaStream_t s);
+
+}  // namespace gc

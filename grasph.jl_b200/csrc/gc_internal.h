@@ -1,0 +1,103 @@
+// gc_internal.h — device-visible parameter structs and kernel launchers
+// shared by the translation units of libgrasph_cuda.so.
+//
+// Layout in HBM: every system slot (one Grasph particle system, repeated
+// across all instances of a context) is packed instance after instance.
+// Per-particle fields are stored component-planar ("SoA"): component c of
+// packed particle g lives at field[c*N + g], N = packed count of the slot.
+// Particle indices are int32 (a context holds < 2^31 particles per slot).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/grasph_cuda.h"
+
+namespace gc {
+
+constexpr int MAXD = 3;   // spatial dimensions
+constexpr int MAXS = 6;   // Voigt components
+constexpr int MAX_STAGES = 8;
+constexpr int MAX_INTER_PER_SYS = 16;
+
+// Device error word bits (OR-ed by kernels, read by the host).
+enum : int {
+    ERR_NONFINITE = 1,      // NaN/Inf or out-of-range position in a key/cell
+    ERR_CAPACITY = 2,       // a cell or ghost index beyond its buffer
+    ERR_GRID_INCONS = 4,    // key order vs cell order disagreement (warning)
+    ERR_TIMEOUT = 8
+};
+
+// Per (system slot, instance) parameters; packed range [base, base+n).
+struct SysInst {
+    int64_t base, n;
+    double mass, c, srcv[MAXD], srcrho;
+    double sort_cutoff;  // 2·h_min of the instance (src/TimeIntegration.jl:612)
+    double dt, half_dt, gamma_dt;
+    // Written on the device each step:
+    double bbmin[MAXD], bbmax[MAXD];  // bounding box (NaN-propagating min/max)
+    int64_t kmin[MAXD], kext[MAXD];   // sort-key lattice box
+    int64_t sort_cellbase, sort_ncells;
+};
+
+// Per (interaction, instance) grid and system_b parameters.
+struct GridInst {
+    double H, cell, cutoff_sq, knorm;  // h, 2h, (2h)^2, kernel normalisation
+    double ming[MAXD];                 // grid origin (src/Interaction.jl:143)
+    int64_t ng[MAXD];                  // cells per dimension (:179)
+    int64_t ncells, cellbase;          // this instance's cells in the packed grid
+    double mina[MAXD], maxa[MAXD];     // system_a bounding box (coupled)
+    // system_b wrapper parameters (src/BoundaryParticles.jl)
+    double normal[MAXD], point[MAXD], beta, ljcut;
+    double bmass, bc;                  // system_b mass and sound speed
+};
+
+// Per (interaction, stage, instance) functor parameters.
+struct PfnInst {
+    double alpha, beta, h, delta;
+    int S, has_delta;
+};
+
+// Per (ghost entry, instance) parameters.
+struct GhostInst {
+    double normals[4][MAXD], points[4][MAXD];  // up to 4 planes
+    double cutoff;
+    int64_t src_base, src_n;   // source particles in the source slot
+    int64_t cap_base, cap;     // capacity range in the packed ghost arrays
+    int64_t base, n;           // current ghosts (written on the device)
+    double mass, c;
+};
+
+// One per-particle field: ncomp planar components with stride N.
+struct Field {
+    double* p;
+    int ncomp;
+};
+
+// Device pointers of one system slot (current buffers).
+struct SlotPtrs {
+    int64_t N;           // packed particle count (capacity for ghosts)
+    int nd, ns, nvort, kind;
+    double *x, *v, *rho, *dvdt, *drhodt, *p, *stress, *sr, *vort, *strain, *strainp, *vadj;
+    double *q0v, *q0rho;
+    int32_t* id;         // 1-based reference id
+    int32_t* inst_of;    // instance of each packed particle
+    SysInst* inst;       // per-instance parameters
+    // ghosts only
+    int32_t *io, *ib;    // 1-based source index / plane index
+    double* normals;     // generation-order normals
+    const int64_t* count;  // device count (ghosts) or nullptr
+};
+
+// Updater descriptor (per system, stage, chain position, instance).
+struct UpdInst {
+    int kind;
+    double prm[GC_UPD_NPARAM];
+    // precomputed on the host with the reference's expressions
+    double pre;        // Tait: rho0*c*c/gamma
+    int gamma_int;     // Tait: gamma is an integer that fits
+    double D0, omn, om2n, a_phi, k_c, a_psi, apex_thr, apex;  // EP / Hooke
+    uint32_t zmask;
+};
+
+}  // namespace gc

@@ -1,0 +1,94 @@
+// gc_kernels.h — host-callable launchers of the device kernels.
+#pragma once
+
+#include <atomic>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gc_internal.h"
+
+namespace gc {
+
+// ---------------------------------------------------------------- scan
+// Exclusive prefix sum of n int32 counts into out[0..n] (out[n] = total).
+// `tmp` must hold scan_tmp_elems(n) int32.
+int64_t scan_tmp_elems(int64_t n);
+void scan_exclusive(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s);
+
+// ---------------------------------------------------------- bounding box
+// Per-instance min/max of a slot's positions into inst[k].bbmin/bbmax.
+// `count` (nullable) bounds the packed range for ghost slots.
+void launch_bbox_reset(SysInst* inst, int ninst, cudaStream_t s);
+void launch_bbox(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count, SysInst* inst,
+                 unsigned long long* scratch, int ninst, int* err, cudaStream_t s);
+
+// ------------------------------------------------------------------ sort
+// Per-instance key lattice from the bbox; writes total cells to *need.
+void launch_sort_plan(SysInst* inst, int ninst, int nd, int64_t* need, int* err, cudaStream_t s);
+// Flat sort key per particle + histogram.
+void launch_sort_keys(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
+                      const SysInst* inst, int32_t* key, int32_t* hist, int64_t cells_cap, int* err, cudaStream_t s);
+void launch_sort_scatter(const int32_t* key, int64_t N, const int64_t* count, const int32_t* start, int32_t* fill,
+                         int32_t* perm, cudaStream_t s);
+void launch_sort_fixup(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
+                       cudaStream_t s);
+void launch_gather(const double* src, double* dst, int ncomp, int64_t N, const int32_t* perm, const int64_t* count,
+                   cudaStream_t s);
+void launch_gather_i32(const int32_t* src, int32_t* dst, int64_t N, const int32_t* perm, const int64_t* count,
+                       cudaStream_t s);
+
+// ------------------------------------------------------------------ grid
+struct GridPlanArgs {
+    GridInst* gi;
+    int ninst, nd;
+    const SysInst* a;      // system_a per-instance bbox
+    const SysInst* b;      // system_b per-instance bbox (nullptr for self)
+    const int64_t* bn;     // ghost-b counts per instance (nullptr otherwise)
+    int64_t* need;         // total cells
+    int* err;
+};
+void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s);
+// cell histogram of the particles of one slot on an interaction's grid.
+void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
+                       const GridInst* gi, int32_t* hist, int64_t cells_cap, int* err,
+                       unsigned long long* incons, cudaStream_t s);
+
+// ---------------------------------------------------------------- ghosts
+struct GhostGenArgs {
+    const double* src_x;   // source slot positions
+    int64_t Nsrc;
+    const int32_t* src_inst_of;
+    GhostInst* gh;
+    int ninst, nd, nplanes;
+    int32_t* flags;        // nplanes*Nsrc
+    int32_t* pos;          // nplanes*Nsrc + 1
+    // raw (generation-order) ghost arrays, capacity nplanes*Nsrc
+    double* gx;
+    int32_t *gio, *gib, *ginst;
+    double* gnormals;
+    int64_t* count;        // total ghosts (device)
+    SysInst* ginst_params; // ghost sort parameters per instance
+};
+void launch_ghost_flags(const GhostGenArgs& a, cudaStream_t s);
+void launch_ghost_fill(const GhostGenArgs& a, cudaStream_t s);
+void launch_ghost_kinematics(int64_t cap, const int64_t* count, int nd, const int32_t* io, const int32_t* ginst,
+                             const double* normals, const GhostInst* gh, const double* src_v, const double* src_rho,
+                             int64_t Nsrc, double* gv, double* grho, cudaStream_t s);
+void launch_ghost_copy(int64_t cap, const int64_t* count, int nd, int ns, const int32_t* io, const int32_t* ginst,
+                       const double* normals, const GhostInst* gh, int field, int mode, const double* src,
+                       int64_t Nsrc, double* dst, cudaStream_t s);
+
+// --------------------------------------------------------------- host I/O
+void launch_aos_to_planar(const double* src, double* dst, int64_t n, int comps, int64_t N, int64_t base,
+                          cudaStream_t s);
+void launch_planar_to_aos(const double* src, double* dst, int64_t n, int comps, int64_t N, int64_t base,
+                          cudaStream_t s);
+void launch_i64_to_i32(const int64_t* src, int32_t* dst, int64_t n, cudaStream_t s);
+void launch_i32_to_i64(const int32_t* src, int64_t* dst, int64_t n, cudaStream_t s);
+
+// ------------------------------------------------------------ measurement
+void launch_sum_counts(const int32_t* c, int64_t n, unsigned long long* out, cudaStream_t s);
+void launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStream_t s);
+extern std::atomic<long long> g_launches;
+
+}  // namespace gc

@@ -1,0 +1,212 @@
+// k_update.cu — leapfrog half/full step and per-particle state updaters.
+//
+// Rounding follows the reference: `@fastmath` axpy on scalar fields
+// (src/Utils.jl:19-29) is a fused multiply-add; on SVector fields the
+// FastMath operators fall back to plain `*` and `+`, two roundings.
+// Compiled with -fmad=false; fused operations are explicit fma().
+#include "gc_device.cuh"
+#include "gc_kernels.h"
+#include "gc_update.h"
+
+namespace gc {
+
+constexpr int UTPB = 256;
+
+static inline int ublk(int64_t n) {
+    int64_t b = (n + UTPB - 1) / UTPB;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// src/TimeIntegration.jl:158 (_halfstep_ps!) with the q0 snapshot of :220.
+__global__ void k_halfstep(StepArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const SysInst& S = a.inst[a.inst_of[g]];
+        const double h = S.half_dt;
+        for (int d = 0; d < a.nd; ++d) {
+            double v = a.v[d * a.N + g];
+            a.q0v[d * a.N + g] = v;
+            a.v[d * a.N + g] = v + h * a.dvdt[d * a.N + g];
+            a.dvdt[d * a.N + g] = S.srcv[d];
+        }
+        double r = a.rho[g];
+        a.q0rho[g] = r;
+        a.rho[g] = fma(h, a.drhodt[g], r);
+        a.drhodt[g] = S.srcrho;
+    }
+}
+
+// src/TimeIntegration.jl:673-682: damping, full step, zero XSPH pass, x += dt·v.
+__global__ void k_fullstep(StepArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const SysInst& S = a.inst[a.inst_of[g]];
+        const double dt = S.dt;
+        for (int d = 0; d < a.nd; ++d) {
+            double dv = a.dvdt[d * a.N + g];
+            if (S.gamma_dt != 0.0) {
+                dv = dv - S.gamma_dt * a.v[d * a.N + g];
+                a.dvdt[d * a.N + g] = dv;
+            }
+            double v = a.q0v[d * a.N + g] + dt * dv;
+            v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
+            a.v[d * a.N + g] = v;
+            a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
+        }
+        a.rho[g] = fma(dt, a.drhodt[g], a.q0rho[g]);
+    }
+}
+
+void launch_halfstep(const StepArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_halfstep<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+void launch_fullstep(const StepArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_fullstep<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+
+// ------------------------------------------------------------- updaters
+// src/StateUpdaters.jl:202-335 (ElastoPlasticStressUpdater, NS = 4)
+__device__ __forceinline__ void ep_update(const UpdInst& u, double dt, double* s, const double* er, double w,
+                                          double* e, double* ep) {
+    const double nu = u.prm[1];
+    const double D0 = u.D0, omn = u.omn, om2n = u.om2n;
+    double sxx = s[0], syy = s[1], szz = s[2], sxy = s[3];
+    double dexx = er[0] * dt, deyy = er[1] * dt, dezz = er[2] * dt, dexy = er[3] * dt;
+    double dsxx = D0 * (omn * dexx + nu * deyy + nu * dezz);
+    double dsyy = D0 * (nu * dexx + omn * deyy + nu * dezz);
+    double dszz = D0 * (nu * dexx + nu * deyy + omn * dezz);
+    double dsxy = D0 * om2n * dexy;
+    double wdt = w * dt;
+    dsxx = dsxx - 2.0 * sxy * wdt;
+    dsyy = dsyy + 2.0 * sxy * wdt;
+    dsxy = dsxy + (sxx - syy) * wdt;
+    double txx = sxx + dsxx, tyy = syy + dsyy, tzz = szz + dszz, txy = sxy + dsxy;
+    double I1 = txx + tyy + tzz;
+    double p3 = I1 / 3.0;
+    double s_xx = txx - p3, s_yy = tyy - p3, s_zz = tzz - p3, s_xy = txy;
+    double J2 = 0.5 * (s_xx * s_xx + s_yy * s_yy + s_zz * s_zz + 2.0 * (s_xy * s_xy));
+    double sqJ2 = sqrt(J2);
+    double f = u.a_phi * I1 + sqJ2 - u.k_c;
+    double depxx = 0.0, depyy = 0.0, depzz = 0.0, depxy = 0.0;
+    if (f > 0.0) {
+        double inv2 = 1.0 / (2.0 * sqJ2);
+        double dfxx = u.a_phi + s_xx * inv2, dfyy = u.a_phi + s_yy * inv2, dfzz = u.a_phi + s_zz * inv2;
+        double dfxy = s_xy * inv2;
+        double dgxx = u.a_psi + s_xx * inv2, dgyy = u.a_psi + s_yy * inv2, dgzz = u.a_psi + s_zz * inv2;
+        double dgxy = s_xy * inv2;
+        double Dxx = D0 * (omn * dgxx + nu * dgyy + nu * dgzz);
+        double Dyy = D0 * (nu * dgxx + omn * dgyy + nu * dgzz);
+        double Dzz = D0 * (nu * dgxx + nu * dgyy + omn * dgzz);
+        double Dxy = D0 * om2n * dgxy;
+        double denom = dfxx * Dxx + dfyy * Dyy + dfzz * Dzz + 2.0 * dfxy * Dxy;
+        double dl = f / denom;
+        depxx = dl * dgxx;
+        depyy = dl * dgyy;
+        depzz = dl * dgzz;
+        depxy = dl * dgxy;
+        dsxx = dsxx - D0 * (omn * depxx + nu * depyy + nu * depzz);
+        dsyy = dsyy - D0 * (nu * depxx + omn * depyy + nu * depzz);
+        dszz = dszz - D0 * (nu * depxx + nu * depyy + omn * depzz);
+        dsxy = dsxy - D0 * om2n * depxy;
+    }
+    s[0] = sxx + dsxx;
+    s[1] = syy + dsyy;
+    s[2] = szz + dszz;
+    s[3] = sxy + dsxy;
+    if (sxx + dsxx + syy + dsyy + szz + dszz > u.apex_thr) {
+        s[0] = u.apex;
+        s[1] = u.apex;
+        s[2] = u.apex;
+        s[3] = 0.0;
+    }
+    e[0] = e[0] + dexx;
+    e[1] = e[1] + deyy;
+    e[2] = e[2] + dezz;
+    e[3] = e[3] + dexy;
+    ep[0] = ep[0] + depxx;
+    ep[1] = ep[1] + depyy;
+    ep[2] = ep[2] + depzz;
+    ep[3] = ep[3] + depxy;
+}
+
+__global__ void k_update(UpdArgs a) {
+    const int64_t N = a.N;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
+        const int k = a.inst_of[g];
+        const UpdInst& u = a.u[k];
+        const double dt = isnan(a.dt) ? a.inst[k].dt : a.dt;
+        switch (u.kind) {
+            case GC_UPD_ZERO_FIELDS:
+                if ((u.zmask >> GC_FIELD_STRAIN_RATE) & 1u)
+                    for (int q = 0; q < a.ns; ++q) a.sr[q * N + g] = 0.0;
+                if ((u.zmask >> GC_FIELD_VORTICITY) & 1u)
+                    for (int q = 0; q < a.nvort; ++q) a.vort[q * N + g] = 0.0;
+                if ((u.zmask >> GC_FIELD_P) & 1u) a.p[g] = 0.0;
+                if ((u.zmask >> GC_FIELD_STRESS) & 1u)
+                    for (int q = 0; q < a.ns; ++q) a.stress[q * N + g] = 0.0;
+                if ((u.zmask >> GC_FIELD_DVDT) & 1u)
+                    for (int d = 0; d < a.nd; ++d) a.dvdt[d * N + g] = 0.0;
+                if ((u.zmask >> GC_FIELD_DRHODT) & 1u) a.drhodt[g] = 0.0;
+                break;
+            case GC_UPD_TAIT_EOS: {
+                // src/StateUpdaters.jl:114-118
+                double ratio = a.rho[g] / u.prm[0];
+                double pw = u.gamma_int ? comp_powi(ratio, (int64_t)u.prm[1]) : pow(ratio, u.prm[1]);
+                a.p[g] = u.pre * (pw - 1.0);
+                break;
+            }
+            case GC_UPD_LINEAR_EOS: {
+                double c = a.inst[k].c;
+                a.p[g] = c * c * (a.rho[g] - u.prm[0]);
+                break;
+            }
+            case GC_UPD_ELASTOPLASTIC: {
+                double s[4], er[4], e[4], ep[4];
+                for (int q = 0; q < 4; ++q) {
+                    s[q] = a.stress[q * N + g];
+                    er[q] = a.sr[q * N + g];
+                    e[q] = a.strain[q * N + g];
+                    ep[q] = a.strainp[q * N + g];
+                }
+                ep_update(u, dt, s, er, a.vort[g], e, ep);
+                for (int q = 0; q < 4; ++q) {
+                    a.stress[q * N + g] = s[q];
+                    a.strain[q * N + g] = e[q];
+                    a.strainp[q * N + g] = ep[q];
+                }
+                break;
+            }
+            case GC_UPD_HOOKE: {
+                // src/StateUpdaters.jl:366-405
+                const double nu = u.prm[1], D0 = u.D0, omn = u.omn, om2n = u.om2n;
+                double sxx = a.stress[g], syy = a.stress[N + g], szz = a.stress[2 * N + g], sxy = a.stress[3 * N + g];
+                double dexx = a.sr[g] * dt, deyy = a.sr[N + g] * dt, dezz = a.sr[2 * N + g] * dt,
+                       dexy = a.sr[3 * N + g] * dt;
+                double dsxx = D0 * (omn * dexx + nu * deyy + nu * dezz);
+                double dsyy = D0 * (nu * dexx + omn * deyy + nu * dezz);
+                double dszz = D0 * (nu * dexx + nu * deyy + omn * dezz);
+                double dsxy = D0 * om2n * dexy;
+                double wdt = a.vort[g] * dt;
+                dsxx = dsxx - 2.0 * sxy * wdt;
+                dsyy = dsyy + 2.0 * sxy * wdt;
+                dsxy = dsxy + (sxx - syy) * wdt;
+                double nxx = sxx + dsxx, nyy = syy + dsyy, nzz = szz + dszz, nxy = sxy + dsxy;
+                a.stress[g] = nxx;
+                a.stress[N + g] = nyy;
+                a.stress[2 * N + g] = nzz;
+                a.stress[3 * N + g] = nxy;
+                a.p[g] = -(nxx + nyy + nzz) / 3.0;
+                break;
+            }
+            default:
+                break;
+        }
+    }
+}
+
+void launch_update(const UpdArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_update<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+
+}  // namespace gc

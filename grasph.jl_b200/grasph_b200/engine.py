@@ -42,7 +42,8 @@ class GcError(RuntimeError):
 
 class GcStats(ct.Structure):
     _fields_ = [("steps_done", ct.c_int64), ("pairs_last_step", ct.c_int64),
-                ("grid_inconsistent", ct.c_int64), ("resorts", ct.c_int64),
+                ("grid_inconsistent", ct.c_int64), ("kernel_launches", ct.c_int64),
+                ("sweep_launches", ct.c_int64), ("sweep_ms", ct.c_double),
                 ("last_status", ct.c_int32), ("pad", ct.c_int32)]
 
 
@@ -88,6 +89,9 @@ def load_library(path: os.PathLike | None = None):
         "gc_sweep": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int]),
         "gc_update_state": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_double]),
         "gc_neighbor_counts": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _i32p, ct.c_int64]),
+        "gc_stream": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_void_p)]),
+        "gc_set_profiling": (ct.c_int, [ct.c_void_p, ct.c_int]),
+        "gc_measure_fp64_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -129,9 +129,12 @@ typedef struct gc_ctx gc_ctx;
 
 typedef struct gc_stats {
     int64_t steps_done;          /* leapfrog steps completed in this context      */
-    int64_t pairs_last_step;     /* accepted pairs of the last step, all stages   */
+    int64_t pairs_last_step;     /* accepted pairs of the last step, one stage:
+                                    unordered self pairs + coupled (a,b) pairs   */
     int64_t grid_inconsistent;   /* cells where key order and cell order disagreed */
-    int64_t resorts;             /* steps whose sort took the slow (permuting) path */
+    int64_t kernel_launches;     /* device kernels launched by this context       */
+    int64_t sweep_launches;      /* pair-sweep launches timed (profiling on)      */
+    double sweep_ms;             /* summed device time of those launches          */
     int32_t last_status;         /* device error word of the last step            */
     int32_t pad;
 } gc_stats;
@@ -213,6 +216,18 @@ int gc_set_precision(gc_ctx* ctx, int mode);
 int gc_step(gc_ctx* ctx, int nsteps, double cfl);
 
 int gc_get_stats(gc_ctx* ctx, gc_stats* out);
+
+/* ======================================================== measurement */
+/* The CUDA stream every kernel of the context is launched on (a
+ * cudaStream_t), for callers that time work with CUDA events.            */
+int gc_stream(gc_ctx* ctx, void** stream_out);
+/* When on, every pair-sweep launch is bracketed by CUDA events on the
+ * context's stream; gc_get_stats reports their summed time.  Resets the
+ * sweep counters.                                                         */
+int gc_set_profiling(gc_ctx* ctx, int on);
+/* Measured FP64 FMA issue rate of the device in TFLOP/s (2 flops per FMA):
+ * the compute ceiling of the FP64 pair sweep.                             */
+int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out);
 
 /* ======================================================== phase hooks */
 /* The same device kernels, one reference phase at a time (parity tests and
