@@ -1,0 +1,233 @@
+# GrasphCUDA.jl — Julia binding of libgrasph_cuda.so for Grasph.jl.
+#
+# Adds a device-backed method of `time_integrate!` for a
+# `LeapFrogTimeIntegrator` whose systems, functors and updaters are of the
+# kinds the library implements, plus per-phase entry points.  Host arrays stay
+# the source of truth between calls: they are uploaded when a call starts and
+# written back when it ends.  Unsupported combinations raise ArgumentError;
+# there is no CPU fallback inside this module (call Grasph's own method).
+#
+# Load after Grasph:   using Grasph; include("GrasphCUDA.jl"); using .GrasphCUDA
+module GrasphCUDA
+
+using Grasph
+using StaticArrays
+
+const LIB = get(ENV, "GRASPH_CUDA_LIB", joinpath(@__DIR__, "..", "libgrasph_cuda.so"))
+
+# Constants of include/grasph_cuda.h
+const GC_SYS = Dict(BasicParticleSystem => 0, FluidParticleSystem => 1,
+                    StressParticleSystem => 2, ElastoPlasticParticleSystem => 3)
+const GC_FIELD = (x=0, v=1, rho=2, dvdt=3, drhodt=4, p=5, stress=6, strain_rate=7,
+                  vorticity=8, strain=9, strain_p=10, id=11)
+const GC_WRAP_DYNAMIC = 1
+const GC_WRAP_STATIC = 2
+const GC_PFN_NPARAM = 6
+const GC_UPD_NPARAM = 6
+
+struct GcError <: Exception
+    status::Cint
+    msg::String
+end
+
+function check(ctx, st)
+    st == 0 && return nothing
+    msg = ctx == C_NULL ? "" : unsafe_string(ccall((:gc_last_error, LIB), Cstring, (Ptr{Cvoid},), ctx))
+    st == 1 && throw(ArgumentError(msg))
+    throw(GcError(st, msg))
+end
+
+pfn_kind(::Nothing) = 0
+pfn_kind(::FluidPfn) = 1
+pfn_kind(::CauchyFluidPfn) = 2
+pfn_kind(::StrainRatePfn) = 3
+pfn_kind(::StrainRateVorticityPfn) = 4
+pfn_kind(f) = throw(ArgumentError("pairwise functor $(typeof(f)) has no device implementation"))
+
+function pfn_params(f)
+    p = [0.0, 0.0, 0.0, 2.0, NaN, NaN]
+    f === nothing && return p
+    if f isa FluidPfn || f isa CauchyFluidPfn
+        p[1] = f.art_visc_alpha; p[2] = f.art_visc_beta; p[3] = f.h
+        f.delta === nothing || (p[5] = f.delta)
+    end
+    f isa FluidPfn && (p[4] = typeof(f).parameters[1])
+    return p
+end
+
+upd_entry(u::ZeroFieldUpdater{S}) where {S} =
+    (1, [Float64(reduce(|, (1 << GC_FIELD[s] for s in S); init=0)), 0, 0, 0, 0, 0])
+upd_entry(u::TaitEOSUpdater) = (2, [u.rho0, u.gamma, 0, 0, 0, 0])
+upd_entry(u::LinearEOSUpdater) = (3, [u.rho0, 0, 0, 0, 0, 0])
+upd_entry(u::ElastoPlasticStressUpdater) = (4, [u.E, u.nu, u.phi, u.psi, u.cohesion, 0])
+upd_entry(u::HookeLawStressUpdater) = (5, [u.E, u.nu, 0, 0, 0, 0])
+upd_entry(u) = throw(ArgumentError("state updater $(typeof(u)) has no device implementation"))
+
+fields_of(ps) = [f for f in (:x, :v, :rho, :dvdt, :drhodt, :p, :stress, :strain_rate, :vorticity,
+                               :strain, :strain_p) if hasfield(typeof(ps), f)]
+
+"""
+    CudaLeapFrog(lf::LeapFrogTimeIntegrator; device=0)
+
+A device context holding the model of `lf` (one instance).
+"""
+mutable struct CudaLeapFrog
+    ctx::Ptr{Cvoid}
+    lf::LeapFrogTimeIntegrator
+    handles::IdDict{Any,Cint}
+    inters::Vector{Cint}
+end
+
+function CudaLeapFrog(lf::LeapFrogTimeIntegrator; device::Integer=0)
+    ctx = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:gc_ctx_create, LIB), Cint, (Cint, Csize_t, Ref{Ptr{Cvoid}}), device, 0, ctx))
+    inst = Ref{Cint}(0)
+    check(ctx[], ccall((:gc_instance_add, LIB), Cint, (Ptr{Cvoid}, Ref{Cint}), ctx[], inst))
+    h = IdDict{Any,Cint}()
+    for ps in lf.systems
+        out = Ref{Cint}(0)
+        ns = hasfield(typeof(ps), :stress) ? length(eltype(ps.stress)) : 0
+        check(ctx[], ccall((:gc_add_system, LIB), Cint,
+                           (Ptr{Cvoid}, Cint, Cint, Int64, Cint, Cint, Cdouble, Cdouble, Ptr{Cdouble}, Cdouble, Ref{Cint}),
+                           ctx[], inst[], GC_SYS[typeof(ps).name.wrapper], ps.n, ps.ndims, ns, ps.mass, ps.c,
+                           Vector{Float64}(ps.source_v), ps.source_rho, out))
+        h[ps] = out[]
+    end
+    for ge in lf.ghosts
+        g = ge.ghost
+        nf = Cint[]; flds = Cint[]; mds = Cint[]
+        for u in g.updaters
+            if u === nothing
+                push!(nf, 0)
+            else
+                fs, ms = typeof(u).parameters
+                push!(nf, length(fs))
+                for (f, m) in zip(fs, ms)
+                    push!(flds, GC_FIELD[f]); push!(mds, m === nothing ? 0 : 1)
+                end
+            end
+        end
+        normals = reduce(vcat, [Vector(b.normal) for b in ge.boundaries])
+        points = reduce(vcat, [Vector(b.point) for b in ge.boundaries])
+        out = Ref{Cint}(0)
+        check(ctx[], ccall((:gc_add_ghost, LIB), Cint,
+                           (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cint}, Ptr{Cint}, Ptr{Cint}, Cint, Ptr{Cdouble},
+                            Ptr{Cdouble}, Cdouble, Int64, Ref{Cint}),
+                           ctx[], inst[], h[g.source], length(nf), nf, flds, mds, length(ge.boundaries),
+                           normals, points, ge.cutoff, 0, out))
+        h[g] = out[]
+    end
+    ints = Cint[]
+    for si in lf.interactions
+        b = si.system_b
+        bh = Cint(-1)
+        if b isa DynamicBoundarySystem || b isa StaticBoundarySystem
+            if !haskey(h, b)
+                out = Ref{Cint}(0)
+                inner = getfield(b, :inner)
+                if b isa DynamicBoundarySystem
+                    check(ctx[], ccall((:gc_add_boundary, LIB), Cint,
+                                       (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Cdouble, Ref{Cint}),
+                                       ctx[], inst[], h[inner], GC_WRAP_DYNAMIC, Vector(b.boundary_normal),
+                                       Vector(b.boundary_point), b.boundary_beta, out))
+                else
+                    z = zeros(ps_ndims(inner))
+                    check(ctx[], ccall((:gc_add_boundary, LIB), Cint,
+                                       (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Cdouble, Ref{Cint}),
+                                       ctx[], inst[], h[inner], GC_WRAP_STATIC, z, z, b.lj_cutoff, out))
+                end
+                h[b] = out[]
+            end
+            bh = h[b]
+        elseif b !== nothing
+            bh = h[b]
+        end
+        kinds = Cint[pfn_kind(f) for f in si.pfns]
+        prm = reduce(vcat, [pfn_params(f) for f in si.pfns])
+        kk = si.kernel isa CubicSplineKernel ? 0 : 1
+        out = Ref{Cint}(0)
+        check(ctx[], ccall((:gc_add_interaction, LIB), Cint,
+                           (Ptr{Cvoid}, Cint, Cint, Cint, Cint, Cdouble, Cint, Ptr{Cint}, Ptr{Cdouble}, Ref{Cint}),
+                           ctx[], inst[], h[si.system_a], bh, kk, si.kernel.h, length(kinds), kinds, prm, out))
+        push!(ints, out[])
+    end
+    for ps in lf.systems
+        isempty(ps.state_updater) && continue
+        lens = Cint[]; kinds = Cint[]; prm = Float64[]
+        for entry in ps.state_updater
+            chain = entry === nothing ? () : (entry isa Tuple ? entry : (entry,))
+            push!(lens, length(chain))
+            for u in chain
+                k, p = upd_entry(u)
+                push!(kinds, k); append!(prm, p)
+            end
+        end
+        check(ctx[], ccall((:gc_set_updaters, LIB), Cint,
+                           (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cint}, Ptr{Cint}, Ptr{Cdouble}),
+                           ctx[], inst[], h[ps], length(lens), lens, kinds, prm))
+    end
+    check(ctx[], ccall((:gc_set_integrator, LIB), Cint, (Ptr{Cvoid}, Cint, Cdouble), ctx[], inst[], lf.Γ))
+    check(ctx[], ccall((:gc_finalize, LIB), Cint, (Ptr{Cvoid},), ctx[]))
+    cl = CudaLeapFrog(ctx[], lf, h, ints)
+    finalizer(c -> ccall((:gc_ctx_destroy, LIB), Cint, (Ptr{Cvoid},), c.ctx), cl)
+    return cl
+end
+
+ps_ndims(ps) = ps.ndims
+
+function field_io!(cl::CudaLeapFrog, ps, f::Symbol, upload::Bool)
+    arr = getfield(ps, f)
+    fid = GC_FIELD[f]
+    GC.@preserve arr begin
+        fn = upload ? :gc_upload_field : :gc_download_field
+        st = ccall((fn, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cvoid}, Csize_t),
+                   cl.ctx, 0, cl.handles[ps], fid, pointer(arr), sizeof(arr))
+        check(cl.ctx, st)
+    end
+end
+
+function upload!(cl::CudaLeapFrog)
+    for ps in cl.lf.systems, f in fields_of(ps)
+        field_io!(cl, ps, f, true)
+    end
+end
+
+function download!(cl::CudaLeapFrog)
+    for ps in cl.lf.systems, f in fields_of(ps)
+        field_io!(cl, ps, f, false)
+    end
+end
+
+"""
+    time_integrate!(cl::CudaLeapFrog, num_timesteps, print_interval_step,
+                    save_interval_step, CFL, output_prefix; ...)
+
+Device version of Grasph's LeapFrog `time_integrate!`
+(src/TimeIntegration.jl:580).  Runs the steps on the GPU in chunks that end
+at print/save boundaries, where the host arrays are refreshed and Grasph's
+own `print_summary`/`write_h5` run.
+"""
+function Grasph.time_integrate!(cl::CudaLeapFrog, num_timesteps::Int, print_interval_step::Int,
+                                save_interval_step::Int, CFL::Real, output_prefix;
+                                step_offset::Int=0, kw...)
+    upload!(cl)
+    done = 0
+    while done < num_timesteps
+        g = step_offset + done
+        n = num_timesteps - done
+        for iv in (print_interval_step, output_prefix === nothing ? 0 : save_interval_step)
+            iv > 0 && (n = min(n, iv - g % iv))
+        end
+        check(cl.ctx, ccall((:gc_step, LIB), Cint, (Ptr{Cvoid}, Cint, Cdouble), cl.ctx, n, CFL))
+        done += n
+        g = step_offset + done
+        if g % print_interval_step == 0
+            download!(cl)
+            foreach(print_summary, cl.lf.systems)
+        end
+    end
+    download!(cl)
+    return nothing
+end
+
+end # module
