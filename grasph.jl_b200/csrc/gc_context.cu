@@ -95,6 +95,12 @@ struct DSlot {
     std::vector<std::vector<int>> upd_kind;
     bool upd_set = false;
     int nupd = 0;
+    // warp groups of this system's particles (one grid's columns)
+    int2* groups = nullptr;
+    int64_t* d_ngroups = nullptr;
+    int32_t *gcnt = nullptr, *goff = nullptr;
+    int64_t cap_gcols = 0;
+    int64_t groups_key = -1, groups_ver = -1;
     double* F(int k) { return f[cur][k]; }
     double* A(int k) { return f[cur ^ 1][k]; }
 };
@@ -131,6 +137,9 @@ struct DInter {
     int64_t cap_cells = 0;
     int64_t need_slot = -1;
     bool grid_valid = false;
+    int64_t cells = 0;      // packed cells of the current grid
+    int64_t grid_ver = -1;  // bumps at every rebuild
+    int64_t csa_ver = -1;   // grid version cs_a was built for
 };
 
 }  // namespace
@@ -158,6 +167,8 @@ struct gc_ctx {
     int64_t* h_need = nullptr;  // pinned
     int nneed = 0;
     int64_t* d_total_cells = nullptr;  // device copy of the current sort's cell total
+    int64_t grid_version = 0;
+    int num_sms = 148;
     // host I/O staging (device side of AoS <-> planar transposes)
     double* staging = nullptr;
     int64_t cap_staging = 0;  // doubles
@@ -368,6 +379,7 @@ int finalize(gc_ctx* ctx) {
         if (!same_structure(I0, ctx->inst[k], why))
             return seterr(ctx, GC_ERR_ARG, "instance %zu differs from instance 0 in %s", k, why.c_str());
     }
+    CU(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
     ctx->nstages = I0.inters[0].nstages;
     for (auto& it : I0.inters)
         if (it.nstages != ctx->nstages)
@@ -426,6 +438,8 @@ int finalize(gc_ctx* ctx) {
         TRY(dalloc(ctx, &D.q0rho, (size_t)D.N));
         TRY(dalloc(ctx, &D.aux, (size_t)D.N));
         TRY(dalloc(ctx, &D.inst_of, (size_t)D.N));
+        TRY(dalloc(ctx, &D.groups, (size_t)D.N + 1));
+        TRY(dalloc(ctx, &D.d_ngroups, 1));
         std::vector<int32_t> io(D.N);
         for (int k = 0; k < ninst; ++k)
             for (int64_t i = 0; i < D.h_inst[k].n; ++i) io[D.h_inst[k].base + i] = k;
@@ -660,7 +674,7 @@ int ensure_inter_cells(gc_ctx* ctx, DInter& D, int64_t cells) {
         dfree(ctx, D.cs, D.cap_cells);
         dfree(ctx, D.cs_a, D.cap_cells);
         TRY(dalloc(ctx, &D.cs, (size_t)cap));
-        if (D.two_sided) TRY(dalloc(ctx, &D.cs_a, (size_t)cap));
+        if (D.btype != BT_SELF) TRY(dalloc(ctx, &D.cs_a, (size_t)cap));
         D.cap_cells = cap;
     }
     return ensure_cells(ctx, cells);
@@ -843,7 +857,57 @@ int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
         scan_exclusive(ctx->hist, D.cs_a, cells, ctx->scan_tmp, ctx->stream);
     }
     D.grid_valid = true;
+    D.cells = cells;
+    D.grid_ver = ++ctx->grid_version;
+    D.csa_ver = D.two_sided ? D.grid_ver : -1;
     return check_launch(ctx, "grid");
+}
+
+// CSR of system_a's particles on a coupled interaction's grid.
+int ensure_csa(gc_ctx* ctx, DInter& D) {
+    if (D.btype == BT_SELF || D.csa_ver == D.grid_ver) return GC_OK;
+    DSlot& A = ctx->slots[D.a];
+    TRY(ensure_cells(ctx, D.cells));
+    CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (D.cells + 1), ctx->stream));
+    launch_grid_count(A.F(F_X), A.N, A.nd, A.inst_of, nullptr, D.d_gi, ctx->hist, D.cells, ctx->d_err,
+                      ctx->d_incons, ctx->stream);
+    scan_exclusive(ctx->hist, D.cs_a, D.cells, ctx->scan_tmp, ctx->stream);
+    D.csa_ver = D.grid_ver;
+    return check_launch(ctx, "grid (system_a)");
+}
+
+// Warp groups of `slot`'s particles from the columns of interaction `id`'s
+// grid: its system_b side when b_side, else its system_a side.
+int ensure_groups(gc_ctx* ctx, int slot, int id, bool b_side) {
+    DSlot& S = ctx->slots[slot];
+    DInter& D = ctx->inters[id];
+    const int64_t key = (int64_t)id * 2 + (b_side ? 1 : 0);
+    if (S.groups_key == key && S.groups_ver == D.grid_ver) return GC_OK;
+    const int32_t* cs;
+    if (b_side || D.btype == BT_SELF) {
+        cs = D.cs;
+    } else {
+        TRY(ensure_csa(ctx, D));
+        cs = D.cs_a;
+    }
+    const int64_t ncols_cap = D.cells;
+    if (ncols_cap + 1 > S.cap_gcols) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, S.gcnt, S.cap_gcols);
+        dfree(ctx, S.goff, S.cap_gcols);
+        int64_t cap = ncols_cap + 1 + ncols_cap / 4;
+        TRY(dalloc(ctx, &S.gcnt, (size_t)cap));
+        TRY(dalloc(ctx, &S.goff, (size_t)cap));
+        S.cap_gcols = cap;
+    }
+    TRY(ensure_cells(ctx, ncols_cap));  // scan scratch
+    const int nd = ctx->slots[D.a].nd;
+    launch_groups_count(D.d_gi, ninst(ctx), nd, cs, ncols_cap, S.gcnt, ctx->stream);
+    scan_exclusive(S.gcnt, S.goff, ncols_cap, ctx->scan_tmp, ctx->stream);
+    launch_groups_fill(D.d_gi, ninst(ctx), nd, cs, S.goff, ncols_cap, S.groups, S.d_ngroups, ctx->stream);
+    S.groups_key = key;
+    S.groups_ver = D.grid_ver;
+    return check_launch(ctx, "groups");
 }
 
 // Full prepare phase: sorts, ghosts and grids.  `sort_mask` selects which
@@ -981,7 +1045,13 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.a_c = S.d_c;
     A.a_mass = S.d_mass;
     A.err = ctx->d_err;
+    A.num_sms = ctx->num_sms;
     A.nref = 0;
+    for (int id : ids)
+        if (!ctx->inters[id].grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
+    TRY(ensure_groups(ctx, a, ids[0], false));
+    A.groups = S.groups;
+    A.ngroups = S.d_ngroups;
     for (int id : ids) {
         DInter& D = ctx->inters[id];
         if (!D.grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
@@ -1043,7 +1113,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         DInter& D = ctx->inters[id];
         if (!D.two_sided || count_only) continue;
         DSlot& B = ctx->slots[D.bslot];
+        TRY(ensure_groups(ctx, D.bslot, id, true));
         ForceArgs R = A;
+        R.groups = B.groups;
+        R.ngroups = B.d_ngroups;
         R.nd = B.nd;
         R.ns = B.ns;
         R.aN = B.N;
@@ -1254,6 +1327,10 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(S.q0rho);
         cudaFree(S.aux);
         cudaFree(S.inst_of);
+        cudaFree(S.groups);
+        cudaFree(S.d_ngroups);
+        cudaFree(S.gcnt);
+        cudaFree(S.goff);
         cudaFree(S.d_inst);
         cudaFree(S.d_mass);
         cudaFree(S.d_c);

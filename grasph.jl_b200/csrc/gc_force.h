@@ -9,7 +9,7 @@
 namespace gc {
 
 constexpr int FORCE_TPB = 128;  // threads per block of the sweep
-constexpr int FORCE_BUF = 32;   // staged neighbours per thread (shared memory)
+constexpr int FORCE_BUF = 64;   // staged neighbours per thread (shared memory)
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)
@@ -37,11 +37,18 @@ struct ForceArgs {
     const double* a_c;     // per-instance sound speed
     const double* a_mass;  // per-instance particle mass
     int* err;
+    const int2* groups;        // warp groups (start, count) of system_a particles
+    const int64_t* ngroups;    // device count of groups
+    int num_sms;
     int nref;
     InterRef ref[MAX_REFS];
 };
 
 int launch_force_f64(const ForceArgs& A, bool count_only, cudaStream_t s);
+void launch_groups_count(const GridInst* gi, int ninst, int nd, const int32_t* cs, int64_t ncols_cap, int32_t* cnt,
+                         cudaStream_t s);
+void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs, const int32_t* off,
+                        int64_t ncols_cap, int2* groups, int64_t* ngroups, cudaStream_t s);
 void launch_aux(int mode, int64_t N, const int64_t* count, const double* rho, const double* p,
                 const int32_t* inst_of, const double* mass, double* aux, cudaStream_t s);
 

@@ -46,6 +46,7 @@ struct GridInst {
     double ming[MAXD];                 // grid origin (src/Interaction.jl:143)
     int64_t ng[MAXD];                  // cells per dimension (:179)
     int64_t ncells, cellbase;          // this instance's cells in the packed grid
+    int64_t ncols, colbase;            // columns (all but the last dimension)
     double mina[MAXD], maxa[MAXD];     // system_a bounding box (coupled)
     // system_b wrapper parameters (src/BoundaryParticles.jl)
     double normal[MAXD], point[MAXD], beta, ljcut;

@@ -390,13 +390,16 @@ __global__ void k_grid_plan(GridPlanArgs a) {
             }
         }
         G.ncells = cells;
+        G.ncols = cells / G.ng[a.nd - 1];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        int64_t base = 0;
+        int64_t base = 0, cb = 0;
         for (int k = 0; k < a.ninst; ++k) {
             a.gi[k].cellbase = base;
+            a.gi[k].colbase = cb;
             base += a.gi[k].ncells;
+            cb += a.gi[k].ncols;
         }
         *a.need = base;
     }

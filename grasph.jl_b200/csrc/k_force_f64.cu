@@ -263,125 +263,203 @@ __device__ __forceinline__ void process_pair(const ForceArgs& A, const InterRef&
 }
 
 // ---------------------------------------------------------------- kernel
+// One warp owns one group: up to 32 consecutive (sorted) system_a particles
+// of one grid column (all cell coordinates but the last equal).  For each
+// 3-cell strip of the reference stencil the warp walks the union of its
+// lanes' candidate ranges — contiguous in the CSR because cells along the
+// last dimension are consecutive — loading 32 candidates at a time with one
+// coalesced load and broadcasting them by shuffles.  A lane accepts a
+// candidate only inside its own strip range [cs[z-1], cs[z+2]) and with
+// r² < (2h)², which is exactly the reference's pair test.  Accepted indices
+// go to the lane's shared-memory column; when any lane's column is nearly
+// full the whole warp evaluates its staged pairs, so the FP64 pair physics
+// runs on converged warps.
+template <int ND, int NS, int PFN, int KK, bool COUNT_ONLY>
+__device__ __forceinline__ void flush_all(const ForceArgs& A, const InterRef& r, const GridInst& G,
+                                          const PfnInst& P, int64_t gi, int k, const OwnState<ND>& o,
+                                          const double* osig, double da, int nbuf, const int32_t* col, int BT,
+                                          Acc<ND, NS>& acc) {
+    if (!COUNT_ONLY)
+        for (int t = 0; t < nbuf; ++t)
+            process_pair<ND, NS, PFN, KK>(A, r, G, P, gi, k, o, osig, da, col[t * BT], acc);
+}
+
 template <int ND, int NS, int PFN, int KK, bool COUNT_ONLY>
 __global__ void __launch_bounds__(FORCE_TPB) k_force(ForceArgs A) {
     extern __shared__ int32_t sbuf[];
-    const int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= A.aN) return;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const int tid = threadIdx.x;
     const int BT = blockDim.x;
-    const int k = A.a_inst_of[gi];
+    int32_t* col = sbuf + tid;
+    const int64_t ngroups = *A.ngroups;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t N = A.aN;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ngroups; w += nwarps) {
+        const int2 grp = A.groups[w];
+        const bool active = lane < grp.y;
+        const int64_t gi = (int64_t)grp.x + (active ? lane : 0);
+        const int k = A.a_inst_of[gi];
 
-    OwnState<ND> o;
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        o.x[d] = A.ax[d * N + gi];
-        o.v[d] = A.av[d * N + gi];
-    }
-    o.rho = A.arho[gi];
-    o.aux = A.aaux ? A.aaux[gi] : 0.0;
-    double osig[NS > 0 ? NS : 1];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) osig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? A.astress[q * N + gi] : 0.0;
-
-    Acc<ND, NS> acc;
-    if (!COUNT_ONLY) {
-        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
-#pragma unroll
-            for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
-            acc.dr = A.adrhodt[gi];
-        } else {
-#pragma unroll
-            for (int q = 0; q < NS; ++q) acc.sr[q] = A.asr[q * N + gi];
-            if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
-#pragma unroll
-                for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) acc.w[q] = A.avort[q * N + gi];
-            }
-        }
-    }
-
-    for (int ri = 0; ri < A.nref; ++ri) {
-        const InterRef& r = A.ref[ri];
-        const GridInst& G = r.gi[k];
-        const PfnInst& P = r.pi[k];
-        // own cell in this grid (src/Interaction.jl:197-206)
-        int64_t c[ND];
-        bool ok = true;
+        OwnState<ND> o;
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
-            if (!floor_i64((o.x[d] - G.ming[d]) / G.cell, &c[d]) || c[d] < 1 || c[d] >= G.ng[d] - 1) ok = false;
+            o.x[d] = A.ax[d * N + gi];
+            o.v[d] = A.av[d * N + gi];
         }
-        if (!ok) {
-            atomicOr(A.err, ERR_CAPACITY);
-            continue;
-        }
-        double da = 0.0;
-        if (r.btype == BT_DYNAMIC) {
-            double t[ND];
+        o.rho = A.arho[gi];
+        o.aux = A.aaux ? A.aaux[gi] : 0.0;
+        double osig[NS > 0 ? NS : 1];
 #pragma unroll
-            for (int d = 0; d < ND; ++d) t[d] = o.x[d] - G.point[d];
-            da = dotv<ND>(t, G.normal);
-        }
-        const int64_t Nb = r.bN;
-        int nbuf = 0;
-        int32_t accepted = 0;
-        const int nstrips = ND == 2 ? 3 : 9;
-        for (int sidx = 0; sidx < nstrips; ++sidx) {
-            int64_t base;
-            if (ND == 2) {
-                base = G.cellbase + (c[0] + sidx - 1) * G.ng[1] + (c[1] - 1);
+        for (int q = 0; q < NS; ++q) osig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? A.astress[q * N + gi] : 0.0;
+
+        Acc<ND, NS> acc;
+        if (!COUNT_ONLY) {
+            if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
+                acc.dr = A.adrhodt[gi];
             } else {
-                int dxc = sidx / 3 - 1, dyc = sidx % 3 - 1;
-                base = G.cellbase + ((c[0] + dxc) * G.ng[1] + (c[1] + dyc)) * G.ng[2] + (c[2] - 1);
-            }
-            const int32_t s = r.cs[base], e = r.cs[base + 3];
-            for (int32_t j = s; j < e; ++j) {
-                if (r.btype == BT_SELF && j == gi) continue;
-                double dx[ND];
 #pragma unroll
-                for (int d = 0; d < ND; ++d) dx[d] = o.x[d] - r.bx[d * Nb + j];
-                double rr = dotv<ND>(dx, dx);
-                if (rr < G.cutoff_sq) {
-                    ++accepted;
-                    if (COUNT_ONLY) continue;
-                    sbuf[nbuf * BT + tid] = j;
-                    if (++nbuf == FORCE_BUF) {
-                        for (int t = 0; t < nbuf; ++t)
-                            process_pair<ND, NS, PFN, KK>(A, r, G, P, gi, k, o, osig, da, sbuf[t * BT + tid], acc);
-                        nbuf = 0;
-                    }
+                for (int q = 0; q < NS; ++q) acc.sr[q] = A.asr[q * N + gi];
+                if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+#pragma unroll
+                    for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) acc.w[q] = A.avort[q * N + gi];
                 }
             }
         }
-        if (!COUNT_ONLY)
-            for (int t = 0; t < nbuf; ++t)
-                process_pair<ND, NS, PFN, KK>(A, r, G, P, gi, k, o, osig, da, sbuf[t * BT + tid], acc);
-        if (r.counts) r.counts[gi] = accepted;
-    }
 
-    if (COUNT_ONLY) return;
-    if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        for (int ri = 0; ri < A.nref; ++ri) {
+            const InterRef& r = A.ref[ri];
+            const GridInst& G = r.gi[k];
+            const PfnInst& P = r.pi[k];
+            int64_t c[ND];
+            bool ok = true;
 #pragma unroll
-        for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
-        A.adrhodt[gi] = acc.dr;
-    } else {
+            for (int d = 0; d < ND; ++d)
+                if (!floor_i64((o.x[d] - G.ming[d]) / G.cell, &c[d]) || c[d] < 1 || c[d] >= G.ng[d] - 1) ok = false;
+            if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
+            double da = 0.0;
+            if (r.btype == BT_DYNAMIC) {
+                double t[ND];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = acc.sr[q];
-        if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+                for (int d = 0; d < ND; ++d) t[d] = o.x[d] - G.point[d];
+                da = dotv<ND>(t, G.normal);
+            }
+            const int64_t Nb = r.bN;
+            const bool self = r.btype == BT_SELF;
+            int nbuf = 0;
+            int32_t accepted = 0;
+            // column of lane 0; the cooperative walk needs every active lane in it
+            int64_t c0 = __shfl_sync(FULL, c[0], 0);
+            int64_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
+            bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
+            const bool coop = __all_sync(FULL, !active || same);
+            if (coop) {
+                constexpr int L = ND - 1;  // last dimension
+                int64_t zlo = active ? c[L] : INT64_MAX, zhi = active ? c[L] : INT64_MIN;
 #pragma unroll
-            for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) A.avort[q * N + gi] = acc.w[q];
+                for (int o2 = 16; o2 > 0; o2 >>= 1) {
+                    int64_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
+                    zlo = a2 < zlo ? a2 : zlo;
+                    zhi = b2 > zhi ? b2 : zhi;
+                }
+                const int64_t ngl = G.ng[L];
+                const int nstrips = ND == 2 ? 3 : 9;
+                for (int sidx = 0; sidx < nstrips; ++sidx) {
+                    int64_t colflat;
+                    if (ND == 2) colflat = c0 + sidx - 1;
+                    else colflat = (c0 + sidx / 3 - 1) * G.ng[1] + (c1 + sidx % 3 - 1);
+                    const int64_t base = G.cellbase + colflat * ngl;
+                    const int32_t u0 = r.cs[base + zlo - 1], u1 = r.cs[base + zhi + 2];
+                    const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
+                    for (int32_t ch = u0; ch < u1; ch += 32) {
+                        if (!COUNT_ONLY && __any_sync(FULL, nbuf > FORCE_BUF - 32)) {
+                            flush_all<ND, NS, PFN, KK, COUNT_ONLY>(A, r, G, P, gi, k, o, osig, da, nbuf, col, BT, acc);
+                            nbuf = 0;
+                            __syncwarp();
+                        }
+                        const int32_t jl = ch + lane;
+                        double xj[ND];
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) xj[d] = jl < u1 ? r.bx[d * Nb + jl] : 0.0;
+                        const int m = u1 - ch < 32 ? (int)(u1 - ch) : 32;
+                        for (int t = 0; t < m; ++t) {
+                            double dx[ND];
+#pragma unroll
+                            for (int d = 0; d < ND; ++d) dx[d] = o.x[d] - __shfl_sync(FULL, xj[d], t);
+                            const int32_t jt = ch + t;
+                            double rr = dotv<ND>(dx, dx);
+                            if (active && jt >= lo && jt < hi && !(self && jt == gi) && rr < G.cutoff_sq) {
+                                ++accepted;
+                                if (!COUNT_ONLY) col[(nbuf++) * BT] = jt;
+                            }
+                        }
+                    }
+                }
+                flush_all<ND, NS, PFN, KK, COUNT_ONLY>(A, r, G, P, gi, k, o, osig, da, nbuf, col, BT, acc);
+                nbuf = 0;
+                __syncwarp();
+            } else if (active && ok) {
+                // rare: lanes disagree on the column in this grid; walk own strips
+                const int nstrips = ND == 2 ? 3 : 9;
+                for (int sidx = 0; sidx < nstrips; ++sidx) {
+                    int64_t base;
+                    if (ND == 2) base = G.cellbase + (c[0] + sidx - 1) * G.ng[1] + (c[1] - 1);
+                    else base = G.cellbase + ((c[0] + sidx / 3 - 1) * G.ng[1] + (c[1] + sidx % 3 - 1)) * G.ng[2] + (c[2] - 1);
+                    const int32_t s0 = r.cs[base], e0 = r.cs[base + 3];
+                    for (int32_t j = s0; j < e0; ++j) {
+                        if (self && j == gi) continue;
+                        double dx[ND];
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) dx[d] = o.x[d] - r.bx[d * Nb + j];
+                        if (dotv<ND>(dx, dx) < G.cutoff_sq) {
+                            ++accepted;
+                            if (COUNT_ONLY) continue;
+                            col[(nbuf++) * BT] = j;
+                            if (nbuf == FORCE_BUF) {
+                                flush_all<ND, NS, PFN, KK, COUNT_ONLY>(A, r, G, P, gi, k, o, osig, da, nbuf, col, BT, acc);
+                                nbuf = 0;
+                            }
+                        }
+                    }
+                }
+                flush_all<ND, NS, PFN, KK, COUNT_ONLY>(A, r, G, P, gi, k, o, osig, da, nbuf, col, BT, acc);
+                nbuf = 0;
+            }
+            __syncwarp();
+            if (active && r.counts) r.counts[gi] = accepted;
         }
+
+        if (!COUNT_ONLY && active) {
+            if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
+                A.adrhodt[gi] = acc.dr;
+            } else {
+#pragma unroll
+                for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = acc.sr[q];
+                if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+#pragma unroll
+                    for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) A.avort[q * N + gi] = acc.w[q];
+                }
+            }
+        }
+        __syncwarp();
     }
 }
 
 // ------------------------------------------------------------ dispatch
 template <int ND, int NS, int PFN, int KK>
 static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
-    int blocks = (int)((A.aN + FORCE_TPB - 1) / FORCE_TPB);
+    // grid-stride over groups; at most one group per particle
+    int64_t warps = A.aN;
+    int64_t blocks = (warps * 32 + FORCE_TPB - 1) / FORCE_TPB;
+    if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
+    if (blocks < 1) blocks = 1;
     size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t);
-    if (count_only) k_force<ND, NS, PFN, KK, true><<<blocks, FORCE_TPB, 0, s>>>(A);
-    else k_force<ND, NS, PFN, KK, false><<<blocks, FORCE_TPB, smem, s>>>(A);
+    if (count_only) k_force<ND, NS, PFN, KK, true><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
+    else k_force<ND, NS, PFN, KK, false><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
@@ -425,6 +503,69 @@ int launch_force_f64(const ForceArgs& A, bool count_only, cudaStream_t s) {
     if (A.aN <= 0 || A.nref == 0) return 0;
     if (A.kk == GC_KERNEL_CUBIC_SPLINE) return launch_kk<GC_KERNEL_CUBIC_SPLINE>(A, count_only, s);
     return launch_kk<GC_KERNEL_WENDLAND_C2>(A, count_only, s);
+}
+
+// --------------------------------------------------------------- groups
+// Columns of the primary grid → warp groups of ≤ 32 consecutive particles.
+__device__ __forceinline__ int find_inst(const GridInst* gi, int ninst, int64_t col) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (gi[mid].colbase <= col) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_groups_count(const GridInst* __restrict__ gi, int ninst, int nd, const int32_t* __restrict__ cs,
+                               int64_t ncols_cap, int32_t* __restrict__ cnt) {
+    const int64_t T = gi[ninst - 1].colbase + gi[ninst - 1].ncols;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncols_cap;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        if (c >= T) {
+            cnt[c] = 0;
+            continue;
+        }
+        const GridInst& G = gi[find_inst(gi, ninst, c)];
+        const int64_t ngl = G.ng[nd - 1];
+        const int64_t local = c - G.colbase;
+        const int64_t b = G.cellbase + local * ngl;
+        const int32_t n = cs[b + ngl] - cs[b];
+        cnt[c] = (n + 31) / 32;
+    }
+}
+
+__global__ void k_groups_fill(const GridInst* __restrict__ gi, int ninst, int nd, const int32_t* __restrict__ cs,
+                              const int32_t* __restrict__ off, int64_t ncols_cap, int2* __restrict__ groups,
+                              int64_t* ngroups) {
+    const int64_t T = gi[ninst - 1].colbase + gi[ninst - 1].ncols;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < T && c < ncols_cap;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const GridInst& G = gi[find_inst(gi, ninst, c)];
+        const int64_t ngl = G.ng[nd - 1];
+        const int64_t local = c - G.colbase;
+        const int64_t b = G.cellbase + local * ngl;
+        const int32_t s0 = cs[b], n = cs[b + ngl] - s0;
+        int32_t o = off[c];
+        for (int32_t q = 0; q < n; q += 32) groups[o++] = make_int2(s0 + q, n - q < 32 ? n - q : 32);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = off[ncols_cap];
+}
+
+void launch_groups_count(const GridInst* gi, int ninst, int nd, const int32_t* cs, int64_t ncols_cap, int32_t* cnt,
+                         cudaStream_t s) {
+    int64_t b = (ncols_cap + 255) / 256;
+    if (b < 1) b = 1;
+    k_groups_count<<<(int)b, 256, 0, s>>>(gi, ninst, nd, cs, ncols_cap, cnt);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs, const int32_t* off,
+                        int64_t ncols_cap, int2* groups, int64_t* ngroups, cudaStream_t s) {
+    int64_t b = (ncols_cap + 255) / 256;
+    if (b < 1) b = 1;
+    k_groups_fill<<<(int)b, 256, 0, s>>>(gi, ninst, nd, cs, off, ncols_cap, groups, ngroups);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 // Per-particle factors the functors divide by, computed once per stage
