@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -169,6 +170,7 @@ struct gc_ctx {
     int64_t* d_total_cells = nullptr;  // device copy of the current sort's cell total
     int64_t grid_version = 0;
     int num_sms = 148;
+    int force_cfg = 0;
     // host I/O staging (device side of AoS <-> planar transposes)
     double* staging = nullptr;
     int64_t cap_staging = 0;  // doubles
@@ -209,6 +211,16 @@ int seterr(gc_ctx* c, int code, const char* fmt, ...) {
         int st_ = (expr);    \
         if (st_) return st_; \
     } while (0)
+
+// Host<->device copy ordered after everything already on the context's
+// stream, complete on return.  (A plain cudaMemcpy runs on the legacy default
+// stream, which does not wait for the context's non-blocking stream.)
+int hcopy(gc_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (bytes == 0) return GC_OK;
+    CU(cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GC_OK;
+}
 
 template <class T>
 int dalloc(gc_ctx* ctx, T** p, size_t count) {
@@ -768,7 +780,7 @@ int read_need(gc_ctx* ctx) {
     CU(cudaStreamSynchronize(ctx->stream));
     TRY(collect_profile(ctx));
     int e = 0;
-    CU(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    TRY(hcopy(ctx, &e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e & ERR_NONFINITE) return seterr(ctx, GC_ERR_NONFINITE, "non-finite or out-of-range particle position");
     if (e & ERR_CAPACITY) return seterr(ctx, GC_ERR_CAPACITY, "grid or key range exceeds 2^31 cells");
     return GC_OK;
@@ -1046,6 +1058,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.a_mass = S.d_mass;
     A.err = ctx->d_err;
     A.num_sms = ctx->num_sms;
+    A.cfg = ctx->force_cfg;
     A.nref = 0;
     for (int id : ids)
         if (!ctx->inters[id].grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
@@ -1062,8 +1075,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs;
         r.counts = D.counts;
+        r.bbox = nullptr;
         if (D.btype == BT_GHOST) {
             DGhost& G = ctx->ghosts[D.bghost];
+            r.bbox = G.d_inst;
             r.bx = G.x[G.cur];
             r.bv = G.v;
             r.brho = G.rho;
@@ -1075,6 +1090,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             r.baux = G.aux;
         } else {
             DSlot& B = ctx->slots[D.bslot];
+            if (D.btype != BT_SELF) r.bbox = B.d_inst;
             r.bx = B.F(F_X);
             r.bv = B.F(F_V);
             r.brho = B.F(F_RHO);
@@ -1132,6 +1148,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         R.nref = 1;
         InterRef& r = R.ref[0];
         r.btype = BT_SYSTEM;
+        r.bbox = S.d_inst;
         r.gi = D.d_gi;
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs_a;
@@ -1194,7 +1211,7 @@ int push_slot_params(gc_ctx* ctx, DSlot& S) {
     // Only the host-owned members; bbox/plan members are device-written.
     const int ni = ninst(ctx);
     std::vector<SysInst> cur(ni);
-    CU(cudaMemcpy(cur.data(), S.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
+    TRY(hcopy(ctx, cur.data(), S.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
     for (int k = 0; k < ni; ++k) {
         cur[k].base = S.h_inst[k].base;
         cur[k].n = S.h_inst[k].n;
@@ -1207,7 +1224,7 @@ int push_slot_params(gc_ctx* ctx, DSlot& S) {
         cur[k].half_dt = S.h_inst[k].half_dt;
         cur[k].gamma_dt = S.h_inst[k].gamma_dt;
     }
-    CU(cudaMemcpy(S.d_inst, cur.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
+    TRY(hcopy(ctx, S.d_inst, cur.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
     return GC_OK;
 }
 
@@ -1266,7 +1283,7 @@ int finish_status(gc_ctx* ctx) {
     CU(cudaStreamSynchronize(ctx->stream));
     TRY(collect_profile(ctx));
     int e = 0;
-    CU(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    TRY(hcopy(ctx, &e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     ctx->last_status = e;
     if (e & ERR_NONFINITE) return seterr(ctx, GC_ERR_NONFINITE, "non-finite or out-of-range particle position");
     if (e & ERR_CAPACITY) return seterr(ctx, GC_ERR_CAPACITY, "a particle fell outside its grid or key range");
@@ -1305,6 +1322,7 @@ int gc_ctx_create(int device, size_t hbm_budget_bytes, gc_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return GC_ERR_CUDA;
     gc_ctx* ctx = new gc_ctx();
     ctx->device = device;
+    if (const char* e = getenv("GC_FORCE_CFG")) ctx->force_cfg = atoi(e);
     ctx->budget = hbm_budget_bytes;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
@@ -1608,14 +1626,14 @@ static int ensure_staging(gc_ctx* ctx, int64_t doubles) {
 static int ghost_field_io(gc_ctx* ctx, int inst, DGhost& G, int field, void* host, size_t bytes) {
     const GhostInst* hg = nullptr;
     std::vector<GhostInst> gh(ninst(ctx));
-    CU(cudaMemcpy(gh.data(), G.d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
+    TRY(hcopy(ctx, gh.data(), G.d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
     hg = &gh[inst];
     const int64_t n = hg->n, base = hg->base;
     auto get_planar = [&](const double* src, int ncomp, int64_t stride) -> int {
         if (bytes != (size_t)(n * ncomp * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
         std::vector<double> tmp((size_t)ncomp * n);
         for (int c = 0; c < ncomp; ++c)
-            if (n) CU(cudaMemcpy(&tmp[(size_t)c * n], src + c * stride + base, n * 8, cudaMemcpyDeviceToHost));
+            if (n) TRY(hcopy(ctx, &tmp[(size_t)c * n], src + c * stride + base, n * 8, cudaMemcpyDeviceToHost));
         double* out = (double*)host;
         for (int64_t i = 0; i < n; ++i)
             for (int c = 0; c < ncomp; ++c) out[i * ncomp + c] = tmp[(size_t)c * n + i];
@@ -1624,7 +1642,7 @@ static int ghost_field_io(gc_ctx* ctx, int inst, DGhost& G, int field, void* hos
     auto get_i32 = [&](const int32_t* src) -> int {
         if (bytes != (size_t)(n * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
         std::vector<int32_t> tmp(n);
-        if (n) CU(cudaMemcpy(tmp.data(), src + base, n * 4, cudaMemcpyDeviceToHost));
+        if (n) TRY(hcopy(ctx, tmp.data(), src + base, n * 4, cudaMemcpyDeviceToHost));
         int64_t* out = (int64_t*)host;
         for (int64_t i = 0; i < n; ++i) out[i] = tmp[i];
         return GC_OK;
@@ -1748,7 +1766,7 @@ int gc_get_count(gc_ctx* ctx, int inst, int handle, int64_t* n_out) {
     if (r.ghost) {
         std::vector<GhostInst> gh(ninst(ctx));
         CU(cudaStreamSynchronize(ctx->stream));
-        CU(cudaMemcpy(gh.data(), r.ghost->d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
+        TRY(hcopy(ctx, gh.data(), r.ghost->d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
         *n_out = gh[inst].n;
     } else {
         *n_out = ctx->inst[inst].sys[r.sys].n;
@@ -1803,7 +1821,7 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
     }
     if (ctx->d_incons) {
         unsigned long long v = 0;
-        CU(cudaMemcpy(&v, ctx->d_incons, sizeof v, cudaMemcpyDeviceToHost));
+        TRY(hcopy(ctx, &v, ctx->d_incons, sizeof v, cudaMemcpyDeviceToHost));
         out->grid_inconsistent = (int64_t)v;
     }
     return GC_OK;
@@ -1820,17 +1838,18 @@ int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* pe
     if (r.ghost) {
         DGhost& G = *r.ghost;
         std::vector<SysInst> gi(ni);
-        CU(cudaMemcpy(gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
+        TRY(hcopy(ctx, gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
         for (auto& g : gi) g.sort_cutoff = cutoff;
-        CU(cudaMemcpy(G.d_inst, gi.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
+        TRY(hcopy(ctx, G.d_inst, gi.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
         TRY(ghost_bbox_and_plan(ctx, G));
         TRY(read_need(ctx));
         TRY(sort_particles_slot(ctx, nullptr, &G, ctx->h_need[G.need_slot]));
+        TRY(finish_status(ctx));  // host reads below must follow the stream's kernels
         if (perm_out) {
-            CU(cudaMemcpy(gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
+            TRY(hcopy(ctx, gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
             const int64_t n = gi[inst].n, base = gi[inst].base;
             std::vector<int32_t> p(n);
-            if (n) CU(cudaMemcpy(p.data(), ctx->perm + base, n * 4, cudaMemcpyDeviceToHost));
+            if (n) TRY(hcopy(ctx, p.data(), ctx->perm + base, n * 4, cudaMemcpyDeviceToHost));
             for (int64_t i = 0; i < n; ++i) perm_out[i] = p[i] - base + 1;
         }
         return finish_status(ctx);
@@ -1842,10 +1861,11 @@ int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* pe
     launch_sort_plan(S.d_inst, ni, S.nd, ctx->d_need + r.sys, ctx->d_err, ctx->stream);
     TRY(read_need(ctx));
     TRY(sort_particles_slot(ctx, &S, nullptr, ctx->h_need[r.sys]));
+    TRY(finish_status(ctx));  // host reads below must follow the stream's kernels
     if (perm_out) {
         const int64_t n = S.h_inst[inst].n, base = S.h_inst[inst].base;
         std::vector<int32_t> p(n);
-        CU(cudaMemcpy(p.data(), ctx->perm + base, n * 4, cudaMemcpyDeviceToHost));
+        TRY(hcopy(ctx, p.data(), ctx->perm + base, n * 4, cudaMemcpyDeviceToHost));
         for (int64_t i = 0; i < n; ++i) perm_out[i] = p[i] - base + 1;
     }
     for (auto& D : ctx->inters) D.grid_valid = false;
@@ -1874,7 +1894,7 @@ int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int
     TRY(build_grid(ctx, D, ctx->h_need[D.need_slot]));
     TRY(finish_status(ctx));
     std::vector<GridInst> gi(ninst(ctx));
-    CU(cudaMemcpy(gi.data(), D.d_gi, gi.size() * sizeof(GridInst), cudaMemcpyDeviceToHost));
+    TRY(hcopy(ctx, gi.data(), D.d_gi, gi.size() * sizeof(GridInst), cudaMemcpyDeviceToHost));
     const GridInst& G = gi[inst];
     const int nd = ctx->slots[D.a].nd;
     if (ncells_out) *ncells_out = G.ncells;
@@ -1885,11 +1905,11 @@ int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int
     if (cell_start_out) {
         if (cap < G.ncells + 1) return seterr(ctx, GC_ERR_CAPACITY, "cell_start buffer too small");
         std::vector<int32_t> cs(G.ncells + 1);
-        CU(cudaMemcpy(cs.data(), D.cs + G.cellbase, cs.size() * 4, cudaMemcpyDeviceToHost));
+        TRY(hcopy(ctx, cs.data(), D.cs + G.cellbase, cs.size() * 4, cudaMemcpyDeviceToHost));
         int64_t bbase;
         if (D.btype == BT_GHOST) {
             std::vector<GhostInst> gh(ninst(ctx));
-            CU(cudaMemcpy(gh.data(), ctx->ghosts[D.bghost].d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
+            TRY(hcopy(ctx, gh.data(), ctx->ghosts[D.bghost].d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
             bbase = gh[inst].base;
         } else {
             bbase = ctx->slots[D.bslot].h_inst[inst].base;
@@ -1972,7 +1992,7 @@ int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, in
     D.pk = saved;
     TRY(st);
     TRY(finish_status(ctx));
-    CU(cudaMemcpy(counts_out, D.counts + S.h_inst[inst].base, n * 4, cudaMemcpyDeviceToHost));
+    TRY(hcopy(ctx, counts_out, D.counts + S.h_inst[inst].base, n * 4, cudaMemcpyDeviceToHost));
     return GC_OK;
 }
 

@@ -9,7 +9,16 @@
 namespace gc {
 
 constexpr int FORCE_TPB = 128;  // threads per block of the sweep
-constexpr int FORCE_BUF = 64;   // staged neighbours per thread (shared memory)
+constexpr int FORCE_BUF = 64;   // largest staged-neighbour column (shared memory)
+
+// Launch configurations of the sweep: (min resident blocks, staged
+// neighbours per thread, pair-loop unroll).  Chosen per (system, stage) by
+// the tuner in gc_context.cu.
+struct ForceCfg {
+    int minb, buf, unroll;
+};
+constexpr int NUM_FORCE_CFG = 4;
+constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1}, {4, 64, 2}, {6, 48, 2}, {8, 40, 1}};
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)
@@ -20,6 +29,7 @@ enum { AUX_P_OVER_RHO2 = 0, AUX_INV_RHO2 = 1, AUX_MASS_OVER_RHO = 2 };
 
 struct InterRef {
     int btype;
+    const SysInst* bbox;  // per-instance bounding box of system_b (nullptr: never skip)
     const GridInst* gi;   // per instance
     const PfnInst* pi;    // per instance, this stage
     const int32_t* cs;    // packed CSR over system_b (global b indices)
@@ -40,6 +50,7 @@ struct ForceArgs {
     const int2* groups;        // warp groups (start, count) of system_a particles
     const int64_t* ngroups;    // device count of groups
     int num_sms;
+    int cfg;                   // index into FORCE_CFGS
     int nref;
     InterRef ref[MAX_REFS];
 };
