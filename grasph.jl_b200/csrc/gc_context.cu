@@ -87,6 +87,9 @@ struct DSlot {
     SysInst* d_inst = nullptr;
     std::vector<SysInst> h_inst;
     double *d_mass = nullptr, *d_c = nullptr;
+    float *d_massf = nullptr, *d_cf = nullptr;
+    float* fpk = nullptr;      // FP32 pack for the FP32-compensated sweep
+    int64_t cap_fpk = 0;
     bool written = false;      // some functor writes this system
     bool moving = true;        // sorted and integrated every step
     bool sorted_once = false;  // static systems: sorted since the last upload
@@ -120,6 +123,8 @@ struct DGhost {
     SysInst* d_inst = nullptr;
     std::vector<SysInst> h_inst;
     double *d_mass = nullptr, *d_c = nullptr;
+    float* fpk = nullptr;
+    int64_t cap_fpk = 0;
     std::vector<std::vector<std::pair<int, int>>> copiers;
     bool ex_p = false, ex_stress = false;
     int64_t need_slot = -1;  // index into need[] for its sort cells
@@ -466,6 +471,15 @@ int finalize(gc_ctx* ctx) {
         }
         CU(cudaMemcpyAsync(D.d_mass, m.data(), ninst * 8, cudaMemcpyHostToDevice, ctx->stream));
         CU(cudaMemcpyAsync(D.d_c, c.data(), ninst * 8, cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<float> mf(ninst), cf(ninst);
+        for (int k = 0; k < ninst; ++k) {
+            mf[k] = (float)m[k];
+            cf[k] = (float)c[k];
+        }
+        TRY(dalloc(ctx, &D.d_massf, (size_t)ninst));
+        TRY(dalloc(ctx, &D.d_cf, (size_t)ninst));
+        CU(cudaMemcpyAsync(D.d_massf, mf.data(), ninst * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(D.d_cf, cf.data(), ninst * 4, cudaMemcpyHostToDevice, ctx->stream));
         // ids default to 1..n per instance
         std::vector<int32_t> ids(D.N);
         for (int k = 0; k < ninst; ++k)
@@ -593,6 +607,8 @@ int finalize(gc_ctx* ctx) {
             G.cell = 2.0 * h.H;
             G.cutoff_sq = G.cell * G.cell;
             G.knorm = kernel_norm(h.kk, I.sys[h.a].nd, h.H);
+            G.f_invH = (float)(1.0 / h.H);
+            G.f_knorm = (float)G.knorm;
             if (h.b >= 0) {
                 const HHandle& hh = I.handles[h.b];
                 for (int d = 0; d < 3; ++d) {
@@ -601,6 +617,9 @@ int finalize(gc_ctx* ctx) {
                 }
                 G.beta = hh.beta;
                 G.ljcut = hh.ljcut;
+                for (int d = 0; d < 3; ++d) G.f_normal[d] = (float)hh.normal[d];
+                G.f_beta = (float)hh.beta;
+                G.f_ljcut = (float)hh.ljcut;
                 if (hh.type == H_GHOST) {
                     const HSys& src = I.sys[I.ghosts[hh.idx].src];
                     G.bmass = src.mass;
@@ -609,6 +628,8 @@ int finalize(gc_ctx* ctx) {
                     G.bmass = I.sys[hh.idx].mass;
                     G.bc = I.sys[hh.idx].c;
                 }
+                G.f_bmass = (float)G.bmass;
+                G.f_bc = (float)G.bc;
             }
         }
         TRY(dalloc(ctx, &D.d_gi, (size_t)ninst));
@@ -624,6 +645,11 @@ int finalize(gc_ctx* ctx) {
                 per[k].S = (int)p[3];
                 per[k].delta = std::isnan(p[4]) ? 0.0 : p[4];
                 per[k].has_delta = std::isnan(p[4]) ? 0 : 1;
+                per[k].f_alpha = (float)p[0];
+                per[k].f_beta = (float)p[1];
+                per[k].f_h = (float)p[2];
+                per[k].f_h2eps = (float)(p[2] * p[2] * 0.01);
+                per[k].f_delta = (float)per[k].delta;
             }
             TRY(dalloc(ctx, &D.d_pi[s], (size_t)ninst));
             CU(cudaMemcpyAsync(D.d_pi[s], per.data(), ninst * sizeof(PfnInst), cudaMemcpyHostToDevice, ctx->stream));
@@ -1023,6 +1049,18 @@ int ghost_copy(gc_ctx* ctx, DGhost& G, int stage) {
     return check_launch(ctx, "ghost copy");
 }
 
+template <class T>
+int ensure_fpk(gc_ctx* ctx, T& X, int64_t N, int ncomp) {
+    int64_t need = N * ncomp;
+    if (need > X.cap_fpk) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, X.fpk, X.cap_fpk);
+        TRY(dalloc(ctx, &X.fpk, (size_t)need));
+        X.cap_fpk = need;
+    }
+    return GC_OK;
+}
+
 int aux_mode_for(int pfn) {
     if (pfn == GC_PFN_FLUID) return AUX_P_OVER_RHO2;
     if (pfn == GC_PFN_CAUCHY_FLUID) return AUX_INV_RHO2;
@@ -1034,8 +1072,18 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     DSlot& S = ctx->slots[a];
     int pfn = ctx->inters[ids[0]].pk[stage - 1];
     const int mode = aux_mode_for(pfn);
+    bool fp32 = ctx->precision == GC_PRECISION_FP32_COMPENSATED && pfn != GC_PFN_COUNT && !count_only;
+    for (int id : ids)
+        if (pfn == GC_PFN_FLUID && ctx->inters[id].h_gi.size() && ctx->inst[0].inters[id].pp[stage - 1][3] == 1.0)
+            fp32 = false;  // the S = 1 (multiphase) pressure form stays in FP64
+    const int pk_ns = pfn == GC_PFN_CAUCHY_FLUID ? S.ns : 0;
     if (pfn != GC_PFN_COUNT) {
         launch_aux(mode, S.N, nullptr, S.F(F_RHO), S.F(F_P), S.inst_of, S.d_mass, S.aux, ctx->stream);
+        if (fp32) {
+            TRY(ensure_fpk(ctx, S, S.N, S.nd + 3 + pk_ns));
+            launch_pack32(mode, S.N, nullptr, S.nd, pk_ns, S.F(F_V), S.F(F_RHO), S.F(F_P), S.F(F_STRESS), S.inst_of,
+                          S.d_mass, S.fpk, ctx->stream);
+        }
     }
     ForceArgs A{};
     A.nd = S.nd;
@@ -1056,6 +1104,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.avort = S.F(F_VORT);
     A.a_c = S.d_c;
     A.a_mass = S.d_mass;
+    A.a_cf = S.d_cf;
+    A.a_massf = S.d_massf;
+    A.afp = fp32 ? S.fpk : nullptr;
+    A.prec = fp32 ? GC_PRECISION_FP32_COMPENSATED : GC_PRECISION_FP64;
     A.err = ctx->d_err;
     A.num_sms = ctx->num_sms;
     A.cfg = ctx->force_cfg;
@@ -1088,6 +1140,13 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             if (pfn != GC_PFN_COUNT)
                 launch_aux(mode, G.CAP, G.d_count, G.rho, G.p, G.ginst[G.cur], G.d_mass, G.aux, ctx->stream);
             r.baux = G.aux;
+            r.bfp = nullptr;
+            if (fp32) {
+                TRY(ensure_fpk(ctx, G, G.CAP, G.nd + 3 + pk_ns));
+                launch_pack32(mode, G.CAP, G.d_count, G.nd, pk_ns, G.v, G.rho, G.p, G.stress, G.ginst[G.cur], G.d_mass,
+                              G.fpk, ctx->stream);
+                r.bfp = G.fpk;
+            }
         } else {
             DSlot& B = ctx->slots[D.bslot];
             if (D.btype != BT_SELF) r.bbox = B.d_inst;
@@ -1097,13 +1156,21 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             r.bp = B.F(F_P);
             r.bstress = B.F(F_STRESS);
             r.bN = B.N;
+            r.bfp = nullptr;
             if (D.btype == BT_SELF) {
                 r.baux = S.aux;
+                r.bfp = fp32 ? S.fpk : nullptr;
             } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT) {
                 launch_aux(mode, B.N, nullptr, B.F(F_RHO), B.F(F_P), B.inst_of, B.d_mass, B.aux, ctx->stream);
                 r.baux = B.aux;
             } else {
                 r.baux = B.aux;
+            }
+            if (fp32 && (D.btype == BT_SYSTEM || D.btype == BT_STATIC)) {
+                TRY(ensure_fpk(ctx, B, B.N, B.nd + 3 + pk_ns));
+                launch_pack32(mode, B.N, nullptr, B.nd, B.kind >= GC_SYS_STRESS ? pk_ns : 0, B.F(F_V), B.F(F_RHO),
+                              B.F(F_P), B.F(F_STRESS), B.inst_of, B.d_mass, B.fpk, ctx->stream);
+                r.bfp = B.fpk;
             }
         }
     }
@@ -1352,6 +1419,9 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(S.d_inst);
         cudaFree(S.d_mass);
         cudaFree(S.d_c);
+        cudaFree(S.d_massf);
+        cudaFree(S.d_cf);
+        cudaFree(S.fpk);
         for (auto& ch : S.d_upd)
             for (auto* p : ch) cudaFree(p);
     }
@@ -1375,6 +1445,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(G.d_inst);
         cudaFree(G.d_mass);
         cudaFree(G.d_c);
+        cudaFree(G.fpk);
     }
     for (auto& D : ctx->inters) {
         cudaFree(D.d_gi);

@@ -17,8 +17,8 @@ constexpr int FORCE_BUF = 64;   // largest staged-neighbour column (shared memor
 struct ForceCfg {
     int minb, buf, unroll;
 };
-constexpr int NUM_FORCE_CFG = 4;
-constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1}, {4, 64, 2}, {6, 48, 2}, {8, 40, 1}};
+constexpr int NUM_FORCE_CFG = 2;
+constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1}, {4, 64, 2}};
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)
@@ -34,6 +34,7 @@ struct InterRef {
     const PfnInst* pi;    // per instance, this stage
     const int32_t* cs;    // packed CSR over system_b (global b indices)
     const double *bx, *bv, *brho, *bp, *bstress, *baux;
+    const float* bfp;     // FP32 pack of system_b (v, rho, aux, 1/rho, stress), planar
     int64_t bN;           // planar stride of system_b's arrays
     int32_t* counts;      // optional per-particle accepted-pair counts
 };
@@ -46,6 +47,10 @@ struct ForceArgs {
     double *advdt, *adrhodt, *asr, *avort;
     const double* a_c;     // per-instance sound speed
     const double* a_mass;  // per-instance particle mass
+    const float* a_cf;     // FP32 copies of the two above
+    const float* a_massf;
+    const float* afp;      // FP32 pack of system_a (FP32-compensated precision)
+    int prec;              // GC_PRECISION_*
     int* err;
     const int2* groups;        // warp groups (start, count) of system_a particles
     const int64_t* ngroups;    // device count of groups
@@ -62,5 +67,9 @@ void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs
                         int64_t ncols_cap, int2* groups, int64_t* ngroups, cudaStream_t s);
 void launch_aux(int mode, int64_t N, const int64_t* count, const double* rho, const double* p,
                 const int32_t* inst_of, const double* mass, double* aux, cudaStream_t s);
+// FP32 pack (planar, stride N): v[nd], rho, aux(mode), 1/rho, stress[ns] (ns may be 0).
+void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* v, const double* rho,
+                   const double* p, const double* stress, const int32_t* inst_of, const double* mass, float* pk,
+                   cudaStream_t s);
 
 }  // namespace gc

@@ -51,12 +51,15 @@ struct GridInst {
     // system_b wrapper parameters (src/BoundaryParticles.jl)
     double normal[MAXD], point[MAXD], beta, ljcut;
     double bmass, bc;                  // system_b mass and sound speed
+    // FP32 copies for the FP32-compensated sweep
+    float f_invH, f_knorm, f_normal[MAXD], f_beta, f_ljcut, f_bmass, f_bc;
 };
 
 // Per (interaction, stage, instance) functor parameters.
 struct PfnInst {
     double alpha, beta, h, delta;
     int S, has_delta;
+    float f_alpha, f_beta, f_h, f_h2eps, f_delta;  // FP32 copies; h2eps = 0.01·h²
 };
 
 // Per (ghost entry, instance) parameters.

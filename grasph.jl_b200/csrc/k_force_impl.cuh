@@ -1,4 +1,4 @@
-// k_force_impl.cuh — the fused pair sweep in the reference's FP64 arithmetic.
+// k_force_impl.cuh — the fused pair sweep (FP64 reference arithmetic and FP32-compensated).
 //
 // Gather formulation of src/Interaction.jl:393-732: one thread owns one
 // system_a particle and sums its side of every accepted pair of every
@@ -15,7 +15,8 @@
 // column of shared memory and processed in batches: the expensive pair
 // physics runs with every lane busy instead of diverging on rejections.
 //
-// Compiled with -fmad=false (reference rounding).
+// The FP64 policy relies on -fmad=false; the FP32 policy uses explicit
+// __dmul_rn/__dadd_rn for the exact acceptance test.
 #pragma once
 #include <cstdio>
 
@@ -267,41 +268,352 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
     return 1;
 }
 
+// ------------------------------------------------------------ policies
+// The candidate walk below is shared by two physics policies:
+//   PhysF64  the reference's FP64 expression trees (bit-identical pair terms)
+//   PhysF32  FP32 pair physics with Kahan-compensated per-particle sums
+// Both apply the exact FP64 acceptance test, so neighbour sets are identical.
+
+template <int ND, int NS, int PFN, int KK>
+struct PhysF64 {
+    struct Own {
+        OwnState<ND> o;
+        double sig[NS > 0 ? NS : 1];
+    };
+    using AccT = Acc<ND, NS>;
+    static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
+        const int64_t N = A.aN;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            w.o.x[d] = A.ax[d * N + gi];
+            w.o.v[d] = A.av[d * N + gi];
+        }
+        w.o.rho = A.arho[gi];
+        w.o.aux = A.aaux ? A.aaux[gi] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) w.sig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? A.astress[q * N + gi] : 0.0;
+    }
+    static __device__ __forceinline__ const double* xpos(const Own& w) { return w.o.x; }
+    static __device__ __forceinline__ void init(const ForceArgs& A, int64_t gi, AccT& acc, bool from_memory) {
+        const int64_t N = A.aN;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) acc.dv[d] = 0.0;
+        acc.dr = 0.0;
+        if (!from_memory) return;
+        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
+            acc.dr = A.adrhodt[gi];
+        } else {
+#pragma unroll
+            for (int q = 0; q < NS; ++q) acc.sr[q] = A.asr[q * N + gi];
+            if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+#pragma unroll
+                for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) acc.w[q] = A.avort[q * N + gi];
+            }
+        }
+    }
+    static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
+        const int64_t N = A.aN;
+        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
+            A.adrhodt[gi] = acc.dr;
+        } else {
+#pragma unroll
+            for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = acc.sr[q];
+            if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+#pragma unroll
+                for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) A.avort[q * N + gi] = acc.w[q];
+            }
+        }
+    }
+    static __device__ __forceinline__ double plane_da(const Own& w, const GridInst& G) {
+        double t[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) t[d] = w.o.x[d] - G.point[d];
+        return dotv<ND>(t, G.normal);
+    }
+    template <int P2>
+    static __device__ __forceinline__ int pair(const ForceArgs& A, const InterRef& r, const GridInst& G,
+                                               const PfnInst& P, int64_t gi, int k, const Own& w, double da,
+                                               int32_t j, AccT& acc) {
+        return process_pair<ND, NS, P2, KK>(A, r, G, P, gi, k, w.o, w.sig, da, j, acc);
+    }
+};
+
+// ---------------------------------------------------------------- FP32
+__device__ __forceinline__ void kadd(float& s, float& c, float x) {
+    // Kahan (compensated) summation: c carries the rounding error of s.
+    float y = x - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+template <int ND>
+__device__ __forceinline__ double dot_exact(const double* a, const double* b) {
+    double s = __dmul_rn(a[0], b[0]);
+#pragma unroll
+    for (int d = 1; d < ND; ++d) s = __dadd_rn(s, __dmul_rn(a[d], b[d]));
+    return s;
+}
+
+template <int ND>
+__device__ __forceinline__ float dotf(const float* a, const float* b) {
+    float s = a[0] * b[0];
+#pragma unroll
+    for (int d = 1; d < ND; ++d) s += a[d] * b[d];
+    return s;
+}
+
+template <int KK>
+__device__ __forceinline__ float kernel_dw_dq_f(float norm, float q) {
+    if (KK == GC_KERNEL_CUBIC_SPLINE) {
+        float a = fmaxf(0.f, 2.f - q), b = fmaxf(0.f, 1.f - q);
+        return norm * (-3.f * (0.25f * (a * a) - (b * b)));
+    } else {
+        float a = fmaxf(0.f, 2.f - q);
+        return ((-norm * 10.f) * q) * (a * a * a);
+    }
+}
+
+template <int ND, int NS, int PFN, int KK>
+struct PhysF32 {
+    struct Own {
+        double x[ND];
+        float v[ND];
+        float rho, aux, irho;
+        float sig[NS > 0 ? NS : 1];
+    };
+    struct AccT {
+        float dv[ND], cdv[ND];
+        float dr, cdr;
+        float sr[NS > 0 ? NS : 1], csr[NS > 0 ? NS : 1];
+        float w[3], cw[3];
+    };
+    static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
+        const int64_t N = A.aN;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            w.x[d] = A.ax[d * N + gi];
+            w.v[d] = A.afp[d * N + gi];
+        }
+        w.rho = A.afp[ND * N + gi];
+        w.aux = A.afp[(ND + 1) * N + gi];
+        w.irho = A.afp[(ND + 2) * N + gi];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) w.sig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? A.afp[(ND + 3 + q) * N + gi] : 0.f;
+    }
+    static __device__ __forceinline__ const double* xpos(const Own& w) { return w.x; }
+    static __device__ __forceinline__ void init(const ForceArgs&, int64_t, AccT& acc, bool) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) acc.dv[d] = acc.cdv[d] = 0.f;
+        acc.dr = acc.cdr = 0.f;
+#pragma unroll
+        for (int q = 0; q < (NS > 0 ? NS : 1); ++q) acc.sr[q] = acc.csr[q] = 0.f;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) acc.w[q] = acc.cw[q] = 0.f;
+    }
+    static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
+        // FP64 state += compensated FP32 sum (s − c)
+        const int64_t N = A.aN;
+        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d)
+                A.advdt[d * N + gi] = A.advdt[d * N + gi] + ((double)acc.dv[d] - (double)acc.cdv[d]);
+            A.adrhodt[gi] = A.adrhodt[gi] + ((double)acc.dr - (double)acc.cdr);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = A.asr[q * N + gi] + ((double)acc.sr[q] - (double)acc.csr[q]);
+            if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+#pragma unroll
+                for (int q = 0; q < (ND == 2 ? 1 : 3); ++q)
+                    A.avort[q * N + gi] = A.avort[q * N + gi] + ((double)acc.w[q] - (double)acc.cw[q]);
+            }
+        }
+    }
+    static __device__ __forceinline__ double plane_da(const Own& w, const GridInst& G) {
+        double t[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) t[d] = w.x[d] - G.point[d];
+        return dotv<ND>(t, G.normal);
+    }
+    template <int P2>
+    static __device__ __forceinline__ int pair(const ForceArgs& A, const InterRef& r, const GridInst& G,
+                                               const PfnInst& P, int64_t gi, int k, const Own& w, double da,
+                                               int32_t j, AccT& acc) {
+        const int64_t Nb = r.bN;
+        double dx[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], r.bx[d * Nb + j]);
+        const double rr = dot_exact<ND>(dx, dx);
+        if (!(rr < G.cutoff_sq)) return 0;
+        if (P2 == GC_PFN_COUNT) {
+            acc.dv[0] += 1.f;
+            acc.dr += 1.f;
+            return 1;
+        }
+        float dxf[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) dxf[d] = (float)dx[d];
+        const float rrf = (float)rr;
+        const float rinv = rsqrtf(rrf);
+        const float rf = rrf * rinv;
+        const float q = rf * G.f_invH;
+        const float gc = kernel_dw_dq_f<KK>(G.f_knorm, q) * G.f_invH * rinv;
+        float gx[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) gx[d] = gc * dxf[d];
+        const float ca = A.a_cf[k], ma = A.a_massf[k];
+
+        float vj[ND], rhoj, auxj, irhoj;
+        if (r.btype == BT_DYNAMIC) {
+            // src/PairwiseFunctors.jl:53,111,222,334: mirrored velocity, own density
+            float db = (float)da;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) db -= dxf[d] * G.f_normal[d];
+            const float m = -fminf(G.f_beta, fabsf(__fdividef(db, (float)da)));
+#pragma unroll
+            for (int d = 0; d < ND; ++d) vj[d] = m * w.v[d];
+            rhoj = w.rho;
+            auxj = w.aux;
+            irhoj = w.irho;
+        } else {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) vj[d] = r.bfp[d * Nb + j];
+            rhoj = r.bfp[ND * Nb + j];
+            auxj = r.bfp[(ND + 1) * Nb + j];
+            irhoj = r.bfp[(ND + 2) * Nb + j];
+        }
+        if (P2 == GC_PFN_STRAIN_RATE || P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
+            float dv[ND];
+#pragma unroll
+            for (int d = 0; d < ND; ++d) dv[d] = vj[d] - w.v[d];
+            const float f = r.btype == BT_DYNAMIC ? w.aux : auxj;  // mass / rho
+            float sr[NS > 0 ? NS : 1];
+            if (ND == 2) {
+                sr[0] = dv[0] * gx[0];
+                sr[1] = dv[1] * gx[1];
+                if (NS == 4) {
+                    sr[2] = 0.f;
+                    sr[3] = 0.5f * (dv[0] * gx[1] + dv[1] * gx[0]);
+                } else {
+                    sr[2] = 0.5f * (dv[0] * gx[1] + dv[1] * gx[0]);
+                }
+            } else {
+                sr[0] = dv[0] * gx[0];
+                sr[1] = dv[1] * gx[1];
+                sr[2] = dv[2] * gx[2];
+                sr[3] = 0.5f * (dv[0] * gx[1] + dv[1] * gx[0]);
+                sr[4] = 0.5f * (dv[0] * gx[2] + dv[2] * gx[0]);
+                sr[5] = 0.5f * (dv[1] * gx[2] + dv[2] * gx[1]);
+            }
+#pragma unroll
+            for (int q2 = 0; q2 < NS; ++q2) kadd(acc.sr[q2], acc.csr[q2], sr[q2] * f);
+            if (P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
+                kadd(acc.w[0], acc.cw[0], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f);
+                if (ND == 3) {
+                    kadd(acc.w[1], acc.cw[1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f);
+                    kadd(acc.w[2], acc.cw[2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f);
+                }
+            }
+            return 1;
+        }
+        // momentum + continuity (FluidPfn, CauchyFluidPfn)
+        float dv[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) dv[d] = w.v[d] - vj[d];
+        const bool self = r.btype == BT_SELF, dyn = r.btype == BT_DYNAMIC;
+        const float cb = (P2 == GC_PFN_CAUCHY_FLUID && r.btype == BT_GHOST) ? G.f_bc : ca;
+        float piv = 0.f;
+        const float vr = dotf<ND>(dxf, dv);
+        if (vr < 0.f) {
+            const float muv = __fdividef(P.f_h * vr, rrf + P.f_h2eps);
+            const float mc = 0.5f * (ca + cb);
+            piv = (P.f_beta * muv - P.f_alpha * mc) * muv * 2.f * w.irho * irhoj;
+        }
+        if (r.btype == BT_STATIC) {
+            const float x = G.f_ljcut * rinv, x2 = x * x, x6 = x2 * x2 * x2;
+            const float lj = rf < G.f_ljcut ? (x6 * x6 - x6) / rrf : 0.f;
+            const float rfj = (0.01f * ca) * ca * lj;
+            const float s = -G.f_bmass * piv;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], s * gx[d] + rfj * dxf[d]);
+            return 1;
+        }
+        const float mj = (self || dyn) ? ma : G.f_bmass;
+        if (P2 == GC_PFN_FLUID) {
+            const float dh = -(w.aux + auxj);
+            const float s = mj * (dh - piv);
+#pragma unroll
+            for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], s * gx[d]);
+        } else {
+            // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
+            float sj[NS > 0 ? NS : 1];
+#pragma unroll
+            for (int q2 = 0; q2 < NS; ++q2) sj[q2] = dyn ? w.sig[q2] : r.bfp[(ND + 3 + q2) * Nb + j];
+            const float ci = w.aux, cj = auxj;
+            float hv[ND];
+            if (ND == 2) {
+                constexpr int XY = NS == 3 ? 2 : 3;
+                hv[0] = (w.sig[0] * gx[0] + w.sig[XY] * gx[1]) * ci + (sj[0] * gx[0] + sj[XY] * gx[1]) * cj;
+                hv[1] = (w.sig[XY] * gx[0] + w.sig[1] * gx[1]) * ci + (sj[XY] * gx[0] + sj[1] * gx[1]) * cj;
+            } else {
+                hv[0] = (w.sig[0] * gx[0] + w.sig[3] * gx[1] + w.sig[4] * gx[2]) * ci +
+                        (sj[0] * gx[0] + sj[3] * gx[1] + sj[4] * gx[2]) * cj;
+                hv[1] = (w.sig[3] * gx[0] + w.sig[1] * gx[1] + w.sig[5] * gx[2]) * ci +
+                        (sj[3] * gx[0] + sj[1] * gx[1] + sj[5] * gx[2]) * cj;
+                hv[2] = (w.sig[4] * gx[0] + w.sig[5] * gx[1] + w.sig[2] * gx[2]) * ci +
+                        (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
+            }
+#pragma unroll
+            for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], mj * (hv[d] - piv * gx[d]));
+        }
+        float tail = 0.f;
+        if (P.has_delta) {
+            const float psi = 2.f * P.f_delta * ca * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
+            tail = psi * irhoj;
+        }
+        kadd(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail));
+        (void)gi;
+        return 1;
+    }
+};
+
 // ---------------------------------------------------------------- kernel
 // One warp owns one group: up to 32 consecutive (sorted) system_a particles
 // of one grid column (all cell coordinates but the last equal).  For each
 // 3-cell strip of the reference stencil the warp walks the union of its
 // lanes' candidate ranges — contiguous in the CSR because cells along the
 // last dimension are consecutive — loading 32 candidates at a time with one
-// coalesced load and broadcasting them by shuffles.  A lane accepts a
-// candidate only inside its own strip range [cs[z-1], cs[z+2]) and with
-// r² < (2h)², which is exactly the reference's pair test.  Accepted indices
-// go to the lane's shared-memory column; when any lane's column is nearly
-// full the whole warp evaluates its staged pairs, so the FP64 pair physics
-// runs on converged warps.
-template <int ND, int NS, int PFN, int KK, bool COUNT_ONLY, int UNROLL>
+// coalesced load and broadcasting them by shuffles.  A lane keeps a
+// candidate only inside its own strip range [cs[z-1], cs[z+2]) and when a
+// conservative FP32 distance test passes; the policy's pair() then applies
+// the exact reference test r² < (2h)² on FP64 positions.  Staged indices go
+// to the lane's shared-memory column; when any column is nearly full the
+// whole warp evaluates its staged pairs, so the pair physics runs on
+// converged warps.
+template <class Phys, bool COUNT_ONLY, int UNROLL, int PFN>
 __device__ __forceinline__ int flush_all(const ForceArgs& A, const InterRef& r, const GridInst& G,
-                                         const PfnInst& P, int64_t gi, int k, const OwnState<ND>& o,
-                                         const double* osig, double da, int nbuf, const int32_t* col, int BT,
-                                         Acc<ND, NS>& acc) {
+                                         const PfnInst& P, int64_t gi, int k, const typename Phys::Own& w,
+                                         double da, int nbuf, const int32_t* col, int BT, typename Phys::AccT& acc) {
+    constexpr int P2 = COUNT_ONLY ? GC_PFN_COUNT : PFN;
     int acc_n = 0;
     int t = 0;
     if (UNROLL == 2) {
-        // two independent pair evaluations in flight; their sums enter acc in order
         for (; t + 1 < nbuf; t += 2) {
             const int32_t j0 = col[t * BT], j1 = col[(t + 1) * BT];
-            acc_n += process_pair<ND, NS, (COUNT_ONLY ? GC_PFN_COUNT : PFN), KK>(A, r, G, P, gi, k, o, osig, da, j0, acc);
-            acc_n += process_pair<ND, NS, (COUNT_ONLY ? GC_PFN_COUNT : PFN), KK>(A, r, G, P, gi, k, o, osig, da, j1, acc);
+            acc_n += Phys::template pair<P2>(A, r, G, P, gi, k, w, da, j0, acc);
+            acc_n += Phys::template pair<P2>(A, r, G, P, gi, k, w, da, j1, acc);
         }
     }
-    for (; t < nbuf; ++t)
-        acc_n += process_pair<ND, NS, (COUNT_ONLY ? GC_PFN_COUNT : PFN), KK>(A, r, G, P, gi, k, o, osig, da,
-                                                                            col[t * BT], acc);
+    for (; t < nbuf; ++t) acc_n += Phys::template pair<P2>(A, r, G, P, gi, k, w, da, col[t * BT], acc);
     return acc_n;
 }
 
-template <int ND, int NS, int PFN, int KK, bool COUNT_ONLY, int MINB, int BUF, int UNROLL>
-__global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
+template <class Phys, int ND, int PFN, bool COUNT_ONLY, int MINB, int BUF, int UNROLL>
+__global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     extern __shared__ int32_t sbuf[];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -310,43 +622,16 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
     int32_t* col = sbuf + tid;
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t N = A.aN;
-    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ngroups; w += nwarps) {
-        const int2 grp = A.groups[w];
+    for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
+        const int2 grp = A.groups[wg];
         const bool active = lane < grp.y;
         const int64_t gi = (int64_t)grp.x + (active ? lane : 0);
         const int k = A.a_inst_of[gi];
-
-        OwnState<ND> o;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-            o.x[d] = A.ax[d * N + gi];
-            o.v[d] = A.av[d * N + gi];
-        }
-        o.rho = A.arho[gi];
-        o.aux = A.aaux ? A.aaux[gi] : 0.0;
-        double osig[NS > 0 ? NS : 1];
-#pragma unroll
-        for (int q = 0; q < NS; ++q) osig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? A.astress[q * N + gi] : 0.0;
-
-        Acc<ND, NS> acc;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) acc.dv[d] = 0.0;
-        acc.dr = 0.0;
-        if (!COUNT_ONLY) {
-            if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
-#pragma unroll
-                for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
-                acc.dr = A.adrhodt[gi];
-            } else {
-#pragma unroll
-                for (int q = 0; q < NS; ++q) acc.sr[q] = A.asr[q * N + gi];
-                if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
-#pragma unroll
-                    for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) acc.w[q] = A.avort[q * N + gi];
-                }
-            }
-        }
+        typename Phys::Own w;
+        Phys::load(A, gi, w);
+        const double* ox = Phys::xpos(w);
+        typename Phys::AccT acc;
+        Phys::init(A, gi, acc, !COUNT_ONLY);
 
         for (int ri = 0; ri < A.nref; ++ri) {
             const InterRef& r = A.ref[ri];
@@ -359,7 +644,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
                 bool near = B.n > 0;
                 const double m = 1.001 * G.cell;
 #pragma unroll
-                for (int d = 0; d < ND; ++d) near = near && o.x[d] >= B.bbmin[d] - m && o.x[d] <= B.bbmax[d] + m;
+                for (int d = 0; d < ND; ++d) near = near && ox[d] >= B.bbmin[d] - m && ox[d] <= B.bbmax[d] + m;
                 if (!__any_sync(FULL, active && near)) {
                     if (active && r.counts) r.counts[gi] = 0;
                     continue;
@@ -369,23 +654,17 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
             bool ok = true;
 #pragma unroll
             for (int d = 0; d < ND; ++d)
-                if (!floor_i64((o.x[d] - G.ming[d]) / G.cell, &c[d]) || c[d] < 1 || c[d] >= G.ng[d] - 1) ok = false;
+                if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &c[d]) || c[d] < 1 || c[d] >= G.ng[d] - 1)
+                    ok = false;
             if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
-            double da = 0.0;
-            if (r.btype == BT_DYNAMIC) {
-                double t[ND];
-#pragma unroll
-                for (int d = 0; d < ND; ++d) t[d] = o.x[d] - G.point[d];
-                da = dotv<ND>(t, G.normal);
-            }
+            const double da = r.btype == BT_DYNAMIC ? Phys::plane_da(w, G) : 0.0;
             const int64_t Nb = r.bN;
             const bool self = r.btype == BT_SELF;
             int nbuf = 0;
             int32_t accepted = 0;
-            // column of lane 0; the cooperative walk needs every active lane in it
-            int64_t c0 = __shfl_sync(FULL, c[0], 0);
-            int64_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
-            bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
+            const int64_t c0 = __shfl_sync(FULL, c[0], 0);
+            const int64_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
+            const bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
             const bool coop = __all_sync(FULL, !active || same);
             if (coop) {
                 constexpr int L = ND - 1;  // last dimension
@@ -403,8 +682,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
                 float xi_f[ND];
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
-                    xref[d] = __shfl_sync(FULL, o.x[d], 0);
-                    xi_f[d] = (float)(o.x[d] - xref[d]);
+                    xref[d] = __shfl_sync(FULL, ox[d], 0);
+                    xi_f[d] = (float)(ox[d] - xref[d]);
                 }
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
                 const int64_t ngl = G.ng[L];
@@ -418,8 +697,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
                     const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
                     for (int32_t ch = u0; ch < u1; ch += 32) {
                         if (__any_sync(FULL, nbuf > BUF - 32)) {
-                            accepted += flush_all<ND, NS, PFN, KK, COUNT_ONLY, UNROLL>(A, r, G, P, gi, k, o, osig, da,
-                                                                                      nbuf, col, BT, acc);
+                            accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
+                                                                                 BT, acc);
                             nbuf = 0;
                             __syncwarp();
                         }
@@ -428,6 +707,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
 #pragma unroll
                         for (int d = 0; d < ND; ++d) xj[d] = jl < u1 ? (float)(r.bx[d * Nb + jl] - xref[d]) : 0.0f;
                         const int m = u1 - ch < 32 ? (int)(u1 - ch) : 32;
+#pragma unroll 4
                         for (int t = 0; t < m; ++t) {
                             float rr = 0.0f;
 #pragma unroll
@@ -441,8 +721,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
                         }
                     }
                 }
-                accepted += flush_all<ND, NS, PFN, KK, COUNT_ONLY, UNROLL>(A, r, G, P, gi, k, o, osig, da, nbuf,
-                                                                          col, BT, acc);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
                 __syncwarp();
             } else if (active && ok) {
@@ -457,40 +736,25 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_force(ForceArgs A) {
                         if (self && j == gi) continue;
                         col[(nbuf++) * BT] = j;
                         if (nbuf == BUF) {
-                            accepted += flush_all<ND, NS, PFN, KK, COUNT_ONLY, UNROLL>(A, r, G, P, gi, k, o, osig, da,
-                                                                                      nbuf, col, BT, acc);
+                            accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
+                                                                                 BT, acc);
                             nbuf = 0;
                         }
                     }
                 }
-                accepted += flush_all<ND, NS, PFN, KK, COUNT_ONLY, UNROLL>(A, r, G, P, gi, k, o, osig, da, nbuf, col,
-                                                                          BT, acc);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
             }
             __syncwarp();
             if (active && r.counts) r.counts[gi] = accepted;
         }
-
-        if (!COUNT_ONLY && active) {
-            if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
-#pragma unroll
-                for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
-                A.adrhodt[gi] = acc.dr;
-            } else {
-#pragma unroll
-                for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = acc.sr[q];
-                if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
-#pragma unroll
-                    for (int q = 0; q < (ND == 2 ? 1 : 3); ++q) A.avort[q * N + gi] = acc.w[q];
-                }
-            }
-        }
+        if (!COUNT_ONLY && active) Phys::store(A, gi, acc);
         __syncwarp();
     }
 }
 
 // ------------------------------------------------------------ dispatch
-template <int ND, int NS, int PFN, int KK, int C>
+template <class Phys, int ND, int PFN, int C>
 static void launch_c(const ForceArgs& A, cudaStream_t s) {
     constexpr ForceCfg cf = FORCE_CFGS[C];
     int64_t warps = A.aN;
@@ -498,27 +762,25 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
     size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t);
-    k_force<ND, NS, PFN, KK, false, cf.minb, cf.buf, cf.unroll><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
+    k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
 }
 
 template <int ND, int NS, int PFN, int KK>
 static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
-    // grid-stride over groups; at most one group per particle
+    using P64 = PhysF64<ND, NS, PFN, KK>;
+    using P32 = PhysF32<ND, NS, PFN, KK>;
     if (count_only) {
         int64_t blocks = (A.aN * 32 + FORCE_TPB - 1) / FORCE_TPB;
         if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
         if (blocks < 1) blocks = 1;
         size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t);
-        k_force<ND, NS, PFN, KK, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
-    } else if (KK != GC_KERNEL_CUBIC_SPLINE || PFN == GC_PFN_COUNT) {
-        launch_c<ND, NS, PFN, KK, 0>(A, s);
+        k_sweep<P64, ND, PFN, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
+    } else if (A.prec == GC_PRECISION_FP32_COMPENSATED && PFN != GC_PFN_COUNT) {
+        if (A.cfg == 1) launch_c<P32, ND, PFN, 1>(A, s);
+        else launch_c<P32, ND, PFN, 0>(A, s);
     } else {
-        switch (A.cfg) {
-            case 1: launch_c<ND, NS, PFN, KK, 1>(A, s); break;
-            case 2: launch_c<ND, NS, PFN, KK, 2>(A, s); break;
-            case 3: launch_c<ND, NS, PFN, KK, 3>(A, s); break;
-            default: launch_c<ND, NS, PFN, KK, 0>(A, s); break;
-        }
+        if (A.cfg == 1 && KK == GC_KERNEL_CUBIC_SPLINE) launch_c<P64, ND, PFN, 1>(A, s);
+        else launch_c<P64, ND, PFN, 0>(A, s);
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }

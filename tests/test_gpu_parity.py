@@ -180,3 +180,32 @@ def test_nonfinite_position_reports_error():
     with pytest.raises(G.GcError) as ei:
         s.step(1, 0.1)
     assert ei.value.status == G.consts.GC_ERR_NONFINITE
+
+
+# ------------------------------------------------ FP32-compensated precision
+# The FP32-compensated sweep keeps the exact FP64 neighbour test (identical
+# pair sets) and FP64 state; pair terms are FP32 with Kahan-compensated sums.
+FP32C_ONE_STEP_TOL = 2e-5    # of each field's scale, after one step
+FP32C_MULTI_STEP_TOL = 1e-4  # after 20 steps
+
+
+def _pair_prec(builder, prec, **kw):
+    lf_g, meta = builder(**kw)
+    lf_c, _ = builder(**kw)
+    g = G.Session([lf_g], backend=make_backend("cuda"), precision=prec)
+    c = G.Session([lf_c], backend=make_backend("oracle"))
+    g.push()
+    c.push()
+    return lf_g, lf_c, g, c, meta
+
+
+@pytest.mark.parametrize("case", list(SMALL))
+@pytest.mark.parametrize("nsteps,tol", [(1, FP32C_ONE_STEP_TOL), (20, FP32C_MULTI_STEP_TOL)])
+def test_fp32_compensated_against_fp64_oracle(case, nsteps, tol):
+    builder, kw = SMALL[case]
+    lf_g, lf_c, g, c, meta = _pair_prec(builder, G.PRECISION_FP32_COMPENSATED, **kw)
+    g.step(nsteps, meta["cfl"])
+    c.step(nsteps, meta["cfl"])
+    g.pull()
+    c.pull()
+    _compare_systems(lf_g, lf_c, tol, exact_ids=(nsteps == 1))
