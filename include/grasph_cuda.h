@@ -263,6 +263,27 @@ int gc_update_state(gc_ctx* ctx, int inst, int sys, int stage, double dt);
  * grid of the last gc_build_grid / gc_step (n_a int32 values).             */
 int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, int64_t n);
 
+/* ============================================= allocation-free variant */
+/* No counterpart in the reference.  The stable cell-key sort permutation of
+ * gc_sort_system for callers that cannot call cudaMalloc — hosts whose
+ * device memory is handed in full to their own pool allocator, and
+ * latency-critical loops that cannot afford cudaMalloc/cudaFree's implicit
+ * device synchronisation.  It allocates nothing: its scratch is a fixed
+ * static device array (about 2 MB, held by every GPU that loads the library
+ * until exit), so n is limited to 65536 particles and the key lattice's
+ * bounding box to 131072 cells (GC_ERR_CAPACITY beyond either).
+ * x_planar: device array, ndims×n doubles, component-major (x of all
+ * particles, then y, ...).  perm_out: device array of n int32 receiving the
+ * 0-based source index of each sorted position (the order of
+ * `sort_particles!`, src/Sorting.jl:157, for keys floor(x_d/cutoff)).
+ * stream: a cudaStream_t (NULL for the default stream); the call returns
+ * after the stream has finished its work.  The first call on each device
+ * resolves the scratch array's device address and should come before any
+ * stream capture.  Calls share the scratch array; calls that overlap on the
+ * GPU race on it.                                                          */
+int gc_cell_sort_perm_noalloc(const double* x_planar, int64_t n, int ndims, double cutoff,
+                              int32_t* perm_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
