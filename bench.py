@@ -2,10 +2,14 @@
 
 Default workload: the 3-D dam break of 1,000,000 fluid particles (100×50×200
 at dx = 0.01 m) in a 4.0×1.0×4.0 m tank with 3-layer dynamic walls on all
-six faces (1,472,616 boundary particles), FP64, synthetic inputs generated
-by grasph_b200.scenarios (hydrostatic initial density).
+six faces (1,472,616 boundary particles), synthetic inputs generated by
+grasph_b200.scenarios (hydrostatic initial density), FP32-compensated sweep.
+The same workload is then run in the plain FP64 path for the same number of
+steps: `fp64_plain` gives its rate and the compensated run's largest error
+against it (density, velocity, acceleration, stress).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload dambreak_3d|dambreak_2d|column] [--precision fp32c|fp64]
 
 Prints one JSON line (rank 0).  `value` counts fluid particle-steps per
 second over all ranks with state resident in HBM; `e2e` measures the same
@@ -39,6 +43,9 @@ SWEEP_BYTES_PER_PARTICLE = {2: 16 + 16 + 8 + 8 + 16 + 8, 3: 24 + 24 + 8 + 8 + 24
 # (kernel + geometry ≈ 20, artificial viscosity, pressure, momentum and
 # continuity terms; FMA counted as 2, division and sqrt as 1).
 FLUID_PAIR_FLOPS = {2: 70, 3: 86}
+# DRAM bytes (read + write) of one sweep launch from an ncu capture, keyed by
+# (workload, scale, precision); the profiles/ summaries give the commands.
+TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 121.48e6}
 
 
 def build_workload(name, scale):
@@ -76,10 +83,18 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait for its first row so the
+        # samples cover the timed region
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
@@ -173,6 +188,70 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _timed_steps(sess, meta, args, lib, be, stream, dist, sample_clocks, local_rank):
+    """Warm-up, then exactly args.steps timed steps between barriers."""
+    import torch
+    sess.step(args.warmup, meta["cfl"])
+    lib.gc_set_profiling(be.ctx, 1)
+    st0 = be.stats()
+    clocks = ClockSampler(local_rank) if sample_clocks else None
+    if clocks:
+        clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sess.step(args.steps, meta["cfl"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    ms = e0.elapsed_time(e1)
+    st1 = be.stats()
+    lib.gc_set_profiling(be.ctx, 0)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, st0, st1, clk
+
+
+def _open(lf, local_rank, prec):
+    import torch
+    import grasph_b200 as G
+    from grasph_b200 import engine
+    sess = G.Session([lf], device=local_rank, precision=prec)
+    be = sess.backend
+    lib = be.lib
+    sess.push()
+    sptr = engine.ct.c_void_p()
+    lib.gc_stream.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_void_p)]
+    lib.gc_stream(be.ctx, engine.ct.byref(sptr))
+    lib.gc_set_profiling.argtypes = [engine.ct.c_void_p, engine.ct.c_int]
+    return sess, be, lib, torch.cuda.ExternalStream(sptr.value)
+
+
+def _rel_errors(lf_a, lf_b):
+    """Largest per-particle error of each field relative to the field's scale
+    (the FP64 run's largest magnitude), over the fluid/soil systems."""
+    out = {}
+    for sa, sb in zip(lf_a.systems, lf_b.systems):
+        ia, ib = np.argsort(sa.id), np.argsort(sb.id)
+        for name in ("rho", "v", "dvdt", "stress"):
+            if not hasattr(sa, name):
+                continue
+            a = np.asarray(getattr(sa, name))[ia]
+            b = np.asarray(getattr(sb, name))[ib]
+            scale = float(np.abs(b).max())
+            if scale == 0.0:
+                continue
+            out[name] = max(out.get(name, 0.0), float(np.abs(a - b).max() / scale))
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import grasph_b200 as G
@@ -186,49 +265,33 @@ def run_ours(args, rank, world, local_rank):
     lf, meta = build_workload(args.workload, args.scale)
     nd = meta["ndims"]
     prec = G.PRECISION_FP64 if args.precision == "fp64" else G.PRECISION_FP32_COMPENSATED
-    sess = G.Session([lf], device=local_rank, precision=prec)
-    be = sess.backend
-    lib = be.lib
-    sess.push()
+    sess, be, lib, stream = _open(lf, local_rank, prec)
     peak = engine.ct.c_double()
     lib.gc_measure_fp64_peak.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_double)]
     lib.gc_measure_fp64_peak(be.ctx, engine.ct.byref(peak))
-    sess.step(args.warmup, meta["cfl"])
-    sptr = engine.ct.c_void_p()
-    lib.gc_stream.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_void_p)]
-    lib.gc_stream(be.ctx, engine.ct.byref(sptr))
-    stream = torch.cuda.ExternalStream(sptr.value)
-    lib.gc_set_profiling.argtypes = [engine.ct.c_void_p, engine.ct.c_int]
-    lib.gc_set_profiling(be.ctx, 1)
-    st0 = be.stats()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    sess.step(args.steps, meta["cfl"])
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    st1 = be.stats()
-    lib.gc_set_profiling(be.ctx, 0)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms, st0, st1, clk = _timed_steps(sess, meta, args, lib, be, stream, dist, True, local_rank)
     launches = st1["kernel_launches"] - st0["kernel_launches"]
-    sweep_ms = st1["sweep_ms"]
-    sweep_launches = max(1, st1["sweep_launches"])
+    sweep_ms = st1["sweep_ms"] - st0["sweep_ms"]
+    sweep_launches = max(1, st1["sweep_launches"] - st0["sweep_launches"])
     pairs = st1["pairs_last_step"]
     n_fluid = meta["n_fluid"]
     value = n_fluid * args.steps / (ms / 1e3) * world
     pair_rate = pairs * args.steps / (ms / 1e3) * world
+
+    # the plain FP64 path on the same workload and step count, and the
+    # FP32-compensated run's error against it
+    fp64 = None
+    if prec != G.PRECISION_FP64 and not args.no_fp64_compare:
+        lf64, _ = build_workload(args.workload, args.scale)
+        s64, be64, lib64, stream64 = _open(lf64, local_rank, G.PRECISION_FP64)
+        ms64, _, _, _ = _timed_steps(s64, meta, args, lib64, be64, stream64, dist, False, local_rank)
+        sess.pull()
+        s64.pull()
+        fp64 = {"value": n_fluid * args.steps / (ms64 / 1e3) * world, "ms_per_step": ms64 / args.steps,
+                "speedup": ms64 / ms,
+                "rel_error_after_steps": args.warmup + args.steps,
+                "rel_error": _rel_errors(lf, lf64)}
+        s64.close()
 
     # end to end through the host API: pinned host buffers in and out per step
     e2e = None
@@ -267,11 +330,12 @@ def run_ours(args, rank, world, local_rank):
     achieved_gbs = per_launch_bytes / sweep_avg_s / 1e9
     flops_per_launch = pairs * FLUID_PAIR_FLOPS[nd]
     achieved_tflops = flops_per_launch / sweep_avg_s / 1e12
-    roof = {"kernel": "k_force (fused FP64 pair sweep)", "bound": "hbm", "achieved": achieved_gbs,
+    roof = {"kernel": "k_sweep (fused pair sweep)", "bound": "hbm", "achieved": achieved_gbs,
             "peak": hbm_peak, "peak_source": src, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
-            "traffic": None, "bytes_per_launch": per_launch_bytes,
-            "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": (sweep_ms / args.steps) / (ms / args.steps),
-            "compute": {"bound": "fp64", "achieved": achieved_tflops, "peak": peak.value,
+            "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, args.scale, args.precision)),
+            "bytes_per_launch": per_launch_bytes,
+            "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_ms / ms,
+            "compute": {"bound": "fp64 pipe", "achieved": achieved_tflops, "peak": peak.value,
                         "peak_source": "measured FP64 FMA issue rate (gc_measure_fp64_peak)",
                         "unit": "TFLOP/s", "frac": achieved_tflops / peak.value,
                         "flops_per_launch": flops_per_launch}}
@@ -291,6 +355,7 @@ def run_ours(args, rank, world, local_rank):
                        precision=args.precision),
         "pair_interactions_per_s": pair_rate, "pairs_per_step": pairs,
         "gpu_launches": launches, "clocks": clk, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
+        "fp64_plain": fp64,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -300,12 +365,13 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column"])
     ap.add_argument("--scale", default="full", choices=["full", "small"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp64", "fp32c"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
