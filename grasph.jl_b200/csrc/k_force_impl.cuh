@@ -620,6 +620,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     const int tid = threadIdx.x;
     const int BT = blockDim.x;
     int32_t* col = sbuf + tid;
+    // per-warp candidate coordinates, ND rows of 32 floats, after the columns
+    float* cand = reinterpret_cast<float*>(sbuf + BUF * FORCE_TPB) + (tid >> 5) * (ND * 32);
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
@@ -678,14 +680,17 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                 // Conservative FP32 prefilter in coordinates relative to lane 0:
                 // |rel| spans a few cells, so single-precision rounding moves r²
                 // by < 1e-5 relative; the 1e-3 margin keeps every true pair.
+                // Inactive lanes test against NaN and so accept nothing.
                 double xref[ND];
-                float xi_f[ND];
+                float2 xi2[ND];
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
                     xref[d] = __shfl_sync(FULL, ox[d], 0);
-                    xi_f[d] = (float)(ox[d] - xref[d]);
+                    const float xi = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
+                    xi2[d] = make_float2(xi, xi);
                 }
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
+                const float2 neg1 = make_float2(-1.0f, -1.0f);
                 const int64_t ngl = G.ng[L];
                 const int nstrips = ND == 2 ? 3 : 9;
                 for (int sidx = 0; sidx < nstrips; ++sidx) {
@@ -702,23 +707,52 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                             nbuf = 0;
                             __syncwarp();
                         }
+                        // 32 candidates, coordinates relative to lane 0, staged in
+                        // shared memory (beyond the range: far away)
                         const int32_t jl = ch + lane;
-                        float xj[ND];
 #pragma unroll
-                        for (int d = 0; d < ND; ++d) xj[d] = jl < u1 ? (float)(r.bx[d * Nb + jl] - xref[d]) : 0.0f;
-                        const int m = u1 - ch < 32 ? (int)(u1 - ch) : 32;
-#pragma unroll 4
-                        for (int t = 0; t < m; ++t) {
-                            float rr = 0.0f;
-#pragma unroll
-                            for (int d = 0; d < ND; ++d) {
-                                float dd = xi_f[d] - __shfl_sync(FULL, xj[d], t);
-                                rr += dd * dd;
-                            }
-                            const int32_t jt = ch + t;
-                            if (active && jt >= lo && jt < hi && !(self && jt == gi) && rr < cut_f)
-                                col[(nbuf++) * BT] = jt;
+                        for (int d = 0; d < ND; ++d)
+                            cand[d * 32 + lane] = jl < u1 ? (float)(r.bx[d * Nb + jl] - xref[d]) : 1e30f;
+                        __syncwarp();
+                        // this lane's own strip range and the self pair, as a mask
+                        // over the batch's 32 positions
+                        const int32_t tlo = lo - ch, thi = hi - ch;
+                        unsigned allow = tlo <= 0 ? 0xffffffffu : (tlo >= 32 ? 0u : 0xffffffffu << tlo);
+                        allow &= thi >= 32 ? 0xffffffffu : (thi <= 0 ? 0u : 0xffffffffu >> (32 - thi));
+                        if (self) {
+                            const int64_t ts = gi - ch;
+                            if (ts >= 0 && ts < 32) allow &= ~(1u << ts);
                         }
+                        const int m = u1 - ch < 32 ? (int)(u1 - ch) : 32;
+                        unsigned hits = 0;
+                        for (int t0 = 0; t0 < m; t0 += 8) {
+                            unsigned h8 = 0;
+#pragma unroll
+                            for (int t = 0; t < 8; t += 2) {
+                                float2 rr;
+                                {
+                                    const float2 xj = *reinterpret_cast<const float2*>(cand + t0 + t);
+                                    const float2 dd = __ffma2_rn(xj, neg1, xi2[0]);
+                                    rr = __fmul2_rn(dd, dd);
+                                }
+#pragma unroll
+                                for (int d = 1; d < ND; ++d) {
+                                    const float2 xj = *reinterpret_cast<const float2*>(cand + d * 32 + t0 + t);
+                                    const float2 dd = __ffma2_rn(xj, neg1, xi2[d]);
+                                    rr = __ffma2_rn(dd, dd, rr);
+                                }
+                                if (rr.x < cut_f) h8 |= 1u << t;
+                                if (rr.y < cut_f) h8 |= 2u << t;
+                            }
+                            hits |= h8 << t0;
+                        }
+                        hits &= allow;
+                        while (hits) {
+                            const int t = __ffs(hits) - 1;
+                            hits &= hits - 1;
+                            col[(nbuf++) * BT] = ch + t;
+                        }
+                        __syncwarp();
                     }
                 }
                 accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
@@ -761,7 +795,7 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     int64_t blocks = (warps * 32 + FORCE_TPB - 1) / FORCE_TPB;
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
-    size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t);
+    size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
     k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
 }
 
@@ -773,7 +807,7 @@ static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
         int64_t blocks = (A.aN * 32 + FORCE_TPB - 1) / FORCE_TPB;
         if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
         if (blocks < 1) blocks = 1;
-        size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t);
+        size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
         k_sweep<P64, ND, PFN, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
     } else if (A.prec == GC_PRECISION_FP32_COMPENSATED && PFN != GC_PFN_COUNT) {
         if (A.cfg == 1) launch_c<P32, ND, PFN, 1>(A, s);
