@@ -362,13 +362,94 @@ def run_ours(args, rank, world, local_rank):
     sess.close()
 
 
+def run_batched(args, rank, world, local_rank):
+    """256 column collapses stepped together (FP32-compensated), against the
+    same instances stepped one at a time in the plain FP64 path."""
+    import torch
+    import grasph_b200 as G
+    from grasph_b200 import scenarios
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+    count = 256 if args.scale == "full" else 32
+    mix = scenarios.batched_columns(count=count)
+    n_tot = sum(m["n_fluid"] for _, m in mix)
+    cfl = mix[0][1]["cfl"]
+    meta = {"cfl": cfl}
+    prec = G.PRECISION_FP64 if args.precision == "fp64" else G.PRECISION_FP32_COMPENSATED
+    lfs = [lf for lf, _ in mix]
+    sess = G.Session(lfs, device=local_rank, precision=prec)
+    be, lib = sess.backend, sess.backend.lib
+    sess.push()
+    from grasph_b200 import engine
+    sptr = engine.ct.c_void_p()
+    lib.gc_stream.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_void_p)]
+    lib.gc_stream(be.ctx, engine.ct.byref(sptr))
+    lib.gc_set_profiling.argtypes = [engine.ct.c_void_p, engine.ct.c_int]
+    stream = torch.cuda.ExternalStream(sptr.value)
+    ms, st0, st1, clk = _timed_steps(sess, meta, args, lib, be, stream, dist, True, local_rank)
+    value = n_tot * args.steps / (ms / 1e3) * world
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+    sweep_ms = st1["sweep_ms"] - st0["sweep_ms"]
+    sweep_launches = max(1, st1["sweep_launches"] - st0["sweep_launches"])
+
+    # one at a time, plain FP64: a size-stratified sample of the instances,
+    # each timed alone; time per step is fitted as a + b·n over the sample
+    # and summed over all instances
+    one = None
+    if not args.no_fp64_compare:
+        order = np.argsort([m["n_fluid"] for _, m in mix])
+        pick = [int(order[int(round(q * (len(order) - 1)))]) for q in np.linspace(0.0, 1.0, 8)]
+        ns, tms = [], []
+        sample_steps = max(10, min(args.steps, 100))
+        a2 = argparse.Namespace(**vars(args))
+        a2.steps = sample_steps
+        for k in pick:
+            lf1, m1 = scenarios.batched_columns(count=count)[k]
+            s1 = G.Session([lf1], device=local_rank, precision=G.PRECISION_FP64)
+            s1.push()
+            lib.gc_stream(s1.backend.ctx, engine.ct.byref(sptr))
+            st = torch.cuda.ExternalStream(sptr.value)
+            t1, _, _, _ = _timed_steps(s1, m1, a2, lib, s1.backend, st, dist, False, local_rank)
+            ns.append(m1["n_fluid"])
+            tms.append(t1 / sample_steps)
+            s1.close()
+        b, a = np.polyfit(np.array(ns, float), np.array(tms, float), 1)
+        total_ms = float(sum(a + b * m["n_fluid"] for _, m in mix))
+        v1 = n_tot / (total_ms / 1e3)
+        one = {"value": v1, "unit": "particle-steps/s", "speedup": value / v1,
+               "ms_per_step_all_instances": total_ms,
+               "sample": f"{len(pick)} instances (size quantiles), {sample_steps} steps each after "
+                         f"{args.warmup} warm-up steps; time per step fitted as a + b*n "
+                         f"(a={a:.4f} ms, b={b * 1e6:.4f} ms per 1e6 particles) and summed"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == G.PRECISION_FP64 else "f32-compensated",
+        "data": "synthetic",
+        "config": {"workload": f"batched_columns x{count}", "n_fluid": n_tot, "instances": count,
+                   "ndims": 2, "parallelism": f"replicas x{world}", "l2": "state larger than L2",
+                   "precision": args.precision},
+        "gpu_launches": launches, "clocks": clk, "e2e": None,
+        "sweep": {"avg_launch_ms": sweep_ms / sweep_launches, "share_of_step": sweep_ms / ms},
+        "one_by_one_fp64": one, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sess.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column"])
+    ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column", "batched"])
     ap.add_argument("--scale", default="full", choices=["full", "small"])
     ap.add_argument("--precision", default="fp32c", choices=["fp64", "fp32c"])
     ap.add_argument("--no-fp64-compare", action="store_true")
@@ -389,7 +470,10 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    run_ours(args, rank, world, local_rank)
+    if args.workload == "batched":
+        run_batched(args, rank, world, local_rank)
+    else:
+        run_ours(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
