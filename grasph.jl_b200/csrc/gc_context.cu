@@ -148,6 +148,26 @@ struct DInter {
     int64_t csa_ver = -1;   // grid version cs_a was built for
 };
 
+// One captured step: valid for the buffer parities `pre` (cur of every slot,
+// then of every ghost), leaves them at `post`.
+struct StepGraph {
+    std::vector<char> pre, post;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;  // kernels per replay
+    // event-record nodes of the sweep timers: (node, pair index, 0 start / 1 end)
+    std::vector<std::array<int64_t, 2>> ev_slots;
+    std::vector<cudaGraphNode_t> ev_nodes;
+};
+
+// Copy of the carried state of a moving slot at the last verified step.
+struct Snapshot {
+    double* f[NF] = {};
+    int32_t* id = nullptr;
+    int cur = 0;
+    int64_t n = 0;  // particles copied (capacity of the buffers)
+};
+
 }  // namespace
 
 struct gc_ctx {
@@ -188,9 +208,32 @@ struct gc_ctx {
     double sweep_ms = 0;
     int64_t sweep_launches = 0;
     unsigned long long* d_pairs = nullptr;
+    // graph stepping: steps sized from capacities (no host read per step),
+    // captured once per buffer parity and replayed; verified every
+    // `sync_every` steps against a snapshot, rolled back and re-run exactly
+    // when a capacity was exceeded
+    bool graphs_on = true;
+    int sync_every = 32;
+    double cap_margin = 1.5;       // capacity = margin × largest need seen
+    bool capmode = false;          // current step sized from capacities
+    bool capturing = false;        // no allocation may happen
+    bool exact_done = false;       // an exact step ran since the last change
+    int64_t alloc_epoch = 0;       // bumps at every (re)allocation
+    int64_t graphs_epoch = -1;     // alloc_epoch the graphs were captured at
+    int graphs_key = -1;           // precision/config/profiling the graphs saw
+    std::vector<StepGraph> graphs;
+    std::vector<int64_t> need_max;  // per plan entry, largest need seen
+    int64_t* d_need_max = nullptr;
+    int64_t* h_need_max = nullptr;  // pinned
+    int64_t* d_need_cap = nullptr;  // per plan entry, the cells capacity mode sizes for
+    std::vector<Snapshot> snaps;    // per slot (moving slots only)
+    int64_t graph_steps = 0, rollbacks = 0;
 };
 
 namespace {
+
+void drop_graphs(gc_ctx* ctx);
+void invalidate_steps(gc_ctx* ctx);
 
 // ---------------------------------------------------------------- errors
 int seterr(gc_ctx* c, int code, const char* fmt, ...) {
@@ -229,6 +272,8 @@ int hcopy(gc_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind 
 
 template <class T>
 int dalloc(gc_ctx* ctx, T** p, size_t count) {
+    if (ctx->capturing) return seterr(ctx, GC_ERR_STATE, "allocation inside a step capture");
+    ctx->alloc_epoch++;
     size_t bytes = count * sizeof(T);
     if (bytes == 0) bytes = 16;
     if (ctx->budget && ctx->allocated + bytes > ctx->budget)
@@ -245,6 +290,7 @@ int dalloc(gc_ctx* ctx, T** p, size_t count) {
 template <class T>
 void dfree(gc_ctx* ctx, T*& p, size_t count) {
     if (p) {
+        ctx->alloc_epoch++;
         cudaFree(p);
         size_t bytes = count * sizeof(T);
         ctx->allocated -= std::min(ctx->allocated, bytes ? bytes : 16);
@@ -675,6 +721,10 @@ int finalize(gc_ctx* ctx) {
     ctx->nneed = (int)(ctx->slots.size() + ctx->ghosts.size() + ctx->inters.size());
     TRY(dalloc(ctx, &ctx->d_need, (size_t)ctx->nneed));
     CU(cudaMallocHost(&ctx->h_need, sizeof(int64_t) * ctx->nneed));
+    TRY(dalloc(ctx, &ctx->d_need_max, (size_t)ctx->nneed));
+    TRY(dalloc(ctx, &ctx->d_need_cap, (size_t)ctx->nneed));
+    CU(cudaMallocHost(&ctx->h_need_max, sizeof(int64_t) * ctx->nneed));
+    ctx->need_max.assign(ctx->nneed, 0);
     for (size_t g = 0; g < ctx->ghosts.size(); ++g) ctx->ghosts[g].need_slot = (int64_t)(ctx->slots.size() + g);
     for (size_t i = 0; i < ctx->inters.size(); ++i)
         ctx->inters[i].need_slot = (int64_t)(ctx->slots.size() + ctx->ghosts.size() + i);
@@ -764,30 +814,30 @@ __global__ void k_ghost_bound(GhostInst* gh, const SysInst* src, SysInst* gi, in
     gi[k].n = S.n;  // upper bound on the count, used only for planning
 }
 
-// Stable counting sort of `S` (or of a ghost set when G != nullptr).
-int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells) {
+// Stable counting sort of `S` (or of a ghost set when G != nullptr) over
+// `cells` packed key cells (an upper bound on the planned total, which the
+// device holds at `total`).
+int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells, const int64_t* total) {
     const int ni = ninst(ctx);
     TRY(ensure_cells(ctx, cells));
     CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
     CU(cudaMemsetAsync(ctx->fill, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
-    int64_t tc = cells;
-    CU(cudaMemcpyAsync(ctx->d_total_cells, &tc, 8, cudaMemcpyHostToDevice, ctx->stream));
     if (S) {
-        launch_sort_keys(S->F(F_X), S->N, S->nd, S->inst_of, nullptr, S->d_inst, ctx->key, ctx->hist, ctx->cap_cells,
+        launch_sort_keys(S->F(F_X), S->N, S->nd, S->inst_of, nullptr, S->d_inst, ctx->key, ctx->hist, cells,
                          ctx->d_err, ctx->stream);
         scan_exclusive(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
         launch_sort_scatter(ctx->key, S->N, nullptr, ctx->start, ctx->fill, ctx->perm, ctx->stream);
-        launch_sort_fixup(ctx->start, cells, ctx->d_total_cells, ctx->perm, ctx->stream);
+        launch_sort_fixup(ctx->start, cells, total, ctx->perm, ctx->stream);
         for (int f = 0; f < NF; ++f)
             if (S->ncomp[f]) launch_gather(S->F(f), S->A(f), S->ncomp[f], S->N, ctx->perm, nullptr, ctx->stream);
         launch_gather_i32(S->id[S->cur], S->id[S->cur ^ 1], S->N, ctx->perm, nullptr, ctx->stream);
         S->cur ^= 1;
     } else {
         launch_sort_keys(G->x[G->cur], G->CAP, G->nd, G->ginst[G->cur], G->d_count, G->d_inst, ctx->key, ctx->hist,
-                         ctx->cap_cells, ctx->d_err, ctx->stream);
+                         cells, ctx->d_err, ctx->stream);
         scan_exclusive(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
         launch_sort_scatter(ctx->key, G->CAP, G->d_count, ctx->start, ctx->fill, ctx->perm, ctx->stream);
-        launch_sort_fixup(ctx->start, cells, ctx->d_total_cells, ctx->perm, ctx->stream);
+        launch_sort_fixup(ctx->start, cells, total, ctx->perm, ctx->stream);
         const int c = G->cur, a = c ^ 1;
         launch_gather(G->x[c], G->x[a], G->nd, G->CAP, ctx->perm, G->d_count, ctx->stream);
         launch_gather_i32(G->io[c], G->io[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
@@ -940,16 +990,32 @@ int ensure_groups(gc_ctx* ctx, int slot, int id, bool b_side) {
     }
     TRY(ensure_cells(ctx, ncols_cap));  // scan scratch
     const int nd = ctx->slots[D.a].nd;
-    launch_groups_count(D.d_gi, ninst(ctx), nd, cs, ncols_cap, S.gcnt, ctx->stream);
+    launch_groups_count(D.d_gi, ninst(ctx), nd, cs, ncols_cap, D.cells, S.gcnt, ctx->stream);
     scan_exclusive(S.gcnt, S.goff, ncols_cap, ctx->scan_tmp, ctx->stream);
-    launch_groups_fill(D.d_gi, ninst(ctx), nd, cs, S.goff, ncols_cap, S.groups, S.d_ngroups, ctx->stream);
+    launch_groups_fill(D.d_gi, ninst(ctx), nd, cs, S.goff, ncols_cap, D.cells, S.groups, S.d_ngroups, ctx->stream);
     S.groups_key = key;
     S.groups_ver = D.grid_ver;
     return check_launch(ctx, "groups");
 }
 
+// Capacity mode: record the largest plans, and flag every plan that does
+// not fit its buffers (the window is then rolled back and re-run exactly).
+__global__ void k_need_max(const int64_t* need, int64_t* need_max, const int64_t* cap, int n, int* err) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        if (need[i] > need_max[i]) need_max[i] = need[i];
+        if (need[i] > cap[i]) atomicOr(err, ERR_CAPACITY);
+    }
+}
+
+// Cell bound for sorts and for interaction D's grid in capacity mode: the
+// shared histogram and the interaction's CSR both have to hold it.
+int64_t cap_sort_cells(gc_ctx* ctx) { return ctx->cap_cells - 1; }
+int64_t cap_grid_cells(gc_ctx* ctx, const DInter& D) { return std::min(D.cap_cells, ctx->cap_cells) - 1; }
+
 // Full prepare phase: sorts, ghosts and grids.  `sort_mask` selects which
-// system slots are sorted.
+// system slots are sorted.  Exact mode reads the planned cell counts back
+// to size every buffer; capacity mode sizes from the buffers' capacities
+// (no host read), and the kernels flag any plan that does not fit.
 int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     const int ni = ninst(ctx);
     CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
@@ -961,20 +1027,34 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     for (auto& G : ctx->ghosts) {
         k_ghost_bound<<<(ni + 127) / 128, 128, 0, ctx->stream>>>(G.d_gh, ctx->slots[G.src].d_inst, G.d_inst, ni, G.nd,
                                                                  G.nplanes);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
         launch_sort_plan(G.d_inst, ni, G.nd, ctx->d_need + G.need_slot, ctx->d_err, ctx->stream);
     }
     for (auto& D : ctx->inters) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
     TRY(check_launch(ctx, "plan"));
-    TRY(read_need(ctx));
-    std::vector<int64_t> need(ctx->h_need, ctx->h_need + ctx->nneed);
+    std::vector<int64_t> need(ctx->nneed);
+    if (ctx->capmode) {
+        k_need_max<<<1, 128, 0, ctx->stream>>>(ctx->d_need, ctx->d_need_max, ctx->d_need_cap, ctx->nneed,
+                                                ctx->d_err);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        for (size_t s = 0; s < ctx->slots.size(); ++s) need[s] = cap_sort_cells(ctx);
+        for (auto& G : ctx->ghosts) need[G.need_slot] = cap_sort_cells(ctx);
+        for (auto& D : ctx->inters) need[D.need_slot] = cap_grid_cells(ctx, D);
+    } else {
+        TRY(read_need(ctx));
+        for (int i = 0; i < ctx->nneed; ++i) {
+            need[i] = ctx->h_need[i];
+            ctx->need_max[i] = std::max(ctx->need_max[i], need[i]);
+        }
+    }
     // sorts
     for (size_t s = 0; s < ctx->slots.size(); ++s)
-        if (sort_mask[s]) TRY(sort_particles_slot(ctx, &ctx->slots[s], nullptr, need[s]));
+        if (sort_mask[s]) TRY(sort_particles_slot(ctx, &ctx->slots[s], nullptr, need[s], ctx->d_need + s));
     // ghosts: generate, bound-checked plan, sort
     for (auto& G : ctx->ghosts) {
         TRY(generate_ghosts(ctx, G));
         TRY(ghost_bbox_and_plan(ctx, G));
-        TRY(sort_particles_slot(ctx, nullptr, &G, need[G.need_slot]));
+        TRY(sort_particles_slot(ctx, nullptr, &G, need[G.need_slot], ctx->d_need + G.need_slot));
     }
     // grids (ghost-b plans are recomputed from the exact ghost boxes; the
     // cell count cannot exceed the planned bound)
@@ -1126,6 +1206,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         r.gi = D.d_gi;
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs;
+        r.cs_cells = D.cells;
         r.counts = D.counts;
         r.bbox = nullptr;
         if (D.btype == BT_GHOST) {
@@ -1185,11 +1266,13 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         e0 = ctx->ev_pool[ctx->ev_used].first;
         e1 = ctx->ev_pool[ctx->ev_used].second;
         ctx->ev_used++;
-        CU(cudaEventRecord(e0, ctx->stream));
+        // inside a capture the record must become a node of the graph
+        CU(cudaEventRecordWithFlags(e0, ctx->stream, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     }
     int st = launch_force_f64(A, count_only, ctx->stream);
     if (st) return seterr(ctx, st, "functor/system combination not implemented on the device");
-    if (e1) CU(cudaEventRecord(e1, ctx->stream));
+    if (e1)
+        CU(cudaEventRecordWithFlags(e1, ctx->stream, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     TRY(check_launch(ctx, "sweep"));
     // b side of two-sided (counting) coupled interactions
     for (int id : ids) {
@@ -1219,6 +1302,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         r.gi = D.d_gi;
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs_a;
+        r.cs_cells = D.cells;
         r.counts = nullptr;
         r.bx = S.F(F_X);
         r.bv = S.F(F_V);
@@ -1295,7 +1379,9 @@ int push_slot_params(gc_ctx* ctx, DSlot& S) {
     return GC_OK;
 }
 
-void decide_motion(gc_ctx* ctx) {
+// Returns true when some slot's motion changed (the step's structure with it).
+bool decide_motion(gc_ctx* ctx) {
+    bool changed = false;
     for (auto& S : ctx->slots) {
         bool src_zero = true;
         for (auto& h : S.h_inst) {
@@ -1304,8 +1390,11 @@ void decide_motion(gc_ctx* ctx) {
         }
         bool kin_zero = true;
         for (auto v : S.nonzero_kin) kin_zero &= v == 0;
-        S.moving = S.written || !src_zero || !kin_zero;
+        const bool m = S.written || !src_zero || !kin_zero;
+        changed |= m != S.moving;
+        S.moving = m;
     }
+    return changed;
 }
 
 int one_step(gc_ctx* ctx) {
@@ -1358,6 +1447,294 @@ int finish_status(gc_ctx* ctx) {
 }
 
 bool valid_inst(gc_ctx* ctx, int inst) { return inst >= 0 && inst < (int)ctx->inst.size(); }
+// ------------------------------------------------------- graph stepping
+void drop_graphs(gc_ctx* ctx) {
+    for (auto& g : ctx->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    ctx->graphs.clear();
+}
+
+// Any change of model state outside gc_step: the next step runs exactly
+// (and sorts static systems again where asked), graphs are recaptured.
+void invalidate_steps(gc_ctx* ctx) {
+    drop_graphs(ctx);
+    ctx->exact_done = false;
+}
+
+std::vector<char> parity(gc_ctx* ctx) {
+    std::vector<char> p;
+    for (auto& S : ctx->slots) p.push_back((char)S.cur);
+    for (auto& G : ctx->ghosts) p.push_back((char)G.cur);
+    return p;
+}
+
+void set_parity(gc_ctx* ctx, const std::vector<char>& p) {
+    size_t i = 0;
+    for (auto& S : ctx->slots) S.cur = p[i++];
+    for (auto& G : ctx->ghosts) G.cur = p[i++];
+}
+
+int graph_key(gc_ctx* ctx) { return (ctx->precision * 64 + ctx->force_cfg) * 2 + (ctx->profiling ? 1 : 0); }
+
+int grow_gcols(gc_ctx* ctx, DSlot& S, int64_t ncols) {
+    if (ncols + 1 <= S.cap_gcols) return GC_OK;
+    CU(cudaStreamSynchronize(ctx->stream));
+    dfree(ctx, S.gcnt, S.cap_gcols);
+    dfree(ctx, S.goff, S.cap_gcols);
+    int64_t cap = ncols + 1 + ncols / 4;
+    TRY(dalloc(ctx, &S.gcnt, (size_t)cap));
+    TRY(dalloc(ctx, &S.goff, (size_t)cap));
+    S.cap_gcols = cap;
+    return GC_OK;
+}
+
+// Capacities for capacity-mode steps: every planned cell count seen so far,
+// times the margin.  Growth happens here, at a verified point, never inside
+// a captured step.
+int size_capacities(gc_ctx* ctx) {
+    const int n = ctx->nneed;
+    CU(cudaMemcpyAsync(ctx->h_need_max, ctx->d_need_max, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < n; ++i) ctx->need_max[i] = std::max(ctx->need_max[i], ctx->h_need_max[i]);
+    const double m = ctx->cap_margin;
+    auto want = [&](int64_t need) { return (int64_t)((double)need * m) + 1024; };
+    auto low = [&](int64_t need) { return (int64_t)((double)need * (1.0 + (m - 1.0) / 2.0)) + 512; };
+    int64_t all = 0;
+    for (int i = 0; i < n; ++i) all = std::max(all, ctx->need_max[i]);
+    if (ctx->cap_cells - 1 < low(all)) TRY(ensure_cells(ctx, want(all)));
+    for (auto& D : ctx->inters) {
+        const int64_t nm = ctx->need_max[D.need_slot];
+        if (D.cap_cells - 1 < low(nm)) TRY(ensure_inter_cells(ctx, D, want(nm)));
+    }
+    // scan scratch for ghost flags and for every capacity-sized scan
+    int64_t scan_n = ctx->cap_cells;
+    for (auto& G : ctx->ghosts) scan_n = std::max(scan_n, G.CAP);
+    int64_t st = scan_tmp_elems(scan_n) + 16;
+    if (st > ctx->cap_scan) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, ctx->scan_tmp, ctx->cap_scan);
+        TRY(dalloc(ctx, &ctx->scan_tmp, (size_t)st));
+        ctx->cap_scan = st;
+    }
+    // warp-group column tables of every system a grid groups
+    for (auto& D : ctx->inters) {
+        const int64_t cells = cap_grid_cells(ctx, D);
+        TRY(grow_gcols(ctx, ctx->slots[D.a], cells));
+        if (D.two_sided && D.bslot >= 0) TRY(grow_gcols(ctx, ctx->slots[D.bslot], cells));
+    }
+    // the bound each plan entry is checked against inside the steps
+    std::vector<int64_t> cap(n);
+    for (size_t s = 0; s < ctx->slots.size(); ++s) cap[s] = cap_sort_cells(ctx);
+    for (auto& G : ctx->ghosts) cap[G.need_slot] = cap_sort_cells(ctx);
+    for (auto& D : ctx->inters) cap[D.need_slot] = cap_grid_cells(ctx, D);
+    TRY(hcopy(ctx, ctx->d_need_cap, cap.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    return GC_OK;
+}
+
+// Snapshot of every moving slot's carried state (current buffers), the
+// rollback point of a capacity-mode window.
+int snapshot(gc_ctx* ctx, std::vector<char>& par) {
+    ctx->snaps.resize(ctx->slots.size());
+    for (size_t s = 0; s < ctx->slots.size(); ++s) {
+        DSlot& S = ctx->slots[s];
+        Snapshot& sn = ctx->snaps[s];
+        if (!S.moving) continue;
+        if (sn.n != S.N) {
+            for (int f = 0; f < NF; ++f) dfree(ctx, sn.f[f], (size_t)S.ncomp[f] * sn.n);
+            dfree(ctx, sn.id, (size_t)sn.n);
+            for (int f = 0; f < NF; ++f)
+                if (S.ncomp[f]) TRY(dalloc(ctx, &sn.f[f], (size_t)S.ncomp[f] * S.N));
+            TRY(dalloc(ctx, &sn.id, (size_t)S.N));
+            sn.n = S.N;
+        }
+        for (int f = 0; f < NF; ++f)
+            if (S.ncomp[f])
+                CU(cudaMemcpyAsync(sn.f[f], S.F(f), sizeof(double) * S.ncomp[f] * S.N, cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+        CU(cudaMemcpyAsync(sn.id, S.id[S.cur], sizeof(int32_t) * S.N, cudaMemcpyDeviceToDevice, ctx->stream));
+        sn.cur = S.cur;
+    }
+    par = parity(ctx);
+    return GC_OK;
+}
+
+int restore(gc_ctx* ctx, const std::vector<char>& par) {
+    set_parity(ctx, par);
+    for (size_t s = 0; s < ctx->slots.size(); ++s) {
+        DSlot& S = ctx->slots[s];
+        Snapshot& sn = ctx->snaps[s];
+        if (!S.moving) continue;
+        for (int f = 0; f < NF; ++f)
+            if (S.ncomp[f])
+                CU(cudaMemcpyAsync(S.F(f), sn.f[f], sizeof(double) * S.ncomp[f] * S.N, cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+        CU(cudaMemcpyAsync(S.id[S.cur], sn.id, sizeof(int32_t) * S.N, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return GC_OK;
+}
+
+int ev_pair(gc_ctx* ctx, size_t i) {
+    while (ctx->ev_pool.size() <= i) {
+        cudaEvent_t a, b;
+        CU(cudaEventCreate(&a));
+        CU(cudaEventCreate(&b));
+        ctx->ev_pool.push_back({a, b});
+    }
+    return GC_OK;
+}
+
+// Capture one capacity-mode step into `g` (nothing runs).
+int capture_step(gc_ctx* ctx, StepGraph& g) {
+    if (ctx->profiling) TRY(ev_pair(ctx, ctx->ev_used + 4 * ctx->slots.size() * (size_t)std::max(ctx->nstages, 1)));
+    g.pre = parity(ctx);
+    const size_t ev0 = ctx->ev_used;
+    const long long l0 = g_launches.load();
+    const int64_t steps0 = ctx->steps_done, resorts0 = ctx->resorts;
+    CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->capturing = true;
+    int st = one_step(ctx);
+    ctx->capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    g.launches = g_launches.load() - l0;
+    g_launches.fetch_sub(g.launches);  // the capture launched nothing
+    ctx->steps_done = steps0;
+    ctx->resorts = resorts0;
+    const size_t ev1 = ctx->ev_used;
+    ctx->ev_used = ev0;
+    if (st != GC_OK || e != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        set_parity(ctx, g.pre);
+        if (st != GC_OK) return st;
+        return seterr(ctx, GC_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+    }
+    g.post = parity(ctx);
+    set_parity(ctx, g.pre);
+    g.graph = graph;
+    if (ev1 > ev0) {
+        size_t nn = 0;
+        CU(cudaGraphGetNodes(graph, nullptr, &nn));
+        std::vector<cudaGraphNode_t> nodes(nn);
+        CU(cudaGraphGetNodes(graph, nodes.data(), &nn));
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            CU(cudaGraphNodeGetType(nd, &t));
+            if (t != cudaGraphNodeTypeEventRecord) continue;
+            cudaEvent_t ev;
+            CU(cudaGraphEventRecordNodeGetEvent(nd, &ev));
+            for (size_t i = ev0; i < ev1; ++i) {
+                if (ctx->ev_pool[i].first == ev || ctx->ev_pool[i].second == ev) {
+                    g.ev_nodes.push_back(nd);
+                    g.ev_slots.push_back({(int64_t)(i - ev0), ctx->ev_pool[i].first == ev ? 0 : 1});
+                }
+            }
+        }
+    }
+    CU(cudaGraphInstantiate(&g.exec, graph, 0));
+    return GC_OK;
+}
+
+int replay_step(gc_ctx* ctx, StepGraph& g) {
+    if (!g.ev_nodes.empty()) {
+        int64_t npairs = 0;
+        for (auto& sl : g.ev_slots) npairs = std::max(npairs, sl[0] + 1);
+        TRY(ev_pair(ctx, ctx->ev_used + (size_t)npairs));
+        for (size_t q = 0; q < g.ev_nodes.size(); ++q) {
+            auto& pr = ctx->ev_pool[ctx->ev_used + (size_t)g.ev_slots[q][0]];
+            CU(cudaGraphExecEventRecordNodeSetEvent(g.exec, g.ev_nodes[q], g.ev_slots[q][1] ? pr.second : pr.first));
+        }
+        ctx->ev_used += (size_t)npairs;
+    }
+    CU(cudaGraphLaunch(g.exec, ctx->stream));
+    set_parity(ctx, g.post);
+    g_launches.fetch_add(g.launches);
+    ctx->steps_done += 1;
+    ctx->resorts += 1;
+    ctx->graph_steps += 1;
+    return GC_OK;
+}
+
+StepGraph* find_graph(gc_ctx* ctx) {
+    const std::vector<char> p = parity(ctx);
+    for (auto& g : ctx->graphs)
+        if (g.pre == p) return &g;
+    return nullptr;
+}
+
+// `nsteps` steps.  Without graphs (or for the first step after a change):
+// exact steps, each sized by one host read of the plan.  Otherwise windows
+// of up to `sync_every` captured capacity-mode steps, verified at the end of
+// each window; a window whose plan outgrew a capacity is rolled back to its
+// snapshot and re-run exactly.
+int run_steps(gc_ctx* ctx, int nsteps) {
+    static const bool env_off = [] {
+        const char* e = getenv("GC_GRAPHS");
+        return e && e[0] == '0';
+    }();
+    bool graphs = ctx->graphs_on && !env_off;
+    int done = 0;
+    while (done < nsteps) {
+        if (!graphs || !ctx->exact_done) {
+            ctx->capmode = false;
+            TRY(one_step(ctx));
+            ctx->exact_done = true;
+            ++done;
+            continue;
+        }
+        TRY(size_capacities(ctx));
+        std::vector<char> par0;
+        TRY(snapshot(ctx, par0));
+        if (ctx->alloc_epoch != ctx->graphs_epoch || graph_key(ctx) != ctx->graphs_key) {
+            drop_graphs(ctx);
+            ctx->graphs_epoch = ctx->alloc_epoch;
+            ctx->graphs_key = graph_key(ctx);
+        }
+        const int W = std::min(ctx->sync_every, nsteps - done);
+        int ran = 0;
+        int cap_err = GC_OK;
+        ctx->capmode = true;
+        for (; ran < W; ++ran) {
+            StepGraph* g = find_graph(ctx);
+            if (!g) {
+                ctx->graphs.emplace_back();
+                cap_err = capture_step(ctx, ctx->graphs.back());
+                if (cap_err != GC_OK) {
+                    ctx->graphs.pop_back();
+                    break;
+                }
+                g = &ctx->graphs.back();
+            }
+            TRY(replay_step(ctx, *g));
+        }
+        ctx->capmode = false;
+        CU(cudaStreamSynchronize(ctx->stream));
+        TRY(collect_profile(ctx));
+        int e = 0;
+        TRY(hcopy(ctx, &e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e & ERR_CAPACITY) {
+            // a plan outgrew a capacity: back to the snapshot, then the same
+            // steps exactly (which size every buffer from the plan)
+            TRY(restore(ctx, par0));
+            ctx->steps_done -= ran;
+            ctx->resorts -= ran;
+            ctx->graph_steps -= ran;
+            ctx->rollbacks += 1;
+            e &= ~ERR_CAPACITY;
+            CU(cudaMemcpyAsync(ctx->d_err, &e, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            for (int w = 0; w < ran; ++w) TRY(one_step(ctx));
+        } else if (e) {
+            return GC_OK;  // finish_status reports it
+        }
+        done += ran;
+        if (cap_err != GC_OK) graphs = false;  // this call continues exactly
+    }
+    return GC_OK;
+}
+
 
 }  // namespace
 
@@ -1466,6 +1843,14 @@ int gc_ctx_destroy(gc_ctx* ctx) {
     cudaFree(ctx->d_need);
     cudaFree(ctx->d_total_cells);
     if (ctx->h_need) cudaFreeHost(ctx->h_need);
+    cudaFree(ctx->d_need_max);
+    cudaFree(ctx->d_need_cap);
+    if (ctx->h_need_max) cudaFreeHost(ctx->h_need_max);
+    drop_graphs(ctx);
+    for (auto& sn : ctx->snaps) {
+        for (int f = 0; f < NF; ++f) cudaFree(sn.f[f]);
+        cudaFree(sn.id);
+    }
     cudaFree(ctx->staging);
     cudaFree(ctx->d_pairs);
     for (auto& e : ctx->ev_pool) {
@@ -1756,6 +2141,7 @@ static int resolve(gc_ctx* ctx, int inst, int handle, HandleRef* r) {
 }
 
 int gc_upload_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx || !host) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, handle, &r));
@@ -1860,9 +2246,9 @@ int gc_step(gc_ctx* ctx, int nsteps, double cfl) {
     cudaSetDevice(ctx->device);
     upload_inst_params(ctx, cfl);
     for (auto& S : ctx->slots) TRY(push_slot_params(ctx, S));
-    decide_motion(ctx);
+    if (decide_motion(ctx)) invalidate_steps(ctx);
     CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
-    for (int s = 0; s < nsteps; ++s) TRY(one_step(ctx));
+    TRY(run_steps(ctx, nsteps));
     return finish_status(ctx);
 }
 
@@ -1874,6 +2260,8 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
     out->kernel_launches = (int64_t)g_launches.load();
     out->sweep_launches = ctx->sweep_launches;
     out->sweep_ms = ctx->sweep_ms;
+    out->graph_steps = ctx->graph_steps;
+    out->rollbacks = ctx->rollbacks;
     if (ctx->finalized && ctx->steps_done > 0) {
         if (!ctx->d_pairs) TRY(dalloc(ctx, &ctx->d_pairs, 1));
         int64_t pairs = 0;
@@ -1900,6 +2288,7 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
 
 // ------------------------------------------------------------- phase hooks
 int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* perm_out) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, handle, &r));
@@ -1914,7 +2303,7 @@ int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* pe
         TRY(hcopy(ctx, G.d_inst, gi.data(), ni * sizeof(SysInst), cudaMemcpyHostToDevice));
         TRY(ghost_bbox_and_plan(ctx, G));
         TRY(read_need(ctx));
-        TRY(sort_particles_slot(ctx, nullptr, &G, ctx->h_need[G.need_slot]));
+        TRY(sort_particles_slot(ctx, nullptr, &G, ctx->h_need[G.need_slot], ctx->d_need + G.need_slot));
         TRY(finish_status(ctx));  // host reads below must follow the stream's kernels
         if (perm_out) {
             TRY(hcopy(ctx, gi.data(), G.d_inst, ni * sizeof(SysInst), cudaMemcpyDeviceToHost));
@@ -1931,7 +2320,7 @@ int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* pe
     TRY(bbox_slot(ctx, S));
     launch_sort_plan(S.d_inst, ni, S.nd, ctx->d_need + r.sys, ctx->d_err, ctx->stream);
     TRY(read_need(ctx));
-    TRY(sort_particles_slot(ctx, &S, nullptr, ctx->h_need[r.sys]));
+    TRY(sort_particles_slot(ctx, &S, nullptr, ctx->h_need[r.sys], ctx->d_need + r.sys));
     TRY(finish_status(ctx));  // host reads below must follow the stream's kernels
     if (perm_out) {
         const int64_t n = S.h_inst[inst].n, base = S.h_inst[inst].base;
@@ -1945,6 +2334,7 @@ int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* pe
 
 int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int64_t cap, double* mingridx_out,
                   int64_t* ngridx_out, int64_t* ncells_out) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
     if (!valid_inst(ctx, inst) || inter < 0 || inter >= (int)ctx->inters.size())
@@ -1991,6 +2381,7 @@ int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int
 }
 
 int gc_generate_ghosts(gc_ctx* ctx, int inst, int ghost) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, ghost, &r));
@@ -2002,6 +2393,7 @@ int gc_generate_ghosts(gc_ctx* ctx, int inst, int ghost) {
 }
 
 int gc_update_ghost_kinematics(gc_ctx* ctx, int inst, int ghost) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, ghost, &r));
@@ -2011,6 +2403,7 @@ int gc_update_ghost_kinematics(gc_ctx* ctx, int inst, int ghost) {
 }
 
 int gc_update_ghost(gc_ctx* ctx, int inst, int ghost, int stage) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, ghost, &r));
@@ -2020,6 +2413,7 @@ int gc_update_ghost(gc_ctx* ctx, int inst, int ghost, int stage) {
 }
 
 int gc_sweep(gc_ctx* ctx, int inst, int inter, int stage) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
     if (!valid_inst(ctx, inst) || inter < 0 || inter >= (int)ctx->inters.size())
@@ -2032,6 +2426,7 @@ int gc_sweep(gc_ctx* ctx, int inst, int inter, int stage) {
 }
 
 int gc_update_state(gc_ctx* ctx, int inst, int sys, int stage, double dt) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, sys, &r));
@@ -2041,6 +2436,7 @@ int gc_update_state(gc_ctx* ctx, int inst, int sys, int stage, double dt) {
 }
 
 int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, int64_t n) {
+    if (ctx) invalidate_steps(ctx);
     if (!ctx || !counts_out) return GC_ERR_ARG;
     if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
     if (!valid_inst(ctx, inst) || inter < 0 || inter >= (int)ctx->inters.size())
@@ -2080,6 +2476,15 @@ int gc_set_profiling(gc_ctx* ctx, int on) {
     ctx->profiling = on != 0;
     ctx->sweep_ms = 0;
     ctx->sweep_launches = 0;
+    return GC_OK;
+}
+
+int gc_set_graphs(gc_ctx* ctx, int on, int sync_every) {
+    if (!ctx) return GC_ERR_ARG;
+    if (sync_every < 1) return seterr(ctx, GC_ERR_ARG, "sync_every must be at least 1");
+    ctx->graphs_on = on != 0;
+    ctx->sync_every = sync_every;
+    invalidate_steps(ctx);
     return GC_OK;
 }
 

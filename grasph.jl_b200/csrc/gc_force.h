@@ -33,6 +33,7 @@ struct InterRef {
     const GridInst* gi;   // per instance
     const PfnInst* pi;    // per instance, this stage
     const int32_t* cs;    // packed CSR over system_b (global b indices)
+    int64_t cs_cells;     // cells of cs that are valid (an instance beyond them is skipped)
     const double *bx, *bv, *brho, *bp, *bstress, *baux;
     const float* bfp;     // FP32 pack of system_b (v, rho, aux, 1/rho, stress), planar
     int64_t bN;           // planar stride of system_b's arrays
@@ -61,10 +62,10 @@ struct ForceArgs {
 };
 
 int launch_force_f64(const ForceArgs& A, bool count_only, cudaStream_t s);
-void launch_groups_count(const GridInst* gi, int ninst, int nd, const int32_t* cs, int64_t ncols_cap, int32_t* cnt,
-                         cudaStream_t s);
+void launch_groups_count(const GridInst* gi, int ninst, int nd, const int32_t* cs, int64_t ncols_cap,
+                         int64_t cells_cap, int32_t* cnt, cudaStream_t s);
 void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs, const int32_t* off,
-                        int64_t ncols_cap, int2* groups, int64_t* ngroups, cudaStream_t s);
+                        int64_t ncols_cap, int64_t cells_cap, int2* groups, int64_t* ngroups, cudaStream_t s);
 void launch_aux(int mode, int64_t N, const int64_t* count, const double* rho, const double* p,
                 const int32_t* inst_of, const double* mass, double* aux, cudaStream_t s);
 // FP32 pack (planar, stride N): v[nd], rho, aux(mode), 1/rho, stress[ns] (ns may be 0).

@@ -324,6 +324,9 @@ __global__ void k_gather(const double* __restrict__ src, double* __restrict__ ds
     int64_t n = count ? *count : N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         int64_t o = perm[g];
+        // a permutation left incomplete by a flagged key overflow may hold
+        // stale entries: keep every read inside the array
+        if ((uint64_t)o >= (uint64_t)N) o = g;
         for (int c = 0; c < ncomp; ++c) dst[c * N + g] = src[c * N + o];
     }
 }
@@ -331,8 +334,11 @@ __global__ void k_gather(const double* __restrict__ src, double* __restrict__ ds
 __global__ void k_gather_i32(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int64_t N,
                              const int32_t* __restrict__ perm, const int64_t* count) {
     int64_t n = count ? *count : N;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x)
-        dst[g] = src[perm[g]];
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = perm[g];
+        if ((uint64_t)o >= (uint64_t)N) o = g;
+        dst[g] = src[o];
+    }
 }
 
 void launch_gather(const double* src, double* dst, int ncomp, int64_t N, const int32_t* perm, const int64_t* count,

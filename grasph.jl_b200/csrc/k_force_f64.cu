@@ -28,8 +28,11 @@ __device__ __forceinline__ int find_inst(const GridInst* gi, int ninst, int64_t 
     return lo;
 }
 
+// `cells_cap`: cells of `cs` that are valid (cs holds cells_cap + 1
+// entries); an instance whose grid reaches beyond them contributes nothing
+// (the grid build has flagged the overflow).
 __global__ void k_groups_count(const GridInst* __restrict__ gi, int ninst, int nd, const int32_t* __restrict__ cs,
-                               int64_t ncols_cap, int32_t* __restrict__ cnt) {
+                               int64_t ncols_cap, int64_t cells_cap, int32_t* __restrict__ cnt) {
     const int64_t T = gi[ninst - 1].colbase + gi[ninst - 1].ncols;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncols_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -41,18 +44,23 @@ __global__ void k_groups_count(const GridInst* __restrict__ gi, int ninst, int n
         const int64_t ngl = G.ng[nd - 1];
         const int64_t local = c - G.colbase;
         const int64_t b = G.cellbase + local * ngl;
+        if (G.cellbase + G.ncells > cells_cap) {
+            cnt[c] = 0;
+            continue;
+        }
         const int32_t n = cs[b + ngl] - cs[b];
         cnt[c] = (n + 31) / 32;
     }
 }
 
 __global__ void k_groups_fill(const GridInst* __restrict__ gi, int ninst, int nd, const int32_t* __restrict__ cs,
-                              const int32_t* __restrict__ off, int64_t ncols_cap, int2* __restrict__ groups,
-                              int64_t* ngroups) {
+                              const int32_t* __restrict__ off, int64_t ncols_cap, int64_t cells_cap,
+                              int2* __restrict__ groups, int64_t* ngroups) {
     const int64_t T = gi[ninst - 1].colbase + gi[ninst - 1].ncols;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < T && c < ncols_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
         const GridInst& G = gi[find_inst(gi, ninst, c)];
+        if (G.cellbase + G.ncells > cells_cap) continue;
         const int64_t ngl = G.ng[nd - 1];
         const int64_t local = c - G.colbase;
         const int64_t b = G.cellbase + local * ngl;
@@ -63,19 +71,19 @@ __global__ void k_groups_fill(const GridInst* __restrict__ gi, int ninst, int nd
     if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = off[ncols_cap];
 }
 
-void launch_groups_count(const GridInst* gi, int ninst, int nd, const int32_t* cs, int64_t ncols_cap, int32_t* cnt,
-                         cudaStream_t s) {
+void launch_groups_count(const GridInst* gi, int ninst, int nd, const int32_t* cs, int64_t ncols_cap,
+                         int64_t cells_cap, int32_t* cnt, cudaStream_t s) {
     int64_t b = (ncols_cap + 255) / 256;
     if (b < 1) b = 1;
-    k_groups_count<<<(int)b, 256, 0, s>>>(gi, ninst, nd, cs, ncols_cap, cnt);
+    k_groups_count<<<(int)b, 256, 0, s>>>(gi, ninst, nd, cs, ncols_cap, cells_cap, cnt);
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs, const int32_t* off,
-                        int64_t ncols_cap, int2* groups, int64_t* ngroups, cudaStream_t s) {
+                        int64_t ncols_cap, int64_t cells_cap, int2* groups, int64_t* ngroups, cudaStream_t s) {
     int64_t b = (ncols_cap + 255) / 256;
     if (b < 1) b = 1;
-    k_groups_fill<<<(int)b, 256, 0, s>>>(gi, ninst, nd, cs, off, ncols_cap, groups, ngroups);
+    k_groups_fill<<<(int)b, 256, 0, s>>>(gi, ninst, nd, cs, off, ncols_cap, cells_cap, groups, ngroups);
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -652,6 +652,12 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                     continue;
                 }
             }
+            if (G.cellbase + G.ncells > r.cs_cells) {
+                // this instance's grid did not fit its buffer: flag it, read nothing
+                if (lane == 0) atomicOr(A.err, ERR_CAPACITY);
+                if (active && r.counts) r.counts[gi] = 0;
+                continue;
+            }
             int64_t c[ND];
             bool ok = true;
 #pragma unroll

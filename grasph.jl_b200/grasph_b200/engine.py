@@ -44,7 +44,8 @@ class GcStats(ct.Structure):
     _fields_ = [("steps_done", ct.c_int64), ("pairs_last_step", ct.c_int64),
                 ("grid_inconsistent", ct.c_int64), ("kernel_launches", ct.c_int64),
                 ("sweep_launches", ct.c_int64), ("sweep_ms", ct.c_double),
-                ("last_status", ct.c_int32), ("pad", ct.c_int32)]
+                ("last_status", ct.c_int32), ("pad", ct.c_int32),
+                ("graph_steps", ct.c_int64), ("rollbacks", ct.c_int64)]
 
 
 _LIB = None
@@ -92,6 +93,7 @@ def load_library(path: os.PathLike | None = None):
         "gc_stream": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_void_p)]),
         "gc_set_profiling": (ct.c_int, [ct.c_void_p, ct.c_int]),
         "gc_measure_fp64_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
+        "gc_set_graphs": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -207,6 +209,9 @@ class CudaBackend:
 
     def set_precision(self, mode):
         self._chk(self.lib.gc_set_precision(self.ctx, mode), "gc_set_precision")
+
+    def set_graphs(self, on, sync_every=32):
+        self._chk(self.lib.gc_set_graphs(self.ctx, 1 if on else 0, sync_every), "gc_set_graphs")
 
     def step(self, nsteps, cfl):
         self._chk(self.lib.gc_step(self.ctx, nsteps, cfl), "gc_step")

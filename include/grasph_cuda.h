@@ -137,6 +137,9 @@ typedef struct gc_stats {
     double sweep_ms;             /* summed device time of those launches          */
     int32_t last_status;         /* device error word of the last step            */
     int32_t pad;
+    int64_t graph_steps;         /* steps run as replays of a captured step graph */
+    int64_t rollbacks;           /* verified windows re-run exactly (a capacity
+                                    was outgrown inside the window)              */
 } gc_stats;
 
 /* ============================================================ lifecycle */
@@ -225,6 +228,16 @@ int gc_stream(gc_ctx* ctx, void** stream_out);
  * context's stream; gc_get_stats reports their summed time.  Resets the
  * sweep counters.                                                         */
 int gc_set_profiling(gc_ctx* ctx, int on);
+/* Step scheduling (no counterpart in the reference, whose loop is host
+ * code).  on = 1 (default): after one exactly-sized step, gc_step captures
+ * a step sized from buffer capacities as a CUDA graph (one per buffer
+ * parity) and replays it, with no host round trip per step; every
+ * `sync_every` steps (default 32) the host verifies the window, grows
+ * capacities, and re-runs the window exactly from a device snapshot if a
+ * plan outgrew them.  Results are bit-identical to on = 0 (every step
+ * sized by one host read of its plan).  The environment variable
+ * GC_GRAPHS=0 forces on = 0.                                              */
+int gc_set_graphs(gc_ctx* ctx, int on, int sync_every);
 /* Measured FP64 FMA issue rate of the device in TFLOP/s (2 flops per FMA):
  * the compute ceiling of the FP64 pair sweep.                             */
 int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out);

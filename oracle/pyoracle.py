@@ -169,6 +169,9 @@ class OracleBackend:
     def set_precision(self, mode):
         pass
 
+    def set_graphs(self, on, sync_every=32):
+        pass
+
     def upload(self, inst, handle, field, array):
         a = np.ascontiguousarray(array)
         self._chk(self.L.oracle_set_field(self.ctx, handle, field, a.ctypes.data, a.nbytes), "set_field")
