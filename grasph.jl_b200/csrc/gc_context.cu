@@ -63,6 +63,10 @@ struct HInter {
     std::vector<int> pk;
     std::vector<std::array<double, GC_PFN_NPARAM>> pp;
 };
+struct HStaged {
+    int handle, field;
+    std::vector<char> bytes;  // the caller's layout, as gc_upload_field takes it
+};
 struct HInst {
     std::vector<HSys> sys;
     std::vector<HHandle> handles;
@@ -70,6 +74,8 @@ struct HInst {
     std::vector<HGhost> ghosts;
     std::vector<HInter> inters;
     double gamma = 0;
+    double cfl = NAN;              // own CFL number (serving); NaN: gc_step's
+    std::vector<HStaged> staged;   // fields given before gc_finalize
 };
 
 // ---------------------------------------------------------- device state
@@ -1348,7 +1354,7 @@ void upload_inst_params(gc_ctx* ctx, double cfl) {
         double h = 1e300, c = -1e300;
         for (auto& it : I.inters) h = std::min(h, it.H);
         for (auto& s : I.sys) c = std::max(c, s.c);
-        double dt = cfl * h / c;
+        double dt = (std::isfinite(I.cfl) ? I.cfl : cfl) * h / c;
         for (auto& S : ctx->slots) {
             S.h_inst[k].dt = dt;
             S.h_inst[k].half_dt = dt / 2.0;
@@ -2064,6 +2070,34 @@ int gc_finalize(gc_ctx* ctx) {
     if (st) return st;
     upload_inst_params(ctx, 0.0);
     for (auto& S : ctx->slots) TRY(push_slot_params(ctx, S));
+    for (size_t k = 0; k < ctx->inst.size(); ++k) {
+        std::vector<HStaged> staged;
+        staged.swap(ctx->inst[k].staged);
+        for (auto& f : staged)
+            TRY(gc_upload_field(ctx, (int)k, f.handle, f.field, f.bytes.data(), f.bytes.size()));
+    }
+    return GC_OK;
+}
+
+int gc_stage_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes) {
+    if (!ctx || (!host && bytes)) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized: use gc_upload_field");
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
+    HInst& I = ctx->inst[inst];
+    if (handle < 0 || handle >= (int)I.handles.size() || I.handles[handle].type == H_GHOST)
+        return seterr(ctx, GC_ERR_ARG, "bad system handle");
+    const HSys& hs = I.sys[I.handles[handle].idx];
+    const int comps = sys_comps(hs, field);
+    if (comps < 0 && field != GC_FIELD_V_ADJUSTMENT)
+        return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", field);
+    const int width = field == GC_FIELD_V_ADJUSTMENT ? hs.nd : comps;
+    if (bytes != (size_t)(hs.n * width * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
+    for (auto& f : I.staged)
+        if (f.handle == handle && f.field == field) {
+            f.bytes.assign((const char*)host, (const char*)host + bytes);
+            return GC_OK;
+        }
+    I.staged.push_back({handle, field, std::vector<char>((const char*)host, (const char*)host + bytes)});
     return GC_OK;
 }
 
@@ -2515,3 +2549,208 @@ int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out) {
 }
 
 }  // extern "C"
+
+// ============================================================ packing
+// Runtime support of the serving loop (gc_serve.cu): contexts are rebuilt
+// with a new set of instances, each copied from a running context (device
+// state) or from a model context (staged host fields).
+namespace gc {
+
+struct PackSeg {
+    const void* src;
+    int64_t src_stride, src_base, dst_base, n;
+};
+
+template <class T>
+__global__ void k_pack(const PackSeg* __restrict__ seg, int ncomp, T* __restrict__ dst, int64_t dst_stride) {
+    const PackSeg S = seg[blockIdx.y];
+    const T* src = (const T*)S.src;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += (int64_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < ncomp; ++c) dst[c * dst_stride + S.dst_base + i] = src[c * S.src_stride + S.src_base + i];
+}
+
+bool ctx_same_structure(gc_ctx* a, int ia, gc_ctx* b, int ib) {
+    std::string why;
+    return same_structure(a->inst[ia], b->inst[ib], why);
+}
+
+bool ctx_finalized(gc_ctx* c) { return c->finalized; }
+int ctx_ninst(gc_ctx* c) { return (int)c->inst.size(); }
+
+int ctx_set_cfl(gc_ctx* c, int inst, double cfl) {
+    if (!valid_inst(c, inst)) return GC_ERR_ARG;
+    c->inst[inst].cfl = cfl;
+    return GC_OK;
+}
+
+int64_t ctx_particles(gc_ctx* c, int inst) {
+    int64_t n = 0;
+    for (auto& s : c->inst[inst].sys) n += s.n;
+    return n;
+}
+
+// Particles whose positions move (the serving throughput counts these).
+int64_t ctx_moving_particles(gc_ctx* c, int inst) {
+    const HInst& I = c->inst[inst];
+    std::vector<char> w(I.sys.size(), 0);
+    for (auto& it : I.inters)
+        for (int p : it.pk)
+            if (p != GC_PFN_NONE) w[it.a] = 1;
+    int64_t n = 0;
+    for (size_t s = 0; s < I.sys.size(); ++s)
+        if (w[s]) n += I.sys[s].n;
+    return n;
+}
+
+// Device bytes one instance of `m` needs in a packed context: its carried
+// fields (two buffers and the rollback snapshot), step temporaries, ghost
+// capacity and the grids over the staged positions' box (doubled for
+// runout), with a quarter on top.
+int64_t ctx_estimate_bytes(gc_ctx* m, int inst) {
+    const HInst& I = m->inst[inst];
+    int64_t b = 0;
+    for (auto& s : I.sys) {
+        int comps = 0;
+        for (int f = 0; f < GC_NFIELDS; ++f) {
+            if (f == GC_FIELD_ID || f == GC_FIELD_V_ADJUSTMENT) continue;
+            const int c = sys_comps(s, f);
+            if (c > 0) comps += c;
+        }
+        b += s.n * (comps * 8 * 3 + (s.nd + 2) * 8 + 4 * 4 + 8 + 4 * (s.nd + 3 + s.ns) + 8 + 4 * 4);
+    }
+    for (auto& g : I.ghosts) {
+        const HSys& src = I.sys[g.src];
+        const int64_t cap = src.n * g.nplanes;
+        b += cap * (src.nd * 8 * 4 + 4 * 8 + 8 * 3 + src.ns * 8 + 4 * (src.nd + 3 + src.ns));
+    }
+    // grid cells from the staged positions' bounding box
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    int nd = I.sys.empty() ? 2 : I.sys[0].nd;
+    bool any = false;
+    for (auto& f : I.staged) {
+        if (f.field != GC_FIELD_X) continue;
+        const double* x = (const double*)f.bytes.data();
+        const int64_t n = (int64_t)f.bytes.size() / 8 / nd;
+        for (int64_t i = 0; i < n; ++i)
+            for (int d = 0; d < nd; ++d) {
+                lo[d] = std::min(lo[d], x[i * nd + d]);
+                hi[d] = std::max(hi[d], x[i * nd + d]);
+                any = true;
+            }
+    }
+    double hmin = 1e300;
+    for (auto& it : I.inters) hmin = std::min(hmin, it.H);
+    if (any && hmin < 1e300) {
+        double cells = 1;
+        for (int d = 0; d < nd; ++d) cells *= (hi[d] - lo[d]) / (2.0 * hmin) * 2.0 + 8.0;
+        b += (int64_t)(cells * (double)I.inters.size() * 4 * 2 * 1.5) + (int64_t)(cells * 4 * 3 * 1.5);
+    }
+    return b + b / 4;
+}
+
+// A context with no device state holding one instance's model (no staged
+// fields): the structure a batch of the serving loop is keyed by.
+int ctx_model_copy(gc_ctx* m, int inst, gc_ctx** out) {
+    gc_ctx* c = nullptr;
+    TRY(gc_ctx_create(m->device, 0, &c));
+    c->inst.push_back(m->inst[inst]);
+    c->inst.back().staged.clear();
+    *out = c;
+    return GC_OK;
+}
+
+int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pair<gc_ctx*, int>>& src,
+             gc_ctx** out, std::string* err) {
+    *out = nullptr;
+    gc_ctx* ctx = nullptr;
+    TRY(gc_ctx_create(device, budget, &ctx));
+    auto fail = [&](int st) {
+        if (err) *err = ctx->err;
+        gc_ctx_destroy(ctx);
+        return st;
+    };
+    for (auto& p : src) {
+        ctx->inst.push_back(p.first->inst[p.second]);
+        ctx->inst.back().staged.clear();
+    }
+    int st = gc_finalize(ctx);
+    if (st) return fail(st);
+    st = gc_set_precision(ctx, precision);
+    if (st) return fail(st);
+    // device state of instances that come from running contexts
+    for (auto& p : src)
+        if (p.first->finalized) cudaStreamSynchronize(p.first->stream);
+    PackSeg* d_seg = nullptr;
+    if (cudaMalloc(&d_seg, sizeof(PackSeg) * std::max<size_t>(src.size(), 1)) != cudaSuccess)
+        return fail(seterr(ctx, GC_ERR_OOM, "pack table"));
+    for (size_t s = 0; s < ctx->slots.size(); ++s) {
+        DSlot& D = ctx->slots[s];
+        for (int f = -1; f < NF; ++f) {  // -1: ids
+            if (f >= 0 && !D.ncomp[f]) continue;
+            std::vector<PackSeg> seg;
+            int64_t nmax = 0;
+            for (size_t k = 0; k < src.size(); ++k) {
+                gc_ctx* sc = src[k].first;
+                if (!sc->finalized) continue;
+                DSlot& S = sc->slots[s];
+                const int si = src[k].second;
+                PackSeg g;
+                g.src = f < 0 ? (const void*)S.id[S.cur] : (const void*)S.F(f);
+                g.src_stride = S.N;
+                g.src_base = S.h_inst[si].base;
+                g.dst_base = D.h_inst[k].base;
+                g.n = S.h_inst[si].n;
+                nmax = std::max(nmax, g.n);
+                seg.push_back(g);
+            }
+            if (seg.empty() || nmax == 0) continue;
+            if (cudaMemcpyAsync(d_seg, seg.data(), sizeof(PackSeg) * seg.size(), cudaMemcpyHostToDevice,
+                                ctx->stream) != cudaSuccess) {
+                cudaFree(d_seg);
+                return fail(seterr(ctx, GC_ERR_CUDA, "pack table upload"));
+            }
+            dim3 grid((unsigned)std::min<int64_t>((nmax + 255) / 256, 64), (unsigned)seg.size());
+            if (f < 0) k_pack<int32_t><<<grid, 256, 0, ctx->stream>>>(d_seg, 1, D.id[D.cur], D.N);
+            else k_pack<double><<<grid, 256, 0, ctx->stream>>>(d_seg, D.ncomp[f], D.F(f), D.N);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+            // the table is reused by the next launch: wait for this one
+            cudaStreamSynchronize(ctx->stream);
+        }
+        for (size_t k = 0; k < src.size(); ++k)
+            if (src[k].first->finalized) D.nonzero_kin[k] = src[k].first->slots[s].nonzero_kin[src[k].second];
+    }
+    cudaFree(d_seg);
+    st = check_launch(ctx, "pack");
+    if (st) return fail(st);
+    // instances that come from model contexts: their staged fields
+    for (size_t k = 0; k < src.size(); ++k) {
+        gc_ctx* sc = src[k].first;
+        if (sc->finalized) continue;
+        for (auto& f : sc->inst[src[k].second].staged) {
+            st = gc_upload_field(ctx, (int)k, f.handle, f.field, f.bytes.data(), f.bytes.size());
+            if (st) return fail(st);
+        }
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    *out = ctx;
+    return GC_OK;
+}
+
+// (handle, field, bytes) of every result field of one instance's systems.
+void ctx_result_fields(gc_ctx* c, int inst, std::vector<std::array<int64_t, 3>>& out) {
+    out.clear();
+    const HInst& I = c->inst[inst];
+    for (size_t h = 0; h < I.handles.size(); ++h) {
+        if (I.handles[h].type != H_SYS) continue;
+        const HSys& s = I.sys[I.handles[h].idx];
+        for (int f = 0; f < GC_NFIELDS; ++f) {
+            const int comps = sys_comps(s, f);
+            if (comps <= 0) continue;
+            out.push_back({(int64_t)h, (int64_t)f, s.n * comps * 8});
+        }
+    }
+}
+
+const char* ctx_error(gc_ctx* c) { return c->err.c_str(); }
+
+}  // namespace gc

@@ -13,7 +13,7 @@ from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, 
                     LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
                     StressParticleSystem, SystemInteraction, TaitEOSUpdater, WenlandC2Kernel,
                     ZeroFieldUpdater, is_coupled)
-from .engine import (CudaBackend, GcError, Session, compile_instance, download_instance, load_library,
+from .engine import (CudaBackend, GcError, Server, Session, compile_instance, download_instance, load_library,
                      time_integrate, upload_instance)
 
 PRECISION_FP64 = consts.GC_PRECISION_FP64

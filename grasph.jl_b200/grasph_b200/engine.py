@@ -94,6 +94,16 @@ def load_library(path: os.PathLike | None = None):
         "gc_set_profiling": (ct.c_int, [ct.c_void_p, ct.c_int]),
         "gc_measure_fp64_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
         "gc_set_graphs": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
+        "gc_stage_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
+        "gc_serve_create": (ct.c_int, [ct.c_int, ct.c_size_t, ct.c_int, ct.c_int, ct.POINTER(ct.c_void_p)]),
+        "gc_serve_destroy": (ct.c_int, [ct.c_void_p]),
+        "gc_serve_last_error": (ct.c_char_p, [ct.c_void_p]),
+        "gc_serve_submit": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double, _i64p]),
+        "gc_serve_pump": (ct.c_int, [ct.c_void_p, _ip]),
+        "gc_serve_poll": (ct.c_int, [ct.c_void_p, ct.c_int64, _ip, _i64p, _dp, _dp, _dp]),
+        "gc_serve_download": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
+        "gc_serve_release": (ct.c_int, [ct.c_void_p, ct.c_int64]),
+        "gc_serve_get_stats": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -192,6 +202,11 @@ class CudaBackend:
         self._chk(self.lib.gc_finalize(self.ctx), "gc_finalize")
 
     # -- state
+    def stage(self, inst, handle, field, array):
+        a = np.ascontiguousarray(array)
+        self._chk(self.lib.gc_stage_field(self.ctx, inst, handle, field, a.ctypes.data, a.nbytes),
+                  "gc_stage_field")
+
     def upload(self, inst, handle, field, array):
         a = np.ascontiguousarray(array)
         self._chk(self.lib.gc_upload_field(self.ctx, inst, handle, field, a.ctypes.data, a.nbytes),
@@ -524,3 +539,99 @@ def time_integrate(integrator: LeapFrogTimeIntegrator, num_timesteps: int, print
     if print_timer:
         print(timer)
     return timer
+
+
+# ---------------------------------------------------------------- serving
+
+class ServeStats(ct.Structure):
+    _fields_ = [("queued", ct.c_int64), ("running", ct.c_int64), ("batches", ct.c_int64),
+                ("rounds", ct.c_int64), ("repacks", ct.c_int64), ("particle_steps", ct.c_int64),
+                ("device_bytes_reserved", ct.c_int64)]
+
+
+class Server:
+    """Many simulations on one device (gc_serve_*): submit integrators at any
+    time, pump rounds, fetch each result when its request is done.
+
+    Simulations of one model structure share a packed context and step
+    together; a result is bit-identical to the same simulation run alone in
+    a Session of the same precision.
+    """
+
+    QUEUED, RUNNING, DONE, FAILED = C.GC_REQ_QUEUED, C.GC_REQ_RUNNING, C.GC_REQ_DONE, C.GC_REQ_FAILED
+
+    def __init__(self, *, device=0, hbm_budget=150 * 10**9, round_steps=50,
+                 precision=C.GC_PRECISION_FP32_COMPENSATED, lib=None):
+        self.lib = lib or load_library()
+        self.srv = ct.c_void_p()
+        self.device = device
+        self._chk(self.lib.gc_serve_create(device, int(hbm_budget), round_steps, precision, ct.byref(self.srv)),
+                  "gc_serve_create")
+        self.maps = {}
+
+    def _chk(self, st, where=""):
+        if st != 0:
+            msg = (self.lib.gc_serve_last_error(self.srv) or b"").decode() if self.srv else ""
+            raise GcError(st, f"{where}: {msg}")
+
+    def close(self):
+        if self.srv:
+            self.lib.gc_serve_destroy(self.srv)
+            self.srv = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, lf: LeapFrogTimeIntegrator, nsteps: int, cfl: float) -> int:
+        """Queue one simulation; its current host state is copied now."""
+        be = CudaBackend(self.device, 0, lib=self.lib)
+        inst = be.instance_add()
+        m = compile_instance(be, inst, lf.systems, lf.interactions, lf.ghosts, lf.gamma)
+        for ps in m.systems:
+            h = m.h(ps)
+            for name, fid in ps.particle_fields():
+                be.stage(inst, h, fid, getattr(ps, name))
+        req = ct.c_int64()
+        st = self.lib.gc_serve_submit(self.srv, be.ctx, nsteps, cfl, ct.byref(req))
+        if st != 0:
+            be.close()
+            self._chk(st, "gc_serve_submit")
+        be.ctx = ct.c_void_p()  # owned by the server now
+        self.maps[req.value] = (lf, m)
+        return req.value
+
+    def pump(self) -> int:
+        n = ct.c_int()
+        self._chk(self.lib.gc_serve_pump(self.srv, ct.byref(n)), "gc_serve_pump")
+        return n.value
+
+    def poll(self, req):
+        st, done = ct.c_int(), ct.c_int64()
+        ts, ta, td = ct.c_double(), ct.c_double(), ct.c_double()
+        self._chk(self.lib.gc_serve_poll(self.srv, req, ct.byref(st), ct.byref(done), ct.byref(ts), ct.byref(ta),
+                                         ct.byref(td)), "gc_serve_poll")
+        return {"state": st.value, "steps_done": done.value, "t_submit": ts.value, "t_admit": ta.value,
+                "t_done": td.value}
+
+    def fetch(self, req):
+        """Write a finished request's fields into its integrator's arrays."""
+        lf, m = self.maps[req]
+        for ps in m.systems:
+            h = m.h(ps)
+            for name, fid in ps.particle_fields():
+                a = getattr(ps, name)
+                self._chk(self.lib.gc_serve_download(self.srv, req, h, fid, a.ctypes.data, a.nbytes),
+                          "gc_serve_download")
+        return lf
+
+    def release(self, req):
+        self._chk(self.lib.gc_serve_release(self.srv, req), "gc_serve_release")
+        self.maps.pop(req, None)
+
+    def stats(self):
+        s = ServeStats()
+        self._chk(self.lib.gc_serve_get_stats(self.srv, ct.byref(s)), "gc_serve_get_stats")
+        return {f: getattr(s, f) for f, _ in ServeStats._fields_}

@@ -297,6 +297,49 @@ int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, in
 int gc_cell_sort_perm_noalloc(const double* x_planar, int64_t n, int ndims, double cutoff,
                               int32_t* perm_out, void* stream);
 
+/* ============================================================= serving */
+/* No counterpart in the reference (one simulation per Julia process).  A
+ * server steps many simulations ("requests") on one device: requests are
+ * admitted in arrival order while their estimated device memory fits
+ * `hbm_budget_bytes`, simulations of one model structure are packed into
+ * shared contexts ("batches") and stepped together, batches of different
+ * structures run concurrently.  At every round boundary finished requests
+ * leave, queued ones join, and each batch advances at most `round_steps`
+ * steps (fewer when a request needs fewer to finish, so every request ends
+ * exactly at its own step count).  A request's result is bit-identical to
+ * the same simulation run alone in a context of the same precision.       */
+typedef struct gc_server gc_server;
+typedef struct gc_serve_stats {
+    int64_t queued, running, batches;
+    int64_t rounds, repacks;
+    int64_t particle_steps;          /* moving particles × steps, all requests */
+    int64_t device_bytes_reserved;   /* estimates of the admitted requests     */
+} gc_serve_stats;
+enum { GC_REQ_FAILED = -1, GC_REQ_QUEUED = 0, GC_REQ_RUNNING = 1, GC_REQ_DONE = 2 };
+
+int gc_serve_create(int device, size_t hbm_budget_bytes, int round_steps, int precision, gc_server** out);
+int gc_serve_destroy(gc_server* srv);
+const char* gc_serve_last_error(gc_server* srv);
+/* `model`: a context with one instance built by gc_instance_add/gc_add_*
+ * and filled by gc_stage_field, not finalized.  The server owns it from
+ * here on (released by gc_serve_release).  Runs `nsteps` steps at `cfl`.  */
+int gc_serve_submit(gc_server* srv, gc_ctx* model, int nsteps, double cfl, int64_t* req_out);
+/* One round: admit, repack, step every batch, retire finished requests
+ * (their fields are copied to host memory).                              */
+int gc_serve_pump(gc_server* srv, int* ncompleted);
+/* state: GC_REQ_*; times in seconds since gc_serve_create (-1: not yet). */
+int gc_serve_poll(gc_server* srv, int64_t req, int* state, int64_t* steps_done, double* t_submit,
+                  double* t_admit, double* t_done);
+/* A finished request's field, same layout as gc_download_field.          */
+int gc_serve_download(gc_server* srv, int64_t req, int handle, int field, void* host, size_t bytes);
+int gc_serve_release(gc_server* srv, int64_t req);
+int gc_serve_get_stats(gc_server* srv, gc_serve_stats* out);
+
+/* Before gc_finalize: keep a copy of a field in host memory; gc_finalize
+ * (or a server admitting the request) uploads it.  Same layout and checks
+ * as gc_upload_field.                                                     */
+int gc_stage_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes);
+
 #ifdef __cplusplus
 }
 #endif
