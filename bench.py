@@ -443,13 +443,136 @@ def run_batched(args, rank, world, local_rank):
     sess.close()
 
 
+def serve_requests(rate, count, seed):
+    """The serving mix: Poisson arrivals at `rate` req/s; 70% 2-D
+    Drucker-Prager column collapses (N ~ logU[5k, 200k], parameters as the
+    batched columns), 30% 3-D dam breaks (N ~ logU[50k, 1M] fluid, dx scaled
+    so the 2:1:4 block holds N); 1000 steps each."""
+    from grasph_b200 import scenarios
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(count):
+        t += rng.exponential(1.0 / rate)
+        if rng.uniform() < 0.7:
+            N = math.exp(rng.uniform(math.log(5000), math.log(200000)))
+            ar = rng.uniform(0.5, 4.0)
+            nx = max(2, int(round(math.sqrt(N / ar))))
+            ny = max(2, int(round(N / nx)))
+            kind = ("column", dict(nx=nx, ny=ny, dx=0.0005, phi_deg=rng.uniform(25.0, 40.0),
+                                   E=rng.uniform(0.5e6, 5.0e6)))
+        else:
+            N = math.exp(rng.uniform(math.log(50000), math.log(1000000)))
+            k = (N / 8.0) ** (1.0 / 3.0)
+            nx, ny, nz = max(2, int(round(2 * k))), max(1, int(round(k))), max(2, int(round(4 * k)))
+            kind = ("dambreak_3d", dict(nx=nx, ny=ny, nz=nz, dx=0.5 / max(1, int(round(k)))))
+        out.append((t, kind, 1000))
+    return out
+
+
+def _build_request(kind):
+    from grasph_b200 import scenarios
+    name, kw = kind
+    if name == "column":
+        return scenarios.column_collapse(**kw)
+    return scenarios.dambreak_3d(**kw)
+
+
+def run_serve(args, rank, world, local_rank):
+    """Continuous batching over the serving mix at several arrival rates:
+    throughput and time-to-completion percentiles, FP32-compensated."""
+    import torch
+    import grasph_b200 as G
+    torch.cuda.set_device(local_rank)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    count = args.serve_requests
+    per_rate = []
+    for rate in rates:
+        reqs = serve_requests(rate, count, seed=20261203 + int(rate))
+        built = [(t, _build_request(kind), n, kind) for t, kind, n in reqs]  # host inputs made before timing
+        srv = G.Server(device=local_rank, hbm_budget=150 * 10**9, round_steps=args.serve_round,
+                       precision=G.PRECISION_FP32_COMPENSATED)
+        t0 = time.perf_counter()
+        ids = []
+        nxt = 0
+        while True:
+            now = time.perf_counter() - t0
+            while nxt < len(built) and built[nxt][0] <= now:
+                t_arr, (lf, meta), n, _ = built[nxt]
+                ids.append((srv.submit(lf, n, meta["cfl"]), t_arr, meta))
+                nxt += 1
+            st = srv.stats()
+            if st["queued"] == 0 and st["running"] == 0:
+                if nxt == len(built):
+                    break
+                time.sleep(max(0.0, built[nxt][0] - (time.perf_counter() - t0)))
+                continue
+            srv.pump()
+        wall = time.perf_counter() - t0
+        ttc, moving = [], 0
+        for rid, t_arr, meta in ids:
+            info = srv.poll(rid)
+            assert info["state"] == G.Server.DONE, info
+            ttc.append(info["t_done"] - t_arr)
+            moving += meta["n_fluid"] * 1000
+        st = srv.stats()
+        per_rate.append({"rate_req_per_s": rate, "requests": len(ids), "particle_steps": moving,
+                         "throughput": moving / wall, "wall_s": wall,
+                         "ttc_p50_s": float(np.percentile(ttc, 50)), "ttc_p99_s": float(np.percentile(ttc, 99)),
+                         "rounds": st["rounds"], "repacks": st["repacks"]})
+        srv.close()
+    # density error of served requests against the plain FP64 path: the
+    # smallest request of each kind, re-run alone
+    err = {}
+    sample = serve_requests(rates[-1], count, seed=20261203 + int(rates[-1]))
+    for name in ("column", "dambreak_3d"):
+        cand = [(r[1][1].get("nx", 0) * r[1][1].get("ny", 0) * r[1][1].get("nz", 1), r) for r in sample
+                if r[1][0] == name]
+        if not cand:
+            continue
+        _, (t, kind, n) = min(cand, key=lambda c: c[0])
+        (lf32, m32), (lf64, _) = _build_request(kind), _build_request(kind)
+        srv = G.Server(device=local_rank, round_steps=args.serve_round, precision=G.PRECISION_FP32_COMPENSATED)
+        rid = srv.submit(lf32, n, m32["cfl"])
+        while srv.poll(rid)["state"] != G.Server.DONE:
+            srv.pump()
+        srv.fetch(rid)
+        srv.close()
+        s64 = G.Session([lf64], device=local_rank)
+        s64.push()
+        s64.step(n, m32["cfl"])
+        s64.pull(with_ghosts=False)
+        s64.close()
+        a, b = lf32.systems[0], lf64.systems[0]
+        ia, ib = np.argsort(a.id), np.argsort(b.id)
+        e = {"rho": float(np.abs(a.rho[ia] - b.rho[ib]).max() / np.abs(b.rho).max())}
+        if hasattr(a, "stress"):
+            e["stress"] = float(np.abs(a.stress[ia] - b.stress[ib]).max() / np.abs(b.stress).max())
+        err[name] = dict(e, steps=n, particles=int(m32["n_fluid"]))
+    top = per_rate[-1]
+    line = {
+        "metric": METRIC, "value": top["throughput"], "unit": "particle-steps/s", "n_gpus": world,
+        "steps": 1000, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-compensated", "data": "synthetic",
+        "config": {"workload": "serving mix (70% 2-D DP columns 5k-200k, 30% 3-D dam breaks 50k-1M)",
+                   "requests_per_rate": count, "round_steps": args.serve_round, "hbm_budget_gb": 150,
+                   "parallelism": f"replicas x{world}"},
+        "serving": per_rate, "fp32c_vs_fp64": err, "e2e": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column", "batched"])
+    ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column", "batched", "serve"])
+    ap.add_argument("--serve-rates", default="10,100,500")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-round", type=int, default=50)
     ap.add_argument("--scale", default="full", choices=["full", "small"])
     ap.add_argument("--precision", default="fp32c", choices=["fp64", "fp32c"])
     ap.add_argument("--no-fp64-compare", action="store_true")
@@ -472,6 +595,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.workload == "batched":
         run_batched(args, rank, world, local_rank)
+    elif args.workload == "serve":
+        run_serve(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
     if world > 1:
