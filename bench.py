@@ -355,6 +355,9 @@ def run_ours(args, rank, world, local_rank):
                        precision=args.precision),
         "pair_interactions_per_s": pair_rate, "pairs_per_step": pairs,
         "gpu_launches": launches, "clocks": clk, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
+        "schedule": {"graph_steps": st1["graph_steps"] - st0["graph_steps"],
+                     "rollbacks": st1["rollbacks"] - st0["rollbacks"],
+                     "sweep_cfg_chosen": st1["sweep_cfg_chosen"]},
         "fp64_plain": fp64,
     }
     if rank == 0:
@@ -436,6 +439,9 @@ def run_batched(args, rank, world, local_rank):
                    "precision": args.precision},
         "gpu_launches": launches, "clocks": clk, "e2e": None,
         "sweep": {"avg_launch_ms": sweep_ms / sweep_launches, "share_of_step": sweep_ms / ms},
+        "schedule": {"graph_steps": st1["graph_steps"] - st0["graph_steps"],
+                     "rollbacks": st1["rollbacks"] - st0["rollbacks"],
+                     "sweep_cfg_chosen": st1["sweep_cfg_chosen"]},
         "one_by_one_fp64": one, "cpu_baseline": None,
     }
     if rank == 0:

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -201,7 +202,17 @@ struct gc_ctx {
     int64_t* d_total_cells = nullptr;  // device copy of the current sort's cell total
     int64_t grid_version = 0;
     int num_sms = 148;
-    int force_cfg = 0;
+    int force_cfg = -1;  // fixed sweep configuration, -1: autotune
+    // autotuning: per (slot, stage, functor) sweep, one timed launch per
+    // configuration, then the fastest
+    struct Tune {
+        int best = -1, next = 0;
+        double ms[NUM_FORCE_CFG] = {};
+    };
+    std::map<int64_t, Tune> tune;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev;
+    std::vector<std::pair<int64_t, int>> tune_rec;  // (key, cfg) of each used tune_ev pair
+    int64_t tune_version = 0;
     // host I/O staging (device side of AoS <-> planar transposes)
     double* staging = nullptr;
     int64_t cap_staging = 0;  // doubles
@@ -1196,7 +1207,29 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.prec = fp32 ? GC_PRECISION_FP32_COMPENSATED : GC_PRECISION_FP64;
     A.err = ctx->d_err;
     A.num_sms = ctx->num_sms;
-    A.cfg = ctx->force_cfg;
+    A.cfg = 0;
+    int tune_slot = -1;
+    if (ctx->force_cfg >= 0) {
+        A.cfg = ctx->force_cfg;
+    } else if (!count_only) {
+        const int64_t key = ((int64_t)a * 16 + stage) * 8 + pfn;
+        auto& t = ctx->tune[key];
+        if (t.best >= 0) {
+            A.cfg = t.best;
+        } else if (ctx->steps_done > 0 && !ctx->capturing && t.next < NUM_FORCE_CFG) {
+            // time this configuration once (the first step, with its cold
+            // sorts, is not timed)
+            A.cfg = t.next++;
+            if (ctx->tune_rec.size() == ctx->tune_ev.size()) {
+                cudaEvent_t e0, e1;
+                CU(cudaEventCreate(&e0));
+                CU(cudaEventCreate(&e1));
+                ctx->tune_ev.push_back({e0, e1});
+            }
+            tune_slot = (int)ctx->tune_rec.size();
+            ctx->tune_rec.push_back({key, A.cfg});
+        }
+    }
     A.nref = 0;
     for (int id : ids)
         if (!ctx->inters[id].grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
@@ -1275,8 +1308,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         // inside a capture the record must become a node of the graph
         CU(cudaEventRecordWithFlags(e0, ctx->stream, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     }
+    if (tune_slot >= 0) CU(cudaEventRecord(ctx->tune_ev[tune_slot].first, ctx->stream));
     int st = launch_force_f64(A, count_only, ctx->stream);
     if (st) return seterr(ctx, st, "functor/system combination not implemented on the device");
+    if (tune_slot >= 0) CU(cudaEventRecord(ctx->tune_ev[tune_slot].second, ctx->stream));
     if (e1)
         CU(cudaEventRecordWithFlags(e1, ctx->stream, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     TRY(check_launch(ctx, "sweep"));
@@ -1431,6 +1466,20 @@ int one_step(gc_ctx* ctx) {
 }
 
 int collect_profile(gc_ctx* ctx) {
+    for (size_t i = 0; i < ctx->tune_rec.size(); ++i) {
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, ctx->tune_ev[i].first, ctx->tune_ev[i].second));
+        auto& t = ctx->tune[ctx->tune_rec[i].first];
+        t.ms[ctx->tune_rec[i].second] += ms;
+        if (t.next == NUM_FORCE_CFG && t.best < 0) {
+            int b = 0;
+            for (int c = 1; c < NUM_FORCE_CFG; ++c)
+                if (t.ms[c] < t.ms[b]) b = c;
+            t.best = b;
+            ctx->tune_version++;
+        }
+    }
+    ctx->tune_rec.clear();
     for (size_t i = 0; i < ctx->ev_used; ++i) {
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, ctx->ev_pool[i].first, ctx->ev_pool[i].second));
@@ -1482,7 +1531,19 @@ void set_parity(gc_ctx* ctx, const std::vector<char>& p) {
     for (auto& G : ctx->ghosts) G.cur = p[i++];
 }
 
-int graph_key(gc_ctx* ctx) { return (ctx->precision * 64 + ctx->force_cfg) * 2 + (ctx->profiling ? 1 : 0); }
+int graph_key(gc_ctx* ctx) {
+    return (int)(((ctx->precision * 64 + ctx->force_cfg + 1) * 2 + (ctx->profiling ? 1 : 0)) * 4096 +
+                 ctx->tune_version % 4096);
+}
+
+// Steps stay exact (and timed) until every sweep has its configuration.
+bool tuning(gc_ctx* ctx) {
+    if (ctx->force_cfg >= 0) return false;
+    if (ctx->tune.empty()) return true;
+    for (auto& kv : ctx->tune)
+        if (kv.second.best < 0) return true;
+    return false;
+}
 
 int grow_gcols(gc_ctx* ctx, DSlot& S, int64_t ncols) {
     if (ncols + 1 <= S.cap_gcols) return GC_OK;
@@ -1683,7 +1744,7 @@ int run_steps(gc_ctx* ctx, int nsteps) {
     bool graphs = ctx->graphs_on && !env_off;
     int done = 0;
     while (done < nsteps) {
-        if (!graphs || !ctx->exact_done) {
+        if (!graphs || !ctx->exact_done || tuning(ctx)) {
             ctx->capmode = false;
             TRY(one_step(ctx));
             ctx->exact_done = true;
@@ -1772,7 +1833,7 @@ int gc_ctx_create(int device, size_t hbm_budget_bytes, gc_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return GC_ERR_CUDA;
     gc_ctx* ctx = new gc_ctx();
     ctx->device = device;
-    if (const char* e = getenv("GC_FORCE_CFG")) ctx->force_cfg = atoi(e);
+    if (const char* e = getenv("GC_FORCE_CFG")) ctx->force_cfg = std::min(std::max(atoi(e), -1), NUM_FORCE_CFG - 1);
     ctx->budget = hbm_budget_bytes;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
@@ -1860,6 +1921,10 @@ int gc_ctx_destroy(gc_ctx* ctx) {
     cudaFree(ctx->staging);
     cudaFree(ctx->d_pairs);
     for (auto& e : ctx->ev_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    for (auto& e : ctx->tune_ev) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
@@ -2296,6 +2361,8 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
     out->sweep_ms = ctx->sweep_ms;
     out->graph_steps = ctx->graph_steps;
     out->rollbacks = ctx->rollbacks;
+    for (auto& kv : ctx->tune)
+        if (kv.second.best >= 0 && kv.second.best < 4) out->sweep_cfg_chosen[kv.second.best] += 1;
     if (ctx->finalized && ctx->steps_done > 0) {
         if (!ctx->d_pairs) TRY(dalloc(ctx, &ctx->d_pairs, 1));
         int64_t pairs = 0;
@@ -2513,11 +2580,22 @@ int gc_set_profiling(gc_ctx* ctx, int on) {
     return GC_OK;
 }
 
-int gc_set_graphs(gc_ctx* ctx, int on, int sync_every) {
+int gc_set_sweep_config(gc_ctx* ctx, int cfg) {
+    if (!ctx) return GC_ERR_ARG;
+    if (cfg < -1 || cfg >= NUM_FORCE_CFG) return seterr(ctx, GC_ERR_ARG, "sweep configuration out of range");
+    ctx->force_cfg = cfg;
+    invalidate_steps(ctx);
+    return GC_OK;
+}
+
+int gc_set_graphs(gc_ctx* ctx, int on, int sync_every, double cap_margin) {
     if (!ctx) return GC_ERR_ARG;
     if (sync_every < 1) return seterr(ctx, GC_ERR_ARG, "sync_every must be at least 1");
+    if (cap_margin != 0.0 && !(cap_margin >= 1.0 && cap_margin <= 16.0))
+        return seterr(ctx, GC_ERR_ARG, "cap_margin must be 0 or in [1, 16]");
     ctx->graphs_on = on != 0;
     ctx->sync_every = sync_every;
+    if (cap_margin != 0.0) ctx->cap_margin = cap_margin;
     invalidate_steps(ctx);
     return GC_OK;
 }

@@ -9,7 +9,7 @@
 namespace gc {
 
 constexpr int FORCE_TPB = 128;  // threads per block of the sweep
-constexpr int FORCE_BUF = 64;   // largest staged-neighbour column (shared memory)
+constexpr int FORCE_BUF = 64;   // staged-neighbour column of the counting sweep (shared memory)
 
 // Launch configurations of the sweep: (min resident blocks, staged
 // neighbours per thread, pair-loop unroll).  Chosen per (system, stage) by
@@ -17,8 +17,8 @@ constexpr int FORCE_BUF = 64;   // largest staged-neighbour column (shared memor
 struct ForceCfg {
     int minb, buf, unroll;
 };
-constexpr int NUM_FORCE_CFG = 2;
-constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1}, {4, 64, 2}};
+constexpr int NUM_FORCE_CFG = GC_NUM_SWEEP_CONFIGS;
+constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1}, {4, 64, 2}, {3, 64, 1}, {4, 96, 1}};
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)

@@ -1,12 +1,9 @@
-// k_force_3d.cu — 3-D instantiations of the fused pair sweep.
-// Compiled with -fmad=false (reference rounding).
+// k_force_3d.cu — 3-D instantiations of the fused pair sweep, FP64 (and neighbour counting).
+// Compiled with -fmad=false (reference rounding of the FP64 parts).
 #include "k_force_impl.cuh"
 
 namespace gc {
 
-int launch_force_f64_3d(const ForceArgs& A, bool count_only, cudaStream_t s) {
-    if (A.kk == GC_KERNEL_CUBIC_SPLINE) return launch_nd<3, GC_KERNEL_CUBIC_SPLINE>(A, count_only, s);
-    return launch_nd<3, GC_KERNEL_WENDLAND_C2>(A, count_only, s);
-}
+GC_DEFINE_FORCE_TU(3, false, launch_force_3d_f64)
 
 }  // namespace gc

@@ -8,12 +8,16 @@
 
 namespace gc {
 
-int launch_force_f64_2d(const ForceArgs& A, bool count_only, cudaStream_t s);
-int launch_force_f64_3d(const ForceArgs& A, bool count_only, cudaStream_t s);
+int launch_force_2d_f64(const ForceArgs& A, bool count_only, cudaStream_t s);
+int launch_force_3d_f64(const ForceArgs& A, bool count_only, cudaStream_t s);
+int launch_force_2d_f32(const ForceArgs& A, bool count_only, cudaStream_t s);
+int launch_force_3d_f32(const ForceArgs& A, bool count_only, cudaStream_t s);
 
 int launch_force_f64(const ForceArgs& A, bool count_only, cudaStream_t s) {
     if (A.aN <= 0 || A.nref == 0) return 0;
-    return A.nd == 2 ? launch_force_f64_2d(A, count_only, s) : launch_force_f64_3d(A, count_only, s);
+    const bool f32 = A.prec == GC_PRECISION_FP32_COMPENSATED && !count_only && A.pfn != GC_PFN_COUNT;
+    if (A.nd == 2) return f32 ? launch_force_2d_f32(A, count_only, s) : launch_force_2d_f64(A, count_only, s);
+    return f32 ? launch_force_3d_f32(A, count_only, s) : launch_force_3d_f64(A, count_only, s);
 }
 
 // --------------------------------------------------------------- groups

@@ -801,63 +801,92 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     int64_t blocks = (warps * 32 + FORCE_TPB - 1) / FORCE_TPB;
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
-    size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
-    k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
+    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
+    auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll>;
+    if (smem > 48 * 1024) {
+        // beyond the default dynamic shared-memory limit: opt in once per kernel
+        static bool opted = false;
+        if (!opted) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            opted = true;
+        }
+    }
+    kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
 }
 
-template <int ND, int NS, int PFN, int KK>
+template <class Phys, int ND, int PFN>
+static void launch_cfg(const ForceArgs& A, cudaStream_t s) {
+    switch (A.cfg) {
+        case 1: launch_c<Phys, ND, PFN, 1>(A, s); break;
+        case 2: launch_c<Phys, ND, PFN, 2>(A, s); break;
+        case 3: launch_c<Phys, ND, PFN, 3>(A, s); break;
+        default: launch_c<Phys, ND, PFN, 0>(A, s); break;
+    }
+}
+
+// F32: this translation unit's precision (the FP32-compensated launches and
+// the FP64 ones are compiled separately).
+template <int ND, int NS, int PFN, int KK, bool F32>
 static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
-    using P64 = PhysF64<ND, NS, PFN, KK>;
-    using P32 = PhysF32<ND, NS, PFN, KK>;
-    if (count_only) {
-        int64_t blocks = (A.aN * 32 + FORCE_TPB - 1) / FORCE_TPB;
-        if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
-        if (blocks < 1) blocks = 1;
-        size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
-        k_sweep<P64, ND, PFN, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
-    } else if (A.prec == GC_PRECISION_FP32_COMPENSATED && PFN != GC_PFN_COUNT) {
-        if (A.cfg == 1) launch_c<P32, ND, PFN, 1>(A, s);
-        else launch_c<P32, ND, PFN, 0>(A, s);
+    if constexpr (F32) {
+        if constexpr (PFN != GC_PFN_COUNT) launch_cfg<PhysF32<ND, NS, PFN, KK>, ND, PFN>(A, s);
     } else {
-        if (A.cfg == 1 && KK == GC_KERNEL_CUBIC_SPLINE) launch_c<P64, ND, PFN, 1>(A, s);
-        else launch_c<P64, ND, PFN, 0>(A, s);
+        using P64 = PhysF64<ND, NS, PFN, KK>;
+        if (count_only) {
+            int64_t blocks = (A.aN * 32 + FORCE_TPB - 1) / FORCE_TPB;
+            if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
+            if (blocks < 1) blocks = 1;
+            size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
+            k_sweep<P64, ND, PFN, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
+        } else {
+            launch_cfg<P64, ND, PFN>(A, s);
+        }
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-template <int ND, int NS, int KK>
+template <int ND, int NS, int KK, bool F32>
 static int launch_pfn(const ForceArgs& A, bool count_only, cudaStream_t s) {
     switch (A.pfn) {
-        case GC_PFN_FLUID: launch_t<ND, NS, GC_PFN_FLUID, KK>(A, count_only, s); return 0;
-        case GC_PFN_COUNT: launch_t<ND, NS, GC_PFN_COUNT, KK>(A, count_only, s); return 0;
+        case GC_PFN_FLUID: launch_t<ND, NS, GC_PFN_FLUID, KK, F32>(A, count_only, s); return 0;
+        case GC_PFN_COUNT: launch_t<ND, NS, GC_PFN_COUNT, KK, F32>(A, count_only, s); return 0;
         case GC_PFN_CAUCHY_FLUID:
             if (NS == 0) return GC_ERR_UNSUPPORTED;
-            launch_t<ND, NS, GC_PFN_CAUCHY_FLUID, KK>(A, count_only, s);
+            launch_t<ND, NS, GC_PFN_CAUCHY_FLUID, KK, F32>(A, count_only, s);
             return 0;
         case GC_PFN_STRAIN_RATE:
             if (NS == 0) return GC_ERR_UNSUPPORTED;
-            launch_t<ND, NS, GC_PFN_STRAIN_RATE, KK>(A, count_only, s);
+            launch_t<ND, NS, GC_PFN_STRAIN_RATE, KK, F32>(A, count_only, s);
             return 0;
         case GC_PFN_STRAIN_RATE_VORTICITY:
             if (NS == 0) return GC_ERR_UNSUPPORTED;
-            launch_t<ND, NS, GC_PFN_STRAIN_RATE_VORTICITY, KK>(A, count_only, s);
+            launch_t<ND, NS, GC_PFN_STRAIN_RATE_VORTICITY, KK, F32>(A, count_only, s);
             return 0;
     }
     return GC_ERR_UNSUPPORTED;
 }
 
-template <int ND, int KK>
+template <int ND, int KK, bool F32>
 static int launch_nd(const ForceArgs& A, bool count_only, cudaStream_t s) {
     const bool stress_pfn = A.pfn == GC_PFN_CAUCHY_FLUID || A.pfn == GC_PFN_STRAIN_RATE ||
                             A.pfn == GC_PFN_STRAIN_RATE_VORTICITY;
-    if (!stress_pfn) return launch_pfn<ND, 0, KK>(A, count_only, s);
+    if (!stress_pfn) return launch_pfn<ND, 0, KK, F32>(A, count_only, s);
     if (ND == 2) {
-        if (A.ns == 3) return launch_pfn<ND, 3, KK>(A, count_only, s);
-        if (A.ns == 4) return launch_pfn<ND, 4, KK>(A, count_only, s);
+        if (A.ns == 3) return launch_pfn<ND, 3, KK, F32>(A, count_only, s);
+        if (A.ns == 4) return launch_pfn<ND, 4, KK, F32>(A, count_only, s);
         return GC_ERR_UNSUPPORTED;
     }
-    if (A.ns == 6) return launch_pfn<ND, 6, KK>(A, count_only, s);
+    if (A.ns == 6) return launch_pfn<ND, 6, KK, F32>(A, count_only, s);
     return GC_ERR_UNSUPPORTED;
 }
+
+// One translation unit per (dimension, precision): defines
+// launch_force_<ND>d_<f32|f64>.
+#define GC_DEFINE_FORCE_TU(NDIM, F32, NAME)                                               \
+    int NAME(const ForceArgs& A, bool count_only, cudaStream_t s) {                      \
+        if (A.kk == GC_KERNEL_CUBIC_SPLINE)                                               \
+            return launch_nd<NDIM, GC_KERNEL_CUBIC_SPLINE, F32>(A, count_only, s);        \
+        return launch_nd<NDIM, GC_KERNEL_WENDLAND_C2, F32>(A, count_only, s);             \
+    }
 
 }  // namespace gc

@@ -45,7 +45,8 @@ class GcStats(ct.Structure):
                 ("grid_inconsistent", ct.c_int64), ("kernel_launches", ct.c_int64),
                 ("sweep_launches", ct.c_int64), ("sweep_ms", ct.c_double),
                 ("last_status", ct.c_int32), ("pad", ct.c_int32),
-                ("graph_steps", ct.c_int64), ("rollbacks", ct.c_int64)]
+                ("graph_steps", ct.c_int64), ("rollbacks", ct.c_int64),
+                ("sweep_cfg_chosen", ct.c_int32 * 4)]
 
 
 _LIB = None
@@ -93,7 +94,8 @@ def load_library(path: os.PathLike | None = None):
         "gc_stream": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_void_p)]),
         "gc_set_profiling": (ct.c_int, [ct.c_void_p, ct.c_int]),
         "gc_measure_fp64_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
-        "gc_set_graphs": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
+        "gc_set_graphs": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double]),
+        "gc_set_sweep_config": (ct.c_int, [ct.c_void_p, ct.c_int]),
         "gc_stage_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         "gc_serve_create": (ct.c_int, [ct.c_int, ct.c_size_t, ct.c_int, ct.c_int, ct.POINTER(ct.c_void_p)]),
         "gc_serve_destroy": (ct.c_int, [ct.c_void_p]),
@@ -225,8 +227,11 @@ class CudaBackend:
     def set_precision(self, mode):
         self._chk(self.lib.gc_set_precision(self.ctx, mode), "gc_set_precision")
 
-    def set_graphs(self, on, sync_every=32):
-        self._chk(self.lib.gc_set_graphs(self.ctx, 1 if on else 0, sync_every), "gc_set_graphs")
+    def set_graphs(self, on, sync_every=32, cap_margin=0.0):
+        self._chk(self.lib.gc_set_graphs(self.ctx, 1 if on else 0, sync_every, cap_margin), "gc_set_graphs")
+
+    def set_sweep_config(self, cfg):
+        self._chk(self.lib.gc_set_sweep_config(self.ctx, cfg), "gc_set_sweep_config")
 
     def step(self, nsteps, cfl):
         self._chk(self.lib.gc_step(self.ctx, nsteps, cfl), "gc_step")
@@ -234,7 +239,9 @@ class CudaBackend:
     def stats(self):
         s = GcStats()
         self._chk(self.lib.gc_get_stats(self.ctx, ct.byref(s)), "gc_get_stats")
-        return {f: getattr(s, f) for f, _ in GcStats._fields_ if f != "pad"}
+        out = {f: getattr(s, f) for f, _ in GcStats._fields_ if f != "pad"}
+        out["sweep_cfg_chosen"] = list(s.sweep_cfg_chosen)
+        return out
 
     # -- phase hooks
     def sort(self, inst, handle, cutoff, n):

@@ -140,7 +140,12 @@ typedef struct gc_stats {
     int64_t graph_steps;         /* steps run as replays of a captured step graph */
     int64_t rollbacks;           /* verified windows re-run exactly (a capacity
                                     was outgrown inside the window)              */
+    int32_t sweep_cfg_chosen[4]; /* tuned (system, stage) sweeps per configuration */
 } gc_stats;
+
+/* Launch configurations of the pair sweep (block residency, staged
+ * neighbours per thread, pair-loop unroll); all give bit-identical results. */
+#define GC_NUM_SWEEP_CONFIGS 4
 
 /* ============================================================ lifecycle */
 /* Create a context on `device`; `hbm_budget_bytes` caps device allocations
@@ -233,11 +238,17 @@ int gc_set_profiling(gc_ctx* ctx, int on);
  * a step sized from buffer capacities as a CUDA graph (one per buffer
  * parity) and replays it, with no host round trip per step; every
  * `sync_every` steps (default 32) the host verifies the window, grows
- * capacities, and re-runs the window exactly from a device snapshot if a
- * plan outgrew them.  Results are bit-identical to on = 0 (every step
- * sized by one host read of its plan).  The environment variable
- * GC_GRAPHS=0 forces on = 0.                                              */
-int gc_set_graphs(gc_ctx* ctx, int on, int sync_every);
+ * capacities to `cap_margin` (>= 1, default 1.5; 0 keeps the current
+ * value) times the largest plan seen, and re-runs the window exactly from
+ * a device snapshot if a plan outgrew them.  Results are bit-identical to
+ * on = 0 (every step sized by one host read of its plan).  The environment
+ * variable GC_GRAPHS=0 forces on = 0.                                     */
+int gc_set_graphs(gc_ctx* ctx, int on, int sync_every, double cap_margin);
+/* cfg = -1 (default): autotune — the first steps of a context time every
+ * sweep configuration once per (system, stage) sweep and keep the fastest.
+ * 0 <= cfg < GC_NUM_SWEEP_CONFIGS: use that one everywhere.  The
+ * environment variable GC_FORCE_CFG=<cfg> has the same effect.            */
+int gc_set_sweep_config(gc_ctx* ctx, int cfg);
 /* Measured FP64 FMA issue rate of the device in TFLOP/s (2 flops per FMA):
  * the compute ceiling of the FP64 pair sweep.                             */
 int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out);

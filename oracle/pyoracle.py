@@ -169,7 +169,10 @@ class OracleBackend:
     def set_precision(self, mode):
         pass
 
-    def set_graphs(self, on, sync_every=32):
+    def set_graphs(self, on, sync_every=32, cap_margin=0.0):
+        pass
+
+    def set_sweep_config(self, cfg):
         pass
 
     def upload(self, inst, handle, field, array):

@@ -21,12 +21,12 @@ CASES = {
 }
 
 
-def _run(builder, kw, graphs, nsteps, sync_every=32, prec=G.PRECISION_FP64, tweak=None, calls=1):
+def _run(builder, kw, graphs, nsteps, sync_every=32, prec=G.PRECISION_FP64, tweak=None, calls=1, margin=0.0):
     lf, meta = builder(**kw)
     if tweak:
         tweak(lf)
     s = G.Session([lf], backend=make_backend("cuda"), precision=prec)
-    s.backend.set_graphs(graphs, sync_every)
+    s.backend.set_graphs(graphs, sync_every, margin)
     s.push()
     per = nsteps // calls
     for _ in range(calls):
@@ -65,7 +65,33 @@ def _fling(lf):
 def test_capacity_overflow_rolls_back_bit_identical():
     builder, kw = CASES["dambreak_2d"]
     lf_e, _ = _run(builder, kw, False, 40, tweak=_fling)
-    lf_g, st = _run(builder, kw, True, 40, sync_every=4, tweak=_fling)
+    lf_g, st = _run(builder, kw, True, 40, sync_every=4, tweak=_fling, margin=1.0)
     _same(lf_g, lf_e)
     assert st["rollbacks"] > 0
+    assert st["graph_steps"] > 0
+
+
+@pytest.mark.parametrize("prec", [G.PRECISION_FP64, G.PRECISION_FP32_COMPENSATED])
+def test_sweep_configs_bit_identical(prec):
+    """Every launch configuration the autotuner picks from gives the same bits."""
+    builder, kw = CASES["column"]
+    ref = None
+    for cfg in range(G.consts.GC_NUM_SWEEP_CONFIGS):
+        lf, meta = builder(**kw)
+        s = G.Session([lf], backend=make_backend("cuda"), precision=prec)
+        s.backend.set_sweep_config(cfg)
+        s.push()
+        s.step(12, meta["cfl"])
+        s.pull()
+        if ref is None:
+            ref = lf
+        else:
+            _same(lf, ref)
+
+
+def test_autotune_chooses_every_sweep():
+    builder, kw = CASES["column"]
+    lf, st = _run(builder, kw, True, 40)
+    # two stages of one system: both sweeps tuned, then graph replays
+    assert sum(st["sweep_cfg_chosen"]) == 2
     assert st["graph_steps"] > 0
