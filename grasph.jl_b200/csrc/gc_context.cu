@@ -216,6 +216,8 @@ struct gc_ctx {
     // host I/O staging (device side of AoS <-> planar transposes)
     double* staging = nullptr;
     int64_t cap_staging = 0;  // doubles
+    int* d_ioflags = nullptr;  // per uploaded field: nonzero seen
+    int cap_ioflags = 0;
     // stats / profiling
     int64_t steps_done = 0, resorts = 0;
     int last_status = 0;
@@ -1146,9 +1148,11 @@ int ghost_copy(gc_ctx* ctx, DGhost& G, int stage) {
     return check_launch(ctx, "ghost copy");
 }
 
+// FP32-sweep buffers of a slot or ghost set: N FP64 positions (pos_stride
+// each) followed by N FP32 records (pack_stride floats each).
 template <class T>
-int ensure_fpk(gc_ctx* ctx, T& X, int64_t N, int ncomp) {
-    int64_t need = N * ncomp;
+int ensure_fpk(gc_ctx* ctx, T& X, int64_t N, int nd, int ns) {
+    int64_t need = N * (2 * pos_stride(nd) + pack_stride(nd, ns));
     if (need > X.cap_fpk) {
         CU(cudaStreamSynchronize(ctx->stream));
         dfree(ctx, X.fpk, X.cap_fpk);
@@ -1174,12 +1178,16 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         if (pfn == GC_PFN_FLUID && ctx->inters[id].h_gi.size() && ctx->inst[0].inters[id].pp[stage - 1][3] == 1.0)
             fp32 = false;  // the S = 1 (multiphase) pressure form stays in FP64
     const int pk_ns = pfn == GC_PFN_CAUCHY_FLUID ? S.ns : 0;
+    // FP32 sweep buffers: positions, then records (see ensure_fpk)
+    auto xp_of = [](float* fpk) { return (double*)fpk; };
+    auto pk_of = [](float* fpk, int64_t N, int nd) { return fpk + N * 2 * pos_stride(nd); };
     if (pfn != GC_PFN_COUNT) {
-        launch_aux(mode, S.N, nullptr, S.F(F_RHO), S.F(F_P), S.inst_of, S.d_mass, S.aux, ctx->stream);
         if (fp32) {
-            TRY(ensure_fpk(ctx, S, S.N, S.nd + 3 + pk_ns));
-            launch_pack32(mode, S.N, nullptr, S.nd, pk_ns, S.F(F_V), S.F(F_RHO), S.F(F_P), S.F(F_STRESS), S.inst_of,
-                          S.d_mass, S.fpk, ctx->stream);
+            TRY(ensure_fpk(ctx, S, S.N, S.nd, pk_ns));
+            launch_pack32(mode, S.N, nullptr, S.nd, pk_ns, S.F(F_X), S.F(F_V), S.F(F_RHO), S.F(F_P), S.F(F_STRESS),
+                          S.inst_of, S.d_mass, xp_of(S.fpk), pk_of(S.fpk, S.N, S.nd), ctx->stream);
+        } else {
+            launch_aux(mode, S.N, nullptr, S.F(F_RHO), S.F(F_P), S.inst_of, S.d_mass, S.aux, ctx->stream);
         }
     }
     ForceArgs A{};
@@ -1203,7 +1211,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.a_mass = S.d_mass;
     A.a_cf = S.d_cf;
     A.a_massf = S.d_massf;
-    A.afp = fp32 ? S.fpk : nullptr;
+    A.afp = fp32 ? pk_of(S.fpk, S.N, S.nd) : nullptr;
     A.prec = fp32 ? GC_PRECISION_FP32_COMPENSATED : GC_PRECISION_FP64;
     A.err = ctx->d_err;
     A.num_sms = ctx->num_sms;
@@ -1257,15 +1265,17 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             r.bp = G.p;
             r.bstress = G.stress;
             r.bN = G.CAP;
-            if (pfn != GC_PFN_COUNT)
+            if (pfn != GC_PFN_COUNT && !fp32)
                 launch_aux(mode, G.CAP, G.d_count, G.rho, G.p, G.ginst[G.cur], G.d_mass, G.aux, ctx->stream);
             r.baux = G.aux;
             r.bfp = nullptr;
+            r.bxp = nullptr;
             if (fp32) {
-                TRY(ensure_fpk(ctx, G, G.CAP, G.nd + 3 + pk_ns));
-                launch_pack32(mode, G.CAP, G.d_count, G.nd, pk_ns, G.v, G.rho, G.p, G.stress, G.ginst[G.cur], G.d_mass,
-                              G.fpk, ctx->stream);
-                r.bfp = G.fpk;
+                TRY(ensure_fpk(ctx, G, G.CAP, G.nd, pk_ns));
+                launch_pack32(mode, G.CAP, G.d_count, G.nd, pk_ns, G.x[G.cur], G.v, G.rho, G.p, G.stress,
+                              G.ginst[G.cur], G.d_mass, xp_of(G.fpk), pk_of(G.fpk, G.CAP, G.nd), ctx->stream);
+                r.bfp = pk_of(G.fpk, G.CAP, G.nd);
+                r.bxp = xp_of(G.fpk);
             }
         } else {
             DSlot& B = ctx->slots[D.bslot];
@@ -1277,20 +1287,28 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             r.bstress = B.F(F_STRESS);
             r.bN = B.N;
             r.bfp = nullptr;
+            r.bxp = nullptr;
             if (D.btype == BT_SELF) {
                 r.baux = S.aux;
-                r.bfp = fp32 ? S.fpk : nullptr;
-            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT) {
+                if (fp32) {
+                    r.bfp = pk_of(S.fpk, S.N, S.nd);
+                    r.bxp = xp_of(S.fpk);
+                }
+            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT && !fp32) {
                 launch_aux(mode, B.N, nullptr, B.F(F_RHO), B.F(F_P), B.inst_of, B.d_mass, B.aux, ctx->stream);
                 r.baux = B.aux;
             } else {
                 r.baux = B.aux;
             }
-            if (fp32 && (D.btype == BT_SYSTEM || D.btype == BT_STATIC)) {
-                TRY(ensure_fpk(ctx, B, B.N, B.nd + 3 + pk_ns));
-                launch_pack32(mode, B.N, nullptr, B.nd, B.kind >= GC_SYS_STRESS ? pk_ns : 0, B.F(F_V), B.F(F_RHO),
-                              B.F(F_P), B.F(F_STRESS), B.inst_of, B.d_mass, B.fpk, ctx->stream);
-                r.bfp = B.fpk;
+            if (fp32 && D.btype != BT_SELF) {
+                // dynamic walls lend only their positions; other systems their records too
+                const bool rec = D.btype == BT_SYSTEM || D.btype == BT_STATIC;
+                TRY(ensure_fpk(ctx, B, B.N, B.nd, pk_ns));
+                launch_pack32(mode, B.N, nullptr, B.nd, pk_ns, B.F(F_X), B.F(F_V), B.F(F_RHO), B.F(F_P),
+                              B.kind >= GC_SYS_STRESS ? B.F(F_STRESS) : nullptr, B.inst_of, B.d_mass, xp_of(B.fpk),
+                              rec ? pk_of(B.fpk, B.N, B.nd) : nullptr, ctx->stream);
+                r.bxp = xp_of(B.fpk);
+                if (rec) r.bfp = pk_of(B.fpk, B.N, B.nd);
             }
         }
     }
@@ -1352,6 +1370,9 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         r.bstress = S.F(F_STRESS);
         r.baux = S.aux;
         r.bN = S.N;
+        r.bfp = nullptr;
+        r.bxp = nullptr;
+        R.afp = nullptr;
         st = launch_force_f64(R, false, ctx->stream);
         if (st) return seterr(ctx, st, "two-sided functor not implemented on the device");
         TRY(check_launch(ctx, "sweep (system_b side)"));
@@ -1919,6 +1940,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(sn.id);
     }
     cudaFree(ctx->staging);
+    cudaFree(ctx->d_ioflags);
     cudaFree(ctx->d_pairs);
     for (auto& e : ctx->ev_pool) {
         cudaEventDestroy(e.first);
@@ -2239,80 +2261,146 @@ static int resolve(gc_ctx* ctx, int inst, int handle, HandleRef* r) {
     return GC_OK;
 }
 
-int gc_upload_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes) {
-    if (ctx) invalidate_steps(ctx);
-    if (!ctx || !host) return GC_ERR_ARG;
-    HandleRef r;
-    TRY(resolve(ctx, inst, handle, &r));
-    if (r.ghost) return seterr(ctx, GC_ERR_ARG, "ghost fields are generated on the device");
-    DSlot& S = *r.slot;
-    const HSys& hs = ctx->inst[inst].sys[r.sys];
-    int comps = sys_comps(hs, field);
-    if (comps < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", field);
-    const int64_t n = hs.n, base = S.h_inst[inst].base;
-    if (bytes != (size_t)(n * comps * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
-    if (field == GC_FIELD_V_ADJUSTMENT) {
-        const double* in = (const double*)host;
-        for (int64_t i = 0; i < n * comps; ++i)
-            if (in[i] != 0.0) return seterr(ctx, GC_ERR_UNSUPPORTED, "non-zero v_adjustment (XSPH) is not supported");
-        return GC_OK;
-    }
-    if (field == GC_FIELD_ID) {
-        TRY(ensure_staging(ctx, n));
-        CU(cudaMemcpyAsync(ctx->staging, host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-        launch_i64_to_i32((const int64_t*)ctx->staging, S.id[S.cur] + base, n, ctx->stream);
-        CU(cudaStreamSynchronize(ctx->stream));
-        return check_launch(ctx, "upload");
-    }
-    int fs = field_slot(field);
-    const double* in = (const double*)host;
+// Nonzero test of uploaded kinematics (and of v_adjustment, which must be
+// zero) on the device: flag[k] = 1 when any of the n doubles is nonzero.
+__global__ void k_any_nonzero(const double* __restrict__ a, int64_t n, int* flag) {
     bool nz = false;
-    if (field == GC_FIELD_V || field == GC_FIELD_DVDT || field == GC_FIELD_DRHODT)
-        for (int64_t i = 0; i < n * comps && !nz; ++i) nz = in[i] != 0.0;
-    TRY(ensure_staging(ctx, n * comps));
-    CU(cudaMemcpyAsync(ctx->staging, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    launch_aos_to_planar(ctx->staging, S.F(fs), n, comps, S.N, base, ctx->stream);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        nz |= a[i] != 0.0;
+    if (__any_sync(0xffffffffu, nz) && (threadIdx.x & 31) == 0) *flag = 1;
+}
+
+static int ensure_ioflags(gc_ctx* ctx, int n) {
+    if (n > ctx->cap_ioflags) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, ctx->d_ioflags, (size_t)ctx->cap_ioflags);
+        const int cap = std::max(n, 64);
+        TRY(dalloc(ctx, &ctx->d_ioflags, (size_t)cap));
+        ctx->cap_ioflags = cap;
+    }
+    return GC_OK;
+}
+
+int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
+    if (!ctx || nio < 0 || (nio && !io)) return GC_ERR_ARG;
+    // validate everything first: nothing is written on a bad request
+    std::vector<HandleRef> ref(nio);
+    std::vector<int> comps(nio);
+    int64_t total = 0;
+    for (int q = 0; q < nio; ++q) {
+        const gc_field_io& f = io[q];
+        if (!f.host) return seterr(ctx, GC_ERR_ARG, "null host buffer");
+        TRY(resolve(ctx, f.inst, f.handle, &ref[q]));
+        if (ref[q].ghost) return seterr(ctx, GC_ERR_ARG, "ghost fields are generated on the device");
+        const HSys& hs = ctx->inst[f.inst].sys[ref[q].sys];
+        comps[q] = sys_comps(hs, f.field);
+        if (comps[q] < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", f.field);
+        if (f.bytes != (size_t)(hs.n * comps[q] * 8))
+            return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", f.bytes);
+        total += hs.n * comps[q];
+    }
+    TRY(ensure_staging(ctx, std::max<int64_t>(total, 1)));
+    TRY(ensure_ioflags(ctx, nio));
+    CU(cudaMemsetAsync(ctx->d_ioflags, 0, sizeof(int) * std::max(nio, 1), ctx->stream));
+    int64_t off = 0;
+    for (int q = 0; q < nio; ++q) {
+        const gc_field_io& f = io[q];
+        DSlot& S = *ref[q].slot;
+        const int64_t n = ctx->inst[f.inst].sys[ref[q].sys].n, base = S.h_inst[f.inst].base;
+        double* st = ctx->staging + off;
+        off += n * comps[q];
+        if (n == 0) continue;
+        CU(cudaMemcpyAsync(st, f.host, f.bytes, cudaMemcpyHostToDevice, ctx->stream));
+        const bool check = f.field == GC_FIELD_V || f.field == GC_FIELD_DVDT || f.field == GC_FIELD_DRHODT ||
+                           f.field == GC_FIELD_V_ADJUSTMENT;
+        if (check) {
+            k_any_nonzero<<<(unsigned)std::min<int64_t>((n * comps[q] + 255) / 256, 1024), 256, 0, ctx->stream>>>(
+                st, n * comps[q], ctx->d_ioflags + q);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+        if (f.field == GC_FIELD_V_ADJUSTMENT) continue;
+        if (f.field == GC_FIELD_ID) launch_i64_to_i32((const int64_t*)st, S.id[S.cur] + base, n, ctx->stream);
+        else launch_aos_to_planar(st, S.F(field_slot(f.field)), n, comps[q], S.N, base, ctx->stream);
+    }
+    std::vector<int> flags(std::max(nio, 1));
+    CU(cudaMemcpyAsync(flags.data(), ctx->d_ioflags, sizeof(int) * std::max(nio, 1), cudaMemcpyDeviceToHost,
+                       ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     TRY(check_launch(ctx, "upload"));
-    if (field == GC_FIELD_X) S.sorted_once = false;
-    if (field == GC_FIELD_V || field == GC_FIELD_DVDT || field == GC_FIELD_DRHODT) {
-        int64_t bit = field == GC_FIELD_V ? 1 : field == GC_FIELD_DVDT ? 2 : 4;
-        if (nz) S.nonzero_kin[inst] |= bit;
-        else S.nonzero_kin[inst] &= ~bit;
+    bool structural = false;
+    for (int q = 0; q < nio; ++q) {
+        const gc_field_io& f = io[q];
+        DSlot& S = *ref[q].slot;
+        if (f.field == GC_FIELD_V_ADJUSTMENT && flags[q])
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "non-zero v_adjustment (XSPH) is not supported");
+        if (f.field == GC_FIELD_X) {
+            // a system that is not sorted every step is sorted again
+            if (!S.moving) structural = true;
+            S.sorted_once = false;
+        }
+        if (f.field == GC_FIELD_V || f.field == GC_FIELD_DVDT || f.field == GC_FIELD_DRHODT) {
+            int64_t bit = f.field == GC_FIELD_V ? 1 : f.field == GC_FIELD_DVDT ? 2 : 4;
+            if (flags[q]) S.nonzero_kin[f.inst] |= bit;
+            else S.nonzero_kin[f.inst] &= ~bit;
+        }
     }
     for (auto& D : ctx->inters) D.grid_valid = false;
+    if (structural) invalidate_steps(ctx);
+    return GC_OK;
+}
+
+int gc_upload_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes) {
+    if (!ctx || !host) return GC_ERR_ARG;
+    gc_field_io f{inst, handle, field, 0, const_cast<void*>(host), bytes};
+    return gc_upload_fields(ctx, 1, &f);
+}
+
+int gc_download_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
+    if (!ctx || nio < 0 || (nio && !io)) return GC_ERR_ARG;
+    std::vector<HandleRef> ref(nio);
+    std::vector<int> comps(nio);
+    int64_t total = 0;
+    for (int q = 0; q < nio; ++q) {
+        const gc_field_io& f = io[q];
+        if (!f.host) return seterr(ctx, GC_ERR_ARG, "null host buffer");
+        TRY(resolve(ctx, f.inst, f.handle, &ref[q]));
+        if (ref[q].ghost) continue;
+        const HSys& hs = ctx->inst[f.inst].sys[ref[q].sys];
+        comps[q] = sys_comps(hs, f.field);
+        if (comps[q] < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", f.field);
+        if (f.bytes != (size_t)(hs.n * comps[q] * 8))
+            return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", f.bytes);
+        total += hs.n * comps[q];
+    }
+    TRY(ensure_staging(ctx, std::max<int64_t>(total, 1)));
+    int64_t off = 0;
+    for (int q = 0; q < nio; ++q) {
+        const gc_field_io& f = io[q];
+        if (ref[q].ghost) continue;
+        DSlot& S = *ref[q].slot;
+        const int64_t n = ctx->inst[f.inst].sys[ref[q].sys].n, base = S.h_inst[f.inst].base;
+        double* st = ctx->staging + off;
+        off += n * comps[q];
+        if (f.field == GC_FIELD_V_ADJUSTMENT) {
+            memset(f.host, 0, f.bytes);
+            continue;
+        }
+        if (n == 0) continue;
+        if (f.field == GC_FIELD_ID) launch_i32_to_i64(S.id[S.cur] + base, (int64_t*)st, n, ctx->stream);
+        else launch_planar_to_aos(S.F(field_slot(f.field)), st, n, comps[q], S.N, base, ctx->stream);
+        CU(cudaMemcpyAsync(f.host, st, f.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    TRY(check_launch(ctx, "download"));
+    for (int q = 0; q < nio; ++q)
+        if (ref[q].ghost) TRY(ghost_field_io(ctx, io[q].inst, *ref[q].ghost, io[q].field, io[q].host, io[q].bytes));
     return GC_OK;
 }
 
 int gc_download_field(gc_ctx* ctx, int inst, int handle, int field, void* host, size_t bytes) {
     if (!ctx || !host) return GC_ERR_ARG;
-    HandleRef r;
-    TRY(resolve(ctx, inst, handle, &r));
-    CU(cudaStreamSynchronize(ctx->stream));
-    if (r.ghost) return ghost_field_io(ctx, inst, *r.ghost, field, host, bytes);
-    DSlot& S = *r.slot;
-    const HSys& hs = ctx->inst[inst].sys[r.sys];
-    int comps = sys_comps(hs, field);
-    if (comps < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", field);
-    const int64_t n = hs.n, base = S.h_inst[inst].base;
-    if (bytes != (size_t)(n * comps * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", bytes);
-    if (field == GC_FIELD_V_ADJUSTMENT) {
-        memset(host, 0, bytes);
-        return GC_OK;
-    }
-    if (field == GC_FIELD_ID) {
-        TRY(ensure_staging(ctx, n));
-        launch_i32_to_i64(S.id[S.cur] + base, (int64_t*)ctx->staging, n, ctx->stream);
-        CU(cudaMemcpyAsync(host, ctx->staging, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
-        return check_launch(ctx, "download");
-    }
-    int fs = field_slot(field);
-    TRY(ensure_staging(ctx, n * comps));
-    launch_planar_to_aos(S.F(fs), ctx->staging, n, comps, S.N, base, ctx->stream);
-    CU(cudaMemcpyAsync(host, ctx->staging, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    return check_launch(ctx, "download");
+    gc_field_io f{inst, handle, field, 0, host, bytes};
+    return gc_download_fields(ctx, 1, &f);
 }
 
 int gc_get_count(gc_ctx* ctx, int inst, int handle, int64_t* n_out) {

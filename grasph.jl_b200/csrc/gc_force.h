@@ -12,13 +12,13 @@ constexpr int FORCE_TPB = 128;  // threads per block of the sweep
 constexpr int FORCE_BUF = 64;   // staged-neighbour column of the counting sweep (shared memory)
 
 // Launch configurations of the sweep: (min resident blocks, staged
-// neighbours per thread, pair-loop unroll).  Chosen per (system, stage) by
-// the tuner in gc_context.cu.
+// neighbours per thread, pair-loop unroll, prefetch ring).  Chosen per
+// (system, stage) by the tuner in gc_context.cu.
 struct ForceCfg {
-    int minb, buf, unroll;
+    int minb, buf, unroll, pre;  // pre: prefetch ring for the FP32-compensated pairs
 };
 constexpr int NUM_FORCE_CFG = GC_NUM_SWEEP_CONFIGS;
-constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1}, {4, 64, 2}, {3, 64, 1}, {4, 96, 1}};
+constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1, 0}, {4, 64, 1, 1}, {3, 64, 1, 1}, {4, 96, 1, 1}};
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)
@@ -35,7 +35,8 @@ struct InterRef {
     const int32_t* cs;    // packed CSR over system_b (global b indices)
     int64_t cs_cells;     // cells of cs that are valid (an instance beyond them is skipped)
     const double *bx, *bv, *brho, *bp, *bstress, *baux;
-    const float* bfp;     // FP32 pack of system_b (v, rho, aux, 1/rho, stress), planar
+    const float* bfp;     // FP32 records of system_b (v, rho, aux, 1/rho, stress), pack_stride floats each
+    const double* bxp;    // FP64 positions of system_b, pos_stride doubles each (FP32 sweep), or nullptr
     int64_t bN;           // planar stride of system_b's arrays
     int32_t* counts;      // optional per-particle accepted-pair counts
 };
@@ -50,7 +51,7 @@ struct ForceArgs {
     const double* a_mass;  // per-instance particle mass
     const float* a_cf;     // FP32 copies of the two above
     const float* a_massf;
-    const float* afp;      // FP32 pack of system_a (FP32-compensated precision)
+    const float* afp;      // FP32 records of system_a (FP32-compensated precision)
     int prec;              // GC_PRECISION_*
     int* err;
     const int2* groups;        // warp groups (start, count) of system_a particles
@@ -68,9 +69,15 @@ void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs
                         int64_t ncols_cap, int64_t cells_cap, int2* groups, int64_t* ngroups, cudaStream_t s);
 void launch_aux(int mode, int64_t N, const int64_t* count, const double* rho, const double* p,
                 const int32_t* inst_of, const double* mass, double* aux, cudaStream_t s);
-// FP32 pack (planar, stride N): v[nd], rho, aux(mode), 1/rho, stress[ns] (ns may be 0).
-void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* v, const double* rho,
-                   const double* p, const double* stress, const int32_t* inst_of, const double* mass, float* pk,
-                   cudaStream_t s);
+// Per-particle records of the FP32-compensated sweep, one record per
+// particle so a neighbour costs one or two sectors instead of one per field:
+//   pk:  v[nd], rho, aux(mode), 1/rho, stress[ns], zero padding — pack_stride floats
+//   xpk: x[nd] in FP64, zero padding — pos_stride doubles (the exact neighbour test)
+// Either may be nullptr.  ns may be 0; stress may be nullptr (zeros).
+__host__ __device__ constexpr int pack_stride(int nd, int ns) { return (nd + 3 + ns + 3) / 4 * 4; }
+__host__ __device__ constexpr int pos_stride(int nd) { return nd == 2 ? 2 : 4; }
+void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* x, const double* v,
+                   const double* rho, const double* p, const double* stress, const int32_t* inst_of,
+                   const double* mass, double* xpk, float* pk, cudaStream_t s);
 
 }  // namespace gc

@@ -105,32 +105,39 @@ __global__ void k_aux(int mode, int64_t N, const int64_t* count, const double* _
     }
 }
 
-__global__ void k_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* __restrict__ v,
-                         const double* __restrict__ rho, const double* __restrict__ p,
-                         const double* __restrict__ stress, const int32_t* __restrict__ inst_of,
-                         const double* __restrict__ mass, float* __restrict__ pk) {
-    int64_t n = count ? *count : N;
+__global__ void k_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* __restrict__ x,
+                         const double* __restrict__ v, const double* __restrict__ rho,
+                         const double* __restrict__ p, const double* __restrict__ stress,
+                         const int32_t* __restrict__ inst_of, const double* __restrict__ mass,
+                         double* __restrict__ xpk, float* __restrict__ pk) {
+    const int64_t n = count ? *count : N;
+    const int R = pack_stride(nd, ns), XD = pos_stride(nd);
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        if (xpk)
+            for (int d = 0; d < XD; ++d) xpk[g * XD + d] = d < nd ? x[d * N + g] : 0.0;
+        if (!pk) continue;
+        float* rec = pk + g * R;
         const double r = rho[g];
-        for (int d = 0; d < nd; ++d) pk[d * N + g] = (float)v[d * N + g];
-        pk[nd * N + g] = (float)r;
+        for (int d = 0; d < nd; ++d) rec[d] = (float)v[d * N + g];
+        rec[nd] = (float)r;
         double aux;
         if (mode == AUX_P_OVER_RHO2) aux = p ? p[g] / (r * r) : 0.0;  // boundaries may have no pressure
         else if (mode == AUX_INV_RHO2) aux = 1.0 / (r * r);
         else aux = mass[inst_of[g]] / r;
-        pk[(nd + 1) * N + g] = (float)aux;
-        pk[(nd + 2) * N + g] = (float)(1.0 / r);
-        for (int q = 0; q < ns; ++q) pk[(nd + 3 + q) * N + g] = (float)stress[q * N + g];
+        rec[nd + 1] = (float)aux;
+        rec[nd + 2] = (float)(1.0 / r);
+        for (int q = 0; q < ns; ++q) rec[nd + 3 + q] = stress ? (float)stress[q * N + g] : 0.0f;
+        for (int q = nd + 3 + ns; q < R; ++q) rec[q] = 0.0f;
     }
 }
 
-void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* v, const double* rho,
-                   const double* p, const double* stress, const int32_t* inst_of, const double* mass, float* pk,
-                   cudaStream_t s) {
-    if (N <= 0) return;
+void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* x, const double* v,
+                   const double* rho, const double* p, const double* stress, const int32_t* inst_of,
+                   const double* mass, double* xpk, float* pk, cudaStream_t s) {
+    if (N <= 0 || (!xpk && !pk)) return;
     int64_t blocks = (N + 255) / 256;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    k_pack32<<<(int)blocks, 256, 0, s>>>(mode, N, count, nd, ns, v, rho, p, stress, inst_of, mass, pk);
+    k_pack32<<<(int)blocks, 256, 0, s>>>(mode, N, count, nd, ns, x, v, rho, p, stress, inst_of, mass, xpk, pk);
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

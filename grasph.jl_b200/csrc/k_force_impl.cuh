@@ -19,6 +19,7 @@
 // __dmul_rn/__dadd_rn for the exact acceptance test.
 #pragma once
 #include <cstdio>
+#include <cuda_pipeline.h>
 
 #include "gc_device.cuh"
 #include "gc_force.h"
@@ -276,6 +277,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
 
 template <int ND, int NS, int PFN, int KK>
 struct PhysF64 {
+    static constexpr int NQ = 0;  // no prefetch ring
     struct Own {
         OwnState<ND> o;
         double sig[NS > 0 ? NS : 1];
@@ -380,12 +382,40 @@ __device__ __forceinline__ float kernel_dw_dq_f(float norm, float q) {
 
 template <int ND, int NS, int PFN, int KK>
 struct PhysF32 {
+    // record layout of the FP32 pack (pack_stride floats per particle)
+    static constexpr int NSP = PFN == GC_PFN_CAUCHY_FLUID ? NS : 0;
+    static constexpr int R = pack_stride(ND, NSP);
+    static constexpr int XD = pos_stride(ND);
     struct Own {
         double x[ND];
         float v[ND];
         float rho, aux, irho;
         float sig[NS > 0 ? NS : 1];
     };
+    // one record by 16-byte loads
+    static __device__ __forceinline__ void rec_load(const float* __restrict__ pk, int64_t j, float* f) {
+        const float4* p = reinterpret_cast<const float4*>(pk + j * R);
+#pragma unroll
+        for (int q = 0; q < R / 4; ++q) {
+            const float4 t = p[q];
+            f[4 * q] = t.x;
+            f[4 * q + 1] = t.y;
+            f[4 * q + 2] = t.z;
+            f[4 * q + 3] = t.w;
+        }
+    }
+    static __device__ __forceinline__ void pos_load(const InterRef& r, int64_t j, double* x) {
+        if (r.bxp) {
+            const double2* p = reinterpret_cast<const double2*>(r.bxp + j * XD);
+            const double2 a = p[0];
+            x[0] = a.x;
+            x[1] = a.y;
+            if (ND == 3) x[ND - 1] = p[1].x;
+        } else {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) x[d] = r.bx[d * r.bN + j];
+        }
+    }
     struct AccT {
         float dv[ND], cdv[ND];
         float dr, cdr;
@@ -394,16 +424,18 @@ struct PhysF32 {
     };
     static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
         const int64_t N = A.aN;
+        float f[R];
+        rec_load(A.afp, gi, f);
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
             w.x[d] = A.ax[d * N + gi];
-            w.v[d] = A.afp[d * N + gi];
+            w.v[d] = f[d];
         }
-        w.rho = A.afp[ND * N + gi];
-        w.aux = A.afp[(ND + 1) * N + gi];
-        w.irho = A.afp[(ND + 2) * N + gi];
+        w.rho = f[ND];
+        w.aux = f[ND + 1];
+        w.irho = f[ND + 2];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) w.sig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? A.afp[(ND + 3 + q) * N + gi] : 0.f;
+        for (int q = 0; q < NS; ++q) w.sig[q] = (PFN == GC_PFN_CAUCHY_FLUID) ? f[ND + 3 + q] : 0.f;
     }
     static __device__ __forceinline__ const double* xpos(const Own& w) { return w.x; }
     static __device__ __forceinline__ void init(const ForceArgs&, int64_t, AccT& acc, bool) {
@@ -443,10 +475,67 @@ struct PhysF32 {
     static __device__ __forceinline__ int pair(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                const PfnInst& P, int64_t gi, int k, const Own& w, double da,
                                                int32_t j, AccT& acc) {
-        const int64_t Nb = r.bN;
+        double xj[ND];
+        pos_load(r, j, xj);
+        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcGlobal{r.bfp, j}, acc);
+    }
+
+    // Where a neighbour's record comes from; read only after the pair passed
+    // the cutoff test, so it is not held in registers across the test.
+    struct SrcGlobal {
+        const float* pk;
+        int64_t j;
+        __device__ __forceinline__ void get(float* f) const { rec_load(pk, j, f); }
+    };
+    struct SrcSlot {
+        const float4* slot;
+        int BT;
+        __device__ __forceinline__ void get(float* f) const {
+#pragma unroll
+            for (int q = 0; q < R / 4; ++q) {
+                const float4 t = slot[(XD / 2 + q) * BT];
+                f[4 * q] = t.x;
+                f[4 * q + 1] = t.y;
+                f[4 * q + 2] = t.z;
+                f[4 * q + 3] = t.w;
+            }
+        }
+    };
+
+    // Prefetch of a neighbour's position and record into shared memory
+    // (16-byte asynchronous copies), chunk q of a thread at slot[q*BT].
+    static constexpr int NQP = XD / 2, NQR = R / 4, NQ = NQP + NQR;
+    static __device__ __forceinline__ void issue(const InterRef& r, int32_t j, float4* slot, int BT) {
+        const float4* px = reinterpret_cast<const float4*>(r.bxp + (int64_t)j * XD);
+#pragma unroll
+        for (int q = 0; q < NQP; ++q) __pipeline_memcpy_async(&slot[q * BT], &px[q], 16);
+        if (r.btype != BT_DYNAMIC) {
+            const float4* pr = reinterpret_cast<const float4*>(r.bfp + (int64_t)j * R);
+#pragma unroll
+            for (int q = 0; q < NQR; ++q) __pipeline_memcpy_async(&slot[(NQP + q) * BT], &pr[q], 16);
+        }
+    }
+    template <int P2>
+    static __device__ __forceinline__ int pair_slot(const ForceArgs& A, const InterRef& r, const GridInst& G,
+                                                    const PfnInst& P, int64_t gi, int k, const Own& w, double da,
+                                                    const float4* slot, int BT, AccT& acc) {
+        double xj[ND];
+#pragma unroll
+        for (int q = 0; q < NQP; ++q) {
+            const double2 t = *reinterpret_cast<const double2*>(&slot[q * BT]);
+            if (2 * q < ND) xj[2 * q] = t.x;
+            if (2 * q + 1 < ND) xj[2 * q + 1] = t.y;
+        }
+        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcSlot{slot, BT}, acc);
+    }
+
+    template <int P2, class Src>
+    static __device__ __forceinline__ int pair_data(const ForceArgs& A, const InterRef& r, const GridInst& G,
+                                                    const PfnInst& P, int64_t gi, int k, const Own& w, double da,
+                                                    const double* xj, const Src& src, AccT& acc) {
         double dx[ND];
 #pragma unroll
-        for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], r.bx[d * Nb + j]);
+        for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], xj[d]);
         const double rr = dot_exact<ND>(dx, dx);
         if (!(rr < G.cutoff_sq)) return 0;
         if (P2 == GC_PFN_COUNT) {
@@ -468,6 +557,7 @@ struct PhysF32 {
         const float ca = A.a_cf[k], ma = A.a_massf[k];
 
         float vj[ND], rhoj, auxj, irhoj;
+        float fj[R];
         if (r.btype == BT_DYNAMIC) {
             // src/PairwiseFunctors.jl:53,111,222,334: mirrored velocity, own density
             float db = (float)da;
@@ -480,11 +570,12 @@ struct PhysF32 {
             auxj = w.aux;
             irhoj = w.irho;
         } else {
+            src.get(fj);
 #pragma unroll
-            for (int d = 0; d < ND; ++d) vj[d] = r.bfp[d * Nb + j];
-            rhoj = r.bfp[ND * Nb + j];
-            auxj = r.bfp[(ND + 1) * Nb + j];
-            irhoj = r.bfp[(ND + 2) * Nb + j];
+            for (int d = 0; d < ND; ++d) vj[d] = fj[d];
+            rhoj = fj[ND];
+            auxj = fj[ND + 1];
+            irhoj = fj[ND + 2];
         }
         if (P2 == GC_PFN_STRAIN_RATE || P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
             float dv[ND];
@@ -552,7 +643,7 @@ struct PhysF32 {
             // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
             float sj[NS > 0 ? NS : 1];
 #pragma unroll
-            for (int q2 = 0; q2 < NS; ++q2) sj[q2] = dyn ? w.sig[q2] : r.bfp[(ND + 3 + q2) * Nb + j];
+            for (int q2 = 0; q2 < NS; ++q2) sj[q2] = dyn ? w.sig[q2] : fj[ND + 3 + q2];
             const float ci = w.aux, cj = auxj;
             float hv[ND];
             if (ND == 2) {
@@ -597,10 +688,29 @@ struct PhysF32 {
 template <class Phys, bool COUNT_ONLY, int UNROLL, int PFN>
 __device__ __forceinline__ int flush_all(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                          const PfnInst& P, int64_t gi, int k, const typename Phys::Own& w,
-                                         double da, int nbuf, const int32_t* col, int BT, typename Phys::AccT& acc) {
+                                         double da, int nbuf, const int32_t* col, int BT, typename Phys::AccT& acc,
+                                         float4* ring) {
     constexpr int P2 = COUNT_ONLY ? GC_PFN_COUNT : PFN;
     int acc_n = 0;
     int t = 0;
+    if constexpr (Phys::NQ > 0 && !COUNT_ONLY) {
+        if (ring) {
+            // software pipeline: the next neighbour's position and record are
+            // copied into this thread's shared-memory ring while the current
+            // pair is evaluated
+            constexpr int NQ = Phys::NQ;
+            if (nbuf > 0) Phys::issue(r, col[0], ring, BT);
+            __pipeline_commit();
+            for (; t < nbuf; ++t) {
+                if (t + 1 < nbuf) Phys::issue(r, col[(t + 1) * BT], ring + ((t + 1) & 1) * NQ * BT, BT);
+                __pipeline_commit();
+                __pipeline_wait_prior(1);
+                acc_n += Phys::template pair_slot<P2>(A, r, G, P, gi, k, w, da, ring + (t & 1) * NQ * BT, BT, acc);
+            }
+            __pipeline_wait_prior(0);
+            return acc_n;
+        }
+    }
     if (UNROLL == 2) {
         for (; t + 1 < nbuf; t += 2) {
             const int32_t j0 = col[t * BT], j1 = col[(t + 1) * BT];
@@ -612,7 +722,7 @@ __device__ __forceinline__ int flush_all(const ForceArgs& A, const InterRef& r, 
     return acc_n;
 }
 
-template <class Phys, int ND, int PFN, bool COUNT_ONLY, int MINB, int BUF, int UNROLL>
+template <class Phys, int ND, int PFN, bool COUNT_ONLY, int MINB, int BUF, int UNROLL, bool PRE = false>
 __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     extern __shared__ int32_t sbuf[];
     const unsigned FULL = 0xffffffffu;
@@ -622,6 +732,9 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     int32_t* col = sbuf + tid;
     // per-warp candidate coordinates, ND rows of 32 floats, after the columns
     float* cand = reinterpret_cast<float*>(sbuf + BUF * FORCE_TPB) + (tid >> 5) * (ND * 32);
+    // per-thread prefetch ring (two slots of Phys::NQ 16-byte chunks), after the candidates
+    float4* ring = PRE ? reinterpret_cast<float4*>(sbuf + BUF * FORCE_TPB + (FORCE_TPB / 32) * ND * 32) + tid
+                       : nullptr;
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
@@ -709,7 +822,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                     for (int32_t ch = u0; ch < u1; ch += 32) {
                         if (__any_sync(FULL, nbuf > BUF - 32)) {
                             accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
-                                                                                 BT, acc);
+                                                                                 BT, acc, ring);
                             nbuf = 0;
                             __syncwarp();
                         }
@@ -761,7 +874,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         __syncwarp();
                     }
                 }
-                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc, ring);
                 nbuf = 0;
                 __syncwarp();
             } else if (active && ok) {
@@ -777,12 +890,12 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         col[(nbuf++) * BT] = j;
                         if (nbuf == BUF) {
                             accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
-                                                                                 BT, acc);
+                                                                                 BT, acc, ring);
                             nbuf = 0;
                         }
                     }
                 }
-                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc, ring);
                 nbuf = 0;
             }
             __syncwarp();
@@ -801,8 +914,10 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     int64_t blocks = (warps * 32 + FORCE_TPB - 1) / FORCE_TPB;
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
-    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
-    auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll>;
+    constexpr bool PRE = cf.pre && Phys::NQ > 0;
+    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float) +
+                        (PRE ? (size_t)2 * Phys::NQ * FORCE_TPB * 16 : 0);
+    auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll, PRE>;
     if (smem > 48 * 1024) {
         // beyond the default dynamic shared-memory limit: opt in once per kernel
         static bool opted = false;

@@ -40,6 +40,11 @@ class GcError(RuntimeError):
         super().__init__(f"{C.STATUS_NAMES.get(status, status)}: {msg}")
 
 
+class FieldIO(ct.Structure):
+    _fields_ = [("inst", ct.c_int), ("handle", ct.c_int), ("field", ct.c_int), ("pad", ct.c_int32),
+                ("host", ct.c_void_p), ("bytes", ct.c_size_t)]
+
+
 class GcStats(ct.Structure):
     _fields_ = [("steps_done", ct.c_int64), ("pairs_last_step", ct.c_int64),
                 ("grid_inconsistent", ct.c_int64), ("kernel_launches", ct.c_int64),
@@ -96,6 +101,8 @@ def load_library(path: os.PathLike | None = None):
         "gc_measure_fp64_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
         "gc_set_graphs": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double]),
         "gc_set_sweep_config": (ct.c_int, [ct.c_void_p, ct.c_int]),
+        "gc_upload_fields": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
+        "gc_download_fields": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
         "gc_stage_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         "gc_serve_create": (ct.c_int, [ct.c_int, ct.c_size_t, ct.c_int, ct.c_int, ct.POINTER(ct.c_void_p)]),
         "gc_serve_destroy": (ct.c_int, [ct.c_void_p]),
@@ -213,6 +220,22 @@ class CudaBackend:
         a = np.ascontiguousarray(array)
         self._chk(self.lib.gc_upload_field(self.ctx, inst, handle, field, a.ctypes.data, a.nbytes),
                   "gc_upload_field")
+
+    def upload_many(self, items):
+        """items: (inst, handle, field, array) tuples; one device synchronisation."""
+        keep = [np.ascontiguousarray(a) for *_, a in items]
+        arr = (FieldIO * max(len(items), 1))()
+        for q, ((inst, h, f, _), a) in enumerate(zip(items, keep)):
+            arr[q] = FieldIO(inst, h, f, 0, a.ctypes.data, a.nbytes)
+        self._chk(self.lib.gc_upload_fields(self.ctx, len(items), arr), "gc_upload_fields")
+
+    def download_many(self, items):
+        """items: (inst, handle, field, out_array) tuples, filled in place."""
+        arr = (FieldIO * max(len(items), 1))()
+        for q, (inst, h, f, a) in enumerate(items):
+            assert a.flags["C_CONTIGUOUS"]
+            arr[q] = FieldIO(inst, h, f, 0, a.ctypes.data, a.nbytes)
+        self._chk(self.lib.gc_download_fields(self.ctx, len(items), arr), "gc_download_fields")
 
     def download_into(self, inst, handle, field, out):
         self._chk(self.lib.gc_download_field(self.ctx, inst, handle, field, out.ctypes.data, out.nbytes),
@@ -360,18 +383,26 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0)
     return m
 
 
-def upload_instance(backend, m: InstanceMap):
-    for ps in m.systems:
-        h = m.h(ps)
-        for name, fid in ps.particle_fields():
-            backend.upload(m.inst, h, fid, getattr(ps, name))
+def upload_instance(backend, m: InstanceMap, systems=None):
+    items = [(m.inst, m.h(ps), fid, getattr(ps, name))
+             for ps in m.systems if systems is None or any(ps is q for q in systems)
+             for name, fid in ps.particle_fields()]
+    if hasattr(backend, "upload_many"):
+        backend.upload_many(items)
+    else:
+        for inst, h, fid, a in items:
+            backend.upload(inst, h, fid, a)
 
 
-def download_instance(backend, m: InstanceMap, with_ghosts=True):
-    for ps in m.systems:
-        h = m.h(ps)
-        for name, fid in ps.particle_fields():
-            backend.download_into(m.inst, h, fid, getattr(ps, name))
+def download_instance(backend, m: InstanceMap, with_ghosts=True, systems=None):
+    items = [(m.inst, m.h(ps), fid, getattr(ps, name))
+             for ps in m.systems if systems is None or any(ps is q for q in systems)
+             for name, fid in ps.particle_fields()]
+    if hasattr(backend, "download_many"):
+        backend.download_many(items)
+    else:
+        for inst, h, fid, a in items:
+            backend.download_into(inst, h, fid, a)
     if with_ghosts:
         for ge in m.ghosts:
             download_ghost(backend, m, ge)
@@ -423,13 +454,15 @@ class Session:
         self.precision = precision
 
     # -- state transfer
-    def push(self):
+    def push(self, systems=None):
+        """Upload every field of every system (or of `systems` only)."""
         for m in self.maps:
-            upload_instance(self.backend, m)
+            upload_instance(self.backend, m, systems)
 
-    def pull(self, with_ghosts=True):
+    def pull(self, with_ghosts=True, systems=None):
+        """Download every field of every system (or of `systems` only)."""
         for m in self.maps:
-            download_instance(self.backend, m, with_ghosts)
+            download_instance(self.backend, m, with_ghosts, systems)
 
     def step(self, nsteps, cfl):
         self.backend.step(nsteps, cfl)

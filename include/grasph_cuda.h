@@ -144,7 +144,8 @@ typedef struct gc_stats {
 } gc_stats;
 
 /* Launch configurations of the pair sweep (block residency, staged
- * neighbours per thread, pair-loop unroll); all give bit-identical results. */
+ * neighbours per thread, prefetch of the next neighbour's data); all give
+ * bit-identical results.                                                  */
 #define GC_NUM_SWEEP_CONFIGS 4
 
 /* ============================================================ lifecycle */
@@ -212,6 +213,17 @@ int gc_finalize(gc_ctx* ctx);
  * (x, v, rho, p, stress, idx_original, idx_boundary, normals).              */
 int gc_upload_field(gc_ctx* ctx, int inst, int handle, int field, const void* host, size_t bytes);
 int gc_download_field(gc_ctx* ctx, int inst, int handle, int field, void* host, size_t bytes);
+/* Many fields at once, one synchronisation for all of them (same layouts
+ * and checks as the single-field calls; nothing is written when any entry
+ * is invalid).                                                            */
+typedef struct gc_field_io {
+    int inst, handle, field;
+    int32_t pad;
+    void* host;
+    size_t bytes;
+} gc_field_io;
+int gc_upload_fields(gc_ctx* ctx, int n, const gc_field_io* io);
+int gc_download_fields(gc_ctx* ctx, int n, const gc_field_io* io);
 /* Current particle count of a handle (ghost counts change every step).    */
 int gc_get_count(gc_ctx* ctx, int inst, int handle, int64_t* n_out);
 
