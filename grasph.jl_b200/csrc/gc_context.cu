@@ -245,6 +245,7 @@ struct gc_ctx {
     int64_t* d_need_max = nullptr;
     int64_t* h_need_max = nullptr;  // pinned
     int64_t* d_need_cap = nullptr;  // per plan entry, the cells capacity mode sizes for
+    GridPlanArgs* d_plan_args = nullptr;  // grid plan arguments of every interaction
     std::vector<Snapshot> snaps;    // per slot (moving slots only)
     int64_t graph_steps = 0, rollbacks = 0;
 };
@@ -253,6 +254,8 @@ namespace {
 
 void drop_graphs(gc_ctx* ctx);
 void invalidate_steps(gc_ctx* ctx);
+struct DInter;
+GridPlanArgs grid_plan_args(gc_ctx* ctx, DInter& D);
 
 // ---------------------------------------------------------------- errors
 int seterr(gc_ctx* c, int code, const char* fmt, ...) {
@@ -733,7 +736,8 @@ int finalize(gc_ctx* ctx) {
     ctx->cap_keyN = std::max<int64_t>(maxN, 1);
     TRY(dalloc(ctx, &ctx->key, (size_t)ctx->cap_keyN));
     TRY(dalloc(ctx, &ctx->perm, (size_t)ctx->cap_keyN));
-    TRY(dalloc(ctx, &ctx->bbox_scratch, (size_t)ninst * 2 * MAXD));
+    TRY(dalloc(ctx, &ctx->bbox_scratch, (size_t)ninst * 2 * MAXD + 1));  // + block counter
+    launch_bbox_reset(ctx->bbox_scratch, ninst, ctx->stream);
     TRY(dalloc(ctx, &ctx->d_err, 1));
     TRY(dalloc(ctx, &ctx->d_incons, 1));
     TRY(dalloc(ctx, &ctx->d_total_cells, 1));
@@ -747,6 +751,12 @@ int finalize(gc_ctx* ctx) {
     for (size_t g = 0; g < ctx->ghosts.size(); ++g) ctx->ghosts[g].need_slot = (int64_t)(ctx->slots.size() + g);
     for (size_t i = 0; i < ctx->inters.size(); ++i)
         ctx->inters[i].need_slot = (int64_t)(ctx->slots.size() + ctx->ghosts.size() + i);
+    {
+        std::vector<GridPlanArgs> pa;
+        for (auto& D : ctx->inters) pa.push_back(grid_plan_args(ctx, D));
+        TRY(dalloc(ctx, &ctx->d_plan_args, pa.size()));
+        TRY(hcopy(ctx, ctx->d_plan_args, pa.data(), pa.size() * sizeof(GridPlanArgs), cudaMemcpyHostToDevice));
+    }
     ctx->finalized = true;
     return GC_OK;
 }
@@ -797,7 +807,7 @@ int check_launch(gc_ctx* ctx, const char* where) {
 int ninst(gc_ctx* ctx) { return (int)ctx->inst.size(); }
 
 int bbox_slot(gc_ctx* ctx, DSlot& S) {
-    launch_bbox(S.F(F_X), S.N, S.nd, S.inst_of, nullptr, S.d_inst, ctx->bbox_scratch, ninst(ctx), ctx->d_err,
+    launch_bbox_fused(S.F(F_X), S.N, S.nd, S.inst_of, nullptr, S.d_inst, ctx->bbox_scratch, ninst(ctx), ctx->d_err,
                 ctx->stream);
     return check_launch(ctx, "bbox");
 }
@@ -838,30 +848,46 @@ __global__ void k_ghost_bound(GhostInst* gh, const SysInst* src, SysInst* gi, in
 // device holds at `total`).
 int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells, const int64_t* total) {
     const int ni = ninst(ctx);
+    // The histogram and fill counters are zero on entry and left zero: the
+    // scan clears what the keys counted, the fix-up what the scatter filled.
     TRY(ensure_cells(ctx, cells));
-    CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
-    CU(cudaMemsetAsync(ctx->fill, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
+    GatherArgs ga{};
     if (S) {
         launch_sort_keys(S->F(F_X), S->N, S->nd, S->inst_of, nullptr, S->d_inst, ctx->key, ctx->hist, cells,
                          ctx->d_err, ctx->stream);
-        scan_exclusive(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
+        scan_exclusive_clear(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
         launch_sort_scatter(ctx->key, S->N, nullptr, ctx->start, ctx->fill, ctx->perm, ctx->stream);
-        launch_sort_fixup(ctx->start, cells, total, ctx->perm, ctx->stream);
+        launch_sort_fixup_clear(ctx->start, cells, total, ctx->perm, ctx->fill, ctx->stream);
         for (int f = 0; f < NF; ++f)
-            if (S->ncomp[f]) launch_gather(S->F(f), S->A(f), S->ncomp[f], S->N, ctx->perm, nullptr, ctx->stream);
-        launch_gather_i32(S->id[S->cur], S->id[S->cur ^ 1], S->N, ctx->perm, nullptr, ctx->stream);
+            if (S->ncomp[f]) {
+                ga.src[ga.nf] = S->F(f);
+                ga.dst[ga.nf] = S->A(f);
+                ga.ncomp[ga.nf++] = S->ncomp[f];
+            }
+        ga.isrc[0] = S->id[S->cur];
+        ga.idst[0] = S->id[S->cur ^ 1];
+        ga.ni = 1;
+        launch_gather_fields(ga, S->N, ctx->perm, nullptr, ctx->stream);
         S->cur ^= 1;
     } else {
         launch_sort_keys(G->x[G->cur], G->CAP, G->nd, G->ginst[G->cur], G->d_count, G->d_inst, ctx->key, ctx->hist,
                          cells, ctx->d_err, ctx->stream);
-        scan_exclusive(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
+        scan_exclusive_clear(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
         launch_sort_scatter(ctx->key, G->CAP, G->d_count, ctx->start, ctx->fill, ctx->perm, ctx->stream);
-        launch_sort_fixup(ctx->start, cells, total, ctx->perm, ctx->stream);
+        launch_sort_fixup_clear(ctx->start, cells, total, ctx->perm, ctx->fill, ctx->stream);
         const int c = G->cur, a = c ^ 1;
-        launch_gather(G->x[c], G->x[a], G->nd, G->CAP, ctx->perm, G->d_count, ctx->stream);
-        launch_gather_i32(G->io[c], G->io[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
-        launch_gather_i32(G->ib[c], G->ib[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
-        launch_gather_i32(G->ginst[c], G->ginst[a], G->CAP, ctx->perm, G->d_count, ctx->stream);
+        ga.src[0] = G->x[c];
+        ga.dst[0] = G->x[a];
+        ga.ncomp[0] = G->nd;
+        ga.nf = 1;
+        ga.isrc[0] = G->io[c];
+        ga.idst[0] = G->io[a];
+        ga.isrc[1] = G->ib[c];
+        ga.idst[1] = G->ib[a];
+        ga.isrc[2] = G->ginst[c];
+        ga.idst[2] = G->ginst[a];
+        ga.ni = 3;
+        launch_gather_fields(ga, G->CAP, ctx->perm, G->d_count, ctx->stream);
         G->cur = a;
     }
     (void)ni;
@@ -929,7 +955,7 @@ int generate_ghosts(gc_ctx* ctx, DGhost& G) {
 }
 
 int ghost_bbox_and_plan(gc_ctx* ctx, DGhost& G) {
-    launch_bbox(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
+    launch_bbox_fused(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
                 ctx->d_err, ctx->stream);
     launch_sort_plan(G.d_inst, ninst(ctx), G.nd, ctx->d_need + G.need_slot, ctx->d_err, ctx->stream);
     return check_launch(ctx, "ghost plan");
@@ -954,14 +980,12 @@ int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
         binst = B.inst_of;
         bN = B.N;
     }
-    CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
     launch_grid_count(bx, bN, A.nd, binst, bcount, D.d_gi, ctx->hist, cells, ctx->d_err, ctx->d_incons, ctx->stream);
-    scan_exclusive(ctx->hist, D.cs, cells, ctx->scan_tmp, ctx->stream);
+    scan_exclusive_clear(ctx->hist, D.cs, cells, ctx->scan_tmp, ctx->stream);
     if (D.two_sided) {
-        CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (cells + 1), ctx->stream));
         launch_grid_count(A.F(F_X), A.N, A.nd, A.inst_of, nullptr, D.d_gi, ctx->hist, cells, ctx->d_err,
                           ctx->d_incons, ctx->stream);
-        scan_exclusive(ctx->hist, D.cs_a, cells, ctx->scan_tmp, ctx->stream);
+        scan_exclusive_clear(ctx->hist, D.cs_a, cells, ctx->scan_tmp, ctx->stream);
     }
     D.grid_valid = true;
     D.cells = cells;
@@ -975,10 +999,9 @@ int ensure_csa(gc_ctx* ctx, DInter& D) {
     if (D.btype == BT_SELF || D.csa_ver == D.grid_ver) return GC_OK;
     DSlot& A = ctx->slots[D.a];
     TRY(ensure_cells(ctx, D.cells));
-    CU(cudaMemsetAsync(ctx->hist, 0, sizeof(int32_t) * (D.cells + 1), ctx->stream));
     launch_grid_count(A.F(F_X), A.N, A.nd, A.inst_of, nullptr, D.d_gi, ctx->hist, D.cells, ctx->d_err,
                       ctx->d_incons, ctx->stream);
-    scan_exclusive(ctx->hist, D.cs_a, D.cells, ctx->scan_tmp, ctx->stream);
+    scan_exclusive_clear(ctx->hist, D.cs_a, D.cells, ctx->scan_tmp, ctx->stream);
     D.csa_ver = D.grid_ver;
     return check_launch(ctx, "grid (system_a)");
 }
@@ -1038,8 +1061,10 @@ int64_t cap_grid_cells(gc_ctx* ctx, const DInter& D) { return std::min(D.cap_cel
 int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     const int ni = ninst(ctx);
     CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
-    // bounding boxes of every real system (positions are current)
-    for (auto& S : ctx->slots) TRY(bbox_slot(ctx, S));
+    // bounding boxes of every real system (positions are current); a system
+    // that does not move keeps the box computed after its last upload
+    for (auto& S : ctx->slots)
+        if (S.moving || !S.sorted_once) TRY(bbox_slot(ctx, S));
     for (size_t s = 0; s < ctx->slots.size(); ++s)
         if (sort_mask[s])
             launch_sort_plan(ctx->slots[s].d_inst, ni, ctx->slots[s].nd, ctx->d_need + s, ctx->d_err, ctx->stream);
@@ -1049,7 +1074,7 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
         g_launches.fetch_add(1, std::memory_order_relaxed);
         launch_sort_plan(G.d_inst, ni, G.nd, ctx->d_need + G.need_slot, ctx->d_err, ctx->stream);
     }
-    for (auto& D : ctx->inters) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
+    launch_grid_plan_all(ctx->d_plan_args, (int)ctx->inters.size(), ctx->stream);
     TRY(check_launch(ctx, "plan"));
     std::vector<int64_t> need(ctx->nneed);
     if (ctx->capmode) {
@@ -1933,6 +1958,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
     if (ctx->h_need) cudaFreeHost(ctx->h_need);
     cudaFree(ctx->d_need_max);
     cudaFree(ctx->d_need_cap);
+    cudaFree(ctx->d_plan_args);
     if (ctx->h_need_max) cudaFreeHost(ctx->h_need_max);
     drop_graphs(ctx);
     for (auto& sn : ctx->snaps) {
@@ -2534,7 +2560,7 @@ int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int
     TRY(bbox_slot(ctx, ctx->slots[D.a]));
     if (D.btype == BT_GHOST) {
         DGhost& G = ctx->ghosts[D.bghost];
-        launch_bbox(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
+        launch_bbox_fused(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
                     ctx->d_err, ctx->stream);
     } else if (D.btype != BT_SELF) {
         TRY(bbox_slot(ctx, ctx->slots[D.bslot]));

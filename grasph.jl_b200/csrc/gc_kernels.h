@@ -13,14 +13,21 @@ namespace gc {
 // Exclusive prefix sum of n int32 counts into out[0..n] (out[n] = total).
 // `tmp` must hold scan_tmp_elems(n) int32.
 int64_t scan_tmp_elems(int64_t n);
+// clear_in: the last pass also zeroes in[0..n) (histograms left ready for
+// their next use, no separate memset).
 void scan_exclusive(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s);
+void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s);
 
 // ---------------------------------------------------------- bounding box
 // Per-instance min/max of a slot's positions into inst[k].bbmin/bbmax.
 // `count` (nullable) bounds the packed range for ghost slots.
-void launch_bbox_reset(SysInst* inst, int ninst, cudaStream_t s);
 void launch_bbox(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count, SysInst* inst,
                  unsigned long long* scratch, int ninst, int* err, cudaStream_t s);
+// One launch; `scratch` (ninst·2·MAXD + 1 words) must have been reset once
+// with launch_bbox_reset and is left reset.
+void launch_bbox_reset(unsigned long long* scratch, int ninst, cudaStream_t s);
+void launch_bbox_fused(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
+                       SysInst* inst, unsigned long long* scratch, int ninst, int* err, cudaStream_t s);
 
 // ------------------------------------------------------------------ sort
 // Per-instance key lattice from the bbox; writes total cells to *need.
@@ -36,6 +43,21 @@ void launch_gather(const double* src, double* dst, int ncomp, int64_t N, const i
                    cudaStream_t s);
 void launch_gather_i32(const int32_t* src, int32_t* dst, int64_t N, const int32_t* perm, const int64_t* count,
                        cudaStream_t s);
+// fixup that also zeroes the per-cell fill counters it has consumed
+void launch_sort_fixup_clear(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
+                             int32_t* fill, cudaStream_t s);
+// Every carried field of a slot in one launch.
+constexpr int GATHER_MAX = 16;
+struct GatherArgs {
+    int nf, ni;
+    const double* src[GATHER_MAX];
+    double* dst[GATHER_MAX];
+    int ncomp[GATHER_MAX];
+    const int32_t* isrc[4];
+    int32_t* idst[4];
+};
+void launch_gather_fields(const GatherArgs& a, int64_t N, const int32_t* perm, const int64_t* count,
+                          cudaStream_t s);
 
 // ------------------------------------------------------------------ grid
 struct GridPlanArgs {
@@ -48,6 +70,8 @@ struct GridPlanArgs {
     int* err;
 };
 void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s);
+// The plans of n interactions (device array of arguments), one block each.
+void launch_grid_plan_all(const GridPlanArgs* d_args, int n, cudaStream_t s);
 // cell histogram of the particles of one slot on an interaction's grid.
 void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                        const GridInst* gi, int32_t* hist, int64_t cells_cap, int* err,

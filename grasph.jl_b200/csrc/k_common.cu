@@ -4,6 +4,7 @@
 //   key  = floor(x_d / cutoff)                    src/Sorting.jl:122-124
 //   cell = floor((x_d - mingridx_d) / cell_size)  src/Interaction.jl:197-206
 // Compiled with -fmad=false.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 
@@ -68,7 +69,7 @@ __global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int32_t
 }
 
 __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const int32_t* __restrict__ boff,
-                             int32_t* __restrict__ out) {
+                             int32_t* __restrict__ out, int32_t* clear) {
     int64_t t0 = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
     int32_t v[SCAN_I];
     int32_t s = 0;
@@ -76,6 +77,11 @@ __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const in
     for (int k = 0; k < SCAN_I; ++k) {
         v[k] = t0 + k < n ? in[t0 + k] : 0;
         s += v[k];
+    }
+    if (clear) {
+#pragma unroll
+        for (int k = 0; k < SCAN_I; ++k)
+            if (t0 + k < n) clear[t0 + k] = 0;
     }
     int32_t total;
     int32_t run = block_excl_scan(s, &total) + (boff ? boff[blockIdx.x] : 0);
@@ -93,19 +99,27 @@ int64_t scan_tmp_elems(int64_t n) {
     return nb + (nb + 1) + scan_tmp_elems(nb);
 }
 
-void scan_exclusive(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s) {
+static void scan_impl(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, int32_t* clear, cudaStream_t s) {
     int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nb <= 1) {
-        k_scan_apply<<<1, SCAN_T, 0, s>>>(in, n, nullptr, out);
+        k_scan_apply<<<1, SCAN_T, 0, s>>>(in, n, nullptr, out, clear);
         COUNTED(1);
         return;
     }
     int32_t* bsum = tmp;
     int32_t* boff = tmp + nb;
     k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, bsum);
-    scan_exclusive(bsum, boff, nb, tmp + nb + nb + 1, s);
-    k_scan_apply<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, boff, out);
+    scan_impl(bsum, boff, nb, tmp + nb + nb + 1, nullptr, s);
+    k_scan_apply<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, boff, out, clear);
     COUNTED(2);
+}
+
+void scan_exclusive(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s) {
+    scan_impl(in, out, n, tmp, nullptr, s);
+}
+
+void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s) {
+    scan_impl(in, out, n, tmp, in, s);
 }
 
 // ========================================================== bounding box
@@ -188,7 +202,98 @@ __global__ void k_bbox_finish(const unsigned long long* scratch, SysInst* inst, 
     }
 }
 
-void launch_bbox_reset(SysInst* inst, int ninst, cudaStream_t s) { (void)inst, (void)ninst, (void)s; }
+void launch_bbox_reset(unsigned long long* scratch, int ninst, cudaStream_t s) {
+    k_bbox_reset<<<nblk(ninst), TPB, 0, s>>>(scratch, ninst);
+    COUNTED(1);
+}
+
+// One-launch bounding box: block reductions into the per-instance scratch,
+// then the last block to finish writes the boxes and resets the scratch
+// (and the block counter after it) for the next launch.
+__global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
+                             const int64_t* count, unsigned long long* scratch, SysInst* inst, int ninst, int* err) {
+    // same reduction as k_bbox
+    {
+        int64_t n = count ? *count : N;
+        int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        bool valid = g < n;
+        int k = valid ? inst_of[g] : -1;
+        unsigned long long mn[MAXD], mx[MAXD];
+        bool bad = false;
+        for (int d = 0; d < MAXD; ++d) {
+            mn[d] = ~0ull;
+            mx[d] = 0ull;
+        }
+        if (valid) {
+            for (int d = 0; d < nd; ++d) {
+                double v = x[d * N + g];
+                if (!isfinite(v)) bad = true;
+                mn[d] = mx[d] = ord_key(v);
+            }
+        }
+        if (bad) atomicOr(err, ERR_NONFINITE);
+        __shared__ int k0;
+        if (threadIdx.x == 0) k0 = k;
+        __syncthreads();
+        int uniform = __syncthreads_and(!valid || k == k0);
+        if (uniform && k0 >= 0) {
+            __shared__ unsigned long long smn[TPB / 32][MAXD], smx[TPB / 32][MAXD];
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            for (int d = 0; d < nd; ++d) {
+                unsigned long long a = mn[d], b = mx[d];
+                for (int o = 16; o > 0; o >>= 1) {
+                    unsigned long long a2 = __shfl_down_sync(0xffffffffu, a, o);
+                    unsigned long long b2 = __shfl_down_sync(0xffffffffu, b, o);
+                    a = a2 < a ? a2 : a;
+                    b = b2 > b ? b2 : b;
+                }
+                if (lane == 0) {
+                    smn[wid][d] = a;
+                    smx[wid][d] = b;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < nd) {
+                int d = threadIdx.x;
+                unsigned long long a = ~0ull, b = 0ull;
+                for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+                    a = smn[w][d] < a ? smn[w][d] : a;
+                    b = smx[w][d] > b ? smx[w][d] : b;
+                }
+                atomicMin(&scratch[(k0 * 2 + 0) * MAXD + d], a);
+                atomicMax(&scratch[(k0 * 2 + 1) * MAXD + d], b);
+            }
+        } else if (valid) {
+            for (int d = 0; d < nd; ++d) {
+                atomicMin(&scratch[(k * 2 + 0) * MAXD + d], mn[d]);
+                atomicMax(&scratch[(k * 2 + 1) * MAXD + d], mx[d]);
+            }
+        }
+    }
+    unsigned long long* counter = scratch + (size_t)ninst * 2 * MAXD;
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1ull) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int k = threadIdx.x; k < ninst; k += blockDim.x) {
+        for (int d = 0; d < nd; ++d) {
+            unsigned long long a = atomicExch(&scratch[(k * 2 + 0) * MAXD + d], ~0ull);
+            unsigned long long b = atomicExch(&scratch[(k * 2 + 1) * MAXD + d], 0ull);
+            inst[k].bbmin[d] = a == ~0ull ? 0.0 : ord_val(a);
+            inst[k].bbmax[d] = b == 0ull ? 0.0 : ord_val(b);
+        }
+    }
+    if (threadIdx.x == 0) atomicExch(counter, 0ull);
+}
+
+void launch_bbox_fused(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
+                       SysInst* inst, unsigned long long* scratch, int ninst, int* err, cudaStream_t s) {
+    k_bbox_fused<<<nblk(std::max<int64_t>(N, 1)), TPB, 0, s>>>(x, N, nd, inst_of, count, scratch, inst, ninst, err);
+    COUNTED(1);
+}
 
 void launch_bbox(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count, SysInst* inst,
                  unsigned long long* scratch, int ninst, int* err, cudaStream_t s) {
@@ -312,6 +417,32 @@ __global__ void k_sort_fixup(const int32_t* __restrict__ start, int64_t ncells_c
     }
 }
 
+__global__ void k_sort_fixup_clear(const int32_t* __restrict__ start, int64_t ncells_cap, const int64_t* total_cells,
+                                   int32_t* __restrict__ perm, int32_t* __restrict__ fill) {
+    int64_t nc = *total_cells;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc && c < ncells_cap;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        int32_t s = start[c], e = start[c + 1];
+        fill[c] = 0;
+        for (int32_t i = s + 1; i < e; ++i) {
+            int32_t v = perm[i];
+            int32_t j = i - 1;
+            while (j >= s && perm[j] > v) {
+                perm[j + 1] = perm[j];
+                --j;
+            }
+            perm[j + 1] = v;
+        }
+    }
+}
+
+void launch_sort_fixup_clear(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
+                             int32_t* fill, cudaStream_t s) {
+    if (ncells_cap <= 0) return;
+    k_sort_fixup_clear<<<nblk(ncells_cap), TPB, 0, s>>>(start, ncells_cap, total_cells, perm, fill);
+    COUNTED(1);
+}
+
 void launch_sort_fixup(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
                        cudaStream_t s) {
     if (ncells_cap <= 0) return;
@@ -341,6 +472,39 @@ __global__ void k_gather_i32(const int32_t* __restrict__ src, int32_t* __restric
     }
 }
 
+// blockIdx.y picks the field (the int32 fields after the double ones), so
+// every thread has one independent gather per component.
+__global__ void k_gather_fields(GatherArgs a, int64_t N, const int32_t* __restrict__ perm, const int64_t* count) {
+    const int64_t n = count ? *count : N;
+    const int f = blockIdx.y;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = perm[g];
+        if ((uint64_t)o >= (uint64_t)N) o = g;
+        if (f < a.nf) {
+            const double* __restrict__ src = a.src[f];
+            double* __restrict__ dst = a.dst[f];
+            const int nc = a.ncomp[f];
+            double v[MAXS];
+#pragma unroll
+            for (int c = 0; c < MAXS; ++c)
+                if (c < nc) v[c] = __ldg(src + c * N + o);
+#pragma unroll
+            for (int c = 0; c < MAXS; ++c)
+                if (c < nc) dst[c * N + g] = v[c];
+        } else {
+            a.idst[f - a.nf][g] = __ldg(a.isrc[f - a.nf] + o);
+        }
+    }
+}
+
+void launch_gather_fields(const GatherArgs& a, int64_t N, const int32_t* perm, const int64_t* count,
+                          cudaStream_t s) {
+    if (N <= 0 || (a.nf == 0 && a.ni == 0)) return;
+    dim3 grid((unsigned)nblk(N), (unsigned)(a.nf + a.ni));
+    k_gather_fields<<<grid, TPB, 0, s>>>(a, N, perm, count);
+    COUNTED(1);
+}
+
 void launch_gather(const double* src, double* dst, int ncomp, int64_t N, const int32_t* perm, const int64_t* count,
                    cudaStream_t s) {
     if (N <= 0 || ncomp <= 0) return;
@@ -358,7 +522,17 @@ void launch_gather_i32(const int32_t* src, int32_t* dst, int64_t N, const int32_
 // ================================================================== grid
 // src/Interaction.jl:131-193: origin snapped to a multiple of the cell
 // size below min−2h, ngridx = floor((max+2h − origin)/h2) + 1.
-__global__ void k_grid_plan(GridPlanArgs a) {
+__device__ void grid_plan_block(const GridPlanArgs& a);
+__global__ void k_grid_plan(GridPlanArgs a) { grid_plan_block(a); }
+__global__ void k_grid_plan_all(const GridPlanArgs* __restrict__ args) { grid_plan_block(args[blockIdx.x]); }
+
+void launch_grid_plan_all(const GridPlanArgs* d_args, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_grid_plan_all<<<n, 1024, 0, s>>>(d_args);
+    COUNTED(1);
+}
+
+__device__ void grid_plan_block(const GridPlanArgs& a) {
     for (int k = threadIdx.x; k < a.ninst; k += blockDim.x) {
         GridInst& G = a.gi[k];
         const SysInst& A = a.a[k];
