@@ -97,6 +97,8 @@ struct DSlot {
     float *d_massf = nullptr, *d_cf = nullptr;
     float* fpk = nullptr;      // FP32 pack for the FP32-compensated sweep
     int64_t cap_fpk = 0;
+    int64_t xpk_epoch = -1;    // pack_epoch the FP64 position copy was made in
+    bool xpk_static = false;   // position copy of a system that does not move is current
     bool written = false;      // some functor writes this system
     bool moving = true;        // sorted and integrated every step
     bool sorted_once = false;  // static systems: sorted since the last upload
@@ -132,6 +134,8 @@ struct DGhost {
     double *d_mass = nullptr, *d_c = nullptr;
     float* fpk = nullptr;
     int64_t cap_fpk = 0;
+    int64_t xpk_epoch = -1;
+    bool xpk_static = false;  // never set: ghosts are regenerated every step
     std::vector<std::vector<std::pair<int, int>>> copiers;
     bool ex_p = false, ex_stress = false;
     int64_t need_slot = -1;  // index into need[] for its sort cells
@@ -248,6 +252,7 @@ struct gc_ctx {
     GridPlanArgs* d_plan_args = nullptr;  // grid plan arguments of every interaction
     std::vector<Snapshot> snaps;    // per slot (moving slots only)
     int64_t graph_steps = 0, rollbacks = 0;
+    int64_t pack_epoch = 0;  // bumps at the start of every issued step (never rolled back)
 };
 
 namespace {
@@ -869,6 +874,7 @@ int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells, const i
         ga.ni = 1;
         launch_gather_fields(ga, S->N, ctx->perm, nullptr, ctx->stream);
         S->cur ^= 1;
+        S->xpk_static = false;
     } else {
         launch_sort_keys(G->x[G->cur], G->CAP, G->nd, G->ginst[G->cur], G->d_count, G->d_inst, ctx->key, ctx->hist,
                          cells, ctx->d_err, ctx->stream);
@@ -1183,6 +1189,8 @@ int ensure_fpk(gc_ctx* ctx, T& X, int64_t N, int nd, int ns) {
         dfree(ctx, X.fpk, X.cap_fpk);
         TRY(dalloc(ctx, &X.fpk, (size_t)need));
         X.cap_fpk = need;
+        X.xpk_epoch = -1;  // the new buffer holds no positions yet
+        X.xpk_static = false;
     }
     return GC_OK;
 }
@@ -1209,8 +1217,11 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     if (pfn != GC_PFN_COUNT) {
         if (fp32) {
             TRY(ensure_fpk(ctx, S, S.N, S.nd, pk_ns));
+            // positions do not change between the stages of a step
+            const bool pos = S.xpk_epoch != ctx->pack_epoch;
             launch_pack32(mode, S.N, nullptr, S.nd, pk_ns, S.F(F_X), S.F(F_V), S.F(F_RHO), S.F(F_P), S.F(F_STRESS),
-                          S.inst_of, S.d_mass, xp_of(S.fpk), pk_of(S.fpk, S.N, S.nd), ctx->stream);
+                          S.inst_of, S.d_mass, pos ? xp_of(S.fpk) : nullptr, pk_of(S.fpk, S.N, S.nd), ctx->stream);
+            S.xpk_epoch = ctx->pack_epoch;
         } else {
             launch_aux(mode, S.N, nullptr, S.F(F_RHO), S.F(F_P), S.inst_of, S.d_mass, S.aux, ctx->stream);
         }
@@ -1297,8 +1308,11 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             r.bxp = nullptr;
             if (fp32) {
                 TRY(ensure_fpk(ctx, G, G.CAP, G.nd, pk_ns));
+                const bool pos = G.xpk_epoch != ctx->pack_epoch;
                 launch_pack32(mode, G.CAP, G.d_count, G.nd, pk_ns, G.x[G.cur], G.v, G.rho, G.p, G.stress,
-                              G.ginst[G.cur], G.d_mass, xp_of(G.fpk), pk_of(G.fpk, G.CAP, G.nd), ctx->stream);
+                              G.ginst[G.cur], G.d_mass, pos ? xp_of(G.fpk) : nullptr, pk_of(G.fpk, G.CAP, G.nd),
+                              ctx->stream);
+                G.xpk_epoch = ctx->pack_epoch;
                 r.bfp = pk_of(G.fpk, G.CAP, G.nd);
                 r.bxp = xp_of(G.fpk);
             }
@@ -1329,9 +1343,13 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
                 // dynamic walls lend only their positions; other systems their records too
                 const bool rec = D.btype == BT_SYSTEM || D.btype == BT_STATIC;
                 TRY(ensure_fpk(ctx, B, B.N, B.nd, pk_ns));
+                // positions: once per step, once for good for a system that does not move
+                const bool pos = B.moving ? B.xpk_epoch != ctx->pack_epoch : !B.xpk_static;
                 launch_pack32(mode, B.N, nullptr, B.nd, pk_ns, B.F(F_X), B.F(F_V), B.F(F_RHO), B.F(F_P),
-                              B.kind >= GC_SYS_STRESS ? B.F(F_STRESS) : nullptr, B.inst_of, B.d_mass, xp_of(B.fpk),
-                              rec ? pk_of(B.fpk, B.N, B.nd) : nullptr, ctx->stream);
+                              B.kind >= GC_SYS_STRESS ? B.F(F_STRESS) : nullptr, B.inst_of, B.d_mass,
+                              pos ? xp_of(B.fpk) : nullptr, rec ? pk_of(B.fpk, B.N, B.nd) : nullptr, ctx->stream);
+                B.xpk_epoch = ctx->pack_epoch;
+                if (!B.moving) B.xpk_static = true;
                 r.bxp = xp_of(B.fpk);
                 if (rec) r.bfp = pk_of(B.fpk, B.N, B.nd);
             }
@@ -1485,6 +1503,7 @@ bool decide_motion(gc_ctx* ctx) {
 }
 
 int one_step(gc_ctx* ctx) {
+    ctx->pack_epoch++;
     std::vector<char> mask(ctx->slots.size());
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
@@ -2363,6 +2382,8 @@ int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
             // a system that is not sorted every step is sorted again
             if (!S.moving) structural = true;
             S.sorted_once = false;
+            S.xpk_static = false;
+            S.xpk_epoch = -1;
         }
         if (f.field == GC_FIELD_V || f.field == GC_FIELD_DVDT || f.field == GC_FIELD_DRHODT) {
             int64_t bit = f.field == GC_FIELD_V ? 1 : f.field == GC_FIELD_DVDT ? 2 : 4;

@@ -211,11 +211,14 @@ void launch_bbox_reset(unsigned long long* scratch, int ninst, cudaStream_t s) {
 // then the last block to finish writes the boxes and resets the scratch
 // (and the block counter after it) for the next launch.
 __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
-                             const int64_t* count, unsigned long long* scratch, SysInst* inst, int ninst, int* err) {
-    // same reduction as k_bbox
-    {
-        int64_t n = count ? *count : N;
-        int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                             const int64_t* count, unsigned long long* scratch, SysInst* inst, int ninst, int* err,
+                             int64_t tiles_per_block) {
+    // each block reduces a contiguous run of 256-particle tiles (as k_bbox
+    // does one), so the block counter below sees few atomics
+    const int64_t n = count ? *count : N;
+    for (int64_t tile = (int64_t)blockIdx.x * tiles_per_block;
+         tile < (int64_t)(blockIdx.x + 1) * tiles_per_block && tile * blockDim.x < n; ++tile) {
+        int64_t g = tile * blockDim.x + threadIdx.x;
         bool valid = g < n;
         int k = valid ? inst_of[g] : -1;
         unsigned long long mn[MAXD], mx[MAXD];
@@ -269,6 +272,7 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
                 atomicMax(&scratch[(k * 2 + 1) * MAXD + d], mx[d]);
             }
         }
+        __syncthreads();  // the shared k0 and partials are reused by the next tile
     }
     unsigned long long* counter = scratch + (size_t)ninst * 2 * MAXD;
     __shared__ bool last;
@@ -291,7 +295,10 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
 
 void launch_bbox_fused(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                        SysInst* inst, unsigned long long* scratch, int ninst, int* err, cudaStream_t s) {
-    k_bbox_fused<<<nblk(std::max<int64_t>(N, 1)), TPB, 0, s>>>(x, N, nd, inst_of, count, scratch, inst, ninst, err);
+    const int64_t tiles = std::max<int64_t>((N + TPB - 1) / TPB, 1);
+    const int64_t per = std::max<int64_t>((tiles + 1183) / 1184, 1);  // about 8 blocks per SM
+    const int blocks = (int)((tiles + per - 1) / per);
+    k_bbox_fused<<<blocks, TPB, 0, s>>>(x, N, nd, inst_of, count, scratch, inst, ninst, err, per);
     COUNTED(1);
 }
 

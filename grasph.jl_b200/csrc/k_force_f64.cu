@@ -111,12 +111,16 @@ __global__ void k_pack32(int mode, int64_t N, const int64_t* count, int nd, int 
                          const int32_t* __restrict__ inst_of, const double* __restrict__ mass,
                          double* __restrict__ xpk, float* __restrict__ pk) {
     const int64_t n = count ? *count : N;
-    const int R = pack_stride(nd, ns), XD = pos_stride(nd);
+    const int R = pack_stride(nd, ns);
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
-        if (xpk)
-            for (int d = 0; d < XD; ++d) xpk[g * XD + d] = d < nd ? x[d * N + g] : 0.0;
+        if (xpk) {
+            // 16-byte stores: (x, y) then (z, 0) in 3-D
+            double2* o = reinterpret_cast<double2*>(xpk + g * pos_stride(nd));
+            o[0] = make_double2(x[g], x[N + g]);
+            if (nd == 3) o[1] = make_double2(x[2 * N + g], 0.0);
+        }
         if (!pk) continue;
-        float* rec = pk + g * R;
+        float rec[16];
         const double r = rho[g];
         for (int d = 0; d < nd; ++d) rec[d] = (float)v[d * N + g];
         rec[nd] = (float)r;
@@ -128,6 +132,8 @@ __global__ void k_pack32(int mode, int64_t N, const int64_t* count, int nd, int 
         rec[nd + 2] = (float)(1.0 / r);
         for (int q = 0; q < ns; ++q) rec[nd + 3 + q] = stress ? (float)stress[q * N + g] : 0.0f;
         for (int q = nd + 3 + ns; q < R; ++q) rec[q] = 0.0f;
+        float4* o = reinterpret_cast<float4*>(pk + g * R);
+        for (int q = 0; q < R / 4; ++q) o[q] = make_float4(rec[4 * q], rec[4 * q + 1], rec[4 * q + 2], rec[4 * q + 3]);
     }
 }
 
