@@ -188,6 +188,21 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(value, dist, device="cuda"):
+    """The slowest rank's time (every rank takes part; no-op for one rank)."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, steps, seconds, world):
+    """Whole-job throughput: units every rank processed ÷ the slowest rank's time."""
+    return units_per_rank * steps * world / seconds
+
+
 def _timed_steps(sess, meta, args, lib, be, stream, dist, sample_clocks, local_rank):
     """Warm-up, then exactly args.steps timed steps between barriers."""
     import torch
@@ -212,10 +227,7 @@ def _timed_steps(sess, meta, args, lib, be, stream, dist, sample_clocks, local_r
     ms = e0.elapsed_time(e1)
     st1 = be.stats()
     lib.gc_set_profiling(be.ctx, 0)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     return ms, st0, st1, clk
 
 
@@ -275,8 +287,8 @@ def run_ours(args, rank, world, local_rank):
     sweep_launches = max(1, st1["sweep_launches"] - st0["sweep_launches"])
     pairs = st1["pairs_last_step"]
     n_fluid = meta["n_fluid"]
-    value = n_fluid * args.steps / (ms / 1e3) * world
-    pair_rate = pairs * args.steps / (ms / 1e3) * world
+    value = job_rate(n_fluid, args.steps, ms / 1e3, world)
+    pair_rate = job_rate(pairs, args.steps, ms / 1e3, world)
 
     # the plain FP64 path on the same workload and step count, and the
     # FP32-compensated run's error against it
@@ -287,7 +299,7 @@ def run_ours(args, rank, world, local_rank):
         ms64, _, _, _ = _timed_steps(s64, meta, args, lib64, be64, stream64, dist, False, local_rank)
         sess.pull()
         s64.pull()
-        fp64 = {"value": n_fluid * args.steps / (ms64 / 1e3) * world, "ms_per_step": ms64 / args.steps,
+        fp64 = {"value": job_rate(n_fluid, args.steps, ms64 / 1e3, world), "ms_per_step": ms64 / args.steps,
                 "speedup": ms64 / ms,
                 "rel_error_after_steps": args.warmup + args.steps,
                 "rel_error": _rel_errors(lf, lf64)}
@@ -315,12 +327,8 @@ def run_ours(args, rank, world, local_rank):
             sess.step(1, meta["cfl"])
             sess.pull(with_ghosts=False, systems=moving)
         torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": n_fluid * e2e_steps / el * world, "unit": "particle-steps/s",
+        el = max_over_ranks(time.perf_counter() - t0, dist)
+        e2e = {"value": job_rate(n_fluid, e2e_steps, el, world), "unit": "particle-steps/s",
                "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
                "ms_per_step": el / e2e_steps * 1e3, "steps": e2e_steps,
                "copied": "every field of the simulated systems, both ways, each step (pinned host memory)"}
@@ -399,7 +407,7 @@ def run_batched(args, rank, world, local_rank):
     lib.gc_set_profiling.argtypes = [engine.ct.c_void_p, engine.ct.c_int]
     stream = torch.cuda.ExternalStream(sptr.value)
     ms, st0, st1, clk = _timed_steps(sess, meta, args, lib, be, stream, dist, True, local_rank)
-    value = n_tot * args.steps / (ms / 1e3) * world
+    value = job_rate(n_tot, args.steps, ms / 1e3, world)
     launches = st1["kernel_launches"] - st0["kernel_launches"]
     sweep_ms = st1["sweep_ms"] - st0["sweep_ms"]
     sweep_launches = max(1, st1["sweep_launches"] - st0["sweep_launches"])
