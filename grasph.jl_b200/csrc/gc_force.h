@@ -18,7 +18,7 @@ struct ForceCfg {
     int minb, buf, unroll, pre;  // pre: prefetch ring for the FP32-compensated pairs
 };
 constexpr int NUM_FORCE_CFG = GC_NUM_SWEEP_CONFIGS;
-constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1, 0}, {4, 64, 1, 1}, {3, 64, 1, 1}, {4, 96, 1, 1}};
+constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1, 0}, {4, 64, 1, 1}, {6, 64, 1, 0}, {5, 64, 1, 0}};
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)

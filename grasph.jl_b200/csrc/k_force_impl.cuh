@@ -731,9 +731,10 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     const int BT = blockDim.x;
     int32_t* col = sbuf + tid;
     // per-warp candidate coordinates, ND rows of 32 floats, after the columns
-    float* cand = reinterpret_cast<float*>(sbuf + BUF * FORCE_TPB) + (tid >> 5) * (ND * 32);
+    // per warp: ND rows of 32 candidate coordinates, then ND doubles (lane 0's position)
+    float* cand = reinterpret_cast<float*>(sbuf + BUF * FORCE_TPB) + (tid >> 5) * (ND * 34);
     // per-thread prefetch ring (two slots of Phys::NQ 16-byte chunks), after the candidates
-    float4* ring = PRE ? reinterpret_cast<float4*>(sbuf + BUF * FORCE_TPB + (FORCE_TPB / 32) * ND * 32) + tid
+    float4* ring = PRE ? reinterpret_cast<float4*>(sbuf + BUF * FORCE_TPB + (FORCE_TPB / 32) * ND * 34) + tid
                        : nullptr;
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -800,14 +801,17 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                 // |rel| spans a few cells, so single-precision rounding moves r²
                 // by < 1e-5 relative; the 1e-3 margin keeps every true pair.
                 // Inactive lanes test against NaN and so accept nothing.
-                double xref[ND];
-                float2 xi2[ND];
+                // lane 0's position, the origin of the relative coordinates,
+                // kept in the warp's shared memory rather than in registers
+                double* xref = reinterpret_cast<double*>(cand + ND * 32);
+                float xi[ND];
+                if (lane == 0) {
 #pragma unroll
-                for (int d = 0; d < ND; ++d) {
-                    xref[d] = __shfl_sync(FULL, ox[d], 0);
-                    const float xi = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
-                    xi2[d] = make_float2(xi, xi);
+                    for (int d = 0; d < ND; ++d) xref[d] = ox[d];
                 }
+                __syncwarp();
+#pragma unroll
+                for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
                 const float2 neg1 = make_float2(-1.0f, -1.0f);
                 const int64_t ngl = G.ng[L];
@@ -851,13 +855,13 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                                 float2 rr;
                                 {
                                     const float2 xj = *reinterpret_cast<const float2*>(cand + t0 + t);
-                                    const float2 dd = __ffma2_rn(xj, neg1, xi2[0]);
+                                    const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[0], xi[0]));
                                     rr = __fmul2_rn(dd, dd);
                                 }
 #pragma unroll
                                 for (int d = 1; d < ND; ++d) {
                                     const float2 xj = *reinterpret_cast<const float2*>(cand + d * 32 + t0 + t);
-                                    const float2 dd = __ffma2_rn(xj, neg1, xi2[d]);
+                                    const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[d], xi[d]));
                                     rr = __ffma2_rn(dd, dd, rr);
                                 }
                                 if (rr.x < cut_f) h8 |= 1u << t;
@@ -915,7 +919,7 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
     constexpr bool PRE = cf.pre && Phys::NQ > 0;
-    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float) +
+    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float) +
                         (PRE ? (size_t)2 * Phys::NQ * FORCE_TPB * 16 : 0);
     auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll, PRE>;
     if (smem > 48 * 1024) {
@@ -951,7 +955,7 @@ static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
             int64_t blocks = (A.aN * 32 + FORCE_TPB - 1) / FORCE_TPB;
             if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
             if (blocks < 1) blocks = 1;
-            size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 32 * sizeof(float);
+            size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float);
             k_sweep<P64, ND, PFN, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
         } else {
             launch_cfg<P64, ND, PFN>(A, s);
