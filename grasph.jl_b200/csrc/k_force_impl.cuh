@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
         const int2 grp = A.groups[wg];
         const bool active = lane < grp.y;
-        const int64_t gi = (int64_t)grp.x + (active ? lane : 0);
+        const int32_t gi = grp.x + (active ? lane : 0);  // packed indices fit int32
         const int k = A.a_inst_of[gi];
         typename Phys::Own w;
         Phys::load(A, gi, w);
@@ -772,28 +772,34 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                 if (active && r.counts) r.counts[gi] = 0;
                 continue;
             }
-            int64_t c[ND];
+            // cell coordinates (a grid has < 2^31 cells, so they fit int32)
+            int32_t c[ND];
             bool ok = true;
 #pragma unroll
-            for (int d = 0; d < ND; ++d)
-                if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &c[d]) || c[d] < 1 || c[d] >= G.ng[d] - 1)
+            for (int d = 0; d < ND; ++d) {
+                int64_t cd;
+                if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &cd) || cd < 1 || cd >= G.ng[d] - 1) {
                     ok = false;
+                    cd = 1;
+                }
+                c[d] = (int32_t)cd;
+            }
             if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
             const double da = r.btype == BT_DYNAMIC ? Phys::plane_da(w, G) : 0.0;
             const int64_t Nb = r.bN;
             const bool self = r.btype == BT_SELF;
             int nbuf = 0;
             int32_t accepted = 0;
-            const int64_t c0 = __shfl_sync(FULL, c[0], 0);
-            const int64_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
+            const int32_t c0 = __shfl_sync(FULL, c[0], 0);
+            const int32_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
             const bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
             const bool coop = __all_sync(FULL, !active || same);
             if (coop) {
                 constexpr int L = ND - 1;  // last dimension
-                int64_t zlo = active ? c[L] : INT64_MAX, zhi = active ? c[L] : INT64_MIN;
+                int32_t zlo = active ? c[L] : INT32_MAX, zhi = active ? c[L] : INT32_MIN;
 #pragma unroll
                 for (int o2 = 16; o2 > 0; o2 >>= 1) {
-                    int64_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
+                    int32_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
                     zlo = a2 < zlo ? a2 : zlo;
                     zhi = b2 > zhi ? b2 : zhi;
                 }
@@ -843,7 +849,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         unsigned allow = tlo <= 0 ? 0xffffffffu : (tlo >= 32 ? 0u : 0xffffffffu << tlo);
                         allow &= thi >= 32 ? 0xffffffffu : (thi <= 0 ? 0u : 0xffffffffu >> (32 - thi));
                         if (self) {
-                            const int64_t ts = gi - ch;
+                            const int32_t ts = gi - ch;
                             if (ts >= 0 && ts < 32) allow &= ~(1u << ts);
                         }
                         const int m = u1 - ch < 32 ? (int)(u1 - ch) : 32;
