@@ -313,7 +313,8 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_e2e:
         pin_arrays(lf)
         moving = [ps for ps in lf.systems if any(it.system_a is ps for it in lf.interactions)]
-        nb = sum(getattr(ps, n).nbytes for ps in moving for n, _ in ps.particle_fields())
+        # bytes that cross PCIe each way (v_adjustment is all zero: neither sent nor read back)
+        nb = sum(getattr(ps, n).nbytes for ps in moving for n, _ in ps.particle_fields() if n != "v_adjustment")
         e2e_steps = max(3, min(args.steps, 20))
         sess.push()
         sess.step(1, meta["cfl"])
