@@ -46,7 +46,7 @@ FLUID_PAIR_FLOPS = {2: 70, 3: 86}
 WARMUP_MIN = 10  # untimed steps: 1 cold step, 4 autotuner steps, then graph capture
 # DRAM bytes (read + write) of one sweep launch from an ncu capture, keyed by
 # (workload, scale, precision); the profiles/ summaries give the commands.
-TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 121.48e6}
+TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 178.57e6}
 
 
 def build_workload(name, scale):
