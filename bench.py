@@ -316,7 +316,9 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_e2e:
         pin_arrays(lf)
         moving = [ps for ps in lf.systems if any(it.system_a is ps for it in lf.interactions)]
-        # bytes that cross PCIe each way (v_adjustment is all zero: neither sent nor read back)
+        # bytes that cross PCIe: every field goes up (v_adjustment only to be
+        # checked for zero on the device); it is not read back (always zero)
+        nb_h2d = sum(getattr(ps, n).nbytes for ps in moving for n, _ in ps.particle_fields())
         nb = sum(getattr(ps, n).nbytes for ps in moving for n, _ in ps.particle_fields() if n != "v_adjustment")
         e2e_steps = max(3, min(args.steps, 20))
         sess.push()
@@ -326,15 +328,24 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
+        split = [0.0, 0.0, 0.0]  # host wall time in push, step, pull (each call returns when done)
         for _ in range(e2e_steps):
+            ta = time.perf_counter()
             sess.push(systems=moving)
+            tb = time.perf_counter()
             sess.step(1, meta["cfl"])
+            tc = time.perf_counter()
             sess.pull(with_ghosts=False, systems=moving)
+            td = time.perf_counter()
+            split[0] += tb - ta
+            split[1] += tc - tb
+            split[2] += td - tc
         torch.cuda.synchronize()
         el = max_over_ranks(time.perf_counter() - t0, dist)
         e2e = {"value": job_rate(n_fluid, e2e_steps, el, world), "unit": "particle-steps/s",
-               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
+               "h2d_bytes_per_step": nb_h2d, "d2h_bytes_per_step": nb,
                "ms_per_step": el / e2e_steps * 1e3, "steps": e2e_steps,
+               "ms_push_step_pull": [x / e2e_steps * 1e3 for x in split],
                "copied": "every field of the simulated systems, both ways, each step (pinned host memory)"}
 
     # roofline of the dominant kernel (the fused pair sweep)

@@ -253,6 +253,8 @@ struct gc_ctx {
     std::vector<Snapshot> snaps;    // per slot (moving slots only)
     int64_t graph_steps = 0, rollbacks = 0;
     int64_t pack_epoch = 0;  // bumps at the start of every issued step (never rolled back)
+    double params_cfl = NAN;  // CFL number the per-instance parameters were pushed for
+    bool params_dirty = true;
 };
 
 namespace {
@@ -1817,14 +1819,18 @@ int run_steps(gc_ctx* ctx, int nsteps) {
             continue;
         }
         TRY(size_capacities(ctx));
+        const int W = std::min(ctx->sync_every, nsteps - done);
+        // A one-step window needs no snapshot: the step's sort gathers every
+        // moving system into its other buffers and leaves the current ones
+        // untouched, so going back is a flip of the buffer parities.
         std::vector<char> par0;
-        TRY(snapshot(ctx, par0));
+        if (W == 1) par0 = parity(ctx);
+        else TRY(snapshot(ctx, par0));
         if (ctx->alloc_epoch != ctx->graphs_epoch || graph_key(ctx) != ctx->graphs_key) {
             drop_graphs(ctx);
             ctx->graphs_epoch = ctx->alloc_epoch;
             ctx->graphs_key = graph_key(ctx);
         }
-        const int W = std::min(ctx->sync_every, nsteps - done);
         int ran = 0;
         int cap_err = GC_OK;
         ctx->capmode = true;
@@ -1849,7 +1855,8 @@ int run_steps(gc_ctx* ctx, int nsteps) {
         if (e & ERR_CAPACITY) {
             // a plan outgrew a capacity: back to the snapshot, then the same
             // steps exactly (which size every buffer from the plan)
-            TRY(restore(ctx, par0));
+            if (W == 1) set_parity(ctx, par0);
+            else TRY(restore(ctx, par0));
             ctx->steps_done -= ran;
             ctx->resorts -= ran;
             ctx->graph_steps -= ran;
@@ -2478,8 +2485,14 @@ int gc_step(gc_ctx* ctx, int nsteps, double cfl) {
     if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
     if (nsteps < 0) return seterr(ctx, GC_ERR_ARG, "negative step count");
     cudaSetDevice(ctx->device);
-    upload_inst_params(ctx, cfl);
-    for (auto& S : ctx->slots) TRY(push_slot_params(ctx, S));
+    // per-instance step parameters change only with the CFL number (or when
+    // a phase hook or the serving loop has edited them)
+    if (ctx->params_dirty || !(cfl == ctx->params_cfl)) {
+        upload_inst_params(ctx, cfl);
+        for (auto& S : ctx->slots) TRY(push_slot_params(ctx, S));
+        ctx->params_cfl = cfl;
+        ctx->params_dirty = false;
+    }
     if (decide_motion(ctx)) invalidate_steps(ctx);
     CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     TRY(run_steps(ctx, nsteps));
@@ -2552,6 +2565,7 @@ int gc_sort_system(gc_ctx* ctx, int inst, int handle, double cutoff, int64_t* pe
     }
     DSlot& S = *r.slot;
     for (auto& h : S.h_inst) h.sort_cutoff = cutoff;
+    ctx->params_dirty = true;  // the next gc_step restores its own cutoff
     TRY(push_slot_params(ctx, S));
     TRY(bbox_slot(ctx, S));
     launch_sort_plan(S.d_inst, ni, S.nd, ctx->d_need + r.sys, ctx->d_err, ctx->stream);
@@ -2793,6 +2807,7 @@ int ctx_ninst(gc_ctx* c) { return (int)c->inst.size(); }
 int ctx_set_cfl(gc_ctx* c, int inst, double cfl) {
     if (!valid_inst(c, inst)) return GC_ERR_ARG;
     c->inst[inst].cfl = cfl;
+    c->params_dirty = true;
     return GC_OK;
 }
 

@@ -384,12 +384,9 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0)
 
 
 def upload_instance(backend, m: InstanceMap, systems=None):
-    # v_adjustment (XSPH) must be zero on this path; an all-zero array is not
-    # sent (the device checks any other)
     items = [(m.inst, m.h(ps), fid, getattr(ps, name))
              for ps in m.systems if systems is None or any(ps is q for q in systems)
-             for name, fid in ps.particle_fields()
-             if not (fid == C.GC_FIELD_V_ADJUSTMENT and not np.any(getattr(ps, name)))]
+             for name, fid in ps.particle_fields()]
     if hasattr(backend, "upload_many"):
         backend.upload_many(items)
     else:
