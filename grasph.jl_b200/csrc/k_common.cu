@@ -99,8 +99,51 @@ int64_t scan_tmp_elems(int64_t n) {
     return nb + (nb + 1) + scan_tmp_elems(nb);
 }
 
+// Second pass for up to SCAN_TILE tiles: each block adds up the sums of the
+// tiles before it itself (at most SCAN_TILE values), so the scan of the tile
+// sums needs no launch of its own.
+__global__ void k_scan_apply_sums(const int32_t* __restrict__ in, int64_t n, const int32_t* __restrict__ bsum,
+                                  int32_t* __restrict__ out, int32_t* clear) {
+    __shared__ int32_t off;
+    {
+        int32_t s = 0;
+        for (int64_t b = threadIdx.x; b < blockIdx.x; b += blockDim.x) s += bsum[b];
+        int32_t total;
+        (void)block_excl_scan(s, &total);
+        if (threadIdx.x == 0) off = total;
+        __syncthreads();
+    }
+    int64_t t0 = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
+    int32_t v[SCAN_I];
+    int32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_I; ++k) {
+        v[k] = t0 + k < n ? in[t0 + k] : 0;
+        sum += v[k];
+    }
+    if (clear) {
+#pragma unroll
+        for (int k = 0; k < SCAN_I; ++k)
+            if (t0 + k < n) clear[t0 + k] = 0;
+    }
+    int32_t total;
+    int32_t run = block_excl_scan(sum, &total) + off;
+#pragma unroll
+    for (int k = 0; k < SCAN_I; ++k) {
+        if (t0 + k < n) out[t0 + k] = run;
+        run += v[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = off + total;
+}
+
 static void scan_impl(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, int32_t* clear, cudaStream_t s) {
     int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb > 1 && nb <= SCAN_TILE) {
+        k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, tmp);
+        k_scan_apply_sums<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, tmp, out, clear);
+        COUNTED(2);
+        return;
+    }
     if (nb <= 1) {
         k_scan_apply<<<1, SCAN_T, 0, s>>>(in, n, nullptr, out, clear);
         COUNTED(1);
