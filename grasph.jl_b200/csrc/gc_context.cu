@@ -75,6 +75,7 @@ struct HInst {
     std::vector<HGhost> ghosts;
     std::vector<HInter> inters;
     double gamma = 0;
+    int integ = GC_INTEGRATOR_LEAPFROG;
     double cfl = NAN;              // own CFL number (serving); NaN: gc_step's
     std::vector<HStaged> staged;   // fields given before gc_finalize
 };
@@ -90,6 +91,7 @@ struct DSlot {
     int32_t* id[2] = {};
     int cur = 0;
     double *q0v = nullptr, *q0rho = nullptr, *aux = nullptr;
+    double *accv = nullptr, *accrho = nullptr;  // RK4 accumulators (allocated on first use)
     int32_t* inst_of = nullptr;
     SysInst* d_inst = nullptr;
     std::vector<SysInst> h_inst;
@@ -403,6 +405,7 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
 
 // ------------------------------------------------------------- finalize
 bool same_structure(const HInst& a, const HInst& b, std::string& why) {
+    if (a.integ != b.integ) return why = "integrator kind", false;
     if (a.sys.size() != b.sys.size()) return why = "system count", false;
     for (size_t s = 0; s < a.sys.size(); ++s) {
         const HSys &x = a.sys[s], &y = b.sys[s];
@@ -1130,6 +1133,8 @@ StepArgs step_args(DSlot& S) {
     a.drhodt = S.F(F_DRHODT);
     a.q0v = S.q0v;
     a.q0rho = S.q0rho;
+    a.accv = S.accv;
+    a.accrho = S.accrho;
     return a;
 }
 
@@ -1504,7 +1509,10 @@ bool decide_motion(gc_ctx* ctx) {
     return changed;
 }
 
+int one_step_rk4(gc_ctx* ctx);
+
 int one_step(gc_ctx* ctx) {
+    if (ctx->inst[0].integ == GC_INTEGRATOR_RK4) return one_step_rk4(ctx);
     ctx->pack_epoch++;
     std::vector<char> mask(ctx->slots.size());
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
@@ -1528,6 +1536,50 @@ int one_step(gc_ctx* ctx) {
     for (auto& S : ctx->slots)
         if (S.moving) launch_fullstep(step_args(S), ctx->stream);
     TRY(check_launch(ctx, "full step"));
+    ctx->steps_done += 1;
+    return GC_OK;
+}
+
+// src/TimeIntegration.jl:771-826: one grid per step, four right-hand-side
+// evaluations from q0, q = q0 + dt·(k1/6 + k2/3 + k3/3 + k4/6), positions once.
+int one_step_rk4(gc_ctx* ctx) {
+    ctx->pack_epoch++;
+    std::vector<char> mask(ctx->slots.size());
+    for (size_t s = 0; s < ctx->slots.size(); ++s) {
+        DSlot& S = ctx->slots[s];
+        mask[s] = S.moving || !S.sorted_once;
+        if (S.moving && !S.accv) {
+            TRY(dalloc(ctx, &S.accv, (size_t)S.nd * S.N));
+            TRY(dalloc(ctx, &S.accrho, (size_t)S.N));
+        }
+    }
+    TRY(prepare(ctx, mask));
+    for (size_t s = 0; s < ctx->slots.size(); ++s)
+        if (mask[s]) ctx->slots[s].sorted_once = true;
+    ctx->resorts += 1;
+    // Julia's T(0.5), T(1.0) and T(1/6), T(1/3) (src/TimeIntegration.jl:742-743)
+    const double advance[4] = {0.0, 0.5, 0.5, 1.0};
+    const double weight[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+    for (auto& S : ctx->slots)
+        if (S.moving) launch_rk4_begin(step_args(S), ctx->stream);
+    for (int it = 0; it < 4; ++it) {
+        if (it > 0)
+            for (auto& S : ctx->slots)
+                if (S.moving) launch_rk4_advance(step_args(S), advance[it], ctx->stream);
+        TRY(check_launch(ctx, "rk4 stage"));
+        for (auto& G : ctx->ghosts) TRY(ghost_kinematics(ctx, G));
+        for (int stage = 1; stage <= ctx->nstages; ++stage) {
+            for (auto& S : ctx->slots)
+                if (S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
+            for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
+            TRY(sweep_stage(ctx, stage));
+        }
+        for (auto& S : ctx->slots)
+            if (S.moving) launch_rk4_acc(step_args(S), weight[it], ctx->stream);
+    }
+    for (auto& S : ctx->slots)
+        if (S.moving) launch_rk4_final(step_args(S), ctx->stream);
+    TRY(check_launch(ctx, "rk4 final"));
     ctx->steps_done += 1;
     return GC_OK;
 }
@@ -1926,6 +1978,8 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         }
         cudaFree(S.q0v);
         cudaFree(S.q0rho);
+        cudaFree(S.accv);
+        cudaFree(S.accrho);
         cudaFree(S.aux);
         cudaFree(S.inst_of);
         cudaFree(S.groups);
@@ -2198,6 +2252,16 @@ int gc_set_integrator(gc_ctx* ctx, int inst, double damping_gamma) {
     if (!ctx) return GC_ERR_ARG;
     if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
     ctx->inst[inst].gamma = damping_gamma;
+    return GC_OK;
+}
+
+int gc_set_integrator_kind(gc_ctx* ctx, int inst, int kind) {
+    if (!ctx) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
+    if (kind != GC_INTEGRATOR_LEAPFROG && kind != GC_INTEGRATOR_RK4)
+        return seterr(ctx, GC_ERR_ARG, "unknown integrator kind %d", kind);
+    ctx->inst[inst].integ = kind;
     return GC_OK;
 }
 

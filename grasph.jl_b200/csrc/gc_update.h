@@ -14,6 +14,7 @@ struct StepArgs {
     const int32_t* inst_of;
     const SysInst* inst;
     double *x, *v, *rho, *dvdt, *drhodt, *q0v, *q0rho;
+    double *accv, *accrho;  // RK4 accumulators (nullptr for LeapFrog)
 };
 
 struct UpdArgs {
@@ -28,6 +29,14 @@ struct UpdArgs {
 
 void launch_halfstep(const StepArgs& a, cudaStream_t s);
 void launch_fullstep(const StepArgs& a, cudaStream_t s);
+// RK4 (src/TimeIntegration.jl:712-838): q0 snapshot, zero accumulators and
+// dqdt reset; stage advance q = q0 + f·dt·dqdt (f = 0.5 or 1) and dqdt reset;
+// damping and acc += w·dqdt after a stage's sweeps; q = q0 + dt·acc, zero
+// XSPH pass and x += dt·v at the end.
+void launch_rk4_begin(const StepArgs& a, cudaStream_t s);
+void launch_rk4_advance(const StepArgs& a, double f, cudaStream_t s);
+void launch_rk4_acc(const StepArgs& a, double w, cudaStream_t s);
+void launch_rk4_final(const StepArgs& a, cudaStream_t s);
 void launch_update(const UpdArgs& a, cudaStream_t s);
 
 }  // namespace gc

@@ -55,6 +55,85 @@ __global__ void k_fullstep(StepArgs a) {
     }
 }
 
+// ------------------------------------------------------------------ RK4
+// src/TimeIntegration.jl:783-791 (_save_q0_all!, _zero_acc_all!) and, for
+// the first stage, :800 (_reset_dqdt_all!).
+__global__ void k_rk4_begin(StepArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const SysInst& S = a.inst[a.inst_of[g]];
+        for (int d = 0; d < a.nd; ++d) {
+            a.q0v[d * a.N + g] = a.v[d * a.N + g];
+            a.accv[d * a.N + g] = 0.0;
+            a.dvdt[d * a.N + g] = S.srcv[d];
+        }
+        a.q0rho[g] = a.rho[g];
+        a.accrho[g] = 0.0;
+        a.drhodt[g] = S.srcrho;
+    }
+}
+
+// :802 (_rk4_advance_all!): q = q0 + (f·dt)·dqdt, then dqdt <- source.
+__global__ void k_rk4_advance(StepArgs a, double f) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const SysInst& S = a.inst[a.inst_of[g]];
+        const double c = f * S.dt;
+        for (int d = 0; d < a.nd; ++d) {
+            a.v[d * a.N + g] = a.q0v[d * a.N + g] + c * a.dvdt[d * a.N + g];
+            a.dvdt[d * a.N + g] = S.srcv[d];
+        }
+        a.rho[g] = fma(c, a.drhodt[g], a.q0rho[g]);
+        a.drhodt[g] = S.srcrho;
+    }
+}
+
+// :814-816: damping (dvdt -= Γ/dt·v), then acc += w·dqdt.
+__global__ void k_rk4_acc(StepArgs a, double w) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const SysInst& S = a.inst[a.inst_of[g]];
+        for (int d = 0; d < a.nd; ++d) {
+            double dv = a.dvdt[d * a.N + g];
+            if (S.gamma_dt != 0.0) {
+                dv = dv - S.gamma_dt * a.v[d * a.N + g];
+                a.dvdt[d * a.N + g] = dv;
+            }
+            a.accv[d * a.N + g] = a.accv[d * a.N + g] + w * dv;
+        }
+        a.accrho[g] = fma(w, a.drhodt[g], a.accrho[g]);
+    }
+}
+
+// :820-826: q = q0 + dt·acc, zero XSPH pass, x += dt·v.
+__global__ void k_rk4_final(StepArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const SysInst& S = a.inst[a.inst_of[g]];
+        const double dt = S.dt;
+        for (int d = 0; d < a.nd; ++d) {
+            double v = a.q0v[d * a.N + g] + dt * a.accv[d * a.N + g];
+            v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
+            a.v[d * a.N + g] = v;
+            a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
+        }
+        a.rho[g] = fma(dt, a.accrho[g], a.q0rho[g]);
+    }
+}
+
+void launch_rk4_begin(const StepArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_rk4_begin<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+void launch_rk4_advance(const StepArgs& a, double f, cudaStream_t s) {
+    if (a.N > 0) k_rk4_advance<<<ublk(a.N), UTPB, 0, s>>>(a, f);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+void launch_rk4_acc(const StepArgs& a, double w, cudaStream_t s) {
+    if (a.N > 0) k_rk4_acc<<<ublk(a.N), UTPB, 0, s>>>(a, w);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+void launch_rk4_final(const StepArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_rk4_final<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+
 void launch_halfstep(const StepArgs& a, cudaStream_t s) {
     if (a.N > 0) k_halfstep<<<ublk(a.N), UTPB, 0, s>>>(a);
     g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);

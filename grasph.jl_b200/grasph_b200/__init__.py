@@ -9,7 +9,7 @@ from . import consts
 from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, CauchyFluidPfn,
                     CountingPfn, CubicSplineKernel, DynamicBoundarySystem, ElastoPlasticParticleSystem,
                     ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn, GhostCopier, GhostEntry,
-                    GhostParticleSystem, HookeLawStressUpdater, HouseholderReflect, LeapFrogTimeIntegrator,
+                    GhostParticleSystem, HookeLawStressUpdater, HouseholderReflect, LeapFrogTimeIntegrator, RK4TimeIntegrator,
                     LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
                     StressParticleSystem, SystemInteraction, TaitEOSUpdater, WenlandC2Kernel,
                     ZeroFieldUpdater, is_coupled)

@@ -81,6 +81,7 @@ def load_library(path: os.PathLike | None = None):
                                           ct.c_int, _ip, _dp, _ip]),
         "gc_set_updaters": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _ip, _ip, _dp]),
         "gc_set_integrator": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double]),
+        "gc_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
         "gc_finalize": (ct.c_int, [ct.c_void_p]),
         "gc_upload_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         "gc_download_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
@@ -207,6 +208,9 @@ class CudaBackend:
     def set_integrator(self, inst, gamma):
         self._chk(self.lib.gc_set_integrator(self.ctx, inst, gamma), "gc_set_integrator")
 
+    def set_integrator_kind(self, inst, kind):
+        self._chk(self.lib.gc_set_integrator_kind(self.ctx, inst, kind), "gc_set_integrator_kind")
+
     def finalize(self):
         self._chk(self.lib.gc_finalize(self.ctx), "gc_finalize")
 
@@ -322,7 +326,8 @@ class InstanceMap:
         return self.handles[id(obj)]
 
 
-def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0) -> InstanceMap:
+def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
+                     kind=C.GC_INTEGRATOR_LEAPFROG) -> InstanceMap:
     """Issue the model-building calls for one simulation (one instance)."""
     m = InstanceMap(inst)
     sys_ids = {id(ps) for ps in systems}
@@ -380,6 +385,8 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0)
         if chains:
             backend.set_updaters(inst, m.h(ps), chains)
     backend.set_integrator(inst, gamma)
+    if kind != C.GC_INTEGRATOR_LEAPFROG:
+        backend.set_integrator_kind(inst, kind)
     return m
 
 
@@ -448,7 +455,7 @@ class Session:
         for lf in self.integrators:
             inst = self.backend.instance_add()
             self.maps.append(compile_instance(self.backend, inst, lf.systems, lf.interactions, lf.ghosts,
-                                              lf.gamma))
+                                              lf.gamma, lf.kind))
         self.backend.finalize()
         self.backend.set_precision(precision)
         self.precision = precision
@@ -629,7 +636,7 @@ class Server:
         """Queue one simulation; its current host state is copied now."""
         be = CudaBackend(self.device, 0, lib=self.lib)
         inst = be.instance_add()
-        m = compile_instance(be, inst, lf.systems, lf.interactions, lf.ghosts, lf.gamma)
+        m = compile_instance(be, inst, lf.systems, lf.interactions, lf.ghosts, lf.gamma, lf.kind)
         for ps in m.systems:
             h = m.h(ps)
             for name, fid in ps.particle_fields():

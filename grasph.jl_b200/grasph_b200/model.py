@@ -552,6 +552,8 @@ def is_coupled(si: SystemInteraction) -> bool:
 class LeapFrogTimeIntegrator:
     """src/TimeIntegration.jl:29-67."""
 
+    kind = C.GC_INTEGRATOR_LEAPFROG
+
     def __init__(self, systems, interactions, *, ghosts=(), gamma=0.0, **kw):
         if "Γ" in kw:
             gamma = kw.pop("Γ")
@@ -571,3 +573,10 @@ class LeapFrogTimeIntegrator:
         self.h = min(it.kernel.h for it in ints)
         self.gamma = float(gamma)
         self._device = None
+
+
+class RK4TimeIntegrator(LeapFrogTimeIntegrator):
+    """src/TimeIntegration.jl:86-113: classical fourth-order Runge-Kutta, one
+    neighbour grid per step, positions advanced once at the end."""
+
+    kind = C.GC_INTEGRATOR_RK4

@@ -66,19 +66,24 @@ upd_entry(u) = throw(ArgumentError("state updater $(typeof(u)) has no device imp
 fields_of(ps) = [f for f in (:x, :v, :rho, :dvdt, :drhodt, :p, :stress, :strain_rate, :vorticity,
                                :strain, :strain_p) if hasfield(typeof(ps), f)]
 
-"""
-    CudaLeapFrog(lf::LeapFrogTimeIntegrator; device=0)
+# integrator kind of the C ABI (GC_INTEGRATOR_LEAPFROG / GC_INTEGRATOR_RK4)
+integ_kind(::LeapFrogTimeIntegrator) = Cint(0)
+integ_kind(::RK4TimeIntegrator) = Cint(1)
 
-A device context holding the model of `lf` (one instance).
+"""
+    CudaLeapFrog(lf::Union{LeapFrogTimeIntegrator,RK4TimeIntegrator}; device=0)
+
+A device context holding the model of `lf` (one instance), stepped with the
+integrator `lf` is (LeapFrog or RK4).
 """
 mutable struct CudaLeapFrog
     ctx::Ptr{Cvoid}
-    lf::LeapFrogTimeIntegrator
+    lf::Union{LeapFrogTimeIntegrator,RK4TimeIntegrator}
     handles::IdDict{Any,Cint}
     inters::Vector{Cint}
 end
 
-function CudaLeapFrog(lf::LeapFrogTimeIntegrator; device::Integer=0)
+function CudaLeapFrog(lf::Union{LeapFrogTimeIntegrator,RK4TimeIntegrator}; device::Integer=0)
     ctx = Ref{Ptr{Cvoid}}(C_NULL)
     check(C_NULL, ccall((:gc_ctx_create, LIB), Cint, (Cint, Csize_t, Ref{Ptr{Cvoid}}), device, 0, ctx))
     inst = Ref{Cint}(0)
@@ -167,6 +172,8 @@ function CudaLeapFrog(lf::LeapFrogTimeIntegrator; device::Integer=0)
                            ctx[], inst[], h[ps], length(lens), lens, kinds, prm))
     end
     check(ctx[], ccall((:gc_set_integrator, LIB), Cint, (Ptr{Cvoid}, Cint, Cdouble), ctx[], inst[], lf.Γ))
+    check(ctx[], ccall((:gc_set_integrator_kind, LIB), Cint, (Ptr{Cvoid}, Cint, Cint), ctx[], inst[],
+                       integ_kind(lf)))
     check(ctx[], ccall((:gc_finalize, LIB), Cint, (Ptr{Cvoid},), ctx[]))
     cl = CudaLeapFrog(ctx[], lf, h, ints)
     finalizer(c -> ccall((:gc_ctx_destroy, LIB), Cint, (Ptr{Cvoid},), c.ctx), cl)

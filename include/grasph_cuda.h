@@ -202,6 +202,12 @@ int gc_set_updaters(gc_ctx* ctx, int inst, int sys, int nstages, const int* chai
  * src/TimeIntegration.jl:53.  The systems list is every system added to
  * the instance in order; the ghosts list every ghost handle.              */
 int gc_set_integrator(gc_ctx* ctx, int inst, double damping_gamma);
+/* The integrator's kind (the same for every instance of a context):
+ * GC_INTEGRATOR_LEAPFROG (default) or GC_INTEGRATOR_RK4, RK4TimeIntegrator
+ * src/TimeIntegration.jl:86 (one grid per step, four right-hand-side
+ * evaluations, positions advanced once at the end).                       */
+enum { GC_INTEGRATOR_LEAPFROG = 0, GC_INTEGRATOR_RK4 = 1 };
+int gc_set_integrator_kind(gc_ctx* ctx, int inst, int kind);
 
 /* Validate every instance against instance 0's structure and allocate the
  * device state.  Model-building calls are refused afterwards.              */

@@ -130,6 +130,7 @@ struct Sys {
     bool upd_set = false;
     std::vector<std::vector<Upd>> upd;  // one chain per updater-tuple entry
     std::vector<double> q0v, q0rho;
+    std::vector<double> accv, accrho;  // RK4 accumulators
     bool has_p() const { return kind >= GC_SYS_FLUID; }
     bool has_stress() const { return kind >= GC_SYS_STRESS; }
     bool is_ep() const { return kind == GC_SYS_ELASTOPLASTIC; }
@@ -184,6 +185,7 @@ struct oracle_ctx {
     std::vector<int> sys_handle;  // handle of each system
     std::vector<Inter> inters;
     double gamma = 0;
+    int integ = GC_INTEGRATOR_LEAPFROG;
     int threads = 1;
     int64_t steps = 0;
     std::string err;
@@ -1350,6 +1352,92 @@ int step_once(oracle_ctx* ctx, double dt) {
     return GC_OK;
 }
 
+// src/TimeIntegration.jl:712-838 (RK4): one grid per step, four right-hand
+// side evaluations from q0, q = q0 + dt·acc, positions once at the end.
+// Rounding as for LeapFrog: `@fastmath` axpy fuses on scalar fields (rho)
+// and rounds twice on SVector fields (v).
+int step_rk4(oracle_ctx* ctx, double dt) {
+    const int nst = num_stages(ctx);
+    double hmin = 1e300;
+    for (auto& it : ctx->inters) hmin = std::min(hmin, it.H);
+    const double sort_cutoff = 2.0 * hmin;
+    // 1. sort every real system
+    for (auto& s : ctx->sys) {
+        int st = sort_system(s, sort_cutoff, nullptr);
+        if (st) return fail(ctx, st, "sort: non-finite position");
+    }
+    // 2. save q0, zero the accumulators (:783-784)
+    for (auto& s : ctx->sys) {
+        s.q0v = s.v;
+        s.q0rho = s.rho;
+        s.accv.assign(s.v.size(), 0.0);
+        s.accrho.assign(s.rho.size(), 0.0);
+    }
+    // 3-5. ghosts, ghost sort, grids (:787-788)
+    for (auto& g : ctx->ghosts) generate_ghosts(ctx, g);
+    for (auto& g : ctx->ghosts) {
+        const Sys& src = ctx->sys[g.src];
+        int st = sort_ghost(g, src.nd, src.ns, sort_cutoff, nullptr);
+        if (st) return fail(ctx, st, "ghost sort: non-finite position");
+    }
+    for (auto& it : ctx->inters) {
+        int st = create_grid(ctx, it);
+        if (st) return st;
+    }
+    // T(0.5), T(1.0), T(1/6), T(1/3) (:742-743)
+    const double advance[4] = {0.0, 0.5, 0.5, 1.0};
+    const double weight[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+    for (int rk = 0; rk < 4; ++rk) {
+        // 6. reset dqdt (first stage) or q = q0 + (f·dt)·dqdt then reset (:797-803)
+        const double c = advance[rk] * dt;
+        for (auto& s : ctx->sys) {
+            const int nd = s.nd;
+            if (rk > 0) {
+                for (int64_t i = 0; i < s.n * nd; ++i) s.v[i] = s.q0v[i] + c * s.dvdt[i];
+                for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(c, s.drhodt[i], s.q0rho[i]);
+            }
+            for (int64_t i = 0; i < s.n; ++i)
+                for (int d = 0; d < nd; ++d) s.dvdt[i * nd + d] = s.srcv[d];
+            for (int64_t i = 0; i < s.n; ++i) s.drhodt[i] = s.srcrho;
+        }
+        // 7. ghost kinematics (:805-807)
+        for (auto& g : ctx->ghosts) ghost_kinematics(ctx, g);
+        // 8. stages (:809-810)
+        for (int stage = 1; stage <= nst; ++stage) {
+            for (auto& s : ctx->sys)
+                if (s.upd_set && (int)s.upd.size() == nst) update_state(s, stage, dt);
+            for (auto& g : ctx->ghosts) update_ghost(ctx, g, stage);
+            for (auto& it : ctx->inters) {
+                int st = sweep(ctx, it, stage);
+                if (st) return st;
+            }
+        }
+        // damping and acc += w·dqdt (:812-814)
+        if (ctx->gamma != 0.0) {
+            const double gdt = ctx->gamma / dt;
+            for (auto& s : ctx->sys)
+                for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
+        }
+        for (auto& s : ctx->sys) {
+            for (int64_t i = 0; i < s.n * s.nd; ++i) s.accv[i] = s.accv[i] + weight[rk] * s.dvdt[i];
+            for (int64_t i = 0; i < s.n; ++i) s.accrho[i] = std::fma(weight[rk], s.drhodt[i], s.accrho[i]);
+        }
+    }
+    // 9. q = q0 + dt·acc (:818)
+    for (auto& s : ctx->sys) {
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.accv[i];
+        for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.accrho[i], s.q0rho[i]);
+    }
+    // 10. XSPH correction with a zero adjustment (:821)
+    for (auto& s : ctx->sys)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = (s.v[i] + (-1.0 * s.vadj[i])) + 1.0 * s.vadj[i];
+    // 11. positions (:824)
+    for (auto& s : ctx->sys)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+    ctx->steps += 1;
+    return GC_OK;
+}
+
 double compute_dt(oracle_ctx* ctx, double cfl) {
     double c = -1e300, h = 1e300;
     for (auto& s : ctx->sys) c = std::max(c, s.c);
@@ -1582,6 +1670,12 @@ int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_
     return GC_OK;
 }
 
+int oracle_set_integrator_kind(oracle_ctx* ctx, int kind) {
+    if (kind != GC_INTEGRATOR_LEAPFROG && kind != GC_INTEGRATOR_RK4) return GC_ERR_ARG;
+    ctx->integ = kind;
+    return GC_OK;
+}
+
 int oracle_set_integrator(oracle_ctx* ctx, double gamma) {
     ctx->gamma = gamma;
     return GC_OK;
@@ -1653,7 +1747,7 @@ int oracle_step(oracle_ctx* ctx, int nsteps, double cfl) {
         if (it.nstages != nst) return fail(ctx, GC_ERR_ARG, "All interactions must have the same number of stages");
     double dt = compute_dt(ctx, cfl);
     for (int s = 0; s < nsteps; ++s) {
-        int st = step_once(ctx, dt);
+        int st = ctx->integ == GC_INTEGRATOR_RK4 ? step_rk4(ctx, dt) : step_once(ctx, dt);
         if (st) return st;
     }
     return GC_OK;
