@@ -448,6 +448,7 @@ UpdInst make_upd(const HUpd& u, const HSys& s) {
         d.pre = rho0 * s.c * s.c / gam;
         d.gamma_int = (gam == std::trunc(gam) && std::fabs(gam) < 9.0e15) ? 1 : 0;
     }
+    if (u.kind == GC_UPD_VISCOPLASTIC_MC) d.pre = std::tan(u.prm[0]);  // tan(φ), hoisted to the host
     if (u.kind == GC_UPD_ELASTOPLASTIC || u.kind == GC_UPD_HOOKE) {
         double E = u.prm[0], nu = u.prm[1], phi = u.prm[2], psi = u.prm[3], coh = u.prm[4];
         d.D0 = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
@@ -2240,7 +2241,9 @@ int gc_set_updaters(gc_ctx* ctx, int inst, int sys, int nstages, const int* chai
                 return seterr(ctx, GC_ERR_ARG, "ElastoPlasticStressUpdater requires NS=4 (plane-strain Voigt)");
             if ((u.kind == GC_UPD_TAIT_EOS || u.kind == GC_UPD_LINEAR_EOS) && s.kind < GC_SYS_FLUID)
                 return seterr(ctx, GC_ERR_ARG, "EOS updater needs a pressure field");
-            if (u.kind < GC_UPD_NONE || u.kind > GC_UPD_HOOKE) return seterr(ctx, GC_ERR_ARG, "bad updater kind");
+            if (u.kind == GC_UPD_VISCOPLASTIC_MC && (s.kind < GC_SYS_STRESS || (s.ns != 3 && s.ns != 4 && s.ns != 6)))
+                return seterr(ctx, GC_ERR_ARG, "ViscoPlasticMCStressUpdater needs stress with NS = 3, 4 or 6");
+            if (u.kind < GC_UPD_NONE || u.kind > GC_UPD_VISCOPLASTIC_MC) return seterr(ctx, GC_ERR_ARG, "bad updater kind");
             if (u.kind != GC_UPD_NONE) chain.push_back(u);
         }
         s.upd.push_back(chain);

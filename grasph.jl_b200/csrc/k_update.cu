@@ -255,6 +255,32 @@ __global__ void k_update(UpdArgs a) {
                 }
                 break;
             }
+            case GC_UPD_VISCOPLASTIC_MC: {
+                // src/StateUpdaters.jl:155-186 after the EOS: rigid-plastic
+                // Mohr–Coulomb stress along the strain rate, minus p, apex clamp
+                const int ns = a.ns;
+                double sr[MAXS];
+                for (int q = 0; q < ns; ++q) sr[q] = a.sr[q * N + g];
+                double m;
+                if (ns == 3) m = sr[0] * sr[0] + sr[1] * sr[1] + 2.0 * (sr[2] * sr[2]);
+                else if (ns == 4) m = sr[0] * sr[0] + sr[1] * sr[1] + 2.0 * (sr[3] * sr[3]);
+                else
+                    m = sr[0] * sr[0] + sr[1] * sr[1] + sr[2] * sr[2] +
+                        2.0 * (sr[3] * sr[3] + sr[4] * sr[4] + sr[5] * sr[5]);
+                m = jmax(sqrt(m), 2.220446049250313e-16);  // eps(Float64)
+                const double p = a.p[g];
+                const double sc = 2.0 * (u.prm[1] + p * u.pre);
+                const int nn = ns == 3 ? 2 : 3;  // normal components
+                double st[MAXS], tr = 0.0;
+                for (int q = 0; q < ns; ++q) {
+                    st[q] = (sc * sr[q]) / m;
+                    st[q] = st[q] - (q < nn ? p : 0.0);
+                }
+                for (int q = 0; q < nn; ++q) tr = q == 0 ? st[0] : tr + st[q];
+                const bool apex = tr > 0.0;
+                for (int q = 0; q < ns; ++q) a.stress[q * N + g] = apex ? 0.0 : st[q];
+                break;
+            }
             case GC_UPD_HOOKE: {
                 // src/StateUpdaters.jl:366-405
                 const double nu = u.prm[1], D0 = u.D0, omn = u.omn, om2n = u.om2n;

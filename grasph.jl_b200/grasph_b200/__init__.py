@@ -11,7 +11,8 @@ from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, 
                     ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn, GhostCopier, GhostEntry,
                     GhostParticleSystem, HookeLawStressUpdater, HouseholderReflect, LeapFrogTimeIntegrator, RK4TimeIntegrator,
                     LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
-                    StressParticleSystem, SystemInteraction, TaitEOSUpdater, WenlandC2Kernel,
+                    StressParticleSystem, SystemInteraction, TaitEOSUpdater, ViscoPlasticMCStressUpdater,
+                    WenlandC2Kernel,
                     ZeroFieldUpdater, is_coupled)
 from .engine import (CudaBackend, GcError, Server, Session, compile_instance, download_instance, load_library,
                      time_integrate, upload_instance)

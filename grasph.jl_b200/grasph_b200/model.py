@@ -421,6 +421,10 @@ class _Updater:
     def params(self):
         return np.zeros(C.GC_UPD_NPARAM)
 
+    def entries(self):
+        """(kind, params) chain entries this updater compiles to."""
+        return [(self.kind, self.params())]
+
 
 class ZeroFieldUpdater(_Updater):
     """src/StateUpdaters.jl:30-42."""
@@ -503,6 +507,29 @@ class HookeLawStressUpdater(_Updater):
         return p
 
 
+class ViscoPlasticMCStressUpdater(_Updater):
+    """Rigid-plastic Mohr–Coulomb stress along the strain rate after an EOS
+    update, src/StateUpdaters.jl:144-186.  Compiles to two chain entries:
+    the EOS, then the stress part."""
+
+    kind = C.GC_UPD_VISCOPLASTIC_MC
+
+    def __init__(self, eos, friction_angle, cohesion):
+        if not isinstance(eos, (TaitEOSUpdater, LinearEOSUpdater)):
+            raise ArgumentError("ViscoPlasticMCStressUpdater: eos must be an EOS updater")
+        self.eos = eos
+        self.friction_angle = float(friction_angle)
+        self.cohesion = float(cohesion)
+
+    def params(self):
+        p = super().params()
+        p[0], p[1] = self.friction_angle, self.cohesion
+        return p
+
+    def entries(self):
+        return self.eos.entries() + [(self.kind, self.params())]
+
+
 def updater_chains(ps: AbstractParticleSystem):
     """The state_updater tuple as per-stage chains of (kind, params)."""
     chains = []
@@ -510,9 +537,9 @@ def updater_chains(ps: AbstractParticleSystem):
         if entry is None:
             chains.append([])
         elif isinstance(entry, tuple):
-            chains.append([(u.kind, u.params()) for u in entry if u is not None])
+            chains.append([e for u in entry if u is not None for e in u.entries()])
         elif isinstance(entry, _Updater):
-            chains.append([(entry.kind, entry.params())])
+            chains.append(entry.entries())
         else:
             raise ArgumentError(f"unsupported state updater {type(entry).__name__}")
     return chains

@@ -20,8 +20,9 @@ import numpy as np
 
 from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, DynamicBoundarySystem,
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
-                    GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator,
-                    StrainRateVorticityPfn, SystemInteraction, TaitEOSUpdater, ZeroFieldUpdater)
+                    GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator, LinearEOSUpdater,
+                    StrainRatePfn, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
+                    TaitEOSUpdater, ViscoPlasticMCStressUpdater, ZeroFieldUpdater)
 
 G = 9.81
 
@@ -188,6 +189,43 @@ def column_collapse(nx=400, ny=200, dx=0.0005, rho0=2650.0, E=0.84e6, nu=0.3, ph
               SystemInteraction(kernel, (srv, cau), fluid, ghost)]
     lf = LeapFrogTimeIntegrator([fluid, bottom], inters, ghosts=(gentry,))
     meta = dict(workload="column_collapse", n_fluid=fluid.n, n_boundary=bottom.n, h=h, c0=c, cfl=cfl,
+                dt=cfl * h / c, ndims=2, phi=phi, E=E)
+    return lf, meta
+
+
+def granular_column(nfx=100, nfy=50, dx=0.002, rho0=1850.0, E=0.84e6, nu=0.3, phi_deg=19.8, cohesion=0.0,
+                    alpha=0.1, beta=0.1, delta=0.1, hfac=1.2, cfl=0.1, bottom_len=0.5, layers=3, wall_beta=3.0):
+    """2-D granular column collapse with the visco-plastic Mohr–Coulomb
+    updater (GranularColumnCollapse.jl layout): StressParticleSystem NS = 3,
+    stages (StrainRatePfn, CauchyFluidPfn with δ-SPH), dynamic bottom, ghost
+    left wall with the stress copied at stage 2, LinearEOS inside the stress
+    updater."""
+    phi = phi_deg * math.pi / 180.0
+    c = math.sqrt(E * (1 - nu) / (rho0 * (1 + nu) * (1 - 2 * nu)))
+    h = hfac * dx
+    mass = rho0 * dx * dx
+    ii, jj = np.meshgrid(np.arange(nfx), np.arange(nfy), indexing="ij")
+    x = np.stack([(ii.ravel() + 0.5) * dx, (jj.ravel() + 0.5) * dx], axis=1)
+    fluid = StressParticleSystem(
+        "fluid", len(x), 2, 3, mass, c, source_v=[0.0, -G],
+        state_updater=(ZeroFieldUpdater("strain_rate"),
+                       ViscoPlasticMCStressUpdater(LinearEOSUpdater(rho0), phi, cohesion)))
+    fluid.x[:] = x
+    fluid.rho[:] = rho0
+    nbx = int(math.floor(bottom_len / dx))
+    bx = np.array([((i - 3.5) * dx, -(j - 0.5) * dx) for i in range(1, nbx + 4) for j in range(1, layers + 1)])
+    bottom = _wall("bottom_boundary", bx, mass, c, rho0)
+    ghost = GhostParticleSystem(fluid, None, GhostCopier("stress"))
+    gentry = GhostEntry(ghost, 3.0 * h, ((1.0, 0.0), (0.0, 0.0)), capacity=int(fluid.n))
+    kernel = CubicSplineKernel(h, ndims=2)
+    sr = StrainRatePfn()
+    cau = CauchyFluidPfn(alpha, beta, h, delta=delta)
+    dyn = DynamicBoundarySystem(bottom, (0.0, 1.0), (0.0, 0.0), wall_beta)
+    inters = [SystemInteraction(kernel, (sr, cau), fluid),
+              SystemInteraction(kernel, (sr, cau), fluid, dyn),
+              SystemInteraction(kernel, (sr, cau), fluid, ghost)]
+    lf = LeapFrogTimeIntegrator([fluid, bottom], inters, ghosts=(gentry,))
+    meta = dict(workload="granular_column", n_fluid=fluid.n, n_boundary=bottom.n, h=h, c0=c, cfl=cfl,
                 dt=cfl * h / c, ndims=2, phi=phi, E=E)
     return lf, meta
 

@@ -108,7 +108,10 @@ enum {
     GC_UPD_TAIT_EOS = 2,      /* TaitEOSUpdater :108; [0] rho0 [1] gamma    */
     GC_UPD_LINEAR_EOS = 3,    /* LinearEOSUpdater :131; [0] rho0            */
     GC_UPD_ELASTOPLASTIC = 4, /* ElastoPlasticStressUpdater :202; [0] E [1] nu [2] phi [3] psi [4] cohesion */
-    GC_UPD_HOOKE = 5          /* HookeLawStressUpdater :356; [0] E [1] nu   */
+    GC_UPD_HOOKE = 5,         /* HookeLawStressUpdater :356; [0] E [1] nu   */
+    GC_UPD_VISCOPLASTIC_MC = 6 /* ViscoPlasticMCStressUpdater :144-186, the stress part; its
+                                  EOS is the chain entry before it. [0] friction angle
+                                  (radians) [1] cohesion; NS = 3, 4 or 6    */
 };
 #define GC_UPD_NPARAM 6
 /* At most this many updaters may be chained in one stage (a Julia tuple of

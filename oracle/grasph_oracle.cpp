@@ -1175,6 +1175,29 @@ void apply_updater(Sys& ps, const Upd& u, double dt) {
         case GC_UPD_HOOKE:
             for (int64_t i = 0; i < n; ++i) hooke_update(ps, i, u, dt);
             break;
+        case GC_UPD_VISCOPLASTIC_MC: {
+            // src/StateUpdaters.jl:155-186 (after the EOS entry before it)
+            const double tphi = std::tan(u.prm[0]), coh = u.prm[1];
+            const int ns = ps.ns, nn = ns == 3 ? 2 : 3;
+            for (int64_t i = 0; i < n; ++i) {
+                const double* sr = &ps.sr[i * ns];
+                double m;
+                if (ns == 3) m = sr[0] * sr[0] + sr[1] * sr[1] + 2.0 * (sr[2] * sr[2]);
+                else if (ns == 4) m = sr[0] * sr[0] + sr[1] * sr[1] + 2.0 * (sr[3] * sr[3]);
+                else
+                    m = sr[0] * sr[0] + sr[1] * sr[1] + sr[2] * sr[2] +
+                        2.0 * (sr[3] * sr[3] + sr[4] * sr[4] + sr[5] * sr[5]);
+                m = jmax(std::sqrt(m), 2.220446049250313e-16);  // eps(Float64)
+                const double p = ps.p[i];
+                const double sc = 2.0 * (coh + p * tphi);
+                double st[6];
+                for (int q = 0; q < ns; ++q) st[q] = (sc * sr[q]) / m - (q < nn ? p : 0.0);
+                double tr = st[0];
+                for (int q = 1; q < nn; ++q) tr = tr + st[q];
+                for (int q = 0; q < ns; ++q) ps.stress[i * ns + q] = tr > 0.0 ? 0.0 : st[q];
+            }
+            break;
+        }
         default:
             break;
     }
@@ -1663,6 +1686,8 @@ int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_
                 return fail(ctx, GC_ERR_ARG, "ElastoPlasticStressUpdater requires NS=4 (plane-strain Voigt)");
             if ((u.kind == GC_UPD_TAIT_EOS || u.kind == GC_UPD_LINEAR_EOS) && !s.has_p())
                 return fail(ctx, GC_ERR_ARG, "EOS updater needs a pressure field");
+            if (u.kind == GC_UPD_VISCOPLASTIC_MC && (!s.has_stress() || (s.ns != 3 && s.ns != 4 && s.ns != 6)))
+                return fail(ctx, GC_ERR_ARG, "ViscoPlasticMCStressUpdater needs stress with NS = 3, 4 or 6");
             chain.push_back(u);
         }
         s.upd.push_back(chain);

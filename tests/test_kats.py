@@ -611,3 +611,31 @@ def test_integrator_regenerates_ghosts_and_mirrors_stress(be):
     for k in range(g.n):
         assert np.array_equal(g.stress[k], ps.stress[g.idx_original[k] - 1])
     assert np.any(ps.strain_rate != 0.0)
+
+
+# ------------------------------------------------ visco-plastic Mohr–Coulomb
+# src/StateUpdaters.jl:144-186.  No reference test pins it; the expected
+# values restate its formula for two strain-rate states: inside the yield
+# cone (stress along the strain rate, minus p) and past the apex (zero).
+
+@pytest.mark.parametrize("be", BACKENDS)
+def test_viscoplastic_mc_updater(be):
+    rho0, phi, coh = 1850.0, 0.35, 50.0
+    ps = G.StressParticleSystem("s", 2, 2, 3, 1.0, 20.0, state_updater=(
+        G.ViscoPlasticMCStressUpdater(G.LinearEOSUpdater(rho0), phi, coh),))
+    ps.x[:] = [[0.0, 0.0], [1.0, 1.0]]
+    ps.rho[:] = [1851.0, 1849.0]
+    ps.strain_rate[:] = [[-0.3, 0.1, 0.05], [0.2, 0.3, -0.1]]
+    lf, s = session(be, [ps], [G.SystemInteraction(kernel(), None, ps)])
+    s.update_state(ps, 1, 1e-4)
+    s.pull()
+    for i in range(2):
+        p = 20.0 * 20.0 * (ps.rho[i] - rho0)
+        sr = ps.strain_rate[i]
+        m = max(math.sqrt(sr[0] * sr[0] + sr[1] * sr[1] + 2.0 * (sr[2] * sr[2])), 2.220446049250313e-16)
+        sc = 2.0 * (coh + p * math.tan(phi))
+        st = [(sc * sr[q]) / m - (p if q < 2 else 0.0) for q in range(3)]
+        if st[0] + st[1] > 0.0:
+            st = [0.0, 0.0, 0.0]
+        assert ps.p[i] == p
+        assert list(ps.stress[i]) == st
