@@ -54,7 +54,7 @@ struct HGhost {
     int src = 0;
     double cutoff = 0;
     int nplanes = 0;
-    double normals[4][3] = {}, points[4][3] = {};
+    double normals[GC_MAX_GHOST_PLANES][3] = {}, points[GC_MAX_GHOST_PLANES][3] = {};
     std::vector<std::vector<std::pair<int, int>>> copiers;
     bool ex_p = false, ex_stress = false;
 };
@@ -145,9 +145,11 @@ struct DGhost {
 
 struct DInter {
     int a = 0, btype = BT_SELF, bslot = -1, bghost = -1, kk = 0, nstages = 0;
-    bool two_sided = false;
+    bool two_sided = false;  // some stage writes system_b too (a second, system_b-side sweep)
+    bool two_fluid = false;  // FluidPfn stages are the two-sided fluid x fluid form
     std::vector<int> pk;
     GridInst* d_gi = nullptr;
+    GridInst* d_gi_b = nullptr;  // system_b side: system_a's mass and sound speed as the neighbour's
     std::vector<GridInst> h_gi;
     std::vector<PfnInst*> d_pi;
     int32_t* cs = nullptr;     // CSR over system_b
@@ -369,6 +371,13 @@ double kernel_norm(int kind, int nd, double H) {
     return 21.0 / ((256.0 * pi) * (H * H * H));
 }
 
+// Does stage `stage` (1-based) of an interaction also write system_b?
+bool b_side_at(const DInter& D, int stage) {
+    const int pk = D.pk[stage - 1];
+    if (pk == GC_PFN_COUNT) return D.btype != BT_SELF && D.btype != BT_GHOST && D.bslot >= 0;
+    return pk == GC_PFN_FLUID && D.two_fluid;
+}
+
 // Functor/system_b combinations implemented (the CPU oracle refuses the same).
 int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     const HSys& a = I.sys[it.a];
@@ -394,11 +403,8 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
         return GC_OK;
     }
     const HSys& b = I.sys[h.idx];
-    if (pk == GC_PFN_FLUID) {
-        if (a.kind == GC_SYS_FLUID && b.kind == GC_SYS_FLUID)
-            return seterr(ctx, GC_ERR_UNSUPPORTED, "two-sided Fluid×Fluid functor not implemented");
+    if (pk == GC_PFN_FLUID)  // two-sided between two fluid systems, one-sided otherwise
         return b.kind >= GC_SYS_FLUID ? GC_OK : seterr(ctx, GC_ERR_ARG, "system_b has no pressure field");
-    }
     if (pk == GC_PFN_CAUCHY_FLUID) return seterr(ctx, GC_ERR_UNSUPPORTED, "two-sided CauchyFluidPfn not implemented");
     return GC_OK;
 }
@@ -674,8 +680,10 @@ int finalize(gc_ctx* ctx) {
                 D.bslot = hh.idx;
             }
         }
+        D.two_fluid = D.btype == BT_SYSTEM && I0.sys[h0.a].kind == GC_SYS_FLUID &&
+                      I0.sys[D.bslot].kind == GC_SYS_FLUID;
         for (int s = 0; s < D.nstages; ++s)
-            if (D.pk[s] == GC_PFN_COUNT && D.btype != BT_SELF && D.btype != BT_GHOST) D.two_sided = true;
+            if (b_side_at(D, s + 1)) D.two_sided = true;
         D.h_gi.resize(ninst);
         for (int k = 0; k < ninst; ++k) {
             const HInst& I = ctx->inst[k];
@@ -713,6 +721,19 @@ int finalize(gc_ctx* ctx) {
         }
         TRY(dalloc(ctx, &D.d_gi, (size_t)ninst));
         CU(cudaMemcpyAsync(D.d_gi, D.h_gi.data(), ninst * sizeof(GridInst), cudaMemcpyHostToDevice, ctx->stream));
+        if (D.two_sided) {
+            std::vector<GridInst> gb = D.h_gi;
+            for (int k = 0; k < ninst; ++k) {
+                const HSys& sa = ctx->inst[k].sys[ctx->inst[k].inters[i].a];
+                gb[k].bmass = sa.mass;
+                gb[k].bc = sa.c;
+                gb[k].f_bmass = (float)sa.mass;
+                gb[k].f_bc = (float)sa.c;
+            }
+            TRY(dalloc(ctx, &D.d_gi_b, (size_t)ninst));
+            CU(cudaMemcpyAsync(D.d_gi_b, gb.data(), ninst * sizeof(GridInst), cudaMemcpyHostToDevice, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+        }
         D.d_pi.resize(D.nstages, nullptr);
         for (int s = 0; s < D.nstages; ++s) {
             std::vector<PfnInst> per(ninst);
@@ -729,6 +750,10 @@ int finalize(gc_ctx* ctx) {
                 per[k].f_h = (float)p[2];
                 per[k].f_h2eps = (float)(p[2] * p[2] * 0.01);
                 per[k].f_delta = (float)per[k].delta;
+                per[k].has_eps = std::isnan(p[5]) ? 0 : 1;
+                per[k].eps = per[k].has_eps ? p[5] : 0.0;
+                per[k].f_eps = (float)per[k].eps;
+                per[k].two = D.two_fluid && D.pk[s] == GC_PFN_FLUID;
             }
             TRY(dalloc(ctx, &D.d_pi[s], (size_t)ninst));
             CU(cudaMemcpyAsync(D.d_pi[s], per.data(), ninst * sizeof(PfnInst), cudaMemcpyHostToDevice, ctx->stream));
@@ -922,6 +947,7 @@ int read_need(gc_ctx* ctx) {
 GridPlanArgs grid_plan_args(gc_ctx* ctx, DInter& D) {
     GridPlanArgs g{};
     g.gi = D.d_gi;
+    g.gi_b = D.d_gi_b;
     g.ninst = ninst(ctx);
     g.nd = ctx->slots[D.a].nd;
     g.a = ctx->slots[D.a].d_inst;
@@ -1384,10 +1410,13 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     if (e1)
         CU(cudaEventRecordWithFlags(e1, ctx->stream, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     TRY(check_launch(ctx, "sweep"));
-    // b side of two-sided (counting) coupled interactions
+    // system_b side of two-sided interactions (counting functor; FluidPfn
+    // between two fluid systems): a gather over system_b's particles through
+    // system_a's CSR on the same grid, the functor's terms with the roles
+    // swapped
     for (int id : ids) {
         DInter& D = ctx->inters[id];
-        if (!D.two_sided || count_only) continue;
+        if (count_only || !b_side_at(D, stage)) continue;
         DSlot& B = ctx->slots[D.bslot];
         TRY(ensure_groups(ctx, D.bslot, id, true));
         ForceArgs R = A;
@@ -1401,15 +1430,22 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         R.av = B.F(F_V);
         R.arho = B.F(F_RHO);
         R.aaux = B.aux;
+        R.astress = B.F(F_STRESS);
+        R.a_p = B.F(F_P);
         R.advdt = B.F(F_DVDT);
         R.adrhodt = B.F(F_DRHODT);
+        R.asr = B.F(F_SR);
+        R.avort = B.F(F_VORT);
         R.a_c = B.d_c;
         R.a_mass = B.d_mass;
+        R.a_cf = B.d_cf;
+        R.a_massf = B.d_massf;
+        R.afp = fp32 ? pk_of(B.fpk, B.N, B.nd) : nullptr;
         R.nref = 1;
         InterRef& r = R.ref[0];
         r.btype = BT_SYSTEM;
         r.bbox = S.d_inst;
-        r.gi = D.d_gi;
+        r.gi = D.d_gi_b;
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs_a;
         r.cs_cells = D.cells;
@@ -1421,9 +1457,8 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         r.bstress = S.F(F_STRESS);
         r.baux = S.aux;
         r.bN = S.N;
-        r.bfp = nullptr;
-        r.bxp = nullptr;
-        R.afp = nullptr;
+        r.bfp = fp32 ? pk_of(S.fpk, S.N, S.nd) : nullptr;
+        r.bxp = fp32 ? xp_of(S.fpk) : nullptr;
         st = launch_force_f64(R, false, ctx->stream);
         if (st) return seterr(ctx, st, "two-sided functor not implemented on the device");
         TRY(check_launch(ctx, "sweep (system_b side)"));
@@ -2020,6 +2055,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
     }
     for (auto& D : ctx->inters) {
         cudaFree(D.d_gi);
+        cudaFree(D.d_gi_b);
         for (auto* p : D.d_pi) cudaFree(p);
         cudaFree(D.cs);
         cudaFree(D.cs_a);
@@ -2147,7 +2183,8 @@ int gc_add_ghost(gc_ctx* ctx, int inst, int src_sys, int ncopiers, const int* co
     int si = sys_of(ctx, inst, src_sys);
     if (si < 0) return seterr(ctx, GC_ERR_ARG, "ghost source must be a system handle");
     if (nplanes < 1) return seterr(ctx, GC_ERR_ARG, "at least one boundary (normal, point) pair is required");
-    if (nplanes > 4) return seterr(ctx, GC_ERR_UNSUPPORTED, "at most 4 planes per ghost entry");
+    if (nplanes > GC_MAX_GHOST_PLANES)
+        return seterr(ctx, GC_ERR_UNSUPPORTED, "at most %d planes per ghost entry", GC_MAX_GHOST_PLANES);
     HInst& I = ctx->inst[inst];
     const HSys& s = I.sys[si];
     HGhost g;

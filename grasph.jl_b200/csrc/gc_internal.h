@@ -57,14 +57,15 @@ struct GridInst {
 
 // Per (interaction, stage, instance) functor parameters.
 struct PfnInst {
-    double alpha, beta, h, delta;
-    int S, has_delta;
-    float f_alpha, f_beta, f_h, f_h2eps, f_delta;  // FP32 copies; h2eps = 0.01·h²
+    double alpha, beta, h, delta, eps;
+    int S, has_delta, has_eps;
+    int two;  // FluidPfn between two fluid systems (both sides written)
+    float f_alpha, f_beta, f_h, f_h2eps, f_delta, f_eps;  // FP32 copies; h2eps = 0.01·h²
 };
 
 // Per (ghost entry, instance) parameters.
 struct GhostInst {
-    double normals[4][MAXD], points[4][MAXD];  // up to 4 planes
+    double normals[GC_MAX_GHOST_PLANES][MAXD], points[GC_MAX_GHOST_PLANES][MAXD];
     double cutoff;
     int64_t src_base, src_n;   // source particles in the source slot
     int64_t cap_base, cap;     // capacity range in the packed ghost arrays

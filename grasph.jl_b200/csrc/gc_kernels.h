@@ -62,6 +62,7 @@ void launch_gather_fields(const GatherArgs& a, int64_t N, const int32_t* perm, c
 // ------------------------------------------------------------------ grid
 struct GridPlanArgs {
     GridInst* gi;
+    GridInst* gi_b;        // system_b-side copy (two-sided interactions): geometry mirrored, or nullptr
     int ninst, nd;
     const SysInst* a;      // system_a per-instance bbox
     const SysInst* b;      // system_b per-instance bbox (nullptr for self)

@@ -633,6 +633,20 @@ __device__ void grid_plan_block(const GridPlanArgs& a) {
         }
         *a.need = base;
     }
+    if (a.gi_b) {
+        // the system_b-side copy keeps its own neighbour mass and sound speed
+        __syncthreads();
+        for (int k = threadIdx.x; k < a.ninst; k += blockDim.x) {
+            GridInst& B = a.gi_b[k];
+            const double bm = B.bmass, bc = B.bc;
+            const float fbm = B.f_bmass, fbc = B.f_bc;
+            B = a.gi[k];
+            B.bmass = bm;
+            B.bc = bc;
+            B.f_bmass = fbm;
+            B.f_bc = fbc;
+        }
+    }
 }
 
 void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s) {

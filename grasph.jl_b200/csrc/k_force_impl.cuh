@@ -206,17 +206,30 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         double dv[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) dv[d] = o.v[d] - vj[d];
-        double piv = art_visc<ND>(dx, dv, rr, P.h, o.rho, rhoj, P.alpha, P.beta, ca, ca);
+        // two-sided fluid x fluid :173 uses both sound speeds, one-sided :193 its own twice
+        const double cb = P.two ? G.bc : ca;
+        double piv = art_visc<ND>(dx, dv, rr, P.h, o.rho, rhoj, P.alpha, P.beta, ca, cb);
         double auxj = r.baux[j];
         double dh = P.S == 1 ? -(A.a_p[gi] + r.bp[j]) / (o.rho * rhoj) : -(o.aux + auxj);
         double mj = r.btype == BT_SELF ? mass_a : G.bmass;
-        double s = mj * (dh - piv);
+        if (P.two) {
+            // dv_tmp = (dh + ast - piv)·gx, then mass_j·dv_tmp; the system_b side
+            // runs this same code with the roles swapped (every factor is
+            // symmetric or flips sign exactly with dx, dv and gx)
+            double c = dh;
+            if (P.has_eps) c = c + P.eps * (-(fabs(A.a_p[gi]) + fabs(r.bp[j])) / (o.rho * rhoj));
+            c = c - piv;
 #pragma unroll
-        for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + s * gx[d];
+            for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + mj * (c * gx[d]);
+        } else {
+            double s = mj * (dh - piv);
+#pragma unroll
+            for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + s * gx[d];
+        }
         double dr = dotv<ND>(dv, gx);
         double tail;
         if (P.has_delta) {
-            double psi = diffusion<ND>(dx, rr, o.rho, rhoj, ca, ca, P.h, P.h, gx, P.delta);
+            double psi = diffusion<ND>(dx, rr, o.rho, rhoj, ca, cb, P.h, P.h, gx, P.delta);
             tail = psi / rhoj;
         } else {
             tail = zero_over(rhoj);
@@ -616,7 +629,8 @@ struct PhysF32 {
 #pragma unroll
         for (int d = 0; d < ND; ++d) dv[d] = w.v[d] - vj[d];
         const bool self = r.btype == BT_SELF, dyn = r.btype == BT_DYNAMIC;
-        const float cb = (P2 == GC_PFN_CAUCHY_FLUID && r.btype == BT_GHOST) ? G.f_bc : ca;
+        const bool two = P2 == GC_PFN_FLUID && P.two;
+        const float cb = ((P2 == GC_PFN_CAUCHY_FLUID && r.btype == BT_GHOST) || two) ? G.f_bc : ca;
         float piv = 0.f;
         const float vr = dotf<ND>(dxf, dv);
         if (vr < 0.f) {
@@ -635,7 +649,10 @@ struct PhysF32 {
         }
         const float mj = (self || dyn) ? ma : G.f_bmass;
         if (P2 == GC_PFN_FLUID) {
-            const float dh = -(w.aux + auxj);
+            float dh = -(w.aux + auxj);
+            // artificial surface tension ε·(−(|p_i| + |p_j|)/(ρ_i ρ_j)), with
+            // |p| = |p/ρ²|·ρ² from the record
+            if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
             const float s = mj * (dh - piv);
 #pragma unroll
             for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], s * gx[d]);
@@ -663,7 +680,8 @@ struct PhysF32 {
         }
         float tail = 0.f;
         if (P.has_delta) {
-            const float psi = 2.f * P.f_delta * ca * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
+            const float cd = two ? 0.5f * (ca + cb) : ca;
+            const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
             tail = psi * irhoj;
         }
         kadd(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail));

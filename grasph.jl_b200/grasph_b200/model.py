@@ -352,17 +352,17 @@ class FluidPfn(_Pfn):
         self.sigma = int(sigma)
         if self.sigma not in (1, 2):
             raise ArgumentError("FluidPfn sigma must be 1 or 2 on the device path")
-        if epsilon is not None:
-            raise ArgumentError("surface tension (epsilon) belongs to the two-sided multiphase "
-                                "functor, which the device library does not implement")
         self.delta = None if delta is None else float(delta)
-        self.epsilon = None
+        # artificial surface tension: used by the two-sided fluid x fluid form only
+        self.epsilon = None if epsilon is None else float(epsilon)
 
     def params(self):
         p = super().params()
         p[0], p[1], p[2], p[3] = self.art_visc_alpha, self.art_visc_beta, self.h, self.sigma
         if self.delta is not None:
             p[4] = self.delta
+        if self.epsilon is not None:
+            p[5] = self.epsilon
         return p
 
 
@@ -455,7 +455,7 @@ class TaitEOSUpdater(_Updater):
 
     kind = C.GC_UPD_TAIT_EOS
 
-    def __init__(self, rho0, *, gamma=7.0):
+    def __init__(self, rho0, gamma=7.0):
         self.rho0 = float(rho0)
         self.gamma = float(gamma)
 

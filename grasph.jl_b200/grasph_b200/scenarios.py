@@ -21,8 +21,8 @@ import numpy as np
 from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, DynamicBoundarySystem,
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
                     GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator, LinearEOSUpdater,
-                    StrainRatePfn, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
-                    TaitEOSUpdater, ViscoPlasticMCStressUpdater, ZeroFieldUpdater)
+                    RK4TimeIntegrator, StrainRatePfn, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
+                    TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, ZeroFieldUpdater)
 
 G = 9.81
 
@@ -227,6 +227,70 @@ def granular_column(nfx=100, nfy=50, dx=0.002, rho0=1850.0, E=0.84e6, nu=0.3, ph
     lf = LeapFrogTimeIntegrator([fluid, bottom], inters, ghosts=(gentry,))
     meta = dict(workload="granular_column", n_fluid=fluid.n, n_boundary=bottom.n, h=h, c0=c, cfl=cfl,
                 dt=cfl * h / c, ndims=2, phi=phi, E=E)
+    return lf, meta
+
+
+# ------------------------------------------------------- multiphase bubble
+
+BUBBLE_VARIANTS = {
+    # rho_Y, c_Y / sqrt(g R), gamma_Y, sigma, epsilon (X-Y), dx
+    "bubble": (500.0, 40.0, 7.0, 2, None, 0.05),
+    "bubble2": (10.0, math.sqrt(16000.0), 1.4, 1, None, 0.04),
+    "bubble3": (1.0, 400.0, 1.4, 1, 0.1, 0.04),
+}
+
+
+def bubble(variant="bubble", R=1.0, dx=None, rho_x=1000.0, alpha=0.01, beta=0.0, hfac=1.2, cfl=1.5,
+           integrator="rk4"):
+    """2-D light-fluid bubble rising in a heavy fluid (bubble.jl /
+    bubble2.jl / bubble3.jl layout, without XSPH): a 6R x 10R column of
+    fluid X with a disc of radius R of fluid Y centred at the origin, both
+    Tait fluids with hydrostatic initial density and zero initial pressure,
+    Wendland C2 kernel, FluidPfn self interactions, the two-sided X-Y
+    FluidPfn with Y first, a one-stage ghost of X with its pressure copied,
+    mirrored across the four walls and the four diagonal corner planes."""
+    rho_y, cy_fac, gamma_y, sigma, eps, dx0 = BUBBLE_VARIANTS[variant]
+    dx = dx0 if dx is None else dx
+    height, width = 10.0 * R, 6.0 * R
+    y_min, x_min = -2.0 * R, -3.0 * R
+    y_max, x_max = y_min + height, x_min + width
+    h = hfac * dx
+    c_x = math.sqrt(800.0 * G * R)
+    c_y = cy_fac * math.sqrt(G * R)
+    nx, ny = int(math.floor(width / dx)), int(math.floor(height / dx))
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    px = x_min + (ii.ravel() + 0.5) * dx
+    py = y_min + (jj.ravel() + 0.5) * dx
+    inside = px * px + py * py < R * R
+    systems = []
+    for name, sel, rho0, c, gamma in (("fluid X", ~inside, rho_x, c_x, 7.0),
+                                       ("fluid Y", inside, rho_y, c_y, gamma_y)):
+        n = int(sel.sum())
+        ps = FluidParticleSystem(name, n, 2, dx * dx * rho0, c, source_v=[0.0, -G],
+                                 state_updater=TaitEOSUpdater(rho0, gamma))
+        ps.x[:, 0] = px[sel]
+        ps.x[:, 1] = py[sel]
+        pressure = (y_min + height - ps.x[:, 1]) * rho_x * G
+        ps.rho[:] = (pressure * gamma / (c * c * rho0) + 1.0) ** (1.0 / gamma) * rho0
+        systems.append(ps)
+    fx, fy = systems
+    ghost = GhostParticleSystem(fx, GhostCopier("p"), name="ghost[fluid_X]")
+    s2 = 1.0 / math.sqrt(2.0)
+    gentry = GhostEntry(ghost, 3.0 * h,
+                        ((1.0, 0.0), (x_min, 0.0)), ((-1.0, 0.0), (x_max, 0.0)),
+                        ((0.0, 1.0), (0.0, y_min)), ((0.0, -1.0), (0.0, y_max)),
+                        ((s2, s2), (x_min, y_min)), ((-s2, s2), (x_max, y_min)),
+                        ((s2, -s2), (x_min, y_max)), ((-s2, -s2), (x_max, y_max)))
+    kernel = WenlandC2Kernel(h, ndims=2)
+    pfn = FluidPfn(alpha, beta, h, sigma=sigma)
+    inters = [SystemInteraction(kernel, pfn, fx),
+              SystemInteraction(kernel, pfn, fy),
+              SystemInteraction(kernel, FluidPfn(alpha, beta, h, sigma=sigma, epsilon=eps), fy, fx),
+              SystemInteraction(kernel, pfn, fx, ghost)]
+    cls = RK4TimeIntegrator if integrator == "rk4" else LeapFrogTimeIntegrator
+    lf = cls([fx, fy], inters, ghosts=(gentry,))
+    meta = dict(workload=variant, n_fluid=fx.n + fy.n, n_x=fx.n, n_y=fy.n, h=h, c0=max(c_x, c_y), cfl=cfl,
+                ndims=2)
     return lf, meta
 
 

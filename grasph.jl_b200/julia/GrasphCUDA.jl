@@ -51,7 +51,10 @@ function pfn_params(f)
         p[1] = f.art_visc_alpha; p[2] = f.art_visc_beta; p[3] = f.h
         f.delta === nothing || (p[5] = f.delta)
     end
-    f isa FluidPfn && (p[4] = typeof(f).parameters[1])
+    if f isa FluidPfn
+        p[4] = typeof(f).parameters[1]
+        f.epsilon === nothing || (p[6] = f.epsilon)
+    end
     return p
 end
 

@@ -181,7 +181,10 @@ int gc_add_boundary(gc_ctx* ctx, int inst, int sys, int kind, const double* norm
  * Copier k (stage k+1) lists copier_nfields[k] (field, mode) entries, taken
  * consecutively from copier_fields/copier_modes; 0 entries = `nothing`.
  * `normals`/`points` hold nplanes×ndims doubles.  `capacity` bounds the ghost
- * count (0 = the source's particle count × nplanes).                        */
+ * count (0 = the source's particle count × nplanes).  At most
+ * GC_MAX_GHOST_PLANES planes per entry (a 3-D box with its 6 faces, 12
+ * edges and 8 corners takes 26).                                          */
+#define GC_MAX_GHOST_PLANES 32
 int gc_add_ghost(gc_ctx* ctx, int inst, int src_sys, int ncopiers,
                  const int* copier_nfields, const int* copier_fields, const int* copier_modes,
                  int nplanes, const double* normals, const double* points, double cutoff,

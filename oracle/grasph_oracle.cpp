@@ -366,6 +366,8 @@ struct Pfn {
     int S;
     double delta;
     bool has_delta;
+    double eps;  // artificial surface tension (two-sided FluidPfn only)
+    bool has_eps;
 };
 
 Pfn make_pfn(int kind, const double* prm) {
@@ -377,6 +379,8 @@ Pfn make_pfn(int kind, const double* prm) {
     f.S = (int)prm[3];
     f.delta = prm[4];
     f.has_delta = !std::isnan(prm[4]);
+    f.eps = prm[5];
+    f.has_eps = !std::isnan(prm[5]);
     return f;
 }
 
@@ -540,6 +544,29 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
         double rf = lennard_jones<ND>(dx, b.ljcut, a.c);
         double s = (-b.mass) * piv;
         for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + (s * gx[d] + rf * dx[d]);
+        return;
+    }
+    if (f.kind == GC_PFN_FLUID && b.type == H_SYS && a.kind == GC_SYS_FLUID && b.sys->kind == GC_SYS_FLUID) {
+        // two-sided fluid x fluid (multiphase) :173-190: both systems' rates,
+        // each side weighted by the other side's mass, mean sound speed
+        Sys& bs = *b.sys;
+        double pi_ = a.p[i], pj = b.p[j];
+        double dv[ND];
+        for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+        double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, bs.c);
+        double dh = pressure_coeff(pi_, pj, ri, rj, f.S);
+        // artificial_surface_tension_coeff src/PairwisePhysics.jl:286-290
+        double ast = f.has_eps ? f.eps * pressure_coeff(std::fabs(pi_), std::fabs(pj), ri, rj, 1) : 0.0;
+        double c = dh + ast - piv;
+        for (int d = 0; d < ND; ++d) {
+            double t = c * gx[d];
+            a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + b.mass * t;
+            bs.dvdt[j * ND + d] = bs.dvdt[j * ND + d] - a.mass * t;
+        }
+        double dr = dot<ND>(dv, gx);
+        double psi = diffusion<ND>(dx, ri, rj, a.c, bs.c, f.h, f.h, gx, f.delta, f.has_delta);
+        a.drhodt[i] = a.drhodt[i] + b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
+        bs.drhodt[j] = bs.drhodt[j] + a.mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri);
         return;
     }
     switch (f.kind) {
@@ -1272,10 +1299,10 @@ int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
         if (pk == GC_PFN_CAUCHY_FLUID && !g.ex_stress) return GC_ERR_UNSUPPORTED;
         return GC_OK;
     }
-    // plain real system_b: one-sided generic functors only
+    // plain real system_b: FluidPfn is two-sided between two fluid systems,
+    // one-sided otherwise
     const Sys& b = ctx->sys[h.idx];
     if (pk == GC_PFN_FLUID) {
-        if (a.kind == GC_SYS_FLUID && b.kind == GC_SYS_FLUID) return GC_ERR_UNSUPPORTED;  // two-sided multiphase
         return b.has_p() ? GC_OK : GC_ERR_ARG;
     }
     if (pk == GC_PFN_CAUCHY_FLUID) return GC_ERR_UNSUPPORTED;  // two-sided real-real

@@ -1,0 +1,181 @@
+"""Two-sided FluidPfn between two fluid systems (multiphase) and the
+bubble scenarios (bubble.jl, bubble2.jl, bubble3.jl without XSPH).
+
+The reference has no tests for this functor.  The known answers restate
+src/PairwiseFunctors.jl:173-190 with src/PairwisePhysics.jl:29-34 (artificial
+viscosity with both sound speeds), :58-64 (pressure coefficient, sigma 1 and
+2), :99-105 (continuity coefficient), :238-243 (density diffusion) and
+:286-288 (artificial surface tension) for one pair, and check both systems'
+rates.  The device path is then held to the oracle on the bubble layouts:
+eight ghost planes (walls and diagonal corners), RK4 and LeapFrog, sigma 1
+and 2, with and without surface tension.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import grasph_b200 as G
+from grasph_b200 import scenarios
+from gc_helpers import BACKENDS, make_backend, session
+
+
+def _pair_case(sigma, eps, delta):
+    h = 0.1
+    a = G.FluidParticleSystem("a", 1, 2, 2.5, 30.0)
+    b = G.FluidParticleSystem("b", 1, 2, 0.75, 45.0)
+    a.x[0], b.x[0] = [0.0, 0.0], [0.07, 0.04]
+    a.v[0], b.v[0] = [0.3, -0.1], [-0.2, 0.25]
+    a.rho[0], b.rho[0] = 1010.0, 480.0
+    a.p[0], b.p[0] = 1500.0, -200.0
+    pfn = G.FluidPfn(0.05, 0.02, h, sigma=sigma, delta=delta, epsilon=eps)
+    si = G.SystemInteraction(G.CubicSplineKernel(h, ndims=2), pfn, a, b)
+    return a, b, si, h
+
+
+def _expected(a, b, h, sigma, eps, delta, alpha=0.05, beta=0.02):
+    k = G.CubicSplineKernel(h, ndims=2)
+    dx = a.x[0] - b.x[0]
+    rr = dx[0] * dx[0] + dx[1] * dx[1]
+    r = math.sqrt(rr)
+    q = r / h
+    t2, t1 = max(0.0, 2 - q), max(0.0, 1 - q)
+    gx = k.norm_coeff * (-3.0 * (0.25 * t2 * t2 - t1 * t1)) / (r * h) * dx
+    dv = a.v[0] - b.v[0]
+    ri, rj, pi_, pj = a.rho[0], b.rho[0], a.p[0], b.p[0]
+    vr = min(dx[0] * dv[0] + dx[1] * dv[1], 0.0)
+    muv = h * vr / (rr + h * h * 0.01)
+    mc = 0.5 * (a.c + b.c)
+    piv = (beta * muv - alpha * mc) * muv / (0.5 * ri * rj)
+    if sigma == 1:
+        dh = -(pi_ + pj) / (ri * rj)
+    else:
+        dh = -(pi_ / (ri * ri) + pj / (rj * rj))
+    ast = 0.0 if eps is None else eps * (-(abs(pi_) + abs(pj)) / (ri * rj))
+    tmp = (dh + ast - piv) * gx
+    dr = dv[0] * gx[0] + dv[1] * gx[1]
+    psi = 0.0
+    if delta is not None:
+        psi = 2.0 * delta * (0.5 * (a.c + b.c)) * h * (ri - rj) * (dx[0] * gx[0] + dx[1] * gx[1]) / rr
+    ci, cj = (ri / rj, rj / ri) if sigma == 1 else (1.0, 1.0)
+    return (b.mass * tmp, -a.mass * tmp,
+            b.mass * (dr * ci + psi / rj), a.mass * (dr * cj - psi / ri))
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+@pytest.mark.parametrize("sigma,eps,delta", [(2, None, None), (1, None, None), (2, 0.1, 0.1), (1, 0.1, None)])
+def test_two_sided_fluid_pair(be, sigma, eps, delta):
+    a, b, si, h = _pair_case(sigma, eps, delta)
+    lf, s = session(be, [a, b], [si])
+    s.create_grid(si)
+    s.sweep(si, 1)
+    s.pull()
+    dva, dvb, dra, drb = _expected(a, b, h, sigma, eps, delta)
+    np.testing.assert_allclose(a.dvdt[0], dva, rtol=1e-12)
+    np.testing.assert_allclose(b.dvdt[0], dvb, rtol=1e-12)
+    assert math.isclose(a.drhodt[0], dra, rel_tol=1e-12)
+    assert math.isclose(b.drhodt[0], drb, rel_tol=1e-12)
+    # momentum exchanged between the phases sums to zero
+    np.testing.assert_allclose(a.mass * a.dvdt[0] + b.mass * b.dvdt[0], 0.0, atol=1e-12 * np.abs(a.mass * dva).max())
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+def test_fluid_against_stress_system_stays_one_sided(be):
+    h = 0.1
+    a = G.FluidParticleSystem("a", 1, 2, 2.5, 30.0)
+    b = G.StressParticleSystem("b", 1, 2, 3, 0.75, 45.0)
+    a.x[0], b.x[0] = [0.0, 0.0], [0.07, 0.04]
+    a.rho[0], b.rho[0] = 1000.0, 1000.0
+    a.p[0], b.p[0] = 10.0, 20.0
+    si = G.SystemInteraction(G.CubicSplineKernel(h, ndims=2), G.FluidPfn(0.05, 0.0, h), a, b)
+    lf, s = session(be, [a, b], [si])
+    s.create_grid(si)
+    s.sweep(si, 1)
+    s.pull()
+    assert np.any(a.dvdt[0] != 0.0)
+    assert np.all(b.dvdt[0] == 0.0) and b.drhodt[0] == 0.0
+
+
+@pytest.mark.parametrize("variant", list(scenarios.BUBBLE_VARIANTS))
+def test_bubble_layout(variant):
+    lf, meta = scenarios.bubble(variant, dx=0.2)
+    fx, fy = lf.systems
+    assert fx.n + fy.n == 30 * 50 and fy.n > 0
+    assert np.all(fy.x[:, 0] ** 2 + fy.x[:, 1] ** 2 < 1.0)
+    assert len(lf.ghosts[0].normals) == 8
+    # hydrostatic: density falls with height in each phase
+    for ps in (fx, fy):
+        order = np.argsort(ps.x[:, 1])
+        assert np.all(np.diff(ps.rho[order]) <= 1e-9)
+
+
+def _run(lf, be, nsteps, cfl, prec=None, graphs=None):
+    kw = {} if prec is None else dict(precision=prec)
+    s = G.Session([lf], backend=make_backend(be), **kw)
+    if graphs is not None:
+        s.backend.set_graphs(graphs, 16)
+    s.push()
+    s.step(nsteps, cfl)
+    s.pull()
+    return s
+
+
+def _cmp(lf_g, lf_c, tol, rate_tol=None):
+    for sg, sc in zip(lf_g.systems, lf_c.systems):
+        ig, ic = np.argsort(sg.id), np.argsort(sc.id)
+        for name, _ in sg.particle_fields():
+            if name in ("id", "v_adjustment"):
+                continue
+            t = rate_tol if (rate_tol is not None and name in ("dvdt", "drhodt")) else tol
+            a = np.asarray(getattr(sg, name), dtype=float)[ig]
+            b = np.asarray(getattr(sc, name), dtype=float)[ic]
+            scale = max(np.abs(b).max(), 1e-300)
+            err = np.abs(a - b).max() / scale
+            assert err <= t, f"{sg.name}.{name}: {err:.3e} > {t}"
+
+
+def test_bubble_oracle_runs_and_conserves_mass():
+    lf, meta = scenarios.bubble("bubble3", dx=0.2)
+    _run(lf, "oracle", 3, meta["cfl"])
+    for ps in lf.systems:
+        assert np.all(np.isfinite(ps.x)) and np.all(np.isfinite(ps.rho))
+    assert np.any(lf.systems[1].dvdt != 0.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", list(scenarios.BUBBLE_VARIANTS))
+@pytest.mark.parametrize("integ", ["rk4", "leapfrog"])
+@pytest.mark.parametrize("nsteps,tol", [(1, 1e-10), (20, 1e-8)])
+def test_bubble_parity_fp64(variant, integ, nsteps, tol):
+    # the scripts' Courant number 1.5 is an RK4 one; LeapFrog needs a smaller step
+    cfl = 1.5 if integ == "rk4" else 0.2
+    lf_g, _ = scenarios.bubble(variant, dx=0.1, integrator=integ, cfl=cfl)
+    lf_c, _ = scenarios.bubble(variant, dx=0.1, integrator=integ, cfl=cfl)
+    _run(lf_g, "cuda", nsteps, cfl)
+    _run(lf_c, "oracle", nsteps, cfl)
+    _cmp(lf_g, lf_c, tol)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["bubble", "bubble3"])
+def test_bubble_parity_fp32c(variant):
+    lf_g, meta = scenarios.bubble(variant, dx=0.1)
+    lf_c, _ = scenarios.bubble(variant, dx=0.1)
+    _run(lf_g, "cuda", 20, meta["cfl"], prec=G.PRECISION_FP32_COMPENSATED)
+    _run(lf_c, "oracle", 20, meta["cfl"])
+    _cmp(lf_g, lf_c, 1e-4, rate_tol=1e-3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [G.PRECISION_FP64, G.PRECISION_FP32_COMPENSATED])
+def test_bubble_graph_steps_bit_identical(prec):
+    out = []
+    for graphs in (False, True):
+        lf, meta = scenarios.bubble("bubble", dx=0.1)
+        st = _run(lf, "cuda", 40, meta["cfl"], prec=prec, graphs=graphs).stats()
+        out.append((lf, st))
+    (le, _), (lg, st) = out
+    assert st["graph_steps"] > 0
+    for se, sg in zip(le.systems, lg.systems):
+        for name, _ in se.particle_fields():
+            assert np.array_equal(getattr(se, name), getattr(sg, name)), f"{se.name}.{name}"
