@@ -63,6 +63,8 @@ struct HInter {
     double H = 0;
     std::vector<int> pk;
     std::vector<std::array<double, GC_PFN_NPARAM>> pp;
+    int vk = GC_PFN_NONE;  // velocity_adjust_pairwise_fn
+    double veps = 0.0;
 };
 struct HStaged {
     int handle, field;
@@ -81,7 +83,7 @@ struct HInst {
 };
 
 // ---------------------------------------------------------- device state
-enum { F_X = 0, F_V, F_RHO, F_DVDT, F_DRHODT, F_P, F_STRESS, F_SR, F_VORT, F_STRAIN, F_STRAINP, NF };
+enum { F_X = 0, F_V, F_RHO, F_DVDT, F_DRHODT, F_P, F_STRESS, F_SR, F_VORT, F_STRAIN, F_STRAINP, F_VADJ, NF };
 
 struct DSlot {
     int64_t N = 0;
@@ -123,6 +125,14 @@ struct DSlot {
 struct DGhost {
     int src = 0, nplanes = 0, nd = 2, ns = 0;
     int64_t CAP = 0;
+    // warp groups of the ghosts (system_b side of an XSPH sweep) and that
+    // sweep's ghost-indexed sums before they are added to the source
+    int2* groups = nullptr;
+    int64_t* d_ngroups = nullptr;
+    int32_t *gcnt = nullptr, *goff = nullptr;
+    int64_t cap_gcols = 0;
+    int64_t groups_key = -1, groups_ver = -1;
+    double* gadj = nullptr;
     double* x[2] = {};
     int32_t *io[2] = {}, *ib[2] = {}, *ginst[2] = {};
     int cur = 0;
@@ -147,6 +157,7 @@ struct DInter {
     int a = 0, btype = BT_SELF, bslot = -1, bghost = -1, kk = 0, nstages = 0;
     bool two_sided = false;  // some stage writes system_b too (a second, system_b-side sweep)
     bool two_fluid = false;  // FluidPfn stages are the two-sided fluid x fluid form
+    bool vadj = false;       // pk[nstages] is the velocity-adjust functor (XSPH)
     std::vector<int> pk;
     GridInst* d_gi = nullptr;
     GridInst* d_gi_b = nullptr;  // system_b side: system_a's mass and sound speed as the neighbour's
@@ -198,6 +209,7 @@ struct gc_ctx {
     std::vector<DGhost> ghosts;
     std::vector<DInter> inters;
     int nstages = 0;
+    bool xsph = false;  // some interaction has a velocity-adjust functor: v_adjustment is carried
     // scratch
     int32_t *key = nullptr, *perm = nullptr, *hist = nullptr, *start = nullptr, *fill = nullptr, *scan_tmp = nullptr;
     int64_t cap_keyN = 0, cap_cells = 0, cap_scan = 0;
@@ -356,6 +368,7 @@ int field_slot(int field) {
         case GC_FIELD_VORTICITY: return F_VORT;
         case GC_FIELD_STRAIN: return F_STRAIN;
         case GC_FIELD_STRAIN_P: return F_STRAINP;
+        case GC_FIELD_V_ADJUSTMENT: return F_VADJ;
         default: return -1;
     }
 }
@@ -371,10 +384,13 @@ double kernel_norm(int kind, int nd, double H) {
     return 21.0 / ((256.0 * pi) * (H * H * H));
 }
 
-// Does stage `stage` (1-based) of an interaction also write system_b?
+// Does stage `stage` (1-based; nstages + 1 is the velocity-adjust functor)
+// of an interaction also write system_b?  XSPHPfn's coupled form writes every
+// system_b kind: a wrapper's system, or a ghost's source at the ghost index.
 bool b_side_at(const DInter& D, int stage) {
     const int pk = D.pk[stage - 1];
     if (pk == GC_PFN_COUNT) return D.btype != BT_SELF && D.btype != BT_GHOST && D.bslot >= 0;
+    if (pk == GC_PFN_XSPH) return D.btype != BT_SELF;
     return pk == GC_PFN_FLUID && D.two_fluid;
 }
 
@@ -382,6 +398,9 @@ bool b_side_at(const DInter& D, int stage) {
 int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     const HSys& a = I.sys[it.a];
     if (pk == GC_PFN_NONE) return GC_OK;
+    if (pk == GC_PFN_XSPH)
+        return seterr(ctx, GC_ERR_UNSUPPORTED, "XSPHPfn is swept as velocity_adjust_pairwise_fn, not as a stage");
+    if (pk < 0 || pk > GC_PFN_COUNT) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
     if (pk == GC_PFN_FLUID && a.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "FluidPfn needs a pressure field");
     if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE) && a.kind < GC_SYS_STRESS)
         return seterr(ctx, GC_ERR_ARG, "functor needs a stress system");
@@ -435,7 +454,7 @@ bool same_structure(const HInst& a, const HInst& b, std::string& why) {
     if (a.inters.size() != b.inters.size()) return why = "interactions", false;
     for (size_t i = 0; i < a.inters.size(); ++i) {
         const HInter &x = a.inters[i], &y = b.inters[i];
-        if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk)
+        if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk || x.vk != y.vk)
             return why = "interactions", false;
         for (int s = 0; s < x.nstages; ++s)
             if (x.pp[s][3] != y.pp[s][3] || std::isnan(x.pp[s][4]) != std::isnan(y.pp[s][4]))
@@ -483,6 +502,8 @@ int finalize(gc_ctx* ctx) {
     }
     CU(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
     ctx->nstages = I0.inters[0].nstages;
+    ctx->xsph = false;
+    for (auto& it : I0.inters) ctx->xsph |= it.vk != GC_PFN_NONE;
     for (auto& it : I0.inters)
         if (it.nstages != ctx->nstages)
             return seterr(ctx, GC_ERR_ARG, "All interactions must have the same number of stages (pfns length)");
@@ -531,6 +552,7 @@ int finalize(gc_ctx* ctx) {
         D.ncomp[F_STRESS] = D.ncomp[F_SR] = D.kind >= GC_SYS_STRESS ? D.ns : 0;
         D.ncomp[F_VORT] = D.kind == GC_SYS_ELASTOPLASTIC ? D.nvort : 0;
         D.ncomp[F_STRAIN] = D.ncomp[F_STRAINP] = D.kind == GC_SYS_ELASTOPLASTIC ? D.ns : 0;
+        D.ncomp[F_VADJ] = ctx->xsph ? D.nd : 0;
         for (int b = 0; b < 2; ++b) {
             for (int f = 0; f < NF; ++f)
                 if (D.ncomp[f]) TRY(dalloc(ctx, &D.f[b][f], (size_t)D.ncomp[f] * D.N));
@@ -667,6 +689,8 @@ int finalize(gc_ctx* ctx) {
         D.kk = h0.kk;
         D.nstages = h0.nstages;
         D.pk = h0.pk;
+        D.vadj = h0.vk != GC_PFN_NONE;
+        if (D.vadj) D.pk.push_back(h0.vk);  // the XSPH pass sweeps it as stage nstages + 1
         if (h0.b < 0) {
             D.btype = BT_SELF;
             D.bslot = h0.a;
@@ -682,7 +706,7 @@ int finalize(gc_ctx* ctx) {
         }
         D.two_fluid = D.btype == BT_SYSTEM && I0.sys[h0.a].kind == GC_SYS_FLUID &&
                       I0.sys[D.bslot].kind == GC_SYS_FLUID;
-        for (int s = 0; s < D.nstages; ++s)
+        for (int s = 0; s < (int)D.pk.size(); ++s)
             if (b_side_at(D, s + 1)) D.two_sided = true;
         D.h_gi.resize(ninst);
         for (int k = 0; k < ninst; ++k) {
@@ -759,10 +783,33 @@ int finalize(gc_ctx* ctx) {
             CU(cudaMemcpyAsync(D.d_pi[s], per.data(), ninst * sizeof(PfnInst), cudaMemcpyHostToDevice, ctx->stream));
             CU(cudaStreamSynchronize(ctx->stream));
         }
+        if (D.vadj) {
+            // XSPHPfn(epsilon): epsilon in `alpha`
+            std::vector<PfnInst> per(ninst);
+            for (int k = 0; k < ninst; ++k) {
+                memset(&per[k], 0, sizeof(PfnInst));
+                per[k].alpha = ctx->inst[k].inters[i].veps;
+                per[k].f_alpha = (float)per[k].alpha;
+            }
+            D.d_pi.push_back(nullptr);
+            TRY(dalloc(ctx, &D.d_pi.back(), (size_t)ninst));
+            CU(cudaMemcpyAsync(D.d_pi.back(), per.data(), ninst * sizeof(PfnInst), cudaMemcpyHostToDevice,
+                               ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            if (D.btype == BT_GHOST) {
+                // the ghosts' own warp groups and sums of the system_b side
+                DGhost& G = ctx->ghosts[D.bghost];
+                if (!G.gadj) {
+                    TRY(dalloc(ctx, &G.groups, (size_t)G.CAP + 1));
+                    TRY(dalloc(ctx, &G.d_ngroups, 1));
+                    TRY(dalloc(ctx, &G.gadj, (size_t)G.nd * G.CAP));
+                }
+            }
+        }
         TRY(dalloc(ctx, &D.counts, (size_t)ctx->slots[D.a].N));
         // writers
         bool writes = false;
-        for (int s = 0; s < D.nstages; ++s) writes |= D.pk[s] != GC_PFN_NONE;
+        for (int s = 0; s < (int)D.pk.size(); ++s) writes |= D.pk[s] != GC_PFN_NONE;
         if (writes) ctx->slots[D.a].written = true;
         if (D.two_sided && D.bslot >= 0) ctx->slots[D.bslot].written = true;
         CU(cudaStreamSynchronize(ctx->stream));
@@ -1044,20 +1091,11 @@ int ensure_csa(gc_ctx* ctx, DInter& D) {
     return check_launch(ctx, "grid (system_a)");
 }
 
-// Warp groups of `slot`'s particles from the columns of interaction `id`'s
-// grid: its system_b side when b_side, else its system_a side.
-int ensure_groups(gc_ctx* ctx, int slot, int id, bool b_side) {
-    DSlot& S = ctx->slots[slot];
-    DInter& D = ctx->inters[id];
-    const int64_t key = (int64_t)id * 2 + (b_side ? 1 : 0);
+// Warp groups of the particles of `cs` (a CSR on interaction D's grid) into
+// the group tables of S (a system slot or a ghost system).
+template <class St>
+int build_groups(gc_ctx* ctx, St& S, DInter& D, int64_t key, const int32_t* cs) {
     if (S.groups_key == key && S.groups_ver == D.grid_ver) return GC_OK;
-    const int32_t* cs;
-    if (b_side || D.btype == BT_SELF) {
-        cs = D.cs;
-    } else {
-        TRY(ensure_csa(ctx, D));
-        cs = D.cs_a;
-    }
     const int64_t ncols_cap = D.cells;
     if (ncols_cap + 1 > S.cap_gcols) {
         CU(cudaStreamSynchronize(ctx->stream));
@@ -1076,6 +1114,23 @@ int ensure_groups(gc_ctx* ctx, int slot, int id, bool b_side) {
     S.groups_key = key;
     S.groups_ver = D.grid_ver;
     return check_launch(ctx, "groups");
+}
+
+// Warp groups of `slot`'s particles from the columns of interaction `id`'s
+// grid: its system_b side when b_side, else its system_a side.
+int ensure_groups(gc_ctx* ctx, int slot, int id, bool b_side) {
+    DSlot& S = ctx->slots[slot];
+    DInter& D = ctx->inters[id];
+    const int64_t key = (int64_t)id * 2 + (b_side ? 1 : 0);
+    if (S.groups_key == key && S.groups_ver == D.grid_ver) return GC_OK;
+    const int32_t* cs;
+    if (b_side || D.btype == BT_SELF) {
+        cs = D.cs;
+    } else {
+        TRY(ensure_csa(ctx, D));
+        cs = D.cs_a;
+    }
+    return build_groups(ctx, S, D, key, cs);
 }
 
 // Capacity mode: record the largest plans, and flag every plan that does
@@ -1162,6 +1217,7 @@ StepArgs step_args(DSlot& S) {
     a.q0rho = S.q0rho;
     a.accv = S.accv;
     a.accrho = S.accrho;
+    a.vadj = S.ncomp[F_VADJ] ? S.F(F_VADJ) : nullptr;
     return a;
 }
 
@@ -1235,12 +1291,87 @@ int aux_mode_for(int pfn) {
     return AUX_MASS_OVER_RHO;
 }
 
+// The ghosts' side of an XSPH sweep against ghost system_b (`A` holds the
+// system_a launch): a gather over the ghosts through system_a's CSR into a
+// ghost-indexed buffer, then added to the ghost SOURCE's v_adjustment at the
+// ghost index, which is where the reference's `ps_b.v_adjustment[j]` lands
+// (a ghost forwards that property to its source, src/GhostParticles.jl:226-236).
+__global__ void k_xsph_ghost_add(const double* __restrict__ gadj, int64_t CAP, const int64_t* count, int nd,
+                                 const int32_t* __restrict__ ginst, const GhostInst* __restrict__ gh,
+                                 const SysInst* __restrict__ src, double* __restrict__ vadj, int64_t Ns, int* err) {
+    const int64_t n = *count;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        const int k = ginst[g];
+        const int64_t local = g - gh[k].base;
+        if (local >= src[k].n) {  // out of bounds in the reference
+            atomicOr(err, ERR_XSPH_GHOST);
+            continue;
+        }
+        const int64_t t = src[k].base + local;
+        for (int d = 0; d < nd; ++d) vadj[d * Ns + t] = vadj[d * Ns + t] + gadj[d * CAP + g];
+    }
+}
+
+int xsph_ghost_side(gc_ctx* ctx, const ForceArgs& A, int id, int stage) {
+    DInter& D = ctx->inters[id];
+    DGhost& G = ctx->ghosts[D.bghost];
+    DSlot& S = ctx->slots[D.a];
+    DSlot& src = ctx->slots[G.src];
+    TRY(ensure_csa(ctx, D));
+    TRY(build_groups(ctx, G, D, (int64_t)id * 2 + 1, D.cs));  // the ghosts' own CSR
+    CU(cudaMemsetAsync(G.gadj, 0, sizeof(double) * G.nd * G.CAP, ctx->stream));
+    ForceArgs R = A;
+    R.groups = G.groups;
+    R.ngroups = G.d_ngroups;
+    R.nd = G.nd;
+    R.ns = G.ns;
+    R.aN = G.CAP;
+    R.a_inst_of = G.ginst[G.cur];
+    R.ax = G.x[G.cur];
+    R.av = G.v;
+    R.arho = G.rho;
+    R.aaux = nullptr;
+    R.astress = nullptr;
+    R.a_p = nullptr;
+    R.advdt = G.gadj;
+    R.adrhodt = nullptr;
+    R.asr = nullptr;
+    R.avort = nullptr;
+    R.a_c = G.d_c;
+    R.a_mass = G.d_mass;
+    R.a_cf = nullptr;
+    R.a_massf = nullptr;
+    R.afp = nullptr;
+    R.prec = GC_PRECISION_FP64;
+    R.nref = 1;
+    InterRef& r = R.ref[0];
+    r = InterRef{};
+    r.btype = BT_SYSTEM;
+    r.bbox = S.d_inst;
+    r.gi = D.d_gi_b;
+    r.pi = D.d_pi[stage - 1];
+    r.cs = D.cs_a;
+    r.cs_cells = D.cells;
+    r.bx = S.F(F_X);
+    r.bv = S.F(F_V);
+    r.brho = S.F(F_RHO);
+    r.bN = S.N;
+    int st = launch_force_f64(R, false, ctx->stream);
+    if (st) return seterr(ctx, st, "XSPH ghost side not implemented on the device");
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((G.CAP + 255) / 256, (int64_t)ctx->num_sms * 8));
+    k_xsph_ghost_add<<<(unsigned)blocks, 256, 0, ctx->stream>>>(G.gadj, G.CAP, G.d_count, G.nd, G.ginst[G.cur],
+                                                                 G.d_gh, src.d_inst, src.F(F_VADJ), src.N, ctx->d_err);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return check_launch(ctx, "sweep (XSPH ghost side)");
+}
+
 // Fused sweep of the interactions `ids` (same system_a, same functor kind).
 int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
     DSlot& S = ctx->slots[a];
     int pfn = ctx->inters[ids[0]].pk[stage - 1];
     const int mode = aux_mode_for(pfn);
-    bool fp32 = ctx->precision == GC_PRECISION_FP32_COMPENSATED && pfn != GC_PFN_COUNT && !count_only;
+    const bool xsph = pfn == GC_PFN_XSPH;  // writes v_adjustment; always FP64
+    bool fp32 = ctx->precision == GC_PRECISION_FP32_COMPENSATED && pfn != GC_PFN_COUNT && !xsph && !count_only;
     for (int id : ids)
         if (pfn == GC_PFN_FLUID && ctx->inters[id].h_gi.size() && ctx->inst[0].inters[id].pp[stage - 1][3] == 1.0)
             fp32 = false;  // the S = 1 (multiphase) pressure form stays in FP64
@@ -1248,7 +1379,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     // FP32 sweep buffers: positions, then records (see ensure_fpk)
     auto xp_of = [](float* fpk) { return (double*)fpk; };
     auto pk_of = [](float* fpk, int64_t N, int nd) { return fpk + N * 2 * pos_stride(nd); };
-    if (pfn != GC_PFN_COUNT) {
+    if (pfn != GC_PFN_COUNT && !xsph) {
         if (fp32) {
             TRY(ensure_fpk(ctx, S, S.N, S.nd, pk_ns));
             // positions do not change between the stages of a step
@@ -1273,7 +1404,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.aaux = S.aux;
     A.astress = S.F(F_STRESS);
     A.a_p = S.F(F_P);
-    A.advdt = S.F(F_DVDT);
+    A.advdt = xsph ? S.F(F_VADJ) : S.F(F_DVDT);
     A.adrhodt = S.F(F_DRHODT);
     A.asr = S.F(F_SR);
     A.avort = S.F(F_VORT);
@@ -1335,7 +1466,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             r.bp = G.p;
             r.bstress = G.stress;
             r.bN = G.CAP;
-            if (pfn != GC_PFN_COUNT && !fp32)
+            if (pfn != GC_PFN_COUNT && !xsph && !fp32)
                 launch_aux(mode, G.CAP, G.d_count, G.rho, G.p, G.ginst[G.cur], G.d_mass, G.aux, ctx->stream);
             r.baux = G.aux;
             r.bfp = nullptr;
@@ -1367,7 +1498,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
                     r.bfp = pk_of(S.fpk, S.N, S.nd);
                     r.bxp = xp_of(S.fpk);
                 }
-            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT && !fp32) {
+            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT && !xsph && !fp32) {
                 launch_aux(mode, B.N, nullptr, B.F(F_RHO), B.F(F_P), B.inst_of, B.d_mass, B.aux, ctx->stream);
                 r.baux = B.aux;
             } else {
@@ -1417,6 +1548,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     for (int id : ids) {
         DInter& D = ctx->inters[id];
         if (count_only || !b_side_at(D, stage)) continue;
+        if (D.btype == BT_GHOST) {
+            TRY(xsph_ghost_side(ctx, A, id, stage));
+            continue;
+        }
         DSlot& B = ctx->slots[D.bslot];
         TRY(ensure_groups(ctx, D.bslot, id, true));
         ForceArgs R = A;
@@ -1432,7 +1567,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         R.aaux = B.aux;
         R.astress = B.F(F_STRESS);
         R.a_p = B.F(F_P);
-        R.advdt = B.F(F_DVDT);
+        R.advdt = xsph ? B.F(F_VADJ) : B.F(F_DVDT);
         R.adrhodt = B.F(F_DRHODT);
         R.asr = B.F(F_SR);
         R.avort = B.F(F_VORT);
@@ -1547,6 +1682,26 @@ bool decide_motion(gc_ctx* ctx) {
 
 int one_step_rk4(gc_ctx* ctx);
 
+// _xsph_correction! src/TimeIntegration.jl:421-436 after the full step has
+// subtracted and zeroed v_adjustment: adjust_v! of every interaction with a
+// velocity-adjust functor (stage nstages + 1, fused per system_a), then
+// v += v_adjustment and the position update.
+int xsph_pass(gc_ctx* ctx) {
+    const int stage = ctx->nstages + 1;
+    for (size_t a = 0; a < ctx->slots.size(); ++a) {
+        std::vector<int> ids;
+        for (size_t i = 0; i < ctx->inters.size(); ++i)
+            if (ctx->inters[i].a == (int)a && ctx->inters[i].vadj) ids.push_back((int)i);
+        for (size_t off = 0; off < ids.size(); off += MAX_REFS) {
+            std::vector<int> chunk(ids.begin() + off, ids.begin() + std::min(ids.size(), off + MAX_REFS));
+            TRY(sweep_group(ctx, (int)a, chunk, stage, false));
+        }
+    }
+    for (auto& S : ctx->slots)
+        if (S.moving) launch_xsph_final(step_args(S), ctx->stream);
+    return check_launch(ctx, "XSPH correction");
+}
+
 int one_step(gc_ctx* ctx) {
     if (ctx->inst[0].integ == GC_INTEGRATOR_RK4) return one_step_rk4(ctx);
     ctx->pack_epoch++;
@@ -1572,6 +1727,7 @@ int one_step(gc_ctx* ctx) {
     for (auto& S : ctx->slots)
         if (S.moving) launch_fullstep(step_args(S), ctx->stream);
     TRY(check_launch(ctx, "full step"));
+    if (ctx->xsph) TRY(xsph_pass(ctx));
     ctx->steps_done += 1;
     return GC_OK;
 }
@@ -1616,6 +1772,7 @@ int one_step_rk4(gc_ctx* ctx) {
     for (auto& S : ctx->slots)
         if (S.moving) launch_rk4_final(step_args(S), ctx->stream);
     TRY(check_launch(ctx, "rk4 final"));
+    if (ctx->xsph) TRY(xsph_pass(ctx));
     ctx->steps_done += 1;
     return GC_OK;
 }
@@ -1653,6 +1810,10 @@ int finish_status(gc_ctx* ctx) {
     ctx->last_status = e;
     if (e & ERR_NONFINITE) return seterr(ctx, GC_ERR_NONFINITE, "non-finite or out-of-range particle position");
     if (e & ERR_CAPACITY) return seterr(ctx, GC_ERR_CAPACITY, "a particle fell outside its grid or key range");
+    if (e & ERR_XSPH_GHOST)
+        return seterr(ctx, GC_ERR_UNSUPPORTED,
+                      "XSPH against a ghost system wrote beyond the ghost source's length (out of bounds in the "
+                      "reference)");
     return GC_OK;
 }
 
@@ -1700,7 +1861,8 @@ bool tuning(gc_ctx* ctx) {
     return false;
 }
 
-int grow_gcols(gc_ctx* ctx, DSlot& S, int64_t ncols) {
+template <class St>
+int grow_gcols(gc_ctx* ctx, St& S, int64_t ncols) {
     if (ncols + 1 <= S.cap_gcols) return GC_OK;
     CU(cudaStreamSynchronize(ctx->stream));
     dfree(ctx, S.gcnt, S.cap_gcols);
@@ -1745,6 +1907,7 @@ int size_capacities(gc_ctx* ctx) {
         const int64_t cells = cap_grid_cells(ctx, D);
         TRY(grow_gcols(ctx, ctx->slots[D.a], cells));
         if (D.two_sided && D.bslot >= 0) TRY(grow_gcols(ctx, ctx->slots[D.bslot], cells));
+        if (D.vadj && D.btype == BT_GHOST) TRY(grow_gcols(ctx, ctx->ghosts[D.bghost], cells));
     }
     // the bound each plan entry is checked against inside the steps
     std::vector<int64_t> cap(n);
@@ -2052,6 +2215,11 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(G.d_mass);
         cudaFree(G.d_c);
         cudaFree(G.fpk);
+        cudaFree(G.groups);
+        cudaFree(G.d_ngroups);
+        cudaFree(G.gcnt);
+        cudaFree(G.goff);
+        cudaFree(G.gadj);
     }
     for (auto& D : ctx->inters) {
         cudaFree(D.d_gi);
@@ -2253,6 +2421,19 @@ int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kerne
     }
     I.inters.push_back(it);
     *inter_out = (int)I.inters.size() - 1;
+    return GC_OK;
+}
+
+int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double epsilon) {
+    if (!ctx) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
+    HInst& I = ctx->inst[inst];
+    if (inter < 0 || inter >= (int)I.inters.size()) return seterr(ctx, GC_ERR_ARG, "bad interaction");
+    if (kind != GC_PFN_NONE && kind != GC_PFN_XSPH)
+        return seterr(ctx, GC_ERR_UNSUPPORTED, "velocity-adjust functor kind %d has no device implementation", kind);
+    I.inters[inter].vk = kind;
+    I.inters[inter].veps = epsilon;
     return GC_OK;
 }
 
@@ -2474,7 +2655,7 @@ int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
                 st, n * comps[q], ctx->d_ioflags + q);
             g_launches.fetch_add(1, std::memory_order_relaxed);
         }
-        if (f.field == GC_FIELD_V_ADJUSTMENT) continue;
+        if (f.field == GC_FIELD_V_ADJUSTMENT && !S.ncomp[F_VADJ]) continue;  // not carried: must be zero
         if (f.field == GC_FIELD_ID) launch_i64_to_i32((const int64_t*)st, S.id[S.cur] + base, n, ctx->stream);
         else launch_aos_to_planar(st, S.F(field_slot(f.field)), n, comps[q], S.N, base, ctx->stream);
     }
@@ -2487,8 +2668,9 @@ int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
     for (int q = 0; q < nio; ++q) {
         const gc_field_io& f = io[q];
         DSlot& S = *ref[q].slot;
-        if (f.field == GC_FIELD_V_ADJUSTMENT && flags[q])
-            return seterr(ctx, GC_ERR_UNSUPPORTED, "non-zero v_adjustment (XSPH) is not supported");
+        if (f.field == GC_FIELD_V_ADJUSTMENT && flags[q] && !S.ncomp[F_VADJ])
+            return seterr(ctx, GC_ERR_UNSUPPORTED,
+                          "non-zero v_adjustment needs a velocity-adjust functor (it is not carried without one)");
         if (f.field == GC_FIELD_X) {
             // a system that is not sorted every step is sorted again
             if (!S.moving) structural = true;
@@ -2496,8 +2678,9 @@ int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
             S.xpk_static = false;
             S.xpk_epoch = -1;
         }
-        if (f.field == GC_FIELD_V || f.field == GC_FIELD_DVDT || f.field == GC_FIELD_DRHODT) {
-            int64_t bit = f.field == GC_FIELD_V ? 1 : f.field == GC_FIELD_DVDT ? 2 : 4;
+        if (f.field == GC_FIELD_V || f.field == GC_FIELD_DVDT || f.field == GC_FIELD_DRHODT ||
+            f.field == GC_FIELD_V_ADJUSTMENT) {
+            int64_t bit = f.field == GC_FIELD_V ? 1 : f.field == GC_FIELD_DVDT ? 2 : f.field == GC_FIELD_DRHODT ? 4 : 8;
             if (flags[q]) S.nonzero_kin[f.inst] |= bit;
             else S.nonzero_kin[f.inst] &= ~bit;
         }
@@ -2539,7 +2722,7 @@ int gc_download_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
         const int64_t n = ctx->inst[f.inst].sys[ref[q].sys].n, base = S.h_inst[f.inst].base;
         double* st = ctx->staging + off;
         off += n * comps[q];
-        if (f.field == GC_FIELD_V_ADJUSTMENT) {
+        if (f.field == GC_FIELD_V_ADJUSTMENT && !S.ncomp[F_VADJ]) {  // not carried: zero
             memset(f.host, 0, f.bytes);
             continue;
         }

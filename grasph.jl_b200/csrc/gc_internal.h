@@ -25,7 +25,8 @@ enum : int {
     ERR_NONFINITE = 1,      // NaN/Inf or out-of-range position in a key/cell
     ERR_CAPACITY = 2,       // a cell or ghost index beyond its buffer
     ERR_GRID_INCONS = 4,    // key order vs cell order disagreement (warning)
-    ERR_TIMEOUT = 8
+    ERR_TIMEOUT = 8,
+    ERR_XSPH_GHOST = 16     // an XSPH write at a ghost index beyond the ghost's source system
 };
 
 // Per (system slot, instance) parameters; packed range [base, base+n).

@@ -15,6 +15,7 @@ struct StepArgs {
     const SysInst* inst;
     double *x, *v, *rho, *dvdt, *drhodt, *q0v, *q0rho;
     double *accv, *accrho;  // RK4 accumulators (nullptr for LeapFrog)
+    double* vadj;           // v_adjustment when an XSPH functor is swept (else nullptr)
 };
 
 struct UpdArgs {
@@ -37,6 +38,10 @@ void launch_rk4_begin(const StepArgs& a, cudaStream_t s);
 void launch_rk4_advance(const StepArgs& a, double f, cudaStream_t s);
 void launch_rk4_acc(const StepArgs& a, double w, cudaStream_t s);
 void launch_rk4_final(const StepArgs& a, cudaStream_t s);
+// src/TimeIntegration.jl:421-436, 684-685: with v_adjustment carried, the
+// full step (or RK4 final) ends at v -= v_adjustment, v_adjustment = 0; after
+// the XSPH sweeps this adds the new adjustment back and moves x by dt·v.
+void launch_xsph_final(const StepArgs& a, cudaStream_t s);
 void launch_update(const UpdArgs& a, cudaStream_t s);
 
 }  // namespace gc

@@ -123,6 +123,23 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         acc.dr += 1.0;
         return 1;
     }
+    if (PFN == GC_PFN_XSPH) {
+        // XSPHPfn src/PairwiseFunctors.jl:364-389, xsph_veladjust
+        // src/PairwisePhysics.jl:268-270: du = ((-ε·dv)·w)/(ρ_i + ρ_j),
+        // v_adjustment_i += du·m_j.  Every system_b kind contributes its stored
+        // velocity and density (a boundary wrapper forwards to its system);
+        // the system_b side is this same term with the roles swapped.
+        const double q = sqrt(rr) / G.H;
+        const double wk = kernel_w<KK>(G.knorm, q);
+        const double den = o.rho + r.brho[j];
+        const double mj = r.btype == BT_SELF ? A.a_mass[k] : G.bmass;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const double du = (((-P.alpha) * (o.v[d] - r.bv[d * Nb + j])) * wk) / den;
+            acc.dv[d] = acc.dv[d] + du * mj;
+        }
+        return 1;
+    }
     double gx[ND];
     Pair<ND, NS, PFN, KK>::geom(dx, rr, G.H, G.knorm, gx);
     const double ca = A.a_c[k];
@@ -315,7 +332,10 @@ struct PhysF64 {
         for (int d = 0; d < ND; ++d) acc.dv[d] = 0.0;
         acc.dr = 0.0;
         if (!from_memory) return;
-        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        if (PFN == GC_PFN_XSPH) {  // advdt is the v_adjustment array here
+#pragma unroll
+            for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
+        } else if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
             acc.dr = A.adrhodt[gi];
@@ -330,7 +350,10 @@ struct PhysF64 {
     }
     static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
         const int64_t N = A.aN;
-        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        if (PFN == GC_PFN_XSPH) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
+        } else if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
             A.adrhodt[gi] = acc.dr;
@@ -972,7 +995,7 @@ static void launch_cfg(const ForceArgs& A, cudaStream_t s) {
 template <int ND, int NS, int PFN, int KK, bool F32>
 static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
     if constexpr (F32) {
-        if constexpr (PFN != GC_PFN_COUNT) launch_cfg<PhysF32<ND, NS, PFN, KK>, ND, PFN>(A, s);
+        if constexpr (PFN != GC_PFN_COUNT && PFN != GC_PFN_XSPH) launch_cfg<PhysF32<ND, NS, PFN, KK>, ND, PFN>(A, s);
     } else {
         using P64 = PhysF64<ND, NS, PFN, KK>;
         if (count_only) {
@@ -993,6 +1016,13 @@ static int launch_pfn(const ForceArgs& A, bool count_only, cudaStream_t s) {
     switch (A.pfn) {
         case GC_PFN_FLUID: launch_t<ND, NS, GC_PFN_FLUID, KK, F32>(A, count_only, s); return 0;
         case GC_PFN_COUNT: launch_t<ND, NS, GC_PFN_COUNT, KK, F32>(A, count_only, s); return 0;
+        case GC_PFN_XSPH:  // FP64 only (a cheap, memory-bound functor)
+            if constexpr (F32) {
+                return GC_ERR_UNSUPPORTED;
+            } else {
+                launch_t<ND, NS, GC_PFN_XSPH, KK, F32>(A, count_only, s);
+                return 0;
+            }
         case GC_PFN_CAUCHY_FLUID:
             if (NS == 0) return GC_ERR_UNSUPPORTED;
             launch_t<ND, NS, GC_PFN_CAUCHY_FLUID, KK, F32>(A, count_only, s);

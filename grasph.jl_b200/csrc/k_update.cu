@@ -47,11 +47,30 @@ __global__ void k_fullstep(StepArgs a) {
                 a.dvdt[d * a.N + g] = dv;
             }
             double v = a.q0v[d * a.N + g] + dt * dv;
-            v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
+            if (a.vadj) {
+                // XSPH correction first half; positions move after the sweeps
+                v = v + (-1.0 * a.vadj[d * a.N + g]);
+                a.vadj[d * a.N + g] = 0.0;
+                a.v[d * a.N + g] = v;
+            } else {
+                v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
+                a.v[d * a.N + g] = v;
+                a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
+            }
+        }
+        a.rho[g] = fma(dt, a.drhodt[g], a.q0rho[g]);
+    }
+}
+
+// :434 and :684-685: v += v_adjustment, then x += dt·v.
+__global__ void k_xsph_final(StepArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
+        const double dt = a.inst[a.inst_of[g]].dt;
+        for (int d = 0; d < a.nd; ++d) {
+            const double v = a.v[d * a.N + g] + 1.0 * a.vadj[d * a.N + g];
             a.v[d * a.N + g] = v;
             a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
         }
-        a.rho[g] = fma(dt, a.drhodt[g], a.q0rho[g]);
     }
 }
 
@@ -109,9 +128,15 @@ __global__ void k_rk4_final(StepArgs a) {
         const double dt = S.dt;
         for (int d = 0; d < a.nd; ++d) {
             double v = a.q0v[d * a.N + g] + dt * a.accv[d * a.N + g];
-            v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
-            a.v[d * a.N + g] = v;
-            a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
+            if (a.vadj) {
+                v = v + (-1.0 * a.vadj[d * a.N + g]);
+                a.vadj[d * a.N + g] = 0.0;
+                a.v[d * a.N + g] = v;
+            } else {
+                v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
+                a.v[d * a.N + g] = v;
+                a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
+            }
         }
         a.rho[g] = fma(dt, a.accrho[g], a.q0rho[g]);
     }
@@ -131,6 +156,11 @@ void launch_rk4_acc(const StepArgs& a, double w, cudaStream_t s) {
 }
 void launch_rk4_final(const StepArgs& a, cudaStream_t s) {
     if (a.N > 0) k_rk4_final<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+
+void launch_xsph_final(const StepArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_xsph_final<<<ublk(a.N), UTPB, 0, s>>>(a);
     g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
 }
 

@@ -82,6 +82,7 @@ def load_library(path: os.PathLike | None = None):
         "gc_set_updaters": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _ip, _ip, _dp]),
         "gc_set_integrator": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double]),
         "gc_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
+        "gc_set_velocity_adjust": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_double]),
         "gc_finalize": (ct.c_int, [ct.c_void_p]),
         "gc_upload_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         "gc_download_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
@@ -196,6 +197,9 @@ class CudaBackend:
         self._chk(self.lib.gc_add_interaction(self.ctx, inst, a, b, kernel_kind, h, len(k),
                                               k.ctypes.data_as(_ip), pp, ct.byref(out)), "gc_add_interaction")
         return out.value
+
+    def set_velocity_adjust(self, inst, inter, kind, epsilon):
+        self._chk(self.lib.gc_set_velocity_adjust(self.ctx, inst, inter, kind, epsilon), "gc_set_velocity_adjust")
 
     def set_updaters(self, inst, sys, chains):
         cl = np.array([len(c) for c in chains] or [0], dtype=np.int32)
@@ -380,6 +384,8 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
         kinds = [_pfn_kind(p) for p in it.pfns]
         params = np.array([_pfn_params(p) for p in it.pfns], dtype=np.float64)
         m.inters[id(it)] = backend.add_interaction(inst, m.h(a), bh, it.kernel.kind, it.kernel.h, kinds, params)
+        if getattr(it, "vadjust_pfn", None) is not None:
+            backend.set_velocity_adjust(inst, m.inters[id(it)], it.vadjust_pfn.kind, it.vadjust_pfn.epsilon)
     for ps in systems:
         chains = updater_chains(ps)
         if chains:

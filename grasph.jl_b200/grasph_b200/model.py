@@ -405,6 +405,17 @@ class CountingPfn(_Pfn):
     kind = C.GC_PFN_COUNT
 
 
+class XSPHPfn(_Pfn):
+    """XSPH velocity smoothing, src/PairwiseFunctors.jl:357-389; only as a
+    `velocity_adjust_pairwise_fn` (swept by adjust_v! in the step's XSPH
+    correction, src/TimeIntegration.jl:421-436)."""
+
+    kind = C.GC_PFN_XSPH
+
+    def __init__(self, epsilon):
+        self.epsilon = float(epsilon)
+
+
 def _pfn_kind(p):
     return C.GC_PFN_NONE if p is None else p.kind
 
@@ -550,7 +561,8 @@ def updater_chains(ps: AbstractParticleSystem):
 class SystemInteraction:
     """src/Interaction.jl:23-92."""
 
-    def __init__(self, kernel: AbstractKernel, pairwise_fn, system_a, system_b=None):
+    def __init__(self, kernel: AbstractKernel, pairwise_fn, system_a, system_b=None, *,
+                 velocity_adjust_pairwise_fn=None):
         nd = system_a.ndims
         if kernel.ndims != nd:
             raise ArgumentError(f"kernel.ndims ({kernel.ndims}) must match system_a.ndims ({nd})")
@@ -559,8 +571,15 @@ class SystemInteraction:
                 f"system_b.ndims ({system_b.ndims}) must match system_a.ndims ({nd})")
         if not isinstance(system_a, AbstractParticleSystem):
             raise ArgumentError("system_a must be a particle system")
+        vpf = velocity_adjust_pairwise_fn
+        if vpf is not None and not isinstance(vpf, XSPHPfn):
+            raise ArgumentError(f"velocity-adjust functor {type(vpf).__name__} has no device implementation")
         self.kernel = kernel
         self.pfns = pairwise_fn if isinstance(pairwise_fn, tuple) else (pairwise_fn,)
+        for f in self.pfns:
+            if isinstance(f, XSPHPfn):
+                raise ArgumentError("XSPHPfn is a velocity-adjust functor, not a stage functor")
+        self.vadjust_pfn = vpf
         self.system_a = system_a
         self.system_b = system_b
         self.ndims = nd

@@ -22,7 +22,7 @@ from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, Dyna
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
                     GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator, LinearEOSUpdater,
                     RK4TimeIntegrator, StrainRatePfn, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
-                    TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, ZeroFieldUpdater)
+                    TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater)
 
 G = 9.81
 
@@ -233,23 +233,26 @@ def granular_column(nfx=100, nfy=50, dx=0.002, rho0=1850.0, E=0.84e6, nu=0.3, ph
 # ------------------------------------------------------- multiphase bubble
 
 BUBBLE_VARIANTS = {
-    # rho_Y, c_Y / sqrt(g R), gamma_Y, sigma, epsilon (X-Y), dx
-    "bubble": (500.0, 40.0, 7.0, 2, None, 0.05),
-    "bubble2": (10.0, math.sqrt(16000.0), 1.4, 1, None, 0.04),
-    "bubble3": (1.0, 400.0, 1.4, 1, 0.1, 0.04),
+    # rho_Y, c_Y / sqrt(g R), gamma_Y, sigma, epsilon (X-Y), XSPH epsilon, dx
+    "bubble": (500.0, 40.0, 7.0, 2, None, None, 0.05),
+    "bubble2": (10.0, math.sqrt(16000.0), 1.4, 1, None, None, 0.04),
+    "bubble3": (1.0, 400.0, 1.4, 1, 0.1, 0.5, 0.04),
 }
 
 
 def bubble(variant="bubble", R=1.0, dx=None, rho_x=1000.0, alpha=0.01, beta=0.0, hfac=1.2, cfl=1.5,
-           integrator="rk4"):
+           integrator="rk4", xsph=True):
     """2-D light-fluid bubble rising in a heavy fluid (bubble.jl /
-    bubble2.jl / bubble3.jl layout, without XSPH): a 6R x 10R column of
-    fluid X with a disc of radius R of fluid Y centred at the origin, both
-    Tait fluids with hydrostatic initial density and zero initial pressure,
-    Wendland C2 kernel, FluidPfn self interactions, the two-sided X-Y
-    FluidPfn with Y first, a one-stage ghost of X with its pressure copied,
-    mirrored across the four walls and the four diagonal corner planes."""
-    rho_y, cy_fac, gamma_y, sigma, eps, dx0 = BUBBLE_VARIANTS[variant]
+    bubble2.jl / bubble3.jl layout): a 6R x 10R column of fluid X with a
+    disc of radius R of fluid Y centred at the origin, both Tait fluids with
+    hydrostatic initial density and zero initial pressure, Wendland C2
+    kernel, FluidPfn self interactions, the two-sided X-Y FluidPfn with Y
+    first, a one-stage ghost of X with its pressure copied, mirrored across
+    the four walls and the four diagonal corner planes.  bubble3 adds
+    XSPHPfn(0.5) velocity adjustment on X, Y and X-ghost (`xsph=False`
+    leaves it out)."""
+    rho_y, cy_fac, gamma_y, sigma, eps, xeps, dx0 = BUBBLE_VARIANTS[variant]
+    xs = XSPHPfn(xeps) if (xsph and xeps is not None) else None
     dx = dx0 if dx is None else dx
     height, width = 10.0 * R, 6.0 * R
     y_min, x_min = -2.0 * R, -3.0 * R
@@ -283,10 +286,10 @@ def bubble(variant="bubble", R=1.0, dx=None, rho_x=1000.0, alpha=0.01, beta=0.0,
                         ((s2, -s2), (x_min, y_max)), ((-s2, -s2), (x_max, y_max)))
     kernel = WenlandC2Kernel(h, ndims=2)
     pfn = FluidPfn(alpha, beta, h, sigma=sigma)
-    inters = [SystemInteraction(kernel, pfn, fx),
-              SystemInteraction(kernel, pfn, fy),
+    inters = [SystemInteraction(kernel, pfn, fx, velocity_adjust_pairwise_fn=xs),
+              SystemInteraction(kernel, pfn, fy, velocity_adjust_pairwise_fn=xs),
               SystemInteraction(kernel, FluidPfn(alpha, beta, h, sigma=sigma, epsilon=eps), fy, fx),
-              SystemInteraction(kernel, pfn, fx, ghost)]
+              SystemInteraction(kernel, pfn, fx, ghost, velocity_adjust_pairwise_fn=xs)]
     cls = RK4TimeIntegrator if integrator == "rk4" else LeapFrogTimeIntegrator
     lf = cls([fx, fy], inters, ghosts=(gentry,))
     meta = dict(workload=variant, n_fluid=fx.n + fy.n, n_x=fx.n, n_y=fy.n, h=h, c0=max(c_x, c_y), cfl=cfl,

@@ -158,6 +158,12 @@ function CudaLeapFrog(lf::Union{LeapFrogTimeIntegrator,RK4TimeIntegrator}; devic
                            (Ptr{Cvoid}, Cint, Cint, Cint, Cint, Cdouble, Cint, Ptr{Cint}, Ptr{Cdouble}, Ref{Cint}),
                            ctx[], inst[], h[si.system_a], bh, kk, si.kernel.h, length(kinds), kinds, prm, out))
         push!(ints, out[])
+        vf = si.vadjust_pfn
+        if vf !== nothing
+            vf isa XSPHPfn || throw(ArgumentError("velocity-adjust functor $(typeof(vf)) has no device implementation"))
+            check(ctx[], ccall((:gc_set_velocity_adjust, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Cint, Cdouble),
+                               ctx[], inst[], out[], 6, vf.epsilon))
+        end
     end
     for ps in lf.systems
         isempty(ps.state_updater) && continue

@@ -92,7 +92,8 @@ enum {
     GC_PFN_CAUCHY_FLUID = 2,            /* CauchyFluidPfn :252                 */
     GC_PFN_STRAIN_RATE = 3,             /* StrainRatePfn :18                   */
     GC_PFN_STRAIN_RATE_VORTICITY = 4,   /* StrainRateVorticityPfn :78          */
-    GC_PFN_COUNT = 5
+    GC_PFN_COUNT = 5,
+    GC_PFN_XSPH = 6                     /* XSPHPfn :360-389; velocity-adjust functor only */
 };
 /* Per-stage functor parameters, GC_PFN_NPARAM doubles each:
  *   [0] art_visc_alpha  [1] art_visc_beta  [2] h
@@ -197,6 +198,12 @@ int gc_add_ghost(gc_ctx* ctx, int inst, int src_sys, int ncopiers,
 int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kernel_kind,
                        double h, int nstages, const int* pfn_kinds, const double* pfn_params,
                        int* inter_out);
+
+/* SystemInteraction(...; velocity_adjust_pairwise_fn) src/Interaction.jl:61-66:
+ * kind GC_PFN_XSPH (XSPHPfn(epsilon)) or GC_PFN_NONE.  Swept by adjust_v!
+ * (:309) in the step's XSPH correction, src/TimeIntegration.jl:421-436.
+ * Every instance of a context must set the same kind on an interaction.   */
+int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double epsilon);
 
 /* The `state_updater` tuple of a system (src/Particles.jl:200): nstages
  * entries, each a chain of `chain_len[s]` updaters (kinds / GC_UPD_NPARAM

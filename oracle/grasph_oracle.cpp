@@ -174,6 +174,8 @@ struct Inter {
     std::vector<int64_t> cs, csa;
     double mina[3] = {0, 0, 0}, maxa[3] = {0, 0, 0};
     bool grid = false;
+    int vk = GC_PFN_NONE;  // velocity_adjust_pairwise_fn (XSPHPfn or nothing)
+    double veps = 0.0;     // its epsilon
 };
 
 }  // namespace
@@ -387,7 +389,7 @@ Pfn make_pfn(int kind, const double* prm) {
 // --------------------------------------------------------- self functors
 // src/PairwiseFunctors.jl :20 (SR), :80 (SRV), :151 (Fluid), :265 (Cauchy)
 template <int ND>
-void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, const double* gx) {
+void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, const double* gx, double w) {
     const int ns = ps.ns;
     switch (f.kind) {
         case GC_PFN_FLUID: {
@@ -460,6 +462,15 @@ void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, con
             ps.drhodt[j] += 1.0;
             break;
         }
+        case GC_PFN_XSPH: {  // :364-375 with xsph_veladjust src/PairwisePhysics.jl:268-270
+            double ri = ps.rho[i], rj = ps.rho[j], den = ri + rj;
+            for (int d = 0; d < ND; ++d) {
+                double du = (((-f.alpha) * (ps.v[i * ND + d] - ps.v[j * ND + d])) * w) / den;
+                ps.vadj[i * ND + d] = ps.vadj[i * ND + d] + du * ps.mass;
+                ps.vadj[j * ND + d] = ps.vadj[j * ND + d] - du * ps.mass;
+            }
+            break;
+        }
         default:
             break;
     }
@@ -470,9 +481,31 @@ void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, con
 // :53/:111/:222/:334; static :210/:322; ghost Cauchy :286; counting (tests).
 template <int ND>
 void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, const double* dx,
-                 const double* gx) {
+                 const double* gx, double w, int* err) {
     const int ns = a.ns;
     const double* vi = &a.v[i * ND];
+    if (f.kind == GC_PFN_XSPH) {
+        // generic coupled XSPHPfn :378-389 for every system_b: its stored v and
+        // rho (a wrapper forwards to the wrapped system), and the write goes to
+        // ps_b.v_adjustment[j] -- for a ghost system that property is the
+        // SOURCE's array (src/GhostParticles.jl:226-236), indexed by the ghost
+        // index j; beyond the source's length the reference writes out of bounds
+        double ri = a.rho[i], rj = b.rho[j], den = ri + rj;
+        double* adj_b = nullptr;
+        if (b.type == H_GHOST) {
+            if (j >= b.sys->n) {
+                *err = 1;
+                return;
+            }
+        }
+        adj_b = b.sys->vadj.data();
+        for (int d = 0; d < ND; ++d) {
+            double du = (((-f.alpha) * (vi[d] - b.v[j * ND + d])) * w) / den;
+            a.vadj[i * ND + d] = a.vadj[i * ND + d] + du * b.mass;
+            adj_b[j * ND + d] = adj_b[j * ND + d] - du * a.mass;
+        }
+        return;
+    }
     if (f.kind == GC_PFN_COUNT) {
         a.dvdt[i * ND] += 1.0;
         a.drhodt[i] += 1.0;
@@ -624,15 +657,16 @@ inline void pair_self(const Pfn& f, const Kern& k, Sys& ps, int64_t i, int64_t j
         double r = std::sqrt(r_sq);
         double q = r / h;
         double gc = kernel_dw_dq(k, q) / (r * h);
+        double w = f.kind == GC_PFN_XSPH ? kernel_w(k, q) : 0.0;
         double gx[ND];
         for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
-        pfn_self<ND>(f, ps, i, j, dx, gx);
+        pfn_self<ND>(f, ps, i, j, dx, gx, w);
     }
 }
 
 template <int ND>
 inline void pair_coupled(const Pfn& f, const Kern& k, Sys& a, const BView& b, int64_t i, int64_t j,
-                         double h, double cutoff_sq) {
+                         double h, double cutoff_sq, int* err) {
     double dx[ND];
     for (int d = 0; d < ND; ++d) dx[d] = a.x[i * ND + d] - b.x[j * ND + d];
     double r_sq = dot<ND>(dx, dx);
@@ -640,9 +674,10 @@ inline void pair_coupled(const Pfn& f, const Kern& k, Sys& a, const BView& b, in
         double r = std::sqrt(r_sq);
         double q = r / h;
         double gc = kernel_dw_dq(k, q) / (r * h);
+        double w = f.kind == GC_PFN_XSPH ? kernel_w(k, q) : 0.0;
         double gx[ND];
         for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
-        pfn_coupled<ND>(f, a, b, i, j, dx, gx);
+        pfn_coupled<ND>(f, a, b, i, j, dx, gx, w, err);
     }
 }
 
@@ -716,8 +751,12 @@ int make_view(oracle_ctx* ctx, int handle, BView* out);
 
 // src/Interaction.jl:600-645 (2-D coupled, 9 colours), :660-715 (3-D, 27 colours)
 template <int ND>
-void sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
+int sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
     Sys& a = ctx->sys[it.a];
+    int err = 0;
+    // a ghost's XSPH writes land in its source's array at ghost indices, which
+    // a-side writes of other cells of the colour may also touch: one thread
+    const int threads = (f.kind == GC_PFN_XSPH && b.type == H_GHOST) ? 1 : ctx->threads;
     Kern k = make_kernel(it.kk, ND, it.H);
     const double h = it.H, cutoff = it.cell;
     const double cutoff_sq = it.cell * it.cell;
@@ -737,7 +776,7 @@ void sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
             int64_t nax = bx <= cmax[0] ? (cmax[0] - bx) / 3 + 1 : 0;
             int64_t nay = by <= cmax[1] ? (cmax[1] - by) / 3 + 1 : 0;
             int64_t total = nax * nay;
-#pragma omp parallel for schedule(static) num_threads(ctx->threads)
+#pragma omp parallel for schedule(static) num_threads(threads)
             for (int64_t flat = 1; flat <= total; ++flat) {
                 int64_t sx = (flat - 1) / nay, sy = (flat - 1) % nay;
                 int64_t cx = bx + sx * 3, cy = by + sy * 3;
@@ -748,7 +787,7 @@ void sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
                         int64_t nb = cell + dcx * ny - 1;
                         int64_t bs = CS(cs, nb), be = CS(cs, nb + 3);
                         for (int64_t pj = bs; pj <= be - 1; ++pj)
-                            pair_coupled<ND>(f, k, a, b, pi_ - 1, pj - 1, h, cutoff_sq);
+                            pair_coupled<ND>(f, k, a, b, pi_ - 1, pj - 1, h, cutoff_sq, &err);
                     }
             }
         }
@@ -760,7 +799,7 @@ void sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
             int64_t nay = by <= cmax[1] ? (cmax[1] - by) / 3 + 1 : 0;
             int64_t naz = bz <= cmax[2] ? (cmax[2] - bz) / 3 + 1 : 0;
             int64_t nayz = nay * naz, total = nax * nayz;
-#pragma omp parallel for schedule(static) num_threads(ctx->threads)
+#pragma omp parallel for schedule(static) num_threads(threads)
             for (int64_t flat = 1; flat <= total; ++flat) {
                 int64_t sx = (flat - 1) / nayz, rem = (flat - 1) % nayz;
                 int64_t sy = rem / naz, sz = rem % naz;
@@ -773,11 +812,12 @@ void sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
                             int64_t nb = cell + dcx * nyz + dcy * nz - 1;
                             int64_t bs = CS(cs, nb), be = CS(cs, nb + 3);
                             for (int64_t pj = bs; pj <= be - 1; ++pj)
-                                pair_coupled<ND>(f, k, a, b, pi_ - 1, pj - 1, h, cutoff_sq);
+                                pair_coupled<ND>(f, k, a, b, pi_ - 1, pj - 1, h, cutoff_sq, &err);
                         }
             }
         }
     }
+    return err ? GC_ERR_CAPACITY : GC_OK;
 }
 
 // ------------------------------------------------------------------- grid
@@ -1254,7 +1294,7 @@ int make_view(oracle_ctx* ctx, int handle, BView* out) {
         b.mass = src.mass;
         b.c = src.c;
         b.ns = src.ns;
-        b.sys = nullptr;
+        b.sys = &src;  // the ghost's forwarded properties (v_adjustment) are the source's
     } else {
         Sys& s = ctx->sys[h.idx];
         b.n = s.n;
@@ -1281,6 +1321,7 @@ int make_view(oracle_ctx* ctx, int handle, BView* out) {
 int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     const Sys& a = ctx->sys[it.a];
     if (pk == GC_PFN_NONE) return GC_OK;
+    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_COUNT) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
     if (pk == GC_PFN_FLUID && !a.has_p()) return GC_ERR_ARG;
     if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE) && !a.has_stress()) return GC_ERR_ARG;
     if (pk == GC_PFN_STRAIN_RATE_VORTICITY && !a.is_ep()) return GC_ERR_ARG;
@@ -1323,9 +1364,47 @@ int sweep(oracle_ctx* ctx, Inter& it, int stage) {
         BView b;
         int st = make_view(ctx, it.b, &b);
         if (st) return st;
-        if (nd == 2) sweep_coupled<2>(ctx, it, f, b);
-        else sweep_coupled<3>(ctx, it, f, b);
+        st = nd == 2 ? sweep_coupled<2>(ctx, it, f, b) : sweep_coupled<3>(ctx, it, f, b);
+        if (st) return fail(ctx, st, "XSPH: a ghost index beyond its source system's length");
     }
+    return GC_OK;
+}
+
+// adjust_v! src/Interaction.jl:309: one sweep of the velocity-adjust functor
+int adjust_v(oracle_ctx* ctx, Inter& it) {
+    if (it.vk == GC_PFN_NONE) return GC_OK;
+    if (!it.grid) return fail(ctx, GC_ERR_STATE, "adjust_v before create_grid");
+    std::array<double, GC_PFN_NPARAM> prm{};
+    prm[0] = it.veps;
+    prm[4] = prm[5] = std::nan("");
+    Pfn f = make_pfn(it.vk, prm.data());
+    const int nd = ctx->sys[it.a].nd;
+    if (it.b < 0) {
+        if (nd == 2) sweep_self<2>(ctx, it, f);
+        else sweep_self<3>(ctx, it, f);
+        return GC_OK;
+    }
+    BView b;
+    int st = make_view(ctx, it.b, &b);
+    if (st) return st;
+    st = nd == 2 ? sweep_coupled<2>(ctx, it, f, b) : sweep_coupled<3>(ctx, it, f, b);
+    if (st) return fail(ctx, st, "XSPH: a ghost index beyond its source system's length");
+    return GC_OK;
+}
+
+// _xsph_correction! src/TimeIntegration.jl:421-436: v -= v_adjustment, zero
+// it, re-run every interaction's velocity-adjust functor, v += v_adjustment
+// (both axpys as separate multiply and add, the SVector form)
+int xsph_correction(oracle_ctx* ctx) {
+    for (auto& s : ctx->sys)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.v[i] + (-1.0 * s.vadj[i]);
+    for (auto& s : ctx->sys) std::fill(s.vadj.begin(), s.vadj.end(), 0.0);
+    for (auto& it : ctx->inters) {
+        int st = adjust_v(ctx, it);
+        if (st) return st;
+    }
+    for (auto& s : ctx->sys)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.v[i] + 1.0 * s.vadj[i];
     return GC_OK;
 }
 
@@ -1392,9 +1471,11 @@ int step_once(oracle_ctx* ctx, double dt) {
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.dvdt[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.drhodt[i], s.q0rho[i]);
     }
-    // 10. XSPH correction with a zero adjustment: v += -1*0; v += 1*0
-    for (auto& s : ctx->sys)
-        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = (s.v[i] + (-1.0 * s.vadj[i])) + 1.0 * s.vadj[i];
+    // 10. XSPH correction
+    {
+        int st = xsph_correction(ctx);
+        if (st) return st;
+    }
     // 11. positions
     for (auto& s : ctx->sys)
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
@@ -1478,9 +1559,11 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.accv[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.accrho[i], s.q0rho[i]);
     }
-    // 10. XSPH correction with a zero adjustment (:821)
-    for (auto& s : ctx->sys)
-        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = (s.v[i] + (-1.0 * s.vadj[i])) + 1.0 * s.vadj[i];
+    // 10. XSPH correction (:821)
+    {
+        int st = xsph_correction(ctx);
+        if (st) return st;
+    }
     // 11. positions (:824)
     for (auto& s : ctx->sys)
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
@@ -1719,6 +1802,14 @@ int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_
         }
         s.upd.push_back(chain);
     }
+    return GC_OK;
+}
+
+int oracle_set_velocity_adjust(oracle_ctx* ctx, int inter, int kind, double epsilon) {
+    if (!ctx || inter < 0 || inter >= (int)ctx->inters.size()) return GC_ERR_ARG;
+    if (kind != GC_PFN_NONE && kind != GC_PFN_XSPH) return fail(ctx, GC_ERR_ARG, "velocity-adjust functor kind");
+    ctx->inters[inter].vk = kind;
+    ctx->inters[inter].veps = epsilon;
     return GC_OK;
 }
 

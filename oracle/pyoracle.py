@@ -50,6 +50,7 @@ def lib():
             "oracle_set_updaters": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _ip, _ip, _dp]),
             "oracle_set_integrator": (ct.c_int, [ct.c_void_p, ct.c_double]),
             "oracle_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int]),
+            "oracle_set_velocity_adjust": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double]),
             "oracle_set_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
             "oracle_get_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
             "oracle_get_count": (ct.c_int, [ct.c_void_p, ct.c_int, _i64p]),
@@ -163,6 +164,9 @@ class OracleBackend:
 
     def set_integrator(self, inst, gamma):
         self._chk(self.L.oracle_set_integrator(self.ctx, gamma), "set_integrator")
+
+    def set_velocity_adjust(self, inst, inter, kind, epsilon):
+        self._chk(self.L.oracle_set_velocity_adjust(self.ctx, inter, kind, epsilon), "set_velocity_adjust")
 
     def set_integrator_kind(self, inst, kind):
         self._chk(self.L.oracle_set_integrator_kind(self.ctx, kind), "set_integrator_kind")

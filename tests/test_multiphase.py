@@ -1,5 +1,5 @@
 """Two-sided FluidPfn between two fluid systems (multiphase) and the
-bubble scenarios (bubble.jl, bubble2.jl, bubble3.jl without XSPH).
+bubble scenarios (bubble.jl, bubble2.jl, bubble3.jl with its XSPH).
 
 The reference has no tests for this functor.  The known answers restate
 src/PairwiseFunctors.jl:173-190 with src/PairwisePhysics.jl:29-34 (artificial
