@@ -391,6 +391,7 @@ bool b_side_at(const DInter& D, int stage) {
     const int pk = D.pk[stage - 1];
     if (pk == GC_PFN_COUNT) return D.btype != BT_SELF && D.btype != BT_GHOST && D.bslot >= 0;
     if (pk == GC_PFN_XSPH) return D.btype != BT_SELF;
+    if (pk == GC_PFN_FLUID_SOLID) return true;
     return pk == GC_PFN_FLUID && D.two_fluid;
 }
 
@@ -400,7 +401,14 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     if (pk == GC_PFN_NONE) return GC_OK;
     if (pk == GC_PFN_XSPH)
         return seterr(ctx, GC_ERR_UNSUPPORTED, "XSPHPfn is swept as velocity_adjust_pairwise_fn, not as a stage");
-    if (pk < 0 || pk > GC_PFN_COUNT) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (pk < 0 || pk > GC_PFN_FLUID_SOLID) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (pk == GC_PFN_FLUID_SOLID) {
+        // only the two-sided (system, system) method exists, src/PairwiseFunctors.jl:494
+        if (a.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "FluidSolidPfn needs system_a's pressure");
+        if (it.b < 0 || I.handles[it.b].type != H_SYS)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "FluidSolidPfn needs a real system as system_b");
+        return GC_OK;
+    }
     if (pk == GC_PFN_FLUID && a.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "FluidPfn needs a pressure field");
     if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE) && a.kind < GC_SYS_STRESS)
         return seterr(ctx, GC_ERR_ARG, "functor needs a stress system");
@@ -753,6 +761,7 @@ int finalize(gc_ctx* ctx) {
                 gb[k].bc = sa.c;
                 gb[k].f_bmass = (float)sa.mass;
                 gb[k].f_bc = (float)sa.c;
+                gb[k].side_b = 1;
             }
             TRY(dalloc(ctx, &D.d_gi_b, (size_t)ninst));
             CU(cudaMemcpyAsync(D.d_gi_b, gb.data(), ninst * sizeof(GridInst), cudaMemcpyHostToDevice, ctx->stream));
@@ -777,7 +786,8 @@ int finalize(gc_ctx* ctx) {
                 per[k].has_eps = std::isnan(p[5]) ? 0 : 1;
                 per[k].eps = per[k].has_eps ? p[5] : 0.0;
                 per[k].f_eps = (float)per[k].eps;
-                per[k].two = D.two_fluid && D.pk[s] == GC_PFN_FLUID;
+                per[k].two = (D.two_fluid && D.pk[s] == GC_PFN_FLUID) || D.pk[s] == GC_PFN_FLUID_SOLID;
+                per[k].fs = D.pk[s] == GC_PFN_FLUID_SOLID;
             }
             TRY(dalloc(ctx, &D.d_pi[s], (size_t)ninst));
             CU(cudaMemcpyAsync(D.d_pi[s], per.data(), ninst * sizeof(PfnInst), cudaMemcpyHostToDevice, ctx->stream));
@@ -1368,7 +1378,9 @@ int xsph_ghost_side(gc_ctx* ctx, const ForceArgs& A, int id, int stage) {
 // Fused sweep of the interactions `ids` (same system_a, same functor kind).
 int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
     DSlot& S = ctx->slots[a];
-    int pfn = ctx->inters[ids[0]].pk[stage - 1];
+    const int pk0 = ctx->inters[ids[0]].pk[stage - 1];
+    // FluidSolidPfn runs the FluidPfn kernel in its fluid-solid mode (PfnInst.fs)
+    const int pfn = pk0 == GC_PFN_FLUID_SOLID ? GC_PFN_FLUID : pk0;
     const int mode = aux_mode_for(pfn);
     const bool xsph = pfn == GC_PFN_XSPH;  // writes v_adjustment; always FP64
     bool fp32 = ctx->precision == GC_PRECISION_FP32_COMPENSATED && pfn != GC_PFN_COUNT && !xsph && !count_only;
@@ -1421,7 +1433,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     if (ctx->force_cfg >= 0) {
         A.cfg = ctx->force_cfg;
     } else if (!count_only) {
-        const int64_t key = ((int64_t)a * 16 + stage) * 8 + pfn;
+        const int64_t key = ((int64_t)a * 16 + stage) * 8 + pk0;
         auto& t = ctx->tune[key];
         if (t.best >= 0) {
             A.cfg = t.best;
@@ -1498,7 +1510,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
                     r.bfp = pk_of(S.fpk, S.N, S.nd);
                     r.bxp = xp_of(S.fpk);
                 }
-            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT && !xsph && !fp32) {
+            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT && !xsph && !fp32 && pk0 != GC_PFN_FLUID_SOLID) {
                 launch_aux(mode, B.N, nullptr, B.F(F_RHO), B.F(F_P), B.inst_of, B.d_mass, B.aux, ctx->stream);
                 r.baux = B.aux;
             } else {
@@ -2413,8 +2425,8 @@ int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kerne
         it.pk.push_back(pfn_kinds[s]);
         std::array<double, GC_PFN_NPARAM> a;
         for (int k = 0; k < GC_PFN_NPARAM; ++k) a[k] = pfn_params[s * GC_PFN_NPARAM + k];
-        if (pfn_kinds[s] == GC_PFN_FLUID && !(a[3] == 1.0 || a[3] == 2.0))
-            return seterr(ctx, GC_ERR_UNSUPPORTED, "FluidPfn sigma must be 1 or 2");
+        if ((pfn_kinds[s] == GC_PFN_FLUID || pfn_kinds[s] == GC_PFN_FLUID_SOLID) && !(a[3] == 1.0 || a[3] == 2.0))
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "FluidPfn/FluidSolidPfn sigma must be 1 or 2");
         it.pp.push_back(a);
         int st = check_combo(ctx, I, it, pfn_kinds[s]);
         if (st) return st;

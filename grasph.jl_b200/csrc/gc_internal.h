@@ -52,6 +52,7 @@ struct GridInst {
     // system_b wrapper parameters (src/BoundaryParticles.jl)
     double normal[MAXD], point[MAXD], beta, ljcut;
     double bmass, bc;                  // system_b mass and sound speed
+    int side_b;                        // 1 in the system_b-side copy of a two-sided interaction
     // FP32 copies for the FP32-compensated sweep
     float f_invH, f_knorm, f_normal[MAXD], f_beta, f_ljcut, f_bmass, f_bc;
 };
@@ -60,7 +61,8 @@ struct GridInst {
 struct PfnInst {
     double alpha, beta, h, delta, eps;
     int S, has_delta, has_eps;
-    int two;  // FluidPfn between two fluid systems (both sides written)
+    int two;  // FluidPfn between two fluid systems, or FluidSolidPfn (both sides written)
+    int fs;   // FluidSolidPfn: system_a's (the fluid's) pressure on both sides
     float f_alpha, f_beta, f_h, f_h2eps, f_delta, f_eps;  // FP32 copies; h2eps = 0.01·h²
 };
 

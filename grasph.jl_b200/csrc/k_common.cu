@@ -640,9 +640,11 @@ __device__ void grid_plan_block(const GridPlanArgs& a) {
             GridInst& B = a.gi_b[k];
             const double bm = B.bmass, bc = B.bc;
             const float fbm = B.f_bmass, fbc = B.f_bc;
+            const int sb = B.side_b;
             B = a.gi[k];
             B.bmass = bm;
             B.bc = bc;
+            B.side_b = sb;
             B.f_bmass = fbm;
             B.f_bc = fbc;
         }

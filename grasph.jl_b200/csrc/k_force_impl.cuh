@@ -226,8 +226,20 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         // two-sided fluid x fluid :173 uses both sound speeds, one-sided :193 its own twice
         const double cb = P.two ? G.bc : ca;
         double piv = art_visc<ND>(dx, dv, rr, P.h, o.rho, rhoj, P.alpha, P.beta, ca, cb);
-        double auxj = r.baux[j];
-        double dh = P.S == 1 ? -(A.a_p[gi] + r.bp[j]) / (o.rho * rhoj) : -(o.aux + auxj);
+        double dh;
+        if (P.fs) {
+            // FluidSolidPfn :494-519: the fluid's pressure on both sides; the
+            // fluid is the neighbour on the system_b side
+            if (G.side_b) {
+                const double pf = r.bp[j];
+                dh = P.S == 1 ? -(pf + pf) / (o.rho * rhoj) : -(r.baux[j] + pf / (o.rho * o.rho));
+            } else {
+                const double pf = A.a_p[gi];
+                dh = P.S == 1 ? -(pf + pf) / (o.rho * rhoj) : -(o.aux + pf / (rhoj * rhoj));
+            }
+        } else {
+            dh = P.S == 1 ? -(A.a_p[gi] + r.bp[j]) / (o.rho * rhoj) : -(o.aux + r.baux[j]);
+        }
         double mj = r.btype == BT_SELF ? mass_a : G.bmass;
         if (P.two) {
             // dv_tmp = (dh + ast - piv)·gx, then mass_j·dv_tmp; the system_b side
@@ -672,7 +684,13 @@ struct PhysF32 {
         }
         const float mj = (self || dyn) ? ma : G.f_bmass;
         if (P2 == GC_PFN_FLUID) {
-            float dh = -(w.aux + auxj);
+            float dh;
+            if (two && P.fs) {  // the fluid's pressure p = (p/ρ²)·ρ² on both sides
+                if (G.side_b) dh = -(auxj + (auxj * rhoj * rhoj) * w.irho * w.irho);
+                else dh = -(w.aux + (w.aux * w.rho * w.rho) * irhoj * irhoj);
+            } else {
+                dh = -(w.aux + auxj);
+            }
             // artificial surface tension ε·(−(|p_i| + |p_j|)/(ρ_i ρ_j)), with
             // |p| = |p/ρ²|·ρ² from the record
             if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);

@@ -8,7 +8,7 @@ that ABI and moves host arrays in and out.
 from . import consts
 from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, CauchyFluidPfn,
                     CountingPfn, CubicSplineKernel, DynamicBoundarySystem, ElastoPlasticParticleSystem,
-                    ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn, GhostCopier, GhostEntry,
+                    ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn, FluidSolidPfn, GhostCopier, GhostEntry,
                     GhostParticleSystem, HookeLawStressUpdater, HouseholderReflect, LeapFrogTimeIntegrator, RK4TimeIntegrator,
                     LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
                     StressParticleSystem, SystemInteraction, TaitEOSUpdater, ViscoPlasticMCStressUpdater,

@@ -366,6 +366,30 @@ class FluidPfn(_Pfn):
         return p
 
 
+class FluidSolidPfn(_Pfn):
+    """Fluid against a linear-elastic solid, src/PairwiseFunctors.jl:463-519:
+    the two-sided fluid form with the fluid's (system_a's) pressure on both
+    sides.  Only the (system, system) method exists."""
+
+    kind = C.GC_PFN_FLUID_SOLID
+
+    def __init__(self, alpha, beta, h, *, sigma=2, delta=None):
+        self.art_visc_alpha = float(alpha)
+        self.art_visc_beta = float(beta)
+        self.h = float(h)
+        self.sigma = int(sigma)
+        if self.sigma not in (1, 2):
+            raise ArgumentError("FluidSolidPfn sigma must be 1 or 2 on the device path")
+        self.delta = None if delta is None else float(delta)
+
+    def params(self):
+        p = super().params()
+        p[0], p[1], p[2], p[3] = self.art_visc_alpha, self.art_visc_beta, self.h, self.sigma
+        if self.delta is not None:
+            p[4] = self.delta
+        return p
+
+
 class CauchyFluidPfn(_Pfn):
     """Cauchy-stress momentum + continuity, src/PairwiseFunctors.jl:252-355."""
 

@@ -20,6 +20,7 @@ import numpy as np
 
 from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, DynamicBoundarySystem,
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
+                    FluidSolidPfn, HookeLawStressUpdater,
                     GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator, LinearEOSUpdater,
                     RK4TimeIntegrator, StrainRatePfn, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
                     TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater)
@@ -227,6 +228,78 @@ def granular_column(nfx=100, nfy=50, dx=0.002, rho0=1850.0, E=0.84e6, nu=0.3, ph
     lf = LeapFrogTimeIntegrator([fluid, bottom], inters, ghosts=(gentry,))
     meta = dict(workload="granular_column", n_fluid=fluid.n, n_boundary=bottom.n, h=h, c0=c, cfl=cfl,
                 dt=cfl * h / c, ndims=2, phi=phi, E=E)
+    return lf, meta
+
+
+# ------------------------------------------------ dam break on an elastic wall
+
+def dambreak_wall(dx=0.5, nfx=50, nfy=50, cfl=0.05, x_wall=60.0):
+    """2-D dam break against a linear-elastic wall (DambreakWall.jl layout):
+    a 25 m x 25 m water column (Tait at stage 2), a 1.5 m x 10 m
+    ElastoPlasticParticleSystem wall (NS = 4, StrainRateVorticityPfn then
+    CauchyFluidPfn, Hooke stress update) standing on the floor at x = 60 m,
+    FluidSolidPfn from the water onto the wall, and four 3-layer dynamic
+    boundaries (floor, left, right, top).  `dx` scales the spacing; the
+    particle counts follow the script's extents; `x_wall` moves the wall
+    (next to the column, the fluid loads it from the first step)."""
+    g = (0.0, -9.81)
+    rho_w, c = 1000.0, 10.0 * math.sqrt(2.0 * 9.81 * 25.0)
+    alpha, beta = 0.02, 0.0
+    rho_s, E, nu = 2400.0, 5.0e8, 0.2
+    c_s = math.sqrt(E * (1 - nu) / (rho_s * (1 + nu) * (1 - 2 * nu)))
+    h = 1.2 * dx
+    fm = rho_w * dx * dx
+    fluid = FluidParticleSystem("fluid", nfx * nfy, 2, fm, c, source_v=g,
+                                state_updater=(None, TaitEOSUpdater(rho_w)))
+    jj, ii = np.meshgrid(np.arange(nfy), np.arange(nfx), indexing="ij")
+    fluid.x[:, 0] = (ii.ravel() + 0.5) * dx
+    fluid.x[:, 1] = (jj.ravel() + 0.5) * dx
+    fluid.rho[:] = rho_w
+    fluid.p[:] = _tait_pressure(fluid.rho, rho_w, c, 7.0)  # update_state!(fluid, 2)
+    nwx, nwy = int(round(1.5 / dx)), int(round(10.0 / dx))
+    wall = ElastoPlasticParticleSystem("wall", nwx * nwy, 2, 4, rho_s * dx * dx, c_s, source_v=g,
+                                       state_updater=(ZeroFieldUpdater("strain_rate", "vorticity"),
+                                                      HookeLawStressUpdater(E, nu)))
+    jj, ii = np.meshgrid(np.arange(nwy), np.arange(nwx), indexing="ij")
+    wall.x[:, 0] = x_wall + (ii.ravel() + 0.5) * dx
+    wall.x[:, 1] = (jj.ravel() + 0.5) * dx
+    wall.rho[:] = rho_s
+    x_right, y_top, layers = 75.0, 40.0, 3
+    nfl = int(round((76.25 + 1.25) / dx)) + 1
+    nly = int(round(40.0 / dx))
+
+    def layer_sys(name, pts):
+        ps = BasicParticleSystem(name, len(pts), 2, fm, c)
+        ps.x[:] = pts
+        ps.rho[:] = rho_w
+        return ps
+
+    floor = layer_sys("floor", np.array([(-1.25 + ix * dx, -(ly + 0.5) * dx)
+                                         for ly in range(layers) for ix in range(nfl)]))
+    left = layer_sys("left", np.array([(-(ly + 0.5) * dx, (iy + 0.5) * dx)
+                                       for ly in range(layers) for iy in range(nly)]))
+    right = layer_sys("right", np.array([(x_right + (ly + 0.5) * dx, (iy + 0.5) * dx)
+                                         for ly in range(layers) for iy in range(nly)]))
+    top = layer_sys("top", np.array([(-1.25 + ix * dx, y_top + (ly + 0.5) * dx)
+                                     for ly in range(layers) for ix in range(nfl)]))
+    floor_d = DynamicBoundarySystem(floor, (0.0, 1.0), (0.0, 0.0), 3.0)
+    left_d = DynamicBoundarySystem(left, (1.0, 0.0), (0.0, 0.0), 3.0)
+    right_d = DynamicBoundarySystem(right, (-1.0, 0.0), (x_right, 0.0), 3.0)
+    top_d = DynamicBoundarySystem(top, (0.0, -1.0), (0.0, y_top), 3.0)
+    kernel = CubicSplineKernel(h, ndims=2)
+    fpfn = FluidPfn(alpha, beta, h)
+    cau = CauchyFluidPfn(alpha, beta, h)
+    srv = StrainRateVorticityPfn()
+    inters = [SystemInteraction(kernel, (None, fpfn), fluid),
+              SystemInteraction(kernel, (srv, cau), wall),
+              SystemInteraction(kernel, (None, FluidSolidPfn(alpha, beta, h)), fluid, wall),
+              SystemInteraction(kernel, (None, fpfn), fluid, floor_d),
+              SystemInteraction(kernel, (None, fpfn), fluid, left_d),
+              SystemInteraction(kernel, (None, fpfn), fluid, right_d),
+              SystemInteraction(kernel, (None, fpfn), fluid, top_d),
+              SystemInteraction(kernel, (srv, cau), wall, floor_d)]
+    lf = LeapFrogTimeIntegrator([fluid, wall, floor, left, right, top], inters)
+    meta = dict(workload="dambreak_wall", n_fluid=fluid.n, n_wall=wall.n, h=h, c0=max(c, c_s), cfl=cfl, ndims=2)
     return lf, meta
 
 

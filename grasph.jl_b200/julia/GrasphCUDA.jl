@@ -42,15 +42,17 @@ pfn_kind(::FluidPfn) = 1
 pfn_kind(::CauchyFluidPfn) = 2
 pfn_kind(::StrainRatePfn) = 3
 pfn_kind(::StrainRateVorticityPfn) = 4
+pfn_kind(::FluidSolidPfn) = 7
 pfn_kind(f) = throw(ArgumentError("pairwise functor $(typeof(f)) has no device implementation"))
 
 function pfn_params(f)
     p = [0.0, 0.0, 0.0, 2.0, NaN, NaN]
     f === nothing && return p
-    if f isa FluidPfn || f isa CauchyFluidPfn
+    if f isa FluidPfn || f isa CauchyFluidPfn || f isa FluidSolidPfn
         p[1] = f.art_visc_alpha; p[2] = f.art_visc_beta; p[3] = f.h
         f.delta === nothing || (p[5] = f.delta)
     end
+    f isa FluidSolidPfn && (p[4] = typeof(f).parameters[1])
     if f isa FluidPfn
         p[4] = typeof(f).parameters[1]
         f.epsilon === nothing || (p[6] = f.epsilon)

@@ -93,11 +93,12 @@ enum {
     GC_PFN_STRAIN_RATE = 3,             /* StrainRatePfn :18                   */
     GC_PFN_STRAIN_RATE_VORTICITY = 4,   /* StrainRateVorticityPfn :78          */
     GC_PFN_COUNT = 5,
-    GC_PFN_XSPH = 6                     /* XSPHPfn :360-389; velocity-adjust functor only */
+    GC_PFN_XSPH = 6,                    /* XSPHPfn :360-389; velocity-adjust functor only */
+    GC_PFN_FLUID_SOLID = 7              /* FluidSolidPfn :479-519 (system_b a real system) */
 };
 /* Per-stage functor parameters, GC_PFN_NPARAM doubles each:
  *   [0] art_visc_alpha  [1] art_visc_beta  [2] h
- *   [3] sigma S (FluidPfn; 2 = Monaghan form)  [4] delta (NaN = nothing)
+ *   [3] sigma S (FluidPfn, FluidSolidPfn; 2 = Monaghan form)  [4] delta (NaN = nothing)
  *   [5] epsilon (NaN = nothing)                                            */
 #define GC_PFN_NPARAM 6
 

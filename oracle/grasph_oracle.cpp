@@ -579,6 +579,27 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
         for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + (s * gx[d] + rf * dx[d]);
         return;
     }
+    if (f.kind == GC_PFN_FLUID_SOLID) {
+        // FluidSolidPfn :494-519: the two-sided fluid form with the fluid's
+        // pressure p_i on both sides of the pressure term, no surface tension
+        Sys& bs = *b.sys;
+        double pi_ = a.p[i];
+        double dv[ND];
+        for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+        double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, bs.c);
+        double dh = pressure_coeff(pi_, pi_, ri, rj, f.S);
+        double c = dh - piv;
+        for (int d = 0; d < ND; ++d) {
+            double t = c * gx[d];
+            a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + b.mass * t;
+            bs.dvdt[j * ND + d] = bs.dvdt[j * ND + d] - a.mass * t;
+        }
+        double dr = dot<ND>(dv, gx);
+        double psi = diffusion<ND>(dx, ri, rj, a.c, bs.c, f.h, f.h, gx, f.delta, f.has_delta);
+        a.drhodt[i] = a.drhodt[i] + b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
+        bs.drhodt[j] = bs.drhodt[j] + a.mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri);
+        return;
+    }
     if (f.kind == GC_PFN_FLUID && b.type == H_SYS && a.kind == GC_SYS_FLUID && b.sys->kind == GC_SYS_FLUID) {
         // two-sided fluid x fluid (multiphase) :173-190: both systems' rates,
         // each side weighted by the other side's mass, mean sound speed
@@ -1321,7 +1342,13 @@ int make_view(oracle_ctx* ctx, int handle, BView* out) {
 int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     const Sys& a = ctx->sys[it.a];
     if (pk == GC_PFN_NONE) return GC_OK;
-    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_COUNT) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_FLUID_SOLID) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (pk == GC_PFN_FLUID_SOLID) {
+        // only the two-sided (system, system) method exists (:494)
+        if (!a.has_p()) return GC_ERR_ARG;
+        if (it.b < 0 || ctx->handles[it.b].type != H_SYS) return GC_ERR_UNSUPPORTED;
+        return GC_OK;
+    }
     if (pk == GC_PFN_FLUID && !a.has_p()) return GC_ERR_ARG;
     if ((pk == GC_PFN_CAUCHY_FLUID || pk == GC_PFN_STRAIN_RATE) && !a.has_stress()) return GC_ERR_ARG;
     if (pk == GC_PFN_STRAIN_RATE_VORTICITY && !a.is_ep()) return GC_ERR_ARG;

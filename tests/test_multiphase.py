@@ -179,3 +179,89 @@ def test_bubble_graph_steps_bit_identical(prec):
     for se, sg in zip(le.systems, lg.systems):
         for name, _ in se.particle_fields():
             assert np.array_equal(getattr(se, name), getattr(sg, name)), f"{se.name}.{name}"
+
+
+# ------------------------------------------------------------ FluidSolidPfn
+# src/PairwiseFunctors.jl:463-519: FluidPfn's two-sided form with the
+# fluid's (system_a's) pressure on both sides and no surface tension.
+
+def _fs_expected(a, b, h, sigma, delta, alpha=0.05, beta=0.02):
+    k = G.CubicSplineKernel(h, ndims=2)
+    dx = a.x[0] - b.x[0]
+    rr = dx[0] * dx[0] + dx[1] * dx[1]
+    r = math.sqrt(rr)
+    q = r / h
+    t2, t1 = max(0.0, 2 - q), max(0.0, 1 - q)
+    gx = k.norm_coeff * (-3.0 * (0.25 * t2 * t2 - t1 * t1)) / (r * h) * dx
+    dv = a.v[0] - b.v[0]
+    ri, rj, pf = a.rho[0], b.rho[0], a.p[0]
+    vr = min(dx[0] * dv[0] + dx[1] * dv[1], 0.0)
+    muv = h * vr / (rr + h * h * 0.01)
+    piv = (beta * muv - alpha * 0.5 * (a.c + b.c)) * muv / (0.5 * ri * rj)
+    dh = -(pf + pf) / (ri * rj) if sigma == 1 else -(pf / (ri * ri) + pf / (rj * rj))
+    tmp = (dh - piv) * gx
+    dr = dv[0] * gx[0] + dv[1] * gx[1]
+    psi = 0.0
+    if delta is not None:
+        psi = 2.0 * delta * (0.5 * (a.c + b.c)) * h * (ri - rj) * (dx[0] * gx[0] + dx[1] * gx[1]) / rr
+    ci, cj = (ri / rj, rj / ri) if sigma == 1 else (1.0, 1.0)
+    return (b.mass * tmp, -a.mass * tmp, b.mass * (dr * ci + psi / rj), a.mass * (dr * cj - psi / ri))
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+@pytest.mark.parametrize("sigma,delta", [(2, None), (1, None), (2, 0.1)])
+def test_fluid_solid_pair(be, sigma, delta):
+    h = 0.1
+    a = G.FluidParticleSystem("water", 1, 2, 2.5, 30.0)
+    b = G.ElastoPlasticParticleSystem("wall", 1, 2, 4, 6.0, 480.0)
+    a.x[0], b.x[0] = [0.0, 0.0], [0.07, 0.04]
+    a.v[0], b.v[0] = [0.3, -0.1], [-0.02, 0.01]
+    a.rho[0], b.rho[0] = 1010.0, 2400.0
+    a.p[0], b.p[0] = 1500.0, -9.0e5  # the wall's own pressure plays no part
+    si = G.SystemInteraction(G.CubicSplineKernel(h, ndims=2), G.FluidSolidPfn(0.05, 0.02, h, sigma=sigma, delta=delta),
+                             a, b)
+    lf, s = session(be, [a, b], [si])
+    s.create_grid(si)
+    s.sweep(si, 1)
+    s.pull()
+    dva, dvb, dra, drb = _fs_expected(a, b, h, sigma, delta)
+    np.testing.assert_allclose(a.dvdt[0], dva, rtol=1e-12)
+    np.testing.assert_allclose(b.dvdt[0], dvb, rtol=1e-12)
+    assert math.isclose(a.drhodt[0], dra, rel_tol=1e-12)
+    assert math.isclose(b.drhodt[0], drb, rel_tol=1e-12)
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+def test_fluid_solid_needs_a_real_system_b(be):
+    h = 0.1
+    a = G.FluidParticleSystem("water", 1, 2, 2.5, 30.0)
+    w = G.BasicParticleSystem("w", 1, 2, 1.0, 30.0)
+    dyn = G.DynamicBoundarySystem(w, (0.0, 1.0), (0.0, 0.0), 3.0)
+    si = G.SystemInteraction(G.CubicSplineKernel(h, ndims=2), G.FluidSolidPfn(0.05, 0.0, h), a, dyn)
+    with pytest.raises(Exception):
+        session(be, [a, w], [si])
+
+
+def test_dambreak_wall_layout():
+    lf, meta = scenarios.dambreak_wall()
+    assert [p.n for p in lf.systems] == [2500, 60, 468, 240, 240, 468]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nsteps,tol", [(1, 1e-10), (20, 1e-8)])
+@pytest.mark.parametrize("x_wall", [60.0, 25.0])
+def test_dambreak_wall_parity(nsteps, tol, x_wall):
+    lf_g, meta = scenarios.dambreak_wall(x_wall=x_wall)
+    lf_c, _ = scenarios.dambreak_wall(x_wall=x_wall)
+    _run(lf_g, "cuda", nsteps, meta["cfl"])
+    _run(lf_c, "oracle", nsteps, meta["cfl"])
+    _cmp(lf_g, lf_c, tol)
+
+
+@pytest.mark.gpu
+def test_dambreak_wall_fp32c():
+    lf_g, meta = scenarios.dambreak_wall(x_wall=25.0)
+    lf_c, _ = scenarios.dambreak_wall(x_wall=25.0)
+    _run(lf_g, "cuda", 20, meta["cfl"], prec=G.PRECISION_FP32_COMPENSATED)
+    _run(lf_c, "oracle", 20, meta["cfl"])
+    _cmp(lf_g, lf_c, 1e-4, rate_tol=1e-3)
