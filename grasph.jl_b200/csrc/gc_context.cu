@@ -44,8 +44,17 @@ struct HSys {
     double mass = 0, c = 0, srcv[3] = {0, 0, 0}, srcrho = 0;
     bool upd_set = false;
     std::vector<std::vector<HUpd>> upd;
+    bool vsrc = false;  // the source of a virtual system (not integrated)
 };
-enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3 };
+enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3, H_VIRT = 4 };
+// VirtualParticleSystem src/Particles.jl:476-528 over source system `src`
+struct HVirt {
+    int src = 0;
+    int zmask = 0;
+    double pv[3] = {0, 0, 0};
+    bool upd_set = false;
+    std::vector<std::vector<HUpd>> upd;
+};
 struct HHandle {
     int type = H_SYS, idx = 0;
     double normal[3] = {0, 0, 0}, point[3] = {0, 0, 0}, beta = 0, ljcut = 0;
@@ -76,6 +85,7 @@ struct HInst {
     std::vector<int> sys_handle;
     std::vector<HGhost> ghosts;
     std::vector<HInter> inters;
+    std::vector<HVirt> virts;
     double gamma = 0;
     int integ = GC_INTEGRATOR_LEAPFROG;
     double cfl = NAN;              // own CFL number (serving); NaN: gc_step's
@@ -105,6 +115,9 @@ struct DSlot {
     bool xpk_static = false;   // position copy of a system that does not move is current
     bool written = false;      // some functor writes this system
     bool moving = true;        // sorted and integrated every step
+    bool vsrc = false;         // source of a virtual system: never integrated
+    bool vmoves = false;       // a virtual system over it has a non-zero prescribed_v
+    bool xmoves() const { return moving || vmoves; }  // positions change every step
     bool sorted_once = false;  // static systems: sorted since the last upload
     std::vector<int64_t> nonzero_kin;  // per instance: uploaded v/dvdt/drhodt nonzero
     // updaters: [stage][chain] -> per-instance UpdInst device array
@@ -153,8 +166,26 @@ struct DGhost {
     int64_t need_slot = -1;  // index into need[] for its sort cells
 };
 
+// A virtual system on the device: its w_sum over the source slot's packed
+// particles, per-instance prescribed_v and updater chains.
+struct DVirt {
+    int src = 0;
+    int zmask = 0;
+    double* wsum = nullptr;
+    VirtInst* d_vi = nullptr;
+    bool moves = false;
+    bool upd_set = false;
+    int nupd = 0;
+    std::vector<std::vector<UpdInst*>> d_upd;
+    std::vector<std::vector<int>> upd_kind;
+};
+
+// system_b kinds of the host side; BT_VIRTUAL sweeps with the device's
+// one-sided boundary forms (BT_GHOST) over the source slot's arrays
+constexpr int BT_VIRTUAL = 5;
+
 struct DInter {
-    int a = 0, btype = BT_SELF, bslot = -1, bghost = -1, kk = 0, nstages = 0;
+    int a = 0, btype = BT_SELF, bslot = -1, bghost = -1, bvirt = -1, kk = 0, nstages = 0;
     bool two_sided = false;  // some stage writes system_b too (a second, system_b-side sweep)
     bool two_fluid = false;  // FluidPfn stages are the two-sided fluid x fluid form
     bool vadj = false;       // pk[nstages] is the velocity-adjust functor (XSPH)
@@ -208,6 +239,7 @@ struct gc_ctx {
     std::vector<DSlot> slots;
     std::vector<DGhost> ghosts;
     std::vector<DInter> inters;
+    std::vector<DVirt> virts;
     int nstages = 0;
     bool xsph = false;  // some interaction has a velocity-adjust functor: v_adjustment is carried
     // scratch
@@ -391,7 +423,7 @@ bool b_side_at(const DInter& D, int stage) {
     const int pk = D.pk[stage - 1];
     if (pk == GC_PFN_COUNT) return D.btype != BT_SELF && D.btype != BT_GHOST && D.bslot >= 0;
     if (pk == GC_PFN_XSPH) return D.btype != BT_SELF;
-    if (pk == GC_PFN_FLUID_SOLID) return true;
+    if (pk == GC_PFN_FLUID_SOLID || pk == GC_PFN_INTERPOLATE) return true;
     return pk == GC_PFN_FLUID && D.two_fluid;
 }
 
@@ -401,7 +433,19 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     if (pk == GC_PFN_NONE) return GC_OK;
     if (pk == GC_PFN_XSPH)
         return seterr(ctx, GC_ERR_UNSUPPORTED, "XSPHPfn is swept as velocity_adjust_pairwise_fn, not as a stage");
-    if (pk < 0 || pk > GC_PFN_FLUID_SOLID) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (pk < 0 || pk > GC_PFN_INTERPOLATE) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (pk == GC_PFN_INTERPOLATE) {
+        // the (real, virtual) method, src/PairwiseFunctors.jl:424; the fields exist on both sides
+        if (it.b < 0 || I.handles[it.b].type != H_VIRT)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "InterpolateFieldFn needs a virtual system as system_b");
+        const HSys& s = I.sys[I.virts[I.handles[it.b].idx].src];
+        const int m = (int)it.pp.back()[0];
+        if (m & ~((1 << GC_FIELD_V) | (1 << GC_FIELD_RHO) | (1 << GC_FIELD_STRESS)))
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "InterpolateFieldFn: fields other than v, rho, stress");
+        if ((m & (1 << GC_FIELD_STRESS)) && !(a.kind >= GC_SYS_STRESS && s.kind >= GC_SYS_STRESS && a.ns == s.ns))
+            return seterr(ctx, GC_ERR_ARG, "InterpolateFieldFn(:stress) needs stress of one size on both systems");
+        return GC_OK;
+    }
     if (pk == GC_PFN_FLUID_SOLID) {
         // only the two-sided (system, system) method exists, src/PairwiseFunctors.jl:494
         if (a.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "FluidSolidPfn needs system_a's pressure");
@@ -420,6 +464,15 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     }
     if (it.b < 0) return GC_OK;
     const HHandle& h = I.handles[it.b];
+    if (h.type == H_VIRT) {
+        // virtual system_b: the one-sided boundary forms (:193, :286, :37, :97)
+        const HSys& s = I.sys[I.virts[h.idx].src];
+        if (pk == GC_PFN_COUNT) return seterr(ctx, GC_ERR_UNSUPPORTED, "counting functor with a virtual system");
+        if (pk == GC_PFN_FLUID && s.kind < GC_SYS_FLUID) return seterr(ctx, GC_ERR_ARG, "system_b has no pressure field");
+        if (pk == GC_PFN_CAUCHY_FLUID && !(s.kind >= GC_SYS_STRESS && s.ns == a.ns))
+            return seterr(ctx, GC_ERR_ARG, "system_b has no stress of system_a's size");
+        return GC_OK;
+    }
     if (pk == GC_PFN_COUNT) return h.type == H_GHOST ? seterr(ctx, GC_ERR_UNSUPPORTED, "counting functor with ghosts") : GC_OK;
     if (h.type == H_DYN || h.type == H_STATIC) return GC_OK;
     if (h.type == H_GHOST) {
@@ -440,9 +493,20 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
 bool same_structure(const HInst& a, const HInst& b, std::string& why) {
     if (a.integ != b.integ) return why = "integrator kind", false;
     if (a.sys.size() != b.sys.size()) return why = "system count", false;
+    if (a.virts.size() != b.virts.size()) return why = "virtual systems", false;
+    for (size_t v = 0; v < a.virts.size(); ++v) {
+        const HVirt &x = a.virts[v], &y = b.virts[v];
+        if (x.src != y.src || x.zmask != y.zmask || x.upd_set != y.upd_set || x.upd.size() != y.upd.size())
+            return why = "virtual systems", false;
+        for (size_t t = 0; t < x.upd.size(); ++t) {
+            if (x.upd[t].size() != y.upd[t].size()) return why = "virtual updaters", false;
+            for (size_t q = 0; q < x.upd[t].size(); ++q)
+                if (x.upd[t][q].kind != y.upd[t][q].kind) return why = "virtual updaters", false;
+        }
+    }
     for (size_t s = 0; s < a.sys.size(); ++s) {
         const HSys &x = a.sys[s], &y = b.sys[s];
-        if (x.kind != y.kind || x.nd != y.nd || x.ns != y.ns) return why = "system kinds", false;
+        if (x.kind != y.kind || x.nd != y.nd || x.ns != y.ns || x.vsrc != y.vsrc) return why = "system kinds", false;
         if (x.upd_set != y.upd_set || x.upd.size() != y.upd.size()) return why = "updater tuples", false;
         for (size_t t = 0; t < x.upd.size(); ++t) {
             if (x.upd[t].size() != y.upd[t].size()) return why = "updater chains", false;
@@ -464,9 +528,12 @@ bool same_structure(const HInst& a, const HInst& b, std::string& why) {
         const HInter &x = a.inters[i], &y = b.inters[i];
         if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk || x.vk != y.vk)
             return why = "interactions", false;
-        for (int s = 0; s < x.nstages; ++s)
+        for (int s = 0; s < x.nstages; ++s) {
             if (x.pp[s][3] != y.pp[s][3] || std::isnan(x.pp[s][4]) != std::isnan(y.pp[s][4]))
                 return why = "functor variants", false;
+            if (x.pk[s] == GC_PFN_INTERPOLATE && (x.pp[s][0] != y.pp[s][0] || x.pp[s][1] != y.pp[s][1]))
+                return why = "interpolated fields", false;
+        }
     }
     return true;
 }
@@ -535,6 +602,8 @@ int finalize(gc_ctx* ctx) {
         D.ns = h0.ns;
         D.nvort = h0.nvort;
         D.kind = h0.kind;
+        D.vsrc = h0.vsrc;
+        D.moving = !D.vsrc;
         D.h_inst.resize(ninst);
         D.nonzero_kin.assign(ninst, 0);
         int64_t base = 0;
@@ -617,6 +686,45 @@ int finalize(gc_ctx* ctx) {
             }
         }
         // Host-side copies must outlive the async copies above.
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+
+    // ---- virtual systems
+    ctx->virts.resize(I0.virts.size());
+    for (size_t v = 0; v < I0.virts.size(); ++v) {
+        DVirt& V = ctx->virts[v];
+        const HVirt& h0 = I0.virts[v];
+        DSlot& S = ctx->slots[h0.src];
+        V.src = h0.src;
+        V.zmask = h0.zmask;
+        V.upd_set = h0.upd_set;
+        V.nupd = (int)h0.upd.size();
+        TRY(dalloc(ctx, &V.wsum, (size_t)std::max<int64_t>(S.N, 1)));
+        CU(cudaMemsetAsync(V.wsum, 0, sizeof(double) * std::max<int64_t>(S.N, 1), ctx->stream));
+        std::vector<VirtInst> vi(ninst);
+        for (int k = 0; k < ninst; ++k) {
+            const HVirt& h = ctx->inst[k].virts[v];
+            for (int d = 0; d < MAXD; ++d) {
+                vi[k].pv[d] = d < S.nd ? h.pv[d] : 0.0;
+                V.moves |= vi[k].pv[d] != 0.0;
+            }
+        }
+        S.vmoves |= V.moves;
+        TRY(dalloc(ctx, &V.d_vi, (size_t)ninst));
+        CU(cudaMemcpyAsync(V.d_vi, vi.data(), ninst * sizeof(VirtInst), cudaMemcpyHostToDevice, ctx->stream));
+        V.d_upd.resize(h0.upd.size());
+        V.upd_kind.resize(h0.upd.size());
+        for (size_t t = 0; t < h0.upd.size(); ++t)
+            for (size_t q = 0; q < h0.upd[t].size(); ++q) {
+                std::vector<UpdInst> per(ninst);
+                for (int k = 0; k < ninst; ++k)
+                    per[k] = make_upd(ctx->inst[k].virts[v].upd[t][q], ctx->inst[k].sys[h0.src]);
+                UpdInst* d = nullptr;
+                TRY(dalloc(ctx, &d, (size_t)ninst));
+                CU(cudaMemcpyAsync(d, per.data(), ninst * sizeof(UpdInst), cudaMemcpyHostToDevice, ctx->stream));
+                V.d_upd[t].push_back(d);
+                V.upd_kind[t].push_back(h0.upd[t][q].kind);
+            }
         CU(cudaStreamSynchronize(ctx->stream));
     }
 
@@ -707,6 +815,10 @@ int finalize(gc_ctx* ctx) {
             if (hh.type == H_GHOST) {
                 D.btype = BT_GHOST;
                 D.bghost = hh.idx;
+            } else if (hh.type == H_VIRT) {
+                D.btype = BT_VIRTUAL;
+                D.bvirt = hh.idx;
+                D.bslot = I0.virts[hh.idx].src;
             } else {
                 D.btype = hh.type == H_DYN ? BT_DYNAMIC : hh.type == H_STATIC ? BT_STATIC : BT_SYSTEM;
                 D.bslot = hh.idx;
@@ -739,8 +851,8 @@ int finalize(gc_ctx* ctx) {
                 for (int d = 0; d < 3; ++d) G.f_normal[d] = (float)hh.normal[d];
                 G.f_beta = (float)hh.beta;
                 G.f_ljcut = (float)hh.ljcut;
-                if (hh.type == H_GHOST) {
-                    const HSys& src = I.sys[I.ghosts[hh.idx].src];
+                if (hh.type == H_GHOST || hh.type == H_VIRT) {
+                    const HSys& src = I.sys[hh.type == H_GHOST ? I.ghosts[hh.idx].src : I.virts[hh.idx].src];
                     G.bmass = src.mass;
                     G.bc = src.c;
                 } else {
@@ -1167,7 +1279,7 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     // bounding boxes of every real system (positions are current); a system
     // that does not move keeps the box computed after its last upload
     for (auto& S : ctx->slots)
-        if (S.moving || !S.sorted_once) TRY(bbox_slot(ctx, S));
+        if (S.xmoves() || !S.sorted_once) TRY(bbox_slot(ctx, S));
     for (size_t s = 0; s < ctx->slots.size(); ++s)
         if (sort_mask[s])
             launch_sort_plan(ctx->slots[s].d_inst, ni, ctx->slots[s].nd, ctx->d_need + s, ctx->d_err, ctx->stream);
@@ -1255,6 +1367,52 @@ int run_updaters(gc_ctx* ctx, DSlot& S, int stage, double dt_override) {
         launch_update(a, ctx->stream);
     }
     return check_launch(ctx, "updater");
+}
+
+// A virtual system's updater chain for `stage` on its source's fields.
+int run_virtual_updaters(gc_ctx* ctx, DVirt& V, int stage) {
+    if (stage < 1 || stage > (int)V.d_upd.size()) return GC_OK;
+    DSlot& S = ctx->slots[V.src];
+    for (size_t q = 0; q < V.d_upd[stage - 1].size(); ++q) {
+        const int kind = V.upd_kind[stage - 1][q];
+        if (kind == GC_UPD_VIRTUAL_NORM || kind == GC_UPD_PRESCRIBED_V) {
+            VirtArgs a{};
+            a.N = S.N;
+            a.nd = S.nd;
+            a.ns = S.ns;
+            a.kind = kind;
+            a.inst_of = S.inst_of;
+            a.vi = V.d_vi;
+            a.u = V.d_upd[stage - 1][q];
+            a.v = S.F(F_V);
+            a.rho = S.F(F_RHO);
+            a.p = S.ncomp[F_P] ? S.F(F_P) : nullptr;
+            a.stress = S.ncomp[F_STRESS] ? S.F(F_STRESS) : nullptr;
+            a.wsum = V.wsum;
+            launch_virtual_update(a, ctx->stream);
+        } else {
+            UpdArgs a{};
+            a.N = S.N;
+            a.nd = S.nd;
+            a.ns = S.ns;
+            a.nvort = S.nvort;
+            a.inst_of = S.inst_of;
+            a.inst = S.d_inst;
+            a.u = V.d_upd[stage - 1][q];
+            a.dt = NAN;
+            a.rho = S.F(F_RHO);
+            a.p = S.F(F_P);
+            a.stress = S.F(F_STRESS);
+            a.sr = S.F(F_SR);
+            a.vort = S.F(F_VORT);
+            a.strain = S.F(F_STRAIN);
+            a.strainp = S.F(F_STRAINP);
+            a.dvdt = S.F(F_DVDT);
+            a.drhodt = S.F(F_DRHODT);
+            launch_update(a, ctx->stream);
+        }
+    }
+    return check_launch(ctx, "virtual updater");
 }
 
 int ghost_kinematics(gc_ctx* ctx, DGhost& G) {
@@ -1375,10 +1533,74 @@ int xsph_ghost_side(gc_ctx* ctx, const ForceArgs& A, int id, int stage) {
     return check_launch(ctx, "sweep (XSPH ghost side)");
 }
 
+// InterpolateFieldFn stages (system_b virtual): nothing is written on the
+// system_a side, so each interaction is one gather over the virtual system's
+// source particles through system_a's CSR on the interaction's grid,
+// accumulating into the source's fields and the virtual system's w_sum.
+int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
+    DSlot& S = ctx->slots[a];
+    for (int id : ids) {
+        DInter& D = ctx->inters[id];
+        DSlot& B = ctx->slots[D.bslot];
+        DVirt& V = ctx->virts[D.bvirt];
+        if (!D.grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
+        TRY(ensure_csa(ctx, D));
+        TRY(ensure_groups(ctx, D.bslot, id, true));
+        const auto& prm = ctx->inst[0].inters[id].pp[stage - 1];
+        ForceArgs R{};
+        R.nd = B.nd;
+        R.ns = B.ns;
+        R.pfn = GC_PFN_INTERPOLATE;
+        R.kk = D.kk;
+        R.aN = B.N;
+        R.a_inst_of = B.inst_of;
+        R.ax = B.F(F_X);
+        R.av = B.F(F_V);
+        R.arho = B.F(F_RHO);
+        R.astress = B.F(F_STRESS);
+        R.a_p = B.F(F_P);
+        R.advdt = B.F(F_V);        // accumulation targets: v, rho, stress, w_sum
+        R.adrhodt = B.F(F_RHO);
+        R.asr = B.F(F_STRESS);
+        R.avort = V.wsum;
+        R.a_c = B.d_c;
+        R.a_mass = B.d_mass;
+        R.a_cf = B.d_cf;
+        R.a_massf = B.d_massf;
+        R.prec = GC_PRECISION_FP64;
+        R.err = ctx->d_err;
+        R.groups = B.groups;
+        R.ngroups = B.d_ngroups;
+        R.num_sms = ctx->num_sms;
+        R.cfg = ctx->force_cfg >= 0 ? ctx->force_cfg : 0;
+        R.imask = (int)prm[0];
+        R.iwsum = prm[1] != 0.0 ? 1 : 0;
+        R.nref = 1;
+        InterRef& r = R.ref[0];
+        r.btype = BT_SYSTEM;
+        r.bbox = S.d_inst;
+        r.gi = D.d_gi_b;
+        r.pi = D.d_pi[stage - 1];
+        r.cs = D.cs_a;
+        r.cs_cells = D.cells;
+        r.bx = S.F(F_X);
+        r.bv = S.F(F_V);
+        r.brho = S.F(F_RHO);
+        r.bp = S.F(F_P);
+        r.bstress = S.F(F_STRESS);
+        r.bN = S.N;
+        int st = launch_force_f64(R, false, ctx->stream);
+        if (st) return seterr(ctx, st, "InterpolateFieldFn not implemented on the device for this system");
+        TRY(check_launch(ctx, "sweep (interpolation)"));
+    }
+    return GC_OK;
+}
+
 // Fused sweep of the interactions `ids` (same system_a, same functor kind).
 int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
     DSlot& S = ctx->slots[a];
     const int pk0 = ctx->inters[ids[0]].pk[stage - 1];
+    if (pk0 == GC_PFN_INTERPOLATE && !count_only) return interp_sweeps(ctx, a, ids, stage);
     // FluidSolidPfn runs the FluidPfn kernel in its fluid-solid mode (PfnInst.fs)
     const int pfn = pk0 == GC_PFN_FLUID_SOLID ? GC_PFN_FLUID : pk0;
     const int mode = aux_mode_for(pfn);
@@ -1462,7 +1684,7 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         if (!D.grid_valid) return seterr(ctx, GC_ERR_STATE, "sweep before create_grid");
         if (A.nref == MAX_REFS) return seterr(ctx, GC_ERR_UNSUPPORTED, "too many interactions on one system");
         InterRef& r = A.ref[A.nref++];
-        r.btype = D.btype;
+        r.btype = D.btype == BT_VIRTUAL ? BT_GHOST : D.btype;  // virtual: the one-sided boundary forms
         r.gi = D.d_gi;
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs;
@@ -1510,7 +1732,8 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
                     r.bfp = pk_of(S.fpk, S.N, S.nd);
                     r.bxp = xp_of(S.fpk);
                 }
-            } else if (D.btype == BT_SYSTEM && pfn != GC_PFN_COUNT && !xsph && !fp32 && pk0 != GC_PFN_FLUID_SOLID) {
+            } else if ((D.btype == BT_SYSTEM || D.btype == BT_VIRTUAL) && pfn != GC_PFN_COUNT && !xsph && !fp32 &&
+                       pk0 != GC_PFN_FLUID_SOLID) {
                 launch_aux(mode, B.N, nullptr, B.F(F_RHO), B.F(F_P), B.inst_of, B.d_mass, B.aux, ctx->stream);
                 r.baux = B.aux;
             } else {
@@ -1518,15 +1741,15 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
             }
             if (fp32 && D.btype != BT_SELF) {
                 // dynamic walls lend only their positions; other systems their records too
-                const bool rec = D.btype == BT_SYSTEM || D.btype == BT_STATIC;
+                const bool rec = D.btype == BT_SYSTEM || D.btype == BT_STATIC || D.btype == BT_VIRTUAL;
                 TRY(ensure_fpk(ctx, B, B.N, B.nd, pk_ns));
                 // positions: once per step, once for good for a system that does not move
-                const bool pos = B.moving ? B.xpk_epoch != ctx->pack_epoch : !B.xpk_static;
+                const bool pos = B.xmoves() ? B.xpk_epoch != ctx->pack_epoch : !B.xpk_static;
                 launch_pack32(mode, B.N, nullptr, B.nd, pk_ns, B.F(F_X), B.F(F_V), B.F(F_RHO), B.F(F_P),
                               B.kind >= GC_SYS_STRESS ? B.F(F_STRESS) : nullptr, B.inst_of, B.d_mass,
                               pos ? xp_of(B.fpk) : nullptr, rec ? pk_of(B.fpk, B.N, B.nd) : nullptr, ctx->stream);
                 B.xpk_epoch = ctx->pack_epoch;
-                if (!B.moving) B.xpk_static = true;
+                if (!B.xmoves()) B.xpk_static = true;
                 r.bxp = xp_of(B.fpk);
                 if (rec) r.bfp = pk_of(B.fpk, B.N, B.nd);
             }
@@ -1642,7 +1865,8 @@ void upload_inst_params(gc_ctx* ctx, double cfl) {
         const HInst& I = ctx->inst[k];
         double h = 1e300, c = -1e300;
         for (auto& it : I.inters) h = std::min(h, it.H);
-        for (auto& s : I.sys) c = std::max(c, s.c);
+        for (auto& s : I.sys)
+            if (!s.vsrc) c = std::max(c, s.c);  // the integrator's systems (src/TimeIntegration.jl:63)
         double dt = (std::isfinite(I.cfl) ? I.cfl : cfl) * h / c;
         for (auto& S : ctx->slots) {
             S.h_inst[k].dt = dt;
@@ -1685,7 +1909,8 @@ bool decide_motion(gc_ctx* ctx) {
         }
         bool kin_zero = true;
         for (auto v : S.nonzero_kin) kin_zero &= v == 0;
-        const bool m = S.written || !src_zero || !kin_zero;
+        // a virtual system's source is not one of the integrator's systems
+        const bool m = !S.vsrc && (S.written || !src_zero || !kin_zero);
         changed |= m != S.moving;
         S.moving = m;
     }
@@ -1693,6 +1918,40 @@ bool decide_motion(gc_ctx* ctx) {
 }
 
 int one_step_rk4(gc_ctx* ctx);
+
+// _sweep_all_stages! src/TimeIntegration.jl:401-419: the virtual systems'
+// w_sum and zero_fields cleared, then per stage the systems' updaters, the
+// ghosts' copiers, the virtual systems' updaters and the sweeps.
+int sweep_all_stages(gc_ctx* ctx) {
+    for (auto& V : ctx->virts) {
+        DSlot& S = ctx->slots[V.src];
+        CU(cudaMemsetAsync(V.wsum, 0, sizeof(double) * S.N, ctx->stream));
+        for (int f = 0; f < GC_NFIELDS; ++f) {
+            if (!(V.zmask & (1 << f))) continue;
+            const int k = field_slot(f);
+            if (k >= 0 && S.ncomp[k]) CU(cudaMemsetAsync(S.F(k), 0, sizeof(double) * S.ncomp[k] * S.N, ctx->stream));
+        }
+    }
+    for (int stage = 1; stage <= ctx->nstages; ++stage) {
+        for (auto& S : ctx->slots)
+            if (!S.vsrc && S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
+        for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
+        for (auto& V : ctx->virts)
+            if (V.upd_set && V.nupd == ctx->nstages) TRY(run_virtual_updaters(ctx, V, stage));
+        TRY(sweep_stage(ctx, stage));
+    }
+    return GC_OK;
+}
+
+// _update_virtual_positions! :389-397, one virtual system after another
+int advance_virtuals(gc_ctx* ctx) {
+    for (auto& V : ctx->virts) {
+        if (!V.moves) continue;  // x += 0·dt leaves x as it is
+        DSlot& S = ctx->slots[V.src];
+        launch_virtual_advance(S.F(F_X), S.N, S.nd, S.inst_of, S.d_inst, V.d_vi, ctx->stream);
+    }
+    return check_launch(ctx, "virtual positions");
+}
 
 // _xsph_correction! src/TimeIntegration.jl:421-436 after the full step has
 // subtracted and zeroed v_adjustment: adjust_v! of every interaction with a
@@ -1720,7 +1979,7 @@ int one_step(gc_ctx* ctx) {
     std::vector<char> mask(ctx->slots.size());
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
-        mask[s] = S.moving || !S.sorted_once;
+        mask[s] = S.xmoves() || !S.sorted_once;
     }
     TRY(prepare(ctx, mask));
     for (size_t s = 0; s < ctx->slots.size(); ++s)
@@ -1730,16 +1989,12 @@ int one_step(gc_ctx* ctx) {
         if (S.moving) launch_halfstep(step_args(S), ctx->stream);
     TRY(check_launch(ctx, "half step"));
     for (auto& G : ctx->ghosts) TRY(ghost_kinematics(ctx, G));
-    for (int stage = 1; stage <= ctx->nstages; ++stage) {
-        for (auto& S : ctx->slots)
-            if (S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
-        for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
-        TRY(sweep_stage(ctx, stage));
-    }
+    TRY(sweep_all_stages(ctx));
     for (auto& S : ctx->slots)
         if (S.moving) launch_fullstep(step_args(S), ctx->stream);
     TRY(check_launch(ctx, "full step"));
     if (ctx->xsph) TRY(xsph_pass(ctx));
+    TRY(advance_virtuals(ctx));
     ctx->steps_done += 1;
     return GC_OK;
 }
@@ -1751,7 +2006,7 @@ int one_step_rk4(gc_ctx* ctx) {
     std::vector<char> mask(ctx->slots.size());
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
-        mask[s] = S.moving || !S.sorted_once;
+        mask[s] = S.xmoves() || !S.sorted_once;
         if (S.moving && !S.accv) {
             TRY(dalloc(ctx, &S.accv, (size_t)S.nd * S.N));
             TRY(dalloc(ctx, &S.accrho, (size_t)S.N));
@@ -1772,12 +2027,7 @@ int one_step_rk4(gc_ctx* ctx) {
                 if (S.moving) launch_rk4_advance(step_args(S), advance[it], ctx->stream);
         TRY(check_launch(ctx, "rk4 stage"));
         for (auto& G : ctx->ghosts) TRY(ghost_kinematics(ctx, G));
-        for (int stage = 1; stage <= ctx->nstages; ++stage) {
-            for (auto& S : ctx->slots)
-                if (S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
-            for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
-            TRY(sweep_stage(ctx, stage));
-        }
+        TRY(sweep_all_stages(ctx));
         for (auto& S : ctx->slots)
             if (S.moving) launch_rk4_acc(step_args(S), weight[it], ctx->stream);
     }
@@ -1785,6 +2035,7 @@ int one_step_rk4(gc_ctx* ctx) {
         if (S.moving) launch_rk4_final(step_args(S), ctx->stream);
     TRY(check_launch(ctx, "rk4 final"));
     if (ctx->xsph) TRY(xsph_pass(ctx));
+    TRY(advance_virtuals(ctx));
     ctx->steps_done += 1;
     return GC_OK;
 }
@@ -1937,7 +2188,7 @@ int snapshot(gc_ctx* ctx, std::vector<char>& par) {
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
         Snapshot& sn = ctx->snaps[s];
-        if (!S.moving) continue;
+        if (!S.xmoves()) continue;
         if (sn.n != S.N) {
             for (int f = 0; f < NF; ++f) dfree(ctx, sn.f[f], (size_t)S.ncomp[f] * sn.n);
             dfree(ctx, sn.id, (size_t)sn.n);
@@ -1962,7 +2213,7 @@ int restore(gc_ctx* ctx, const std::vector<char>& par) {
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
         Snapshot& sn = ctx->snaps[s];
-        if (!S.moving) continue;
+        if (!S.xmoves()) continue;
         for (int f = 0; f < NF; ++f)
             if (S.ncomp[f])
                 CU(cudaMemcpyAsync(S.F(f), sn.f[f], sizeof(double) * S.ncomp[f] * S.N, cudaMemcpyDeviceToDevice,
@@ -2233,6 +2484,12 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(G.goff);
         cudaFree(G.gadj);
     }
+    for (auto& V : ctx->virts) {
+        cudaFree(V.wsum);
+        cudaFree(V.d_vi);
+        for (auto& chain : V.d_upd)
+            for (auto* p : chain) cudaFree(p);
+    }
     for (auto& D : ctx->inters) {
         cudaFree(D.d_gi);
         cudaFree(D.d_gi_b);
@@ -2436,6 +2693,31 @@ int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kerne
     return GC_OK;
 }
 
+int gc_add_virtual(gc_ctx* ctx, int inst, int src_sys, int zero_mask, const double* prescribed_v,
+                   int* handle_out) {
+    if (!ctx || !handle_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    int si = sys_of(ctx, inst, src_sys);
+    if (si < 0) return seterr(ctx, GC_ERR_ARG, "a virtual system needs a source system handle");
+    HInst& I = ctx->inst[inst];
+    const int allowed = (1 << GC_FIELD_V) | (1 << GC_FIELD_RHO) | (1 << GC_FIELD_P) | (1 << GC_FIELD_STRESS) |
+                        (1 << GC_FIELD_DVDT) | (1 << GC_FIELD_DRHODT) | (1 << GC_FIELD_STRAIN_RATE);
+    if (zero_mask & ~allowed) return seterr(ctx, GC_ERR_UNSUPPORTED, "zero_fields outside v, rho, p, stress, rates");
+    HVirt v;
+    v.src = si;
+    v.zmask = zero_mask;
+    if (prescribed_v)
+        for (int d = 0; d < I.sys[si].nd; ++d) v.pv[d] = prescribed_v[d];
+    I.sys[si].vsrc = true;
+    I.virts.push_back(v);
+    HHandle h;
+    h.type = H_VIRT;
+    h.idx = (int)I.virts.size() - 1;
+    I.handles.push_back(h);
+    *handle_out = (int)I.handles.size() - 1;
+    return GC_OK;
+}
+
 int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double epsilon) {
     if (!ctx) return GC_ERR_ARG;
     if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
@@ -2453,6 +2735,28 @@ int gc_set_updaters(gc_ctx* ctx, int inst, int sys, int nstages, const int* chai
                     const double* params) {
     if (!ctx) return GC_ERR_ARG;
     if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    if (valid_inst(ctx, inst) && sys >= 0 && sys < (int)ctx->inst[inst].handles.size() &&
+        ctx->inst[inst].handles[sys].type == H_VIRT) {
+        HVirt& vp = ctx->inst[inst].virts[ctx->inst[inst].handles[sys].idx];
+        vp.upd.clear();
+        vp.upd_set = true;
+        int pos = 0;
+        for (int st = 0; st < nstages; ++st) {
+            if (chain_len[st] > GC_UPD_MAX_CHAIN) return seterr(ctx, GC_ERR_UNSUPPORTED, "updater chain too long");
+            std::vector<HUpd> chain;
+            for (int k = 0; k < chain_len[st]; ++k, ++pos) {
+                HUpd u;
+                u.kind = kinds[pos];
+                for (int q = 0; q < GC_UPD_NPARAM; ++q) u.prm[q] = params[pos * GC_UPD_NPARAM + q];
+                if (u.kind != GC_UPD_NONE && u.kind != GC_UPD_ZERO_FIELDS && u.kind != GC_UPD_VIRTUAL_NORM &&
+                    u.kind != GC_UPD_PRESCRIBED_V)
+                    return seterr(ctx, GC_ERR_UNSUPPORTED, "updater kind %d on a virtual system", u.kind);
+                if (u.kind != GC_UPD_NONE) chain.push_back(u);
+            }
+            vp.upd.push_back(chain);
+        }
+        return GC_OK;
+    }
     int si = sys_of(ctx, inst, sys);
     if (si < 0) return seterr(ctx, GC_ERR_ARG, "updaters need a system handle");
     HSys& s = ctx->inst[inst].sys[si];
@@ -2473,6 +2777,8 @@ int gc_set_updaters(gc_ctx* ctx, int inst, int sys, int nstages, const int* chai
                 return seterr(ctx, GC_ERR_ARG, "EOS updater needs a pressure field");
             if (u.kind == GC_UPD_VISCOPLASTIC_MC && (s.kind < GC_SYS_STRESS || (s.ns != 3 && s.ns != 4 && s.ns != 6)))
                 return seterr(ctx, GC_ERR_ARG, "ViscoPlasticMCStressUpdater needs stress with NS = 3, 4 or 6");
+            if (u.kind == GC_UPD_VIRTUAL_NORM || u.kind == GC_UPD_PRESCRIBED_V)
+                return seterr(ctx, GC_ERR_ARG, "this updater acts on a virtual system");
             if (u.kind < GC_UPD_NONE || u.kind > GC_UPD_VISCOPLASTIC_MC) return seterr(ctx, GC_ERR_ARG, "bad updater kind");
             if (u.kind != GC_UPD_NONE) chain.push_back(u);
         }
@@ -2593,6 +2899,7 @@ static int ghost_field_io(gc_ctx* ctx, int inst, DGhost& G, int field, void* hos
 struct HandleRef {
     DSlot* slot = nullptr;
     DGhost* ghost = nullptr;
+    DVirt* virt = nullptr;
     int sys = -1;
 };
 
@@ -2602,8 +2909,12 @@ static int resolve(gc_ctx* ctx, int inst, int handle, HandleRef* r) {
     HInst& I = ctx->inst[inst];
     if (handle < 0 || handle >= (int)I.handles.size()) return seterr(ctx, GC_ERR_ARG, "bad handle");
     const HHandle& h = I.handles[handle];
-    if (h.type == H_GHOST) r->ghost = &ctx->ghosts[h.idx];
-    else {
+    if (h.type == H_GHOST) {
+        r->ghost = &ctx->ghosts[h.idx];
+    } else if (h.type == H_VIRT) {
+        r->virt = &ctx->virts[h.idx];
+        r->sys = ctx->virts[h.idx].src;
+    } else {
         r->slot = &ctx->slots[h.idx];
         r->sys = h.idx;
     }
@@ -2641,6 +2952,7 @@ int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
         if (!f.host) return seterr(ctx, GC_ERR_ARG, "null host buffer");
         TRY(resolve(ctx, f.inst, f.handle, &ref[q]));
         if (ref[q].ghost) return seterr(ctx, GC_ERR_ARG, "ghost fields are generated on the device");
+        if (ref[q].virt) return seterr(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
         const HSys& hs = ctx->inst[f.inst].sys[ref[q].sys];
         comps[q] = sys_comps(hs, f.field);
         if (comps[q] < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", f.field);
@@ -2719,6 +3031,13 @@ int gc_download_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
         TRY(resolve(ctx, f.inst, f.handle, &ref[q]));
         if (ref[q].ghost) continue;
         const HSys& hs = ctx->inst[f.inst].sys[ref[q].sys];
+        if (ref[q].virt) {  // a virtual system holds only w_sum; its fields are its source's
+            if (f.field != GC_FIELD_W_SUM) return seterr(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
+            if (f.bytes != (size_t)(hs.n * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", f.bytes);
+            comps[q] = 1;
+            total += hs.n;
+            continue;
+        }
         comps[q] = sys_comps(hs, f.field);
         if (comps[q] < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", f.field);
         if (f.bytes != (size_t)(hs.n * comps[q] * 8))
@@ -2730,10 +3049,14 @@ int gc_download_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
     for (int q = 0; q < nio; ++q) {
         const gc_field_io& f = io[q];
         if (ref[q].ghost) continue;
-        DSlot& S = *ref[q].slot;
+        DSlot& S = ref[q].virt ? ctx->slots[ref[q].virt->src] : *ref[q].slot;
         const int64_t n = ctx->inst[f.inst].sys[ref[q].sys].n, base = S.h_inst[f.inst].base;
         double* st = ctx->staging + off;
         off += n * comps[q];
+        if (ref[q].virt) {
+            if (n) CU(cudaMemcpyAsync(f.host, ref[q].virt->wsum + base, f.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+            continue;
+        }
         if (f.field == GC_FIELD_V_ADJUSTMENT && !S.ncomp[F_VADJ]) {  // not carried: zero
             memset(f.host, 0, f.bytes);
             continue;
@@ -2766,7 +3089,7 @@ int gc_get_count(gc_ctx* ctx, int inst, int handle, int64_t* n_out) {
         TRY(hcopy(ctx, gh.data(), r.ghost->d_gh, gh.size() * sizeof(GhostInst), cudaMemcpyDeviceToHost));
         *n_out = gh[inst].n;
     } else {
-        *n_out = ctx->inst[inst].sys[r.sys].n;
+        *n_out = ctx->inst[inst].sys[r.sys].n;  // a virtual system: its source's count
     }
     return GC_OK;
 }
@@ -2979,6 +3302,10 @@ int gc_update_state(gc_ctx* ctx, int inst, int sys, int stage, double dt) {
     if (!ctx) return GC_ERR_ARG;
     HandleRef r;
     TRY(resolve(ctx, inst, sys, &r));
+    if (r.virt) {
+        TRY(run_virtual_updaters(ctx, *r.virt, stage));
+        return finish_status(ctx);
+    }
     if (!r.slot) return seterr(ctx, GC_ERR_ARG, "not a system handle");
     TRY(run_updaters(ctx, *r.slot, stage, dt));
     return finish_status(ctx);

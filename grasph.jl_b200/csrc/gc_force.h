@@ -58,6 +58,7 @@ struct ForceArgs {
     const int64_t* ngroups;    // device count of groups
     int num_sms;
     int cfg;                   // index into FORCE_CFGS
+    int imask, iwsum;          // InterpolateFieldFn: fields (1<<GC_FIELD_*), accumulate w_sum into avort
     int nref;
     InterRef ref[MAX_REFS];
 };

@@ -66,6 +66,11 @@ struct PfnInst {
     float f_alpha, f_beta, f_h, f_h2eps, f_delta, f_eps;  // FP32 copies; h2eps = 0.01·h²
 };
 
+// Per (virtual system, instance) parameters.
+struct VirtInst {
+    double pv[MAXD];  // prescribed_v
+};
+
 // Per (ghost entry, instance) parameters.
 struct GhostInst {
     double normals[GC_MAX_GHOST_PLANES][MAXD], points[GC_MAX_GHOST_PLANES][MAXD];

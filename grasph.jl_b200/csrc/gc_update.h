@@ -44,4 +44,20 @@ void launch_rk4_final(const StepArgs& a, cudaStream_t s);
 void launch_xsph_final(const StepArgs& a, cudaStream_t s);
 void launch_update(const UpdArgs& a, cudaStream_t s);
 
+// VirtualNormUpdater / PrescribedVelocityUpdater on a virtual system's
+// source fields (src/StateUpdaters.jl:44-97).
+struct VirtArgs {
+    int64_t N;
+    int nd, ns, kind;
+    const int32_t* inst_of;
+    const VirtInst* vi;  // per instance
+    const UpdInst* u;    // per instance
+    double *v, *rho, *p, *stress;
+    const double* wsum;
+};
+void launch_virtual_update(const VirtArgs& a, cudaStream_t s);
+// _update_virtual_positions! src/TimeIntegration.jl:389-397: x += prescribed_v·dt.
+void launch_virtual_advance(double* x, int64_t N, int nd, const int32_t* inst_of, const SysInst* inst,
+                            const VirtInst* vi, cudaStream_t s);
+
 }  // namespace gc

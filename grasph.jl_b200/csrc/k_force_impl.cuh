@@ -123,6 +123,24 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         acc.dr += 1.0;
         return 1;
     }
+    if (PFN == GC_PFN_INTERPOLATE) {
+        // InterpolateFieldFn(ps_a, ps_b::VirtualParticleSystem)
+        // src/PairwiseFunctors.jl:424-428 from the virtual particle's side:
+        // kw = w·(m_a/ρ_a[i]); f[j] += kw·f_a[i]; w_sum[j] += kw
+        const double q = sqrt(rr) / G.H;
+        const double kw = kernel_w<KK>(G.knorm, q) * (G.bmass / r.brho[j]);
+        if (A.imask & (1 << GC_FIELD_V)) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + kw * r.bv[d * Nb + j];
+        }
+        if (A.imask & (1 << GC_FIELD_RHO)) acc.dr = acc.dr + kw * r.brho[j];
+        if (A.imask & (1 << GC_FIELD_STRESS)) {
+#pragma unroll
+            for (int q2 = 0; q2 < NS; ++q2) acc.sr[q2] = acc.sr[q2] + kw * r.bstress[q2 * Nb + j];
+        }
+        if (A.iwsum) acc.w[0] = acc.w[0] + kw;
+        return 1;
+    }
     if (PFN == GC_PFN_XSPH) {
         // XSPHPfn src/PairwiseFunctors.jl:364-389, xsph_veladjust
         // src/PairwisePhysics.jl:268-270: du = ((-ε·dv)·w)/(ρ_i + ρ_j),
@@ -344,7 +362,19 @@ struct PhysF64 {
         for (int d = 0; d < ND; ++d) acc.dv[d] = 0.0;
         acc.dr = 0.0;
         if (!from_memory) return;
-        if (PFN == GC_PFN_XSPH) {  // advdt is the v_adjustment array here
+        if (PFN == GC_PFN_INTERPOLATE) {
+            // targets: v (advdt), rho (adrhodt), stress (asr), w_sum (avort)
+            if (A.imask & (1 << GC_FIELD_V)) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
+            }
+            if (A.imask & (1 << GC_FIELD_RHO)) acc.dr = A.adrhodt[gi];
+            if (A.imask & (1 << GC_FIELD_STRESS)) {
+#pragma unroll
+                for (int q = 0; q < NS; ++q) acc.sr[q] = A.asr[q * N + gi];
+            }
+            acc.w[0] = A.iwsum ? A.avort[gi] : 0.0;
+        } else if (PFN == GC_PFN_XSPH) {  // advdt is the v_adjustment array here
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
         } else if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
@@ -362,7 +392,18 @@ struct PhysF64 {
     }
     static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
         const int64_t N = A.aN;
-        if (PFN == GC_PFN_XSPH) {
+        if (PFN == GC_PFN_INTERPOLATE) {
+            if (A.imask & (1 << GC_FIELD_V)) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
+            }
+            if (A.imask & (1 << GC_FIELD_RHO)) A.adrhodt[gi] = acc.dr;
+            if (A.imask & (1 << GC_FIELD_STRESS)) {
+#pragma unroll
+                for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = acc.sr[q];
+            }
+            if (A.iwsum) A.avort[gi] = acc.w[0];
+        } else if (PFN == GC_PFN_XSPH) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
         } else if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
@@ -1013,7 +1054,8 @@ static void launch_cfg(const ForceArgs& A, cudaStream_t s) {
 template <int ND, int NS, int PFN, int KK, bool F32>
 static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
     if constexpr (F32) {
-        if constexpr (PFN != GC_PFN_COUNT && PFN != GC_PFN_XSPH) launch_cfg<PhysF32<ND, NS, PFN, KK>, ND, PFN>(A, s);
+        if constexpr (PFN != GC_PFN_COUNT && PFN != GC_PFN_XSPH && PFN != GC_PFN_INTERPOLATE)
+            launch_cfg<PhysF32<ND, NS, PFN, KK>, ND, PFN>(A, s);
     } else {
         using P64 = PhysF64<ND, NS, PFN, KK>;
         if (count_only) {
@@ -1034,6 +1076,13 @@ static int launch_pfn(const ForceArgs& A, bool count_only, cudaStream_t s) {
     switch (A.pfn) {
         case GC_PFN_FLUID: launch_t<ND, NS, GC_PFN_FLUID, KK, F32>(A, count_only, s); return 0;
         case GC_PFN_COUNT: launch_t<ND, NS, GC_PFN_COUNT, KK, F32>(A, count_only, s); return 0;
+        case GC_PFN_INTERPOLATE:  // FP64 only
+            if constexpr (F32) {
+                return GC_ERR_UNSUPPORTED;
+            } else {
+                launch_t<ND, NS, GC_PFN_INTERPOLATE, KK, F32>(A, count_only, s);
+                return 0;
+            }
         case GC_PFN_XSPH:  // FP64 only (a cheap, memory-bound functor)
             if constexpr (F32) {
                 return GC_ERR_UNSUPPORTED;
@@ -1060,7 +1109,8 @@ static int launch_pfn(const ForceArgs& A, bool count_only, cudaStream_t s) {
 template <int ND, int KK, bool F32>
 static int launch_nd(const ForceArgs& A, bool count_only, cudaStream_t s) {
     const bool stress_pfn = A.pfn == GC_PFN_CAUCHY_FLUID || A.pfn == GC_PFN_STRAIN_RATE ||
-                            A.pfn == GC_PFN_STRAIN_RATE_VORTICITY;
+                            A.pfn == GC_PFN_STRAIN_RATE_VORTICITY ||
+                            (A.pfn == GC_PFN_INTERPOLATE && (A.imask & (1 << GC_FIELD_STRESS)));
     if (!stress_pfn) return launch_pfn<ND, 0, KK, F32>(A, count_only, s);
     if (ND == 2) {
         if (A.ns == 3) return launch_pfn<ND, 3, KK, F32>(A, count_only, s);

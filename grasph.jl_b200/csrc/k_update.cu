@@ -344,4 +344,53 @@ void launch_update(const UpdArgs& a, cudaStream_t s) {
     g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
 }
 
+// ----------------------------------------------------------- virtual systems
+// VirtualNormUpdater (src/StateUpdaters.jl:65-76): each listed field divided
+// by w_sum (zero where w_sum is zero), then v = v·v_mult + prescribed_v, two
+// roundings (a fused broadcast, no contraction); PrescribedVelocityUpdater
+// (:95-97): v += prescribed_v.
+__global__ void k_virtual_update(VirtArgs a) {
+    const int64_t N = a.N;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
+        const int k = a.inst_of[g];
+        const double* pv = a.vi[k].pv;
+        if (a.kind == GC_UPD_PRESCRIBED_V) {
+            for (int d = 0; d < a.nd; ++d) a.v[d * N + g] = a.v[d * N + g] + pv[d];
+            continue;
+        }
+        const UpdInst& u = a.u[k];
+        const int m = (int)u.prm[3];
+        const double w = a.wsum[g];
+        if (m & (1 << GC_FIELD_V))
+            for (int d = 0; d < a.nd; ++d) {
+                const double val = w == 0.0 ? 0.0 : a.v[d * N + g] / w;
+                a.v[d * N + g] = val * u.prm[d] + pv[d];
+            }
+        if (m & (1 << GC_FIELD_RHO)) a.rho[g] = w == 0.0 ? 0.0 : a.rho[g] / w;
+        if ((m & (1 << GC_FIELD_P)) && a.p) a.p[g] = w == 0.0 ? 0.0 : a.p[g] / w;
+        if ((m & (1 << GC_FIELD_STRESS)) && a.stress)
+            for (int q = 0; q < a.ns; ++q) a.stress[q * N + g] = w == 0.0 ? 0.0 : a.stress[q * N + g] / w;
+    }
+}
+
+void launch_virtual_update(const VirtArgs& a, cudaStream_t s) {
+    if (a.N > 0) k_virtual_update<<<ublk(a.N), UTPB, 0, s>>>(a);
+    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+}
+
+__global__ void k_virtual_advance(double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
+                                  const SysInst* __restrict__ inst, const VirtInst* __restrict__ vi) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
+        const int k = inst_of[g];
+        const double dt = inst[k].dt;
+        for (int d = 0; d < nd; ++d) x[d * N + g] = x[d * N + g] + vi[k].pv[d] * dt;
+    }
+}
+
+void launch_virtual_advance(double* x, int64_t N, int nd, const int32_t* inst_of, const SysInst* inst,
+                            const VirtInst* vi, cudaStream_t s) {
+    if (N > 0) k_virtual_advance<<<ublk(N), UTPB, 0, s>>>(x, N, nd, inst_of, inst, vi);
+    g_launches.fetch_add(N > 0, std::memory_order_relaxed);
+}
+
 }  // namespace gc

@@ -12,7 +12,8 @@ from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, 
                     GhostParticleSystem, HookeLawStressUpdater, HouseholderReflect, LeapFrogTimeIntegrator, RK4TimeIntegrator,
                     LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
                     StressParticleSystem, SystemInteraction, TaitEOSUpdater, ViscoPlasticMCStressUpdater,
-                    WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater, is_coupled)
+                    WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater, is_coupled, VirtualParticleSystem,
+                    InterpolateFieldFn, VirtualNormUpdater, PrescribedVelocityUpdater)
 from .engine import (CudaBackend, GcError, Server, Session, compile_instance, download_instance, load_library,
                      time_integrate, upload_instance)
 

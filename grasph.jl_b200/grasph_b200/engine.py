@@ -21,7 +21,7 @@ import numpy as np
 from . import consts as C
 from .model import (AbstractBoundarySystem, AbstractParticleSystem, ArgumentError,
                     GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator,
-                    SystemInteraction, updater_chains, _pfn_kind, _pfn_params)
+                    SystemInteraction, VirtualParticleSystem, updater_chains, _pfn_kind, _pfn_params)
 
 PKG_DIR = Path(__file__).resolve().parents[1]
 LIB_PATH = PKG_DIR / "libgrasph_cuda.so"
@@ -83,6 +83,7 @@ def load_library(path: os.PathLike | None = None):
         "gc_set_integrator": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double]),
         "gc_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
         "gc_set_velocity_adjust": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_double]),
+        "gc_add_virtual": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _dp, _ip]),
         "gc_finalize": (ct.c_int, [ct.c_void_p]),
         "gc_upload_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         "gc_download_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
@@ -200,6 +201,12 @@ class CudaBackend:
 
     def set_velocity_adjust(self, inst, inter, kind, epsilon):
         self._chk(self.lib.gc_set_velocity_adjust(self.ctx, inst, inter, kind, epsilon), "gc_set_velocity_adjust")
+
+    def add_virtual(self, inst, src, zero_mask, prescribed_v):
+        pv, pvp = _arr(prescribed_v, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_virtual(self.ctx, inst, src, zero_mask, pvp, ct.byref(out)), "gc_add_virtual")
+        return out.value
 
     def set_updaters(self, inst, sys, chains):
         cl = np.array([len(c) for c in chains] or [0], dtype=np.int32)
@@ -325,13 +332,14 @@ class InstanceMap:
         self.inters = {}
         self.systems = []
         self.ghosts = []
+        self.virtuals = []
 
     def h(self, obj):
         return self.handles[id(obj)]
 
 
 def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
-                     kind=C.GC_INTEGRATOR_LEAPFROG) -> InstanceMap:
+                     kind=C.GC_INTEGRATOR_LEAPFROG, virtuals=()) -> InstanceMap:
     """Issue the model-building calls for one simulation (one instance)."""
     m = InstanceMap(inst)
     sys_ids = {id(ps) for ps in systems}
@@ -341,6 +349,20 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
         m.handles[id(ps)] = backend.add_system(inst, ps.kind, ps.n, ps.ndims, ps.ns, ps.mass, ps.c,
                                                ps.source_v, ps.source_rho)
         m.systems.append(ps)
+    for vps in virtuals:
+        src = vps.source
+        if id(src) in sys_ids:
+            raise ArgumentError("a virtual system's source must not be one of the integrator's systems")
+        if id(src) not in m.handles:
+            # the source is a slot of its own: moved with the state, never integrated
+            m.handles[id(src)] = backend.add_system(inst, src.kind, src.n, src.ndims, src.ns, src.mass, src.c,
+                                                    src.source_v, src.source_rho)
+            m.systems.append(src)
+        m.handles[id(vps)] = backend.add_virtual(inst, m.h(src), vps.zero_mask, vps.prescribed_v)
+        m.virtuals.append(vps)
+        chains = updater_chains(vps)
+        if chains:
+            backend.set_updaters(inst, m.h(vps), chains)
     for ge in ghosts:
         g = ge.ghost
         if id(g.source) not in sys_ids:
@@ -376,6 +398,10 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
         elif isinstance(b, GhostParticleSystem):
             if id(b) not in m.handles:
                 raise ArgumentError("a ghost used as system_b must belong to a GhostEntry in `ghosts`")
+            bh = m.h(b)
+        elif isinstance(b, VirtualParticleSystem):
+            if id(b) not in m.handles:
+                raise ArgumentError("a virtual system used as system_b must be in `virtual_systems`")
             bh = m.h(b)
         else:
             if id(b) not in sys_ids:
@@ -419,6 +445,8 @@ def download_instance(backend, m: InstanceMap, with_ghosts=True, systems=None):
     if with_ghosts:
         for ge in m.ghosts:
             download_ghost(backend, m, ge)
+        for vps in m.virtuals:
+            backend.download_into(m.inst, m.h(vps), C.GC_FIELD_W_SUM, vps.w_sum)
 
 
 def download_ghost(backend, m: InstanceMap, ge: GhostEntry):
@@ -461,7 +489,7 @@ class Session:
         for lf in self.integrators:
             inst = self.backend.instance_add()
             self.maps.append(compile_instance(self.backend, inst, lf.systems, lf.interactions, lf.ghosts,
-                                              lf.gamma, lf.kind))
+                                              lf.gamma, lf.kind, getattr(lf, "virtual_systems", ())))
         self.backend.finalize()
         self.backend.set_precision(precision)
         self.precision = precision
@@ -642,7 +670,8 @@ class Server:
         """Queue one simulation; its current host state is copied now."""
         be = CudaBackend(self.device, 0, lib=self.lib)
         inst = be.instance_add()
-        m = compile_instance(be, inst, lf.systems, lf.interactions, lf.ghosts, lf.gamma, lf.kind)
+        m = compile_instance(be, inst, lf.systems, lf.interactions, lf.ghosts, lf.gamma, lf.kind,
+                             getattr(lf, "virtual_systems", ()))
         for ps in m.systems:
             h = m.h(ps)
             for name, fid in ps.particle_fields():

@@ -429,6 +429,32 @@ class CountingPfn(_Pfn):
     kind = C.GC_PFN_COUNT
 
 
+_INTERP_FIELDS = {"v": C.GC_FIELD_V, "rho": C.GC_FIELD_RHO, "stress": C.GC_FIELD_STRESS}
+
+
+class InterpolateFieldFn(_Pfn):
+    """SPH interpolation f_j += (m_i/ρ_i)·f_i·W_ij from real system_a particles
+    into a VirtualParticleSystem system_b, src/PairwiseFunctors.jl:392-428."""
+
+    kind = C.GC_PFN_INTERPOLATE
+
+    def __init__(self, *fields, accumulate_wsum=True):
+        names = [str(f).lstrip(":") for f in fields]
+        if not names:
+            raise ArgumentError("InterpolateFieldFn needs at least one field")
+        for n in names:
+            if n not in _INTERP_FIELDS:
+                raise ArgumentError(f"InterpolateFieldFn: field :{n} has no device implementation")
+        self.fields = tuple(names)
+        self.accumulate_wsum = bool(accumulate_wsum)
+
+    def params(self):
+        p = super().params()
+        p[0] = float(sum(1 << _INTERP_FIELDS[n] for n in self.fields))
+        p[1] = 1.0 if self.accumulate_wsum else 0.0
+        return p
+
+
 class XSPHPfn(_Pfn):
     """XSPH velocity smoothing, src/PairwiseFunctors.jl:357-389; only as a
     `velocity_adjust_pairwise_fn` (swept by adjust_v! in the step's XSPH
@@ -528,6 +554,34 @@ class ElastoPlasticStressUpdater(_Updater):
         return p
 
 
+class VirtualNormUpdater(_Updater):
+    """Normalise the listed fields of a VirtualParticleSystem by its w_sum
+    and apply the velocity multiplier, src/StateUpdaters.jl:44-76."""
+
+    kind = C.GC_UPD_VIRTUAL_NORM
+    _ok = {"v": C.GC_FIELD_V, "rho": C.GC_FIELD_RHO, "p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS}
+
+    def __init__(self, v_mult, *fields):
+        self.v_mult = np.asarray(v_mult, dtype=np.float64).ravel()
+        names = [str(f).lstrip(":") for f in fields]
+        for n in names:
+            if n not in self._ok:
+                raise ArgumentError(f"VirtualNormUpdater: field :{n} has no device implementation")
+        self.fields = tuple(names)
+
+    def params(self):
+        p = super().params()
+        p[:self.v_mult.size] = self.v_mult
+        p[3] = float(sum(1 << self._ok[n] for n in self.fields))
+        return p
+
+
+class PrescribedVelocityUpdater(_Updater):
+    """v += prescribed_v on a VirtualParticleSystem, src/StateUpdaters.jl:78-97."""
+
+    kind = C.GC_UPD_PRESCRIBED_V
+
+
 class HookeLawStressUpdater(_Updater):
     """Plane-strain Hooke update, src/StateUpdaters.jl:356-405."""
 
@@ -619,12 +673,54 @@ def is_coupled(si: SystemInteraction) -> bool:
 
 # ------------------------------------------------------------- integrator
 
+class VirtualParticleSystem:
+    """A source system seen through SPH interpolation, src/Particles.jl:476-528.
+
+    Every per-particle field is the source's (the same arrays); `w_sum`, the
+    state updaters and `prescribed_v` are its own.  The source is not one of
+    the integrator's systems: it is sorted with the virtual systems, never
+    integrated, and moved by prescribed_v·dt after each step."""
+
+    def __init__(self, ps: AbstractParticleSystem, name, n, ndims, mass, c, *, dtype=np.float64,
+                 state_updater=(), zero_fields=(), prescribed_v=None):
+        if int(ndims) != ps.ndims:
+            raise ArgumentError(f"ndims={ndims} does not match source ndims={ps.ndims}")
+        if int(n) != ps.n:
+            raise ArgumentError(f"n={n} does not match source n={ps.n}")
+        self.name = str(name)
+        self.source = ps
+        self.w_sum = np.zeros(ps.n)
+        ups = state_updater if isinstance(state_updater, tuple) else (state_updater,)
+        self.state_updater = ups
+        zf = [str(f).lstrip(":") for f in zero_fields]
+        for f in zf:
+            if f not in ("v", "rho", "p", "stress", "dvdt", "drhodt", "strain_rate"):
+                raise ArgumentError(f"zero_fields: :{f} has no device implementation")
+        self.zero_fields = tuple(zf)
+        pv = np.zeros(ps.ndims) if prescribed_v is None else np.asarray(prescribed_v, dtype=np.float64).ravel()
+        if pv.shape != (ps.ndims,):
+            raise ArgumentError("prescribed_v must have ndims components")
+        self.prescribed_v = pv
+
+    def __getattr__(self, name):
+        # forwarded to the source (only reached for attributes not set above)
+        if name == "source":
+            raise AttributeError(name)
+        return getattr(self.source, name)
+
+    @property
+    def zero_mask(self):
+        ids = {"v": C.GC_FIELD_V, "rho": C.GC_FIELD_RHO, "p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS,
+               "dvdt": C.GC_FIELD_DVDT, "drhodt": C.GC_FIELD_DRHODT, "strain_rate": C.GC_FIELD_STRAIN_RATE}
+        return sum(1 << ids[f] for f in self.zero_fields)
+
+
 class LeapFrogTimeIntegrator:
     """src/TimeIntegration.jl:29-67."""
 
     kind = C.GC_INTEGRATOR_LEAPFROG
 
-    def __init__(self, systems, interactions, *, ghosts=(), gamma=0.0, **kw):
+    def __init__(self, systems, interactions, *, ghosts=(), gamma=0.0, virtual_systems=(), **kw):
         if "Γ" in kw:
             gamma = kw.pop("Γ")
         if kw:
@@ -639,6 +735,11 @@ class LeapFrogTimeIntegrator:
         self.systems = sys_
         self.interactions = ints
         self.ghosts = gsts
+        vs = (virtual_systems,) if isinstance(virtual_systems, VirtualParticleSystem) else tuple(virtual_systems)
+        for v in vs:
+            if not isinstance(v, VirtualParticleSystem):
+                raise ArgumentError("virtual_systems must be VirtualParticleSystems")
+        self.virtual_systems = vs
         self.c = max(ps.c for ps in sys_)
         self.h = min(it.kernel.h for it in ints)
         self.gamma = float(gamma)

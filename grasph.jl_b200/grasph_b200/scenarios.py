@@ -22,7 +22,8 @@ from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, Dyna
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
                     FluidSolidPfn, HookeLawStressUpdater,
                     GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator, LinearEOSUpdater,
-                    RK4TimeIntegrator, StrainRatePfn, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
+                    RK4TimeIntegrator, StrainRatePfn, InterpolateFieldFn, VirtualNormUpdater,
+                    VirtualParticleSystem, PrescribedVelocityUpdater, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
                     TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater)
 
 G = 9.81
@@ -228,6 +229,70 @@ def granular_column(nfx=100, nfy=50, dx=0.002, rho0=1850.0, E=0.84e6, nu=0.3, ph
     lf = LeapFrogTimeIntegrator([fluid, bottom], inters, ghosts=(gentry,))
     meta = dict(workload="granular_column", n_fluid=fluid.n, n_boundary=bottom.n, h=h, c0=c, cfl=cfl,
                 dt=cfl * h / c, ndims=2, phi=phi, E=E)
+    return lf, meta
+
+
+# ------------------------------------- EP column with virtual-particle walls
+
+def ep_column_virtual(dx=0.002, width=0.2, height=0.1, bottom_len=0.5, rho0=1850.0, E=0.84e6, nu=0.3,
+                      phi_deg=19.8, psi=0.0, cohesion=0.0, alpha=0.1, beta=0.1, hfac=1.2, cfl=0.1,
+                      bottom_v=None, geostatic=False):
+    """2-D elasto-plastic column collapse with virtual-particle boundaries
+    (EP_ColumnCollapse2.jl layout): ElastoPlasticParticleSystem NS = 4 with
+    four stages (nothing / zero strain rate and vorticity / EP stress
+    update / nothing), a 3-layer bottom and a 3-column left wall as
+    VirtualParticleSystems over StressParticleSystem sources, filled by
+    InterpolateFieldFn(:v, :rho) at stage 1 and (:stress) at stage 3 and
+    normalised by VirtualNormUpdater at stages 2 and 4 (bottom: no-slip,
+    left: free-slip).  `bottom_v` gives the bottom a prescribed velocity
+    (then it also carries a PrescribedVelocityUpdater at stage 2);
+    `geostatic` starts the column from K0 stress instead of the script's
+    zero stress."""
+    phi = phi_deg * math.pi / 180.0
+    c = math.sqrt(E * (1 - nu) / (rho0 * (1 + nu) * (1 - 2 * nu)))
+    h = hfac * dx
+    mass = rho0 * dx * dx
+    nfx, nfy, nbx = int(math.floor(width / dx)), int(math.floor(height / dx)), int(math.floor(bottom_len / dx))
+    fluid = ElastoPlasticParticleSystem(
+        "fluid", nfx * nfy, 2, 4, mass, c, source_v=[0.0, -G],
+        state_updater=(None, ZeroFieldUpdater("strain_rate", "vorticity"),
+                       ElastoPlasticStressUpdater(E, nu, phi, psi, cohesion), None))
+    ii, jj = np.meshgrid(np.arange(nfx), np.arange(nfy), indexing="ij")
+    fluid.x[:, 0] = (ii.ravel() + 0.5) * dx
+    fluid.x[:, 1] = (jj.ravel() + 0.5) * dx
+    fluid.rho[:] = rho0
+    if geostatic:
+        K0 = 1.0 - math.sin(phi)
+        syy = -rho0 * G * (nfy * dx - fluid.x[:, 1])
+        fluid.stress[:, 0] = K0 * syy
+        fluid.stress[:, 1] = syy
+        fluid.stress[:, 2] = K0 * syy
+    bsrc = StressParticleSystem("bottom_boundary", 3 * (nbx + 3), 2, 4, mass, c)
+    bsrc.x[:] = [((i - 3.5) * dx, -(j - 0.5) * dx) for i in range(1, nbx + 4) for j in range(1, 4)]
+    bsrc.rho[:] = rho0
+    lsrc = StressParticleSystem("left_boundary", 3 * nfy, 2, 4, mass, c)
+    lsrc.x[:] = [(-(col - 0.5) * dx, (j + 0.5) * dx) for j in range(nfy) for col in range(1, 4)]
+    lsrc.rho[:] = rho0
+    norm_b = VirtualNormUpdater((-1.0, -1.0), "v", "rho")
+    bottom = VirtualParticleSystem(
+        bsrc, "bottom_virt", bsrc.n, 2, mass, c, zero_fields=("v", "rho", "stress"), prescribed_v=bottom_v,
+        state_updater=(None, norm_b if bottom_v is None else (norm_b, PrescribedVelocityUpdater()), None,
+                       VirtualNormUpdater((-1.0, -1.0), "stress")))
+    left = VirtualParticleSystem(
+        lsrc, "left_virt", lsrc.n, 2, mass, c, zero_fields=("v", "rho", "stress"),
+        state_updater=(None, VirtualNormUpdater((-1.0, 1.0), "v", "rho"), None,
+                       VirtualNormUpdater((-1.0, 1.0), "stress")))
+    kernel = CubicSplineKernel(h, ndims=2)
+    sr = StrainRateVorticityPfn()
+    kin = CauchyFluidPfn(alpha, beta, h)
+    iv = InterpolateFieldFn("v", "rho", accumulate_wsum=True)
+    istr = InterpolateFieldFn("stress", accumulate_wsum=False)
+    inters = [SystemInteraction(kernel, (None, sr, None, kin), fluid),
+              SystemInteraction(kernel, (iv, sr, istr, kin), fluid, bottom),
+              SystemInteraction(kernel, (iv, sr, istr, kin), fluid, left)]
+    lf = LeapFrogTimeIntegrator([fluid], inters, virtual_systems=(bottom, left))
+    meta = dict(workload="ep_column_virtual", n_fluid=fluid.n, n_bottom=bsrc.n, n_left=lsrc.n, h=h, c0=c,
+                cfl=cfl, dt=cfl * h / c, ndims=2)
     return lf, meta
 
 

@@ -43,6 +43,7 @@ pfn_kind(::CauchyFluidPfn) = 2
 pfn_kind(::StrainRatePfn) = 3
 pfn_kind(::StrainRateVorticityPfn) = 4
 pfn_kind(::FluidSolidPfn) = 7
+pfn_kind(::InterpolateFieldFn) = 8
 pfn_kind(f) = throw(ArgumentError("pairwise functor $(typeof(f)) has no device implementation"))
 
 function pfn_params(f)
@@ -53,6 +54,10 @@ function pfn_params(f)
         f.delta === nothing || (p[5] = f.delta)
     end
     f isa FluidSolidPfn && (p[4] = typeof(f).parameters[1])
+    if f isa InterpolateFieldFn
+        fs, acc = typeof(f).parameters
+        p[1] = Float64(reduce(|, (1 << GC_FIELD[s] for s in fs); init=0)); p[2] = acc ? 1.0 : 0.0
+    end
     if f isa FluidPfn
         p[4] = typeof(f).parameters[1]
         f.epsilon === nothing || (p[6] = f.epsilon)
@@ -66,7 +71,30 @@ upd_entry(u::TaitEOSUpdater) = (2, [u.rho0, u.gamma, 0, 0, 0, 0])
 upd_entry(u::LinearEOSUpdater) = (3, [u.rho0, 0, 0, 0, 0, 0])
 upd_entry(u::ElastoPlasticStressUpdater) = (4, [u.E, u.nu, u.phi, u.psi, u.cohesion, 0])
 upd_entry(u::HookeLawStressUpdater) = (5, [u.E, u.nu, 0, 0, 0, 0])
+function upd_entry(u::VirtualNormUpdater{S}) where {S}
+    p = zeros(6)
+    p[1:length(u.v_mult)] .= u.v_mult
+    p[4] = Float64(reduce(|, (1 << GC_FIELD[s] for s in S); init=0))
+    return (7, p)
+end
+upd_entry(u::PrescribedVelocityUpdater) = (8, zeros(6))
 upd_entry(u) = throw(ArgumentError("state updater $(typeof(u)) has no device implementation"))
+
+function set_updaters!(ctx, inst, handle, updaters)
+    isempty(updaters) && return nothing
+    lens = Cint[]; kinds = Cint[]; prm = Float64[]
+    for entry in updaters
+        chain = entry === nothing ? () : (entry isa Tuple ? entry : (entry,))
+        push!(lens, length(chain))
+        for u in chain
+            k, p = upd_entry(u)
+            push!(kinds, k); append!(prm, p)
+        end
+    end
+    check(ctx, ccall((:gc_set_updaters, LIB), Cint,
+                     (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cint}, Ptr{Cint}, Ptr{Cdouble}),
+                     ctx, inst, handle, length(lens), lens, kinds, prm))
+end
 
 fields_of(ps) = [f for f in (:x, :v, :rho, :dvdt, :drhodt, :p, :stress, :strain_rate, :vorticity,
                                :strain, :strain_p) if hasfield(typeof(ps), f)]
@@ -102,6 +130,27 @@ function CudaLeapFrog(lf::Union{LeapFrogTimeIntegrator,RK4TimeIntegrator}; devic
                            ctx[], inst[], GC_SYS[typeof(ps).name.wrapper], ps.n, ps.ndims, ns, ps.mass, ps.c,
                            Vector{Float64}(ps.source_v), ps.source_rho, out))
         h[ps] = out[]
+    end
+    # virtual systems: the source becomes a system of its own, never integrated
+    for vps in lf.virtual_systems
+        src = getfield(vps, :source)
+        if !haskey(h, src)
+            out = Ref{Cint}(0)
+            ns = hasfield(typeof(src), :stress) ? length(eltype(src.stress)) : 0
+            check(ctx[], ccall((:gc_add_system, LIB), Cint,
+                               (Ptr{Cvoid}, Cint, Cint, Int64, Cint, Cint, Cdouble, Cdouble, Ptr{Cdouble}, Cdouble,
+                                Ref{Cint}),
+                               ctx[], inst[], GC_SYS[typeof(src).name.wrapper], src.n, src.ndims, ns, src.mass,
+                               src.c, Vector{Float64}(src.source_v), src.source_rho, out))
+            h[src] = out[]
+        end
+        zf = typeof(vps).parameters[5]
+        zmask = Cint(reduce(|, (1 << GC_FIELD[s] for s in zf); init=0))
+        out = Ref{Cint}(0)
+        check(ctx[], ccall((:gc_add_virtual, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cdouble}, Ref{Cint}),
+                           ctx[], inst[], h[src], zmask, Vector{Float64}(getfield(vps, :prescribed_v)), out))
+        h[vps] = out[]
+        set_updaters!(ctx[], inst[], h[vps], getfield(vps, :state_updater))
     end
     for ge in lf.ghosts
         g = ge.ghost

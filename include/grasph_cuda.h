@@ -71,7 +71,8 @@ enum {
     GC_FIELD_IDX_ORIGINAL = 13,/* ghosts: int64 source index, 1-based         */
     GC_FIELD_IDX_BOUNDARY = 14,/* ghosts: int64 plane index, 1-based          */
     GC_FIELD_NORMALS = 15,     /* ghosts: ND doubles                          */
-    GC_NFIELDS = 16
+    GC_FIELD_W_SUM = 16,       /* virtual systems: 1 double, kernel-weight sum */
+    GC_NFIELDS = 17
 };
 
 /* ------------------------------------------------------ boundary wrappers */
@@ -94,7 +95,10 @@ enum {
     GC_PFN_STRAIN_RATE_VORTICITY = 4,   /* StrainRateVorticityPfn :78          */
     GC_PFN_COUNT = 5,
     GC_PFN_XSPH = 6,                    /* XSPHPfn :360-389; velocity-adjust functor only */
-    GC_PFN_FLUID_SOLID = 7              /* FluidSolidPfn :479-519 (system_b a real system) */
+    GC_PFN_FLUID_SOLID = 7,             /* FluidSolidPfn :479-519 (system_b a real system) */
+    GC_PFN_INTERPOLATE = 8              /* InterpolateFieldFn :392-428, system_b a virtual
+                                           system: [0] bitmask of 1<<GC_FIELD_* out of v, rho,
+                                           stress  [1] accumulate_wsum (0 or 1)  */
 };
 /* Per-stage functor parameters, GC_PFN_NPARAM doubles each:
  *   [0] art_visc_alpha  [1] art_visc_beta  [2] h
@@ -111,9 +115,12 @@ enum {
     GC_UPD_LINEAR_EOS = 3,    /* LinearEOSUpdater :131; [0] rho0            */
     GC_UPD_ELASTOPLASTIC = 4, /* ElastoPlasticStressUpdater :202; [0] E [1] nu [2] phi [3] psi [4] cohesion */
     GC_UPD_HOOKE = 5,         /* HookeLawStressUpdater :356; [0] E [1] nu   */
-    GC_UPD_VISCOPLASTIC_MC = 6 /* ViscoPlasticMCStressUpdater :144-186, the stress part; its
+    GC_UPD_VISCOPLASTIC_MC = 6, /* ViscoPlasticMCStressUpdater :144-186, the stress part; its
                                   EOS is the chain entry before it. [0] friction angle
                                   (radians) [1] cohesion; NS = 3, 4 or 6    */
+    GC_UPD_VIRTUAL_NORM = 7,  /* VirtualNormUpdater :44-76 (virtual systems): [0..2] v_mult,
+                                 [3] bitmask of 1<<GC_FIELD_* out of v, rho, p, stress */
+    GC_UPD_PRESCRIBED_V = 8   /* PrescribedVelocityUpdater :78-97 (virtual systems)    */
 };
 #define GC_UPD_NPARAM 6
 /* At most this many updaters may be chained in one stage (a Julia tuple of
@@ -205,6 +212,18 @@ int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kerne
  * (:309) in the step's XSPH correction, src/TimeIntegration.jl:421-436.
  * Every instance of a context must set the same kind on an interaction.   */
 int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double epsilon);
+
+/* VirtualParticleSystem(source, name, n, ndims, mass, c; state_updater,
+ * zero_fields, prescribed_v) src/Particles.jl:476-528, one of the
+ * integrator's virtual_systems (src/TimeIntegration.jl:364-419, 683).
+ * The source `src_sys` (a system handle) holds the virtual particles'
+ * positions and fields; it is sorted with the virtual systems each step,
+ * never integrated, and moved by prescribed_v·dt after each step.
+ * zero_mask: bitmask of 1<<GC_FIELD_* zeroed, with w_sum, before each pass
+ * of stage sweeps; prescribed_v: ndims doubles or NULL (zero).  The handle
+ * serves as system_b and takes gc_set_updaters.                           */
+int gc_add_virtual(gc_ctx* ctx, int inst, int src_sys, int zero_mask, const double* prescribed_v,
+                   int* handle_out);
 
 /* The `state_updater` tuple of a system (src/Particles.jl:200): nstages
  * entries, each a chain of `chain_len[s]` updaters (kinds / GC_UPD_NPARAM

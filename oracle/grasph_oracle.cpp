@@ -131,6 +131,7 @@ struct Sys {
     std::vector<std::vector<Upd>> upd;  // one chain per updater-tuple entry
     std::vector<double> q0v, q0rho;
     std::vector<double> accv, accrho;  // RK4 accumulators
+    bool vsrc = false;  // the source of a virtual system: not one of the integrator's systems
     bool has_p() const { return kind >= GC_SYS_FLUID; }
     bool has_stress() const { return kind >= GC_SYS_STRESS; }
     bool is_ep() const { return kind == GC_SYS_ELASTOPLASTIC; }
@@ -152,7 +153,18 @@ struct Ghost {
     std::vector<int64_t> io, ib;
 };
 
-enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3 };
+enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3, H_VIRT = 4 };
+
+// VirtualParticleSystem src/Particles.jl:476-528: every per-particle field is
+// the source system's; w_sum, the updaters and prescribed_v are its own.
+struct Virt {
+    int src = 0;
+    int zmask = 0;  // zero_fields as 1<<GC_FIELD_*
+    double pv[3] = {0, 0, 0};
+    std::vector<double> wsum;
+    bool upd_set = false;
+    std::vector<std::vector<Upd>> upd;
+};
 struct Handle {
     int type = H_SYS;
     int idx = 0;  // system index (H_SYS, wrappers) or ghost index
@@ -186,6 +198,7 @@ struct oracle_ctx {
     std::vector<Handle> handles;
     std::vector<int> sys_handle;  // handle of each system
     std::vector<Inter> inters;
+    std::vector<Virt> virts;
     double gamma = 0;
     int integ = GC_INTEGRATOR_LEAPFROG;
     int threads = 1;
@@ -357,6 +370,7 @@ struct BView {
     double mass, c;
     int ns;
     Sys* sys;  // backing system for two-sided writes (H_SYS and wrappers)
+    Virt* virt;  // H_VIRT: the virtual system (w_sum)
     const double* normal;
     const double* point;
     double beta, ljcut;
@@ -370,6 +384,8 @@ struct Pfn {
     bool has_delta;
     double eps;  // artificial surface tension (two-sided FluidPfn only)
     bool has_eps;
+    int imask;   // InterpolateFieldFn: fields (1<<GC_FIELD_*)
+    bool iwsum;  // InterpolateFieldFn: accumulate w_sum
 };
 
 Pfn make_pfn(int kind, const double* prm) {
@@ -383,6 +399,8 @@ Pfn make_pfn(int kind, const double* prm) {
     f.has_delta = !std::isnan(prm[4]);
     f.eps = prm[5];
     f.has_eps = !std::isnan(prm[5]);
+    f.imask = kind == GC_PFN_INTERPOLATE ? (int)prm[0] : 0;
+    f.iwsum = kind == GC_PFN_INTERPOLATE && prm[1] != 0.0;
     return f;
 }
 
@@ -484,6 +502,19 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
                  const double* gx, double w, int* err) {
     const int ns = a.ns;
     const double* vi = &a.v[i * ND];
+    if (f.kind == GC_PFN_INTERPOLATE) {
+        // InterpolateFieldFn(ps_a, ps_b::VirtualParticleSystem) :424-428:
+        // f_b[j] += kw·f_a[i] with kw = w·(m_a/ρ_a[i]); w_sum[j] += kw
+        Sys& bs = *b.sys;
+        const double kw = w * (a.mass / a.rho[i]);
+        if (f.imask & (1 << GC_FIELD_V))
+            for (int d = 0; d < ND; ++d) bs.v[j * ND + d] = bs.v[j * ND + d] + kw * a.v[i * ND + d];
+        if (f.imask & (1 << GC_FIELD_RHO)) bs.rho[j] = bs.rho[j] + kw * a.rho[i];
+        if (f.imask & (1 << GC_FIELD_STRESS))
+            for (int q = 0; q < ns; ++q) bs.stress[j * ns + q] = bs.stress[j * ns + q] + kw * a.stress[i * ns + q];
+        if (f.iwsum) b.virt->wsum[j] = b.virt->wsum[j] + kw;
+        return;
+    }
     if (f.kind == GC_PFN_XSPH) {
         // generic coupled XSPHPfn :378-389 for every system_b: its stored v and
         // rho (a wrapper forwards to the wrapped system), and the write goes to
@@ -695,7 +726,7 @@ inline void pair_coupled(const Pfn& f, const Kern& k, Sys& a, const BView& b, in
         double r = std::sqrt(r_sq);
         double q = r / h;
         double gc = kernel_dw_dq(k, q) / (r * h);
-        double w = f.kind == GC_PFN_XSPH ? kernel_w(k, q) : 0.0;
+        double w = (f.kind == GC_PFN_XSPH || f.kind == GC_PFN_INTERPOLATE) ? kernel_w(k, q) : 0.0;
         double gx[ND];
         for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
         pfn_coupled<ND>(f, a, b, i, j, dx, gx, w, err);
@@ -1303,7 +1334,21 @@ int make_view(oracle_ctx* ctx, int handle, BView* out) {
     const Handle& h = ctx->handles[handle];
     BView b{};
     b.type = h.type;
-    if (h.type == H_GHOST) {
+    if (h.type == H_VIRT) {
+        Virt& vp = ctx->virts[h.idx];
+        Sys& s = ctx->sys[vp.src];
+        b.n = s.n;
+        b.x = s.x.data();
+        b.v = s.v.data();
+        b.rho = s.rho.data();
+        b.p = s.has_p() ? s.p.data() : nullptr;
+        b.stress = s.has_stress() ? s.stress.data() : nullptr;
+        b.mass = s.mass;
+        b.c = s.c;
+        b.ns = s.ns;
+        b.sys = &s;
+        b.virt = &vp;
+    } else if (h.type == H_GHOST) {
         Ghost& g = ctx->ghosts[h.idx];
         Sys& src = ctx->sys[g.src];
         b.n = g.n;
@@ -1342,7 +1387,16 @@ int make_view(oracle_ctx* ctx, int handle, BView* out) {
 int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     const Sys& a = ctx->sys[it.a];
     if (pk == GC_PFN_NONE) return GC_OK;
-    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_FLUID_SOLID) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_INTERPOLATE) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (pk == GC_PFN_INTERPOLATE) {
+        // the (real, virtual) method :424; the fields exist on both sides
+        if (it.b < 0 || ctx->handles[it.b].type != H_VIRT) return GC_ERR_UNSUPPORTED;
+        const Sys& s = ctx->sys[ctx->virts[ctx->handles[it.b].idx].src];
+        const int m = (int)it.pp.back()[0];
+        if (m & ~((1 << GC_FIELD_V) | (1 << GC_FIELD_RHO) | (1 << GC_FIELD_STRESS))) return GC_ERR_UNSUPPORTED;
+        if ((m & (1 << GC_FIELD_STRESS)) && !(a.has_stress() && s.has_stress() && a.ns == s.ns)) return GC_ERR_ARG;
+        return GC_OK;
+    }
     if (pk == GC_PFN_FLUID_SOLID) {
         // only the two-sided (system, system) method exists (:494)
         if (!a.has_p()) return GC_ERR_ARG;
@@ -1358,6 +1412,14 @@ int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     }
     if (it.b < 0) return GC_OK;
     const Handle& h = ctx->handles[it.b];
+    if (h.type == H_VIRT) {
+        // virtual system_b: the one-sided boundary forms (:193, :286, :37, :97)
+        const Sys& s = ctx->sys[ctx->virts[h.idx].src];
+        if (pk == GC_PFN_COUNT) return GC_ERR_UNSUPPORTED;
+        if (pk == GC_PFN_FLUID) return s.has_p() ? GC_OK : GC_ERR_ARG;
+        if (pk == GC_PFN_CAUCHY_FLUID) return s.has_stress() && s.ns == a.ns ? GC_OK : GC_ERR_ARG;
+        return GC_OK;
+    }
     if (pk == GC_PFN_COUNT) return h.type == H_GHOST ? GC_ERR_UNSUPPORTED : GC_OK;
     if (h.type == H_DYN) return GC_OK;
     if (h.type == H_STATIC) return GC_OK;
@@ -1424,14 +1486,17 @@ int adjust_v(oracle_ctx* ctx, Inter& it) {
 // (both axpys as separate multiply and add, the SVector form)
 int xsph_correction(oracle_ctx* ctx) {
     for (auto& s : ctx->sys)
-        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.v[i] + (-1.0 * s.vadj[i]);
-    for (auto& s : ctx->sys) std::fill(s.vadj.begin(), s.vadj.end(), 0.0);
+        if (!s.vsrc)
+            for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.v[i] + (-1.0 * s.vadj[i]);
+    for (auto& s : ctx->sys)
+        if (!s.vsrc) std::fill(s.vadj.begin(), s.vadj.end(), 0.0);
     for (auto& it : ctx->inters) {
         int st = adjust_v(ctx, it);
         if (st) return st;
     }
     for (auto& s : ctx->sys)
-        for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.v[i] + 1.0 * s.vadj[i];
+        if (!s.vsrc)
+            for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.v[i] + 1.0 * s.vadj[i];
     return GC_OK;
 }
 
@@ -1439,35 +1504,130 @@ int xsph_correction(oracle_ctx* ctx) {
 // src/TimeIntegration.jl:580-697 (LeapFrog)
 int num_stages(oracle_ctx* ctx) { return ctx->inters.empty() ? 0 : ctx->inters[0].nstages; }
 
-int step_once(oracle_ctx* ctx, double dt) {
-    const int nst = num_stages(ctx);
-    double hmin = 1e300;
-    for (auto& it : ctx->inters) hmin = std::min(hmin, it.H);
-    const double sort_cutoff = 2.0 * hmin;
-    // 1. sort every real system
-    for (auto& s : ctx->sys) {
-        int st = sort_system(s, sort_cutoff, nullptr);
-        if (st) return fail(ctx, st, "sort: non-finite position");
+// Virtual systems (src/Particles.jl:476-528, src/TimeIntegration.jl:364-419)
+void zero_field(Sys& s, int field) {
+    switch (field) {
+        case GC_FIELD_V: std::fill(s.v.begin(), s.v.end(), 0.0); break;
+        case GC_FIELD_RHO: std::fill(s.rho.begin(), s.rho.end(), 0.0); break;
+        case GC_FIELD_DVDT: std::fill(s.dvdt.begin(), s.dvdt.end(), 0.0); break;
+        case GC_FIELD_DRHODT: std::fill(s.drhodt.begin(), s.drhodt.end(), 0.0); break;
+        case GC_FIELD_P: std::fill(s.p.begin(), s.p.end(), 0.0); break;
+        case GC_FIELD_STRESS: std::fill(s.stress.begin(), s.stress.end(), 0.0); break;
+        case GC_FIELD_STRAIN_RATE: std::fill(s.sr.begin(), s.sr.end(), 0.0); break;
+        default: break;
     }
-    // 2. save q0
-    for (auto& s : ctx->sys) {
-        s.q0v = s.v;
-        s.q0rho = s.rho;
+}
+
+// auto_zero_virtual! :510-514: w_sum and the zero_fields
+void auto_zero_virtual(oracle_ctx* ctx, Virt& vp) {
+    std::fill(vp.wsum.begin(), vp.wsum.end(), 0.0);
+    for (int f = 0; f < GC_NFIELDS; ++f)
+        if (vp.zmask & (1 << f)) zero_field(ctx->sys[vp.src], f);
+}
+
+// VirtualNormUpdater src/StateUpdaters.jl:65-76, PrescribedVelocityUpdater
+// :95-97; other updaters act on the source's fields
+void apply_virtual_updater(Sys& s, Virt& vp, const Upd& u, double dt) {
+    const int64_t n = s.n;
+    const int nd = s.nd, ns = s.ns;
+    if (u.kind == GC_UPD_VIRTUAL_NORM) {
+        const int m = (int)u.prm[3];
+        for (int64_t i = 0; i < n; ++i) {
+            const double w = vp.wsum[i];
+            if (m & (1 << GC_FIELD_V))
+                for (int d = 0; d < nd; ++d) {
+                    const double val = w == 0.0 ? 0.0 : s.v[i * nd + d] / w;
+                    s.v[i * nd + d] = val * u.prm[d] + vp.pv[d];
+                }
+            if (m & (1 << GC_FIELD_RHO)) s.rho[i] = w == 0.0 ? 0.0 : s.rho[i] / w;
+            if (m & (1 << GC_FIELD_P)) s.p[i] = w == 0.0 ? 0.0 : s.p[i] / w;
+            if (m & (1 << GC_FIELD_STRESS))
+                for (int q = 0; q < ns; ++q) s.stress[i * ns + q] = w == 0.0 ? 0.0 : s.stress[i * ns + q] / w;
+        }
+    } else if (u.kind == GC_UPD_PRESCRIBED_V) {
+        for (int64_t i = 0; i < n; ++i)
+            for (int d = 0; d < nd; ++d) s.v[i * nd + d] = s.v[i * nd + d] + vp.pv[d];
+    } else {
+        apply_updater(s, u, dt);
     }
-    // 3-5. ghosts, ghost sort, grids
+}
+
+// _sweep_all_stages! :401-419: auto-zero the virtuals, then per stage the
+// systems' updaters, the ghosts' copiers, the virtuals' updaters and every
+// interaction's sweep
+int sweep_all_stages(oracle_ctx* ctx, int nst, double dt) {
+    for (auto& vp : ctx->virts) auto_zero_virtual(ctx, vp);
+    for (int stage = 1; stage <= nst; ++stage) {
+        for (auto& s : ctx->sys)
+            if (!s.vsrc && s.upd_set && (int)s.upd.size() == nst) update_state(s, stage, dt);
+        for (auto& g : ctx->ghosts) update_ghost(ctx, g, stage);
+        for (auto& vp : ctx->virts)
+            if (vp.upd_set && (int)vp.upd.size() == nst)
+                for (const Upd& u : vp.upd[stage - 1]) apply_virtual_updater(ctx->sys[vp.src], vp, u, dt);
+        for (auto& it : ctx->inters) {
+            int st = sweep(ctx, it, stage);
+            if (st) return st;
+        }
+    }
+    return GC_OK;
+}
+
+// _prepare_grids! :364-379: ghosts, ghost sort, virtual (source) sort, grids
+int prepare_grids(oracle_ctx* ctx, double sort_cutoff) {
     for (auto& g : ctx->ghosts) generate_ghosts(ctx, g);
     for (auto& g : ctx->ghosts) {
         const Sys& src = ctx->sys[g.src];
         int st = sort_ghost(g, src.nd, src.ns, sort_cutoff, nullptr);
         if (st) return fail(ctx, st, "ghost sort: non-finite position");
     }
+    for (auto& vp : ctx->virts) {
+        int st = sort_system(ctx->sys[vp.src], sort_cutoff, nullptr);
+        if (st) return fail(ctx, st, "virtual sort: non-finite position");
+    }
     for (auto& it : ctx->inters) {
         int st = create_grid(ctx, it);
+        if (st) return st;
+    }
+    return GC_OK;
+}
+
+// _update_virtual_positions! :389-397: x += prescribed_v·dt, per virtual system
+void update_virtual_positions(oracle_ctx* ctx, double dt) {
+    for (auto& vp : ctx->virts) {
+        Sys& s = ctx->sys[vp.src];
+        double step[3];
+        for (int d = 0; d < s.nd; ++d) step[d] = vp.pv[d] * dt;
+        for (int64_t i = 0; i < s.n; ++i)
+            for (int d = 0; d < s.nd; ++d) s.x[i * s.nd + d] = s.x[i * s.nd + d] + step[d];
+    }
+}
+
+int step_once(oracle_ctx* ctx, double dt) {
+    const int nst = num_stages(ctx);
+    double hmin = 1e300;
+    for (auto& it : ctx->inters) hmin = std::min(hmin, it.H);
+    const double sort_cutoff = 2.0 * hmin;
+    // 1. sort every real system (a virtual's source is sorted with the virtuals)
+    for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
+        int st = sort_system(s, sort_cutoff, nullptr);
+        if (st) return fail(ctx, st, "sort: non-finite position");
+    }
+    // 2. save q0
+    for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
+        s.q0v = s.v;
+        s.q0rho = s.rho;
+    }
+    // 3-5. ghosts, ghost sort, virtual sort, grids
+    {
+        int st = prepare_grids(ctx, sort_cutoff);
         if (st) return st;
     }
     // 6. half-step: q += dt/2 * dqdt, dqdt <- source
     const double half = dt / 2.0;
     for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
         const int nd = s.nd;
         for (int64_t i = 0; i < s.n * nd; ++i) s.v[i] = s.v[i] + half * s.dvdt[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(half, s.drhodt[i], s.rho[i]);
@@ -1478,23 +1638,20 @@ int step_once(oracle_ctx* ctx, double dt) {
     // 7. ghost kinematics
     for (auto& g : ctx->ghosts) ghost_kinematics(ctx, g);
     // 8. stages
-    for (int stage = 1; stage <= nst; ++stage) {
-        for (auto& s : ctx->sys)
-            if (s.upd_set && (int)s.upd.size() == nst) update_state(s, stage, dt);
-        for (auto& g : ctx->ghosts) update_ghost(ctx, g, stage);
-        for (auto& it : ctx->inters) {
-            int st = sweep(ctx, it, stage);
-            if (st) return st;
-        }
+    {
+        int st = sweep_all_stages(ctx, nst, dt);
+        if (st) return st;
     }
     // 8b. damping
     if (ctx->gamma != 0.0) {
         const double gdt = ctx->gamma / dt;
         for (auto& s : ctx->sys)
-            for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
+            if (!s.vsrc)
+                for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
     }
     // 9. full step: q = q0 + dt * dqdt
     for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.dvdt[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.drhodt[i], s.q0rho[i]);
     }
@@ -1503,9 +1660,11 @@ int step_once(oracle_ctx* ctx, double dt) {
         int st = xsph_correction(ctx);
         if (st) return st;
     }
-    // 11. positions
+    // 11. positions, then the virtual systems'
     for (auto& s : ctx->sys)
-        for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+        if (!s.vsrc)
+            for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+    update_virtual_positions(ctx, dt);
     ctx->steps += 1;
     return GC_OK;
 }
@@ -1521,25 +1680,21 @@ int step_rk4(oracle_ctx* ctx, double dt) {
     const double sort_cutoff = 2.0 * hmin;
     // 1. sort every real system
     for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
         int st = sort_system(s, sort_cutoff, nullptr);
         if (st) return fail(ctx, st, "sort: non-finite position");
     }
     // 2. save q0, zero the accumulators (:783-784)
     for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
         s.q0v = s.v;
         s.q0rho = s.rho;
         s.accv.assign(s.v.size(), 0.0);
         s.accrho.assign(s.rho.size(), 0.0);
     }
-    // 3-5. ghosts, ghost sort, grids (:787-788)
-    for (auto& g : ctx->ghosts) generate_ghosts(ctx, g);
-    for (auto& g : ctx->ghosts) {
-        const Sys& src = ctx->sys[g.src];
-        int st = sort_ghost(g, src.nd, src.ns, sort_cutoff, nullptr);
-        if (st) return fail(ctx, st, "ghost sort: non-finite position");
-    }
-    for (auto& it : ctx->inters) {
-        int st = create_grid(ctx, it);
+    // 3-5. ghosts, ghost sort, virtual sort, grids (:787-788)
+    {
+        int st = prepare_grids(ctx, sort_cutoff);
         if (st) return st;
     }
     // T(0.5), T(1.0), T(1/6), T(1/3) (:742-743)
@@ -1549,6 +1704,7 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         // 6. reset dqdt (first stage) or q = q0 + (f·dt)·dqdt then reset (:797-803)
         const double c = advance[rk] * dt;
         for (auto& s : ctx->sys) {
+            if (s.vsrc) continue;
             const int nd = s.nd;
             if (rk > 0) {
                 for (int64_t i = 0; i < s.n * nd; ++i) s.v[i] = s.q0v[i] + c * s.dvdt[i];
@@ -1561,28 +1717,26 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         // 7. ghost kinematics (:805-807)
         for (auto& g : ctx->ghosts) ghost_kinematics(ctx, g);
         // 8. stages (:809-810)
-        for (int stage = 1; stage <= nst; ++stage) {
-            for (auto& s : ctx->sys)
-                if (s.upd_set && (int)s.upd.size() == nst) update_state(s, stage, dt);
-            for (auto& g : ctx->ghosts) update_ghost(ctx, g, stage);
-            for (auto& it : ctx->inters) {
-                int st = sweep(ctx, it, stage);
-                if (st) return st;
-            }
+        {
+            int st = sweep_all_stages(ctx, nst, dt);
+            if (st) return st;
         }
         // damping and acc += w·dqdt (:812-814)
         if (ctx->gamma != 0.0) {
             const double gdt = ctx->gamma / dt;
             for (auto& s : ctx->sys)
-                for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
+                if (!s.vsrc)
+                    for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
         }
         for (auto& s : ctx->sys) {
+            if (s.vsrc) continue;
             for (int64_t i = 0; i < s.n * s.nd; ++i) s.accv[i] = s.accv[i] + weight[rk] * s.dvdt[i];
             for (int64_t i = 0; i < s.n; ++i) s.accrho[i] = std::fma(weight[rk], s.drhodt[i], s.accrho[i]);
         }
     }
     // 9. q = q0 + dt·acc (:818)
     for (auto& s : ctx->sys) {
+        if (s.vsrc) continue;
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.accv[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.accrho[i], s.q0rho[i]);
     }
@@ -1591,16 +1745,19 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         int st = xsph_correction(ctx);
         if (st) return st;
     }
-    // 11. positions (:824)
+    // 11. positions (:824), then the virtual systems' (:825)
     for (auto& s : ctx->sys)
-        for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+        if (!s.vsrc)
+            for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+    update_virtual_positions(ctx, dt);
     ctx->steps += 1;
     return GC_OK;
 }
 
 double compute_dt(oracle_ctx* ctx, double cfl) {
     double c = -1e300, h = 1e300;
-    for (auto& s : ctx->sys) c = std::max(c, s.c);
+    for (auto& s : ctx->sys)
+        if (!s.vsrc) c = std::max(c, s.c);  // the integrator's systems (:108)
     for (auto& it : ctx->inters) h = std::min(h, it.H);
     return cfl * h / c;
 }
@@ -1805,8 +1962,47 @@ int oracle_add_interaction(oracle_ctx* ctx, int sys_a, int b_handle, int kernel_
     return GC_OK;
 }
 
+int oracle_add_virtual(oracle_ctx* ctx, int src_sys, int zero_mask, const double* prescribed_v, int* handle_out) {
+    int si = sys_index(ctx, src_sys);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "a virtual system needs a source system");
+    Virt vp;
+    vp.src = si;
+    vp.zmask = zero_mask;
+    Sys& s = ctx->sys[si];
+    if (prescribed_v)
+        for (int d = 0; d < s.nd; ++d) vp.pv[d] = prescribed_v[d];
+    vp.wsum.assign((size_t)s.n, 0.0);
+    s.vsrc = true;
+    ctx->virts.push_back(vp);
+    Handle h;
+    h.type = H_VIRT;
+    h.idx = (int)ctx->virts.size() - 1;
+    ctx->handles.push_back(h);
+    *handle_out = (int)ctx->handles.size() - 1;
+    return GC_OK;
+}
+
 int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_len, const int* kinds,
                         const double* params) {
+    if (sys >= 0 && sys < (int)ctx->handles.size() && ctx->handles[sys].type == H_VIRT) {
+        Virt& vp = ctx->virts[ctx->handles[sys].idx];
+        vp.upd.clear();
+        vp.upd_set = true;
+        int pos = 0;
+        for (int st = 0; st < nstages; ++st) {
+            std::vector<Upd> chain;
+            for (int k = 0; k < chain_len[st]; ++k, ++pos) {
+                Upd u;
+                u.kind = kinds[pos];
+                for (int q = 0; q < GC_UPD_NPARAM; ++q) u.prm[q] = params[pos * GC_UPD_NPARAM + q];
+                if (u.kind != GC_UPD_ZERO_FIELDS && u.kind != GC_UPD_VIRTUAL_NORM && u.kind != GC_UPD_PRESCRIBED_V)
+                    return fail(ctx, GC_ERR_UNSUPPORTED, "updater kind on a virtual system");
+                chain.push_back(u);
+            }
+            vp.upd.push_back(chain);
+        }
+        return GC_OK;
+    }
     int si = sys_index(ctx, sys);
     if (si < 0) return fail(ctx, GC_ERR_ARG, "updaters need a system");
     Sys& s = ctx->sys[si];
@@ -1825,6 +2021,8 @@ int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_
                 return fail(ctx, GC_ERR_ARG, "EOS updater needs a pressure field");
             if (u.kind == GC_UPD_VISCOPLASTIC_MC && (!s.has_stress() || (s.ns != 3 && s.ns != 4 && s.ns != 6)))
                 return fail(ctx, GC_ERR_ARG, "ViscoPlasticMCStressUpdater needs stress with NS = 3, 4 or 6");
+            if (u.kind == GC_UPD_VIRTUAL_NORM || u.kind == GC_UPD_PRESCRIBED_V)
+                return fail(ctx, GC_ERR_ARG, "this updater acts on a virtual system");
             chain.push_back(u);
         }
         s.upd.push_back(chain);
@@ -1871,13 +2069,22 @@ int oracle_set_field(oracle_ctx* ctx, int handle, int field, const void* host, s
 int oracle_get_count(oracle_ctx* ctx, int handle, int64_t* n_out) {
     if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
     const Handle& h = ctx->handles[handle];
-    *n_out = h.type == H_GHOST ? ctx->ghosts[h.idx].n : ctx->sys[h.idx].n;
+    *n_out = h.type == H_GHOST  ? ctx->ghosts[h.idx].n
+             : h.type == H_VIRT ? ctx->sys[ctx->virts[h.idx].src].n
+                                : ctx->sys[h.idx].n;
     return GC_OK;
 }
 
 int oracle_get_field(oracle_ctx* ctx, int handle, int field, void* host, size_t bytes) {
     if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
     const Handle& h = ctx->handles[handle];
+    if (h.type == H_VIRT) {
+        const Virt& vp = ctx->virts[h.idx];
+        if (field != GC_FIELD_W_SUM) return fail(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
+        if (bytes != vp.wsum.size() * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+        if (bytes) std::memcpy(host, vp.wsum.data(), bytes);
+        return GC_OK;
+    }
     if (h.type == H_GHOST) {
         Ghost& g = ctx->ghosts[h.idx];
         const Sys& s = ctx->sys[g.src];
@@ -1999,6 +2206,12 @@ int oracle_sweep(oracle_ctx* ctx, int inter, int stage) {
 }
 
 int oracle_update_state(oracle_ctx* ctx, int sys, int stage, double dt) {
+    if (sys >= 0 && sys < (int)ctx->handles.size() && ctx->handles[sys].type == H_VIRT) {
+        Virt& vp = ctx->virts[ctx->handles[sys].idx];
+        if (stage >= 1 && stage <= (int)vp.upd.size())
+            for (const Upd& u : vp.upd[stage - 1]) apply_virtual_updater(ctx->sys[vp.src], vp, u, dt);
+        return GC_OK;
+    }
     int si = sys_index(ctx, sys);
     if (si < 0) return fail(ctx, GC_ERR_ARG, "not a system handle");
     update_state(ctx->sys[si], stage, dt);

@@ -51,6 +51,7 @@ def lib():
             "oracle_set_integrator": (ct.c_int, [ct.c_void_p, ct.c_double]),
             "oracle_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int]),
             "oracle_set_velocity_adjust": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double]),
+            "oracle_add_virtual": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _dp, _ip]),
             "oracle_set_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
             "oracle_get_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
             "oracle_get_count": (ct.c_int, [ct.c_void_p, ct.c_int, _i64p]),
@@ -164,6 +165,13 @@ class OracleBackend:
 
     def set_integrator(self, inst, gamma):
         self._chk(self.L.oracle_set_integrator(self.ctx, gamma), "set_integrator")
+
+    def add_virtual(self, inst, src, zero_mask, prescribed_v):
+        pv = _a(prescribed_v, np.float64)
+        out = ct.c_int()
+        self._chk(self.L.oracle_add_virtual(self.ctx, src, zero_mask, pv.ctypes.data_as(_dp), ct.byref(out)),
+                  "add_virtual")
+        return out.value
 
     def set_velocity_adjust(self, inst, inter, kind, epsilon):
         self._chk(self.L.oracle_set_velocity_adjust(self.ctx, inter, kind, epsilon), "set_velocity_adjust")
