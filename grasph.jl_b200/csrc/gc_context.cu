@@ -45,6 +45,7 @@ struct HSys {
     bool upd_set = false;
     std::vector<std::vector<HUpd>> upd;
     bool vsrc = false;  // the source of a virtual system (not integrated)
+    bool probe = false; // a probe's own arrays (the count extra lives in drhodt)
 };
 enum { H_SYS = 0, H_DYN = 1, H_STATIC = 2, H_GHOST = 3, H_VIRT = 4 };
 // VirtualParticleSystem src/Particles.jl:476-528 over source system `src`
@@ -54,6 +55,8 @@ struct HVirt {
     double pv[3] = {0, 0, 0};
     bool upd_set = false;
     std::vector<std::vector<HUpd>> upd;
+    bool probe = false;  // ProbeParticleSystem src/ProbeParticles.jl:23-102 (source = its own arrays)
+    int mirror = -1;     // its mirror_target system, or -1
 };
 struct HHandle {
     int type = H_SYS, idx = 0;
@@ -74,6 +77,7 @@ struct HInter {
     std::vector<std::array<double, GC_PFN_NPARAM>> pp;
     int vk = GC_PFN_NONE;  // velocity_adjust_pairwise_fn
     double veps = 0.0;
+    bool probe = false;    // one of the integrator's probe_interactions
 };
 struct HStaged {
     int handle, field;
@@ -116,6 +120,7 @@ struct DSlot {
     bool written = false;      // some functor writes this system
     bool moving = true;        // sorted and integrated every step
     bool vsrc = false;         // source of a virtual system: never integrated
+    bool probe = false;        // a probe's arrays
     bool vmoves = false;       // a virtual system over it has a non-zero prescribed_v
     bool xmoves() const { return moving || vmoves; }  // positions change every step
     bool sorted_once = false;  // static systems: sorted since the last upload
@@ -178,6 +183,9 @@ struct DVirt {
     int nupd = 0;
     std::vector<std::vector<UpdInst*>> d_upd;
     std::vector<std::vector<int>> upd_kind;
+    bool probe = false;
+    int mirror = -1;             // mirror_target slot of a probe
+    double* wsum_alt = nullptr;  // a probe's w_sum, reordered by id at measurement
 };
 
 // system_b kinds of the host side; BT_VIRTUAL sweeps with the device's
@@ -188,6 +196,7 @@ struct DInter {
     int a = 0, btype = BT_SELF, bslot = -1, bghost = -1, bvirt = -1, kk = 0, nstages = 0;
     bool two_sided = false;  // some stage writes system_b too (a second, system_b-side sweep)
     bool two_fluid = false;  // FluidPfn stages are the two-sided fluid x fluid form
+    bool probe = false;      // a probe interaction: swept by gc_measure_probes only
     bool vadj = false;       // pk[nstages] is the velocity-adjust functor (XSPH)
     std::vector<int> pk;
     GridInst* d_gi = nullptr;
@@ -251,6 +260,7 @@ struct gc_ctx {
     int64_t* d_need = nullptr;
     int64_t* h_need = nullptr;  // pinned
     int nneed = 0;
+    int nplan = 0;  // entries of d_plan_args (the steps' interactions)
     int64_t* d_total_cells = nullptr;  // device copy of the current sort's cell total
     int64_t grid_version = 0;
     int num_sms = 148;
@@ -383,6 +393,7 @@ int sys_comps(const HSys& s, int field) {
         case GC_FIELD_STRESS: case GC_FIELD_STRAIN_RATE: return s.kind >= GC_SYS_STRESS ? s.ns : -1;
         case GC_FIELD_VORTICITY: return s.kind == GC_SYS_ELASTOPLASTIC ? s.nvort : -1;
         case GC_FIELD_STRAIN: case GC_FIELD_STRAIN_P: return s.kind == GC_SYS_ELASTOPLASTIC ? s.ns : -1;
+        case GC_FIELD_COUNT: return s.probe ? 1 : -1;
         default: return -1;
     }
 }
@@ -401,6 +412,7 @@ int field_slot(int field) {
         case GC_FIELD_STRAIN: return F_STRAIN;
         case GC_FIELD_STRAIN_P: return F_STRAINP;
         case GC_FIELD_V_ADJUSTMENT: return F_VADJ;
+        case GC_FIELD_COUNT: return F_DRHODT;  // a probe's count extra
         default: return -1;
     }
 }
@@ -423,7 +435,7 @@ bool b_side_at(const DInter& D, int stage) {
     const int pk = D.pk[stage - 1];
     if (pk == GC_PFN_COUNT) return D.btype != BT_SELF && D.btype != BT_GHOST && D.bslot >= 0;
     if (pk == GC_PFN_XSPH) return D.btype != BT_SELF;
-    if (pk == GC_PFN_FLUID_SOLID || pk == GC_PFN_INTERPOLATE) return true;
+    if (pk == GC_PFN_FLUID_SOLID || pk == GC_PFN_INTERPOLATE || pk == GC_PFN_NEIGHBOR_COUNT) return true;
     return pk == GC_PFN_FLUID && D.two_fluid;
 }
 
@@ -433,7 +445,12 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     if (pk == GC_PFN_NONE) return GC_OK;
     if (pk == GC_PFN_XSPH)
         return seterr(ctx, GC_ERR_UNSUPPORTED, "XSPHPfn is swept as velocity_adjust_pairwise_fn, not as a stage");
-    if (pk < 0 || pk > GC_PFN_INTERPOLATE) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (pk < 0 || pk > GC_PFN_NEIGHBOR_COUNT) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (pk == GC_PFN_NEIGHBOR_COUNT) {  // the (real, probe) method, src/PairwiseFunctors.jl:455
+        if (it.b < 0 || I.handles[it.b].type != H_VIRT || !I.virts[I.handles[it.b].idx].probe)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "NeighborCountFn needs a probe as system_b");
+        return GC_OK;
+    }
     if (pk == GC_PFN_INTERPOLATE) {
         // the (real, virtual) method, src/PairwiseFunctors.jl:424; the fields exist on both sides
         if (it.b < 0 || I.handles[it.b].type != H_VIRT)
@@ -496,8 +513,9 @@ bool same_structure(const HInst& a, const HInst& b, std::string& why) {
     if (a.virts.size() != b.virts.size()) return why = "virtual systems", false;
     for (size_t v = 0; v < a.virts.size(); ++v) {
         const HVirt &x = a.virts[v], &y = b.virts[v];
-        if (x.src != y.src || x.zmask != y.zmask || x.upd_set != y.upd_set || x.upd.size() != y.upd.size())
-            return why = "virtual systems", false;
+        if (x.src != y.src || x.zmask != y.zmask || x.upd_set != y.upd_set || x.upd.size() != y.upd.size() ||
+            x.probe != y.probe || x.mirror != y.mirror)
+            return why = "virtual systems or probes", false;
         for (size_t t = 0; t < x.upd.size(); ++t) {
             if (x.upd[t].size() != y.upd[t].size()) return why = "virtual updaters", false;
             for (size_t q = 0; q < x.upd[t].size(); ++q)
@@ -526,7 +544,8 @@ bool same_structure(const HInst& a, const HInst& b, std::string& why) {
     if (a.inters.size() != b.inters.size()) return why = "interactions", false;
     for (size_t i = 0; i < a.inters.size(); ++i) {
         const HInter &x = a.inters[i], &y = b.inters[i];
-        if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk || x.vk != y.vk)
+        if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk || x.vk != y.vk ||
+            x.probe != y.probe)
             return why = "interactions", false;
         for (int s = 0; s < x.nstages; ++s) {
             if (x.pp[s][3] != y.pp[s][3] || std::isnan(x.pp[s][4]) != std::isnan(y.pp[s][4]))
@@ -576,11 +595,17 @@ int finalize(gc_ctx* ctx) {
             return seterr(ctx, GC_ERR_ARG, "instance %zu differs from instance 0 in %s", k, why.c_str());
     }
     CU(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    ctx->nstages = I0.inters[0].nstages;
+    ctx->nstages = 0;
+    for (auto& it : I0.inters)
+        if (!it.probe) {
+            ctx->nstages = it.nstages;
+            break;
+        }
+    if (ctx->nstages == 0) return seterr(ctx, GC_ERR_ARG, "interactions must not be empty");
     ctx->xsph = false;
     for (auto& it : I0.inters) ctx->xsph |= it.vk != GC_PFN_NONE;
     for (auto& it : I0.inters)
-        if (it.nstages != ctx->nstages)
+        if (!it.probe && it.nstages != ctx->nstages)
             return seterr(ctx, GC_ERR_ARG, "All interactions must have the same number of stages (pfns length)");
     if (ctx->nstages > MAX_STAGES) return seterr(ctx, GC_ERR_UNSUPPORTED, "too many stages");
     const int ninst = (int)ctx->inst.size();
@@ -588,7 +613,8 @@ int finalize(gc_ctx* ctx) {
     // per-instance dt inputs
     std::vector<double> hmin(ninst, 1e300), cmax(ninst, -1e300);
     for (int k = 0; k < ninst; ++k) {
-        for (auto& it : ctx->inst[k].inters) hmin[k] = std::min(hmin[k], it.H);
+        for (auto& it : ctx->inst[k].inters)
+            if (!it.probe) hmin[k] = std::min(hmin[k], it.H);
         for (auto& s : ctx->inst[k].sys) cmax[k] = std::max(cmax[k], s.c);
     }
 
@@ -603,6 +629,7 @@ int finalize(gc_ctx* ctx) {
         D.nvort = h0.nvort;
         D.kind = h0.kind;
         D.vsrc = h0.vsrc;
+        D.probe = h0.probe;
         D.moving = !D.vsrc;
         D.h_inst.resize(ninst);
         D.nonzero_kin.assign(ninst, 0);
@@ -699,6 +726,9 @@ int finalize(gc_ctx* ctx) {
         V.zmask = h0.zmask;
         V.upd_set = h0.upd_set;
         V.nupd = (int)h0.upd.size();
+        V.probe = h0.probe;
+        V.mirror = h0.mirror;
+        if (V.probe) TRY(dalloc(ctx, &V.wsum_alt, (size_t)std::max<int64_t>(S.N, 1)));
         TRY(dalloc(ctx, &V.wsum, (size_t)std::max<int64_t>(S.N, 1)));
         CU(cudaMemsetAsync(V.wsum, 0, sizeof(double) * std::max<int64_t>(S.N, 1), ctx->stream));
         std::vector<VirtInst> vi(ninst);
@@ -805,6 +835,7 @@ int finalize(gc_ctx* ctx) {
         D.kk = h0.kk;
         D.nstages = h0.nstages;
         D.pk = h0.pk;
+        D.probe = h0.probe;
         D.vadj = h0.vk != GC_PFN_NONE;
         if (D.vadj) D.pk.push_back(h0.vk);  // the XSPH pass sweeps it as stage nstages + 1
         if (h0.b < 0) {
@@ -957,8 +988,10 @@ int finalize(gc_ctx* ctx) {
     for (size_t i = 0; i < ctx->inters.size(); ++i)
         ctx->inters[i].need_slot = (int64_t)(ctx->slots.size() + ctx->ghosts.size() + i);
     {
-        std::vector<GridPlanArgs> pa;
-        for (auto& D : ctx->inters) pa.push_back(grid_plan_args(ctx, D));
+        std::vector<GridPlanArgs> pa;  // the steps' interactions; probe grids are planned at measurement
+        for (auto& D : ctx->inters)
+            if (!D.probe) pa.push_back(grid_plan_args(ctx, D));
+        ctx->nplan = (int)pa.size();
         TRY(dalloc(ctx, &ctx->d_plan_args, pa.size()));
         TRY(hcopy(ctx, ctx->d_plan_args, pa.data(), pa.size() * sizeof(GridPlanArgs), cudaMemcpyHostToDevice));
     }
@@ -1289,7 +1322,7 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
         g_launches.fetch_add(1, std::memory_order_relaxed);
         launch_sort_plan(G.d_inst, ni, G.nd, ctx->d_need + G.need_slot, ctx->d_err, ctx->stream);
     }
-    launch_grid_plan_all(ctx->d_plan_args, (int)ctx->inters.size(), ctx->stream);
+    launch_grid_plan_all(ctx->d_plan_args, ctx->nplan, ctx->stream);
     TRY(check_launch(ctx, "plan"));
     std::vector<int64_t> need(ctx->nneed);
     if (ctx->capmode) {
@@ -1298,7 +1331,7 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
         g_launches.fetch_add(1, std::memory_order_relaxed);
         for (size_t s = 0; s < ctx->slots.size(); ++s) need[s] = cap_sort_cells(ctx);
         for (auto& G : ctx->ghosts) need[G.need_slot] = cap_sort_cells(ctx);
-        for (auto& D : ctx->inters) need[D.need_slot] = cap_grid_cells(ctx, D);
+        for (auto& D : ctx->inters) need[D.need_slot] = D.probe ? 0 : cap_grid_cells(ctx, D);
     } else {
         TRY(read_need(ctx));
         for (int i = 0; i < ctx->nneed; ++i) {
@@ -1318,6 +1351,7 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     // grids (ghost-b plans are recomputed from the exact ghost boxes; the
     // cell count cannot exceed the planned bound)
     for (auto& D : ctx->inters) {
+        if (D.probe) continue;
         if (D.btype == BT_GHOST) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
         TRY(build_grid(ctx, D, need[D.need_slot]));
     }
@@ -1547,6 +1581,7 @@ int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
         TRY(ensure_csa(ctx, D));
         TRY(ensure_groups(ctx, D.bslot, id, true));
         const auto& prm = ctx->inst[0].inters[id].pp[stage - 1];
+        const bool count = D.pk[stage - 1] == GC_PFN_NEIGHBOR_COUNT;  // NeighborCountFn :455-460
         ForceArgs R{};
         R.nd = B.nd;
         R.ns = B.ns;
@@ -1562,7 +1597,7 @@ int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
         R.advdt = B.F(F_V);        // accumulation targets: v, rho, stress, w_sum
         R.adrhodt = B.F(F_RHO);
         R.asr = B.F(F_STRESS);
-        R.avort = V.wsum;
+        R.avort = count ? B.F(F_DRHODT) : V.wsum;  // w_sum, or the count extra
         R.a_c = B.d_c;
         R.a_mass = B.d_mass;
         R.a_cf = B.d_cf;
@@ -1573,8 +1608,8 @@ int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
         R.ngroups = B.d_ngroups;
         R.num_sms = ctx->num_sms;
         R.cfg = ctx->force_cfg >= 0 ? ctx->force_cfg : 0;
-        R.imask = (int)prm[0];
-        R.iwsum = prm[1] != 0.0 ? 1 : 0;
+        R.imask = count ? 0 : (int)prm[0];
+        R.iwsum = count ? 2 : (prm[1] != 0.0 ? 1 : 0);
         R.nref = 1;
         InterRef& r = R.ref[0];
         r.btype = BT_SYSTEM;
@@ -1600,7 +1635,8 @@ int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
 int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
     DSlot& S = ctx->slots[a];
     const int pk0 = ctx->inters[ids[0]].pk[stage - 1];
-    if (pk0 == GC_PFN_INTERPOLATE && !count_only) return interp_sweeps(ctx, a, ids, stage);
+    if ((pk0 == GC_PFN_INTERPOLATE || pk0 == GC_PFN_NEIGHBOR_COUNT) && !count_only)
+        return interp_sweeps(ctx, a, ids, stage);
     // FluidSolidPfn runs the FluidPfn kernel in its fluid-solid mode (PfnInst.fs)
     const int pfn = pk0 == GC_PFN_FLUID_SOLID ? GC_PFN_FLUID : pk0;
     const int mode = aux_mode_for(pfn);
@@ -1842,6 +1878,7 @@ int sweep_stage(gc_ctx* ctx, int stage) {
         std::vector<int> kinds;
         for (size_t i = 0; i < ctx->inters.size(); ++i) {
             DInter& D = ctx->inters[i];
+            if (D.probe) continue;
             int pk = D.pk[stage - 1];
             if (D.a != (int)a || pk == GC_PFN_NONE) continue;
             if (std::find(kinds.begin(), kinds.end(), pk) == kinds.end()) kinds.push_back(pk);
@@ -1849,7 +1886,8 @@ int sweep_stage(gc_ctx* ctx, int stage) {
         for (int pk : kinds) {
             std::vector<int> ids;
             for (size_t i = 0; i < ctx->inters.size(); ++i)
-                if (ctx->inters[i].a == (int)a && ctx->inters[i].pk[stage - 1] == pk) ids.push_back((int)i);
+                if (!ctx->inters[i].probe && ctx->inters[i].a == (int)a && ctx->inters[i].pk[stage - 1] == pk)
+                    ids.push_back((int)i);
             for (size_t off = 0; off < ids.size(); off += MAX_REFS) {
                 std::vector<int> chunk(ids.begin() + off, ids.begin() + std::min(ids.size(), off + MAX_REFS));
                 TRY(sweep_group(ctx, (int)a, chunk, stage, false));
@@ -1864,7 +1902,8 @@ void upload_inst_params(gc_ctx* ctx, double cfl) {
     for (int k = 0; k < ni; ++k) {
         const HInst& I = ctx->inst[k];
         double h = 1e300, c = -1e300;
-        for (auto& it : I.inters) h = std::min(h, it.H);
+        for (auto& it : I.inters)
+            if (!it.probe) h = std::min(h, it.H);
         for (auto& s : I.sys)
             if (!s.vsrc) c = std::max(c, s.c);  // the integrator's systems (src/TimeIntegration.jl:63)
         double dt = (std::isfinite(I.cfl) ? I.cfl : cfl) * h / c;
@@ -1924,6 +1963,7 @@ int one_step_rk4(gc_ctx* ctx);
 // ghosts' copiers, the virtual systems' updaters and the sweeps.
 int sweep_all_stages(gc_ctx* ctx) {
     for (auto& V : ctx->virts) {
+        if (V.probe) continue;  // probes are cleared at measurement
         DSlot& S = ctx->slots[V.src];
         CU(cudaMemsetAsync(V.wsum, 0, sizeof(double) * S.N, ctx->stream));
         for (int f = 0; f < GC_NFIELDS; ++f) {
@@ -1937,7 +1977,7 @@ int sweep_all_stages(gc_ctx* ctx) {
             if (!S.vsrc && S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
         for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
         for (auto& V : ctx->virts)
-            if (V.upd_set && V.nupd == ctx->nstages) TRY(run_virtual_updaters(ctx, V, stage));
+            if (!V.probe && V.upd_set && V.nupd == ctx->nstages) TRY(run_virtual_updaters(ctx, V, stage));
         TRY(sweep_stage(ctx, stage));
     }
     return GC_OK;
@@ -1979,7 +2019,7 @@ int one_step(gc_ctx* ctx) {
     std::vector<char> mask(ctx->slots.size());
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
-        mask[s] = S.xmoves() || !S.sorted_once;
+        mask[s] = !S.probe && (S.xmoves() || !S.sorted_once);  // probes: sorted at measurement
     }
     TRY(prepare(ctx, mask));
     for (size_t s = 0; s < ctx->slots.size(); ++s)
@@ -2006,7 +2046,7 @@ int one_step_rk4(gc_ctx* ctx) {
     std::vector<char> mask(ctx->slots.size());
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& S = ctx->slots[s];
-        mask[s] = S.xmoves() || !S.sorted_once;
+        mask[s] = !S.probe && (S.xmoves() || !S.sorted_once);  // probes: sorted at measurement
         if (S.moving && !S.accv) {
             TRY(dalloc(ctx, &S.accv, (size_t)S.nd * S.N));
             TRY(dalloc(ctx, &S.accrho, (size_t)S.N));
@@ -2152,6 +2192,7 @@ int size_capacities(gc_ctx* ctx) {
     for (int i = 0; i < n; ++i) all = std::max(all, ctx->need_max[i]);
     if (ctx->cap_cells - 1 < low(all)) TRY(ensure_cells(ctx, want(all)));
     for (auto& D : ctx->inters) {
+        if (D.probe) continue;
         const int64_t nm = ctx->need_max[D.need_slot];
         if (D.cap_cells - 1 < low(nm)) TRY(ensure_inter_cells(ctx, D, want(nm)));
     }
@@ -2167,6 +2208,7 @@ int size_capacities(gc_ctx* ctx) {
     }
     // warp-group column tables of every system a grid groups
     for (auto& D : ctx->inters) {
+        if (D.probe) continue;
         const int64_t cells = cap_grid_cells(ctx, D);
         TRY(grow_gcols(ctx, ctx->slots[D.a], cells));
         if (D.two_sided && D.bslot >= 0) TRY(grow_gcols(ctx, ctx->slots[D.bslot], cells));
@@ -2176,7 +2218,7 @@ int size_capacities(gc_ctx* ctx) {
     std::vector<int64_t> cap(n);
     for (size_t s = 0; s < ctx->slots.size(); ++s) cap[s] = cap_sort_cells(ctx);
     for (auto& G : ctx->ghosts) cap[G.need_slot] = cap_sort_cells(ctx);
-    for (auto& D : ctx->inters) cap[D.need_slot] = cap_grid_cells(ctx, D);
+    for (auto& D : ctx->inters) cap[D.need_slot] = D.probe ? INT64_MAX : cap_grid_cells(ctx, D);
     TRY(hcopy(ctx, ctx->d_need_cap, cap.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
     return GC_OK;
 }
@@ -2338,7 +2380,12 @@ int run_steps(gc_ctx* ctx, int nsteps) {
         // moving system into its other buffers and leaves the current ones
         // untouched, so going back is a flip of the buffer parities.
         std::vector<char> par0;
-        if (W == 1) par0 = parity(ctx);
+        // a probe moved by prescribed_v is not re-sorted in the step, so only
+        // a snapshot takes it back
+        bool probe_moves = false;
+        for (auto& S : ctx->slots) probe_moves |= S.probe && S.vmoves;
+        const bool snap = W > 1 || probe_moves;
+        if (!snap) par0 = parity(ctx);
         else TRY(snapshot(ctx, par0));
         if (ctx->alloc_epoch != ctx->graphs_epoch || graph_key(ctx) != ctx->graphs_key) {
             drop_graphs(ctx);
@@ -2369,7 +2416,7 @@ int run_steps(gc_ctx* ctx, int nsteps) {
         if (e & ERR_CAPACITY) {
             // a plan outgrew a capacity: back to the snapshot, then the same
             // steps exactly (which size every buffer from the plan)
-            if (W == 1) set_parity(ctx, par0);
+            if (!snap) set_parity(ctx, par0);
             else TRY(restore(ctx, par0));
             ctx->steps_done -= ran;
             ctx->resorts -= ran;
@@ -2486,6 +2533,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
     }
     for (auto& V : ctx->virts) {
         cudaFree(V.wsum);
+        cudaFree(V.wsum_alt);
         cudaFree(V.d_vi);
         for (auto& chain : V.d_upd)
             for (auto* p : chain) cudaFree(p);
@@ -2718,6 +2766,182 @@ int gc_add_virtual(gc_ctx* ctx, int inst, int src_sys, int zero_mask, const doub
     return GC_OK;
 }
 
+int gc_add_probe(gc_ctx* ctx, int inst, int64_t n, int ndims, const double* positions, int mirror_sys,
+                 int extras_mask, int ns, const double* prescribed_v, int* handle_out) {
+    if (!ctx || !handle_out) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
+    if (n <= 0) return seterr(ctx, GC_ERR_ARG, "positions must not be empty");
+    if (ndims < 2 || ndims > 3) return seterr(ctx, GC_ERR_UNSUPPORTED, "ndims must be 2 or 3, got %d", ndims);
+    HInst& I = ctx->inst[inst];
+    int mi = -1;
+    if (mirror_sys >= 0) {
+        mi = sys_of(ctx, inst, mirror_sys);
+        if (mi < 0 || I.sys[mi].n != n || I.sys[mi].nd != ndims)
+            return seterr(ctx, GC_ERR_ARG, "mirror target must be a system of n particles");
+    } else if (!positions) {
+        return seterr(ctx, GC_ERR_ARG, "probe positions or a mirror target are required");
+    }
+    const int allowed = (1 << GC_FIELD_V) | (1 << GC_FIELD_RHO) | (1 << GC_FIELD_P) | (1 << GC_FIELD_STRESS) |
+                        (1 << GC_FIELD_COUNT);
+    if (extras_mask & ~allowed) return seterr(ctx, GC_ERR_UNSUPPORTED, "probe extras outside v, rho, p, stress, count");
+    const bool st = extras_mask & (1 << GC_FIELD_STRESS);
+    if (st && !(ns == 3 || ns == 4 || ns == 6)) return seterr(ctx, GC_ERR_ARG, "ns must be 3, 4, or 6");
+    HSys s;
+    s.kind = st ? GC_SYS_STRESS : (extras_mask & (1 << GC_FIELD_P)) ? GC_SYS_FLUID : GC_SYS_BASIC;
+    s.nd = ndims;
+    s.ns = st ? ns : 0;
+    s.n = n;
+    s.vsrc = true;
+    s.probe = true;
+    I.sys.push_back(s);
+    HVirt v;
+    v.src = (int)I.sys.size() - 1;
+    v.probe = true;
+    v.mirror = mi;
+    if (prescribed_v)
+        for (int d = 0; d < ndims; ++d) v.pv[d] = prescribed_v[d];
+    I.virts.push_back(v);
+    HHandle h;
+    h.type = H_VIRT;
+    h.idx = (int)I.virts.size() - 1;
+    I.handles.push_back(h);
+    *handle_out = (int)I.handles.size() - 1;
+    if (positions)
+        TRY(gc_stage_field(ctx, inst, *handle_out, GC_FIELD_X, positions, (size_t)(n * ndims * 8)));
+    return GC_OK;
+}
+
+int gc_add_probe_interaction(gc_ctx* ctx, int inst, int sys_a, int probe, int kernel_kind, double h,
+                             int pfn_kind, const double* pfn_params, int* inter_out) {
+    if (!ctx || !inter_out || !pfn_params) return GC_ERR_ARG;
+    if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
+    int si = sys_of(ctx, inst, sys_a);
+    if (si < 0) return seterr(ctx, GC_ERR_ARG, "system_a must be a system handle");
+    HInst& I = ctx->inst[inst];
+    if (probe < 0 || probe >= (int)I.handles.size() || I.handles[probe].type != H_VIRT ||
+        !I.virts[I.handles[probe].idx].probe)
+        return seterr(ctx, GC_ERR_ARG, "system_b must be a probe");
+    if (pfn_kind != GC_PFN_INTERPOLATE && pfn_kind != GC_PFN_NEIGHBOR_COUNT)
+        return seterr(ctx, GC_ERR_UNSUPPORTED, "probe interactions take InterpolateFieldFn or NeighborCountFn");
+    if (kernel_kind != GC_KERNEL_CUBIC_SPLINE && kernel_kind != GC_KERNEL_WENDLAND_C2)
+        return seterr(ctx, GC_ERR_ARG, "bad kernel kind");
+    HInter it;
+    it.a = si;
+    it.b = probe;
+    it.kk = kernel_kind;
+    it.H = h;
+    it.nstages = 1;
+    it.probe = true;
+    it.pk.push_back(pfn_kind);
+    std::array<double, GC_PFN_NPARAM> a;
+    for (int k = 0; k < GC_PFN_NPARAM; ++k) a[k] = pfn_params[k];
+    it.pp.push_back(a);
+    TRY(check_combo(ctx, I, it, pfn_kind));
+    I.inters.push_back(it);
+    *inter_out = (int)I.inters.size() - 1;
+    return GC_OK;
+}
+
+// mirror_target positions into probe slots, x_p[id_src[i]] = x_src[i] (the
+// probes are in id order between measurements)
+__global__ void k_probe_mirror(double* __restrict__ xp, int64_t Np, const SysInst* __restrict__ pinst,
+                               const double* __restrict__ xs, int64_t Ns, const int32_t* __restrict__ sid,
+                               const int32_t* __restrict__ sinst_of, int nd) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < Ns; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = pinst[sinst_of[g]].base + sid[g] - 1;
+        for (int d = 0; d < nd; ++d) xp[d * Np + t] = xs[d * Ns + g];
+    }
+}
+
+// perm[base + id - 1] = position: the gather that puts a slot back in id order
+__global__ void k_perm_by_id(const int32_t* __restrict__ id, const int32_t* __restrict__ inst_of,
+                             const SysInst* __restrict__ inst, int64_t N, int32_t* __restrict__ perm) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x)
+        perm[inst[inst_of[g]].base + id[g] - 1] = (int32_t)g;
+}
+
+// sort_particles! of one slot at measurement: its box, its plan, its sort
+static int resort_slot(gc_ctx* ctx, int s) {
+    DSlot& S = ctx->slots[s];
+    TRY(bbox_slot(ctx, S));
+    launch_sort_plan(S.d_inst, ninst(ctx), S.nd, ctx->d_need + s, ctx->d_err, ctx->stream);
+    TRY(read_need(ctx));
+    TRY(sort_particles_slot(ctx, &S, nullptr, ctx->h_need[s], ctx->d_need + s));
+    S.xpk_static = false;
+    S.xpk_epoch = -1;
+    return check_launch(ctx, "measurement sort");
+}
+
+int gc_measure_probes(gc_ctx* ctx) {
+    if (ctx) invalidate_steps(ctx);
+    if (!ctx) return GC_ERR_ARG;
+    if (!ctx->finalized) return seterr(ctx, GC_ERR_STATE, "call gc_finalize first");
+    const unsigned nb = (unsigned)std::max(1, ctx->num_sms * 8);
+    CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
+    // the probe interactions' system_a, re-sorted: positions moved since the step's sort
+    std::vector<char> done(ctx->slots.size(), 0);
+    for (auto& D : ctx->inters)
+        if (D.probe && !done[D.a]) {
+            done[D.a] = 1;
+            TRY(resort_slot(ctx, D.a));
+        }
+    for (auto& V : ctx->virts) {
+        if (!V.probe || V.mirror < 0) continue;
+        DSlot& P = ctx->slots[V.src];
+        DSlot& M = ctx->slots[V.mirror];
+        k_probe_mirror<<<nb, 256, 0, ctx->stream>>>(P.F(F_X), P.N, P.d_inst, M.F(F_X), M.N, M.id[M.cur], M.inst_of,
+                                                    P.nd);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+    for (auto& V : ctx->virts)
+        if (V.probe) TRY(resort_slot(ctx, V.src));
+    for (auto& D : ctx->inters) {
+        if (!D.probe) continue;
+        launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
+        TRY(read_need(ctx));
+        TRY(build_grid(ctx, D, ctx->h_need[D.need_slot]));
+    }
+    // auto_zero_probe! src/ProbeParticles.jl:117-124: w_sum and every extra
+    for (auto& V : ctx->virts) {
+        if (!V.probe) continue;
+        DSlot& P = ctx->slots[V.src];
+        CU(cudaMemsetAsync(V.wsum, 0, sizeof(double) * P.N, ctx->stream));
+        for (int f : {F_V, F_RHO, F_P, F_STRESS, F_DRHODT})
+            if (P.ncomp[f]) CU(cudaMemsetAsync(P.F(f), 0, sizeof(double) * P.ncomp[f] * P.N, ctx->stream));
+    }
+    for (size_t i = 0; i < ctx->inters.size(); ++i)
+        if (ctx->inters[i].probe) TRY(interp_sweeps(ctx, ctx->inters[i].a, {(int)i}, 1));
+    for (auto& V : ctx->virts)  // update_state!(probe): stage 1
+        if (V.probe && V.nupd >= 1) TRY(run_virtual_updaters(ctx, V, 1));
+    // _sort_probe_by_id! src/ProbeParticles.jl:129-143
+    for (auto& V : ctx->virts) {
+        if (!V.probe) continue;
+        DSlot& P = ctx->slots[V.src];
+        k_perm_by_id<<<nb, 256, 0, ctx->stream>>>(P.id[P.cur], P.inst_of, P.d_inst, P.N, ctx->perm);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        GatherArgs ga{};
+        for (int f = 0; f < NF; ++f)
+            if (P.ncomp[f]) {
+                ga.src[ga.nf] = P.F(f);
+                ga.dst[ga.nf] = P.A(f);
+                ga.ncomp[ga.nf++] = P.ncomp[f];
+            }
+        ga.src[ga.nf] = V.wsum;
+        ga.dst[ga.nf] = V.wsum_alt;
+        ga.ncomp[ga.nf++] = 1;
+        ga.isrc[0] = P.id[P.cur];
+        ga.idst[0] = P.id[P.cur ^ 1];
+        ga.ni = 1;
+        launch_gather_fields(ga, P.N, ctx->perm, nullptr, ctx->stream);
+        P.cur ^= 1;
+        std::swap(V.wsum, V.wsum_alt);
+    }
+    TRY(check_launch(ctx, "probe measurement"));
+    return finish_status(ctx);
+}
+
 int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double epsilon) {
     if (!ctx) return GC_ERR_ARG;
     if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
@@ -2826,9 +3050,11 @@ int gc_stage_field(gc_ctx* ctx, int inst, int handle, int field, const void* hos
     if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized: use gc_upload_field");
     if (!valid_inst(ctx, inst)) return seterr(ctx, GC_ERR_ARG, "bad instance");
     HInst& I = ctx->inst[inst];
-    if (handle < 0 || handle >= (int)I.handles.size() || I.handles[handle].type == H_GHOST)
+    if (handle < 0 || handle >= (int)I.handles.size() || I.handles[handle].type == H_GHOST ||
+        (I.handles[handle].type == H_VIRT && !I.virts[I.handles[handle].idx].probe))
         return seterr(ctx, GC_ERR_ARG, "bad system handle");
-    const HSys& hs = I.sys[I.handles[handle].idx];
+    const HHandle& hh = I.handles[handle];
+    const HSys& hs = I.sys[hh.type == H_VIRT ? I.virts[hh.idx].src : hh.idx];
     const int comps = sys_comps(hs, field);
     if (comps < 0 && field != GC_FIELD_V_ADJUSTMENT)
         return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", field);
@@ -2914,6 +3140,7 @@ static int resolve(gc_ctx* ctx, int inst, int handle, HandleRef* r) {
     } else if (h.type == H_VIRT) {
         r->virt = &ctx->virts[h.idx];
         r->sys = ctx->virts[h.idx].src;
+        if (r->virt->probe) r->slot = &ctx->slots[r->sys];  // a probe's fields are its own
     } else {
         r->slot = &ctx->slots[h.idx];
         r->sys = h.idx;
@@ -2952,7 +3179,7 @@ int gc_upload_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
         if (!f.host) return seterr(ctx, GC_ERR_ARG, "null host buffer");
         TRY(resolve(ctx, f.inst, f.handle, &ref[q]));
         if (ref[q].ghost) return seterr(ctx, GC_ERR_ARG, "ghost fields are generated on the device");
-        if (ref[q].virt) return seterr(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
+        if (ref[q].virt && !ref[q].slot) return seterr(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
         const HSys& hs = ctx->inst[f.inst].sys[ref[q].sys];
         comps[q] = sys_comps(hs, f.field);
         if (comps[q] < 0) return seterr(ctx, GC_ERR_ARG, "field %d not present on this system", f.field);
@@ -3031,7 +3258,8 @@ int gc_download_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
         TRY(resolve(ctx, f.inst, f.handle, &ref[q]));
         if (ref[q].ghost) continue;
         const HSys& hs = ctx->inst[f.inst].sys[ref[q].sys];
-        if (ref[q].virt) {  // a virtual system holds only w_sum; its fields are its source's
+        if (ref[q].virt && (f.field == GC_FIELD_W_SUM || !ref[q].slot)) {
+            // a virtual system holds only w_sum; its fields are its source's (a probe's are its own)
             if (f.field != GC_FIELD_W_SUM) return seterr(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
             if (f.bytes != (size_t)(hs.n * 8)) return seterr(ctx, GC_ERR_ARG, "byte count mismatch (%zu)", f.bytes);
             comps[q] = 1;
@@ -3053,7 +3281,7 @@ int gc_download_fields(gc_ctx* ctx, int nio, const gc_field_io* io) {
         const int64_t n = ctx->inst[f.inst].sys[ref[q].sys].n, base = S.h_inst[f.inst].base;
         double* st = ctx->staging + off;
         off += n * comps[q];
-        if (ref[q].virt) {
+        if (ref[q].virt && f.field == GC_FIELD_W_SUM) {
             if (n) CU(cudaMemcpyAsync(f.host, ref[q].virt->wsum + base, f.bytes, cudaMemcpyDeviceToHost, ctx->stream));
             continue;
         }
@@ -3137,6 +3365,7 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
         if (!ctx->d_pairs) TRY(dalloc(ctx, &ctx->d_pairs, 1));
         int64_t pairs = 0;
         for (auto& D : ctx->inters) {
+            if (D.probe) continue;
             bool active = false;
             for (int p : D.pk) active |= p != GC_PFN_NONE;
             if (!active) continue;

@@ -138,7 +138,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
 #pragma unroll
             for (int q2 = 0; q2 < NS; ++q2) acc.sr[q2] = acc.sr[q2] + kw * r.bstress[q2 * Nb + j];
         }
-        if (A.iwsum) acc.w[0] = acc.w[0] + kw;
+        if (A.iwsum) acc.w[0] = acc.w[0] + (A.iwsum == 2 ? 1.0 : kw);  // 2: NeighborCountFn's count
         return 1;
     }
     if (PFN == GC_PFN_XSPH) {

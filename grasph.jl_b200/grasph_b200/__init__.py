@@ -13,7 +13,8 @@ from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, 
                     LinearEOSUpdater, StaticBoundarySystem, StrainRatePfn, StrainRateVorticityPfn,
                     StressParticleSystem, SystemInteraction, TaitEOSUpdater, ViscoPlasticMCStressUpdater,
                     WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater, is_coupled, VirtualParticleSystem,
-                    InterpolateFieldFn, VirtualNormUpdater, PrescribedVelocityUpdater)
+                    InterpolateFieldFn, VirtualNormUpdater, PrescribedVelocityUpdater, ProbeParticleSystem,
+                    NeighborCountFn)
 from .engine import (CudaBackend, GcError, Server, Session, compile_instance, download_instance, load_library,
                      time_integrate, upload_instance)
 

@@ -21,7 +21,8 @@ import numpy as np
 from . import consts as C
 from .model import (AbstractBoundarySystem, AbstractParticleSystem, ArgumentError,
                     GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator,
-                    SystemInteraction, VirtualParticleSystem, updater_chains, _pfn_kind, _pfn_params)
+                    SystemInteraction, VirtualParticleSystem, ProbeParticleSystem, updater_chains, _pfn_kind,
+                    _pfn_params)
 
 PKG_DIR = Path(__file__).resolve().parents[1]
 LIB_PATH = PKG_DIR / "libgrasph_cuda.so"
@@ -84,6 +85,11 @@ def load_library(path: os.PathLike | None = None):
         "gc_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
         "gc_set_velocity_adjust": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_double]),
         "gc_add_virtual": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _dp, _ip]),
+        "gc_add_probe": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int64, ct.c_int, _dp, ct.c_int, ct.c_int, ct.c_int,
+                                    _dp, _ip]),
+        "gc_add_probe_interaction": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_double,
+                                                ct.c_int, _dp, _ip]),
+        "gc_measure_probes": (ct.c_int, [ct.c_void_p]),
         "gc_finalize": (ct.c_int, [ct.c_void_p]),
         "gc_upload_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         "gc_download_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
@@ -207,6 +213,24 @@ class CudaBackend:
         out = ct.c_int()
         self._chk(self.lib.gc_add_virtual(self.ctx, inst, src, zero_mask, pvp, ct.byref(out)), "gc_add_virtual")
         return out.value
+
+    def add_probe(self, inst, n, nd, positions, mirror, extras_mask, ns, prescribed_v):
+        pos, posp = (None, None) if positions is None else _arr(positions, np.float64, _dp)
+        pv, pvp = _arr(prescribed_v, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_probe(self.ctx, inst, n, nd, posp, mirror, extras_mask, ns, pvp, ct.byref(out)),
+                  "gc_add_probe")
+        return out.value
+
+    def add_probe_interaction(self, inst, a, probe, kernel_kind, h, pfn_kind, pfn_params):
+        p, pp = _arr(pfn_params, np.float64, _dp)
+        out = ct.c_int()
+        self._chk(self.lib.gc_add_probe_interaction(self.ctx, inst, a, probe, kernel_kind, h, pfn_kind, pp,
+                                                    ct.byref(out)), "gc_add_probe_interaction")
+        return out.value
+
+    def measure_probes(self):
+        self._chk(self.lib.gc_measure_probes(self.ctx), "gc_measure_probes")
 
     def set_updaters(self, inst, sys, chains):
         cl = np.array([len(c) for c in chains] or [0], dtype=np.int32)
@@ -333,13 +357,14 @@ class InstanceMap:
         self.systems = []
         self.ghosts = []
         self.virtuals = []
+        self.probes = []
 
     def h(self, obj):
         return self.handles[id(obj)]
 
 
 def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
-                     kind=C.GC_INTEGRATOR_LEAPFROG, virtuals=()) -> InstanceMap:
+                     kind=C.GC_INTEGRATOR_LEAPFROG, virtuals=(), probes=(), probe_interactions=()) -> InstanceMap:
     """Issue the model-building calls for one simulation (one instance)."""
     m = InstanceMap(inst)
     sys_ids = {id(ps) for ps in systems}
@@ -412,6 +437,26 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
         m.inters[id(it)] = backend.add_interaction(inst, m.h(a), bh, it.kernel.kind, it.kernel.h, kinds, params)
         if getattr(it, "vadjust_pfn", None) is not None:
             backend.set_velocity_adjust(inst, m.inters[id(it)], it.vadjust_pfn.kind, it.vadjust_pfn.epsilon)
+    for pr in probes:
+        mh = -1
+        if pr.mirror_target is not None:
+            if id(pr.mirror_target) not in m.handles:
+                raise ArgumentError("a probe's mirror target must be one of the systems")
+            mh = m.h(pr.mirror_target)
+        m.handles[id(pr)] = backend.add_probe(inst, pr.n, pr.ndims, pr.x, mh, pr.extras_mask, pr.ns,
+                                              pr.prescribed_v)
+        m.probes.append(pr)
+        chains = updater_chains(pr)
+        if chains:
+            backend.set_updaters(inst, m.h(pr), chains)
+    for it in probe_interactions:
+        if id(it.system_a) not in sys_ids:
+            raise ArgumentError("system_a must be in the integrator's systems")
+        pf = it.pfns[0]
+        if len(it.pfns) != 1 or pf is None:
+            raise ArgumentError("a probe interaction takes one functor")
+        m.inters[id(it)] = backend.add_probe_interaction(inst, m.h(it.system_a), m.h(it.system_b), it.kernel.kind,
+                                                         it.kernel.h, _pfn_kind(pf), _pfn_params(pf))
     for ps in systems:
         chains = updater_chains(ps)
         if chains:
@@ -447,6 +492,24 @@ def download_instance(backend, m: InstanceMap, with_ghosts=True, systems=None):
             download_ghost(backend, m, ge)
         for vps in m.virtuals:
             backend.download_into(m.inst, m.h(vps), C.GC_FIELD_W_SUM, vps.w_sum)
+        for pr in m.probes:
+            download_probe(backend, m, pr)
+
+
+def download_probe(backend, m: InstanceMap, pr):
+    h = m.h(pr)
+    backend.download_into(m.inst, h, C.GC_FIELD_X, pr.x)
+    backend.download_into(m.inst, h, C.GC_FIELD_ID, pr.id)
+    backend.download_into(m.inst, h, C.GC_FIELD_W_SUM, pr.w_sum)
+    for k, arr in pr.extras.items():
+        if k == pr.count_field:
+            buf = np.zeros(pr.n)
+            backend.download_into(m.inst, h, C.GC_FIELD_COUNT, buf)
+            arr[:] = np.rint(buf).astype(np.int64)
+        else:
+            buf = np.zeros(arr.shape)
+            backend.download_into(m.inst, h, ProbeParticleSystem._fields[k], buf)
+            arr[:] = buf
 
 
 def download_ghost(backend, m: InstanceMap, ge: GhostEntry):
@@ -489,7 +552,8 @@ class Session:
         for lf in self.integrators:
             inst = self.backend.instance_add()
             self.maps.append(compile_instance(self.backend, inst, lf.systems, lf.interactions, lf.ghosts,
-                                              lf.gamma, lf.kind, getattr(lf, "virtual_systems", ())))
+                                              lf.gamma, lf.kind, getattr(lf, "virtual_systems", ()),
+                                              getattr(lf, "probes", ()), getattr(lf, "probe_interactions", ())))
         self.backend.finalize()
         self.backend.set_precision(precision)
         self.precision = precision
@@ -507,6 +571,15 @@ class Session:
 
     def step(self, nsteps, cfl):
         self.backend.step(nsteps, cfl)
+
+    def measure_probes(self, pull=True):
+        """_measure_probes! (src/TimeIntegration.jl:454-502), then the probes'
+        x, id, w_sum and extras downloaded in probe order."""
+        self.backend.measure_probes()
+        if pull:
+            for m in self.maps:
+                for pr in m.probes:
+                    download_probe(self.backend, m, pr)
 
     def stats(self):
         return self.backend.stats()
@@ -671,7 +744,8 @@ class Server:
         be = CudaBackend(self.device, 0, lib=self.lib)
         inst = be.instance_add()
         m = compile_instance(be, inst, lf.systems, lf.interactions, lf.ghosts, lf.gamma, lf.kind,
-                             getattr(lf, "virtual_systems", ()))
+                             getattr(lf, "virtual_systems", ()), getattr(lf, "probes", ()),
+                             getattr(lf, "probe_interactions", ()))
         for ps in m.systems:
             h = m.h(ps)
             for name, fid in ps.particle_fields():

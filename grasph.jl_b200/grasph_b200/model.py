@@ -455,6 +455,15 @@ class InterpolateFieldFn(_Pfn):
         return p
 
 
+class NeighborCountFn(_Pfn):
+    """probe.field[j] += 1 per neighbour, src/PairwiseFunctors.jl:442-460."""
+
+    kind = C.GC_PFN_NEIGHBOR_COUNT
+
+    def __init__(self, field):
+        self.field = str(field).lstrip(":")
+
+
 class XSPHPfn(_Pfn):
     """XSPH velocity smoothing, src/PairwiseFunctors.jl:357-389; only as a
     `velocity_adjust_pairwise_fn` (swept by adjust_v! in the step's XSPH
@@ -715,12 +724,82 @@ class VirtualParticleSystem:
         return sum(1 << ids[f] for f in self.zero_fields)
 
 
+class ProbeParticleSystem:
+    """Passive observers measured only at save cadence,
+    src/ProbeParticles.jl:23-102.
+
+    `ProbeParticleSystem(name, positions, ...)` or
+    `ProbeParticleSystem(name, mirror_target, ...)` (positions taken from
+    that system at each measurement).  `extras` maps names to per-probe
+    arrays: v, rho, p, stress take InterpolateFieldFn sums, one integer
+    array takes a NeighborCountFn count."""
+
+    _fields = {"v": C.GC_FIELD_V, "rho": C.GC_FIELD_RHO, "p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS}
+
+    def __init__(self, name, positions_or_target, *, extras=None, state_updater=(), prescribed_v=None,
+                 dtype=np.float64):
+        if np.dtype(dtype) != np.float64:
+            raise ArgumentError("only Float64 probes are supported by the device library")
+        self.name = str(name)
+        if isinstance(positions_or_target, AbstractParticleSystem):
+            self.mirror_target = positions_or_target
+            self.x = np.array(positions_or_target.x, dtype=np.float64)
+        else:
+            self.mirror_target = None
+            self.x = np.array(positions_or_target, dtype=np.float64)
+            if self.x.size == 0:
+                raise ArgumentError("positions must not be empty")
+        if self.x.ndim != 2:
+            raise ArgumentError("positions must be n×ndims")
+        self.n, self.ndims = self.x.shape
+        self.id = np.arange(1, self.n + 1, dtype=np.int64)
+        self.w_sum = np.zeros(self.n)
+        self.extras = {}
+        self.count_field = None
+        for k, arr in (extras or {}).items():
+            a = np.array(arr)
+            if a.shape[0] != self.n:
+                raise ArgumentError(f"extras.{k} has length {a.shape[0]} but n={self.n}")
+            if k not in self._fields:
+                if not np.issubdtype(a.dtype, np.integer) or self.count_field is not None:
+                    raise ArgumentError(f"extras.{k}: only v, rho, p, stress and one integer count are supported")
+                self.count_field = k
+            self.extras[k] = a.astype(np.int64 if k == self.count_field else np.float64)
+        ups = state_updater if isinstance(state_updater, tuple) else (state_updater,)
+        self.state_updater = ups
+        pv = np.zeros(self.ndims) if prescribed_v is None else np.asarray(prescribed_v, dtype=np.float64).ravel()
+        if pv.shape != (self.ndims,):
+            raise ArgumentError("prescribed_v must have ndims components")
+        self.prescribed_v = pv
+
+    def __getattr__(self, name):
+        extras = self.__dict__.get("extras", {})
+        if name in extras:
+            return extras[name]
+        mt = self.__dict__.get("mirror_target")
+        if mt is not None:
+            return getattr(mt, name)
+        raise AttributeError(f"ProbeParticleSystem has no field {name}")
+
+    @property
+    def extras_mask(self):
+        m = sum(1 << self._fields[k] for k in self.extras if k in self._fields)
+        if self.count_field is not None:
+            m |= 1 << C.GC_FIELD_COUNT
+        return m
+
+    @property
+    def ns(self):
+        return self.extras["stress"].shape[1] if "stress" in self.extras else 0
+
+
 class LeapFrogTimeIntegrator:
     """src/TimeIntegration.jl:29-67."""
 
     kind = C.GC_INTEGRATOR_LEAPFROG
 
-    def __init__(self, systems, interactions, *, ghosts=(), gamma=0.0, virtual_systems=(), **kw):
+    def __init__(self, systems, interactions, *, ghosts=(), gamma=0.0, virtual_systems=(), probes=(),
+                 probe_interactions=(), **kw):
         if "Γ" in kw:
             gamma = kw.pop("Γ")
         if kw:
@@ -740,6 +819,15 @@ class LeapFrogTimeIntegrator:
             if not isinstance(v, VirtualParticleSystem):
                 raise ArgumentError("virtual_systems must be VirtualParticleSystems")
         self.virtual_systems = vs
+        self.probes = (probes,) if isinstance(probes, ProbeParticleSystem) else tuple(probes)
+        self.probe_interactions = ((probe_interactions,) if isinstance(probe_interactions, SystemInteraction)
+                                   else tuple(probe_interactions))
+        for p in self.probes:
+            if not isinstance(p, ProbeParticleSystem):
+                raise ArgumentError("probes must be ProbeParticleSystems")
+        for si in self.probe_interactions:
+            if not any(si.system_b is p for p in self.probes):
+                raise ArgumentError("a probe interaction's system_b must be one of `probes`")
         self.c = max(ps.c for ps in sys_)
         self.h = min(it.kernel.h for it in ints)
         self.gamma = float(gamma)

@@ -44,6 +44,7 @@ pfn_kind(::StrainRatePfn) = 3
 pfn_kind(::StrainRateVorticityPfn) = 4
 pfn_kind(::FluidSolidPfn) = 7
 pfn_kind(::InterpolateFieldFn) = 8
+pfn_kind(::NeighborCountFn) = 9
 pfn_kind(f) = throw(ArgumentError("pairwise functor $(typeof(f)) has no device implementation"))
 
 function pfn_params(f)
@@ -176,6 +177,37 @@ function CudaLeapFrog(lf::Union{LeapFrogTimeIntegrator,RK4TimeIntegrator}; devic
                            normals, points, ge.cutoff, 0, out))
         h[g] = out[]
     end
+    # probes (measured by measure_probes!) after the systems and virtual systems
+    for pr in lf.probes
+        ex = getfield(pr, :extras)
+        mask = Cint(0); ns = Cint(0)
+        for k in keys(ex)
+            if haskey(GC_FIELD, k) && k in (:v, :rho, :p, :stress)
+                mask |= Cint(1) << GC_FIELD[k]
+                k === :stress && (ns = Cint(length(eltype(ex[k]))))
+            else
+                mask |= Cint(1) << 17  # GC_FIELD_COUNT: a NeighborCountFn array
+            end
+        end
+        mt = getfield(pr, :mirror_target)
+        pos = reduce(vcat, [Vector(p) for p in getfield(pr, :x)])
+        out = Ref{Cint}(0)
+        check(ctx[], ccall((:gc_add_probe, LIB), Cint,
+                           (Ptr{Cvoid}, Cint, Int64, Cint, Ptr{Cdouble}, Cint, Cint, Cint, Ptr{Cdouble}, Ref{Cint}),
+                           ctx[], inst[], pr.n, pr.ndims, pos, mt === nothing ? Cint(-1) : h[mt], mask, ns,
+                           Vector{Float64}(getfield(pr, :prescribed_v)), out))
+        h[pr] = out[]
+        set_updaters!(ctx[], inst[], h[pr], getfield(pr, :state_updater))
+    end
+    for pi in lf.probe_interactions
+        f = first(pi.pfns)
+        out = Ref{Cint}(0)
+        kk = pi.kernel isa CubicSplineKernel ? 0 : 1
+        check(ctx[], ccall((:gc_add_probe_interaction, LIB), Cint,
+                           (Ptr{Cvoid}, Cint, Cint, Cint, Cint, Cdouble, Cint, Ptr{Cdouble}, Ref{Cint}),
+                           ctx[], inst[], h[pi.system_a], h[pi.system_b], kk, pi.kernel.h, pfn_kind(f),
+                           pfn_params(f), out))
+    end
     ints = Cint[]
     for si in lf.interactions
         b = si.system_b
@@ -253,6 +285,34 @@ function field_io!(cl::CudaLeapFrog, ps, f::Symbol, upload::Bool)
     end
 end
 
+"""
+    measure_probes!(cl::CudaLeapFrog)
+
+The save-time probe measurement (`_measure_probes!`) on the device, then each
+probe's x, id, w_sum and extras copied back in id order.
+"""
+function measure_probes!(cl::CudaLeapFrog)
+    check(cl.ctx, ccall((:gc_measure_probes, LIB), Cint, (Ptr{Cvoid},), cl.ctx))
+    for pr in cl.lf.probes
+        h = cl.handles[pr]
+        io(arr, fid) = GC.@preserve arr check(cl.ctx, ccall((:gc_download_field, LIB), Cint,
+                                              (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cvoid}, Csize_t),
+                                              cl.ctx, 0, h, fid, pointer(arr), sizeof(arr)))
+        io(getfield(pr, :x), GC_FIELD.x)
+        io(getfield(pr, :id), GC_FIELD.id)
+        io(getfield(pr, :w_sum), 16)
+        for (k, arr) in pairs(getfield(pr, :extras))
+            if k in (:v, :rho, :p, :stress)
+                io(arr, GC_FIELD[k])
+            else
+                buf = zeros(Float64, length(arr)); io(buf, 17)
+                arr .= round.(eltype(arr), buf)
+            end
+        end
+    end
+    return nothing
+end
+
 function upload!(cl::CudaLeapFrog)
     for ps in cl.lf.systems, f in fields_of(ps)
         field_io!(cl, ps, f, true)
@@ -291,6 +351,10 @@ function Grasph.time_integrate!(cl::CudaLeapFrog, num_timesteps::Int, print_inte
         if g % print_interval_step == 0
             download!(cl)
             foreach(print_summary, cl.lf.systems)
+        end
+        # probes are measured at save cadence, as _maybe_save! does
+        if output_prefix !== nothing && !isempty(cl.lf.probes) && g % save_interval_step == 0
+            measure_probes!(cl)
         end
     end
     download!(cl)

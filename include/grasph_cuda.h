@@ -71,8 +71,9 @@ enum {
     GC_FIELD_IDX_ORIGINAL = 13,/* ghosts: int64 source index, 1-based         */
     GC_FIELD_IDX_BOUNDARY = 14,/* ghosts: int64 plane index, 1-based          */
     GC_FIELD_NORMALS = 15,     /* ghosts: ND doubles                          */
-    GC_FIELD_W_SUM = 16,       /* virtual systems: 1 double, kernel-weight sum */
-    GC_NFIELDS = 17
+    GC_FIELD_W_SUM = 16,       /* virtual systems, probes: 1 double, kernel-weight sum */
+    GC_FIELD_COUNT = 17,       /* probes: 1 double, the NeighborCountFn extra   */
+    GC_NFIELDS = 18
 };
 
 /* ------------------------------------------------------ boundary wrappers */
@@ -96,9 +97,11 @@ enum {
     GC_PFN_COUNT = 5,
     GC_PFN_XSPH = 6,                    /* XSPHPfn :360-389; velocity-adjust functor only */
     GC_PFN_FLUID_SOLID = 7,             /* FluidSolidPfn :479-519 (system_b a real system) */
-    GC_PFN_INTERPOLATE = 8              /* InterpolateFieldFn :392-428, system_b a virtual
-                                           system: [0] bitmask of 1<<GC_FIELD_* out of v, rho,
-                                           stress  [1] accumulate_wsum (0 or 1)  */
+    GC_PFN_INTERPOLATE = 8,             /* InterpolateFieldFn :392-440, system_b a virtual
+                                           system or a probe: [0] bitmask of 1<<GC_FIELD_* out
+                                           of v, rho, stress  [1] accumulate_wsum (0 or 1)  */
+    GC_PFN_NEIGHBOR_COUNT = 9           /* NeighborCountFn :442-460, system_b a probe:
+                                           its GC_FIELD_COUNT extra += 1 per neighbour  */
 };
 /* Per-stage functor parameters, GC_PFN_NPARAM doubles each:
  *   [0] art_visc_alpha  [1] art_visc_beta  [2] h
@@ -224,6 +227,31 @@ int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double ep
  * serves as system_b and takes gc_set_updaters.                           */
 int gc_add_virtual(gc_ctx* ctx, int inst, int src_sys, int zero_mask, const double* prescribed_v,
                    int* handle_out);
+
+/* ProbeParticleSystem(name, positions | mirror_target; extras, state_updater,
+ * prescribed_v) src/ProbeParticles.jl:23-102: n passive observers, measured
+ * only by gc_measure_probes.  positions: n×ndims doubles, or NULL with
+ * mirror_sys a system handle of n particles whose positions the probes take
+ * at each measurement (-1: none).  extras_mask: bitmask of 1<<GC_FIELD_* out
+ * of v, rho, p, stress (ns components) and count.  prescribed_v: ndims
+ * doubles or NULL; probes move by prescribed_v·dt after each step.  The
+ * handle takes gc_set_updaters (one stage) and gc_download_field (x, id,
+ * w_sum and the extras, in probe order after a measurement).              */
+int gc_add_probe(gc_ctx* ctx, int inst, int64_t n, int ndims, const double* positions, int mirror_sys,
+                 int extras_mask, int ns, const double* prescribed_v, int* handle_out);
+
+/* One of the integrator's probe_interactions: SystemInteraction(kernel,
+ * pfn, system_a, probe) with pfn GC_PFN_INTERPOLATE or
+ * GC_PFN_NEIGHBOR_COUNT (GC_PFN_NPARAM params), swept only by
+ * gc_measure_probes.                                                       */
+int gc_add_probe_interaction(gc_ctx* ctx, int inst, int sys_a, int probe, int kernel_kind, double h,
+                             int pfn_kind, const double* pfn_params, int* inter_out);
+
+/* _measure_probes! src/TimeIntegration.jl:454-502, for every instance: the
+ * probe interactions' system_a re-sorted, mirrored probe positions taken,
+ * probes sorted by cell, grids built, w_sum and extras zeroed, one sweep,
+ * the probes' updaters, probes sorted back by id.                          */
+int gc_measure_probes(gc_ctx* ctx);
 
 /* The `state_updater` tuple of a system (src/Particles.jl:200): nstages
  * entries, each a chain of `chain_len[s]` updaters (kinds / GC_UPD_NPARAM

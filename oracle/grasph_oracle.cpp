@@ -132,6 +132,7 @@ struct Sys {
     std::vector<double> q0v, q0rho;
     std::vector<double> accv, accrho;  // RK4 accumulators
     bool vsrc = false;  // the source of a virtual system: not one of the integrator's systems
+    bool probe = false; // a probe's own arrays (count extra in drhodt)
     bool has_p() const { return kind >= GC_SYS_FLUID; }
     bool has_stress() const { return kind >= GC_SYS_STRESS; }
     bool is_ep() const { return kind == GC_SYS_ELASTOPLASTIC; }
@@ -164,6 +165,8 @@ struct Virt {
     std::vector<double> wsum;
     bool upd_set = false;
     std::vector<std::vector<Upd>> upd;
+    bool probe = false;  // ProbeParticleSystem src/ProbeParticles.jl:23-102 (source = its own arrays)
+    int mirror = -1;     // its mirror_target system, or -1
 };
 struct Handle {
     int type = H_SYS;
@@ -186,6 +189,7 @@ struct Inter {
     std::vector<int64_t> cs, csa;
     double mina[3] = {0, 0, 0}, maxa[3] = {0, 0, 0};
     bool grid = false;
+    bool probe = false;  // one of the integrator's probe_interactions (swept at measurement only)
     int vk = GC_PFN_NONE;  // velocity_adjust_pairwise_fn (XSPHPfn or nothing)
     double veps = 0.0;     // its epsilon
 };
@@ -502,6 +506,10 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
                  const double* gx, double w, int* err) {
     const int ns = a.ns;
     const double* vi = &a.v[i * ND];
+    if (f.kind == GC_PFN_NEIGHBOR_COUNT) {  // NeighborCountFn :455-460 (count extra)
+        b.sys->drhodt[j] += 1.0;
+        return;
+    }
     if (f.kind == GC_PFN_INTERPOLATE) {
         // InterpolateFieldFn(ps_a, ps_b::VirtualParticleSystem) :424-428:
         // f_b[j] += kw·f_a[i] with kw = w·(m_a/ρ_a[i]); w_sum[j] += kw
@@ -1007,6 +1015,27 @@ int sort_order(const double* x, int64_t n, int nd, double cutoff, std::vector<in
     return 1;
 }
 
+void permute_system(Sys& s, const std::vector<int64_t>& perm) {
+    const int nd = s.nd, ns = s.ns;
+    apply_perm(s.x, perm, nd);
+    apply_perm(s.id, perm, 1);
+    apply_perm(s.v, perm, nd);
+    apply_perm(s.vadj, perm, nd);
+    apply_perm(s.rho, perm, 1);
+    apply_perm(s.dvdt, perm, nd);
+    apply_perm(s.drhodt, perm, 1);
+    if (s.has_p()) apply_perm(s.p, perm, 1);
+    if (s.has_stress()) {
+        apply_perm(s.stress, perm, ns);
+        apply_perm(s.sr, perm, ns);
+    }
+    if (s.is_ep()) {
+        apply_perm(s.vort, perm, s.nvort);
+        apply_perm(s.strain, perm, ns);
+        apply_perm(s.strainp, perm, ns);
+    }
+}
+
 int sort_system(Sys& s, double cutoff, std::vector<int64_t>* perm_out) {
     std::vector<int64_t> perm;
     int r = sort_order(s.x.data(), s.n, s.nd, cutoff, perm);
@@ -1387,7 +1416,12 @@ int make_view(oracle_ctx* ctx, int handle, BView* out) {
 int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     const Sys& a = ctx->sys[it.a];
     if (pk == GC_PFN_NONE) return GC_OK;
-    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_INTERPOLATE) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_NEIGHBOR_COUNT) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (pk == GC_PFN_NEIGHBOR_COUNT) {  // the (real, probe) method :455
+        if (it.b < 0 || ctx->handles[it.b].type != H_VIRT || !ctx->virts[ctx->handles[it.b].idx].probe)
+            return GC_ERR_UNSUPPORTED;
+        return GC_OK;
+    }
     if (pk == GC_PFN_INTERPOLATE) {
         // the (real, virtual) method :424; the fields exist on both sides
         if (it.b < 0 || ctx->handles[it.b].type != H_VIRT) return GC_ERR_UNSUPPORTED;
@@ -1502,7 +1536,11 @@ int xsph_correction(oracle_ctx* ctx) {
 
 // ------------------------------------------------------------- integrator
 // src/TimeIntegration.jl:580-697 (LeapFrog)
-int num_stages(oracle_ctx* ctx) { return ctx->inters.empty() ? 0 : ctx->inters[0].nstages; }
+int num_stages(oracle_ctx* ctx) {
+    for (auto& it : ctx->inters)
+        if (!it.probe) return it.nstages;
+    return 0;
+}
 
 // Virtual systems (src/Particles.jl:476-528, src/TimeIntegration.jl:364-419)
 void zero_field(Sys& s, int field) {
@@ -1556,15 +1594,17 @@ void apply_virtual_updater(Sys& s, Virt& vp, const Upd& u, double dt) {
 // systems' updaters, the ghosts' copiers, the virtuals' updaters and every
 // interaction's sweep
 int sweep_all_stages(oracle_ctx* ctx, int nst, double dt) {
-    for (auto& vp : ctx->virts) auto_zero_virtual(ctx, vp);
+    for (auto& vp : ctx->virts)
+        if (!vp.probe) auto_zero_virtual(ctx, vp);
     for (int stage = 1; stage <= nst; ++stage) {
         for (auto& s : ctx->sys)
             if (!s.vsrc && s.upd_set && (int)s.upd.size() == nst) update_state(s, stage, dt);
         for (auto& g : ctx->ghosts) update_ghost(ctx, g, stage);
         for (auto& vp : ctx->virts)
-            if (vp.upd_set && (int)vp.upd.size() == nst)
+            if (!vp.probe && vp.upd_set && (int)vp.upd.size() == nst)
                 for (const Upd& u : vp.upd[stage - 1]) apply_virtual_updater(ctx->sys[vp.src], vp, u, dt);
         for (auto& it : ctx->inters) {
+            if (it.probe) continue;
             int st = sweep(ctx, it, stage);
             if (st) return st;
         }
@@ -1581,12 +1621,73 @@ int prepare_grids(oracle_ctx* ctx, double sort_cutoff) {
         if (st) return fail(ctx, st, "ghost sort: non-finite position");
     }
     for (auto& vp : ctx->virts) {
+        if (vp.probe) continue;  // probes are sorted at measurement
         int st = sort_system(ctx->sys[vp.src], sort_cutoff, nullptr);
         if (st) return fail(ctx, st, "virtual sort: non-finite position");
     }
     for (auto& it : ctx->inters) {
+        if (it.probe) continue;
         int st = create_grid(ctx, it);
         if (st) return st;
+    }
+    return GC_OK;
+}
+
+// _measure_probes! src/TimeIntegration.jl:454-502
+int measure_probes(oracle_ctx* ctx) {
+    double hmin = 1e300;
+    for (auto& it : ctx->inters)
+        if (!it.probe) hmin = std::min(hmin, it.H);
+    const double cutoff = 2.0 * hmin;
+    // the probe interactions' system_a, re-sorted (positions moved since the step's sort)
+    std::vector<char> done(ctx->sys.size(), 0);
+    for (auto& it : ctx->inters) {
+        if (!it.probe || done[it.a]) continue;
+        done[it.a] = 1;
+        int st = sort_system(ctx->sys[it.a], cutoff, nullptr);
+        if (st) return fail(ctx, st, "sort: non-finite position");
+    }
+    // mirrored positions: x[id_src[i]] = x_src[i] (probe ids are 1..n here)
+    for (auto& vp : ctx->virts) {
+        if (!vp.probe || vp.mirror < 0) continue;
+        Sys& p = ctx->sys[vp.src];
+        const Sys& m = ctx->sys[vp.mirror];
+        for (int64_t i = 0; i < m.n; ++i)
+            for (int d = 0; d < p.nd; ++d) p.x[(size_t)((m.id[i] - 1) * p.nd + d)] = m.x[(size_t)(i * m.nd + d)];
+    }
+    for (auto& vp : ctx->virts) {
+        if (!vp.probe) continue;
+        int st = sort_system(ctx->sys[vp.src], cutoff, nullptr);
+        if (st) return fail(ctx, st, "probe sort: non-finite position");
+    }
+    for (auto& it : ctx->inters) {
+        if (!it.probe) continue;
+        int st = create_grid(ctx, it);
+        if (st) return st;
+    }
+    // auto_zero_probe! src/ProbeParticles.jl:117-124: w_sum and every extra
+    for (auto& vp : ctx->virts) {
+        if (!vp.probe) continue;
+        Sys& p = ctx->sys[vp.src];
+        std::fill(vp.wsum.begin(), vp.wsum.end(), 0.0);
+        for (int f : {GC_FIELD_V, GC_FIELD_RHO, GC_FIELD_P, GC_FIELD_STRESS, GC_FIELD_DRHODT}) zero_field(p, f);
+    }
+    for (auto& it : ctx->inters) {
+        if (!it.probe) continue;
+        int st = sweep(ctx, it, 1);
+        if (st) return st;
+    }
+    for (auto& vp : ctx->virts)  // update_state!(probe): stage 1, dt = 0
+        if (vp.probe && !vp.upd.empty())
+            for (const Upd& u : vp.upd[0]) apply_virtual_updater(ctx->sys[vp.src], vp, u, 0.0);
+    // _sort_probe_by_id! :129-143
+    for (auto& vp : ctx->virts) {
+        if (!vp.probe) continue;
+        Sys& p = ctx->sys[vp.src];
+        std::vector<int64_t> perm((size_t)p.n);
+        for (int64_t i = 0; i < p.n; ++i) perm[(size_t)(p.id[i] - 1)] = i;
+        permute_system(p, perm);
+        apply_perm(vp.wsum, perm, 1);
     }
     return GC_OK;
 }
@@ -1758,7 +1859,8 @@ double compute_dt(oracle_ctx* ctx, double cfl) {
     double c = -1e300, h = 1e300;
     for (auto& s : ctx->sys)
         if (!s.vsrc) c = std::max(c, s.c);  // the integrator's systems (:108)
-    for (auto& it : ctx->inters) h = std::min(h, it.H);
+    for (auto& it : ctx->inters)
+        if (!it.probe) h = std::min(h, it.H);
     return cfl * h / c;
 }
 
@@ -1962,6 +2064,89 @@ int oracle_add_interaction(oracle_ctx* ctx, int sys_a, int b_handle, int kernel_
     return GC_OK;
 }
 
+int oracle_add_probe(oracle_ctx* ctx, int64_t n, int nd, const double* positions, int mirror_sys, int extras_mask,
+                     int ns, const double* prescribed_v, int* handle_out) {
+    if (n <= 0) return fail(ctx, GC_ERR_ARG, "positions must not be empty");
+    if (nd < 2 || nd > 3) return fail(ctx, GC_ERR_UNSUPPORTED, "ndims must be 2 or 3");
+    int mi = -1;
+    if (mirror_sys >= 0) {
+        mi = sys_index(ctx, mirror_sys);
+        if (mi < 0 || ctx->sys[mi].n != n || ctx->sys[mi].nd != nd)
+            return fail(ctx, GC_ERR_ARG, "mirror target must be a system of n particles");
+    } else if (!positions) {
+        return fail(ctx, GC_ERR_ARG, "probe positions or a mirror target are required");
+    }
+    const bool st = extras_mask & (1 << GC_FIELD_STRESS);
+    if (st && !(ns == 3 || ns == 4 || ns == 6)) return fail(ctx, GC_ERR_ARG, "ns must be 3, 4, or 6");
+    Sys s;
+    s.kind = st ? GC_SYS_STRESS : (extras_mask & (1 << GC_FIELD_P)) ? GC_SYS_FLUID : GC_SYS_BASIC;
+    s.n = n;
+    s.nd = nd;
+    s.ns = st ? ns : 0;
+    s.x.assign((size_t)n * nd, 0.0);
+    if (positions) std::memcpy(s.x.data(), positions, sizeof(double) * n * nd);
+    else s.x = ctx->sys[mi].x;
+    s.v.assign((size_t)n * nd, 0.0);
+    s.vadj.assign((size_t)n * nd, 0.0);
+    s.rho.assign((size_t)n, 0.0);
+    s.dvdt.assign((size_t)n * nd, 0.0);
+    s.drhodt.assign((size_t)n, 0.0);
+    s.id.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) s.id[i] = i + 1;
+    if (s.has_p()) s.p.assign((size_t)n, 0.0);
+    if (s.has_stress()) {
+        s.stress.assign((size_t)n * s.ns, 0.0);
+        s.sr.assign((size_t)n * s.ns, 0.0);
+    }
+    s.vsrc = true;
+    s.probe = true;
+    ctx->sys.push_back(std::move(s));
+    Virt vp;
+    vp.src = (int)ctx->sys.size() - 1;
+    vp.probe = true;
+    vp.mirror = mi;
+    if (prescribed_v)
+        for (int d = 0; d < nd; ++d) vp.pv[d] = prescribed_v[d];
+    vp.wsum.assign((size_t)n, 0.0);
+    ctx->virts.push_back(vp);
+    Handle h;
+    h.type = H_VIRT;
+    h.idx = (int)ctx->virts.size() - 1;
+    ctx->handles.push_back(h);
+    *handle_out = (int)ctx->handles.size() - 1;
+    return GC_OK;
+}
+
+int oracle_add_probe_interaction(oracle_ctx* ctx, int sys_a, int probe, int kernel_kind, double h, int pfn_kind,
+                                 const double* pfn_params, int* inter_out) {
+    int si = sys_index(ctx, sys_a);
+    if (si < 0) return fail(ctx, GC_ERR_ARG, "system_a must be a system");
+    if (probe < 0 || probe >= (int)ctx->handles.size() || ctx->handles[probe].type != H_VIRT ||
+        !ctx->virts[ctx->handles[probe].idx].probe)
+        return fail(ctx, GC_ERR_ARG, "system_b must be a probe");
+    if (pfn_kind != GC_PFN_INTERPOLATE && pfn_kind != GC_PFN_NEIGHBOR_COUNT)
+        return fail(ctx, GC_ERR_UNSUPPORTED, "probe interactions take InterpolateFieldFn or NeighborCountFn");
+    Inter it;
+    it.a = si;
+    it.b = probe;
+    it.kk = kernel_kind;
+    it.H = h;
+    it.nstages = 1;
+    it.cell = 2.0 * h;
+    it.probe = true;
+    it.pk.push_back(pfn_kind);
+    std::array<double, GC_PFN_NPARAM> a;
+    for (int k = 0; k < GC_PFN_NPARAM; ++k) a[k] = pfn_params[k];
+    it.pp.push_back(a);
+    int st = check_combo(ctx, it, pfn_kind);
+    if (st) return fail(ctx, st, "unsupported probe functor / system combination");
+    ctx->inters.push_back(std::move(it));
+    *inter_out = (int)ctx->inters.size() - 1;
+    return GC_OK;
+}
+
+int oracle_measure_probes(oracle_ctx* ctx) { return measure_probes(ctx); }
+
 int oracle_add_virtual(oracle_ctx* ctx, int src_sys, int zero_mask, const double* prescribed_v, int* handle_out) {
     int si = sys_index(ctx, src_sys);
     if (si < 0) return fail(ctx, GC_ERR_ARG, "a virtual system needs a source system");
@@ -2053,7 +2238,9 @@ int oracle_set_field(oracle_ctx* ctx, int handle, int field, const void* host, s
     if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
     const Handle& h = ctx->handles[handle];
     if (h.type == H_GHOST) return fail(ctx, GC_ERR_ARG, "ghost fields are generated, not set");
-    Sys& s = ctx->sys[h.idx];
+    if (h.type == H_VIRT && !ctx->virts[h.idx].probe)
+        return fail(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
+    Sys& s = ctx->sys[h.type == H_VIRT ? ctx->virts[h.idx].src : h.idx];
     int comps = field_comps(s, field);
     if (comps < 0) return fail(ctx, GC_ERR_ARG, "field not present on this system");
     if (bytes != (size_t)s.n * comps * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
@@ -2080,9 +2267,18 @@ int oracle_get_field(oracle_ctx* ctx, int handle, int field, void* host, size_t 
     const Handle& h = ctx->handles[handle];
     if (h.type == H_VIRT) {
         const Virt& vp = ctx->virts[h.idx];
-        if (field != GC_FIELD_W_SUM) return fail(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
-        if (bytes != vp.wsum.size() * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
-        if (bytes) std::memcpy(host, vp.wsum.data(), bytes);
+        if (field == GC_FIELD_W_SUM) {
+            if (bytes != vp.wsum.size() * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+            if (bytes) std::memcpy(host, vp.wsum.data(), bytes);
+            return GC_OK;
+        }
+        if (!vp.probe) return fail(ctx, GC_ERR_ARG, "a virtual system's fields are its source's");
+        Sys& p = ctx->sys[vp.src];
+        const int comps = field == GC_FIELD_COUNT ? 1 : field_comps(p, field);
+        if (comps < 0) return fail(ctx, GC_ERR_ARG, "field not present on this probe");
+        if (bytes != (size_t)p.n * comps * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+        if (field == GC_FIELD_ID) std::memcpy(host, p.id.data(), bytes);
+        else std::memcpy(host, (field == GC_FIELD_COUNT ? &p.drhodt : field_vec(p, field))->data(), bytes);
         return GC_OK;
     }
     if (h.type == H_GHOST) {
@@ -2121,7 +2317,8 @@ int oracle_step(oracle_ctx* ctx, int nsteps, double cfl) {
     if (ctx->inters.empty()) return fail(ctx, GC_ERR_ARG, "interactions must not be empty");
     const int nst = num_stages(ctx);
     for (auto& it : ctx->inters)
-        if (it.nstages != nst) return fail(ctx, GC_ERR_ARG, "All interactions must have the same number of stages");
+        if (!it.probe && it.nstages != nst)
+            return fail(ctx, GC_ERR_ARG, "All interactions must have the same number of stages");
     double dt = compute_dt(ctx, cfl);
     for (int s = 0; s < nsteps; ++s) {
         int st = ctx->integ == GC_INTEGRATOR_RK4 ? step_rk4(ctx, dt) : step_once(ctx, dt);

@@ -52,6 +52,11 @@ def lib():
             "oracle_set_integrator_kind": (ct.c_int, [ct.c_void_p, ct.c_int]),
             "oracle_set_velocity_adjust": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double]),
             "oracle_add_virtual": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _dp, _ip]),
+            "oracle_add_probe": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, _dp, ct.c_int, ct.c_int, ct.c_int,
+                                            _dp, _ip]),
+            "oracle_add_probe_interaction": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_double,
+                                                        ct.c_int, _dp, _ip]),
+            "oracle_measure_probes": (ct.c_int, [ct.c_void_p]),
             "oracle_set_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
             "oracle_get_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
             "oracle_get_count": (ct.c_int, [ct.c_void_p, ct.c_int, _i64p]),
@@ -172,6 +177,24 @@ class OracleBackend:
         self._chk(self.L.oracle_add_virtual(self.ctx, src, zero_mask, pv.ctypes.data_as(_dp), ct.byref(out)),
                   "add_virtual")
         return out.value
+
+    def add_probe(self, inst, n, nd, positions, mirror, extras_mask, ns, prescribed_v):
+        pos = None if positions is None else _a(positions, np.float64)
+        pv = _a(prescribed_v, np.float64)
+        out = ct.c_int()
+        self._chk(self.L.oracle_add_probe(self.ctx, n, nd, None if pos is None else pos.ctypes.data_as(_dp), mirror,
+                                          extras_mask, ns, pv.ctypes.data_as(_dp), ct.byref(out)), "add_probe")
+        return out.value
+
+    def add_probe_interaction(self, inst, a, probe, kernel_kind, h, pfn_kind, pfn_params):
+        p = _a(pfn_params, np.float64)
+        out = ct.c_int()
+        self._chk(self.L.oracle_add_probe_interaction(self.ctx, a, probe, kernel_kind, h, pfn_kind,
+                                                      p.ctypes.data_as(_dp), ct.byref(out)), "add_probe_interaction")
+        return out.value
+
+    def measure_probes(self):
+        self._chk(self.L.oracle_measure_probes(self.ctx), "measure_probes")
 
     def set_velocity_adjust(self, inst, inter, kind, epsilon):
         self._chk(self.L.oracle_set_velocity_adjust(self.ctx, inter, kind, epsilon), "set_velocity_adjust")
