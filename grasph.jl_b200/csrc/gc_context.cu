@@ -1665,6 +1665,9 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
     A.nd = S.nd;
     A.ns = S.ns;
     A.pfn = pfn;
+    if (pfn == GC_PFN_FLUID)  // a two-sided or fluid-solid reference needs the general fluid code
+        for (int id : ids)
+            if (pk0 == GC_PFN_FLUID_SOLID || ctx->inters[id].two_fluid) A.pfn = PFN_FLUID2;
     A.kk = ctx->inters[ids[0]].kk;
     A.aN = S.N;
     A.a_inst_of = S.inst_of;

@@ -27,6 +27,15 @@ enum { BT_SELF = 0, BT_DYNAMIC = 1, BT_STATIC = 2, BT_GHOST = 3, BT_SYSTEM = 4 }
 // per-particle divisor caches (one per slot, refreshed before each sweep)
 enum { AUX_P_OVER_RHO2 = 0, AUX_INV_RHO2 = 1, AUX_MASS_OVER_RHO = 2 };
 
+// Device-side functor code: FluidPfn with its two-sided (multiphase),
+// fluid-solid and surface-tension forms enabled; the plain GC_PFN_FLUID code
+// compiles them out of the pair loop.
+constexpr int PFN_FLUID2 = 16;
+template <int P>
+__host__ __device__ constexpr bool fluid_pfn() {
+    return P == GC_PFN_FLUID || P == PFN_FLUID2;
+}
+
 struct InterRef {
     int btype;
     const SysInst* bbox;  // per-instance bounding box of system_b (nullptr: never skip)

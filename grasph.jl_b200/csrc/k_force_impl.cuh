@@ -173,12 +173,12 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         double vj[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) vj[d] = m * o.v[d];
-        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID) {
+        if (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID) {
             double dv[ND];
 #pragma unroll
             for (int d = 0; d < ND; ++d) dv[d] = o.v[d] - vj[d];
             double piv = art_visc<ND>(dx, dv, rr, P.h, o.rho, o.rho, P.alpha, P.beta, ca, ca);
-            if (PFN == GC_PFN_FLUID) {
+            if (fluid_pfn<PFN>()) {
                 double dh = P.S == 1 ? -(A.a_p[gi] + A.a_p[gi]) / (o.rho * o.rho) : -(o.aux + o.aux);
                 double s = mass_a * (dh - piv);
 #pragma unroll
@@ -197,8 +197,8 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
             } else {
                 tail = zero_over(o.rho);
             }
-            double cdc = (PFN == GC_PFN_FLUID && P.S == 1) ? o.rho / o.rho : 1.0;
-            acc.dr = acc.dr + mass_a * ((PFN == GC_PFN_FLUID ? dr * cdc : dr) + tail);
+            double cdc = (fluid_pfn<PFN>() && P.S == 1) ? o.rho / o.rho : 1.0;
+            acc.dr = acc.dr + mass_a * ((fluid_pfn<PFN>() ? dr * cdc : dr) + tail);
         } else {  // strain rate (+ vorticity)
             double dv[ND];
 #pragma unroll
@@ -224,7 +224,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
     for (int d = 0; d < ND; ++d) vj[d] = r.bv[d * Nb + j];
     const double rhoj = r.brho[j];
 
-    if (r.btype == BT_STATIC && (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID)) {
+    if (r.btype == BT_STATIC && (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID)) {
         // src/PairwiseFunctors.jl:210-219, :322-331
         double dv[ND];
 #pragma unroll
@@ -237,15 +237,16 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         return 1;
     }
 
-    if (PFN == GC_PFN_FLUID) {
+    if (fluid_pfn<PFN>()) {
         double dv[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) dv[d] = o.v[d] - vj[d];
         // two-sided fluid x fluid :173 uses both sound speeds, one-sided :193 its own twice
-        const double cb = P.two ? G.bc : ca;
+        const bool two = PFN == PFN_FLUID2 && P.two;  // multiphase / fluid-solid variant only
+        const double cb = two ? G.bc : ca;
         double piv = art_visc<ND>(dx, dv, rr, P.h, o.rho, rhoj, P.alpha, P.beta, ca, cb);
         double dh;
-        if (P.fs) {
+        if (PFN == PFN_FLUID2 && P.fs) {
             // FluidSolidPfn :494-519: the fluid's pressure on both sides; the
             // fluid is the neighbour on the system_b side
             if (G.side_b) {
@@ -259,7 +260,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
             dh = P.S == 1 ? -(A.a_p[gi] + r.bp[j]) / (o.rho * rhoj) : -(o.aux + r.baux[j]);
         }
         double mj = r.btype == BT_SELF ? mass_a : G.bmass;
-        if (P.two) {
+        if (two) {
             // dv_tmp = (dh + ast - piv)·gx, then mass_j·dv_tmp; the system_b side
             // runs this same code with the roles swapped (every factor is
             // symmetric or flips sign exactly with dx, dv and gx)
@@ -377,7 +378,7 @@ struct PhysF64 {
         } else if (PFN == GC_PFN_XSPH) {  // advdt is the v_adjustment array here
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
-        } else if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        } else if (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc.dv[d] = A.advdt[d * N + gi];
             acc.dr = A.adrhodt[gi];
@@ -406,7 +407,7 @@ struct PhysF64 {
         } else if (PFN == GC_PFN_XSPH) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
-        } else if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        } else if (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) A.advdt[d * N + gi] = acc.dv[d];
             A.adrhodt[gi] = acc.dr;
@@ -539,7 +540,7 @@ struct PhysF32 {
     static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
         // FP64 state += compensated FP32 sum (s − c)
         const int64_t N = A.aN;
-        if (PFN == GC_PFN_FLUID || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        if (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
 #pragma unroll
             for (int d = 0; d < ND; ++d)
                 A.advdt[d * N + gi] = A.advdt[d * N + gi] + ((double)acc.dv[d] - (double)acc.cdv[d]);
@@ -705,7 +706,7 @@ struct PhysF32 {
 #pragma unroll
         for (int d = 0; d < ND; ++d) dv[d] = w.v[d] - vj[d];
         const bool self = r.btype == BT_SELF, dyn = r.btype == BT_DYNAMIC;
-        const bool two = P2 == GC_PFN_FLUID && P.two;
+        const bool two = P2 == PFN_FLUID2 && P.two;  // multiphase / fluid-solid variant only
         const float cb = ((P2 == GC_PFN_CAUCHY_FLUID && r.btype == BT_GHOST) || two) ? G.f_bc : ca;
         float piv = 0.f;
         const float vr = dotf<ND>(dxf, dv);
@@ -724,7 +725,7 @@ struct PhysF32 {
             return 1;
         }
         const float mj = (self || dyn) ? ma : G.f_bmass;
-        if (P2 == GC_PFN_FLUID) {
+        if (fluid_pfn<P2>()) {
             float dh;
             if (two && P.fs) {  // the fluid's pressure p = (p/ρ²)·ρ² on both sides
                 if (G.side_b) dh = -(auxj + (auxj * rhoj * rhoj) * w.irho * w.irho);
@@ -1075,6 +1076,7 @@ template <int ND, int NS, int KK, bool F32>
 static int launch_pfn(const ForceArgs& A, bool count_only, cudaStream_t s) {
     switch (A.pfn) {
         case GC_PFN_FLUID: launch_t<ND, NS, GC_PFN_FLUID, KK, F32>(A, count_only, s); return 0;
+        case PFN_FLUID2: launch_t<ND, NS, PFN_FLUID2, KK, F32>(A, count_only, s); return 0;
         case GC_PFN_COUNT: launch_t<ND, NS, GC_PFN_COUNT, KK, F32>(A, count_only, s); return 0;
         case GC_PFN_INTERPOLATE:  // FP64 only
             if constexpr (F32) {
