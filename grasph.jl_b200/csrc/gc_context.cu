@@ -78,6 +78,7 @@ struct HInter {
     int vk = GC_PFN_NONE;  // velocity_adjust_pairwise_fn
     double veps = 0.0;
     bool probe = false;    // one of the integrator's probe_interactions
+    int ag = -1;           // system_a is this ghost system (a = its source); InterpolateFieldFn only
 };
 struct HStaged {
     int handle, field;
@@ -198,6 +199,7 @@ struct DInter {
     bool two_fluid = false;  // FluidPfn stages are the two-sided fluid x fluid form
     bool probe = false;      // a probe interaction: swept by gc_measure_probes only
     bool vadj = false;       // pk[nstages] is the velocity-adjust functor (XSPH)
+    int ag = -1;             // system_a is this ghost system (a = its source slot)
     std::vector<int> pk;
     GridInst* d_gi = nullptr;
     GridInst* d_gi_b = nullptr;  // system_b side: system_a's mass and sound speed as the neighbour's
@@ -446,6 +448,15 @@ int check_combo(gc_ctx* ctx, const HInst& I, const HInter& it, int pk) {
     if (pk == GC_PFN_XSPH)
         return seterr(ctx, GC_ERR_UNSUPPORTED, "XSPHPfn is swept as velocity_adjust_pairwise_fn, not as a stage");
     if (pk < 0 || pk > GC_PFN_NEIGHBOR_COUNT) return seterr(ctx, GC_ERR_ARG, "bad functor kind %d", pk);
+    if (it.ag >= 0) {
+        // a ghost system_a (Trapdoor.jl's ghost_bottom): InterpolateFieldFn
+        // into a virtual system, reading the ghosts' current arrays
+        if (pk != GC_PFN_INTERPOLATE || it.b < 0 || I.handles[it.b].type != H_VIRT || I.virts[I.handles[it.b].idx].probe)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "a ghost system_a sweeps only InterpolateFieldFn into a virtual system");
+        const int m = (int)it.pp.back()[0];
+        if ((m & (1 << GC_FIELD_STRESS)) && !I.ghosts[it.ag].ex_stress)
+            return seterr(ctx, GC_ERR_UNSUPPORTED, "InterpolateFieldFn(:stress) from ghosts that carry no stress");
+    }
     if (pk == GC_PFN_NEIGHBOR_COUNT) {  // the (real, probe) method, src/PairwiseFunctors.jl:455
         if (it.b < 0 || I.handles[it.b].type != H_VIRT || !I.virts[I.handles[it.b].idx].probe)
             return seterr(ctx, GC_ERR_UNSUPPORTED, "NeighborCountFn needs a probe as system_b");
@@ -545,7 +556,7 @@ bool same_structure(const HInst& a, const HInst& b, std::string& why) {
     for (size_t i = 0; i < a.inters.size(); ++i) {
         const HInter &x = a.inters[i], &y = b.inters[i];
         if (x.a != y.a || x.b != y.b || x.kk != y.kk || x.nstages != y.nstages || x.pk != y.pk || x.vk != y.vk ||
-            x.probe != y.probe)
+            x.probe != y.probe || x.ag != y.ag)
             return why = "interactions", false;
         for (int s = 0; s < x.nstages; ++s) {
             if (x.pp[s][3] != y.pp[s][3] || std::isnan(x.pp[s][4]) != std::isnan(y.pp[s][4]))
@@ -836,6 +847,7 @@ int finalize(gc_ctx* ctx) {
         D.nstages = h0.nstages;
         D.pk = h0.pk;
         D.probe = h0.probe;
+        D.ag = h0.ag;
         D.vadj = h0.vk != GC_PFN_NONE;
         if (D.vadj) D.pk.push_back(h0.vk);  // the XSPH pass sweeps it as stage nstages + 1
         if (h0.b < 0) {
@@ -959,11 +971,11 @@ int finalize(gc_ctx* ctx) {
                 }
             }
         }
-        TRY(dalloc(ctx, &D.counts, (size_t)ctx->slots[D.a].N));
+        TRY(dalloc(ctx, &D.counts, (size_t)(D.ag >= 0 ? ctx->ghosts[D.ag].CAP : ctx->slots[D.a].N)));
         // writers
         bool writes = false;
         for (int s = 0; s < (int)D.pk.size(); ++s) writes |= D.pk[s] != GC_PFN_NONE;
-        if (writes) ctx->slots[D.a].written = true;
+        if (writes && D.ag < 0) ctx->slots[D.a].written = true;
         if (D.two_sided && D.bslot >= 0) ctx->slots[D.bslot].written = true;
         CU(cudaStreamSynchronize(ctx->stream));
     }
@@ -1152,7 +1164,7 @@ GridPlanArgs grid_plan_args(gc_ctx* ctx, DInter& D) {
     g.gi_b = D.d_gi_b;
     g.ninst = ninst(ctx);
     g.nd = ctx->slots[D.a].nd;
-    g.a = ctx->slots[D.a].d_inst;
+    g.a = D.ag >= 0 ? ctx->ghosts[D.ag].d_inst : ctx->slots[D.a].d_inst;
     if (D.btype == BT_GHOST) g.b = ctx->ghosts[D.bghost].d_inst;
     else if (D.btype != BT_SELF) g.b = ctx->slots[D.bslot].d_inst;
     g.need = ctx->d_need + D.need_slot;
@@ -1201,6 +1213,23 @@ int ghost_bbox_and_plan(gc_ctx* ctx, DGhost& G) {
     return check_launch(ctx, "ghost plan");
 }
 
+// system_a's particles of an interaction: a system slot's arrays, or (a
+// ghost system_a) the ghosts' current buffers up to the generated count
+struct AParts {
+    const double* x;
+    int64_t N;
+    const int32_t* inst_of;
+    const int64_t* count;
+};
+AParts a_parts(gc_ctx* ctx, const DInter& D) {
+    if (D.ag >= 0) {
+        DGhost& G = ctx->ghosts[D.ag];
+        return AParts{G.x[G.cur], G.CAP, G.ginst[G.cur], G.d_count};
+    }
+    DSlot& A = ctx->slots[D.a];
+    return AParts{A.F(F_X), A.N, A.inst_of, nullptr};
+}
+
 int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
     TRY(ensure_inter_cells(ctx, D, cells));
     DSlot& A = ctx->slots[D.a];
@@ -1223,7 +1252,8 @@ int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
     launch_grid_count(bx, bN, A.nd, binst, bcount, D.d_gi, ctx->hist, cells, ctx->d_err, ctx->d_incons, ctx->stream);
     scan_exclusive_clear(ctx->hist, D.cs, cells, ctx->scan_tmp, ctx->stream);
     if (D.two_sided) {
-        launch_grid_count(A.F(F_X), A.N, A.nd, A.inst_of, nullptr, D.d_gi, ctx->hist, cells, ctx->d_err,
+        const AParts ap = a_parts(ctx, D);
+        launch_grid_count(ap.x, ap.N, A.nd, ap.inst_of, ap.count, D.d_gi, ctx->hist, cells, ctx->d_err,
                           ctx->d_incons, ctx->stream);
         scan_exclusive_clear(ctx->hist, D.cs_a, cells, ctx->scan_tmp, ctx->stream);
     }
@@ -1237,9 +1267,9 @@ int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
 // CSR of system_a's particles on a coupled interaction's grid.
 int ensure_csa(gc_ctx* ctx, DInter& D) {
     if (D.btype == BT_SELF || D.csa_ver == D.grid_ver) return GC_OK;
-    DSlot& A = ctx->slots[D.a];
+    const AParts ap = a_parts(ctx, D);
     TRY(ensure_cells(ctx, D.cells));
-    launch_grid_count(A.F(F_X), A.N, A.nd, A.inst_of, nullptr, D.d_gi, ctx->hist, D.cells, ctx->d_err,
+    launch_grid_count(ap.x, ap.N, ctx->slots[D.a].nd, ap.inst_of, ap.count, D.d_gi, ctx->hist, D.cells, ctx->d_err,
                       ctx->d_incons, ctx->stream);
     scan_exclusive_clear(ctx->hist, D.cs_a, D.cells, ctx->scan_tmp, ctx->stream);
     D.csa_ver = D.grid_ver;
@@ -1352,7 +1382,7 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     // cell count cannot exceed the planned bound)
     for (auto& D : ctx->inters) {
         if (D.probe) continue;
-        if (D.btype == BT_GHOST) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
+        if (D.btype == BT_GHOST || D.ag >= 0) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
         TRY(build_grid(ctx, D, need[D.need_slot]));
     }
     return GC_OK;
@@ -1618,12 +1648,25 @@ int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
         r.pi = D.d_pi[stage - 1];
         r.cs = D.cs_a;
         r.cs_cells = D.cells;
-        r.bx = S.F(F_X);
-        r.bv = S.F(F_V);
-        r.brho = S.F(F_RHO);
-        r.bp = S.F(F_P);
-        r.bstress = S.F(F_STRESS);
-        r.bN = S.N;
+        if (D.ag >= 0) {
+            // Trapdoor.jl's ghost_bottom: the ghosts' current arrays (stress
+            // as the last GhostCopier left it), the source's mass in gi_b
+            DGhost& Gh = ctx->ghosts[D.ag];
+            r.bbox = Gh.d_inst;
+            r.bx = Gh.x[Gh.cur];
+            r.bv = Gh.v;
+            r.brho = Gh.rho;
+            r.bp = Gh.p;
+            r.bstress = Gh.stress;
+            r.bN = Gh.CAP;
+        } else {
+            r.bx = S.F(F_X);
+            r.bv = S.F(F_V);
+            r.brho = S.F(F_RHO);
+            r.bp = S.F(F_P);
+            r.bstress = S.F(F_STRESS);
+            r.bN = S.N;
+        }
         int st = launch_force_f64(R, false, ctx->stream);
         if (st) return seterr(ctx, st, "InterpolateFieldFn not implemented on the device for this system");
         TRY(check_launch(ctx, "sweep (interpolation)"));
@@ -2717,6 +2760,12 @@ int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kerne
     if (!ctx || !inter_out) return GC_ERR_ARG;
     if (ctx->finalized) return seterr(ctx, GC_ERR_STATE, "context already finalized");
     int si = sys_of(ctx, inst, sys_a);
+    int ag = -1;
+    if (si < 0 && valid_inst(ctx, inst) && sys_a >= 0 && sys_a < (int)ctx->inst[inst].handles.size() &&
+        ctx->inst[inst].handles[sys_a].type == H_GHOST) {
+        ag = ctx->inst[inst].handles[sys_a].idx;
+        si = ctx->inst[inst].ghosts[ag].src;
+    }
     if (si < 0) return seterr(ctx, GC_ERR_ARG, "system_a must be a system handle");
     HInst& I = ctx->inst[inst];
     if (b_handle >= (int)I.handles.size()) return seterr(ctx, GC_ERR_ARG, "bad system_b handle");
@@ -2725,6 +2774,7 @@ int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kerne
         return seterr(ctx, GC_ERR_ARG, "bad kernel kind");
     HInter it;
     it.a = si;
+    it.ag = ag;
     it.b = b_handle;
     it.kk = kernel_kind;
     it.H = h;
@@ -2953,6 +3003,8 @@ int gc_set_velocity_adjust(gc_ctx* ctx, int inst, int inter, int kind, double ep
     if (inter < 0 || inter >= (int)I.inters.size()) return seterr(ctx, GC_ERR_ARG, "bad interaction");
     if (kind != GC_PFN_NONE && kind != GC_PFN_XSPH)
         return seterr(ctx, GC_ERR_UNSUPPORTED, "velocity-adjust functor kind %d has no device implementation", kind);
+    if (kind != GC_PFN_NONE && I.inters[inter].ag >= 0)
+        return seterr(ctx, GC_ERR_UNSUPPORTED, "no velocity-adjust functor on a ghost system_a");
     I.inters[inter].vk = kind;
     I.inters[inter].veps = epsilon;
     return GC_OK;
@@ -3369,8 +3421,9 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
         int64_t pairs = 0;
         for (auto& D : ctx->inters) {
             if (D.probe) continue;
+            // InterpolateFieldFn stages gather on the system_b side and count nothing
             bool active = false;
-            for (int p : D.pk) active |= p != GC_PFN_NONE;
+            for (int p : D.pk) active |= p != GC_PFN_NONE && p != GC_PFN_INTERPOLATE && p != GC_PFN_NEIGHBOR_COUNT;
             if (!active) continue;
             CU(cudaMemsetAsync(ctx->d_pairs, 0, 8, ctx->stream));
             launch_sum_counts(D.counts, ctx->slots[D.a].N, ctx->d_pairs, ctx->stream);
@@ -3446,7 +3499,13 @@ int gc_build_grid(gc_ctx* ctx, int inst, int inter, int64_t* cell_start_out, int
     DInter& D = ctx->inters[inter];
     CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     CU(cudaMemsetAsync(ctx->d_need, 0, sizeof(int64_t) * ctx->nneed, ctx->stream));
-    TRY(bbox_slot(ctx, ctx->slots[D.a]));
+    if (D.ag >= 0) {
+        DGhost& G = ctx->ghosts[D.ag];
+        launch_bbox_fused(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
+                          ctx->d_err, ctx->stream);
+    } else {
+        TRY(bbox_slot(ctx, ctx->slots[D.a]));
+    }
     if (D.btype == BT_GHOST) {
         DGhost& G = ctx->ghosts[D.bghost];
         launch_bbox_fused(G.x[G.cur], G.CAP, G.nd, G.ginst[G.cur], G.d_count, G.d_inst, ctx->bbox_scratch, ninst(ctx),
@@ -3551,6 +3610,7 @@ int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, in
         return seterr(ctx, GC_ERR_ARG, "bad interaction");
     DInter& D = ctx->inters[inter];
     DSlot& S = ctx->slots[D.a];
+    if (D.ag >= 0) return seterr(ctx, GC_ERR_UNSUPPORTED, "neighbour counts of a ghost system_a");
     if (n != S.h_inst[inst].n) return seterr(ctx, GC_ERR_ARG, "count buffer length mismatch");
     // A counting sweep: the first non-`nothing` stage's functor kind decides
     // the launch; counts do not depend on it.

@@ -403,7 +403,11 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
         m.ghosts.append(ge)
     for it in interactions:
         a = it.system_a
-        if id(a) not in sys_ids:
+        if isinstance(a, GhostParticleSystem):
+            # InterpolateFieldFn from the ghosts' current arrays (Trapdoor.jl's ghost_bottom)
+            if id(a) not in m.handles:
+                raise ArgumentError("a ghost used as system_a must belong to a GhostEntry in `ghosts`")
+        elif id(a) not in sys_ids:
             raise ArgumentError("system_a must be in the integrator's systems")
         b = it.system_b
         if b is None:

@@ -656,7 +656,7 @@ class SystemInteraction:
         if system_b is not None and system_b.ndims != nd:
             raise ArgumentError(
                 f"system_b.ndims ({system_b.ndims}) must match system_a.ndims ({nd})")
-        if not isinstance(system_a, AbstractParticleSystem):
+        if not isinstance(system_a, (AbstractParticleSystem, GhostParticleSystem)):
             raise ArgumentError("system_a must be a particle system")
         vpf = velocity_adjust_pairwise_fn
         if vpf is not None and not isinstance(vpf, XSPHPfn):

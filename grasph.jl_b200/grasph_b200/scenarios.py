@@ -21,7 +21,8 @@ import numpy as np
 from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, DynamicBoundarySystem,
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
                     FluidSolidPfn, HookeLawStressUpdater,
-                    GhostCopier, GhostEntry, GhostParticleSystem, LeapFrogTimeIntegrator, LinearEOSUpdater,
+                    GhostCopier, GhostEntry, GhostParticleSystem, HouseholderReflect, LeapFrogTimeIntegrator,
+                    LinearEOSUpdater, ProbeParticleSystem,
                     RK4TimeIntegrator, StrainRatePfn, InterpolateFieldFn, VirtualNormUpdater,
                     VirtualParticleSystem, PrescribedVelocityUpdater, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
                     TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater)
@@ -293,6 +294,85 @@ def ep_column_virtual(dx=0.002, width=0.2, height=0.1, bottom_len=0.5, rho0=1850
     lf = LeapFrogTimeIntegrator([fluid], inters, virtual_systems=(bottom, left))
     meta = dict(workload="ep_column_virtual", n_fluid=fluid.n, n_bottom=bsrc.n, n_left=lsrc.n, h=h, c0=c,
                 cfl=cfl, dt=cfl * h / c, ndims=2)
+    return lf, meta
+
+
+# ------------------------------------------------------------------ trapdoor
+
+def trapdoor(nx=264, ny=100, ntd_x=40, n_layers=10, dx=0.05, rho0=1600.0, E=10.0e6, nu=0.33, phi_deg=39.0,
+             psi_deg=19.0, cohesion=0.0, alpha=0.1, beta=0.0, moving=False, trapdoor_v=-0.005, damping=0.002,
+             cfl=0.1, geostatic=False):
+    """2-D trapdoor (Trapdoor.jl layout): an nx x ny ElastoPlasticParticleSystem
+    soil (NS = 4, four stages), left and right free-slip walls as one
+    GhostEntry whose ghosts copy the stress (Householder-reflected) at stage
+    3, a static bottom on both flanks and a centre trapdoor of ntd_x columns
+    as VirtualParticleSystems (n_layers layers below y = 0), filled by
+    InterpolateFieldFn(:rho) at stage 1 and (:stress) at stage 3 from the
+    soil and from the wall ghosts (ghost_bottom: the ghost system as
+    system_a), normalised at stages 2 and 4, and five stress probes across
+    the trapdoor's top.  `moving=False` is the script's settling integrator
+    (trapdoor and probes static, damping Γ); `moving=True` its second
+    integrator (trapdoor and probes at trapdoor_v, no damping).
+    `geostatic` starts the soil from K0 stress instead of zero stress."""
+    phi, psi = phi_deg * math.pi / 180.0, psi_deg * math.pi / 180.0
+    c = math.sqrt(E * (1 - nu) / (rho0 * (1 + nu) * (1 - 2 * nu)))
+    h = 1.2 * dx
+    mass = rho0 * dx * dx
+    nleft = (nx - ntd_x) // 2
+    soil = ElastoPlasticParticleSystem(
+        "soil", nx * ny, 2, 4, mass, c, source_v=[0.0, -G],
+        state_updater=(None, ZeroFieldUpdater("strain_rate", "vorticity"),
+                       ElastoPlasticStressUpdater(E, nu, phi, psi, cohesion), None))
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")  # i outer, j inner
+    soil.x[:, 0] = (ii.ravel() + 0.5) * dx
+    soil.x[:, 1] = (jj.ravel() + 0.5) * dx
+    soil.rho[:] = rho0
+    if geostatic:
+        K0 = 1.0 - math.sin(phi)
+        syy = -rho0 * G * (ny * dx - soil.x[:, 1])
+        soil.stress[:, 0] = K0 * syy
+        soil.stress[:, 1] = syy
+        soil.stress[:, 2] = K0 * syy
+    flank = [i for i in range(-5, nleft)] + [i for i in range(nleft + ntd_x, nx + 5)]
+    bpts = [((i + 0.5) * dx, -(j - 0.5) * dx) for j in range(1, n_layers + 1) for i in flank]
+    bsrc = StressParticleSystem("bottom_source", len(bpts), 2, 4, mass, c)
+    bsrc.x[:] = bpts
+    bsrc.rho[:] = rho0
+    tpts = [((i + 0.5) * dx, -(j - 0.5) * dx) for j in range(1, n_layers + 1) for i in range(nleft, nleft + ntd_x)]
+    tsrc = StressParticleSystem("trapdoor_source", len(tpts), 2, 4, mass, c)
+    tsrc.x[:] = tpts
+    tsrc.rho[:] = rho0
+    upd = (None, (VirtualNormUpdater((0.0, 0.0), "rho"), PrescribedVelocityUpdater()), None,
+           VirtualNormUpdater((0.0, 0.0), "stress"))
+    bottom = VirtualParticleSystem(bsrc, "bottom_virt", bsrc.n, 2, mass, c, zero_fields=("v", "rho", "stress"),
+                                   state_updater=upd)
+    pv = (0.0, trapdoor_v) if moving else None
+    door = VirtualParticleSystem(tsrc, "trapdoor_moving_virt" if moving else "trapdoor_static_virt", tsrc.n, 2,
+                                 mass, c, zero_fields=("v", "rho", "stress"), prescribed_v=pv, state_updater=upd)
+    ghost = GhostParticleSystem(soil, None, None, GhostCopier(("stress", HouseholderReflect())), None,
+                                name="walls_ghost")
+    walls = GhostEntry(ghost, 3.0 * h, ((1.0, 0.0), (0.0, 0.0)), ((-1.0, 0.0), (nx * dx, 0.0)))
+    kernel = CubicSplineKernel(h, ndims=2)
+    sr = StrainRateVorticityPfn()
+    kin = CauchyFluidPfn(alpha, beta, h)
+    irho = InterpolateFieldFn("rho", accumulate_wsum=True)
+    istr = InterpolateFieldFn("stress", accumulate_wsum=False)
+    inters = [SystemInteraction(kernel, (None, sr, None, kin), soil),
+              SystemInteraction(kernel, (irho, sr, istr, kin), soil, bottom),
+              SystemInteraction(kernel, (irho, None, istr, None), ghost, bottom),
+              SystemInteraction(kernel, (irho, sr, istr, kin), soil, door),
+              SystemInteraction(kernel, (None, sr, None, kin), soil, ghost)]
+    npr = 5
+    ppos = [(nleft * dx + k * (ntd_x * dx / (npr - 1)), 0.0) for k in range(npr)]
+    probe = ProbeParticleSystem("td_probe_moving" if moving else "td_probe_static", ppos,
+                                extras={"stress": np.zeros((npr, 4))},
+                                state_updater=VirtualNormUpdater((1.0, 1.0), "stress"), prescribed_v=pv)
+    pint = SystemInteraction(kernel, InterpolateFieldFn("stress"), soil, probe)
+    kw = {} if moving else {"Γ": damping}
+    lf = LeapFrogTimeIntegrator([soil], inters, ghosts=(walls,), virtual_systems=(bottom, door), probes=(probe,),
+                                probe_interactions=(pint,), **kw)
+    meta = dict(workload="trapdoor", n_soil=soil.n, n_bottom=bsrc.n, n_trapdoor=tsrc.n, h=h, c0=c, cfl=cfl,
+                dt=cfl * h / c, ndims=2)
     return lf, meta
 
 

@@ -205,7 +205,9 @@ int gc_add_ghost(gc_ctx* ctx, int inst, int src_sys, int ncopiers,
 /* SystemInteraction(kernel, pfns, system_a[, system_b]) src/Interaction.jl:61,
  * with CubicSplineKernel(h; ndims) src/Kernels.jl:34 or WenlandC2Kernel :108.
  * b_handle = -1 for a self interaction.  pfn_params holds
- * nstages×GC_PFN_NPARAM doubles.                                           */
+ * nstages×GC_PFN_NPARAM doubles.  sys_a may be a ghost handle when every
+ * stage is `nothing` or InterpolateFieldFn into a virtual system_b: the
+ * ghosts' current arrays are interpolated (Trapdoor.jl's ghost_bottom).    */
 int gc_add_interaction(gc_ctx* ctx, int inst, int sys_a, int b_handle, int kernel_kind,
                        double h, int nstages, const int* pfn_kinds, const double* pfn_params,
                        int* inter_out);

@@ -190,6 +190,8 @@ struct Inter {
     double mina[3] = {0, 0, 0}, maxa[3] = {0, 0, 0};
     bool grid = false;
     bool probe = false;  // one of the integrator's probe_interactions (swept at measurement only)
+    int ag = -1;         // system_a is this ghost system (a = its source); InterpolateFieldFn only
+    Sys proxy;           // the ghost's current arrays as a system (system_a of such an interaction)
     int vk = GC_PFN_NONE;  // velocity_adjust_pairwise_fn (XSPHPfn or nothing)
     double veps = 0.0;     // its epsilon
 };
@@ -809,10 +811,35 @@ void sweep_self(oracle_ctx* ctx, Inter& it, const Pfn& f) {
 
 int make_view(oracle_ctx* ctx, int handle, BView* out);
 
+// system_a of an interaction: a system, or (InterpolateFieldFn from ghosts,
+// Trapdoor.jl's ghost_bottom) a ghost system's current arrays with its
+// source's mass and sound speed
+Sys& system_a(oracle_ctx* ctx, Inter& it) {
+    if (it.ag < 0) return ctx->sys[it.a];
+    const Ghost& g = ctx->ghosts[it.ag];
+    const Sys& src = ctx->sys[g.src];
+    Sys& p = it.proxy;
+    p.kind = src.kind;
+    p.nd = src.nd;
+    p.ns = src.ns;
+    p.n = g.n;
+    p.mass = src.mass;
+    p.c = src.c;
+    const size_t n = (size_t)g.n, nd = (size_t)src.nd, ns = (size_t)src.ns;
+    p.x.assign(g.x.begin(), g.x.begin() + n * nd);
+    p.v.assign(g.v.begin(), g.v.begin() + n * nd);
+    p.rho.assign(g.rho.begin(), g.rho.begin() + n);
+    if (g.ex_stress) p.stress.assign(g.stress.begin(), g.stress.begin() + n * ns);
+    else p.stress.assign(n * ns, 0.0);
+    if (g.ex_p) p.p.assign(g.p.begin(), g.p.begin() + n);
+    else p.p.assign(n, 0.0);
+    return p;
+}
+
 // src/Interaction.jl:600-645 (2-D coupled, 9 colours), :660-715 (3-D, 27 colours)
 template <int ND>
 int sweep_coupled(oracle_ctx* ctx, Inter& it, const Pfn& f, const BView& b) {
-    Sys& a = ctx->sys[it.a];
+    Sys& a = system_a(ctx, it);
     int err = 0;
     // a ghost's XSPH writes land in its source's array at ghost indices, which
     // a-side writes of other cells of the colour may also touch: one thread
@@ -929,7 +956,7 @@ void bbox(const double* x, int64_t n, int nd, double* mn, double* mx, bool init)
 }
 
 int create_grid(oracle_ctx* ctx, Inter& it) {
-    Sys& a = ctx->sys[it.a];
+    Sys& a = system_a(ctx, it);
     const int nd = a.nd;
     const double cutoff = it.cell;
     double mn[3], mx[3];
@@ -1417,6 +1444,14 @@ int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     const Sys& a = ctx->sys[it.a];
     if (pk == GC_PFN_NONE) return GC_OK;
     if (pk == GC_PFN_XSPH || pk < 0 || pk > GC_PFN_NEIGHBOR_COUNT) return GC_ERR_UNSUPPORTED;  // XSPH: velocity-adjust only
+    if (it.ag >= 0) {
+        // a ghost system_a: only InterpolateFieldFn into a virtual system
+        if (pk != GC_PFN_INTERPOLATE || it.b < 0 || ctx->handles[it.b].type != H_VIRT ||
+            ctx->virts[ctx->handles[it.b].idx].probe)
+            return GC_ERR_UNSUPPORTED;
+        const int m = (int)it.pp.back()[0];
+        if ((m & (1 << GC_FIELD_STRESS)) && !ctx->ghosts[it.ag].ex_stress) return GC_ERR_UNSUPPORTED;
+    }
     if (pk == GC_PFN_NEIGHBOR_COUNT) {  // the (real, probe) method :455
         if (it.b < 0 || ctx->handles[it.b].type != H_VIRT || !ctx->virts[ctx->handles[it.b].idx].probe)
             return GC_ERR_UNSUPPORTED;
@@ -2042,10 +2077,16 @@ int oracle_add_ghost(oracle_ctx* ctx, int src_sys, int ncopiers, const int* copi
 int oracle_add_interaction(oracle_ctx* ctx, int sys_a, int b_handle, int kernel_kind, double h, int nstages,
                            const int* pfn_kinds, const double* pfn_params, int* inter_out) {
     int si = sys_index(ctx, sys_a);
+    int ag = -1;
+    if (si < 0 && sys_a >= 0 && sys_a < (int)ctx->handles.size() && ctx->handles[sys_a].type == H_GHOST) {
+        ag = ctx->handles[sys_a].idx;
+        si = ctx->ghosts[ag].src;
+    }
     if (si < 0) return fail(ctx, GC_ERR_ARG, "system_a must be a system");
     if (b_handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad system_b handle");
     Inter it;
     it.a = si;
+    it.ag = ag;
     it.b = b_handle;
     it.kk = kernel_kind;
     it.H = h;
@@ -2218,6 +2259,8 @@ int oracle_set_updaters(oracle_ctx* ctx, int sys, int nstages, const int* chain_
 int oracle_set_velocity_adjust(oracle_ctx* ctx, int inter, int kind, double epsilon) {
     if (!ctx || inter < 0 || inter >= (int)ctx->inters.size()) return GC_ERR_ARG;
     if (kind != GC_PFN_NONE && kind != GC_PFN_XSPH) return fail(ctx, GC_ERR_ARG, "velocity-adjust functor kind");
+    if (kind != GC_PFN_NONE && ctx->inters[inter].ag >= 0)
+        return fail(ctx, GC_ERR_UNSUPPORTED, "no velocity-adjust functor on a ghost system_a");
     ctx->inters[inter].vk = kind;
     ctx->inters[inter].veps = epsilon;
     return GC_OK;
