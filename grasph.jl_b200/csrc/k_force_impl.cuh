@@ -1017,6 +1017,232 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     }
 }
 
+// ------------------------------------------------- staged FP32 sweep
+// Shared memory of one warp of k_sweep_stg: the staged copies of a chunk of
+// CH candidates ([NQ][CH] 16-byte chunks: FP64 position, then FP32 record),
+// lane 0's position (the origin of the prefilter), and the candidates'
+// FP32 coordinates relative to it ([ND][CH]).
+template <int ND, int NQ, int CH>
+__host__ __device__ constexpr int stg_warp_bytes() {
+    return NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16;
+}
+
+// The FP32-compensated sweep with chunk staging.  The walk is k_sweep's (one
+// warp per group of one grid column, the union of its lanes' candidate
+// ranges strip by strip), but the warp copies each chunk of up to CH
+// consecutive candidates of a strip into its shared memory once (16-byte
+// asynchronous copies, one round trip per chunk), tests them against every
+// lane with the FP32 prefilter, and then evaluates each lane's accepted
+// candidates of the chunk from the staged copies.  No pair waits on a
+// global load; the exact cutoff test and the pair arithmetic are the
+// policy's pair_data, as in k_sweep.
+template <class Phys, int ND, int PFN, int MINB, int CH>
+__global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
+    static_assert(CH % 32 == 0 && CH >= 32 && CH <= 128, "chunk of 1 to 4 batches of 32");
+    constexpr int NB = CH / 32;
+    constexpr int NQ = Phys::NQ;
+    constexpr int WB = stg_warp_bytes<ND, NQ, CH>();
+    extern __shared__ float4 sstg[];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    char* wbase = reinterpret_cast<char*>(sstg) + (threadIdx.x >> 5) * WB;
+    float4* slots = reinterpret_cast<float4*>(wbase);
+    double* xref = reinterpret_cast<double*>(wbase + NQ * CH * 16);
+    float* cand = reinterpret_cast<float*>(wbase + NQ * CH * 16 + 32);
+    const int64_t ngroups = *A.ngroups;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
+        const int2 grp = A.groups[wg];
+        const bool active = lane < grp.y;
+        const int32_t gi = grp.x + (active ? lane : 0);  // packed indices fit int32
+        const int k = A.a_inst_of[gi];
+        typename Phys::Own w;
+        Phys::load(A, gi, w);
+        const double* ox = Phys::xpos(w);
+        typename Phys::AccT acc;
+        Phys::init(A, gi, acc, true);
+
+        for (int ri = 0; ri < A.nref; ++ri) {
+            const InterRef& r = A.ref[ri];
+            const GridInst& G = r.gi[k];
+            const PfnInst& P = r.pi[k];
+            if (r.bbox) {
+                // no system_b particle within the cutoff of any lane (0.1% margin)
+                const SysInst& B = r.bbox[k];
+                bool near = B.n > 0;
+                const double m = 1.001 * G.cell;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) near = near && ox[d] >= B.bbmin[d] - m && ox[d] <= B.bbmax[d] + m;
+                if (!__any_sync(FULL, active && near)) {
+                    if (active && r.counts) r.counts[gi] = 0;
+                    continue;
+                }
+            }
+            if (G.cellbase + G.ncells > r.cs_cells) {
+                // this instance's grid did not fit its buffer: flag it, read nothing
+                if (lane == 0) atomicOr(A.err, ERR_CAPACITY);
+                if (active && r.counts) r.counts[gi] = 0;
+                continue;
+            }
+            int32_t c[ND];
+            bool ok = true;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                int64_t cd;
+                if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &cd) || cd < 1 || cd >= G.ng[d] - 1) {
+                    ok = false;
+                    cd = 1;
+                }
+                c[d] = (int32_t)cd;
+            }
+            if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
+            const double da = r.btype == BT_DYNAMIC ? Phys::plane_da(w, G) : 0.0;
+            const bool self = r.btype == BT_SELF;
+            int32_t accepted = 0;
+            const int32_t c0 = __shfl_sync(FULL, c[0], 0);
+            const int32_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
+            const bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
+            const bool coop = __all_sync(FULL, !active || same);
+            const int nstrips = ND == 2 ? 3 : 9;
+            if (coop) {
+                constexpr int L = ND - 1;
+                int32_t zlo = active ? c[L] : INT32_MAX, zhi = active ? c[L] : INT32_MIN;
+#pragma unroll
+                for (int o2 = 16; o2 > 0; o2 >>= 1) {
+                    int32_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
+                    zlo = a2 < zlo ? a2 : zlo;
+                    zhi = b2 > zhi ? b2 : zhi;
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) xref[d] = ox[d];
+                }
+                __syncwarp();
+                // conservative FP32 prefilter relative to lane 0 (k_sweep's);
+                // inactive lanes test against NaN and accept nothing
+                float xi[ND];
+#pragma unroll
+                for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
+                const float cut_f = (float)(G.cutoff_sq * 1.001);
+                const float2 neg1 = make_float2(-1.0f, -1.0f);
+                const int64_t ngl = G.ng[L];
+                auto strip_base = [&](int s2) -> int64_t {
+                    int64_t colflat;
+                    if (ND == 2) colflat = c0 + s2 - 1;
+                    else colflat = (c0 + s2 / 3 - 1) * G.ng[1] + (c1 + s2 % 3 - 1);
+                    return G.cellbase + colflat * ngl;
+                };
+                // every strip's warp-wide candidate range, lane s holding strip s's
+                int32_t su0 = 0, su1 = 0;
+                if (lane < nstrips) {
+                    const int64_t b2 = strip_base(lane);
+                    su0 = r.cs[b2 + zlo - 1];
+                    su1 = r.cs[b2 + zhi + 2];
+                }
+                for (int sidx = 0; sidx < nstrips; ++sidx) {
+                    const int32_t u0 = __shfl_sync(FULL, su0, sidx), u1 = __shfl_sync(FULL, su1, sidx);
+                    if (u0 >= u1) continue;  // warp-uniform
+                    const int64_t base = strip_base(sidx);
+                    // this lane's own strip range [cs[z-1], cs[z+2])
+                    const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
+                    for (int32_t ch = u0; ch < u1; ch += CH) {
+                        const int n = u1 - ch < CH ? (int)(u1 - ch) : CH;
+                        for (int i = lane; i < n; i += 32) Phys::issue(r, ch + i, slots + i, CH);
+                        __pipeline_commit();
+                        __pipeline_wait_prior(0);
+                        // this lane's staged positions -> relative FP32 coordinates
+#pragma unroll
+                        for (int i0 = 0; i0 < CH; i0 += 32) {
+                            const int i = i0 + lane;
+#pragma unroll
+                            for (int d = 0; d < ND; ++d) {
+                                float v = 1e30f;  // beyond the chunk: far away
+                                if (i < n) {
+                                    const double2 t = *reinterpret_cast<const double2*>(&slots[(d >> 1) * CH + i]);
+                                    v = (float)(((d & 1) ? t.y : t.x) - xref[d]);
+                                }
+                                cand[d * CH + i] = v;
+                            }
+                        }
+                        __syncwarp();
+                        // accepted candidates of the chunk, one mask per batch of 32
+                        unsigned msk[NB];
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) {
+                            msk[b] = 0u;
+                            if (32 * b < n) {
+                                const int mb = n - 32 * b < 32 ? n - 32 * b : 32;
+                                const float* cb = cand + 32 * b;
+                                unsigned hits = 0;
+                                for (int t0 = 0; t0 < mb; t0 += 8) {
+                                    unsigned h8 = 0;
+#pragma unroll
+                                    for (int t = 0; t < 8; t += 2) {
+                                        float2 rr;
+                                        {
+                                            const float2 xj = *reinterpret_cast<const float2*>(cb + t0 + t);
+                                            const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[0], xi[0]));
+                                            rr = __fmul2_rn(dd, dd);
+                                        }
+#pragma unroll
+                                        for (int d = 1; d < ND; ++d) {
+                                            const float2 xj = *reinterpret_cast<const float2*>(cb + d * CH + t0 + t);
+                                            const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[d], xi[d]));
+                                            rr = __ffma2_rn(dd, dd, rr);
+                                        }
+                                        if (rr.x < cut_f) h8 |= 1u << t;
+                                        if (rr.y < cut_f) h8 |= 2u << t;
+                                    }
+                                    hits |= h8 << t0;
+                                }
+                                // this lane's own strip range and the self pair
+                                const int32_t jb = ch + 32 * b;
+                                const int32_t tlo = lo - jb, thi = hi - jb;
+                                unsigned allow = tlo <= 0 ? 0xffffffffu : (tlo >= 32 ? 0u : 0xffffffffu << tlo);
+                                allow &= thi >= 32 ? 0xffffffffu : (thi <= 0 ? 0u : 0xffffffffu >> (32 - thi));
+                                if (self) {
+                                    const int32_t ts = gi - jb;
+                                    if (ts >= 0 && ts < 32) allow &= ~(1u << ts);
+                                }
+                                msk[b] = hits & allow;
+                            }
+                        }
+                        // this lane's accepted candidates, from the staged copies
+                        while (true) {
+                            int t = -1;
+#pragma unroll
+                            for (int b = 0; b < NB; ++b)
+                                if (t < 0 && msk[b]) {
+                                    t = 32 * b + __ffs(msk[b]) - 1;
+                                    msk[b] &= msk[b] - 1;
+                                }
+                            if (t < 0) break;
+                            accepted += Phys::template pair_slot<PFN>(A, r, G, P, gi, k, w, da, slots + t, CH, acc);
+                        }
+                        __syncwarp();  // every lane is done with the chunk before the next one lands
+                    }
+                }
+            } else if (active && ok) {
+                // rare: lanes disagree on the column in this grid; walk own strips
+                for (int sidx = 0; sidx < nstrips; ++sidx) {
+                    int64_t base;
+                    if (ND == 2) base = G.cellbase + (c[0] + sidx - 1) * G.ng[1] + (c[1] - 1);
+                    else base = G.cellbase + ((c[0] + sidx / 3 - 1) * G.ng[1] + (c[1] + sidx % 3 - 1)) * G.ng[2] + (c[2] - 1);
+                    const int32_t s0 = r.cs[base], e0 = r.cs[base + 3];
+                    for (int32_t j = s0; j < e0; ++j) {
+                        if (self && j == gi) continue;
+                        accepted += Phys::template pair<PFN>(A, r, G, P, gi, k, w, da, j, acc);
+                    }
+                }
+            }
+            __syncwarp();
+            if (active && r.counts) r.counts[gi] = accepted;
+        }
+        if (active) Phys::store(A, gi, acc);
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------ dispatch
 template <class Phys, int ND, int PFN, int C>
 static void launch_c(const ForceArgs& A, cudaStream_t s) {
@@ -1025,6 +1251,19 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     int64_t blocks = (warps * 32 + FORCE_TPB - 1) / FORCE_TPB;
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
+    if constexpr (cf.stg > 0 && Phys::NQ > 0) {
+        constexpr size_t smem = (size_t)(FORCE_TPB / 32) * stg_warp_bytes<ND, Phys::NQ, cf.stg>();
+        auto kern = k_sweep_stg<Phys, ND, PFN, cf.minb, cf.stg>;
+        if (smem > 48 * 1024) {
+            static bool opted = false;
+            if (!opted) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                opted = true;
+            }
+        }
+        kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
+        return;
+    }
     constexpr bool PRE = cf.pre && Phys::NQ > 0;
     const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float) +
                         (PRE ? (size_t)2 * Phys::NQ * FORCE_TPB * 16 : 0);
