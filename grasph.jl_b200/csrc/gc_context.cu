@@ -267,8 +267,9 @@ struct gc_ctx {
     int64_t grid_version = 0;
     int num_sms = 148;
     int force_cfg = -1;  // fixed sweep configuration, -1: autotune
-    // autotuning: per (slot, stage, functor) sweep, one timed launch per
-    // configuration, then the fastest
+    // autotuning: per (slot, stage, functor) sweep, TUNE_ROUNDS timed
+    // launches per configuration, then the fastest by its best launch
+    static constexpr int TUNE_ROUNDS = 2;
     struct Tune {
         int best = -1, next = 0;
         double ms[NUM_FORCE_CFG] = {};
@@ -1741,10 +1742,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
         auto& t = ctx->tune[key];
         if (t.best >= 0) {
             A.cfg = t.best;
-        } else if (ctx->steps_done > 0 && !ctx->capturing && t.next < NUM_FORCE_CFG) {
-            // time this configuration once (the first step, with its cold
+        } else if (ctx->steps_done > 0 && !ctx->capturing && t.next < gc_ctx::TUNE_ROUNDS * NUM_FORCE_CFG) {
+            // time the configurations in turn (the first step, with its cold
             // sorts, is not timed)
-            A.cfg = t.next++;
+            A.cfg = t.next++ % NUM_FORCE_CFG;
             if (ctx->tune_rec.size() == ctx->tune_ev.size()) {
                 cudaEvent_t e0, e1;
                 CU(cudaEventCreate(&e0));
@@ -2131,8 +2132,9 @@ int collect_profile(gc_ctx* ctx) {
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, ctx->tune_ev[i].first, ctx->tune_ev[i].second));
         auto& t = ctx->tune[ctx->tune_rec[i].first];
-        t.ms[ctx->tune_rec[i].second] += ms;
-        if (t.next == NUM_FORCE_CFG && t.best < 0) {
+        double& m = t.ms[ctx->tune_rec[i].second];
+        m = m > 0.0 ? std::min(m, (double)ms) : (double)ms;
+        if (t.next == gc_ctx::TUNE_ROUNDS * NUM_FORCE_CFG && t.best < 0) {
             int b = 0;
             for (int c = 1; c < NUM_FORCE_CFG; ++c)
                 if (t.ms[c] < t.ms[b]) b = c;

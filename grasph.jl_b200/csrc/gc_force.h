@@ -12,15 +12,14 @@ constexpr int FORCE_TPB = 128;  // threads per block of the sweep
 constexpr int FORCE_BUF = 64;   // staged-neighbour column of the counting sweep (shared memory)
 
 // Launch configurations of the sweep: (min resident blocks, staged
-// neighbours per thread, pair-loop unroll, prefetch ring, chunk staging).
-// Chosen per (system, stage) by the tuner in gc_context.cu.
+// neighbours per thread, pair-loop unroll, chunk staging).  Chosen per
+// (system, stage) by the tuner in gc_context.cu.
 struct ForceCfg {
-    int minb, buf, unroll, pre;  // pre: prefetch ring for the FP32-compensated pairs
-    int stg;                     // > 0: k_sweep_stg with chunks of stg candidates (FP32-compensated)
+    int minb, buf, unroll;
+    int stg;  // > 0: k_sweep_stg with chunks of stg candidates (FP32-compensated records)
 };
 constexpr int NUM_FORCE_CFG = GC_NUM_SWEEP_CONFIGS;
-constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {
-    {4, 64, 1, 0, 0}, {6, 64, 1, 0, 0}, {4, 64, 1, 0, 96}, {6, 64, 1, 0, 96}};
+constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1, 0}, {6, 64, 1, 0}, {5, 64, 1, 96}, {6, 64, 1, 96}};
 constexpr int MAX_REFS = 8;     // interactions fused into one launch
 
 // system_b kinds as seen by a functor (src/PairwiseFunctors.jl dispatch)

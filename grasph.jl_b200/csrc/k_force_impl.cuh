@@ -338,7 +338,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
 
 template <int ND, int NS, int PFN, int KK>
 struct PhysF64 {
-    static constexpr int NQ = 0;  // no prefetch ring
+    static constexpr int NQ = 0;  // no staged copies (k_sweep only)
     struct Own {
         OwnState<ND> o;
         double sig[NS > 0 ? NS : 1];
@@ -442,6 +442,16 @@ __device__ __forceinline__ void kadd(float& s, float& c, float x) {
     c = (t - s) - y;
     s = t;
 }
+
+// kadd when `on`, else nothing (a select, not a branch)
+__device__ __forceinline__ void kadd_if(float& s, float& c, float x, bool on) {
+    const float y = x - c;
+    const float t = s + y;
+    const float cn = (t - s) - y;
+    s = on ? t : s;
+    c = on ? cn : c;
+}
+
 
 template <int ND>
 __device__ __forceinline__ double dot_exact(const double* a, const double* b) {
@@ -570,8 +580,8 @@ struct PhysF32 {
         return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcGlobal{r.bfp, j}, acc);
     }
 
-    // Where a neighbour's record comes from; read only after the pair passed
-    // the cutoff test, so it is not held in registers across the test.
+    // Where a neighbour's record comes from: global memory (k_sweep) or a
+    // staged shared-memory slot (k_sweep_stg).
     struct SrcGlobal {
         const float* pk;
         int64_t j;
@@ -592,8 +602,8 @@ struct PhysF32 {
         }
     };
 
-    // Prefetch of a neighbour's position and record into shared memory
-    // (16-byte asynchronous copies), chunk q of a thread at slot[q*BT].
+    // Copy of a neighbour's position and record into a shared-memory slot
+    // (16-byte asynchronous copies), chunk q at slot[q*BT]; pair_slot reads it.
     static constexpr int NQP = XD / 2, NQR = R / 4, NQ = NQP + NQR;
     static __device__ __forceinline__ void issue(const InterRef& r, int32_t j, float4* slot, int BT) {
         const float4* px = reinterpret_cast<const float4*>(r.bxp + (int64_t)j * XD);
@@ -627,8 +637,11 @@ struct PhysF32 {
 #pragma unroll
         for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], xj[d]);
         const double rr = dot_exact<ND>(dx, dx);
-        if (!(rr < G.cutoff_sq)) return 0;
+        // the exact test decides, without a branch, whether the pair's terms
+        // are added (the pair's arithmetic stays one straight-line block)
+        const bool in = rr < G.cutoff_sq;
         if (P2 == GC_PFN_COUNT) {
+            if (!in) return 0;
             acc.dv[0] += 1.f;
             acc.dr += 1.f;
             return 1;
@@ -691,15 +704,15 @@ struct PhysF32 {
                 sr[5] = 0.5f * (dv[1] * gx[2] + dv[2] * gx[1]);
             }
 #pragma unroll
-            for (int q2 = 0; q2 < NS; ++q2) kadd(acc.sr[q2], acc.csr[q2], sr[q2] * f);
+            for (int q2 = 0; q2 < NS; ++q2) kadd_if(acc.sr[q2], acc.csr[q2], sr[q2] * f, in);
             if (P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
-                kadd(acc.w[0], acc.cw[0], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f);
+                kadd_if(acc.w[0], acc.cw[0], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f, in);
                 if (ND == 3) {
-                    kadd(acc.w[1], acc.cw[1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f);
-                    kadd(acc.w[2], acc.cw[2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f);
+                    kadd_if(acc.w[1], acc.cw[1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f, in);
+                    kadd_if(acc.w[2], acc.cw[2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f, in);
                 }
             }
-            return 1;
+            return in ? 1 : 0;
         }
         // momentum + continuity (FluidPfn, CauchyFluidPfn)
         float dv[ND];
@@ -721,8 +734,8 @@ struct PhysF32 {
             const float rfj = (0.01f * ca) * ca * lj;
             const float s = -G.f_bmass * piv;
 #pragma unroll
-            for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], s * gx[d] + rfj * dxf[d]);
-            return 1;
+            for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d] + rfj * dxf[d], in);
+            return in ? 1 : 0;
         }
         const float mj = (self || dyn) ? ma : G.f_bmass;
         if (fluid_pfn<P2>()) {
@@ -738,7 +751,7 @@ struct PhysF32 {
             if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
             const float s = mj * (dh - piv);
 #pragma unroll
-            for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], s * gx[d]);
+            for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d], in);
         } else {
             // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
             float sj[NS > 0 ? NS : 1];
@@ -759,7 +772,7 @@ struct PhysF32 {
                         (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
             }
 #pragma unroll
-            for (int d = 0; d < ND; ++d) kadd(acc.dv[d], acc.cdv[d], mj * (hv[d] - piv * gx[d]));
+            for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], mj * (hv[d] - piv * gx[d]), in);
         }
         float tail = 0.f;
         if (P.has_delta) {
@@ -767,9 +780,9 @@ struct PhysF32 {
             const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
             tail = psi * irhoj;
         }
-        kadd(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail));
+        kadd_if(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail), in);
         (void)gi;
-        return 1;
+        return in ? 1 : 0;
     }
 };
 
@@ -789,29 +802,10 @@ struct PhysF32 {
 template <class Phys, bool COUNT_ONLY, int UNROLL, int PFN>
 __device__ __forceinline__ int flush_all(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                          const PfnInst& P, int64_t gi, int k, const typename Phys::Own& w,
-                                         double da, int nbuf, const int32_t* col, int BT, typename Phys::AccT& acc,
-                                         float4* ring) {
+                                         double da, int nbuf, const int32_t* col, int BT, typename Phys::AccT& acc) {
     constexpr int P2 = COUNT_ONLY ? GC_PFN_COUNT : PFN;
     int acc_n = 0;
     int t = 0;
-    if constexpr (Phys::NQ > 0 && !COUNT_ONLY) {
-        if (ring) {
-            // software pipeline: the next neighbour's position and record are
-            // copied into this thread's shared-memory ring while the current
-            // pair is evaluated
-            constexpr int NQ = Phys::NQ;
-            if (nbuf > 0) Phys::issue(r, col[0], ring, BT);
-            __pipeline_commit();
-            for (; t < nbuf; ++t) {
-                if (t + 1 < nbuf) Phys::issue(r, col[(t + 1) * BT], ring + ((t + 1) & 1) * NQ * BT, BT);
-                __pipeline_commit();
-                __pipeline_wait_prior(1);
-                acc_n += Phys::template pair_slot<P2>(A, r, G, P, gi, k, w, da, ring + (t & 1) * NQ * BT, BT, acc);
-            }
-            __pipeline_wait_prior(0);
-            return acc_n;
-        }
-    }
     if (UNROLL == 2) {
         for (; t + 1 < nbuf; t += 2) {
             const int32_t j0 = col[t * BT], j1 = col[(t + 1) * BT];
@@ -823,7 +817,7 @@ __device__ __forceinline__ int flush_all(const ForceArgs& A, const InterRef& r, 
     return acc_n;
 }
 
-template <class Phys, int ND, int PFN, bool COUNT_ONLY, int MINB, int BUF, int UNROLL, bool PRE = false>
+template <class Phys, int ND, int PFN, bool COUNT_ONLY, int MINB, int BUF, int UNROLL>
 __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     extern __shared__ int32_t sbuf[];
     const unsigned FULL = 0xffffffffu;
@@ -834,9 +828,6 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     // per-warp candidate coordinates, ND rows of 32 floats, after the columns
     // per warp: ND rows of 32 candidate coordinates, then ND doubles (lane 0's position)
     float* cand = reinterpret_cast<float*>(sbuf + BUF * FORCE_TPB) + (tid >> 5) * (ND * 34);
-    // per-thread prefetch ring (two slots of Phys::NQ 16-byte chunks), after the candidates
-    float4* ring = PRE ? reinterpret_cast<float4*>(sbuf + BUF * FORCE_TPB + (FORCE_TPB / 32) * ND * 34) + tid
-                       : nullptr;
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
@@ -933,7 +924,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                     for (int32_t ch = u0; ch < u1; ch += 32) {
                         if (__any_sync(FULL, nbuf > BUF - 32)) {
                             accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
-                                                                                 BT, acc, ring);
+                                                                                 BT, acc);
                             nbuf = 0;
                             __syncwarp();
                         }
@@ -985,7 +976,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         __syncwarp();
                     }
                 }
-                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc, ring);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
                 __syncwarp();
             } else if (active && ok) {
@@ -1001,12 +992,12 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         col[(nbuf++) * BT] = j;
                         if (nbuf == BUF) {
                             accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
-                                                                                 BT, acc, ring);
+                                                                                 BT, acc);
                             nbuf = 0;
                         }
                     }
                 }
-                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc, ring);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
             }
             __syncwarp();
@@ -1264,10 +1255,8 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
         kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
         return;
     }
-    constexpr bool PRE = cf.pre && Phys::NQ > 0;
-    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float) +
-                        (PRE ? (size_t)2 * Phys::NQ * FORCE_TPB * 16 : 0);
-    auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll, PRE>;
+    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float);
+    auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll>;
     if (smem > 48 * 1024) {
         // beyond the default dynamic shared-memory limit: opt in once per kernel
         static bool opted = false;
