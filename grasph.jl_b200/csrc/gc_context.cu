@@ -214,6 +214,11 @@ struct DInter {
     int64_t cells = 0;      // packed cells of the current grid
     int64_t grid_ver = -1;  // bumps at every rebuild
     int64_t csa_ver = -1;   // grid version cs_a was built for
+    // one-sided against a system_b whose positions do not change: its CSR
+    // stays current while the grid's geometry does, and a step's count and
+    // scan are skipped on the device when the geometry is unchanged
+    int* d_keep = nullptr;          // [0] cs is current for d_gi_prev, [1] this step's grid equals it
+    GridInst* d_gi_prev = nullptr;  // geometry cs was last counted on, per instance
 };
 
 // One captured step: valid for the buffer parities `pre` (cur of every slot,
@@ -973,6 +978,11 @@ int finalize(gc_ctx* ctx) {
             }
         }
         TRY(dalloc(ctx, &D.counts, (size_t)(D.ag >= 0 ? ctx->ghosts[D.ag].CAP : ctx->slots[D.a].N)));
+        if (!D.probe && D.ag < 0 && !D.two_sided && D.bslot >= 0 && D.btype != BT_SELF) {
+            TRY(dalloc(ctx, &D.d_keep, 2));
+            TRY(dalloc(ctx, &D.d_gi_prev, (size_t)ninst));
+            CU(cudaMemsetAsync(D.d_keep, 0, 2 * sizeof(int), ctx->stream));
+        }
         // writers
         bool writes = false;
         for (int s = 0; s < (int)D.pk.size(); ++s) writes |= D.pk[s] != GC_PFN_NONE;
@@ -1044,6 +1054,7 @@ int ensure_inter_cells(gc_ctx* ctx, DInter& D, int64_t cells) {
         TRY(dalloc(ctx, &D.cs, (size_t)cap));
         if (D.btype != BT_SELF) TRY(dalloc(ctx, &D.cs_a, (size_t)cap));
         D.cap_cells = cap;
+        if (D.d_keep) CU(cudaMemsetAsync(D.d_keep, 0, sizeof(int), ctx->stream));  // new buffer: nothing counted
     }
     return ensure_cells(ctx, cells);
 }
@@ -1231,9 +1242,20 @@ AParts a_parts(gc_ctx* ctx, const DInter& D) {
     return AParts{A.F(F_X), A.N, A.inst_of, nullptr};
 }
 
-int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
+// allow_keep: system_b's positions have not changed since its CSR was last
+// counted, so an unchanged geometry keeps the CSR (decided on the device).
+int build_grid(gc_ctx* ctx, DInter& D, int64_t cells, bool allow_keep = false) {
     TRY(ensure_inter_cells(ctx, D, cells));
     DSlot& A = ctx->slots[D.a];
+    const int* skip = nullptr;
+    if (D.d_keep) {
+        if (allow_keep) {
+            launch_grid_keep(D.d_gi, D.d_gi_prev, ninst(ctx), A.nd, D.d_keep, ctx->stream);
+            skip = D.d_keep + 1;
+        } else {
+            CU(cudaMemsetAsync(D.d_keep, 0, sizeof(int), ctx->stream));  // counted on a geometry not recorded
+        }
+    }
     const double* bx;
     const int32_t* binst;
     const int64_t* bcount = nullptr;
@@ -1250,8 +1272,9 @@ int build_grid(gc_ctx* ctx, DInter& D, int64_t cells) {
         binst = B.inst_of;
         bN = B.N;
     }
-    launch_grid_count(bx, bN, A.nd, binst, bcount, D.d_gi, ctx->hist, cells, ctx->d_err, ctx->d_incons, ctx->stream);
-    scan_exclusive_clear(ctx->hist, D.cs, cells, ctx->scan_tmp, ctx->stream);
+    launch_grid_count(bx, bN, A.nd, binst, bcount, D.d_gi, ctx->hist, cells, ctx->d_err, ctx->d_incons, ctx->stream,
+                      skip);
+    scan_exclusive_clear(ctx->hist, D.cs, cells, ctx->scan_tmp, ctx->stream, skip);
     if (D.two_sided) {
         const AParts ap = a_parts(ctx, D);
         launch_grid_count(ap.x, ap.N, A.nd, ap.inst_of, ap.count, D.d_gi, ctx->hist, cells, ctx->d_err,
@@ -1384,7 +1407,8 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     for (auto& D : ctx->inters) {
         if (D.probe) continue;
         if (D.btype == BT_GHOST || D.ag >= 0) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
-        TRY(build_grid(ctx, D, need[D.need_slot]));
+        const bool b_still = D.d_keep && !sort_mask[D.bslot] && !ctx->slots[D.bslot].xmoves();
+        TRY(build_grid(ctx, D, need[D.need_slot], b_still));
     }
     return GC_OK;
 }
@@ -2470,6 +2494,8 @@ int run_steps(gc_ctx* ctx, int nsteps) {
             ctx->resorts -= ran;
             ctx->graph_steps -= ran;
             ctx->rollbacks += 1;
+            for (auto& D : ctx->inters)  // a CSR counted inside the window may not have fitted
+                if (D.d_keep) CU(cudaMemsetAsync(D.d_keep, 0, sizeof(int), ctx->stream));
             e &= ~ERR_CAPACITY;
             CU(cudaMemcpyAsync(ctx->d_err, &e, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
             CU(cudaStreamSynchronize(ctx->stream));
@@ -2593,6 +2619,8 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaFree(D.cs);
         cudaFree(D.cs_a);
         cudaFree(D.counts);
+        cudaFree(D.d_keep);
+        cudaFree(D.d_gi_prev);
     }
     cudaFree(ctx->key);
     cudaFree(ctx->perm);

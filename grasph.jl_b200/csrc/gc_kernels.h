@@ -16,7 +16,9 @@ int64_t scan_tmp_elems(int64_t n);
 // clear_in: the last pass also zeroes in[0..n) (histograms left ready for
 // their next use, no separate memset).
 void scan_exclusive(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s);
-void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s);
+// skip: optional device flag; when set, the launches return at once.
+void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s,
+                          const int* skip = nullptr);
 
 // ---------------------------------------------------------- bounding box
 // Per-instance min/max of a slot's positions into inst[k].bbmin/bbmax.
@@ -73,10 +75,14 @@ struct GridPlanArgs {
 void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s);
 // The plans of n interactions (device array of arguments), one block each.
 void launch_grid_plan_all(const GridPlanArgs* d_args, int n, cudaStream_t s);
-// cell histogram of the particles of one slot on an interaction's grid.
+// cell histogram of the particles of one slot on an interaction's grid
+// (skip: optional device flag; when set, the launch returns at once).
 void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                        const GridInst* gi, int32_t* hist, int64_t cells_cap, int* err,
-                       unsigned long long* incons, cudaStream_t s);
+                       unsigned long long* incons, cudaStream_t s, const int* skip = nullptr);
+// state[1] = (every instance's grid equals prev) && state[0]; prev = grid;
+// state[0] = 1 (see k_grid_keep).
+void launch_grid_keep(const GridInst* gi, GridInst* prev, int ninst, int nd, int* state, cudaStream_t s);
 
 // ---------------------------------------------------------------- ghosts
 struct GhostGenArgs {

@@ -57,7 +57,9 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* total) {
     return base + x - v;
 }
 
-__global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int32_t* __restrict__ bsum) {
+__global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int32_t* __restrict__ bsum,
+                              const int* skip) {
+    if (skip && *skip) return;
     int64_t t0 = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
     int32_t s = 0;
 #pragma unroll
@@ -69,7 +71,8 @@ __global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int32_t
 }
 
 __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const int32_t* __restrict__ boff,
-                             int32_t* __restrict__ out, int32_t* clear) {
+                             int32_t* __restrict__ out, int32_t* clear, const int* skip) {
+    if (skip && *skip) return;
     int64_t t0 = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
     int32_t v[SCAN_I];
     int32_t s = 0;
@@ -103,7 +106,8 @@ int64_t scan_tmp_elems(int64_t n) {
 // tiles before it itself (at most SCAN_TILE values), so the scan of the tile
 // sums needs no launch of its own.
 __global__ void k_scan_apply_sums(const int32_t* __restrict__ in, int64_t n, const int32_t* __restrict__ bsum,
-                                  int32_t* __restrict__ out, int32_t* clear) {
+                                  int32_t* __restrict__ out, int32_t* clear, const int* skip) {
+    if (skip && *skip) return;
     __shared__ int32_t off;
     {
         int32_t s = 0;
@@ -136,33 +140,36 @@ __global__ void k_scan_apply_sums(const int32_t* __restrict__ in, int64_t n, con
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = off + total;
 }
 
-static void scan_impl(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, int32_t* clear, cudaStream_t s) {
+// skip: when non-null and *skip is set on the device, every launch returns
+// at once (the output is already current).
+static void scan_impl(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, int32_t* clear, cudaStream_t s,
+                      const int* skip) {
     int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nb > 1 && nb <= SCAN_TILE) {
-        k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, tmp);
-        k_scan_apply_sums<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, tmp, out, clear);
+        k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, tmp, skip);
+        k_scan_apply_sums<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, tmp, out, clear, skip);
         COUNTED(2);
         return;
     }
     if (nb <= 1) {
-        k_scan_apply<<<1, SCAN_T, 0, s>>>(in, n, nullptr, out, clear);
+        k_scan_apply<<<1, SCAN_T, 0, s>>>(in, n, nullptr, out, clear, skip);
         COUNTED(1);
         return;
     }
     int32_t* bsum = tmp;
     int32_t* boff = tmp + nb;
-    k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, bsum);
-    scan_impl(bsum, boff, nb, tmp + nb + nb + 1, nullptr, s);
-    k_scan_apply<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, boff, out, clear);
+    k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, bsum, skip);
+    scan_impl(bsum, boff, nb, tmp + nb + nb + 1, nullptr, s, skip);
+    k_scan_apply<<<(unsigned)nb, SCAN_T, 0, s>>>(in, n, boff, out, clear, skip);
     COUNTED(2);
 }
 
 void scan_exclusive(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s) {
-    scan_impl(in, out, n, tmp, nullptr, s);
+    scan_impl(in, out, n, tmp, nullptr, s, nullptr);
 }
 
-void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s) {
-    scan_impl(in, out, n, tmp, in, s);
+void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s, const int* skip) {
+    scan_impl(in, out, n, tmp, in, s, skip);
 }
 
 // ========================================================== bounding box
@@ -671,7 +678,8 @@ __device__ __forceinline__ bool cell_flat(const double* __restrict__ x, int64_t 
 
 __global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                              const int64_t* count, const GridInst* __restrict__ gi, int32_t* __restrict__ hist,
-                             int64_t cells_cap, int* err, unsigned long long* incons) {
+                             int64_t cells_cap, int* err, unsigned long long* incons, const int* skip) {
+    if (skip && *skip) return;
     int64_t n = count ? *count : N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         int k = inst_of[g];
@@ -696,9 +704,39 @@ __global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, co
 
 void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                        const GridInst* gi, int32_t* hist, int64_t cells_cap, int* err, unsigned long long* incons,
-                       cudaStream_t s) {
+                       cudaStream_t s, const int* skip) {
     if (N <= 0) return;
-    k_grid_count<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, gi, hist, cells_cap, err, incons);
+    k_grid_count<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, gi, hist, cells_cap, err, incons, skip);
+    COUNTED(1);
+}
+
+// Does every instance's grid of an interaction equal the one its CSR was
+// last counted on?  state[0]: that CSR is current for prev; state[1]
+// (output): equal, so the count and scan of this step may be skipped.  prev
+// takes this step's geometry.
+__global__ void k_grid_keep(const GridInst* __restrict__ gi, GridInst* __restrict__ prev, int ninst, int nd,
+                            int* state) {
+    __shared__ int same;
+    if (threadIdx.x == 0) same = state[0];
+    __syncthreads();
+    for (int k = threadIdx.x; k < ninst; k += blockDim.x) {
+        const GridInst& a = gi[k];
+        const GridInst& b = prev[k];
+        bool eq = a.cellbase == b.cellbase && a.ncells == b.ncells;
+        for (int d = 0; d < nd; ++d)
+            eq = eq && a.ng[d] == b.ng[d] && __double_as_longlong(a.ming[d]) == __double_as_longlong(b.ming[d]);
+        if (!eq) atomicAnd(&same, 0);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < ninst; k += blockDim.x) prev[k] = gi[k];
+    if (threadIdx.x == 0) {
+        state[1] = same;
+        state[0] = 1;
+    }
+}
+
+void launch_grid_keep(const GridInst* gi, GridInst* prev, int ninst, int nd, int* state, cudaStream_t s) {
+    k_grid_keep<<<1, 128, 0, s>>>(gi, prev, ninst, nd, state);
     COUNTED(1);
 }
 

@@ -95,3 +95,50 @@ def test_autotune_chooses_every_sweep():
     # two stages of one system: both sweeps tuned, then graph replays
     assert sum(st["sweep_cfg_chosen"]) == 2
     assert st["graph_steps"] > 0
+
+
+def _passing_block():
+    """A fluid block sliding (no gravity) along a short static wall and past
+    its end: the union box of the fluid-wall grid, hence its geometry, changes
+    every few steps while the wall's particles never move."""
+    dx, c = 0.02, 1.0
+    h = 1.2 * dx
+    n = 6
+    fluid = G.FluidParticleSystem("fluid", n * n, 2, 1000.0 * dx * dx, c, state_updater=G.TaitEOSUpdater(1000.0))
+    ii, jj = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    fluid.x[:, 0] = (ii.ravel() + 0.5) * dx
+    fluid.x[:, 1] = (jj.ravel() + 0.5) * dx
+    fluid.v[:] = [1.0, 0.0]
+    fluid.rho[:] = 1000.0
+    xs = np.arange(-0.1, 0.2 + 1e-9, dx)
+    wall = G.BasicParticleSystem("wall", 3 * len(xs), 2, 1000.0 * dx * dx, c)
+    wall.x[:] = [(x, -(l + 0.5) * dx) for l in range(3) for x in xs]
+    wall.rho[:] = 1000.0
+    k = G.CubicSplineKernel(h, ndims=2)
+    pfn = G.FluidPfn(0.1, 0.0, h)
+    si = G.SystemInteraction(k, pfn, fluid, G.DynamicBoundarySystem(wall, (0.0, 1.0), (0.0, 0.0), 3.0))
+    return G.LeapFrogTimeIntegrator([fluid, wall], [si]), 0.2
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_still_wall_grid_follows_geometry_changes(graphs):
+    """The CSR over a wall that never moves is kept on the device while its
+    grid's geometry is unchanged and recounted when it changes: the device
+    stays with the oracle while the block slides past the wall's end."""
+    out = []
+    for be in ("cuda", "oracle"):
+        lf, cfl = _passing_block()
+        s = G.Session([lf], backend=make_backend(be))
+        if be == "cuda":
+            s.backend.set_graphs(graphs, 8)
+        s.push()
+        s.step(40, cfl)
+        s.pull()
+        out.append(lf)
+    fg, fc = out[0].systems[0], out[1].systems[0]
+    ig, ic = np.argsort(fg.id), np.argsort(fc.id)
+    assert fc.x[:, 0].max() > 0.3  # the block left the wall's end behind
+    for name in ("x", "v", "rho", "dvdt", "drhodt"):
+        a, b = getattr(fg, name)[ig], getattr(fc, name)[ic]
+        scale = max(np.abs(b).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-10 * scale, name
