@@ -786,6 +786,113 @@ struct PhysF32 {
     }
 };
 
+// ------------------------------------------------ shared sweep pieces
+// Per (warp, interaction) set-up of both sweeps.  Returns false when the
+// warp has nothing to do with this interaction: system_b's box is out of
+// reach of every lane (the box test has a 0.1% margin, so no pair is lost)
+// or the instance's grid did not fit its buffer (flagged, nothing read).
+// Otherwise c holds each lane's cell coordinates (ok: inside the grid, with
+// a flagged error when not), c0/c1 lane 0's first two, and coop whether all
+// active lanes share lane 0's grid column.
+template <int ND>
+__device__ __forceinline__ bool ref_cells(const ForceArgs& A, const InterRef& r, const GridInst& G, int k,
+                                          const double* ox, bool active, int lane, int32_t gi, int32_t* c,
+                                          bool& ok, int32_t& c0, int32_t& c1, bool& coop) {
+    const unsigned FULL = 0xffffffffu;
+    if (r.bbox) {
+        const SysInst& B = r.bbox[k];
+        bool near = B.n > 0;
+        const double m = 1.001 * G.cell;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) near = near && ox[d] >= B.bbmin[d] - m && ox[d] <= B.bbmax[d] + m;
+        if (!__any_sync(FULL, active && near)) {
+            if (active && r.counts) r.counts[gi] = 0;
+            return false;
+        }
+    }
+    if (G.cellbase + G.ncells > r.cs_cells) {
+        if (lane == 0) atomicOr(A.err, ERR_CAPACITY);
+        if (active && r.counts) r.counts[gi] = 0;
+        return false;
+    }
+    // cell coordinates (a grid has < 2^31 cells, so they fit int32)
+    ok = true;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        int64_t cd;
+        if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &cd) || cd < 1 || cd >= G.ng[d] - 1) {
+            ok = false;
+            cd = 1;
+        }
+        c[d] = (int32_t)cd;
+    }
+    if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
+    c0 = __shfl_sync(FULL, c[0], 0);
+    c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
+    const bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
+    coop = __all_sync(FULL, !active || same);
+    return true;
+}
+
+// The warp's range [zlo, zhi] of last-dimension cells over its active lanes.
+template <int ND>
+__device__ __forceinline__ void warp_zrange(const int32_t* c, bool active, int32_t& zlo, int32_t& zhi) {
+    const unsigned FULL = 0xffffffffu;
+    zlo = active ? c[ND - 1] : INT32_MAX;
+    zhi = active ? c[ND - 1] : INT32_MIN;
+#pragma unroll
+    for (int o2 = 16; o2 > 0; o2 >>= 1) {
+        const int32_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
+        zlo = a2 < zlo ? a2 : zlo;
+        zhi = b2 > zhi ? b2 : zhi;
+    }
+}
+
+// Conservative FP32 prefilter of a batch of mb <= 32 candidates against this
+// lane (coordinates relative to lane 0; rows of the batch `stride` floats
+// apart, entries past mb far away): bit t set when candidate t may be within
+// the cutoff.  Two candidates per packed FP32x2 instruction.
+template <int ND>
+__device__ __forceinline__ unsigned batch_hits(const float* cb, int stride, int mb, const float* xi, float cut_f) {
+    const float2 neg1 = make_float2(-1.0f, -1.0f);
+    unsigned hits = 0;
+    for (int t0 = 0; t0 < mb; t0 += 8) {
+        unsigned h8 = 0;
+#pragma unroll
+        for (int t = 0; t < 8; t += 2) {
+            float2 rr;
+            {
+                const float2 xj = *reinterpret_cast<const float2*>(cb + t0 + t);
+                const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[0], xi[0]));
+                rr = __fmul2_rn(dd, dd);
+            }
+#pragma unroll
+            for (int d = 1; d < ND; ++d) {
+                const float2 xj = *reinterpret_cast<const float2*>(cb + d * stride + t0 + t);
+                const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[d], xi[d]));
+                rr = __ffma2_rn(dd, dd, rr);
+            }
+            if (rr.x < cut_f) h8 |= 1u << t;
+            if (rr.y < cut_f) h8 |= 2u << t;
+        }
+        hits |= h8 << t0;
+    }
+    return hits;
+}
+
+// This lane's own strip range [lo, hi) and the self pair as a mask over the
+// batch of 32 candidates starting at index jb.
+__device__ __forceinline__ unsigned own_allow(int32_t lo, int32_t hi, int32_t jb, bool self, int32_t gi) {
+    const int32_t tlo = lo - jb, thi = hi - jb;
+    unsigned allow = tlo <= 0 ? 0xffffffffu : (tlo >= 32 ? 0u : 0xffffffffu << tlo);
+    allow &= thi >= 32 ? 0xffffffffu : (thi <= 0 ? 0u : 0xffffffffu >> (32 - thi));
+    if (self) {
+        const int32_t ts = gi - jb;
+        if (ts >= 0 && ts < 32) allow &= ~(1u << ts);
+    }
+    return allow;
+}
+
 // ---------------------------------------------------------------- kernel
 // One warp owns one group: up to 32 consecutive (sorted) system_a particles
 // of one grid column (all cell coordinates but the last equal).  For each
@@ -845,56 +952,18 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
             const InterRef& r = A.ref[ri];
             const GridInst& G = r.gi[k];
             const PfnInst& P = r.pi[k];
-            if (r.bbox) {
-                // No system_b particle can be within the cutoff of any lane:
-                // skip (the box test has a 0.1% margin, so no pair is lost).
-                const SysInst& B = r.bbox[k];
-                bool near = B.n > 0;
-                const double m = 1.001 * G.cell;
-#pragma unroll
-                for (int d = 0; d < ND; ++d) near = near && ox[d] >= B.bbmin[d] - m && ox[d] <= B.bbmax[d] + m;
-                if (!__any_sync(FULL, active && near)) {
-                    if (active && r.counts) r.counts[gi] = 0;
-                    continue;
-                }
-            }
-            if (G.cellbase + G.ncells > r.cs_cells) {
-                // this instance's grid did not fit its buffer: flag it, read nothing
-                if (lane == 0) atomicOr(A.err, ERR_CAPACITY);
-                if (active && r.counts) r.counts[gi] = 0;
-                continue;
-            }
-            // cell coordinates (a grid has < 2^31 cells, so they fit int32)
-            int32_t c[ND];
-            bool ok = true;
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                int64_t cd;
-                if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &cd) || cd < 1 || cd >= G.ng[d] - 1) {
-                    ok = false;
-                    cd = 1;
-                }
-                c[d] = (int32_t)cd;
-            }
-            if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
+            int32_t c[ND], c0, c1;
+            bool ok, coop;
+            if (!ref_cells<ND>(A, r, G, k, ox, active, lane, gi, c, ok, c0, c1, coop)) continue;
             const double da = r.btype == BT_DYNAMIC ? Phys::plane_da(w, G) : 0.0;
             const int64_t Nb = r.bN;
             const bool self = r.btype == BT_SELF;
             int nbuf = 0;
             int32_t accepted = 0;
-            const int32_t c0 = __shfl_sync(FULL, c[0], 0);
-            const int32_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
-            const bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
-            const bool coop = __all_sync(FULL, !active || same);
             if (coop) {
                 constexpr int L = ND - 1;  // last dimension
-                int32_t zlo = active ? c[L] : INT32_MAX, zhi = active ? c[L] : INT32_MIN;
-#pragma unroll
-                for (int o2 = 16; o2 > 0; o2 >>= 1) {
-                    int32_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
-                    zlo = a2 < zlo ? a2 : zlo;
-                    zhi = b2 > zhi ? b2 : zhi;
-                }
+                int32_t zlo, zhi;
+                warp_zrange<ND>(c, active, zlo, zhi);
                 // Conservative FP32 prefilter in coordinates relative to lane 0:
                 // |rel| spans a few cells, so single-precision rounding moves r²
                 // by < 1e-5 relative; the 1e-3 margin keeps every true pair.
@@ -911,7 +980,6 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
 #pragma unroll
                 for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
-                const float2 neg1 = make_float2(-1.0f, -1.0f);
                 const int64_t ngl = G.ng[L];
                 const int nstrips = ND == 2 ? 3 : 9;
                 for (int sidx = 0; sidx < nstrips; ++sidx) {
@@ -935,39 +1003,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         for (int d = 0; d < ND; ++d)
                             cand[d * 32 + lane] = jl < u1 ? (float)(r.bx[d * Nb + jl] - xref[d]) : 1e30f;
                         __syncwarp();
-                        // this lane's own strip range and the self pair, as a mask
-                        // over the batch's 32 positions
-                        const int32_t tlo = lo - ch, thi = hi - ch;
-                        unsigned allow = tlo <= 0 ? 0xffffffffu : (tlo >= 32 ? 0u : 0xffffffffu << tlo);
-                        allow &= thi >= 32 ? 0xffffffffu : (thi <= 0 ? 0u : 0xffffffffu >> (32 - thi));
-                        if (self) {
-                            const int32_t ts = gi - ch;
-                            if (ts >= 0 && ts < 32) allow &= ~(1u << ts);
-                        }
                         const int m = u1 - ch < 32 ? (int)(u1 - ch) : 32;
-                        unsigned hits = 0;
-                        for (int t0 = 0; t0 < m; t0 += 8) {
-                            unsigned h8 = 0;
-#pragma unroll
-                            for (int t = 0; t < 8; t += 2) {
-                                float2 rr;
-                                {
-                                    const float2 xj = *reinterpret_cast<const float2*>(cand + t0 + t);
-                                    const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[0], xi[0]));
-                                    rr = __fmul2_rn(dd, dd);
-                                }
-#pragma unroll
-                                for (int d = 1; d < ND; ++d) {
-                                    const float2 xj = *reinterpret_cast<const float2*>(cand + d * 32 + t0 + t);
-                                    const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[d], xi[d]));
-                                    rr = __ffma2_rn(dd, dd, rr);
-                                }
-                                if (rr.x < cut_f) h8 |= 1u << t;
-                                if (rr.y < cut_f) h8 |= 2u << t;
-                            }
-                            hits |= h8 << t0;
-                        }
-                        hits &= allow;
+                        unsigned hits = batch_hits<ND>(cand, 32, m, xi, cut_f) & own_allow(lo, hi, ch, self, gi);
                         while (hits) {
                             const int t = __ffs(hits) - 1;
                             hits &= hits - 1;
@@ -1057,53 +1094,17 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
             const InterRef& r = A.ref[ri];
             const GridInst& G = r.gi[k];
             const PfnInst& P = r.pi[k];
-            if (r.bbox) {
-                // no system_b particle within the cutoff of any lane (0.1% margin)
-                const SysInst& B = r.bbox[k];
-                bool near = B.n > 0;
-                const double m = 1.001 * G.cell;
-#pragma unroll
-                for (int d = 0; d < ND; ++d) near = near && ox[d] >= B.bbmin[d] - m && ox[d] <= B.bbmax[d] + m;
-                if (!__any_sync(FULL, active && near)) {
-                    if (active && r.counts) r.counts[gi] = 0;
-                    continue;
-                }
-            }
-            if (G.cellbase + G.ncells > r.cs_cells) {
-                // this instance's grid did not fit its buffer: flag it, read nothing
-                if (lane == 0) atomicOr(A.err, ERR_CAPACITY);
-                if (active && r.counts) r.counts[gi] = 0;
-                continue;
-            }
-            int32_t c[ND];
-            bool ok = true;
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                int64_t cd;
-                if (!floor_i64(__dsub_rn(ox[d], G.ming[d]) / G.cell, &cd) || cd < 1 || cd >= G.ng[d] - 1) {
-                    ok = false;
-                    cd = 1;
-                }
-                c[d] = (int32_t)cd;
-            }
-            if (active && !ok) atomicOr(A.err, ERR_CAPACITY);
+            int32_t c[ND], c0, c1;
+            bool ok, coop;
+            if (!ref_cells<ND>(A, r, G, k, ox, active, lane, gi, c, ok, c0, c1, coop)) continue;
             const double da = r.btype == BT_DYNAMIC ? Phys::plane_da(w, G) : 0.0;
             const bool self = r.btype == BT_SELF;
             int32_t accepted = 0;
-            const int32_t c0 = __shfl_sync(FULL, c[0], 0);
-            const int32_t c1 = ND == 3 ? __shfl_sync(FULL, c[1], 0) : 0;
-            const bool same = ok && c[0] == c0 && (ND == 2 || c[1] == c1);
-            const bool coop = __all_sync(FULL, !active || same);
             const int nstrips = ND == 2 ? 3 : 9;
             if (coop) {
                 constexpr int L = ND - 1;
-                int32_t zlo = active ? c[L] : INT32_MAX, zhi = active ? c[L] : INT32_MIN;
-#pragma unroll
-                for (int o2 = 16; o2 > 0; o2 >>= 1) {
-                    int32_t a2 = __shfl_xor_sync(FULL, zlo, o2), b2 = __shfl_xor_sync(FULL, zhi, o2);
-                    zlo = a2 < zlo ? a2 : zlo;
-                    zhi = b2 > zhi ? b2 : zhi;
-                }
+                int32_t zlo, zhi;
+                warp_zrange<ND>(c, active, zlo, zhi);
                 if (lane == 0) {
 #pragma unroll
                     for (int d = 0; d < ND; ++d) xref[d] = ox[d];
@@ -1115,7 +1116,6 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
 #pragma unroll
                 for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
-                const float2 neg1 = make_float2(-1.0f, -1.0f);
                 const int64_t ngl = G.ng[L];
                 auto strip_base = [&](int s2) -> int64_t {
                     int64_t colflat;
@@ -1163,39 +1163,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                             msk[b] = 0u;
                             if (32 * b < n) {
                                 const int mb = n - 32 * b < 32 ? n - 32 * b : 32;
-                                const float* cb = cand + 32 * b;
-                                unsigned hits = 0;
-                                for (int t0 = 0; t0 < mb; t0 += 8) {
-                                    unsigned h8 = 0;
-#pragma unroll
-                                    for (int t = 0; t < 8; t += 2) {
-                                        float2 rr;
-                                        {
-                                            const float2 xj = *reinterpret_cast<const float2*>(cb + t0 + t);
-                                            const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[0], xi[0]));
-                                            rr = __fmul2_rn(dd, dd);
-                                        }
-#pragma unroll
-                                        for (int d = 1; d < ND; ++d) {
-                                            const float2 xj = *reinterpret_cast<const float2*>(cb + d * CH + t0 + t);
-                                            const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[d], xi[d]));
-                                            rr = __ffma2_rn(dd, dd, rr);
-                                        }
-                                        if (rr.x < cut_f) h8 |= 1u << t;
-                                        if (rr.y < cut_f) h8 |= 2u << t;
-                                    }
-                                    hits |= h8 << t0;
-                                }
-                                // this lane's own strip range and the self pair
-                                const int32_t jb = ch + 32 * b;
-                                const int32_t tlo = lo - jb, thi = hi - jb;
-                                unsigned allow = tlo <= 0 ? 0xffffffffu : (tlo >= 32 ? 0u : 0xffffffffu << tlo);
-                                allow &= thi >= 32 ? 0xffffffffu : (thi <= 0 ? 0u : 0xffffffffu >> (32 - thi));
-                                if (self) {
-                                    const int32_t ts = gi - jb;
-                                    if (ts >= 0 && ts < 32) allow &= ~(1u << ts);
-                                }
-                                msk[b] = hits & allow;
+                                msk[b] = batch_hits<ND>(cand + 32 * b, CH, mb, xi, cut_f) &
+                                         own_allow(lo, hi, ch + 32 * b, self, gi);
                             }
                         }
                         // this lane's accepted candidates, from the staged copies
@@ -1253,19 +1222,19 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
             }
         }
         kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
-        return;
-    }
-    const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float);
-    auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll>;
-    if (smem > 48 * 1024) {
-        // beyond the default dynamic shared-memory limit: opt in once per kernel
-        static bool opted = false;
-        if (!opted) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            opted = true;
+    } else {
+        const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float);
+        auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll>;
+        if (smem > 48 * 1024) {
+            // beyond the default dynamic shared-memory limit: opt in once per kernel
+            static bool opted = false;
+            if (!opted) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                opted = true;
+            }
         }
+        kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
     }
-    kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
 }
 
 template <class Phys, int ND, int PFN>
