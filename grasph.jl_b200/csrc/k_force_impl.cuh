@@ -577,7 +577,8 @@ struct PhysF32 {
                                                int32_t j, AccT& acc) {
         double xj[ND];
         pos_load(r, j, xj);
-        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcGlobal{r.bfp, j}, acc);
+        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcGlobal{r.bfp, j}, make_float2(A.a_cf[k], A.a_massf[k]),
+                             acc);
     }
 
     // Where a neighbour's record comes from: global memory (k_sweep) or a
@@ -616,9 +617,10 @@ struct PhysF32 {
         }
     }
     template <int P2>
+    // cam: system_a's (FP32) sound speed and mass of this instance
     static __device__ __forceinline__ int pair_slot(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                     const PfnInst& P, int64_t gi, int k, const Own& w, double da,
-                                                    const float4* slot, int BT, AccT& acc) {
+                                                    const float4* slot, int BT, const float2* cam, AccT& acc) {
         double xj[ND];
 #pragma unroll
         for (int q = 0; q < NQP; ++q) {
@@ -626,13 +628,13 @@ struct PhysF32 {
             if (2 * q < ND) xj[2 * q] = t.x;
             if (2 * q + 1 < ND) xj[2 * q + 1] = t.y;
         }
-        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcSlot{slot, BT}, acc);
+        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcSlot{slot, BT}, *cam, acc);
     }
 
     template <int P2, class Src>
     static __device__ __forceinline__ int pair_data(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                     const PfnInst& P, int64_t gi, int k, const Own& w, double da,
-                                                    const double* xj, const Src& src, AccT& acc) {
+                                                    const double* xj, const Src& src, float2 cam, AccT& acc) {
         double dx[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], xj[d]);
@@ -657,7 +659,7 @@ struct PhysF32 {
         float gx[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) gx[d] = gc * dxf[d];
-        const float ca = A.a_cf[k], ma = A.a_massf[k];
+        const float ca = cam.x, ma = cam.y;
 
         float vj[ND], rhoj, auxj, irhoj;
         float fj[R];
@@ -1048,11 +1050,23 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
 // ------------------------------------------------- staged FP32 sweep
 // Shared memory of one warp of k_sweep_stg: the staged copies of a chunk of
 // CH candidates ([NQ][CH] 16-byte chunks: FP64 position, then FP32 record),
-// lane 0's position (the origin of the prefilter), and the candidates'
-// FP32 coordinates relative to it ([ND][CH]).
+// lane 0's position (the origin of the prefilter), the candidates' FP32
+// coordinates relative to it ([ND][CH]), and copies of the interaction's
+// grid and functor parameters for this warp's instance.
+constexpr int STG_GI_BYTES = ((int)sizeof(GridInst) + 15) / 16 * 16;
+constexpr int STG_PI_BYTES = ((int)sizeof(PfnInst) + 15) / 16 * 16;
 template <int ND, int NQ, int CH>
 __host__ __device__ constexpr int stg_warp_bytes() {
-    return NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16;
+    return NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16 + STG_GI_BYTES + STG_PI_BYTES + 16;
+}
+
+// Copy of a parameter block into a warp's shared memory, 4 bytes per lane.
+template <class T>
+__device__ __forceinline__ void warp_copy(T* dst, const T& src, int lane) {
+    static_assert(sizeof(T) % 4 == 0, "4-byte words");
+    const int* s = reinterpret_cast<const int*>(&src);
+    int* d = reinterpret_cast<int*>(dst);
+    for (int i = lane; i < (int)(sizeof(T) / 4); i += 32) d[i] = s[i];
 }
 
 // The FP32-compensated sweep with chunk staging.  The walk is k_sweep's (one
@@ -1077,6 +1091,12 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
     float4* slots = reinterpret_cast<float4*>(wbase);
     double* xref = reinterpret_cast<double*>(wbase + NQ * CH * 16);
     float* cand = reinterpret_cast<float*>(wbase + NQ * CH * 16 + 32);
+    // the pair loop reads the interaction's parameters from these copies
+    // (loop-invariant loads the register budget would otherwise re-issue
+    // from global memory for every pair)
+    GridInst* gsm = reinterpret_cast<GridInst*>(wbase + NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16);
+    PfnInst* psm = reinterpret_cast<PfnInst*>(reinterpret_cast<char*>(gsm) + STG_GI_BYTES);
+    float2* camsm = reinterpret_cast<float2*>(reinterpret_cast<char*>(psm) + STG_PI_BYTES);
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
@@ -1101,6 +1121,12 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
             const bool self = r.btype == BT_SELF;
             int32_t accepted = 0;
             const int nstrips = ND == 2 ? 3 : 9;
+            warp_copy(gsm, G, lane);
+            warp_copy(psm, P, lane);
+            if (lane == 0) *camsm = make_float2(A.a_cf[k], A.a_massf[k]);
+            __syncwarp();
+            const GridInst& Gs = *gsm;
+            const PfnInst& Ps = *psm;
             if (coop) {
                 constexpr int L = ND - 1;
                 int32_t zlo, zhi;
@@ -1177,7 +1203,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                                     msk[b] &= msk[b] - 1;
                                 }
                             if (t < 0) break;
-                            accepted += Phys::template pair_slot<PFN>(A, r, G, P, gi, k, w, da, slots + t, CH, acc);
+                            accepted += Phys::template pair_slot<PFN>(A, r, Gs, Ps, gi, k, w, da, slots + t, CH, camsm, acc);
                         }
                         __syncwarp();  // every lane is done with the chunk before the next one lands
                     }
