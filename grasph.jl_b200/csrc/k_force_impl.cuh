@@ -895,6 +895,30 @@ __device__ __forceinline__ unsigned own_allow(int32_t lo, int32_t hi, int32_t jb
     return allow;
 }
 
+// Per-warp copies of an interaction's grid and functor parameters (the pair
+// loops read these: loop-invariant values the register budget would
+// otherwise re-load from global memory for every pair).
+constexpr int SWEEP_GI_BYTES = ((int)sizeof(GridInst) + 15) / 16 * 16;
+constexpr int SWEEP_PI_BYTES = ((int)sizeof(PfnInst) + 15) / 16 * 16;
+constexpr int SWEEP_PARAM_BYTES = SWEEP_GI_BYTES + SWEEP_PI_BYTES;
+
+// Copy of a parameter block into a warp's shared memory, 4 bytes per lane.
+template <class T>
+__device__ __forceinline__ void warp_copy(T* dst, const T& src, int lane) {
+    static_assert(sizeof(T) % 4 == 0, "4-byte words");
+    const int* s = reinterpret_cast<const int*>(&src);
+    int* d = reinterpret_cast<int*>(dst);
+    for (int i = lane; i < (int)(sizeof(T) / 4); i += 32) d[i] = s[i];
+}
+
+// Shared memory of one block of k_sweep: the staged-neighbour columns, the
+// per-warp candidate coordinates (ND rows of 32, then lane 0's position) and
+// the per-warp parameter copies.
+template <int ND>
+__host__ __device__ constexpr int sweep_smem_bytes(int buf) {
+    return (buf * FORCE_TPB * 4 + (FORCE_TPB / 32) * ND * 34 * 4 + 15) / 16 * 16 + (FORCE_TPB / 32) * SWEEP_PARAM_BYTES;
+}
+
 // ---------------------------------------------------------------- kernel
 // One warp owns one group: up to 32 consecutive (sorted) system_a particles
 // of one grid column (all cell coordinates but the last equal).  For each
@@ -937,6 +961,10 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
     // per-warp candidate coordinates, ND rows of 32 floats, after the columns
     // per warp: ND rows of 32 candidate coordinates, then ND doubles (lane 0's position)
     float* cand = reinterpret_cast<float*>(sbuf + BUF * FORCE_TPB) + (tid >> 5) * (ND * 34);
+    char* pbase = reinterpret_cast<char*>(sbuf) + (BUF * FORCE_TPB * 4 + (FORCE_TPB / 32) * ND * 34 * 4 + 15) / 16 * 16 +
+                  (tid >> 5) * SWEEP_PARAM_BYTES;
+    GridInst* gsm = reinterpret_cast<GridInst*>(pbase);
+    PfnInst* psm = reinterpret_cast<PfnInst*>(pbase + SWEEP_GI_BYTES);
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
@@ -958,6 +986,11 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
             bool ok, coop;
             if (!ref_cells<ND>(A, r, G, k, ox, active, lane, gi, c, ok, c0, c1, coop)) continue;
             const double da = r.btype == BT_DYNAMIC ? Phys::plane_da(w, G) : 0.0;
+            warp_copy(gsm, G, lane);
+            warp_copy(psm, P, lane);
+            __syncwarp();
+            const GridInst& Gs = *gsm;
+            const PfnInst& Ps = *psm;
             const int64_t Nb = r.bN;
             const bool self = r.btype == BT_SELF;
             int nbuf = 0;
@@ -993,7 +1026,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                     const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
                     for (int32_t ch = u0; ch < u1; ch += 32) {
                         if (__any_sync(FULL, nbuf > BUF - 32)) {
-                            accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
+                            accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col,
                                                                                  BT, acc);
                             nbuf = 0;
                             __syncwarp();
@@ -1015,7 +1048,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         __syncwarp();
                     }
                 }
-                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
                 __syncwarp();
             } else if (active && ok) {
@@ -1030,13 +1063,13 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         if (self && j == gi) continue;
                         col[(nbuf++) * BT] = j;
                         if (nbuf == BUF) {
-                            accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col,
+                            accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col,
                                                                                  BT, acc);
                             nbuf = 0;
                         }
                     }
                 }
-                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, G, P, gi, k, w, da, nbuf, col, BT, acc);
+                accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
             }
             __syncwarp();
@@ -1053,21 +1086,13 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
 // lane 0's position (the origin of the prefilter), the candidates' FP32
 // coordinates relative to it ([ND][CH]), and copies of the interaction's
 // grid and functor parameters for this warp's instance.
-constexpr int STG_GI_BYTES = ((int)sizeof(GridInst) + 15) / 16 * 16;
-constexpr int STG_PI_BYTES = ((int)sizeof(PfnInst) + 15) / 16 * 16;
+constexpr int STG_GI_BYTES = SWEEP_GI_BYTES;
+constexpr int STG_PI_BYTES = SWEEP_PI_BYTES;
 template <int ND, int NQ, int CH>
 __host__ __device__ constexpr int stg_warp_bytes() {
     return NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16 + STG_GI_BYTES + STG_PI_BYTES + 16;
 }
 
-// Copy of a parameter block into a warp's shared memory, 4 bytes per lane.
-template <class T>
-__device__ __forceinline__ void warp_copy(T* dst, const T& src, int lane) {
-    static_assert(sizeof(T) % 4 == 0, "4-byte words");
-    const int* s = reinterpret_cast<const int*>(&src);
-    int* d = reinterpret_cast<int*>(dst);
-    for (int i = lane; i < (int)(sizeof(T) / 4); i += 32) d[i] = s[i];
-}
 
 // The FP32-compensated sweep with chunk staging.  The walk is k_sweep's (one
 // warp per group of one grid column, the union of its lanes' candidate
@@ -1249,7 +1274,7 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
         }
         kern<<<(int)blocks, FORCE_TPB, smem, s>>>(A);
     } else {
-        const size_t smem = (size_t)cf.buf * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float);
+        const size_t smem = (size_t)sweep_smem_bytes<ND>(cf.buf);
         auto kern = k_sweep<Phys, ND, PFN, false, cf.minb, cf.buf, cf.unroll>;
         if (smem > 48 * 1024) {
             // beyond the default dynamic shared-memory limit: opt in once per kernel
@@ -1286,7 +1311,7 @@ static void launch_t(const ForceArgs& A, bool count_only, cudaStream_t s) {
             int64_t blocks = (A.aN * 32 + FORCE_TPB - 1) / FORCE_TPB;
             if (blocks > (int64_t)A.num_sms * 16) blocks = (int64_t)A.num_sms * 16;
             if (blocks < 1) blocks = 1;
-            size_t smem = (size_t)FORCE_BUF * FORCE_TPB * sizeof(int32_t) + (FORCE_TPB / 32) * ND * 34 * sizeof(float);
+            const size_t smem = (size_t)sweep_smem_bytes<ND>(FORCE_BUF);
             k_sweep<P64, ND, PFN, true, 4, FORCE_BUF, 1><<<(int)blocks, FORCE_TPB, smem, s>>>(A);
         } else {
             launch_cfg<P64, ND, PFN>(A, s);
