@@ -18,6 +18,7 @@
 // The FP64 policy relies on -fmad=false; the FP32 policy uses explicit
 // __dmul_rn/__dadd_rn for the exact acceptance test.
 #pragma once
+#include <type_traits>
 #include <cstdio>
 #include <cuda_pipeline.h>
 
@@ -616,8 +617,9 @@ struct PhysF32 {
             for (int q = 0; q < NQR; ++q) __pipeline_memcpy_async(&slot[(NQP + q) * BT], &pr[q], 16);
         }
     }
-    template <int P2>
-    // cam: system_a's (FP32) sound speed and mass of this instance
+    // cam: system_a's (FP32) sound speed and mass of this instance; BTK: the
+    // system_b kind when known at compile time (-1: r.btype)
+    template <int P2, int BTK = -1>
     static __device__ __forceinline__ int pair_slot(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                     const PfnInst& P, int64_t gi, int k, const Own& w, double da,
                                                     const float4* slot, int BT, const float2* cam, AccT& acc) {
@@ -628,13 +630,14 @@ struct PhysF32 {
             if (2 * q < ND) xj[2 * q] = t.x;
             if (2 * q + 1 < ND) xj[2 * q + 1] = t.y;
         }
-        return pair_data<P2>(A, r, G, P, gi, k, w, da, xj, SrcSlot{slot, BT}, *cam, acc);
+        return pair_data<P2, BTK>(A, r, G, P, gi, k, w, da, xj, SrcSlot{slot, BT}, *cam, acc);
     }
 
-    template <int P2, class Src>
+    template <int P2, int BTK = -1, class Src>
     static __device__ __forceinline__ int pair_data(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                     const PfnInst& P, int64_t gi, int k, const Own& w, double da,
                                                     const double* xj, const Src& src, float2 cam, AccT& acc) {
+        const int bt = BTK >= 0 ? BTK : r.btype;
         double dx[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], xj[d]);
@@ -663,7 +666,7 @@ struct PhysF32 {
 
         float vj[ND], rhoj, auxj, irhoj;
         float fj[R];
-        if (r.btype == BT_DYNAMIC) {
+        if (bt == BT_DYNAMIC) {
             // src/PairwiseFunctors.jl:53,111,222,334: mirrored velocity, own density
             float db = (float)da;
 #pragma unroll
@@ -686,7 +689,7 @@ struct PhysF32 {
             float dv[ND];
 #pragma unroll
             for (int d = 0; d < ND; ++d) dv[d] = vj[d] - w.v[d];
-            const float f = r.btype == BT_DYNAMIC ? w.aux : auxj;  // mass / rho
+            const float f = bt == BT_DYNAMIC ? w.aux : auxj;  // mass / rho
             float sr[NS > 0 ? NS : 1];
             if (ND == 2) {
                 sr[0] = dv[0] * gx[0];
@@ -720,9 +723,9 @@ struct PhysF32 {
         float dv[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) dv[d] = w.v[d] - vj[d];
-        const bool self = r.btype == BT_SELF, dyn = r.btype == BT_DYNAMIC;
+        const bool self = bt == BT_SELF, dyn = bt == BT_DYNAMIC;
         const bool two = P2 == PFN_FLUID2 && P.two;  // multiphase / fluid-solid variant only
-        const float cb = ((P2 == GC_PFN_CAUCHY_FLUID && r.btype == BT_GHOST) || two) ? G.f_bc : ca;
+        const float cb = ((P2 == GC_PFN_CAUCHY_FLUID && bt == BT_GHOST) || two) ? G.f_bc : ca;
         float piv = 0.f;
         const float vr = dotf<ND>(dxf, dv);
         if (vr < 0.f) {
@@ -730,7 +733,7 @@ struct PhysF32 {
             const float mc = 0.5f * (ca + cb);
             piv = (P.f_beta * muv - P.f_alpha * mc) * muv * 2.f * w.irho * irhoj;
         }
-        if (r.btype == BT_STATIC) {
+        if (bt == BT_STATIC) {
             const float x = G.f_ljcut * rinv, x2 = x * x, x6 = x2 * x2 * x2;
             const float lj = rf < G.f_ljcut ? (x6 * x6 - x6) / rrf : 0.f;
             const float rfj = (0.01f * ca) * ca * lj;
@@ -1181,58 +1184,65 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                     su0 = r.cs[b2 + zlo - 1];
                     su1 = r.cs[b2 + zhi + 2];
                 }
-                for (int sidx = 0; sidx < nstrips; ++sidx) {
-                    const int32_t u0 = __shfl_sync(FULL, su0, sidx), u1 = __shfl_sync(FULL, su1, sidx);
-                    if (u0 >= u1) continue;  // warp-uniform
-                    const int64_t base = strip_base(sidx);
-                    // this lane's own strip range [cs[z-1], cs[z+2])
-                    const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
-                    for (int32_t ch = u0; ch < u1; ch += CH) {
-                        const int n = u1 - ch < CH ? (int)(u1 - ch) : CH;
-                        for (int i = lane; i < n; i += 32) Phys::issue(r, ch + i, slots + i, CH);
-                        __pipeline_commit();
-                        __pipeline_wait_prior(0);
-                        // this lane's staged positions -> relative FP32 coordinates
+                // the strips, with the pair code specialised for a self
+                // interaction (the dominant kind) and generic otherwise
+                auto strips = [&](auto btk) {
+                    constexpr int BTK = decltype(btk)::value;
+                    for (int sidx = 0; sidx < nstrips; ++sidx) {
+                        const int32_t u0 = __shfl_sync(FULL, su0, sidx), u1 = __shfl_sync(FULL, su1, sidx);
+                        if (u0 >= u1) continue;  // warp-uniform
+                        const int64_t base = strip_base(sidx);
+                        // this lane's own strip range [cs[z-1], cs[z+2])
+                        const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
+                        for (int32_t ch = u0; ch < u1; ch += CH) {
+                            const int n = u1 - ch < CH ? (int)(u1 - ch) : CH;
+                            for (int i = lane; i < n; i += 32) Phys::issue(r, ch + i, slots + i, CH);
+                            __pipeline_commit();
+                            __pipeline_wait_prior(0);
+                            // this lane's staged positions -> relative FP32 coordinates
 #pragma unroll
-                        for (int i0 = 0; i0 < CH; i0 += 32) {
-                            const int i = i0 + lane;
+                            for (int i0 = 0; i0 < CH; i0 += 32) {
+                                const int i = i0 + lane;
 #pragma unroll
-                            for (int d = 0; d < ND; ++d) {
-                                float v = 1e30f;  // beyond the chunk: far away
-                                if (i < n) {
-                                    const double2 t = *reinterpret_cast<const double2*>(&slots[(d >> 1) * CH + i]);
-                                    v = (float)(((d & 1) ? t.y : t.x) - xref[d]);
+                                for (int d = 0; d < ND; ++d) {
+                                    float v = 1e30f;  // beyond the chunk: far away
+                                    if (i < n) {
+                                        const double2 t = *reinterpret_cast<const double2*>(&slots[(d >> 1) * CH + i]);
+                                        v = (float)(((d & 1) ? t.y : t.x) - xref[d]);
+                                    }
+                                    cand[d * CH + i] = v;
                                 }
-                                cand[d * CH + i] = v;
                             }
-                        }
-                        __syncwarp();
-                        // accepted candidates of the chunk, one mask per batch of 32
-                        unsigned msk[NB];
+                            __syncwarp();
+                            // accepted candidates of the chunk, one mask per batch of 32
+                            unsigned msk[NB];
 #pragma unroll
-                        for (int b = 0; b < NB; ++b) {
-                            msk[b] = 0u;
-                            if (32 * b < n) {
-                                const int mb = n - 32 * b < 32 ? n - 32 * b : 32;
-                                msk[b] = batch_hits<ND>(cand + 32 * b, CH, mb, xi, cut_f) &
-                                         own_allow(lo, hi, ch + 32 * b, self, gi);
-                            }
-                        }
-                        // this lane's accepted candidates, from the staged copies
-                        while (true) {
-                            int t = -1;
-#pragma unroll
-                            for (int b = 0; b < NB; ++b)
-                                if (t < 0 && msk[b]) {
-                                    t = 32 * b + __ffs(msk[b]) - 1;
-                                    msk[b] &= msk[b] - 1;
+                            for (int b = 0; b < NB; ++b) {
+                                msk[b] = 0u;
+                                if (32 * b < n) {
+                                    const int mb = n - 32 * b < 32 ? n - 32 * b : 32;
+                                    msk[b] = batch_hits<ND>(cand + 32 * b, CH, mb, xi, cut_f) &
+                                             own_allow(lo, hi, ch + 32 * b, self, gi);
                                 }
-                            if (t < 0) break;
-                            accepted += Phys::template pair_slot<PFN>(A, r, Gs, Ps, gi, k, w, da, slots + t, CH, camsm, acc);
+                            }
+                            // this lane's accepted candidates, from the staged copies
+                            while (true) {
+                                int t = -1;
+#pragma unroll
+                                for (int b = 0; b < NB; ++b)
+                                    if (t < 0 && msk[b]) {
+                                        t = 32 * b + __ffs(msk[b]) - 1;
+                                        msk[b] &= msk[b] - 1;
+                                    }
+                                if (t < 0) break;
+                                accepted += Phys::template pair_slot<PFN, BTK>(A, r, Gs, Ps, gi, k, w, da, slots + t, CH, camsm, acc);
+                            }
+                            __syncwarp();  // every lane is done with the chunk before the next one lands
                         }
-                        __syncwarp();  // every lane is done with the chunk before the next one lands
                     }
-                }
+                };
+                if (self) strips(std::integral_constant<int, BT_SELF>{});
+                else strips(std::integral_constant<int, -1>{});
             } else if (active && ok) {
                 // rare: lanes disagree on the column in this grid; walk own strips
                 for (int sidx = 0; sidx < nstrips; ++sidx) {
