@@ -685,7 +685,7 @@ struct PhysF32 {
             auxj = fj[ND + 1];
             irhoj = fj[ND + 2];
         }
-        if (P2 == GC_PFN_STRAIN_RATE || P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
+        if constexpr (P2 == GC_PFN_STRAIN_RATE || P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
             float dv[ND];
 #pragma unroll
             for (int d = 0; d < ND; ++d) dv[d] = vj[d] - w.v[d];
@@ -718,76 +718,77 @@ struct PhysF32 {
                 }
             }
             return in ? 1 : 0;
-        }
-        // momentum + continuity (FluidPfn, CauchyFluidPfn)
-        float dv[ND];
+        } else {
+            // momentum + continuity (FluidPfn, CauchyFluidPfn)
+            float dv[ND];
 #pragma unroll
-        for (int d = 0; d < ND; ++d) dv[d] = w.v[d] - vj[d];
-        const bool self = bt == BT_SELF, dyn = bt == BT_DYNAMIC;
-        const bool two = P2 == PFN_FLUID2 && P.two;  // multiphase / fluid-solid variant only
-        const float cb = ((P2 == GC_PFN_CAUCHY_FLUID && bt == BT_GHOST) || two) ? G.f_bc : ca;
-        float piv = 0.f;
-        const float vr = dotf<ND>(dxf, dv);
-        if (vr < 0.f) {
-            const float muv = __fdividef(P.f_h * vr, rrf + P.f_h2eps);
-            const float mc = 0.5f * (ca + cb);
-            piv = (P.f_beta * muv - P.f_alpha * mc) * muv * 2.f * w.irho * irhoj;
-        }
-        if (bt == BT_STATIC) {
-            const float x = G.f_ljcut * rinv, x2 = x * x, x6 = x2 * x2 * x2;
-            const float lj = rf < G.f_ljcut ? (x6 * x6 - x6) / rrf : 0.f;
-            const float rfj = (0.01f * ca) * ca * lj;
-            const float s = -G.f_bmass * piv;
+            for (int d = 0; d < ND; ++d) dv[d] = w.v[d] - vj[d];
+            const bool self = bt == BT_SELF, dyn = bt == BT_DYNAMIC;
+            const bool two = P2 == PFN_FLUID2 && P.two;  // multiphase / fluid-solid variant only
+            const float cb = ((P2 == GC_PFN_CAUCHY_FLUID && bt == BT_GHOST) || two) ? G.f_bc : ca;
+            float piv = 0.f;
+            const float vr = dotf<ND>(dxf, dv);
+            if (vr < 0.f) {
+                const float muv = __fdividef(P.f_h * vr, rrf + P.f_h2eps);
+                const float mc = 0.5f * (ca + cb);
+                piv = (P.f_beta * muv - P.f_alpha * mc) * muv * 2.f * w.irho * irhoj;
+            }
+            if (bt == BT_STATIC) {
+                const float x = G.f_ljcut * rinv, x2 = x * x, x6 = x2 * x2 * x2;
+                const float lj = rf < G.f_ljcut ? (x6 * x6 - x6) / rrf : 0.f;
+                const float rfj = (0.01f * ca) * ca * lj;
+                const float s = -G.f_bmass * piv;
 #pragma unroll
-            for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d] + rfj * dxf[d], in);
+                for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d] + rfj * dxf[d], in);
+                return in ? 1 : 0;
+            }
+            const float mj = (self || dyn) ? ma : G.f_bmass;
+            if (fluid_pfn<P2>()) {
+                float dh;
+                if (two && P.fs) {  // the fluid's pressure p = (p/ρ²)·ρ² on both sides
+                    if (G.side_b) dh = -(auxj + (auxj * rhoj * rhoj) * w.irho * w.irho);
+                    else dh = -(w.aux + (w.aux * w.rho * w.rho) * irhoj * irhoj);
+                } else {
+                    dh = -(w.aux + auxj);
+                }
+                // artificial surface tension ε·(−(|p_i| + |p_j|)/(ρ_i ρ_j)), with
+                // |p| = |p/ρ²|·ρ² from the record
+                if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
+                const float s = mj * (dh - piv);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d], in);
+            } else {
+                // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
+                float sj[NS > 0 ? NS : 1];
+#pragma unroll
+                for (int q2 = 0; q2 < NS; ++q2) sj[q2] = dyn ? w.sig[q2] : fj[ND + 3 + q2];
+                const float ci = w.aux, cj = auxj;
+                float hv[ND];
+                if (ND == 2) {
+                    constexpr int XY = NS == 3 ? 2 : 3;
+                    hv[0] = (w.sig[0] * gx[0] + w.sig[XY] * gx[1]) * ci + (sj[0] * gx[0] + sj[XY] * gx[1]) * cj;
+                    hv[1] = (w.sig[XY] * gx[0] + w.sig[1] * gx[1]) * ci + (sj[XY] * gx[0] + sj[1] * gx[1]) * cj;
+                } else {
+                    hv[0] = (w.sig[0] * gx[0] + w.sig[3] * gx[1] + w.sig[4] * gx[2]) * ci +
+                            (sj[0] * gx[0] + sj[3] * gx[1] + sj[4] * gx[2]) * cj;
+                    hv[1] = (w.sig[3] * gx[0] + w.sig[1] * gx[1] + w.sig[5] * gx[2]) * ci +
+                            (sj[3] * gx[0] + sj[1] * gx[1] + sj[5] * gx[2]) * cj;
+                    hv[2] = (w.sig[4] * gx[0] + w.sig[5] * gx[1] + w.sig[2] * gx[2]) * ci +
+                            (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
+                }
+#pragma unroll
+                for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], mj * (hv[d] - piv * gx[d]), in);
+            }
+            float tail = 0.f;
+            if (P.has_delta) {
+                const float cd = two ? 0.5f * (ca + cb) : ca;
+                const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
+                tail = psi * irhoj;
+            }
+            kadd_if(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail), in);
+            (void)gi;
             return in ? 1 : 0;
         }
-        const float mj = (self || dyn) ? ma : G.f_bmass;
-        if (fluid_pfn<P2>()) {
-            float dh;
-            if (two && P.fs) {  // the fluid's pressure p = (p/ρ²)·ρ² on both sides
-                if (G.side_b) dh = -(auxj + (auxj * rhoj * rhoj) * w.irho * w.irho);
-                else dh = -(w.aux + (w.aux * w.rho * w.rho) * irhoj * irhoj);
-            } else {
-                dh = -(w.aux + auxj);
-            }
-            // artificial surface tension ε·(−(|p_i| + |p_j|)/(ρ_i ρ_j)), with
-            // |p| = |p/ρ²|·ρ² from the record
-            if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
-            const float s = mj * (dh - piv);
-#pragma unroll
-            for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d], in);
-        } else {
-            // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
-            float sj[NS > 0 ? NS : 1];
-#pragma unroll
-            for (int q2 = 0; q2 < NS; ++q2) sj[q2] = dyn ? w.sig[q2] : fj[ND + 3 + q2];
-            const float ci = w.aux, cj = auxj;
-            float hv[ND];
-            if (ND == 2) {
-                constexpr int XY = NS == 3 ? 2 : 3;
-                hv[0] = (w.sig[0] * gx[0] + w.sig[XY] * gx[1]) * ci + (sj[0] * gx[0] + sj[XY] * gx[1]) * cj;
-                hv[1] = (w.sig[XY] * gx[0] + w.sig[1] * gx[1]) * ci + (sj[XY] * gx[0] + sj[1] * gx[1]) * cj;
-            } else {
-                hv[0] = (w.sig[0] * gx[0] + w.sig[3] * gx[1] + w.sig[4] * gx[2]) * ci +
-                        (sj[0] * gx[0] + sj[3] * gx[1] + sj[4] * gx[2]) * cj;
-                hv[1] = (w.sig[3] * gx[0] + w.sig[1] * gx[1] + w.sig[5] * gx[2]) * ci +
-                        (sj[3] * gx[0] + sj[1] * gx[1] + sj[5] * gx[2]) * cj;
-                hv[2] = (w.sig[4] * gx[0] + w.sig[5] * gx[1] + w.sig[2] * gx[2]) * ci +
-                        (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
-            }
-#pragma unroll
-            for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], mj * (hv[d] - piv * gx[d]), in);
-        }
-        float tail = 0.f;
-        if (P.has_delta) {
-            const float cd = two ? 0.5f * (ca + cb) : ca;
-            const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
-            tail = psi * irhoj;
-        }
-        kadd_if(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail), in);
-        (void)gi;
-        return in ? 1 : 0;
     }
 };
 
