@@ -210,3 +210,22 @@ def test_trapdoor_graph_steps_bit_identical(moving):
     for ve, vg in zip(le.virtual_systems, lg.virtual_systems):
         assert np.array_equal(ve.w_sum, vg.w_sum)
     assert np.array_equal(le.probes[0].stress, lg.probes[0].stress)
+
+
+def test_trapdoor_script_size_on_the_oracle():
+    """The script's sizes (264 x 100 soil, 10-layer bottom and trapdoor, wall
+    ghosts, five probes) through two steps and a measurement on the oracle."""
+    lf, meta = scenarios.trapdoor(geostatic=True)
+    s = G.Session([lf], backend=make_backend("oracle"))
+    s.push()
+    s.step(2, meta["cfl"])
+    s.measure_probes()
+    s.pull()
+    soil = lf.systems[0]
+    assert np.all(np.isfinite(soil.x)) and np.all(np.isfinite(soil.stress))
+    bottom, door = lf.virtual_systems
+    assert (bottom.w_sum > 0).sum() > 0 and (door.w_sum > 0).sum() > 0
+    probe = lf.probes[0]
+    # geostatic σ_yy at the soil's base, 5 m of soil at 1600 kg/m³
+    assert np.all(probe.stress[:, 1] < 0.0)
+    assert np.all(np.abs(probe.stress[:, 1]) < 1600.0 * 9.81 * 5.0 * 1.1)
