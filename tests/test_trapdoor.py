@@ -229,3 +229,13 @@ def test_trapdoor_script_size_on_the_oracle():
     # geostatic σ_yy at the soil's base, 5 m of soil at 1600 kg/m³
     assert np.all(probe.stress[:, 1] < 0.0)
     assert np.all(np.abs(probe.stress[:, 1]) < 1600.0 * 9.81 * 5.0 * 1.1)
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+def test_ghost_system_a_takes_no_velocity_adjustment(be):
+    real, ghost, ge, src, virt, si, lf, h = _ghost_pair()
+    it = G.SystemInteraction(G.CubicSplineKernel(h, ndims=2), G.InterpolateFieldFn("v"), ghost, virt,
+                             velocity_adjust_pairwise_fn=G.XSPHPfn(0.5))
+    lf2 = G.LeapFrogTimeIntegrator([real], [it], ghosts=(ge,), virtual_systems=(virt,))
+    with pytest.raises(Exception):
+        G.Session([lf2], backend=make_backend(be))
