@@ -588,6 +588,29 @@ class Session:
     def stats(self):
         return self.backend.stats()
 
+    # -- snapshots and restarts (grasph_b200.snapshot: write_h5 / read_h5!'s layout)
+    def save(self, path, inst=0):
+        """_maybe_save! (src/TimeIntegration.jl:520-549) of one instance: its
+        state downloaded and written to `path` with the step count."""
+        from .snapshot import write_snapshot
+        m = self._m(inst)
+        download_instance(self.backend, m)
+        write_snapshot(m.systems, path, step=self.stats()["steps_done"],
+                       probes=[pr for pr in m.probes if pr.mirror_target is None])
+
+    def load(self, path, inst=0):
+        """_load_restart! (src/Driver.jl:79-96) of one instance: `path` read
+        into its systems (and free probes' positions) and uploaded; returns
+        the saved step."""
+        from .snapshot import read_snapshot
+        m = self._m(inst)
+        free = [pr for pr in m.probes if pr.mirror_target is None]
+        step = read_snapshot(m.systems, path, probes=free)
+        upload_instance(self.backend, m)
+        for pr in free:
+            self.backend.upload(m.inst, m.h(pr), C.GC_FIELD_X, pr.x)
+        return step
+
     # -- per-phase hooks (instance 0 unless given)
     def _m(self, inst):
         return self.maps[inst]

@@ -1,0 +1,80 @@
+"""Snapshots and restarts: write_h5 / read_h5! (src/Particles.jl:699-787),
+_maybe_save! (src/TimeIntegration.jl:520-549) and _load_restart!
+(src/Driver.jl:79-96), with the groups, attributes and datasets of the
+reference's files in a NumPy container (no HDF5 library here).
+
+A run that stops, saves and restarts in a fresh session from the file must
+continue exactly as the uninterrupted run; read_h5!'s checks of n and ndims
+are restated."""
+import numpy as np
+import pytest
+
+import grasph_b200 as G
+from grasph_b200 import scenarios
+from grasph_b200.snapshot import read_snapshot, write_snapshot
+from gc_helpers import BACKENDS, make_backend
+
+
+def _fields(lf):
+    out = {}
+    for ps in list(lf.systems) + [v.source for v in getattr(lf, "virtual_systems", ())]:
+        for name, _ in ps.particle_fields():
+            out[(ps.name, name)] = np.array(getattr(ps, name), copy=True)
+    return out
+
+
+def _restart_case(build, be, tmp_path, n1=4, n2=5):
+    lf, meta = build()
+    s = G.Session([lf], backend=make_backend(be))
+    s.push()
+    s.step(n1, meta["cfl"])
+    path = tmp_path / "snap.npz"
+    s.save(path)
+    s.step(n2, meta["cfl"])
+    s.pull()
+    straight = _fields(lf)
+    lf2, _ = build()
+    s2 = G.Session([lf2], backend=make_backend(be))
+    step = s2.load(path)
+    assert step == n1
+    s2.step(n2, meta["cfl"])
+    s2.pull()
+    return straight, _fields(lf2)
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+def test_restart_continues_the_run_dambreak(be, tmp_path):
+    build = lambda: scenarios.dambreak_2d(nx=12, ny=24, dx=0.05, tank=(1.5, 2.0))
+    a, b = _restart_case(build, be, tmp_path)
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+def test_restart_continues_the_run_virtual_walls(be, tmp_path):
+    build = lambda: scenarios.ep_column_virtual(dx=0.004, geostatic=True, bottom_v=(0.0, -0.05))
+    a, b = _restart_case(build, be, tmp_path)
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
+
+
+def test_snapshot_layout_and_checks(tmp_path):
+    ps = G.FluidParticleSystem("fluid", 3, 2, 0.5, 10.0)
+    ps.x[:] = [[0.0, 0.0], [1.0, 0.0], [2.0, 0.5]]
+    ps.rho[:] = [1000.0, 1001.0, 1002.0]
+    path = tmp_path / "s.npz"
+    write_snapshot([ps], path, step=7)
+    with np.load(path) as f:
+        assert int(f["fluid/@n"]) == 3 and int(f["fluid/@ndims"]) == 2
+        assert float(f["fluid/@mass"]) == 0.5 and float(f["fluid/@c"]) == 10.0
+        np.testing.assert_array_equal(f["fluid/x"], ps.x)
+        assert int(f["@step"]) == 7
+    back = G.FluidParticleSystem("fluid", 3, 2, 0.5, 10.0)
+    assert read_snapshot([back], path) == 7
+    np.testing.assert_array_equal(back.rho, ps.rho)
+    wrong_n = G.FluidParticleSystem("fluid", 4, 2, 0.5, 10.0)
+    with pytest.raises(G.ArgumentError):
+        read_snapshot([wrong_n], path)
+    wrong_nd = G.FluidParticleSystem("fluid", 3, 3, 0.5, 10.0)
+    with pytest.raises(G.ArgumentError):
+        read_snapshot([wrong_nd], path)
