@@ -12,6 +12,7 @@ module GrasphCUDA
 
 using Grasph
 using StaticArrays
+using HDF5
 
 const LIB = get(ENV, "GRASPH_CUDA_LIB", joinpath(@__DIR__, "..", "libgrasph_cuda.so"))
 
@@ -98,7 +99,18 @@ function set_updaters!(ctx, inst, handle, updaters)
 end
 
 fields_of(ps) = [f for f in (:x, :v, :rho, :dvdt, :drhodt, :p, :stress, :strain_rate, :vorticity,
-                               :strain, :strain_p) if hasfield(typeof(ps), f)]
+                               :strain, :strain_p, :id) if hasfield(typeof(ps), f)]
+
+# The systems held on the device: the integrator's, then the virtual systems'
+# sources (sorted, moved and filled on the device like the others).
+function device_systems(lf)
+    out = Any[ps for ps in lf.systems]
+    for vps in lf.virtual_systems
+        src = getfield(vps, :source)
+        any(s -> s === src, out) || push!(out, src)
+    end
+    return out
+end
 
 # integrator kind of the C ABI (GC_INTEGRATOR_LEAPFROG / GC_INTEGRATOR_RK4)
 integ_kind(::LeapFrogTimeIntegrator) = Cint(0)
@@ -314,15 +326,39 @@ function measure_probes!(cl::CudaLeapFrog)
 end
 
 function upload!(cl::CudaLeapFrog)
-    for ps in cl.lf.systems, f in fields_of(ps)
+    for ps in device_systems(cl.lf), f in fields_of(ps)
         field_io!(cl, ps, f, true)
     end
 end
 
 function download!(cl::CudaLeapFrog)
-    for ps in cl.lf.systems, f in fields_of(ps)
+    for ps in device_systems(cl.lf), f in fields_of(ps)
         field_io!(cl, ps, f, false)
     end
+end
+
+# _maybe_save!'s file (src/TimeIntegration.jl:520-549) from the downloaded
+# state: step and sim_time attributes, one group per system, virtual system
+# and probe written by Grasph's own write_h5.  Ghosts are regenerated on the
+# device every step and are not downloaded, so they have no group here.
+function save_h5(cl::CudaLeapFrog, output_prefix, global_step::Int, width::Int, dt)
+    path = "$(output_prefix)_$(lpad(global_step, width, '0')).h5"
+    d = dirname(path)
+    !isempty(d) && mkpath(d)
+    h5open(path, "w") do f
+        HDF5.attrs(f)["step"] = global_step
+        HDF5.attrs(f)["sim_time"] = Float64(global_step * dt)
+        for ps in cl.lf.systems
+            Grasph.write_h5(ps, create_group(f, ps.name))
+        end
+        for vps in cl.lf.virtual_systems
+            Grasph.write_h5(vps, create_group(f, vps.name))
+        end
+        for probe in cl.lf.probes
+            Grasph.write_h5(probe, create_group(f, probe.name))
+        end
+    end
+    return path
 end
 
 """
@@ -336,7 +372,10 @@ own `print_summary`/`write_h5` run.
 """
 function Grasph.time_integrate!(cl::CudaLeapFrog, num_timesteps::Int, print_interval_step::Int,
                                 save_interval_step::Int, CFL::Real, output_prefix;
-                                step_offset::Int=0, kw...)
+                                step_offset::Int=0, output_width=nothing, kw...)
+    T = typeof(cl.lf.c)
+    dt = T(CFL) * cl.lf.h / cl.lf.c
+    width = output_width === nothing ? ndigits(step_offset + num_timesteps) : output_width
     upload!(cl)
     done = 0
     while done < num_timesteps
@@ -352,9 +391,11 @@ function Grasph.time_integrate!(cl::CudaLeapFrog, num_timesteps::Int, print_inte
             download!(cl)
             foreach(print_summary, cl.lf.systems)
         end
-        # probes are measured at save cadence, as _maybe_save! does
-        if output_prefix !== nothing && !isempty(cl.lf.probes) && g % save_interval_step == 0
-            measure_probes!(cl)
+        # _maybe_save!: probes measured, then the snapshot file
+        if output_prefix !== nothing && g % save_interval_step == 0
+            isempty(cl.lf.probes) || measure_probes!(cl)
+            download!(cl)
+            save_h5(cl, output_prefix, g, width, dt)
         end
     end
     download!(cl)
