@@ -78,3 +78,30 @@ def test_snapshot_layout_and_checks(tmp_path):
     wrong_nd = G.FluidParticleSystem("fluid", 3, 3, 0.5, 10.0)
     with pytest.raises(G.ArgumentError):
         read_snapshot([wrong_nd], path)
+
+
+def test_restart_with_moving_probes_on_the_oracle(tmp_path):
+    """Free probes moving with the trapdoor keep their positions across a
+    restart; the measurement after it matches the uninterrupted run's."""
+    def build():
+        return scenarios.trapdoor(nx=48, ny=20, ntd_x=12, n_layers=4, moving=True, geostatic=True)
+    lf, meta = build()
+    s = G.Session([lf], backend=make_backend("oracle"))
+    s.push()
+    s.step(3, meta["cfl"])
+    path = tmp_path / "td.npz"
+    s.save(path)
+    s.step(3, meta["cfl"])
+    s.measure_probes()
+    s.pull()
+    lf2, _ = build()
+    s2 = G.Session([lf2], backend=make_backend("oracle"))
+    assert s2.load(path) == 3
+    s2.step(3, meta["cfl"])
+    s2.measure_probes()
+    s2.pull()
+    p1, p2 = lf.probes[0], lf2.probes[0]
+    assert np.array_equal(p1.x, p2.x) and np.array_equal(p1.stress, p2.stress)
+    a, b = _fields(lf), _fields(lf2)
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
