@@ -19,7 +19,7 @@ import numpy as np
 
 from .model import ArgumentError
 
-__all__ = ["write_snapshot", "read_snapshot"]
+__all__ = ["write_snapshot", "read_snapshot", "write_h5", "read_h5", "system_from_h5"]
 
 
 def _systems_of(items):
@@ -34,18 +34,65 @@ def _systems_of(items):
     return out
 
 
+def _put_group(arrays, ps, prefix):
+    """_write_to_group! (src/Particles.jl:720-734) under key prefix `prefix`."""
+    arrays[f"{prefix}@n"] = np.int64(ps.n)
+    arrays[f"{prefix}@ndims"] = np.int64(ps.ndims)
+    arrays[f"{prefix}@mass"] = np.float64(ps.mass)
+    arrays[f"{prefix}@c"] = np.float64(ps.c)
+    for name, _ in ps.particle_fields():
+        arrays[f"{prefix}{name}"] = np.asarray(getattr(ps, name))
+
+
+def _get_group(f, ps, prefix):
+    """_read_from_group! (src/Particles.jl:761-787): n and ndims checked,
+    the arrays present in both read, mass and c left as they are."""
+    _check_group(f, prefix, ps.n, ps.ndims)
+    for name, _ in ps.particle_fields():
+        key = f"{prefix}{name}"
+        if key in f:
+            getattr(ps, name)[...] = f[key]
+
+
+def write_h5(ps, path):
+    """write_h5(ps, path) (src/Particles.jl:711): one system at the file's
+    root."""
+    arrays = {}
+    _put_group(arrays, ps, "")
+    with open(path, "wb") as f:
+        np.savez(f, **arrays)
+
+
+def read_h5(ps, path):
+    """read_h5!(ps, path) (src/Particles.jl:749): the file's root group into
+    `ps` (its name need not match); returns `ps`."""
+    with np.load(path) as f:
+        _get_group(f, ps, "")
+    return ps
+
+
+def system_from_h5(cls, path, name, **kw):
+    """The reference's path constructors (`FluidParticleSystem(path, name;
+    kw...)` and the like): a new system of type `cls` sized and
+    parameterised (n, ndims, mass, c, stress width) from the file's root
+    group, its arrays read back."""
+    with np.load(path) as f:
+        n, nd = int(f["@n"]), int(f["@ndims"])
+        mass, c = float(f["@mass"]), float(f["@c"])
+        if getattr(cls, "has_stress", False):
+            ps = cls(name, n, nd, int(f["stress"].shape[1]), mass, c, **kw)
+        else:
+            ps = cls(name, n, nd, mass, c, **kw)
+        _get_group(f, ps, "")
+    return ps
+
+
 def write_snapshot(systems, path, step=None, probes=()):
     """Write every field of `systems` (and the positions and ids of
-    `probes`) to `path`, one group per system as `write_h5` lays it out."""
+    `probes`) to `path`, one group per system as `_maybe_save!` lays it out."""
     arrays = {}
     for ps in _systems_of(systems):
-        g = ps.name
-        arrays[f"{g}/@n"] = np.int64(ps.n)
-        arrays[f"{g}/@ndims"] = np.int64(ps.ndims)
-        arrays[f"{g}/@mass"] = np.float64(ps.mass)
-        arrays[f"{g}/@c"] = np.float64(ps.c)
-        for name, _ in ps.particle_fields():
-            arrays[f"{g}/{name}"] = np.asarray(getattr(ps, name))
+        _put_group(arrays, ps, f"{ps.name}/")
     for pr in _systems_of(probes):
         g = pr.name
         arrays[f"{g}/@n"] = np.int64(pr.n)
@@ -58,10 +105,10 @@ def write_snapshot(systems, path, step=None, probes=()):
         np.savez(f, **arrays)
 
 
-def _check_group(f, g, n, ndims):
-    if f"{g}/@n" not in f:
-        raise ArgumentError(f"no saved group for system {g!r}")
-    sn, snd = int(f[f"{g}/@n"]), int(f[f"{g}/@ndims"])
+def _check_group(f, prefix, n, ndims):
+    if f"{prefix}@n" not in f:
+        raise ArgumentError(f"no saved group {prefix!r}")
+    sn, snd = int(f[f"{prefix}@n"]), int(f[f"{prefix}@ndims"])
     if sn != n:
         raise ArgumentError(f"Saved particle count ({sn}) does not match system count ({n})")
     if snd != ndims:
@@ -73,15 +120,10 @@ def read_snapshot(systems, path, probes=()):
     the saved step, or None."""
     with np.load(path) as f:
         for ps in _systems_of(systems):
-            g = ps.name
-            _check_group(f, g, ps.n, ps.ndims)
-            for name, _ in ps.particle_fields():
-                key = f"{g}/{name}"
-                if key in f:
-                    getattr(ps, name)[...] = f[key]
+            _get_group(f, ps, f"{ps.name}/")
         for pr in _systems_of(probes):
             g = pr.name
-            _check_group(f, g, pr.n, pr.ndims)
+            _check_group(f, f"{g}/", pr.n, pr.ndims)
             pr.x[...] = f[f"{g}/x"]
             pr.id[...] = f[f"{g}/id"]
         return int(f["@step"]) if "@step" in f else None

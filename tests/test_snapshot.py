@@ -105,3 +105,69 @@ def test_restart_with_moving_probes_on_the_oracle(tmp_path):
     a, b = _fields(lf), _fields(lf2)
     for key in a:
         assert np.array_equal(a[key], b[key]), key
+
+
+# test/test_read_h5.jl restated (the container is NumPy's, the groups,
+# attributes and checks the reference's)
+from grasph_b200.snapshot import read_h5, system_from_h5, write_h5  # noqa: E402
+
+
+def test_read_h5_basic_round_trip(tmp_path):
+    ps1 = G.BasicParticleSystem("test1", 3, 2, 1.5, 2.0)
+    ps1.x[:] = [[0.0, 1.0], [2.0, 3.0], [4.0, 5.0]]
+    ps1.v[:] = [[0.1, 0.2], [0.3, 0.4], [0.5, 0.6]]
+    ps1.rho[:] = [1.0, 2.0, 3.0]
+    path = tmp_path / "out.npz"
+    write_h5(ps1, path)
+    ps2 = G.BasicParticleSystem("test2", 3, 2, 1.0, 1.0)
+    read_h5(ps2, path)
+    np.testing.assert_allclose(ps2.x, ps1.x)
+    np.testing.assert_allclose(ps2.v, ps1.v)
+    np.testing.assert_allclose(ps2.rho, ps1.rho)
+    assert ps2.mass == 1.0 and ps2.c == 1.0  # metadata is not overwritten
+    ps_new = system_from_h5(G.BasicParticleSystem, path, "test1")
+    assert (ps_new.n, ps_new.ndims, ps_new.mass, ps_new.c) == (3, 2, 1.5, 2.0)
+    np.testing.assert_allclose(ps_new.x, ps1.x)
+    np.testing.assert_allclose(ps_new.v, ps1.v)
+    np.testing.assert_allclose(ps_new.rho, ps1.rho)
+
+
+def test_read_h5_fluid_path_constructor(tmp_path):
+    ps1 = G.FluidParticleSystem("fluid1", 2, 2, 0.5, 10.0, source_v=[0.0, -9.81])
+    ps1.x[:] = [[0.1, 0.2], [0.3, 0.4]]
+    ps1.v[:] = [[0.5, 0.6], [0.7, 0.8]]
+    ps1.rho[:] = 1000.0
+    ps1.p[:] = [1.0, 2.0]
+    path = tmp_path / "out.npz"
+    write_h5(ps1, path)
+    ps_new = system_from_h5(G.FluidParticleSystem, path, "fluid1", source_v=[0.0, -9.81])
+    assert (ps_new.n, ps_new.mass, ps_new.c) == (2, 0.5, 10.0)
+    for name in ("x", "v", "rho", "p"):
+        np.testing.assert_allclose(getattr(ps_new, name), getattr(ps1, name))
+    np.testing.assert_array_equal(ps_new.source_v, [0.0, -9.81])
+
+
+def test_read_h5_stress_path_constructor(tmp_path):
+    ps1 = G.StressParticleSystem("stress1", 2, 2, 3, 1.2, 5.0)
+    ps1.x[:] = [[0.1, 0.2], [0.3, 0.4]]
+    ps1.v[:] = [[0.5, 0.6], [0.7, 0.8]]
+    ps1.rho[:] = 1800.0
+    ps1.stress[:] = [[1.0, 2.0, 3.0], [4.0, 5.0, 6.0]]
+    ps1.strain_rate[:] = [[0.1, 0.2, 0.3], [0.4, 0.5, 0.6]]
+    path = tmp_path / "out.npz"
+    write_h5(ps1, path)
+    ps_new = system_from_h5(G.StressParticleSystem, path, "stress1")
+    assert ps_new.n == 2 and ps_new.stress.shape == (2, 3)
+    assert (ps_new.mass, ps_new.c) == (1.2, 5.0)
+    for name in ("x", "v", "rho", "stress", "strain_rate"):
+        np.testing.assert_allclose(getattr(ps_new, name), getattr(ps1, name))
+
+
+def test_read_h5_catches_mismatch_errors(tmp_path):
+    ps1 = G.BasicParticleSystem("test1", 3, 2, 1.5, 2.0)
+    path = tmp_path / "out.npz"
+    write_h5(ps1, path)
+    with pytest.raises(G.ArgumentError):
+        read_h5(G.BasicParticleSystem("wrong_n", 4, 2, 1.0, 1.0), path)
+    with pytest.raises(G.ArgumentError):
+        read_h5(G.BasicParticleSystem("wrong_ndims", 3, 3, 1.0, 1.0), path)
