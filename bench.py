@@ -68,6 +68,73 @@ def workload_desc(meta):
     return {k: meta[k] for k in ("workload", "n_fluid", "n_boundary", "ndims") if k in meta}
 
 
+class NvmlClockSampler:
+    """SM clock, power and clock-event reasons polled through NVML every
+    millisecond or so from a host thread during the timed region (a timed
+    region of tens of milliseconds is too short for nvidia-smi's loop)."""
+
+    _REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+                "sw_power_cap": 0x4}
+
+    def __init__(self, torch_device):
+        import threading
+        import pynvml
+        import torch
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(torch_device).uuid)
+        self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        self.rows = []
+        self.stop_flag = threading.Event()
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+
+    def _poll(self):
+        nv, h = self.nv, self.h
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+            except Exception:
+                break
+            self.rows.append((sm, reasons, pw))
+            time.sleep(0.001)
+
+    def start(self):
+        self.thread.start()
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 2.0:
+            time.sleep(0.001)
+
+    def stop(self):
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows), "source": "nvml"}
+        try:
+            out["sm_max_mhz"] = self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+        except Exception:
+            pass
+        if self.rows:
+            sm = sorted(r[0] for r in self.rows)
+            out["sm_mhz"] = sm[len(sm) // 2]
+            out["power_w_max"] = max(r[2] for r in self.rows)
+            reasons = set()
+            for _, bits, _ in self.rows:
+                for nm, b in self._REASONS.items():
+                    if bits & b:
+                        reasons.add(nm)
+            out["reasons"] = sorted(reasons)
+        return out
+
+
+def clock_sampler(index):
+    """NVML polling when pynvml is importable, else nvidia-smi's loop."""
+    try:
+        return NvmlClockSampler(index)
+    except Exception:
+        return ClockSampler(index)
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -129,6 +196,7 @@ class ClockSampler:
                     reasons.add(nm)
         out["reasons"] = sorted(reasons)
         out["samples"] = len(rows)
+        out["source"] = "nvidia-smi"
         return out
 
 
@@ -150,8 +218,13 @@ def field_bytes(lf):
     return sum(getattr(ps, n).nbytes for ps in lf.systems for n, _ in ps.particle_fields())
 
 
+CPU_SAMPLE_S = 15.0  # seconds of CPU work in the timed baseline sample
+
+
 def cpu_sample(workload, scale, steps, threads):
-    """Time the CPU restatement of the reference on a bounded sample."""
+    """Time the CPU restatement of the reference on a bounded sample:
+    `steps` steps, or (None) as many as fill about CPU_SAMPLE_S seconds
+    judged by the warm-up step.  Returns (particle-steps/s, seconds, steps)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import grasph_b200 as G
     from pyoracle import OracleBackend
@@ -159,11 +232,15 @@ def cpu_sample(workload, scale, steps, threads):
     be = OracleBackend(threads=threads)
     s = G.Session([lf], backend=be)
     s.push()
+    t0 = time.perf_counter()
     s.step(1, meta["cfl"])  # first step sorts every system from scratch
+    first = time.perf_counter() - t0
+    if steps is None:
+        steps = int(max(2, min(200, CPU_SAMPLE_S / max(first, 1e-3))))
     t0 = time.perf_counter()
     s.step(steps, meta["cfl"])
     dt = time.perf_counter() - t0
-    return meta["n_fluid"] * steps / dt, dt, meta
+    return meta["n_fluid"] * steps / dt, dt, steps
 
 
 def run_reference(args, rank, world):
@@ -173,15 +250,17 @@ def run_reference(args, rank, world):
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     pyoracle.build()
-    steps = max(1, min(args.steps, 3))
-    value, secs, meta = cpu_sample(args.workload, args.scale, steps, threads)
+    lf, meta = build_workload(args.workload, args.scale)
+    del lf
+    value, secs, steps = cpu_sample(args.workload, args.scale, None, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": secs / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": dict(workload_desc(meta), parallelism="cpu threads"),
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{steps} full steps after 1 warm-up step on {threads} threads; "
+                         "sample": f"{steps} full steps after 1 warm-up step on {threads} threads, sized to "
+                          f"about {CPU_SAMPLE_S:.0f} s of CPU work; "
                                    "the reference's Julia is not available on this box, so the CPU "
                                    "restatement of its algorithm (coloured sweeps, OpenMP) is timed"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -212,7 +291,7 @@ def _timed_steps(sess, meta, args, lib, be, stream, dist, sample_clocks, local_r
     lib.gc_set_profiling(be.ctx, 1)
     sess.step(args.warmup, meta["cfl"])
     st0 = be.stats()
-    clocks = ClockSampler(local_rank) if sample_clocks else None
+    clocks = clock_sampler(local_rank) if sample_clocks else None
     if clocks:
         clocks.start()
     if dist:
@@ -249,21 +328,47 @@ def _open(lf, local_rank, prec):
     return sess, be, lib, torch.cuda.ExternalStream(sptr.value)
 
 
-def _rel_errors(lf_a, lf_b):
-    """Largest per-particle error of each field relative to the field's scale
-    (the FP64 run's largest magnitude), over the fluid/soil systems."""
+# Step count at which the compensated run's error against the FP64 path is
+# reported: the configurations' own run lengths (the 3-D dam break 500 steps,
+# the 2-D dam break and the column 1000 steps).
+ERROR_STEPS = {"dambreak_3d": 500, "dambreak_2d": 1000, "column": 1000}
+G_ACC = 9.81
+ERROR_METRIC = ("largest per-particle error, each particle on its own scale: density |rho_i|; velocity "
+                "max(|v_i|, g*t); acceleration max(|a_i|, g); stress max(|sigma_i|, rho*g*h) (vector and "
+                "tensor max-norms; g*t is the free-fall speed after the run, rho*g*h the weight of one "
+                "smoothing length of material), FP32-compensated against the plain FP64 path")
+
+
+def _rel_errors(lf_a, lf_b, meta, nsteps):
+    """Largest per-particle error of the compensated run `lf_a` against the
+    FP64 run `lf_b` over the moving systems, every particle on its own scale
+    (ERROR_METRIC): density on |rho_i|, velocity on the particle's speed
+    floored at the free-fall speed g·t of the run, acceleration on its
+    magnitude floored at g, stress on its max-norm floored at ρ·g·h."""
     out = {}
-    for sa, sb in zip(lf_a.systems, lf_b.systems):
+    t = nsteps * meta["dt"]
+    h = meta["h"]
+    moving = [i for i, s in enumerate(lf_b.systems) if any(it.system_a is s for it in lf_b.interactions)]
+    for k in moving:
+        sa, sb = lf_a.systems[k], lf_b.systems[k]
         ia, ib = np.argsort(sa.id), np.argsort(sb.id)
-        for name in ("rho", "v", "dvdt", "stress"):
-            if not hasattr(sa, name):
-                continue
-            a = np.asarray(getattr(sa, name))[ia]
-            b = np.asarray(getattr(sb, name))[ib]
-            scale = float(np.abs(b).max())
-            if scale == 0.0:
-                continue
-            out[name] = max(out.get(name, 0.0), float(np.abs(a - b).max() / scale))
+
+        def rows(name):
+            a = np.asarray(getattr(sa, name), dtype=float)[ia]
+            b = np.asarray(getattr(sb, name), dtype=float)[ib]
+            return a.reshape(len(a), -1), b.reshape(len(b), -1)
+
+        a, b = rows("rho")
+        out["rho"] = max(out.get("rho", 0.0), float((np.abs(a - b) / np.abs(b)).max()))
+        for name, floor in (("v", G_ACC * t), ("dvdt", G_ACC)):
+            a, b = rows(name)
+            scale = np.maximum(np.abs(b).max(axis=1, keepdims=True), floor)
+            out[name] = max(out.get(name, 0.0), float((np.abs(a - b) / scale).max()))
+        if hasattr(sa, "stress"):
+            a, b = rows("stress")
+            rho = np.asarray(sb.rho)[ib].reshape(-1, 1)
+            scale = np.maximum(np.abs(b).max(axis=1, keepdims=True), rho * G_ACC * h)
+            out["stress"] = max(out.get("stress", 0.0), float((np.abs(a - b) / scale).max()))
     return out
 
 
@@ -281,9 +386,12 @@ def run_ours(args, rank, world, local_rank):
     nd = meta["ndims"]
     prec = G.PRECISION_FP64 if args.precision == "fp64" else G.PRECISION_FP32_COMPENSATED
     sess, be, lib, stream = _open(lf, local_rank, prec)
+    # the sweep's compute ceiling: the measured FMA issue rate of the pipe its
+    # pair arithmetic runs on (FP32 for the compensated sweep, FP64 otherwise)
     peak = engine.ct.c_double()
-    lib.gc_measure_fp64_peak.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_double)]
-    lib.gc_measure_fp64_peak(be.ctx, engine.ct.byref(peak))
+    peak_fn = lib.gc_measure_fp32_peak if prec == G.PRECISION_FP32_COMPENSATED else lib.gc_measure_fp64_peak
+    peak_fn.argtypes = [engine.ct.c_void_p, engine.ct.POINTER(engine.ct.c_double)]
+    peak_fn(be.ctx, engine.ct.byref(peak))
     ms, st0, st1, clk = _timed_steps(sess, meta, args, lib, be, stream, dist, True, local_rank)
     launches = st1["kernel_launches"] - st0["kernel_launches"]
     sweep_ms = st1["sweep_ms"] - st0["sweep_ms"]
@@ -300,12 +408,19 @@ def run_ours(args, rank, world, local_rank):
         lf64, _ = build_workload(args.workload, args.scale)
         s64, be64, lib64, stream64 = _open(lf64, local_rank, G.PRECISION_FP64)
         ms64, _, _, _ = _timed_steps(s64, meta, args, lib64, be64, stream64, dist, False, local_rank)
+        # both runs continued (untimed) to the configuration's own step count
+        done = args.warmup + args.steps
+        total = max(done, ERROR_STEPS.get(args.workload, done))
+        if total > done:
+            sess.step(total - done, meta["cfl"])
+            s64.step(total - done, meta["cfl"])
         sess.pull()
         s64.pull()
         fp64 = {"value": job_rate(n_fluid, args.steps, ms64 / 1e3, world), "ms_per_step": ms64 / args.steps,
                 "speedup": ms64 / ms,
-                "rel_error_after_steps": args.warmup + args.steps,
-                "rel_error": _rel_errors(lf, lf64)}
+                "rel_error_after_steps": total,
+                "rel_error": _rel_errors(lf, lf64, meta, total),
+                "rel_error_metric": ERROR_METRIC}
         s64.close()
 
     # end to end through the host API, from pinned host buffers: every step
@@ -348,7 +463,12 @@ def run_ours(args, rank, world, local_rank):
                "ms_push_step_pull": [x / e2e_steps * 1e3 for x in split],
                "copied": "every field of the simulated systems, both ways, each step (pinned host memory)"}
 
-    # roofline of the dominant kernel (the fused pair sweep)
+    # roofline of the dominant kernel (the fused pair sweep): not a dense
+    # contraction and not bandwidth-bound, it is bound by instruction issue;
+    # its ceiling is the measured FMA issue rate of the pipe its pair
+    # arithmetic runs on, and its algorithmic FLOPs are the reference's work
+    # (unordered accepted pairs x FLOPs per FluidPfn pair).  The HBM view
+    # (algorithmic bytes against the measured copy bandwidth) is kept beside it.
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     hbm_peak, src = 6650.0, "fallback"
     if peaks_file.exists():
@@ -358,24 +478,25 @@ def run_ours(args, rank, world, local_rank):
     achieved_gbs = per_launch_bytes / sweep_avg_s / 1e9
     flops_per_launch = pairs * FLUID_PAIR_FLOPS[nd]
     achieved_tflops = flops_per_launch / sweep_avg_s / 1e12
-    kname = ("k_sweep_stg (fused pair sweep, chunk-staged)" if args.precision == "fp32c"
-             else "k_sweep (fused pair sweep)")
-    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved_gbs,
-            "peak": hbm_peak, "peak_source": src, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+    f32 = prec == G.PRECISION_FP32_COMPENSATED
+    kname = "k_sweep_stg (fused pair sweep, chunk-staged)" if f32 else "k_sweep (fused pair sweep)"
+    roof = {"kernel": kname, "bound": "fp32" if f32 else "fp64", "achieved": achieved_tflops,
+            "peak": peak.value, "unit": "TFLOP/s", "frac": achieved_tflops / peak.value,
+            "peak_source": ("measured FP32 FMA issue rate (gc_measure_fp32_peak)" if f32
+                            else "measured FP64 FMA issue rate (gc_measure_fp64_peak)"),
+            "flops_per_launch": flops_per_launch,
             "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, args.scale, args.precision)),
-            "bytes_per_launch": per_launch_bytes,
             "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_ms / ms,
-            "compute": {"bound": "fp64 pipe", "achieved": achieved_tflops, "peak": peak.value,
-                        "peak_source": "measured FP64 FMA issue rate (gc_measure_fp64_peak)",
-                        "unit": "TFLOP/s", "frac": achieved_tflops / peak.value,
-                        "flops_per_launch": flops_per_launch}}
+            "hbm": {"achieved": achieved_gbs, "peak": hbm_peak, "peak_source": src, "unit": "GB/s",
+                    "frac": achieved_gbs / hbm_peak, "bytes_per_launch": per_launch_bytes}}
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
-        v, secs, _ = cpu_sample(args.workload, args.scale, 1, threads)
+        v, secs, nst = cpu_sample(args.workload, args.scale, None, threads)
         cpu = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-               "sample": f"1 full step after 1 warm-up step of the same workload on {threads} threads "
-                         f"({secs:.1f} s); CPU restatement of the reference algorithm"}
+               "sample": f"{nst} full steps after 1 warm-up step of the same workload on {threads} threads "
+                         f"({secs:.1f} s, sized to about {CPU_SAMPLE_S:.0f} s); CPU restatement of the "
+                         "reference algorithm"}
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -3723,6 +3723,32 @@ int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out) {
     return GC_OK;
 }
 
+int gc_measure_fp32_peak(gc_ctx* ctx, double* tflops_out) {
+    if (!ctx || !tflops_out) return GC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    float* out = nullptr;
+    TRY(dalloc(ctx, &out, 1));
+    const int threads = 256, blocks = sms * 8, iters = 1 << 17;
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    launch_fp32_peak(out, blocks, threads, 1024, ctx->stream);  // warm-up
+    CU(cudaEventRecord(a, ctx->stream));
+    launch_fp32_peak(out, blocks, threads, iters, ctx->stream);
+    CU(cudaEventRecord(b, ctx->stream));
+    CU(cudaEventSynchronize(b));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    dfree(ctx, out, 1);
+    double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+    *tflops_out = flops / (ms * 1e-3) / 1e12;
+    return GC_OK;
+}
+
 }  // extern "C"
 
 // ============================================================ packing

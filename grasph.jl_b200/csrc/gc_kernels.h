@@ -120,6 +120,7 @@ void launch_i32_to_i64(const int32_t* src, int64_t* dst, int64_t n, cudaStream_t
 // ------------------------------------------------------------ measurement
 void launch_sum_counts(const int32_t* c, int64_t n, unsigned long long* out, cudaStream_t s);
 void launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStream_t s);
+void launch_fp32_peak(float* out, int blocks, int threads, int iters, cudaStream_t s);
 extern std::atomic<long long> g_launches;
 
 }  // namespace gc

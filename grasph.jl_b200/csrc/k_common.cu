@@ -1000,4 +1000,26 @@ void launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStrea
     COUNTED(1);
 }
 
+// FP32 FMA issue rate: eight independent dependent chains per thread.
+__global__ void k_fp32_peak(float* out, int iters, float a, float b) {
+    float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
+          x7 = x0 + 7;
+    for (int i = 0; i < iters; ++i) {
+        x0 = fmaf(x0, a, b);
+        x1 = fmaf(x1, a, b);
+        x2 = fmaf(x2, a, b);
+        x3 = fmaf(x3, a, b);
+        x4 = fmaf(x4, a, b);
+        x5 = fmaf(x5, a, b);
+        x6 = fmaf(x6, a, b);
+        x7 = fmaf(x7, a, b);
+    }
+    float r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (r == 12345.678f) out[0] = r;  // keeps the chains live
+}
+void launch_fp32_peak(float* out, int blocks, int threads, int iters, cudaStream_t s) {
+    k_fp32_peak<<<blocks, threads, 0, s>>>(out, iters, 0.9999999f, 1e-9f);
+    COUNTED(1);
+}
+
 }  // namespace gc

@@ -13,10 +13,11 @@
 // parts that must start at zero, and calls that overlap on the GPU (two
 // streams, or two host threads) race on it.
 //
-// Host code only ever sees a stand-in for the array's name; the device
-// address is obtained with cudaGetSymbolAddress, once per device, the first
-// time the entry point runs with that device current.  That first call
-// should therefore come before any stream capture.
+// Host code only ever sees a stand-in for the array's name; every call
+// resolves the array's device address with cudaGetSymbolAddress (which
+// allocates nothing) on the caller's current device, so the address is
+// right for the device and context of that call, also after a
+// cudaDeviceReset has re-created the context.
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -44,8 +45,6 @@ constexpr int64_t NA_WORDS = NA_TAIL + NA_TAIL_BYTES / 4;
 
 __device__ __align__(256) int32_t g_noalloc_scratch[NA_WORDS];
 
-int32_t* g_scratch_addr[64] = {};  // device address of the array, per device
-
 __global__ void k_na_init(SysInst* S, int64_t n, double cutoff, int64_t* cells, int* err) {
     SysInst s{};
     s.base = 0;
@@ -66,17 +65,12 @@ extern "C" int gc_cell_sort_perm_noalloc(const double* x_planar, int64_t n, int 
     if (ndims < 2 || ndims > 3 || !(cutoff > 0.0) || !std::isfinite(cutoff)) return GC_ERR_ARG;
     if (n > 0 && (!x_planar || !perm_out)) return GC_ERR_ARG;
     if (n == 0) return GC_OK;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GC_ERR_CUDA;
-    if (!g_scratch_addr[dev]) {
-        // one-time set-up on this device (it is current here)
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GC_ERR_CUDA;
-        g_scratch_addr[dev] = (int32_t*)p;
-    }
+    // the scratch array's address on the current device
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return GC_ERR_CUDA;
     if (scan_tmp_elems(NA_MAX_CELLS) > NA_SCAN_WORDS) return GC_ERR_CAPACITY;
     cudaStream_t s = (cudaStream_t)stream;
-    int32_t* base = g_scratch_addr[dev];
+    int32_t* base = (int32_t*)addr;
     int32_t* key = base + NA_KEY;
     int32_t* inst_of = base + NA_INST;
     int32_t* hist = base + NA_HIST;

@@ -2,7 +2,7 @@
 
 `compile_instance` walks a LeapFrogTimeIntegrator (systems, ghost entries,
 interactions, updaters) and issues the C-ABI model-building calls — the same
-sequence a Julia `ccall` shim issues.  `Device` owns one
+sequence the Julia `ccall` binding (julia/GrasphCUDA.jl) issues.  `Device` owns one
 context; `time_integrate` is the drop-in for
 `time_integrate!(::LeapFrogTimeIntegrator, ...)` (src/TimeIntegration.jl:580).
 
@@ -108,6 +108,7 @@ def load_library(path: os.PathLike | None = None):
         "gc_stream": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_void_p)]),
         "gc_set_profiling": (ct.c_int, [ct.c_void_p, ct.c_int]),
         "gc_measure_fp64_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
+        "gc_measure_fp32_peak": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double)]),
         "gc_set_graphs": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double]),
         "gc_set_sweep_config": (ct.c_int, [ct.c_void_p, ct.c_int]),
         "gc_upload_fields": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
@@ -561,6 +562,9 @@ class Session:
         self.backend.finalize()
         self.backend.set_precision(precision)
         self.precision = precision
+        # the global step of the loaded restart (_load_restart!'s return,
+        # from which the reference's loop continues global_step)
+        self.step_offset = 0
 
     # -- state transfer
     def push(self, systems=None):
@@ -595,7 +599,7 @@ class Session:
         from .snapshot import write_snapshot
         m = self._m(inst)
         download_instance(self.backend, m)
-        write_snapshot(m.systems, path, step=self.stats()["steps_done"],
+        write_snapshot(m.systems, path, step=self.step_offset + self.stats()["steps_done"],
                        probes=[pr for pr in m.probes if pr.mirror_target is None])
 
     def load(self, path, inst=0):
@@ -609,6 +613,8 @@ class Session:
         upload_instance(self.backend, m)
         for pr in free:
             self.backend.upload(m.inst, m.h(pr), C.GC_FIELD_X, pr.x)
+        # later saves count from the restart's step
+        self.step_offset = step - self.stats()["steps_done"]
         return step
 
     # -- per-phase hooks (instance 0 unless given)

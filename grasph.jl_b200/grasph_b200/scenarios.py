@@ -22,7 +22,7 @@ from .model import (BasicParticleSystem, CauchyFluidPfn, CubicSplineKernel, Dyna
                     ElastoPlasticParticleSystem, ElastoPlasticStressUpdater, FluidParticleSystem, FluidPfn,
                     FluidSolidPfn, HookeLawStressUpdater,
                     GhostCopier, GhostEntry, GhostParticleSystem, HouseholderReflect, LeapFrogTimeIntegrator,
-                    LinearEOSUpdater, ProbeParticleSystem,
+                    LinearEOSUpdater, ProbeParticleSystem, StaticBoundarySystem,
                     RK4TimeIntegrator, StrainRatePfn, InterpolateFieldFn, VirtualNormUpdater,
                     VirtualParticleSystem, PrescribedVelocityUpdater, StrainRateVorticityPfn, StressParticleSystem, SystemInteraction,
                     TaitEOSUpdater, ViscoPlasticMCStressUpdater, WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater)
@@ -145,6 +145,92 @@ def dambreak_3d(nx=100, ny=50, nz=200, dx=0.01, tank=(4.0, 1.0, 4.0), layers=3, 
     lf = LeapFrogTimeIntegrator(systems, inters)
     meta = dict(workload="dambreak_3d", n_fluid=fluid.n, n_boundary=sum(s.n for s in systems[1:]),
                 h=h, c0=c0, cfl=cfl, dt=cfl * h / c0, ndims=3)
+    return lf, meta
+
+
+# ------------------------------------- dam breaks with a static (LJ) wall
+
+def dambreak_lj_2d(nfx=50, nfy=50, nbx=150, nby=80, dx=0.5, rho0=1000.0, alpha=0.01, beta=0.0, hfac=1.2,
+                   cfl=0.05, column_height=None):
+    """2-D dam break in a single-layer Lennard-Jones wall (dambreak.jl
+    layout): an nfx×nfy fluid block at ((i+½)dx, (j+½)dx), i outer, at rest
+    with ρ = ρ0 and p from the Tait EOS (zero), in a box nbx·dx wide and
+    nby·dx tall whose wall particles (bottom and top rows from i = -1 to nbx,
+    then the left and right columns) form one BasicParticleSystem wrapped as
+    StaticBoundarySystem(boundary, dx).  c0 = 10·sqrt(2 g H) with H the
+    column height (25 m in the script)."""
+    H = nfy * dx if column_height is None else column_height
+    c0 = 10.0 * math.sqrt(2.0 * G * H)
+    h = hfac * dx
+    mass = rho0 * dx * dx
+    ii, jj = np.meshgrid(np.arange(nfx), np.arange(nfy), indexing="ij")
+    fluid = FluidParticleSystem("fluid", nfx * nfy, 2, mass, c0, source_v=[0.0, -G],
+                                state_updater=TaitEOSUpdater(rho0))
+    fluid.x[:, 0] = (ii.ravel() + 0.5) * dx
+    fluid.x[:, 1] = (jj.ravel() + 0.5) * dx
+    fluid.rho[:] = rho0
+    fluid.p[:] = _tait_pressure(fluid.rho, rho0, c0, 7.0)
+    W, T = nbx * dx, nby * dx
+    row = np.arange(-1, nbx + 1)
+    col = np.arange(nby)
+    pts = np.concatenate([
+        np.stack([(row + 0.5) * dx, np.full(row.size, -0.5 * dx)], axis=1),
+        np.stack([(row + 0.5) * dx, np.full(row.size, T + 0.5 * dx)], axis=1),
+        np.stack([np.full(col.size, -0.5 * dx), (col + 0.5) * dx], axis=1),
+        np.stack([np.full(col.size, W + 0.5 * dx), (col + 0.5) * dx], axis=1)])
+    boundary = _wall("boundary", pts, mass, c0, rho0)
+    kernel = CubicSplineKernel(h, ndims=2)
+    inters = [SystemInteraction(kernel, FluidPfn(alpha, beta, h), fluid),
+              SystemInteraction(kernel, FluidPfn(alpha, beta, h), fluid, StaticBoundarySystem(boundary, dx))]
+    lf = LeapFrogTimeIntegrator([fluid, boundary], inters)
+    meta = dict(workload="dambreak_lj_2d", n_fluid=fluid.n, n_boundary=boundary.n, h=h, c0=c0, cfl=cfl,
+                dt=cfl * h / c0, ndims=2)
+    return lf, meta
+
+
+def dambreak_lj_3d(nfx=50, nfy=12, nfz=50, nbx=150, nby=12, nbz=80, dx=0.5, rho0=1000.0, alpha=0.005, beta=0.0,
+                   hfac=1.2, cfl=0.05, column_height=None):
+    """3-D dam break in a single-layer Lennard-Jones box (dambreak_3d.jl
+    layout, z vertical): an nfx×nfy×nfz block (i, j, m loops, m innermost)
+    at rest, and six faces of wall particles in the script's order (floor
+    and ceiling from -1 to nbx × -1 to nby, left and right nby×nbz, front
+    and back nbx×nbz) in one BasicParticleSystem wrapped as
+    StaticBoundarySystem(boundary, dx)."""
+    H = nfz * dx if column_height is None else column_height
+    c0 = 10.0 * math.sqrt(2.0 * G * H)
+    h = hfac * dx
+    mass = rho0 * dx ** 3
+    ii, jj, mm = np.meshgrid(np.arange(nfx), np.arange(nfy), np.arange(nfz), indexing="ij")
+    fluid = FluidParticleSystem("fluid", nfx * nfy * nfz, 3, mass, c0, source_v=[0.0, 0.0, -G],
+                                state_updater=TaitEOSUpdater(rho0))
+    fluid.x[:] = np.stack([(ii.ravel() + 0.5) * dx, (jj.ravel() + 0.5) * dx, (mm.ravel() + 0.5) * dx], axis=1)
+    fluid.rho[:] = rho0
+    fluid.p[:] = _tait_pressure(fluid.rho, rho0, c0, 7.0)
+    X, Y, Z = nbx * dx, nby * dx, nbz * dx
+
+    def face(a, b, fixed_axis, value):
+        A, B = np.meshgrid(a, b, indexing="ij")
+        cols = [None, None, None]
+        free = [ax for ax in range(3) if ax != fixed_axis]
+        cols[free[0]], cols[free[1]] = A.ravel(), B.ravel()
+        cols[fixed_axis] = np.full(A.size, value)
+        return np.stack(cols, axis=1)
+
+    ex = (np.arange(-1, nbx + 1) + 0.5) * dx
+    ey = (np.arange(-1, nby + 1) + 0.5) * dx
+    iy = (np.arange(nby) + 0.5) * dx
+    iz = (np.arange(nbz) + 0.5) * dx
+    ix = (np.arange(nbx) + 0.5) * dx
+    pts = np.concatenate([face(ex, ey, 2, -0.5 * dx), face(ex, ey, 2, Z + 0.5 * dx),
+                          face(iy, iz, 0, -0.5 * dx), face(iy, iz, 0, X + 0.5 * dx),
+                          face(ix, iz, 1, -0.5 * dx), face(ix, iz, 1, Y + 0.5 * dx)])
+    boundary = _wall("boundary", pts, mass, c0, rho0)
+    kernel = CubicSplineKernel(h, ndims=3)
+    inters = [SystemInteraction(kernel, FluidPfn(alpha, beta, h), fluid),
+              SystemInteraction(kernel, FluidPfn(alpha, beta, h), fluid, StaticBoundarySystem(boundary, dx))]
+    lf = LeapFrogTimeIntegrator([fluid, boundary], inters)
+    meta = dict(workload="dambreak_lj_3d", n_fluid=fluid.n, n_boundary=boundary.n, h=h, c0=c0, cfl=cfl,
+                dt=cfl * h / c0, ndims=3)
     return lf, meta
 
 

@@ -15,6 +15,8 @@ updated.
 """
 from __future__ import annotations
 
+import warnings
+
 import numpy as np
 
 from .model import ArgumentError
@@ -116,14 +118,26 @@ def _check_group(f, prefix, n, ndims):
 
 
 def read_snapshot(systems, path, probes=()):
-    """Read `path` into `systems` (and `probes`) as `read_h5!` does; returns
-    the saved step, or None."""
+    """Read `path` into `systems` (and `probes`) as `_load_restart!`
+    (src/Driver.jl:79-96) does: a system or probe without a group in the
+    file is left untouched with a warning, the others are read with
+    `read_h5!`'s checks; returns the saved step, or 0 with a warning when
+    the file holds none."""
     with np.load(path) as f:
         for ps in _systems_of(systems):
+            if f"{ps.name}/@n" not in f:
+                warnings.warn(f"Restart file {path} has no group for system {ps.name!r}; leaving it untouched")
+                continue
             _get_group(f, ps, f"{ps.name}/")
         for pr in _systems_of(probes):
             g = pr.name
+            if f"{g}/@n" not in f:
+                warnings.warn(f"Restart file {path} has no group for probe {g!r}; leaving it untouched")
+                continue
             _check_group(f, f"{g}/", pr.n, pr.ndims)
             pr.x[...] = f[f"{g}/x"]
             pr.id[...] = f[f"{g}/id"]
-        return int(f["@step"]) if "@step" in f else None
+        if "@step" not in f:
+            warnings.warn(f'Restart file {path} has no "step" attribute; assuming step 0')
+            return 0
+        return int(f["@step"])

@@ -337,10 +337,39 @@ function download!(cl::CudaLeapFrog)
     end
 end
 
+"""
+    download_ghosts!(cl::CudaLeapFrog)
+
+Each ghost system's current particles (generated and sorted on the device in
+the last step) copied into its host arrays, resized to the device's count:
+x, v, rho, idx_original, idx_boundary, normals and the copier extras.
+"""
+function download_ghosts!(cl::CudaLeapFrog)
+    for ge in cl.lf.ghosts
+        g = ge.ghost
+        h = cl.handles[g]
+        n = Ref{Int64}(0)
+        check(cl.ctx, ccall((:gc_get_count, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Ref{Int64}), cl.ctx, 0, h, n))
+        io(arr, fid) = GC.@preserve arr check(cl.ctx, ccall((:gc_download_field, LIB), Cint,
+                                              (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cvoid}, Csize_t),
+                                              cl.ctx, 0, h, fid, pointer(arr), sizeof(arr)))
+        for (f, fid) in ((:x, GC_FIELD.x), (:v, GC_FIELD.v), (:rho, GC_FIELD.rho),
+                         (:idx_original, 13), (:idx_boundary, 14), (:normals, 15))
+            arr = getfield(g, f)
+            resize!(arr, n[])
+            n[] > 0 && io(arr, fid)
+        end
+        for (k, arr) in pairs(getfield(g, :extras))
+            resize!(arr, n[])
+            n[] > 0 && io(arr, GC_FIELD[k])
+        end
+    end
+    return nothing
+end
+
 # _maybe_save!'s file (src/TimeIntegration.jl:520-549) from the downloaded
-# state: step and sim_time attributes, one group per system, virtual system
-# and probe written by Grasph's own write_h5.  Ghosts are regenerated on the
-# device every step and are not downloaded, so they have no group here.
+# state: step and sim_time attributes, one group per system, ghost system,
+# virtual system and probe written by Grasph's own write_h5.
 function save_h5(cl::CudaLeapFrog, output_prefix, global_step::Int, width::Int, dt)
     path = "$(output_prefix)_$(lpad(global_step, width, '0')).h5"
     d = dirname(path)
@@ -350,6 +379,9 @@ function save_h5(cl::CudaLeapFrog, output_prefix, global_step::Int, width::Int, 
         HDF5.attrs(f)["sim_time"] = Float64(global_step * dt)
         for ps in cl.lf.systems
             Grasph.write_h5(ps, create_group(f, ps.name))
+        end
+        for ge in cl.lf.ghosts
+            Grasph.write_h5(ge.ghost, create_group(f, ge.ghost.name))
         end
         for vps in cl.lf.virtual_systems
             Grasph.write_h5(vps, create_group(f, vps.name))
@@ -395,6 +427,7 @@ function Grasph.time_integrate!(cl::CudaLeapFrog, num_timesteps::Int, print_inte
         if output_prefix !== nothing && g % save_interval_step == 0
             isempty(cl.lf.probes) || measure_probes!(cl)
             download!(cl)
+            download_ghosts!(cl)
             save_h5(cl, output_prefix, g, width, dt)
         end
     end

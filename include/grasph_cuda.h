@@ -333,6 +333,9 @@ int gc_set_sweep_config(gc_ctx* ctx, int cfg);
 /* Measured FP64 FMA issue rate of the device in TFLOP/s (2 flops per FMA):
  * the compute ceiling of the FP64 pair sweep.                             */
 int gc_measure_fp64_peak(gc_ctx* ctx, double* tflops_out);
+/* Measured FP32 FMA issue rate of the device in TFLOP/s (2 flops per FMA):
+ * the compute ceiling of the FP32-compensated pair sweep.                 */
+int gc_measure_fp32_peak(gc_ctx* ctx, double* tflops_out);
 
 /* ======================================================== phase hooks */
 /* The same device kernels, one reference phase at a time (parity tests and
@@ -382,10 +385,10 @@ int gc_neighbor_counts(gc_ctx* ctx, int inst, int inter, int32_t* counts_out, in
  * 0-based source index of each sorted position (the order of
  * `sort_particles!`, src/Sorting.jl:157, for keys floor(x_d/cutoff)).
  * stream: a cudaStream_t (NULL for the default stream); the call returns
- * after the stream has finished its work.  The first call on each device
- * resolves the scratch array's device address and should come before any
- * stream capture.  Calls share the scratch array; calls that overlap on the
- * GPU race on it.                                                          */
+ * after the stream has finished its work.  Each call resolves the scratch
+ * array's device address on the current device (cudaGetSymbolAddress,
+ * which allocates nothing).  Calls share the scratch array; calls that
+ * overlap on the GPU race on it.                                           */
 int gc_cell_sort_perm_noalloc(const double* x_planar, int64_t n, int ndims, double cutoff,
                               int32_t* perm_out, void* stream);
 

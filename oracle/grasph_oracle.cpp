@@ -131,6 +131,19 @@ struct Sys {
     std::vector<std::vector<Upd>> upd;  // one chain per updater-tuple entry
     std::vector<double> q0v, q0rho;
     std::vector<double> accv, accrho;  // RK4 accumulators
+    // Magnitude shadows of the rate fields (test infrastructure, track_mag):
+    // |value| when the field is set (reset to its source term, zeroed,
+    // uploaded), then + |term| for every pair term and damping term added
+    // to it.  Permuted with the particles.
+    std::vector<double> mdvdt, mdrhodt, msr, mvort;
+    // Integrated-state shadows (track_mag): Σ over steps of each increment's
+    // magnitude, dt·M(dv/dt) for v, dt·M(dρ/dt) for ρ, dt·max(|v|, M(v)) for
+    // x; zero when the field is set.  The scale of a trajectory's error.
+    std::vector<double> mvi, mrhoi, mxi, accmv, accmrho;
+    // Elasto-plastic and Hooke systems (track_mag): Σ over steps of the
+    // stress increment's magnitude, dt·|D|·M(ε̇) + 2·dt·|σ|·M(ω) per
+    // component, and of the strain increment's, dt·M(ε̇).
+    std::vector<double> mstr, mstrain;
     bool vsrc = false;  // the source of a virtual system: not one of the integrator's systems
     bool probe = false; // a probe's own arrays (count extra in drhodt)
     bool has_p() const { return kind >= GC_SYS_FLUID; }
@@ -208,6 +221,7 @@ struct oracle_ctx {
     double gamma = 0;
     int integ = GC_INTEGRATOR_LEAPFROG;
     int threads = 1;
+    int track_mag = 0;  // magnitude shadows: 0 off, 1 over the terms, 2 over the inputs
     int64_t steps = 0;
     std::string err;
 };
@@ -262,6 +276,19 @@ inline double kernel_dw_dq(const Kern& k, double q) {
 // ------------------------------------------------------------- primitives
 // src/PairwisePhysics.jl
 
+// Test infrastructure: set (read-only) during a magnitude pass over the
+// inputs (track_mag 2).  Every difference or signed sum a pair term is built
+// from -- velocities, densities, pressures, stresses, gradient components --
+// is then taken as the sum of the magnitudes, so the shadow bounds how far
+// the term moves when its inputs carry relative errors (a trajectory that
+// drifted by a few ulps, or inputs rounded to FP32).  Zero otherwise.
+int g_mag_inputs = 0;
+
+template <int ND>
+inline void vdiff(const double* a, const double* b, double* out) {
+    for (int d = 0; d < ND; ++d) out[d] = g_mag_inputs ? std::fabs(a[d]) + std::fabs(b[d]) : a[d] - b[d];
+}
+
 template <int ND>
 inline double dot(const double* a, const double* b) {
     double s = a[0] * b[0];
@@ -269,11 +296,18 @@ inline double dot(const double* a, const double* b) {
     return s;
 }
 
+template <int ND>
+inline double dot_abs(const double* a, const double* b) {
+    double s = 0.0;
+    for (int d = 0; d < ND; ++d) s += std::fabs(a[d]) * std::fabs(b[d]);
+    return s;
+}
+
 // :29-34
 template <int ND>
 inline double art_visc(const double* dx, const double* dv, double h, double ri, double rj,
                        double alpha, double beta, double ci, double cj) {
-    double vr = jmin(dot<ND>(dx, dv), 0.0);
+    double vr = g_mag_inputs ? -dot_abs<ND>(dx, dv) : jmin(dot<ND>(dx, dv), 0.0);
     double muv = (h * vr) / (dot<ND>(dx, dx) + (h * h) * 0.01);
     double mc = 0.5 * (ci + cj);
     return ((beta * muv - alpha * mc) * muv) / ((0.5 * ri) * rj);
@@ -281,6 +315,10 @@ inline double art_visc(const double* dx, const double* dv, double h, double ri, 
 
 // :58-69
 inline double pressure_coeff(double pi_, double pj, double ri, double rj, int S) {
+    if (g_mag_inputs) {
+        pi_ = std::fabs(pi_);
+        pj = std::fabs(pj);
+    }
     if (S == 1) return -(pi_ + pj) / (ri * rj);
     return -(pi_ / (ri * ri) + pj / (rj * rj));
 }
@@ -296,7 +334,8 @@ inline double diffusion(const double* dx, double ri, double rj, double ci, doubl
     double rr = dot<ND>(dx, dx);
     double c = 0.5 * (ci + cj);
     double h = 0.5 * (hi + hj);
-    return (((((2.0 * delta) * c) * h) * (ri - rj)) * dot<ND>(dx, gx)) / rr;
+    const double drho = g_mag_inputs ? std::fabs(ri) + std::fabs(rj) : ri - rj;
+    return (((((2.0 * delta) * c) * h) * drho) * dot<ND>(dx, gx)) / rr;
 }
 
 // :258-263
@@ -311,10 +350,21 @@ inline double lennard_jones(const double* dx, double cutoff, double c) {
 
 // :125-151; out has ND components
 template <int ND>
-inline void cauchy(const double* si, const double* sj, int ns, double ri, double rj, const double* g,
+inline void cauchy(const double* si_, const double* sj_, int ns, double ri, double rj, const double* g,
                    double* out) {
     double ci = 1.0 / (ri * ri);
     double cj = 1.0 / (rj * rj);
+    double ai[6], aj[6];
+    const double* si = si_;
+    const double* sj = sj_;
+    if (g_mag_inputs) {
+        for (int q = 0; q < ns; ++q) {
+            ai[q] = std::fabs(si_[q]);
+            aj[q] = std::fabs(sj_[q]);
+        }
+        si = ai;
+        sj = aj;
+    }
     if (ND == 2) {
         int xy = ns == 3 ? 2 : 3;
         out[0] = (si[0] * g[0] + si[xy] * g[1]) * ci + (sj[0] * g[0] + sj[xy] * g[1]) * cj;
@@ -354,6 +404,14 @@ inline void strain_rate_t(const double* dv, const double* g, int ns, double* sr)
 // :210-220
 template <int ND>
 inline void vorticity_t(const double* dv, const double* g, double* w) {
+    if (g_mag_inputs) {
+        w[0] = 0.5 * (dv[0] * g[1] + dv[1] * g[0]);
+        if (ND == 3) {
+            w[1] = 0.5 * (dv[0] * g[2] + dv[2] * g[0]);
+            w[2] = 0.5 * (dv[1] * g[2] + dv[2] * g[1]);
+        }
+        return;
+    }
     if (ND == 2) {
         w[0] = 0.5 * (dv[0] * g[1] - dv[1] * g[0]);
     } else {
@@ -392,7 +450,15 @@ struct Pfn {
     bool has_eps;
     int imask;   // InterpolateFieldFn: fields (1<<GC_FIELD_*)
     bool iwsum;  // InterpolateFieldFn: accumulate w_sum
+    bool mag = false;  // magnitude pass: rate accumulators sum |term| (see track_mag)
 };
+
+// One pair term added to (acc) or subtracted from (dec) a rate accumulator,
+// rounded as the reference's `a += t` / `a -= t`.  In a magnitude pass the
+// accumulator is a magnitude shadow and receives |t|: the per-particle
+// Σ|terms| that scales a summation-order difference.
+inline void acc(const Pfn& f, double& x, double t) { x = f.mag ? x + std::fabs(t) : x + t; }
+inline void dec(const Pfn& f, double& x, double t) { x = f.mag ? x + std::fabs(t) : x - t; }
 
 Pfn make_pfn(int kind, const double* prm) {
     Pfn f;
@@ -422,19 +488,19 @@ void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, con
             double ri = ps.rho[i], rj = ps.rho[j], pi_ = ps.p[i], pj = ps.p[j];
             double mass = ps.mass;
             double dv[ND];
-            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            vdiff<ND>(vi, vj, dv);
             double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, ps.c, ps.c);
             double dh = pressure_coeff(pi_, pj, ri, rj, f.S);
             double s = mass * (dh - piv);
             for (int d = 0; d < ND; ++d) {
                 double t = s * gx[d];
-                ps.dvdt[i * ND + d] = ps.dvdt[i * ND + d] + t;
-                ps.dvdt[j * ND + d] = ps.dvdt[j * ND + d] - t;
+                acc(f, ps.dvdt[i * ND + d], t);
+                dec(f, ps.dvdt[j * ND + d], t);
             }
             double dr = dot<ND>(dv, gx);
             double psi = diffusion<ND>(dx, ri, rj, ps.c, ps.c, f.h, f.h, gx, f.delta, f.has_delta);
-            ps.drhodt[i] = ps.drhodt[i] + mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
-            ps.drhodt[j] = ps.drhodt[j] + mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri);
+            acc(f, ps.drhodt[i], mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj));
+            acc(f, ps.drhodt[j], mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri));
             break;
         }
         case GC_PFN_CAUCHY_FLUID: {
@@ -443,18 +509,18 @@ void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, con
             double ri = ps.rho[i], rj = ps.rho[j];
             double mass = ps.mass;
             double dv[ND], hv[ND];
-            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            vdiff<ND>(vi, vj, dv);
             double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, ps.c, ps.c);
             cauchy<ND>(&ps.stress[i * ns], &ps.stress[j * ns], ns, ri, rj, gx, hv);
             for (int d = 0; d < ND; ++d) {
                 double t = mass * (hv[d] - piv * gx[d]);
-                ps.dvdt[i * ND + d] = ps.dvdt[i * ND + d] + t;
-                ps.dvdt[j * ND + d] = ps.dvdt[j * ND + d] - t;
+                acc(f, ps.dvdt[i * ND + d], t);
+                dec(f, ps.dvdt[j * ND + d], t);
             }
             double dr = dot<ND>(dv, gx);
             double psi = diffusion<ND>(dx, ri, rj, ps.c, ps.c, f.h, f.h, gx, f.delta, f.has_delta);
-            ps.drhodt[i] = ps.drhodt[i] + mass * (dr + psi / rj);
-            ps.drhodt[j] = ps.drhodt[j] + mass * (dr - psi / ri);
+            acc(f, ps.drhodt[i], mass * (dr + psi / rj));
+            acc(f, ps.drhodt[j], mass * (dr - psi / ri));
             break;
         }
         case GC_PFN_STRAIN_RATE:
@@ -462,19 +528,19 @@ void pfn_self(const Pfn& f, Sys& ps, int64_t i, int64_t j, const double* dx, con
             double ri = ps.rho[i], rj = ps.rho[j];
             double mass = ps.mass;
             double dv[ND], sr[6], w[3];
-            for (int d = 0; d < ND; ++d) dv[d] = ps.v[j * ND + d] - ps.v[i * ND + d];
+            vdiff<ND>(&ps.v[j * ND], &ps.v[i * ND], dv);
             strain_rate_t<ND>(dv, gx, ns, sr);
             double fi = mass / rj, fj = mass / ri;
             for (int k = 0; k < ns; ++k) {
-                ps.sr[i * ns + k] = ps.sr[i * ns + k] + sr[k] * fi;
-                ps.sr[j * ns + k] = ps.sr[j * ns + k] + sr[k] * fj;
+                acc(f, ps.sr[i * ns + k], sr[k] * fi);
+                acc(f, ps.sr[j * ns + k], sr[k] * fj);
             }
             if (f.kind == GC_PFN_STRAIN_RATE_VORTICITY) {
                 vorticity_t<ND>(dv, gx, w);
                 const int nv = ps.nvort;
                 for (int k = 0; k < nv; ++k) {
-                    ps.vort[i * nv + k] = ps.vort[i * nv + k] + w[k] * fi;
-                    ps.vort[j * nv + k] = ps.vort[j * nv + k] + w[k] * fj;
+                    acc(f, ps.vort[i * nv + k], w[k] * fi);
+                    acc(f, ps.vort[j * nv + k], w[k] * fj);
                 }
             }
             break;
@@ -569,40 +635,40 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
             case GC_PFN_FLUID: {
                 double pi_ = a.p[i];
                 double dv[ND];
-                for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+                vdiff<ND>(vi, vj, dv);
                 double piv = art_visc<ND>(dx, dv, f.h, ri, ri, f.alpha, f.beta, a.c, a.c);
                 double dh = pressure_coeff(pi_, pi_, ri, ri, f.S);
                 double s = mass * (dh - piv);
-                for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + s * gx[d];
+                for (int d = 0; d < ND; ++d) acc(f, a.dvdt[i * ND + d], s * gx[d]);
                 double dr = dot<ND>(dv, gx);
                 double psi = diffusion<ND>(dx, ri, ri, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
-                a.drhodt[i] = a.drhodt[i] + mass * (dr * cont_coeff(ri, ri, f.S) + psi / ri);
+                acc(f, a.drhodt[i], mass * (dr * cont_coeff(ri, ri, f.S) + psi / ri));
                 break;
             }
             case GC_PFN_CAUCHY_FLUID: {
                 double dv[ND], hv[ND];
-                for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+                vdiff<ND>(vi, vj, dv);
                 double piv = art_visc<ND>(dx, dv, f.h, ri, ri, f.alpha, f.beta, a.c, a.c);
                 const double* si = &a.stress[i * ns];
                 cauchy<ND>(si, si, ns, ri, ri, gx, hv);
                 for (int d = 0; d < ND; ++d)
-                    a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + mass * (hv[d] - piv * gx[d]);
+                    acc(f, a.dvdt[i * ND + d], mass * (hv[d] - piv * gx[d]));
                 double dr = dot<ND>(dv, gx);
                 double psi = diffusion<ND>(dx, ri, ri, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
-                a.drhodt[i] = a.drhodt[i] + mass * (dr + psi / ri);
+                acc(f, a.drhodt[i], mass * (dr + psi / ri));
                 break;
             }
             case GC_PFN_STRAIN_RATE:
             case GC_PFN_STRAIN_RATE_VORTICITY: {
                 double dv[ND], sr[6], w[3];
-                for (int d = 0; d < ND; ++d) dv[d] = vj[d] - vi[d];
+                vdiff<ND>(vj, vi, dv);
                 strain_rate_t<ND>(dv, gx, ns, sr);
                 double fi = mass / ri;
-                for (int k = 0; k < ns; ++k) a.sr[i * ns + k] = a.sr[i * ns + k] + sr[k] * fi;
+                for (int k = 0; k < ns; ++k) acc(f, a.sr[i * ns + k], sr[k] * fi);
                 if (f.kind == GC_PFN_STRAIN_RATE_VORTICITY) {
                     vorticity_t<ND>(dv, gx, w);
                     for (int k = 0; k < a.nvort; ++k)
-                        a.vort[i * a.nvort + k] = a.vort[i * a.nvort + k] + w[k] * fi;
+                        acc(f, a.vort[i * a.nvort + k], w[k] * fi);
                 }
                 break;
             }
@@ -613,11 +679,11 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
     double ri = a.rho[i], rj = b.rho[j];
     if (b.type == H_STATIC && (f.kind == GC_PFN_FLUID || f.kind == GC_PFN_CAUCHY_FLUID)) {
         double dv[ND];
-        for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+        vdiff<ND>(vi, vj, dv);
         double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, a.c);
         double rf = lennard_jones<ND>(dx, b.ljcut, a.c);
         double s = (-b.mass) * piv;
-        for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + (s * gx[d] + rf * dx[d]);
+        for (int d = 0; d < ND; ++d) acc(f, a.dvdt[i * ND + d], (s * gx[d] + rf * dx[d]));
         return;
     }
     if (f.kind == GC_PFN_FLUID_SOLID) {
@@ -626,19 +692,19 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
         Sys& bs = *b.sys;
         double pi_ = a.p[i];
         double dv[ND];
-        for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+        vdiff<ND>(vi, vj, dv);
         double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, bs.c);
         double dh = pressure_coeff(pi_, pi_, ri, rj, f.S);
         double c = dh - piv;
         for (int d = 0; d < ND; ++d) {
             double t = c * gx[d];
-            a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + b.mass * t;
-            bs.dvdt[j * ND + d] = bs.dvdt[j * ND + d] - a.mass * t;
+            acc(f, a.dvdt[i * ND + d], b.mass * t);
+            dec(f, bs.dvdt[j * ND + d], a.mass * t);
         }
         double dr = dot<ND>(dv, gx);
         double psi = diffusion<ND>(dx, ri, rj, a.c, bs.c, f.h, f.h, gx, f.delta, f.has_delta);
-        a.drhodt[i] = a.drhodt[i] + b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
-        bs.drhodt[j] = bs.drhodt[j] + a.mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri);
+        acc(f, a.drhodt[i], b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj));
+        acc(f, bs.drhodt[j], a.mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri));
         return;
     }
     if (f.kind == GC_PFN_FLUID && b.type == H_SYS && a.kind == GC_SYS_FLUID && b.sys->kind == GC_SYS_FLUID) {
@@ -647,7 +713,7 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
         Sys& bs = *b.sys;
         double pi_ = a.p[i], pj = b.p[j];
         double dv[ND];
-        for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+        vdiff<ND>(vi, vj, dv);
         double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, bs.c);
         double dh = pressure_coeff(pi_, pj, ri, rj, f.S);
         // artificial_surface_tension_coeff src/PairwisePhysics.jl:286-290
@@ -655,52 +721,52 @@ void pfn_coupled(const Pfn& f, Sys& a, const BView& b, int64_t i, int64_t j, con
         double c = dh + ast - piv;
         for (int d = 0; d < ND; ++d) {
             double t = c * gx[d];
-            a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + b.mass * t;
-            bs.dvdt[j * ND + d] = bs.dvdt[j * ND + d] - a.mass * t;
+            acc(f, a.dvdt[i * ND + d], b.mass * t);
+            dec(f, bs.dvdt[j * ND + d], a.mass * t);
         }
         double dr = dot<ND>(dv, gx);
         double psi = diffusion<ND>(dx, ri, rj, a.c, bs.c, f.h, f.h, gx, f.delta, f.has_delta);
-        a.drhodt[i] = a.drhodt[i] + b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
-        bs.drhodt[j] = bs.drhodt[j] + a.mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri);
+        acc(f, a.drhodt[i], b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj));
+        acc(f, bs.drhodt[j], a.mass * (dr * cont_coeff(rj, ri, f.S) - psi / ri));
         return;
     }
     switch (f.kind) {
         case GC_PFN_FLUID: {  // generic one-sided :193
             double pi_ = a.p[i], pj = b.p[j];
             double dv[ND];
-            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            vdiff<ND>(vi, vj, dv);
             double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, a.c);
             double dh = pressure_coeff(pi_, pj, ri, rj, f.S);
             double s = b.mass * (dh - piv);
-            for (int d = 0; d < ND; ++d) a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + s * gx[d];
+            for (int d = 0; d < ND; ++d) acc(f, a.dvdt[i * ND + d], s * gx[d]);
             double dr = dot<ND>(dv, gx);
             double psi = diffusion<ND>(dx, ri, rj, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
-            a.drhodt[i] = a.drhodt[i] + b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj);
+            acc(f, a.drhodt[i], b.mass * (dr * cont_coeff(ri, rj, f.S) + psi / rj));
             break;
         }
         case GC_PFN_CAUCHY_FLUID: {  // ghost one-sided :286
             double dv[ND], hv[ND];
-            for (int d = 0; d < ND; ++d) dv[d] = vi[d] - vj[d];
+            vdiff<ND>(vi, vj, dv);
             double piv = art_visc<ND>(dx, dv, f.h, ri, rj, f.alpha, f.beta, a.c, b.c);
             cauchy<ND>(&a.stress[i * ns], &b.stress[j * ns], ns, ri, rj, gx, hv);
             for (int d = 0; d < ND; ++d)
-                a.dvdt[i * ND + d] = a.dvdt[i * ND + d] + b.mass * (hv[d] - piv * gx[d]);
+                acc(f, a.dvdt[i * ND + d], b.mass * (hv[d] - piv * gx[d]));
             double dr = dot<ND>(dv, gx);
             double psi = diffusion<ND>(dx, ri, rj, a.c, a.c, f.h, f.h, gx, f.delta, f.has_delta);
-            a.drhodt[i] = a.drhodt[i] + b.mass * (dr + psi / rj);
+            acc(f, a.drhodt[i], b.mass * (dr + psi / rj));
             break;
         }
         case GC_PFN_STRAIN_RATE:
         case GC_PFN_STRAIN_RATE_VORTICITY: {  // generic one-sided :37/:97
             double dv[ND], sr[6], w[3];
-            for (int d = 0; d < ND; ++d) dv[d] = vj[d] - vi[d];
+            vdiff<ND>(vj, vi, dv);
             strain_rate_t<ND>(dv, gx, ns, sr);
             double fi = b.mass / rj;
-            for (int k = 0; k < ns; ++k) a.sr[i * ns + k] = a.sr[i * ns + k] + sr[k] * fi;
+            for (int k = 0; k < ns; ++k) acc(f, a.sr[i * ns + k], sr[k] * fi);
             if (f.kind == GC_PFN_STRAIN_RATE_VORTICITY) {
                 vorticity_t<ND>(dv, gx, w);
                 for (int k = 0; k < a.nvort; ++k)
-                    a.vort[i * a.nvort + k] = a.vort[i * a.nvort + k] + w[k] * fi;
+                    acc(f, a.vort[i * a.nvort + k], w[k] * fi);
             }
             break;
         }
@@ -721,7 +787,7 @@ inline void pair_self(const Pfn& f, const Kern& k, Sys& ps, int64_t i, int64_t j
         double gc = kernel_dw_dq(k, q) / (r * h);
         double w = f.kind == GC_PFN_XSPH ? kernel_w(k, q) : 0.0;
         double gx[ND];
-        for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
+        for (int d = 0; d < ND; ++d) gx[d] = g_mag_inputs ? std::fabs(gc * dx[d]) : gc * dx[d];
         pfn_self<ND>(f, ps, i, j, dx, gx, w);
     }
 }
@@ -738,7 +804,7 @@ inline void pair_coupled(const Pfn& f, const Kern& k, Sys& a, const BView& b, in
         double gc = kernel_dw_dq(k, q) / (r * h);
         double w = (f.kind == GC_PFN_XSPH || f.kind == GC_PFN_INTERPOLATE) ? kernel_w(k, q) : 0.0;
         double gx[ND];
-        for (int d = 0; d < ND; ++d) gx[d] = gc * dx[d];
+        for (int d = 0; d < ND; ++d) gx[d] = g_mag_inputs ? std::fabs(gc * dx[d]) : gc * dx[d];
         pfn_coupled<ND>(f, a, b, i, j, dx, gx, w, err);
     }
 }
@@ -1042,6 +1108,37 @@ int sort_order(const double* x, int64_t n, int nd, double cutoff, std::vector<in
     return 1;
 }
 
+// ------------------------------------------------- magnitude shadows
+// Test infrastructure, not part of the reference: with track_mag on, each
+// rate field (dvdt, drhodt, strain rate, vorticity) has a shadow holding
+// |initial value| + Σ|every term added since|, the per-particle scale on
+// which a result summed in another order is compared.
+void mag_set(const std::vector<double>& f, std::vector<double>& m) {
+    m.resize(f.size());
+    for (size_t k = 0; k < f.size(); ++k) m[k] = std::fabs(f[k]);
+}
+
+void mag_ensure(Sys& s) {
+    if (s.mstr.size() != s.stress.size()) s.mstr.assign(s.stress.size(), 0.0);
+    if (s.mstrain.size() != s.strain.size()) s.mstrain.assign(s.strain.size(), 0.0);
+    if (s.mvi.size() != s.v.size()) s.mvi.assign(s.v.size(), 0.0);
+    if (s.mrhoi.size() != s.rho.size()) s.mrhoi.assign(s.rho.size(), 0.0);
+    if (s.mxi.size() != s.x.size()) s.mxi.assign(s.x.size(), 0.0);
+    if (s.mdvdt.size() != s.dvdt.size()) mag_set(s.dvdt, s.mdvdt);
+    if (s.mdrhodt.size() != s.drhodt.size()) mag_set(s.drhodt, s.mdrhodt);
+    if (s.msr.size() != s.sr.size()) mag_set(s.sr, s.msr);
+    if (s.mvort.size() != s.vort.size()) mag_set(s.vort, s.mvort);
+}
+
+void mag_swap(Sys& s) {
+    s.dvdt.swap(s.mdvdt);
+    s.drhodt.swap(s.mdrhodt);
+    s.sr.swap(s.msr);
+    s.vort.swap(s.mvort);
+}
+
+void mag_permute(Sys& s, const std::vector<int64_t>& perm);
+
 void permute_system(Sys& s, const std::vector<int64_t>& perm) {
     const int nd = s.nd, ns = s.ns;
     apply_perm(s.x, perm, nd);
@@ -1061,6 +1158,19 @@ void permute_system(Sys& s, const std::vector<int64_t>& perm) {
         apply_perm(s.strain, perm, ns);
         apply_perm(s.strainp, perm, ns);
     }
+    mag_permute(s, perm);
+}
+
+void mag_permute(Sys& s, const std::vector<int64_t>& perm) {
+    if (s.mstr.size() == s.stress.size() && !s.mstr.empty()) apply_perm(s.mstr, perm, s.ns);
+    if (s.mstrain.size() == s.strain.size() && !s.mstrain.empty()) apply_perm(s.mstrain, perm, s.ns);
+    if (s.mvi.size() == s.v.size() && !s.mvi.empty()) apply_perm(s.mvi, perm, s.nd);
+    if (s.mrhoi.size() == s.rho.size() && !s.mrhoi.empty()) apply_perm(s.mrhoi, perm, 1);
+    if (s.mxi.size() == s.x.size() && !s.mxi.empty()) apply_perm(s.mxi, perm, s.nd);
+    if (s.mdvdt.size() == s.dvdt.size() && !s.mdvdt.empty()) apply_perm(s.mdvdt, perm, s.nd);
+    if (s.mdrhodt.size() == s.drhodt.size() && !s.mdrhodt.empty()) apply_perm(s.mdrhodt, perm, 1);
+    if (s.msr.size() == s.sr.size() && !s.msr.empty()) apply_perm(s.msr, perm, s.ns);
+    if (s.mvort.size() == s.vort.size() && !s.mvort.empty()) apply_perm(s.mvort, perm, s.nvort);
 }
 
 int sort_system(Sys& s, double cutoff, std::vector<int64_t>* perm_out) {
@@ -1086,6 +1196,7 @@ int sort_system(Sys& s, double cutoff, std::vector<int64_t>* perm_out) {
             apply_perm(s.strain, perm, ns);
             apply_perm(s.strainp, perm, ns);
         }
+        mag_permute(s, perm);
     }
     if (perm_out) *perm_out = perm;
     return GC_OK;
@@ -1216,8 +1327,29 @@ void update_ghost(oracle_ctx* ctx, Ghost& g, int stage) {
 
 // --------------------------------------------------------------- updaters
 // src/StateUpdaters.jl
+// The magnitude shadows of a plane-strain stress update from the strain
+// rate and vorticity shadows (test infrastructure; a no-op unless the
+// shadows are kept).
+void mag_stress_increment(Sys& ps, int64_t i, double E, double nu, double dt) {
+    if (ps.mstr.size() != ps.stress.size() || ps.msr.size() != ps.sr.size() || ps.mvort.size() != ps.vort.size())
+        return;
+    const double* m = &ps.msr[i * 4];
+    const double* s = &ps.stress[i * 4];
+    const double D0 = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double mxx = m[0] * dt, myy = m[1] * dt, mzz = m[2] * dt, mxy = m[3] * dt;
+    const double mw = ps.mvort[i * ps.nvort] * dt;
+    double* o = &ps.mstr[i * 4];
+    o[0] += D0 * ((1.0 - nu) * mxx + nu * myy + nu * mzz) + 2.0 * std::fabs(s[3]) * mw;
+    o[1] += D0 * (nu * mxx + (1.0 - nu) * myy + nu * mzz) + 2.0 * std::fabs(s[3]) * mw;
+    o[2] += D0 * (nu * mxx + nu * myy + (1.0 - nu) * mzz);
+    o[3] += D0 * (1.0 - 2.0 * nu) * mxy + (std::fabs(s[0]) + std::fabs(s[1])) * mw;
+    if (ps.mstrain.size() == ps.strain.size())
+        for (int q = 0; q < 4; ++q) ps.mstrain[i * 4 + q] += m[q] * dt;
+}
+
 void ep_update(Sys& ps, int64_t i, const Upd& u, double dt) {
     const double E = u.prm[0], nu = u.prm[1], phi = u.prm[2], psi = u.prm[3], coh = u.prm[4];
+    mag_stress_increment(ps, i, E, nu, dt);
     double* s = &ps.stress[i * 4];
     const double* er = &ps.sr[i * 4];
     double w = ps.vort[i * ps.nvort];
@@ -1292,6 +1424,7 @@ void ep_update(Sys& ps, int64_t i, const Upd& u, double dt) {
 
 void hooke_update(Sys& ps, int64_t i, const Upd& u, double dt) {
     const double E = u.prm[0], nu = u.prm[1];
+    mag_stress_increment(ps, i, E, nu, dt);
     double* s = &ps.stress[i * 4];
     const double* er = &ps.sr[i * 4];
     double w = ps.vort[i * ps.nvort];
@@ -1331,6 +1464,10 @@ void apply_updater(Sys& ps, const Upd& u, double dt) {
                     for (int d = 0; d < ps.nd; ++d) ps.dvdt[i * ps.nd + d] = 0.0;
                 if (mask & (1u << GC_FIELD_DRHODT)) ps.drhodt[i] = 0.0;
             }
+            if (mask & (1u << GC_FIELD_STRAIN_RATE)) std::fill(ps.msr.begin(), ps.msr.end(), 0.0);
+            if (mask & (1u << GC_FIELD_VORTICITY)) std::fill(ps.mvort.begin(), ps.mvort.end(), 0.0);
+            if (mask & (1u << GC_FIELD_DVDT)) std::fill(ps.mdvdt.begin(), ps.mdvdt.end(), 0.0);
+            if (mask & (1u << GC_FIELD_DRHODT)) std::fill(ps.mdrhodt.begin(), ps.mdrhodt.end(), 0.0);
             break;
         }
         case GC_UPD_TAIT_EOS: {
@@ -1508,12 +1645,16 @@ int check_combo(oracle_ctx* ctx, const Inter& it, int pk) {
     return GC_OK;
 }
 
-int sweep(oracle_ctx* ctx, Inter& it, int stage) {
+// mag: the magnitude pass of track_mag (rate fields swapped with their
+// shadows by the caller); functors that write no rate field are skipped.
+int sweep(oracle_ctx* ctx, Inter& it, int stage, bool mag = false) {
     if (stage < 1 || stage > it.nstages) return GC_OK;
     int pk = it.pk[stage - 1];
     if (pk == GC_PFN_NONE) return GC_OK;
+    if (mag && (pk == GC_PFN_INTERPOLATE || pk == GC_PFN_NEIGHBOR_COUNT || pk == GC_PFN_XSPH)) return GC_OK;
     if (!it.grid) return fail(ctx, GC_ERR_STATE, "sweep before create_grid");
     Pfn f = make_pfn(pk, it.pp[stage - 1].data());
+    f.mag = mag;
     const int nd = ctx->sys[it.a].nd;
     if (it.b < 0) {
         if (nd == 2) sweep_self<2>(ctx, it, f);
@@ -1582,11 +1723,20 @@ void zero_field(Sys& s, int field) {
     switch (field) {
         case GC_FIELD_V: std::fill(s.v.begin(), s.v.end(), 0.0); break;
         case GC_FIELD_RHO: std::fill(s.rho.begin(), s.rho.end(), 0.0); break;
-        case GC_FIELD_DVDT: std::fill(s.dvdt.begin(), s.dvdt.end(), 0.0); break;
-        case GC_FIELD_DRHODT: std::fill(s.drhodt.begin(), s.drhodt.end(), 0.0); break;
+        case GC_FIELD_DVDT:
+            std::fill(s.dvdt.begin(), s.dvdt.end(), 0.0);
+            std::fill(s.mdvdt.begin(), s.mdvdt.end(), 0.0);
+            break;
+        case GC_FIELD_DRHODT:
+            std::fill(s.drhodt.begin(), s.drhodt.end(), 0.0);
+            std::fill(s.mdrhodt.begin(), s.mdrhodt.end(), 0.0);
+            break;
         case GC_FIELD_P: std::fill(s.p.begin(), s.p.end(), 0.0); break;
         case GC_FIELD_STRESS: std::fill(s.stress.begin(), s.stress.end(), 0.0); break;
-        case GC_FIELD_STRAIN_RATE: std::fill(s.sr.begin(), s.sr.end(), 0.0); break;
+        case GC_FIELD_STRAIN_RATE:
+            std::fill(s.sr.begin(), s.sr.end(), 0.0);
+            std::fill(s.msr.begin(), s.msr.end(), 0.0);
+            break;
         default: break;
     }
 }
@@ -1643,8 +1793,65 @@ int sweep_all_stages(oracle_ctx* ctx, int nst, double dt) {
             int st = sweep(ctx, it, stage);
             if (st) return st;
         }
+        if (ctx->track_mag) {  // the same sweeps again, summing |term| into the shadows
+            for (auto& s : ctx->sys) {
+                mag_ensure(s);
+                mag_swap(s);
+            }
+            g_mag_inputs = ctx->track_mag == 2;
+            int st = GC_OK;
+            for (auto& it : ctx->inters) {
+                if (it.probe) continue;
+                st = sweep(ctx, it, stage, true);
+                if (st) break;
+            }
+            g_mag_inputs = 0;
+            for (auto& s : ctx->sys) mag_swap(s);
+            if (st) return st;
+        }
     }
     return GC_OK;
+}
+
+// Shadows of the rate fields just reset to their source terms.
+void mag_reset_rates(oracle_ctx* ctx, Sys& s) {
+    if (!ctx->track_mag) return;
+    mag_set(s.dvdt, s.mdvdt);
+    mag_set(s.drhodt, s.mdrhodt);
+}
+
+// Damping's term -(Γ/dt)·v added to the shadow of dvdt.
+void mag_damping(oracle_ctx* ctx, Sys& s, double gdt) {
+    if (!ctx->track_mag) return;
+    mag_ensure(s);
+    for (int64_t i = 0; i < s.n * s.nd; ++i) s.mdvdt[i] = s.mdvdt[i] + std::fabs(gdt * s.v[i]);
+}
+
+// The integrated-state shadows after a step's full update q = q0 + dt·rate
+// (LeapFrog: the rates' shadows; RK4: the weighted sum of its four).
+void mag_integrate(oracle_ctx* ctx, Sys& s, double dt, const std::vector<double>& mv,
+                   const std::vector<double>& mrho) {
+    if (!ctx->track_mag) return;
+    mag_ensure(s);
+    for (int64_t i = 0; i < s.n * s.nd; ++i) s.mvi[i] = s.mvi[i] + dt * mv[i];
+    for (int64_t i = 0; i < s.n; ++i) s.mrhoi[i] = s.mrhoi[i] + dt * mrho[i];
+}
+
+// XSPH's velocity adjustment added to the v shadow; the position update
+// x += dt·v added to the x shadow with v's scale max(|v|, M(v)).
+void mag_positions(oracle_ctx* ctx, Sys& s, double dt, bool xsph) {
+    if (!ctx->track_mag) return;
+    mag_ensure(s);
+    if (xsph)
+        for (int64_t i = 0; i < s.n * s.nd; ++i) s.mvi[i] = s.mvi[i] + std::fabs(s.vadj[i]);
+    for (int64_t i = 0; i < s.n * s.nd; ++i)
+        s.mxi[i] = s.mxi[i] + dt * std::max(std::fabs(s.v[i]), s.mvi[i]);
+}
+
+bool any_xsph(oracle_ctx* ctx) {
+    for (auto& it : ctx->inters)
+        if (it.vk != GC_PFN_NONE) return true;
+    return false;
 }
 
 // _prepare_grids! :364-379: ghosts, ghost sort, virtual (source) sort, grids
@@ -1770,6 +1977,7 @@ int step_once(oracle_ctx* ctx, double dt) {
         for (int64_t i = 0; i < s.n; ++i)
             for (int d = 0; d < nd; ++d) s.dvdt[i * nd + d] = s.srcv[d];
         for (int64_t i = 0; i < s.n; ++i) s.drhodt[i] = s.srcrho;
+        mag_reset_rates(ctx, s);
     }
     // 7. ghost kinematics
     for (auto& g : ctx->ghosts) ghost_kinematics(ctx, g);
@@ -1782,14 +1990,20 @@ int step_once(oracle_ctx* ctx, double dt) {
     if (ctx->gamma != 0.0) {
         const double gdt = ctx->gamma / dt;
         for (auto& s : ctx->sys)
-            if (!s.vsrc)
+            if (!s.vsrc) {
                 for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
+                mag_damping(ctx, s, gdt);
+            }
     }
     // 9. full step: q = q0 + dt * dqdt
     for (auto& s : ctx->sys) {
         if (s.vsrc) continue;
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.dvdt[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.drhodt[i], s.q0rho[i]);
+        if (ctx->track_mag) {
+            mag_ensure(s);
+            mag_integrate(ctx, s, dt, s.mdvdt, s.mdrhodt);
+        }
     }
     // 10. XSPH correction
     {
@@ -1797,9 +2011,12 @@ int step_once(oracle_ctx* ctx, double dt) {
         if (st) return st;
     }
     // 11. positions, then the virtual systems'
+    const bool xs = any_xsph(ctx);
     for (auto& s : ctx->sys)
-        if (!s.vsrc)
+        if (!s.vsrc) {
             for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+            mag_positions(ctx, s, dt, xs);
+        }
     update_virtual_positions(ctx, dt);
     ctx->steps += 1;
     return GC_OK;
@@ -1827,6 +2044,10 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         s.q0rho = s.rho;
         s.accv.assign(s.v.size(), 0.0);
         s.accrho.assign(s.rho.size(), 0.0);
+        if (ctx->track_mag) {
+            s.accmv.assign(s.v.size(), 0.0);
+            s.accmrho.assign(s.rho.size(), 0.0);
+        }
     }
     // 3-5. ghosts, ghost sort, virtual sort, grids (:787-788)
     {
@@ -1849,6 +2070,7 @@ int step_rk4(oracle_ctx* ctx, double dt) {
             for (int64_t i = 0; i < s.n; ++i)
                 for (int d = 0; d < nd; ++d) s.dvdt[i * nd + d] = s.srcv[d];
             for (int64_t i = 0; i < s.n; ++i) s.drhodt[i] = s.srcrho;
+            mag_reset_rates(ctx, s);
         }
         // 7. ghost kinematics (:805-807)
         for (auto& g : ctx->ghosts) ghost_kinematics(ctx, g);
@@ -1861,13 +2083,20 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         if (ctx->gamma != 0.0) {
             const double gdt = ctx->gamma / dt;
             for (auto& s : ctx->sys)
-                if (!s.vsrc)
+                if (!s.vsrc) {
                     for (int64_t i = 0; i < s.n * s.nd; ++i) s.dvdt[i] = s.dvdt[i] - gdt * s.v[i];
+                    mag_damping(ctx, s, gdt);
+                }
         }
         for (auto& s : ctx->sys) {
             if (s.vsrc) continue;
             for (int64_t i = 0; i < s.n * s.nd; ++i) s.accv[i] = s.accv[i] + weight[rk] * s.dvdt[i];
             for (int64_t i = 0; i < s.n; ++i) s.accrho[i] = std::fma(weight[rk], s.drhodt[i], s.accrho[i]);
+            if (ctx->track_mag) {
+                mag_ensure(s);
+                for (int64_t i = 0; i < s.n * s.nd; ++i) s.accmv[i] = s.accmv[i] + weight[rk] * s.mdvdt[i];
+                for (int64_t i = 0; i < s.n; ++i) s.accmrho[i] = s.accmrho[i] + weight[rk] * s.mdrhodt[i];
+            }
         }
     }
     // 9. q = q0 + dt·acc (:818)
@@ -1875,6 +2104,7 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         if (s.vsrc) continue;
         for (int64_t i = 0; i < s.n * s.nd; ++i) s.v[i] = s.q0v[i] + dt * s.accv[i];
         for (int64_t i = 0; i < s.n; ++i) s.rho[i] = std::fma(dt, s.accrho[i], s.q0rho[i]);
+        mag_integrate(ctx, s, dt, s.accmv, s.accmrho);
     }
     // 10. XSPH correction (:821)
     {
@@ -1882,9 +2112,12 @@ int step_rk4(oracle_ctx* ctx, double dt) {
         if (st) return st;
     }
     // 11. positions (:824), then the virtual systems' (:825)
+    const bool xs = any_xsph(ctx);
     for (auto& s : ctx->sys)
-        if (!s.vsrc)
+        if (!s.vsrc) {
             for (int64_t i = 0; i < s.n * s.nd; ++i) s.x[i] = s.x[i] + dt * s.v[i];
+            mag_positions(ctx, s, dt, xs);
+        }
     update_virtual_positions(ctx, dt);
     ctx->steps += 1;
     return GC_OK;
@@ -2293,6 +2526,79 @@ int oracle_set_field(oracle_ctx* ctx, int handle, int field, const void* host, s
     }
     std::vector<double>* vec = field_vec(s, field);
     std::memcpy(vec->data(), host, bytes);
+    if (ctx->track_mag) {
+        mag_ensure(s);
+        if (field == GC_FIELD_V) std::fill(s.mvi.begin(), s.mvi.end(), 0.0);
+        if (field == GC_FIELD_RHO) std::fill(s.mrhoi.begin(), s.mrhoi.end(), 0.0);
+        if (field == GC_FIELD_X) std::fill(s.mxi.begin(), s.mxi.end(), 0.0);
+        if (field == GC_FIELD_STRESS) std::fill(s.mstr.begin(), s.mstr.end(), 0.0);
+        if (field == GC_FIELD_STRAIN) std::fill(s.mstrain.begin(), s.mstrain.end(), 0.0);
+        if (field == GC_FIELD_DVDT) mag_set(s.dvdt, s.mdvdt);
+        if (field == GC_FIELD_DRHODT) mag_set(s.drhodt, s.mdrhodt);
+        if (field == GC_FIELD_STRAIN_RATE) mag_set(s.sr, s.msr);
+        if (field == GC_FIELD_VORTICITY) mag_set(s.vort, s.mvort);
+    }
+    return GC_OK;
+}
+
+// Test infrastructure: keep the rate fields' magnitude shadows, summing
+// each pair term's magnitude (mode 1) or the magnitude it takes with every
+// difference of its inputs replaced by the sum of their magnitudes (mode 2);
+// 0 turns them off.  Switching on sets every shadow to |field| (rates) or 0
+// (integrated fields).
+int oracle_set_track_magnitude(oracle_ctx* ctx, int on) {
+    if (on < 0 || on > 2) return fail(ctx, GC_ERR_ARG, "magnitude mode is 0, 1 or 2");
+    ctx->track_mag = on;
+    for (auto& s : ctx->sys) {
+        if (ctx->track_mag) {
+            mag_set(s.dvdt, s.mdvdt);
+            mag_set(s.drhodt, s.mdrhodt);
+            mag_set(s.sr, s.msr);
+            mag_set(s.vort, s.mvort);
+            s.mvi.assign(s.v.size(), 0.0);
+            s.mrhoi.assign(s.rho.size(), 0.0);
+            s.mxi.assign(s.x.size(), 0.0);
+            s.mstr.assign(s.stress.size(), 0.0);
+            s.mstrain.assign(s.strain.size(), 0.0);
+        } else {
+            s.mstr.clear();
+            s.mstrain.clear();
+            s.mvi.clear();
+            s.mrhoi.clear();
+            s.mxi.clear();
+            s.mdvdt.clear();
+            s.mdrhodt.clear();
+            s.msr.clear();
+            s.mvort.clear();
+        }
+    }
+    return GC_OK;
+}
+
+// The magnitude shadow of a rate field (dvdt, drhodt, strain rate,
+// vorticity) or of an integrated field (v, rho, x, stress, strain: the
+// summed increments' magnitudes) of a system, in the layout of
+// oracle_get_field.
+int oracle_get_magnitude(oracle_ctx* ctx, int handle, int field, void* host, size_t bytes) {
+    if (!ctx->track_mag) return fail(ctx, GC_ERR_STATE, "magnitude tracking is off");
+    if (handle < 0 || handle >= (int)ctx->handles.size()) return fail(ctx, GC_ERR_ARG, "bad handle");
+    const Handle& h = ctx->handles[handle];
+    if (h.type != H_SYS) return fail(ctx, GC_ERR_ARG, "magnitudes are kept for systems only");
+    Sys& s = ctx->sys[h.idx];
+    mag_ensure(s);
+    const std::vector<double>* m = field == GC_FIELD_DVDT          ? &s.mdvdt
+                                   : field == GC_FIELD_DRHODT      ? &s.mdrhodt
+                                   : field == GC_FIELD_STRAIN_RATE ? &s.msr
+                                   : field == GC_FIELD_VORTICITY   ? &s.mvort
+                                   : field == GC_FIELD_V           ? &s.mvi
+                                   : field == GC_FIELD_RHO         ? &s.mrhoi
+                                   : field == GC_FIELD_X           ? &s.mxi
+                                   : field == GC_FIELD_STRESS      ? &s.mstr
+                                   : field == GC_FIELD_STRAIN      ? &s.mstrain
+                                                                   : nullptr;
+    if (!m) return fail(ctx, GC_ERR_ARG, "no magnitude shadow for this field");
+    if (bytes != m->size() * 8) return fail(ctx, GC_ERR_ARG, "byte count mismatch");
+    if (bytes) std::memcpy(host, m->data(), bytes);
     return GC_OK;
 }
 

@@ -74,6 +74,8 @@ def lib():
             "oracle_kernel_dw_dq": (ct.c_double, [ct.c_int, ct.c_int, ct.c_double, ct.c_double]),
             "oracle_powi": (ct.c_double, [ct.c_double, ct.c_int64]),
             "oracle_steps": (ct.c_int64, [ct.c_void_p]),
+            "oracle_set_track_magnitude": (ct.c_int, [ct.c_void_p, ct.c_int]),
+            "oracle_get_magnitude": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_size_t]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -96,12 +98,14 @@ def _a(x, dt):
 class OracleBackend:
     """Same interface as CudaBackend; a single instance (inst must be 0)."""
 
-    def __init__(self, threads: int = 1):
+    def __init__(self, threads: int = 1, track_magnitude=False):
         self.L = lib()
         self.ctx = ct.c_void_p()
         self.L.oracle_create(ct.byref(self.ctx))
         self.L.oracle_set_threads(self.ctx, threads)
         self._inst = 0
+        # False/0: off; True/1: over the pair terms; 2: over the inputs
+        self._track = int(track_magnitude)
 
     def _chk(self, st, where=""):
         if st != 0:
@@ -203,7 +207,23 @@ class OracleBackend:
         self._chk(self.L.oracle_set_integrator_kind(self.ctx, kind), "set_integrator_kind")
 
     def finalize(self):
-        pass
+        if self._track:
+            self.set_track_magnitude(self._track)
+
+    def set_track_magnitude(self, mode):
+        """Keep the magnitude shadows, the per-particle scale of the parity
+        tests: mode 1 sums each pair term's magnitude (|initial| +
+        Σ|terms|), mode 2 the magnitude each term takes with every
+        difference of its inputs replaced by the sum of their magnitudes
+        (inputs that carry relative errors); 0 turns them off."""
+        self._track = int(mode)
+        self._chk(self.L.oracle_set_track_magnitude(self.ctx, self._track), "set_track_magnitude")
+
+    def magnitude(self, inst, handle, field, out):
+        """The magnitude shadow of a rate field, in download_into's layout."""
+        self._chk(self.L.oracle_get_magnitude(self.ctx, handle, field, out.ctypes.data, out.nbytes),
+                  "get_magnitude")
+        return out
 
     def set_precision(self, mode):
         pass

@@ -1,6 +1,8 @@
 """Helpers shared by the tests: backend construction and small builders."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -8,11 +10,27 @@ import grasph_b200 as G
 from grasph_b200 import consts as C
 
 
-def make_backend(name):
+def oracle_threads():
+    """Host threads for oracle runs at the configs' sizes."""
+    return max(1, min(32, os.cpu_count() or 1))
+
+
+def make_backend(name, track=False, threads=1):
+    """`track`: the oracle keeps magnitude shadows, the per-particle scale
+    of tests/parity.py (True or 1: over the pair terms; 2: over the
+    inputs)."""
     if name == "oracle":
         from pyoracle import OracleBackend
-        return OracleBackend()
+        return OracleBackend(threads=threads, track_magnitude=track)
     return G.CudaBackend()
+
+
+def step_dt(lf, cfl):
+    """The step's dt, CFL·h_min/c_max over the integrator's systems
+    (src/TimeIntegration.jl:598)."""
+    h = min(si.kernel.h for si in lf.interactions)
+    c = max(ps.c for ps in lf.systems)
+    return cfl * h / c
 
 
 BACKENDS = ["oracle", pytest.param("cuda", marks=pytest.mark.gpu)]

@@ -1,54 +1,59 @@
 """Parity of libgrasph_cuda.so against the CPU oracle on identical inputs.
 
 Bit-exact: sort permutation (particle ids), grid origin/extent/cell_start,
-per-particle neighbour counts, ghost sets.  FP64 physics after one step:
-within 1e-10 of the field's scale (summation order is the only difference:
-the device gathers each particle's pair terms, the reference scatters them
-in colour order).  After several steps: 1e-8.
+per-particle neighbour counts, ghost sets.  Physics on the per-particle
+scale of tests/parity.py (max(|ref|, Σ|terms|) for the rate fields; the
+device sums each particle's pair terms in another order than the
+reference's colour order, the terms themselves are identical): FP64 within
+1e-10 after one step; after 20 steps the state within 1e-8 of its
+integrated scale and one further step from the device's state at 1e-10.
+
+The configurations' own sizes are covered too: the 2-D dam break of 50×100
+particles (one step, and 1000 steps), the 2-D column of 400×200 particles at
+h = 1.5dx, where lattice pairs sit exactly on the 2h cutoff (one step,
+neighbour counts and grids; 1000 FP32-compensated steps against the FP64
+oracle), and the 3-D dam break of 1,000,000 particles (one step:
+permutation, grids, neighbour counts and physics).
 """
+import time
+
 import numpy as np
 import pytest
 
 import grasph_b200 as G
 from grasph_b200 import scenarios
-from gc_helpers import make_backend
+from gc_helpers import make_backend, oracle_threads
+import parity
 
 pytestmark = pytest.mark.gpu
 
 ONE_STEP_TOL = 1e-10
 MULTI_STEP_TOL = 1e-8
+# 1000 FP64 steps of the 2-D dam break: the two summation orders' last-ulp
+# differences feed back through the state every step
+LONG_RUN_TOL = 1e-8
 
 
-def _pair(builder, **kw):
+def _pair(builder, prec=G.PRECISION_FP64, threads=1, mode=None, **kw):
+    """Device and oracle sessions of one scenario.  mode: the oracle's
+    shadows (tests/parity.py): over the terms for one FP64 step (default),
+    over the inputs for the compensated mode."""
     lf_g, meta = builder(**kw)
     lf_c, _ = builder(**kw)
-    g = G.Session([lf_g], backend=make_backend("cuda"))
-    c = G.Session([lf_c], backend=make_backend("oracle"))
+    if mode is None:
+        mode = parity.one_step_mode(lf_g, prec)
+    g = G.Session([lf_g], backend=make_backend("cuda"), precision=prec)
+    c = G.Session([lf_c], backend=make_backend("oracle", track=mode, threads=threads))
     g.push()
     c.push()
     return lf_g, lf_c, g, c, meta
 
 
-def _cmp_field(a, b, tol, name):
-    a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
-    scale = max(np.abs(b).max(), 1e-300)
-    err = np.abs(a - b).max() / scale
-    assert err <= tol, f"{name}: max error {err:.3e} of scale {scale:.3e} exceeds {tol}"
-    return err
-
-
-def _compare_systems(lf_g, lf_c, tol, exact_ids=True, rate_tol=None):
-    """rate_tol (default tol): tolerance of the rate fields (dv/dt, dρ/dt,
-    strain rate, vorticity), which hold the last sweep's pair sums as they are."""
-    rates = ("dvdt", "drhodt", "strain_rate", "vorticity")
-    for sg, sc in zip(lf_g.systems, lf_c.systems):
-        if exact_ids:
-            assert np.array_equal(sg.id, sc.id), f"{sg.name}: permutation differs"
-        for name, _ in sg.particle_fields():
-            if name in ("id", "v_adjustment"):
-                continue
-            t = rate_tol if (rate_tol is not None and name in rates) else tol
-            _cmp_field(getattr(sg, name), getattr(sc, name), t, f"{sg.name}.{name}")
+def _run(lf_g, lf_c, g, c, meta, nsteps):
+    g.step(nsteps, meta["cfl"])
+    c.step(nsteps, meta["cfl"])
+    g.pull()
+    c.pull()
 
 
 SMALL = {
@@ -56,6 +61,8 @@ SMALL = {
     "dambreak_3d": (scenarios.dambreak_3d, dict(nx=8, ny=6, nz=12, dx=0.05, tank=(1.0, 0.5, 1.0))),
     "column": (scenarios.column_collapse, dict(nx=40, ny=20, dx=0.005)),
     "granular": (scenarios.granular_column, dict(nfx=40, nfy=20, dx=0.005)),
+    "dambreak_lj_2d": (scenarios.dambreak_lj_2d, dict(nfx=20, nfy=20, nbx=60, nby=32)),
+    "dambreak_lj_3d": (scenarios.dambreak_lj_3d, dict(nfx=10, nfy=6, nfz=10, nbx=30, nby=6, nbz=16)),
 }
 
 
@@ -63,32 +70,25 @@ SMALL = {
 def test_one_step_parity(case):
     builder, kw = SMALL[case]
     lf_g, lf_c, g, c, meta = _pair(builder, **kw)
-    g.step(1, meta["cfl"])
-    c.step(1, meta["cfl"])
-    g.pull()
-    c.pull()
-    _compare_systems(lf_g, lf_c, ONE_STEP_TOL)
+    _run(lf_g, lf_c, g, c, meta, 1)
+    parity.compare_integrators(lf_g, lf_c, c, ONE_STEP_TOL)
 
 
 @pytest.mark.parametrize("case", list(SMALL))
 def test_multi_step_parity(case):
+    """20 steps: the state fields on the integrated scale; then one more
+    step from the device's state with every field at the one-step bar."""
     builder, kw = SMALL[case]
-    lf_g, lf_c, g, c, meta = _pair(builder, **kw)
-    g.step(20, meta["cfl"])
-    c.step(20, meta["cfl"])
-    g.pull()
-    c.pull()
-    _compare_systems(lf_g, lf_c, MULTI_STEP_TOL, exact_ids=False)
+    lf_g, lf_c, g, c, meta = _pair(builder, mode=parity.INPUTS, **kw)
+    _run(lf_g, lf_c, g, c, meta, 20)
+    parity.compare_integrators(lf_g, lf_c, c, MULTI_STEP_TOL, exact_ids=False, skip=parity.RATES)
+    parity.one_step_from_device_state(lf_g, lf_c, g, c, meta["cfl"], ONE_STEP_TOL)
 
 
-@pytest.mark.parametrize("case", list(SMALL))
-def test_neighbour_counts_and_grids_bit_exact(case):
-    builder, kw = SMALL[case]
-    lf_g, lf_c, g, c, meta = _pair(builder, **kw)
-    # one step so the systems are sorted and ghosts generated, then rebuild
-    # the grids on identical (downloaded) state in both backends
-    g.step(1, meta["cfl"])
-    g.pull()
+def _grids_and_counts(lf_g, lf_c, g, c, threads=1):
+    """Rebuild every grid on identical (downloaded) state in both backends:
+    origin, extent and cell_start bit-exact, per-particle neighbour counts
+    bit-exact against the oracle's own sweep loops."""
     for sg, sc in zip(lf_g.systems, lf_c.systems):
         for name, _ in sg.particle_fields():
             getattr(sc, name)[...] = getattr(sg, name)
@@ -109,17 +109,26 @@ def test_neighbour_counts_and_grids_bit_exact(case):
         assert np.array_equal(mg_g, mg_c) and np.array_equal(ng_g, ng_c)
         assert np.array_equal(cs_g, cs_c)
         cnt = g.neighbor_counts(si_g)
-        # oracle counts: a counting sweep over the same interaction
-        ref = _oracle_counts(lf_c, si_c, c)
+        ref = _oracle_counts(si_c, threads)
         assert np.array_equal(cnt, ref), f"neighbour counts differ ({np.sum(cnt != ref)} particles)"
 
 
-def _oracle_counts(lf_c, si_c, sess):
+@pytest.mark.parametrize("case", list(SMALL))
+def test_neighbour_counts_and_grids_bit_exact(case):
+    builder, kw = SMALL[case]
+    lf_g, lf_c, g, c, meta = _pair(builder, **kw)
+    # one step so the systems are sorted and ghosts generated
+    g.step(1, meta["cfl"])
+    g.pull()
+    _grids_and_counts(lf_g, lf_c, g, c)
+
+
+def _oracle_counts(si_c, threads=1):
     """Per-particle accepted-pair counts from the oracle's own sweep loops."""
     a = si_c.system_a
     b = si_c.system_b
     from grasph_b200.model import GhostParticleSystem, AbstractBoundarySystem
-    # Build a fresh oracle session with a counting functor on the same state.
+    # a fresh oracle session with a counting functor on the same positions
     sys_a = G.BasicParticleSystem("a", a.n, a.ndims, 1.0, 1.0)
     sys_a.x[:] = a.x
     systems = [sys_a]
@@ -140,12 +149,125 @@ def _oracle_counts(lf_c, si_c, sess):
         systems.append(sys_b)
         si = G.SystemInteraction(si_c.kernel, G.CountingPfn(), sys_a, sys_b)
     lf = G.LeapFrogTimeIntegrator(systems, [si])
-    s = G.Session([lf], backend=make_backend("oracle"))
+    s = G.Session([lf], backend=make_backend("oracle", threads=threads))
     s.push()
     s.create_grid(si)
     s.sweep(si, 1)
     s.pull()
     return sys_a.drhodt.astype(np.int32)
+
+
+# ------------------------------------------------- the configurations' sizes
+
+def test_c0_dambreak_2d_full_size():
+    """50×100 fluid particles, dx = 0.02, 3-layer dynamic walls
+    in a 4×4 m tank: one step at 1e-10, then to 1000 steps at LONG_RUN_TOL,
+    with the permutation still bit-exact."""
+    t = oracle_threads()
+    lf_g, lf_c, g, c, meta = _pair(scenarios.dambreak_2d, threads=t)
+    _run(lf_g, lf_c, g, c, meta, 1)
+    parity.compare_integrators(lf_g, lf_c, c, ONE_STEP_TOL)
+    c.backend.set_track_magnitude(parity.INPUTS)
+    _run(lf_g, lf_c, g, c, meta, 999)
+    rep = {}
+    parity.compare_integrators(lf_g, lf_c, c, LONG_RUN_TOL, exact_ids=False, skip=parity.RATES, report=rep)
+    print("C0 after 1000 steps:", rep)
+    assert np.array_equal(lf_g.systems[0].id, lf_c.systems[0].id)
+    parity.one_step_from_device_state(lf_g, lf_c, g, c, meta["cfl"], ONE_STEP_TOL)
+
+
+def test_c2_column_full_size_cutoff_ties():
+    """the 400×200 column at h = 1.5dx (lattice neighbours at
+    exactly 3dx = 2h, decided by the last ulp of r² < (2h)²): one step at
+    1e-10, then grids and neighbour counts bit-exact."""
+    t = oracle_threads()
+    lf_g, lf_c, g, c, meta = _pair(scenarios.column_collapse, threads=t)
+    _run(lf_g, lf_c, g, c, meta, 1)
+    parity.compare_integrators(lf_g, lf_c, c, ONE_STEP_TOL)
+    _grids_and_counts(lf_g, lf_c, g, c, t)
+
+
+def test_c1_dambreak_3d_full_size_one_step():
+    """1,000,000 fluid and 1,472,616 wall particles, one FP64
+    step: permutation bit-exact, physics within 1e-10 per particle, then
+    every interaction's grid and the per-particle neighbour counts
+    bit-exact."""
+    t = oracle_threads()
+    t0 = time.time()
+    lf_g, lf_c, g, c, meta = _pair(scenarios.dambreak_3d, threads=t)
+    assert meta["n_fluid"] == 1_000_000
+    _run(lf_g, lf_c, g, c, meta, 1)
+    rep = {}
+    parity.compare_integrators(lf_g, lf_c, c, ONE_STEP_TOL, report=rep)
+    print("C1 one step:", rep["fluid"], f"{time.time() - t0:.1f} s")
+    _grids_and_counts(lf_g, lf_c, g, c, t)
+
+
+# ------------------------------------------------ FP32-compensated precision
+# The FP32-compensated sweep keeps the exact FP64 neighbour test (identical
+# pair sets) and FP64 state; pair terms are FP32 with Kahan-compensated sums.
+FP32C_ONE_STEP_TOL = 2e-5    # per particle, after one step
+FP32C_RATE_TOL = 1e-3        # rate fields: the last step's FP32 pair sums
+# After 20 steps: the state within 1e-4, except the strains.  The FP32
+# records hold v rounded to FP32, so a strain rate (v_j - v_i)·∇W of a
+# column near rest, whose velocity differences are ~1e-3 of the velocities,
+# carries ~1e-4 relative error; the integrated strain keeps it.
+FP32C_MULTI_STEP_TOL = {"*": 1e-4, "strain": 1e-2, "strain_p": 1e-2}
+
+
+@pytest.mark.parametrize("case", list(SMALL))
+def test_fp32_compensated_one_step_against_fp64_oracle(case):
+    builder, kw = SMALL[case]
+    lf_g, lf_c, g, c, meta = _pair(builder, G.PRECISION_FP32_COMPENSATED, **kw)
+    _run(lf_g, lf_c, g, c, meta, 1)
+    parity.compare_integrators(lf_g, lf_c, c, FP32C_ONE_STEP_TOL, rate_tol=FP32C_RATE_TOL)
+
+
+@pytest.mark.parametrize("case", list(SMALL))
+def test_fp32_compensated_multi_step_against_fp64_oracle(case):
+    """20 FP32-compensated steps: the state on the integrated scale.  The
+    rates are held to the one-step bar from the initial state only: the
+    FP32 records round v to FP32, so once a column falls freely or rests,
+    its pair terms' velocity differences sit at the FP32 resolution of the
+    velocities and the rates' FP32 noise exceeds the terms themselves."""
+    builder, kw = SMALL[case]
+    lf_g, lf_c, g, c, meta = _pair(builder, G.PRECISION_FP32_COMPENSATED, **kw)
+    _run(lf_g, lf_c, g, c, meta, 20)
+    parity.compare_integrators(lf_g, lf_c, c, FP32C_MULTI_STEP_TOL, exact_ids=False, skip=parity.RATES)
+
+
+# The bar for the compensated mode: 1e-4 relative density and 1e-3 relative
+# stress against the FP64 oracle after 1000 steps; the other state fields
+# within 1e-3, the strains (see FP32C_MULTI_STEP_TOL) within 1e-2
+FP32C_LONG_TOL = {"*": 1e-3, "rho": 1e-4, "stress": 1e-3, "strain": 1e-2, "strain_p": 1e-2}
+
+
+def test_c2_column_fp32_compensated_1000_steps():
+    """configs[2] at its size, FP32-compensated sweeps with FP64 return
+    mapping, 1000 steps against the FP64 oracle: density within 1e-4 and
+    stress within 1e-3 per particle (the other state fields as
+    FP32C_LONG_TOL states)."""
+    t = oracle_threads()
+    lf_g, lf_c, g, c, meta = _pair(scenarios.column_collapse, G.PRECISION_FP32_COMPENSATED, threads=t)
+    t0 = time.time()
+    _run(lf_g, lf_c, g, c, meta, 1000)
+    rep = {}
+    parity.compare_integrators(lf_g, lf_c, c, FP32C_LONG_TOL, exact_ids=False, skip=parity.RATES, report=rep)
+    print("C2 FP32c after 1000 steps:", rep, f"{time.time() - t0:.1f} s")
+
+
+def test_nonfinite_position_reports_error():
+    ps = G.FluidParticleSystem("f", 10, 2, 1.0, 1.0)
+    ps.x[:] = np.linspace(0, 1, 20).reshape(10, 2)
+    ps.rho[:] = 1.0
+    ps.x[3, 0] = np.nan
+    k = G.CubicSplineKernel(0.1, ndims=2)
+    lf = G.LeapFrogTimeIntegrator([ps], [G.SystemInteraction(k, G.FluidPfn(0.1, 0.0, 0.1), ps)])
+    s = G.Session([lf], backend=make_backend("cuda"))
+    s.push()
+    with pytest.raises(G.GcError) as ei:
+        s.step(1, 0.1)
+    assert ei.value.status == G.consts.GC_ERR_NONFINITE
 
 
 def test_sort_permutation_random_points():
@@ -171,47 +293,3 @@ def test_sort_permutation_random_points():
         g.pull()
         c.pull()
         assert np.array_equal(ps_g.x, ps_c.x)
-
-
-def test_nonfinite_position_reports_error():
-    ps = G.FluidParticleSystem("f", 10, 2, 1.0, 1.0)
-    ps.x[:] = np.linspace(0, 1, 20).reshape(10, 2)
-    ps.rho[:] = 1.0
-    ps.x[3, 0] = np.nan
-    k = G.CubicSplineKernel(0.1, ndims=2)
-    lf = G.LeapFrogTimeIntegrator([ps], [G.SystemInteraction(k, G.FluidPfn(0.1, 0.0, 0.1), ps)])
-    s = G.Session([lf], backend=make_backend("cuda"))
-    s.push()
-    with pytest.raises(G.GcError) as ei:
-        s.step(1, 0.1)
-    assert ei.value.status == G.consts.GC_ERR_NONFINITE
-
-
-# ------------------------------------------------ FP32-compensated precision
-# The FP32-compensated sweep keeps the exact FP64 neighbour test (identical
-# pair sets) and FP64 state; pair terms are FP32 with Kahan-compensated sums.
-FP32C_ONE_STEP_TOL = 2e-5    # of each field's scale, after one step
-FP32C_MULTI_STEP_TOL = 1e-4  # after 20 steps (state: x, v, ρ, p, stress, strains)
-FP32C_RATE_TOL = 1e-3        # rate fields: the last step's FP32 pair sums
-
-
-def _pair_prec(builder, prec, **kw):
-    lf_g, meta = builder(**kw)
-    lf_c, _ = builder(**kw)
-    g = G.Session([lf_g], backend=make_backend("cuda"), precision=prec)
-    c = G.Session([lf_c], backend=make_backend("oracle"))
-    g.push()
-    c.push()
-    return lf_g, lf_c, g, c, meta
-
-
-@pytest.mark.parametrize("case", list(SMALL))
-@pytest.mark.parametrize("nsteps,tol", [(1, FP32C_ONE_STEP_TOL), (20, FP32C_MULTI_STEP_TOL)])
-def test_fp32_compensated_against_fp64_oracle(case, nsteps, tol):
-    builder, kw = SMALL[case]
-    lf_g, lf_c, g, c, meta = _pair_prec(builder, G.PRECISION_FP32_COMPENSATED, **kw)
-    g.step(nsteps, meta["cfl"])
-    c.step(nsteps, meta["cfl"])
-    g.pull()
-    c.pull()
-    _compare_systems(lf_g, lf_c, tol, exact_ids=(nsteps == 1), rate_tol=max(tol, FP32C_RATE_TOL))

@@ -639,3 +639,58 @@ def test_viscoplastic_mc_updater(be):
             st = [0.0, 0.0, 0.0]
         assert ps.p[i] == p
         assert list(ps.stress[i]) == st
+
+
+# ---------------------------------------- static (Lennard-Jones) boundary
+# FluidPfn against a StaticBoundarySystem, src/PairwiseFunctors.jl:209-219:
+# dv/dt_i += -m_j·Π_ij·∇W + f_LJ·dx with artificial_viscosity
+# (src/PairwisePhysics.jl:29-34) and lennard_jones(dx, lj_cutoff, c_a, 12, 6)
+# (:258-263); the density rate is untouched.
+
+def _lj_expected(xi, xj, vi, vj, rho_i, rho_j, m_j, c, h, alpha, beta, cut):
+    dx = np.asarray(xi, float) - np.asarray(xj, float)
+    dv = np.asarray(vi, float) - np.asarray(vj, float)
+    rr = float(dx @ dx)
+    r = math.sqrt(rr)
+    q = r / h
+    nd = dx.size
+    norm = 10.0 / (7.0 * math.pi * h * h) if nd == 2 else 1.0 / (math.pi * h ** 3)
+    dwdq = norm * (-3.0 * (0.25 * max(0.0, 2.0 - q) ** 2 - max(0.0, 1.0 - q) ** 2))
+    gx = dwdq / (r * h) * dx
+    vr = min(float(dx @ dv), 0.0)
+    muv = h * vr / (rr + h * h * 0.01)
+    piv = (beta * muv - alpha * c) * muv / (0.5 * rho_i * rho_j)
+    f = ((cut / r) ** 12 - (cut / r) ** 6) / rr if r < cut else 0.0
+    return -m_j * piv * gx + 0.01 * c * c * f * dx
+
+
+@pytest.mark.parametrize("be", BACKENDS)
+@pytest.mark.parametrize("nd", [2, 3])
+@pytest.mark.parametrize("sep", [0.8, 1.0, 1.6])
+def test_static_boundary_lennard_jones_pair(be, nd, sep):
+    """One fluid particle moving towards one static wall particle at
+    sep·lj_cutoff: inside the cutoff LJ repulsion plus viscosity; at exactly
+    the cutoff and beyond (still inside 2h) viscosity alone."""
+    dx_sp, h, c, alpha, beta = 0.5, 0.6, 20.0, 0.3, 0.2
+    f = G.FluidParticleSystem("fluid", 1, nd, 250.0, c)
+    w = G.BasicParticleSystem("wall", 1, nd, 125.0, c)
+    f.x[0] = [0.1] * (nd - 1) + [sep * dx_sp]
+    w.x[0] = [0.1] * nd
+    w.x[0, -1] = 0.0
+    f.v[0] = [0.3] + [0.0] * (nd - 2) + [-1.5]
+    f.rho[:] = 1003.0
+    w.rho[:] = 998.0
+    f.p[:] = 1234.0
+    si = G.SystemInteraction(G.CubicSplineKernel(h, ndims=nd), G.FluidPfn(alpha, beta, h), f,
+                             G.StaticBoundarySystem(w, dx_sp))
+    lf, s = session(be, [f, w], [si])
+    s.create_grid(si)
+    s.sweep(si, 1)
+    s.pull()
+    want = _lj_expected(f.x[0], w.x[0], f.v[0], w.v[0], 1003.0, 998.0, 125.0, c, h, alpha, beta, dx_sp)
+    assert np.allclose(f.dvdt[0], want, rtol=1e-13, atol=0.0), (f.dvdt[0], want)
+    assert f.drhodt[0] == 0.0
+    assert np.all(w.dvdt == 0.0) and w.drhodt[0] == 0.0
+    if sep < 1.0:
+        # the repulsion points away from the wall and dominates
+        assert f.dvdt[0, -1] > 0.0

@@ -17,6 +17,7 @@ import pytest
 
 import grasph_b200 as G
 from grasph_b200 import scenarios
+import parity
 from gc_helpers import BACKENDS, make_backend, session
 
 
@@ -120,18 +121,6 @@ def _run(lf, be, nsteps, cfl, prec=None, graphs=None):
     return s
 
 
-def _cmp(lf_g, lf_c, tol, rate_tol=None):
-    for sg, sc in zip(lf_g.systems, lf_c.systems):
-        ig, ic = np.argsort(sg.id), np.argsort(sc.id)
-        for name, _ in sg.particle_fields():
-            if name in ("id", "v_adjustment"):
-                continue
-            t = rate_tol if (rate_tol is not None and name in ("dvdt", "drhodt")) else tol
-            a = np.asarray(getattr(sg, name), dtype=float)[ig]
-            b = np.asarray(getattr(sc, name), dtype=float)[ic]
-            scale = max(np.abs(b).max(), 1e-300)
-            err = np.abs(a - b).max() / scale
-            assert err <= t, f"{sg.name}.{name}: {err:.3e} > {t}"
 
 
 def test_bubble_oracle_runs_and_conserves_mass():
@@ -149,21 +138,15 @@ def test_bubble_oracle_runs_and_conserves_mass():
 def test_bubble_parity_fp64(variant, integ, nsteps, tol):
     # the scripts' Courant number 1.5 is an RK4 one; LeapFrog needs a smaller step
     cfl = 1.5 if integ == "rk4" else 0.2
-    lf_g, _ = scenarios.bubble(variant, dx=0.1, integrator=integ, cfl=cfl)
-    lf_c, _ = scenarios.bubble(variant, dx=0.1, integrator=integ, cfl=cfl)
-    _run(lf_g, "cuda", nsteps, cfl)
-    _run(lf_c, "oracle", nsteps, cfl)
-    _cmp(lf_g, lf_c, tol)
+    parity.run_and_compare(lambda: scenarios.bubble(variant, dx=0.1, integrator=integ, cfl=cfl), nsteps, cfl, tol)
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant", ["bubble", "bubble3"])
 def test_bubble_parity_fp32c(variant):
-    lf_g, meta = scenarios.bubble(variant, dx=0.1)
-    lf_c, _ = scenarios.bubble(variant, dx=0.1)
-    _run(lf_g, "cuda", 20, meta["cfl"], prec=G.PRECISION_FP32_COMPENSATED)
-    _run(lf_c, "oracle", 20, meta["cfl"])
-    _cmp(lf_g, lf_c, 1e-4, rate_tol=1e-3)
+    _, meta = scenarios.bubble(variant, dx=0.1)
+    parity.run_and_compare(lambda: scenarios.bubble(variant, dx=0.1), 20, meta["cfl"], 1e-4,
+                           precision=G.PRECISION_FP32_COMPENSATED)
 
 
 @pytest.mark.gpu
@@ -251,17 +234,12 @@ def test_dambreak_wall_layout():
 @pytest.mark.parametrize("nsteps,tol", [(1, 1e-10), (20, 1e-8)])
 @pytest.mark.parametrize("x_wall", [60.0, 25.0])
 def test_dambreak_wall_parity(nsteps, tol, x_wall):
-    lf_g, meta = scenarios.dambreak_wall(x_wall=x_wall)
-    lf_c, _ = scenarios.dambreak_wall(x_wall=x_wall)
-    _run(lf_g, "cuda", nsteps, meta["cfl"])
-    _run(lf_c, "oracle", nsteps, meta["cfl"])
-    _cmp(lf_g, lf_c, tol)
+    _, meta = scenarios.dambreak_wall(x_wall=x_wall)
+    parity.run_and_compare(lambda: scenarios.dambreak_wall(x_wall=x_wall), nsteps, meta["cfl"], tol)
 
 
 @pytest.mark.gpu
 def test_dambreak_wall_fp32c():
-    lf_g, meta = scenarios.dambreak_wall(x_wall=25.0)
-    lf_c, _ = scenarios.dambreak_wall(x_wall=25.0)
-    _run(lf_g, "cuda", 20, meta["cfl"], prec=G.PRECISION_FP32_COMPENSATED)
-    _run(lf_c, "oracle", 20, meta["cfl"])
-    _cmp(lf_g, lf_c, 1e-4, rate_tol=1e-3)
+    _, meta = scenarios.dambreak_wall(x_wall=25.0)
+    parity.run_and_compare(lambda: scenarios.dambreak_wall(x_wall=25.0), 20, meta["cfl"],
+                           {"*": 1e-4, "strain": 1e-2, "strain_p": 1e-2}, precision=G.PRECISION_FP32_COMPENSATED)

@@ -39,6 +39,11 @@ def _restart_case(build, be, tmp_path, n1=4, n2=5):
     assert step == n1
     s2.step(n2, meta["cfl"])
     s2.pull()
+    # a save after the restart records the global step (restart + steps since)
+    path2 = tmp_path / "snap2.npz"
+    s2.save(path2)
+    with np.load(path2) as f:
+        assert int(f["@step"]) == n1 + n2
     return straight, _fields(lf2)
 
 
@@ -78,6 +83,17 @@ def test_snapshot_layout_and_checks(tmp_path):
     wrong_nd = G.FluidParticleSystem("fluid", 3, 3, 0.5, 10.0)
     with pytest.raises(G.ArgumentError):
         read_snapshot([wrong_nd], path)
+    # _load_restart!: a system without a group is left untouched with a
+    # warning; a file without a step restarts from step 0 with a warning
+    other = G.FluidParticleSystem("other", 2, 2, 0.5, 10.0)
+    other.rho[:] = 5.0
+    with pytest.warns(UserWarning, match="no group for system 'other'"):
+        assert read_snapshot([back, other], path) == 7
+    assert np.all(other.rho == 5.0)
+    nostep = tmp_path / "nostep.npz"
+    write_snapshot([ps], nostep)
+    with pytest.warns(UserWarning, match="assuming step 0"):
+        assert read_snapshot([back], nostep) == 0
 
 
 def test_restart_with_moving_probes_on_the_oracle(tmp_path):

@@ -19,6 +19,7 @@ import pytest
 
 import grasph_b200 as G
 from grasph_b200 import scenarios
+import parity
 from gc_helpers import BACKENDS, make_backend
 
 
@@ -116,18 +117,6 @@ def test_xsph_as_stage_functor_is_refused(be):
         G.SystemInteraction(G.CubicSplineKernel(0.1, ndims=2), G.XSPHPfn(0.5), ps)
 
 
-def _cmp(lf_g, lf_c, tol, rate_tol=None):
-    for sg, sc in zip(lf_g.systems, lf_c.systems):
-        ig, ic = np.argsort(sg.id), np.argsort(sc.id)
-        for name, _ in sg.particle_fields():
-            if name == "id":
-                continue
-            t = rate_tol if (rate_tol is not None and name in ("dvdt", "drhodt", "v_adjustment")) else tol
-            a = np.asarray(getattr(sg, name), dtype=float)[ig]
-            b = np.asarray(getattr(sc, name), dtype=float)[ic]
-            scale = max(np.abs(b).max(), 1e-300)
-            err = np.abs(a - b).max() / scale
-            assert err <= t, f"{sg.name}.{name}: {err:.3e} > {t}"
 
 
 def _run(lf, be, nsteps, cfl, prec=None, graphs=None):
@@ -159,11 +148,7 @@ def test_bubble3_oracle_xsph_moves_the_adjustment():
 @pytest.mark.parametrize("nsteps,tol", [(1, 1e-10), (20, 1e-8)])
 def test_bubble3_xsph_parity(integ, nsteps, tol):
     cfl = 1.5 if integ == "rk4" else 0.2
-    lf_g, _ = scenarios.bubble("bubble3", dx=0.1, integrator=integ, cfl=cfl)
-    lf_c, _ = scenarios.bubble("bubble3", dx=0.1, integrator=integ, cfl=cfl)
-    _run(lf_g, "cuda", nsteps, cfl)
-    _run(lf_c, "oracle", nsteps, cfl)
-    _cmp(lf_g, lf_c, tol)
+    parity.run_and_compare(lambda: scenarios.bubble("bubble3", dx=0.1, integrator=integ, cfl=cfl), nsteps, cfl, tol)
 
 
 @pytest.mark.gpu
@@ -171,20 +156,15 @@ def test_bubble3_xsph_parity(integ, nsteps, tol):
 def test_dambreak_xsph_with_dynamic_walls_parity(nsteps, tol):
     # XSPH against a DynamicBoundarySystem uses the wall's stored v and rho and
     # writes the wall's own v_adjustment, so the walls move
-    lf_g, meta = _dambreak_xsph()
-    lf_c, _ = _dambreak_xsph()
-    _run(lf_g, "cuda", nsteps, meta["cfl"])
-    _run(lf_c, "oracle", nsteps, meta["cfl"])
-    _cmp(lf_g, lf_c, tol)
+    _, meta = _dambreak_xsph()
+    parity.run_and_compare(_dambreak_xsph, nsteps, meta["cfl"], tol)
 
 
 @pytest.mark.gpu
 def test_bubble3_xsph_fp32c():
-    lf_g, meta = scenarios.bubble("bubble3", dx=0.1)
-    lf_c, _ = scenarios.bubble("bubble3", dx=0.1)
-    _run(lf_g, "cuda", 20, meta["cfl"], prec=G.PRECISION_FP32_COMPENSATED)
-    _run(lf_c, "oracle", 20, meta["cfl"])
-    _cmp(lf_g, lf_c, 1e-4, rate_tol=1e-3)
+    _, meta = scenarios.bubble("bubble3", dx=0.1)
+    parity.run_and_compare(lambda: scenarios.bubble("bubble3", dx=0.1), 20, meta["cfl"], 1e-4,
+                           precision=G.PRECISION_FP32_COMPENSATED)
 
 
 @pytest.mark.gpu
