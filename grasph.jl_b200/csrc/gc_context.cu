@@ -131,6 +131,11 @@ struct DSlot {
     std::vector<std::vector<int>> upd_kind;
     bool upd_set = false;
     int nupd = 0;
+    // the fused half step of this pack_epoch already ran the stage-1
+    // updaters and packed the stage-1 records (mode, record stress width)
+    int64_t upd_fused_epoch = -1;
+    int64_t pack_done_epoch = -1;
+    int pack_done_stage = 0, pack_done_mode = -1, pack_done_ns = -1;
     // warp groups of this system's particles (one grid's columns)
     int2* groups = nullptr;
     int64_t* d_ngroups = nullptr;
@@ -1432,29 +1437,32 @@ StepArgs step_args(DSlot& S) {
     return a;
 }
 
+UpdArgs upd_args(DSlot& S, int stage, size_t q, double dt_override) {
+    UpdArgs a{};
+    a.N = S.N;
+    a.kind = S.upd_kind[stage - 1][q];
+    a.nd = S.nd;
+    a.ns = S.ns;
+    a.nvort = S.nvort;
+    a.inst_of = S.inst_of;
+    a.inst = S.d_inst;
+    a.u = S.d_upd[stage - 1][q];
+    a.dt = dt_override;
+    a.rho = S.F(F_RHO);
+    a.p = S.F(F_P);
+    a.stress = S.F(F_STRESS);
+    a.sr = S.F(F_SR);
+    a.vort = S.F(F_VORT);
+    a.strain = S.F(F_STRAIN);
+    a.strainp = S.F(F_STRAINP);
+    a.dvdt = S.F(F_DVDT);
+    a.drhodt = S.F(F_DRHODT);
+    return a;
+}
+
 int run_updaters(gc_ctx* ctx, DSlot& S, int stage, double dt_override) {
     if (stage < 1 || stage > (int)S.d_upd.size()) return GC_OK;
-    for (size_t q = 0; q < S.d_upd[stage - 1].size(); ++q) {
-        UpdArgs a{};
-        a.N = S.N;
-        a.nd = S.nd;
-        a.ns = S.ns;
-        a.nvort = S.nvort;
-        a.inst_of = S.inst_of;
-        a.inst = S.d_inst;
-        a.u = S.d_upd[stage - 1][q];
-        a.dt = dt_override;
-        a.rho = S.F(F_RHO);
-        a.p = S.F(F_P);
-        a.stress = S.F(F_STRESS);
-        a.sr = S.F(F_SR);
-        a.vort = S.F(F_VORT);
-        a.strain = S.F(F_STRAIN);
-        a.strainp = S.F(F_STRAINP);
-        a.dvdt = S.F(F_DVDT);
-        a.drhodt = S.F(F_DRHODT);
-        launch_update(a, ctx->stream);
-    }
+    for (size_t q = 0; q < S.d_upd[stage - 1].size(); ++q) launch_update(upd_args(S, stage, q, dt_override), ctx->stream);
     return check_launch(ctx, "updater");
 }
 
@@ -1482,6 +1490,7 @@ int run_virtual_updaters(gc_ctx* ctx, DVirt& V, int stage) {
         } else {
             UpdArgs a{};
             a.N = S.N;
+            a.kind = kind;
             a.nd = S.nd;
             a.ns = S.ns;
             a.nvort = S.nvort;
@@ -1700,31 +1709,78 @@ int interp_sweeps(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage) {
 }
 
 // Fused sweep of the interactions `ids` (same system_a, same functor kind).
+// How sweep_group treats system_a's state for a group of interactions of
+// one functor kind: the functor the kernel runs, its per-particle divisor
+// mode, whether the sweep is FP32-compensated and its record's stress width.
+struct PackPlan {
+    int pk0 = GC_PFN_NONE, pfn = GC_PFN_NONE, mode = 0, pk_ns = 0;
+    bool interp = false, xsph = false, fp32 = false;
+};
+
+PackPlan pack_plan(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
+    DSlot& S = ctx->slots[a];
+    PackPlan pl;
+    pl.pk0 = ctx->inters[ids[0]].pk[stage - 1];
+    pl.interp = (pl.pk0 == GC_PFN_INTERPOLATE || pl.pk0 == GC_PFN_NEIGHBOR_COUNT) && !count_only;
+    // FluidSolidPfn runs the FluidPfn kernel in its fluid-solid mode (PfnInst.fs)
+    pl.pfn = pl.pk0 == GC_PFN_FLUID_SOLID ? GC_PFN_FLUID : pl.pk0;
+    pl.mode = aux_mode_for(pl.pfn);
+    pl.xsph = pl.pfn == GC_PFN_XSPH;  // writes v_adjustment; always FP64
+    pl.fp32 = ctx->precision == GC_PRECISION_FP32_COMPENSATED && pl.pfn != GC_PFN_COUNT && !pl.xsph && !count_only;
+    for (int id : ids)
+        if (pl.pfn == GC_PFN_FLUID && ctx->inters[id].h_gi.size() && ctx->inst[0].inters[id].pp[stage - 1][3] == 1.0)
+            pl.fp32 = false;  // the S = 1 (multiphase) pressure form stays in FP64
+    pl.pk_ns = pl.pfn == GC_PFN_CAUCHY_FLUID ? S.ns : 0;
+    return pl;
+}
+
+// The interaction groups a stage sweeps with system `a` as system_a, in
+// launch order: grouped by functor kind in order of first appearance, at
+// most MAX_REFS interactions per launch.
+std::vector<std::vector<int>> stage_groups(gc_ctx* ctx, int a, int stage) {
+    std::vector<int> kinds;
+    for (size_t i = 0; i < ctx->inters.size(); ++i) {
+        DInter& D = ctx->inters[i];
+        if (D.probe) continue;
+        int pk = D.pk[stage - 1];
+        if (D.a != a || pk == GC_PFN_NONE) continue;
+        if (std::find(kinds.begin(), kinds.end(), pk) == kinds.end()) kinds.push_back(pk);
+    }
+    std::vector<std::vector<int>> out;
+    for (int pk : kinds) {
+        std::vector<int> ids;
+        for (size_t i = 0; i < ctx->inters.size(); ++i)
+            if (!ctx->inters[i].probe && ctx->inters[i].a == a && ctx->inters[i].pk[stage - 1] == pk)
+                ids.push_back((int)i);
+        for (size_t off = 0; off < ids.size(); off += MAX_REFS)
+            out.emplace_back(ids.begin() + off, ids.begin() + std::min(ids.size(), off + MAX_REFS));
+    }
+    return out;
+}
+
 int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool count_only) {
     DSlot& S = ctx->slots[a];
-    const int pk0 = ctx->inters[ids[0]].pk[stage - 1];
-    if ((pk0 == GC_PFN_INTERPOLATE || pk0 == GC_PFN_NEIGHBOR_COUNT) && !count_only)
-        return interp_sweeps(ctx, a, ids, stage);
-    // FluidSolidPfn runs the FluidPfn kernel in its fluid-solid mode (PfnInst.fs)
-    const int pfn = pk0 == GC_PFN_FLUID_SOLID ? GC_PFN_FLUID : pk0;
-    const int mode = aux_mode_for(pfn);
-    const bool xsph = pfn == GC_PFN_XSPH;  // writes v_adjustment; always FP64
-    bool fp32 = ctx->precision == GC_PRECISION_FP32_COMPENSATED && pfn != GC_PFN_COUNT && !xsph && !count_only;
-    for (int id : ids)
-        if (pfn == GC_PFN_FLUID && ctx->inters[id].h_gi.size() && ctx->inst[0].inters[id].pp[stage - 1][3] == 1.0)
-            fp32 = false;  // the S = 1 (multiphase) pressure form stays in FP64
-    const int pk_ns = pfn == GC_PFN_CAUCHY_FLUID ? S.ns : 0;
+    const PackPlan pl = pack_plan(ctx, a, ids, stage, count_only);
+    if (pl.interp) return interp_sweeps(ctx, a, ids, stage);
+    const int pk0 = pl.pk0, pfn = pl.pfn, mode = pl.mode, pk_ns = pl.pk_ns;
+    const bool xsph = pl.xsph, fp32 = pl.fp32;
     // FP32 sweep buffers: positions, then records (see ensure_fpk)
     auto xp_of = [](float* fpk) { return (double*)fpk; };
     auto pk_of = [](float* fpk, int64_t N, int nd) { return fpk + N * 2 * pos_stride(nd); };
     if (pfn != GC_PFN_COUNT && !xsph) {
         if (fp32) {
             TRY(ensure_fpk(ctx, S, S.N, S.nd, pk_ns));
-            // positions do not change between the stages of a step
-            const bool pos = S.xpk_epoch != ctx->pack_epoch;
-            launch_pack32(mode, S.N, nullptr, S.nd, pk_ns, S.F(F_X), S.F(F_V), S.F(F_RHO), S.F(F_P), S.F(F_STRESS),
-                          S.inst_of, S.d_mass, pos ? xp_of(S.fpk) : nullptr, pk_of(S.fpk, S.N, S.nd), ctx->stream);
-            S.xpk_epoch = ctx->pack_epoch;
+            // the fused half step of this step may have packed these records
+            const bool done = S.pack_done_epoch == ctx->pack_epoch && S.pack_done_stage == stage &&
+                              S.pack_done_mode == mode && S.pack_done_ns == pk_ns;
+            if (!done) {
+                // positions do not change between the stages of a step
+                const bool pos = S.xpk_epoch != ctx->pack_epoch;
+                launch_pack32(mode, S.N, nullptr, S.nd, pk_ns, S.F(F_X), S.F(F_V), S.F(F_RHO), S.F(F_P),
+                              S.F(F_STRESS), S.inst_of, S.d_mass, pos ? xp_of(S.fpk) : nullptr,
+                              pk_of(S.fpk, S.N, S.nd), ctx->stream);
+                S.xpk_epoch = ctx->pack_epoch;
+            }
         } else {
             launch_aux(mode, S.N, nullptr, S.F(F_RHO), S.F(F_P), S.inst_of, S.d_mass, S.aux, ctx->stream);
         }
@@ -1858,7 +1914,10 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
                 B.xpk_epoch = ctx->pack_epoch;
                 if (!B.xmoves()) B.xpk_static = true;
                 r.bxp = xp_of(B.fpk);
-                if (rec) r.bfp = pk_of(B.fpk, B.N, B.nd);
+                if (rec) {
+                    r.bfp = pk_of(B.fpk, B.N, B.nd);
+                    B.pack_done_epoch = -1;  // packed in this sweep's mode: B's own sweep packs again
+                }
             }
         }
     }
@@ -1944,27 +2003,8 @@ int sweep_group(gc_ctx* ctx, int a, const std::vector<int>& ids, int stage, bool
 }
 
 int sweep_stage(gc_ctx* ctx, int stage) {
-    for (size_t a = 0; a < ctx->slots.size(); ++a) {
-        // group this system's interactions by functor kind
-        std::vector<int> kinds;
-        for (size_t i = 0; i < ctx->inters.size(); ++i) {
-            DInter& D = ctx->inters[i];
-            if (D.probe) continue;
-            int pk = D.pk[stage - 1];
-            if (D.a != (int)a || pk == GC_PFN_NONE) continue;
-            if (std::find(kinds.begin(), kinds.end(), pk) == kinds.end()) kinds.push_back(pk);
-        }
-        for (int pk : kinds) {
-            std::vector<int> ids;
-            for (size_t i = 0; i < ctx->inters.size(); ++i)
-                if (!ctx->inters[i].probe && ctx->inters[i].a == (int)a && ctx->inters[i].pk[stage - 1] == pk)
-                    ids.push_back((int)i);
-            for (size_t off = 0; off < ids.size(); off += MAX_REFS) {
-                std::vector<int> chunk(ids.begin() + off, ids.begin() + std::min(ids.size(), off + MAX_REFS));
-                TRY(sweep_group(ctx, (int)a, chunk, stage, false));
-            }
-        }
-    }
+    for (size_t a = 0; a < ctx->slots.size(); ++a)
+        for (auto& ids : stage_groups(ctx, (int)a, stage)) TRY(sweep_group(ctx, (int)a, ids, stage, false));
     return GC_OK;
 }
 
@@ -2045,7 +2085,9 @@ int sweep_all_stages(gc_ctx* ctx) {
     }
     for (int stage = 1; stage <= ctx->nstages; ++stage) {
         for (auto& S : ctx->slots)
-            if (!S.vsrc && S.upd_set && S.nupd == ctx->nstages) TRY(run_updaters(ctx, S, stage, NAN));
+            if (!S.vsrc && S.upd_set && S.nupd == ctx->nstages &&
+                !(stage == 1 && S.upd_fused_epoch == ctx->pack_epoch))
+                TRY(run_updaters(ctx, S, stage, NAN));
         for (auto& G : ctx->ghosts) TRY(ghost_copy(ctx, G, stage));
         for (auto& V : ctx->virts)
             if (!V.probe && V.upd_set && V.nupd == ctx->nstages) TRY(run_virtual_updaters(ctx, V, stage));
@@ -2084,6 +2126,44 @@ int xsph_pass(gc_ctx* ctx) {
     return check_launch(ctx, "XSPH correction");
 }
 
+// The LeapFrog half step of slot `a` fused with the stage-1 work that
+// follows it for the same particles: its stage-1 updater when that is one
+// light elementwise kind (moved here from _sweep_all_stages!, :401-419;
+// nothing between the two reads or writes what it touches) and, for an
+// FP32-compensated first sweep after it, that sweep's records
+// (sweep_group then finds them packed).
+int halfstep_stage1(gc_ctx* ctx, int a) {
+    DSlot& S = ctx->slots[a];
+    UpdArgs u{};
+    u.kind = -1;
+    // a stage-1 chain of at most one light updater moves into the half step
+    const bool has1 = !S.vsrc && S.upd_set && S.nupd == ctx->nstages && ctx->nstages >= 1 && !S.d_upd.empty();
+    const bool upd = has1 && S.d_upd[0].size() == 1 && halfstep_fuses(S.upd_kind[0][0]);
+    if (upd) u = upd_args(S, 1, 0, NAN);
+    PackArgs pk{};
+    if (upd || !has1 || S.d_upd[0].empty()) {  // the pack follows the stage-1 updaters
+        const auto groups = ctx->nstages >= 1 ? stage_groups(ctx, a, 1) : std::vector<std::vector<int>>{};
+        if (!groups.empty()) {
+            const PackPlan pl = pack_plan(ctx, a, groups[0], 1, false);
+            if (pl.fp32 && !pl.interp && !pl.xsph && pl.pfn != GC_PFN_COUNT) {
+                TRY(ensure_fpk(ctx, S, S.N, S.nd, pl.pk_ns));
+                const bool pos = S.xpk_epoch != ctx->pack_epoch;
+                pk = PackArgs{pl.mode, S.nd, pl.pk_ns, S.N, S.F(F_X), S.F(F_V), S.F(F_RHO), S.F(F_P), S.F(F_STRESS),
+                              S.inst_of, S.d_mass, pos ? (double*)S.fpk : nullptr,
+                              S.fpk + S.N * 2 * pos_stride(S.nd)};
+                S.xpk_epoch = ctx->pack_epoch;
+                S.pack_done_epoch = ctx->pack_epoch;
+                S.pack_done_stage = 1;
+                S.pack_done_mode = pl.mode;
+                S.pack_done_ns = pl.pk_ns;
+            }
+        }
+    }
+    launch_halfstep_fused(step_args(S), u, pk, ctx->stream);
+    if (upd) S.upd_fused_epoch = ctx->pack_epoch;
+    return GC_OK;
+}
+
 int one_step(gc_ctx* ctx) {
     if (ctx->inst[0].integ == GC_INTEGRATOR_RK4) return one_step_rk4(ctx);
     ctx->pack_epoch++;
@@ -2096,8 +2176,8 @@ int one_step(gc_ctx* ctx) {
     for (size_t s = 0; s < ctx->slots.size(); ++s)
         if (mask[s]) ctx->slots[s].sorted_once = true;
     ctx->resorts += 1;
-    for (auto& S : ctx->slots)
-        if (S.moving) launch_halfstep(step_args(S), ctx->stream);
+    for (size_t a = 0; a < ctx->slots.size(); ++a)
+        if (ctx->slots[a].moving) TRY(halfstep_stage1(ctx, (int)a));
     TRY(check_launch(ctx, "half step"));
     for (auto& G : ctx->ghosts) TRY(ghost_kinematics(ctx, G));
     TRY(sweep_all_stages(ctx));

@@ -20,6 +20,7 @@ struct StepArgs {
 
 struct UpdArgs {
     int64_t N;
+    int kind;           // GC_UPD_* of every instance (the model structure is shared)
     int nd, ns, nvort;
     const int32_t* inst_of;
     const SysInst* inst;
@@ -28,7 +29,30 @@ struct UpdArgs {
     double *rho, *p, *stress, *sr, *vort, *strain, *strainp, *dvdt, *drhodt;
 };
 
+// One slot's FP32 sweep records (launch_pack32's arguments; xpk or pk may
+// be nullptr).
+struct PackArgs {
+    int mode, nd, ns;
+    int64_t N;
+    const double *x, *v, *rho, *p, *stress;
+    const int32_t* inst_of;
+    const double* mass;
+    double* xpk;
+    float* pk;
+};
+
+
 void launch_halfstep(const StepArgs& a, cudaStream_t s);
+// The half step fused with what follows it for the same particles before
+// the first sweeps (src/TimeIntegration.jl:158, then _sweep_all_stages!'s
+// stage-1 state updater :401-419): per particle the half step, the updater
+// u (u.kind < 0: none; an elementwise kind), then (pk.pk or pk.xpk set) the
+// FP32 records of the stage's first sweep.  One pass over the state instead
+// of three.
+void launch_halfstep_fused(const StepArgs& a, const UpdArgs& u, const PackArgs& pk, cudaStream_t s);
+// Whether launch_halfstep_fused takes updater kind `kind` (the light,
+// elementwise ones; the stress updaters keep their own launch).
+bool halfstep_fuses(int kind);
 void launch_fullstep(const StepArgs& a, cudaStream_t s);
 // RK4 (src/TimeIntegration.jl:712-838): q0 snapshot, zero accumulators and
 // dqdt reset; stage advance q = q0 + f·dt·dqdt (f = 0.5 or 1) and dqdt reset;

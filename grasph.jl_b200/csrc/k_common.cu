@@ -27,6 +27,22 @@ static inline int nblk(int64_t n, int tpb = TPB) {
 // Every launcher adds the number of kernels it enqueued.
 #define COUNTED(n) (g_launches.fetch_add((n), std::memory_order_relaxed))
 
+// Warp-aggregated counter increment: every lane of the warp calls it; each
+// valid lane adds 1 to ctr[k] and receives a distinct slot of the counter's
+// old value + its rank among the warp's lanes with the same k (in lane
+// order).  Sorted or nearly sorted keys give one atomic per distinct key per
+// warp instead of one per particle.
+__device__ __forceinline__ int32_t warp_agg_inc(int32_t* ctr, int32_t k, bool valid) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned grp = __match_any_sync(FULL, valid ? k : INT32_MIN);
+    const int leader = __ffs(grp) - 1;
+    int32_t base = 0;
+    if (valid && lane == leader) base = atomicAdd(&ctr[k], __popc(grp));
+    base = __shfl_sync(FULL, base, leader);
+    return base + __popc(grp & ((1u << lane) - 1u));
+}
+
 // ================================================================== scan
 constexpr int SCAN_T = 512, SCAN_I = 4, SCAN_TILE = SCAN_T * SCAN_I;
 
@@ -402,35 +418,43 @@ __global__ void k_sort_keys(const double* __restrict__ x, int64_t N, int nd, con
                             const int64_t* count, const SysInst* __restrict__ inst, int32_t* __restrict__ key,
                             int32_t* __restrict__ hist, int64_t cells_cap, int* err) {
     int64_t n = count ? *count : N;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
-        const SysInst& S = inst[inst_of[g]];
-        int64_t flat = 0;
-        bool ok = true;
-        for (int d = 0; d < nd; ++d) {
-            int64_t kd;
-            if (!floor_i64(x[d * N + g] / S.sort_cutoff, &kd)) {
-                ok = false;
-                break;
+    // whole warps iterate together (warp-aggregated histogram)
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {
+        const int64_t g = g0 + threadIdx.x;
+        bool valid = g < n;
+        int32_t kk = -1;
+        if (valid) {
+            const SysInst& S = inst[inst_of[g]];
+            int64_t flat = 0;
+            bool ok = true;
+            for (int d = 0; d < nd; ++d) {
+                int64_t kd;
+                if (!floor_i64(x[d * N + g] / S.sort_cutoff, &kd)) {
+                    ok = false;
+                    break;
+                }
+                int64_t rel = kd - S.kmin[d];
+                if (rel < 0 || rel >= S.kext[d]) ok = false;
+                flat = flat * S.kext[d] + rel;
             }
-            int64_t rel = kd - S.kmin[d];
-            if (rel < 0 || rel >= S.kext[d]) ok = false;
-            flat = flat * S.kext[d] + rel;
+            flat += S.sort_cellbase;
+            if (!ok || flat < 0 || flat >= cells_cap) {
+                atomicOr(err, ok ? ERR_CAPACITY : ERR_NONFINITE);
+                valid = false;
+            } else {
+                kk = (int32_t)flat;
+            }
+            key[g] = kk;
         }
-        flat += S.sort_cellbase;
-        if (!ok || flat < 0 || flat >= cells_cap) {
-            atomicOr(err, ok ? ERR_CAPACITY : ERR_NONFINITE);
-            key[g] = -1;
-            continue;
-        }
-        key[g] = (int32_t)flat;
-        atomicAdd(&hist[flat], 1);
+        warp_agg_inc(hist, kk, valid);
     }
 }
 
 void launch_sort_keys(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                       const SysInst* inst, int32_t* key, int32_t* hist, int64_t cells_cap, int* err, cudaStream_t s) {
     if (N <= 0) return;
-    k_sort_keys<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, inst, key, hist, cells_cap, err);
+    k_sort_keys<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, inst, key, hist, cells_cap, err);  // TPB % 32 == 0
     COUNTED(1);
 }
 
@@ -438,11 +462,15 @@ __global__ void k_sort_scatter(const int32_t* __restrict__ key, int64_t N, const
                                const int32_t* __restrict__ start, int32_t* __restrict__ fill,
                                int32_t* __restrict__ perm) {
     int64_t n = count ? *count : N;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
-        int32_t k = key[g];
-        if (k < 0) continue;
-        int32_t pos = start[k] + atomicAdd(&fill[k], 1);
-        perm[pos] = (int32_t)g;
+    // whole warps iterate together (warp-aggregated fill counters); the
+    // order inside a cell is restored by the fix-up
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {
+        const int64_t g = g0 + threadIdx.x;
+        const int32_t k = g < n ? key[g] : -1;
+        const bool valid = k >= 0;
+        const int32_t slot = warp_agg_inc(fill, k, valid);
+        if (valid) perm[start[k] + slot] = (int32_t)g;
     }
 }
 
@@ -474,21 +502,72 @@ __global__ void k_sort_fixup(const int32_t* __restrict__ start, int64_t ncells_c
     }
 }
 
+// Sort W values in registers (a bitonic network: no data-dependent
+// branches, every index known at compile time, so v stays in registers).
+template <int W>
+__device__ __forceinline__ void reg_sort(int32_t* v) {
+#pragma unroll
+    for (int k = 2; k <= W; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < W; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const int32_t a = v[i], b = v[l];
+                    const bool up = (i & k) == 0;
+                    v[i] = up ? min(a, b) : max(a, b);
+                    v[l] = up ? max(a, b) : min(a, b);
+                }
+            }
+}
+
+// One cell's segment perm[s, s + m) with m <= W sorted ascending in
+// registers (padding INT32_MAX), unless it already is.
+template <int W>
+__device__ __forceinline__ void sort_segment(int32_t* __restrict__ perm, int32_t s, int32_t m) {
+    int32_t v[W];
+    bool sorted = true;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        v[q] = q < m ? perm[s + q] : INT32_MAX;
+        if (q > 0 && v[q] < v[q - 1]) sorted = false;
+    }
+    if (sorted) return;
+    reg_sort<W>(v);
+#pragma unroll
+    for (int q = 0; q < W; ++q)
+        if (q < m) perm[s + q] = v[q];
+}
+
+// One thread per cell: the fill counter cleared, then the cell's segment
+// sorted by source index in registers (segments of up to 32 members; a
+// larger one by an insertion sort in place).
 __global__ void k_sort_fixup_clear(const int32_t* __restrict__ start, int64_t ncells_cap, const int64_t* total_cells,
                                    int32_t* __restrict__ perm, int32_t* __restrict__ fill) {
     int64_t nc = *total_cells;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc && c < ncells_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
-        int32_t s = start[c], e = start[c + 1];
+        const int32_t s = start[c], e = start[c + 1];
         fill[c] = 0;
-        for (int32_t i = s + 1; i < e; ++i) {
-            int32_t v = perm[i];
-            int32_t j = i - 1;
-            while (j >= s && perm[j] > v) {
-                perm[j + 1] = perm[j];
-                --j;
+        const int32_t m = e - s;
+        if (m <= 1) continue;
+        if (m <= 8) {
+            sort_segment<8>(perm, s, m);
+        } else if (m <= 16) {
+            sort_segment<16>(perm, s, m);
+        } else if (m <= 32) {
+            sort_segment<32>(perm, s, m);
+        } else {
+            for (int32_t i = s + 1; i < e; ++i) {
+                int32_t v = perm[i];
+                int32_t j = i - 1;
+                while (j >= s && perm[j] > v) {
+                    perm[j + 1] = perm[j];
+                    --j;
+                }
+                perm[j + 1] = v;
             }
-            perm[j + 1] = v;
         }
     }
 }
@@ -681,23 +760,39 @@ __global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, co
                              int64_t cells_cap, int* err, unsigned long long* incons, const int* skip) {
     if (skip && *skip) return;
     int64_t n = count ? *count : N;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
-        int k = inst_of[g];
-        const GridInst& G = gi[k];
-        int64_t f;
-        if (!cell_flat(x, N, g, nd, G, &f) || G.cellbase + f >= cells_cap) {
-            atomicOr(err, ERR_CAPACITY);
-            continue;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    // whole warps iterate together (warp-aggregated histogram; the previous
+    // particle's cell comes from the neighbouring lane)
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {
+        const int64_t g = g0 + threadIdx.x;
+        bool valid = g < n;
+        int k = -1;
+        int64_t f = -1;
+        if (valid) {
+            k = inst_of[g];
+            const GridInst& G = gi[k];
+            if (!cell_flat(x, N, g, nd, G, &f) || G.cellbase + f >= cells_cap) {
+                atomicOr(err, ERR_CAPACITY);
+                valid = false;
+                f = -1;
+            }
         }
-        atomicAdd(&hist[G.cellbase + f], 1);
+        const int32_t cell = valid ? (int32_t)(gi[k].cellbase + f) : -1;
+        warp_agg_inc(hist, cell, valid);
         // src/Interaction.jl:214-236 assumes the sort order makes cells
         // non-decreasing; count the places where it does not.
-        if (g > 0 && inst_of[g - 1] == k) {
-            int64_t fp;
-            if (cell_flat(x, N, g - 1, nd, G, &fp) && fp > f) {
-                atomicAdd(incons, 1ull);
-                atomicOr(err, ERR_GRID_INCONS);
-            }
+        int64_t fp = __shfl_up_sync(FULL, f, 1);
+        int kp = __shfl_up_sync(FULL, k, 1);
+        bool have = lane > 0;
+        if (lane == 0 && valid && g > 0) {
+            kp = inst_of[g - 1];
+            have = kp == k && cell_flat(x, N, g - 1, nd, gi[k], &fp);
+        }
+        if (valid && have && kp == k && fp > f) {
+            atomicAdd(incons, 1ull);
+            atomicOr(err, ERR_GRID_INCONS);
         }
     }
 }

@@ -5,6 +5,7 @@
 #include "gc_device.cuh"
 #include "gc_force.h"
 #include "gc_kernels.h"
+#include "gc_pack.cuh"
 
 namespace gc {
 
@@ -105,36 +106,10 @@ __global__ void k_aux(int mode, int64_t N, const int64_t* count, const double* _
     }
 }
 
-__global__ void k_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* __restrict__ x,
-                         const double* __restrict__ v, const double* __restrict__ rho,
-                         const double* __restrict__ p, const double* __restrict__ stress,
-                         const int32_t* __restrict__ inst_of, const double* __restrict__ mass,
-                         double* __restrict__ xpk, float* __restrict__ pk) {
-    const int64_t n = count ? *count : N;
-    const int R = pack_stride(nd, ns);
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
-        if (xpk) {
-            // 16-byte stores: (x, y) then (z, 0) in 3-D
-            double2* o = reinterpret_cast<double2*>(xpk + g * pos_stride(nd));
-            o[0] = make_double2(x[g], x[N + g]);
-            if (nd == 3) o[1] = make_double2(x[2 * N + g], 0.0);
-        }
-        if (!pk) continue;
-        float rec[16];
-        const double r = rho[g];
-        for (int d = 0; d < nd; ++d) rec[d] = (float)v[d * N + g];
-        rec[nd] = (float)r;
-        double aux;
-        if (mode == AUX_P_OVER_RHO2) aux = p ? p[g] / (r * r) : 0.0;  // boundaries may have no pressure
-        else if (mode == AUX_INV_RHO2) aux = 1.0 / (r * r);
-        else aux = mass[inst_of[g]] / r;
-        rec[nd + 1] = (float)aux;
-        rec[nd + 2] = (float)(1.0 / r);
-        for (int q = 0; q < ns; ++q) rec[nd + 3 + q] = stress ? (float)stress[q * N + g] : 0.0f;
-        for (int q = nd + 3 + ns; q < R; ++q) rec[q] = 0.0f;
-        float4* o = reinterpret_cast<float4*>(pk + g * R);
-        for (int q = 0; q < R / 4; ++q) o[q] = make_float4(rec[4 * q], rec[4 * q + 1], rec[4 * q + 2], rec[4 * q + 3]);
-    }
+__global__ void k_pack32(PackArgs a, const int64_t* count) {
+    const int64_t n = count ? *count : a.N;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x)
+        pack_one(a, g);
 }
 
 void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, const double* x, const double* v,
@@ -143,7 +118,8 @@ void launch_pack32(int mode, int64_t N, const int64_t* count, int nd, int ns, co
     if (N <= 0 || (!xpk && !pk)) return;
     int64_t blocks = (N + 255) / 256;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    k_pack32<<<(int)blocks, 256, 0, s>>>(mode, N, count, nd, ns, x, v, rho, p, stress, inst_of, mass, xpk, pk);
+    PackArgs a{mode, nd, ns, N, x, v, rho, p, stress, inst_of, mass, xpk, pk};
+    k_pack32<<<(int)blocks, 256, 0, s>>>(a, count);
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

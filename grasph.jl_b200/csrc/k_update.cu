@@ -7,6 +7,7 @@
 #include "gc_device.cuh"
 #include "gc_kernels.h"
 #include "gc_update.h"
+#include "gc_pack.cuh"
 
 namespace gc {
 
@@ -18,20 +19,36 @@ static inline int ublk(int64_t n) {
 }
 
 // src/TimeIntegration.jl:158 (_halfstep_ps!) with the q0 snapshot of :220.
+__device__ __forceinline__ void halfstep_one(const StepArgs& a, int64_t g) {
+    const SysInst& S = a.inst[a.inst_of[g]];
+    const double h = S.half_dt;
+    for (int d = 0; d < a.nd; ++d) {
+        double v = a.v[d * a.N + g];
+        a.q0v[d * a.N + g] = v;
+        a.v[d * a.N + g] = v + h * a.dvdt[d * a.N + g];
+        a.dvdt[d * a.N + g] = S.srcv[d];
+    }
+    double r = a.rho[g];
+    a.q0rho[g] = r;
+    a.rho[g] = fma(h, a.drhodt[g], r);
+    a.drhodt[g] = S.srcrho;
+}
+
 __global__ void k_halfstep(StepArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x)
+        halfstep_one(a, g);
+}
+
+template <int KIND>
+__device__ __forceinline__ void update_one(const UpdArgs& a, int64_t g);
+
+// KIND: the updater's GC_UPD_* kind, or -1 for none
+template <int KIND>
+__global__ void k_halfstep_fused(StepArgs a, UpdArgs u, PackArgs pk) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
-        const SysInst& S = a.inst[a.inst_of[g]];
-        const double h = S.half_dt;
-        for (int d = 0; d < a.nd; ++d) {
-            double v = a.v[d * a.N + g];
-            a.q0v[d * a.N + g] = v;
-            a.v[d * a.N + g] = v + h * a.dvdt[d * a.N + g];
-            a.dvdt[d * a.N + g] = S.srcv[d];
-        }
-        double r = a.rho[g];
-        a.q0rho[g] = r;
-        a.rho[g] = fma(h, a.drhodt[g], r);
-        a.drhodt[g] = S.srcrho;
+        halfstep_one(a, g);
+        if (KIND >= 0) update_one<KIND>(u, g);
+        if (pk.pk || pk.xpk) pack_one(pk, g);
     }
 }
 
@@ -168,6 +185,16 @@ void launch_halfstep(const StepArgs& a, cudaStream_t s) {
     if (a.N > 0) k_halfstep<<<ublk(a.N), UTPB, 0, s>>>(a);
     g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
 }
+void launch_halfstep_fused(const StepArgs& a, const UpdArgs& u, const PackArgs& pk, cudaStream_t s) {
+    if (a.N <= 0) return;
+    switch (u.kind) {
+        case GC_UPD_ZERO_FIELDS: k_halfstep_fused<GC_UPD_ZERO_FIELDS><<<ublk(a.N), UTPB, 0, s>>>(a, u, pk); break;
+        case GC_UPD_TAIT_EOS: k_halfstep_fused<GC_UPD_TAIT_EOS><<<ublk(a.N), UTPB, 0, s>>>(a, u, pk); break;
+        case GC_UPD_LINEAR_EOS: k_halfstep_fused<GC_UPD_LINEAR_EOS><<<ublk(a.N), UTPB, 0, s>>>(a, u, pk); break;
+        default: k_halfstep_fused<-1><<<ublk(a.N), UTPB, 0, s>>>(a, u, pk); break;
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
 void launch_fullstep(const StepArgs& a, cudaStream_t s) {
     if (a.N > 0) k_fullstep<<<ublk(a.N), UTPB, 0, s>>>(a);
     g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
@@ -238,13 +265,24 @@ __device__ __forceinline__ void ep_update(const UpdInst& u, double dt, double* s
     ep[3] = ep[3] + depxy;
 }
 
+// One kernel per updater kind, so the light equation-of-state kinds are not
+// held to the registers of the stress return mappings.
+template <int KIND>
 __global__ void k_update(UpdArgs a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x)
+        update_one<KIND>(a, g);
+}
+
+// One particle's updater of kind KIND (src/StateUpdaters.jl), the body of
+// k_update.
+template <int KIND>
+__device__ __forceinline__ void update_one(const UpdArgs& a, int64_t g) {
     const int64_t N = a.N;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
+    {
         const int k = a.inst_of[g];
         const UpdInst& u = a.u[k];
         const double dt = isnan(a.dt) ? a.inst[k].dt : a.dt;
-        switch (u.kind) {
+        switch (KIND) {
             case GC_UPD_ZERO_FIELDS:
                 if ((u.zmask >> GC_FIELD_STRAIN_RATE) & 1u)
                     for (int q = 0; q < a.ns; ++q) a.sr[q * N + g] = 0.0;
@@ -340,8 +378,21 @@ __global__ void k_update(UpdArgs a) {
 }
 
 void launch_update(const UpdArgs& a, cudaStream_t s) {
-    if (a.N > 0) k_update<<<ublk(a.N), UTPB, 0, s>>>(a);
-    g_launches.fetch_add(a.N > 0, std::memory_order_relaxed);
+    if (a.N <= 0) return;
+    switch (a.kind) {
+        case GC_UPD_ZERO_FIELDS: k_update<GC_UPD_ZERO_FIELDS><<<ublk(a.N), UTPB, 0, s>>>(a); break;
+        case GC_UPD_TAIT_EOS: k_update<GC_UPD_TAIT_EOS><<<ublk(a.N), UTPB, 0, s>>>(a); break;
+        case GC_UPD_LINEAR_EOS: k_update<GC_UPD_LINEAR_EOS><<<ublk(a.N), UTPB, 0, s>>>(a); break;
+        case GC_UPD_ELASTOPLASTIC: k_update<GC_UPD_ELASTOPLASTIC><<<ublk(a.N), UTPB, 0, s>>>(a); break;
+        case GC_UPD_VISCOPLASTIC_MC: k_update<GC_UPD_VISCOPLASTIC_MC><<<ublk(a.N), UTPB, 0, s>>>(a); break;
+        case GC_UPD_HOOKE: k_update<GC_UPD_HOOKE><<<ublk(a.N), UTPB, 0, s>>>(a); break;
+        default: return;  // no per-particle work
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+bool halfstep_fuses(int kind) {
+    return kind == GC_UPD_ZERO_FIELDS || kind == GC_UPD_TAIT_EOS || kind == GC_UPD_LINEAR_EOS;
 }
 
 // ----------------------------------------------------------- virtual systems
