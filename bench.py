@@ -550,35 +550,27 @@ def run_batched(args, rank, world, local_rank):
     sweep_ms = st1["sweep_ms"] - st0["sweep_ms"]
     sweep_launches = max(1, st1["sweep_launches"] - st0["sweep_launches"])
 
-    # one at a time, plain FP64: a size-stratified sample of the instances,
-    # each timed alone; time per step is fitted as a + b·n over the sample
-    # and summed over all instances
+    # one at a time, plain FP64: every instance stepped alone in its own
+    # session, each timed over the same step count after its own warm-up
     one = None
     if not args.no_fp64_compare:
-        order = np.argsort([m["n_fluid"] for _, m in mix])
-        pick = [int(order[int(round(q * (len(order) - 1)))]) for q in np.linspace(0.0, 1.0, 8)]
-        ns, tms = [], []
         sample_steps = max(10, min(args.steps, 100))
         a2 = argparse.Namespace(**vars(args))
         a2.steps = sample_steps
-        for k in pick:
-            lf1, m1 = scenarios.batched_columns(count=count)[k]
+        total_ms = 0.0
+        for k, (lf1, m1) in enumerate(scenarios.batched_columns(count=count)):
             s1 = G.Session([lf1], device=local_rank, precision=G.PRECISION_FP64)
             s1.push()
             lib.gc_stream(s1.backend.ctx, engine.ct.byref(sptr))
             st = torch.cuda.ExternalStream(sptr.value)
             t1, _, _, _ = _timed_steps(s1, m1, a2, lib, s1.backend, st, dist, False, local_rank)
-            ns.append(m1["n_fluid"])
-            tms.append(t1 / sample_steps)
+            total_ms += t1 / sample_steps
             s1.close()
-        b, a = np.polyfit(np.array(ns, float), np.array(tms, float), 1)
-        total_ms = float(sum(a + b * m["n_fluid"] for _, m in mix))
         v1 = n_tot / (total_ms / 1e3)
         one = {"value": v1, "unit": "particle-steps/s", "speedup": value / v1,
                "ms_per_step_all_instances": total_ms,
-               "sample": f"{len(pick)} instances (size quantiles), {sample_steps} steps each after "
-                         f"{args.warmup} warm-up steps; time per step fitted as a + b*n "
-                         f"(a={a:.4f} ms, b={b * 1e6:.4f} ms per 1e6 particles) and summed"}
+               "sample": f"all {count} instances, each alone in the plain FP64 path, {sample_steps} steps each "
+                         f"after {args.warmup} warm-up steps (CUDA events), summed"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
@@ -604,13 +596,15 @@ def serve_requests(rate, count, seed):
     """The serving mix: Poisson arrivals at `rate` req/s; 70% 2-D
     Drucker-Prager column collapses (N ~ logU[5k, 200k], parameters as the
     batched columns), 30% 3-D dam breaks (N ~ logU[50k, 1M] fluid, dx scaled
-    so the 2:1:4 block holds N); 1000 steps each."""
+    so the 2:1:4 block holds N); 1000 steps each.  The requests and the
+    unit-rate arrival gaps come from `seed`; `rate` only scales the gaps, so
+    every rate serves the same mix."""
     from grasph_b200 import scenarios
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for _ in range(count):
-        t += rng.exponential(1.0 / rate)
+        t += rng.exponential(1.0) / rate
         if rng.uniform() < 0.7:
             N = math.exp(rng.uniform(math.log(5000), math.log(200000)))
             ar = rng.uniform(0.5, 4.0)
@@ -643,9 +637,10 @@ def run_serve(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     rates = [float(r) for r in args.serve_rates.split(",")]
     count = args.serve_requests
+    seed = 20261203
     per_rate = []
     for rate in rates:
-        reqs = serve_requests(rate, count, seed=20261203 + int(rate))
+        reqs = serve_requests(rate, count, seed)
         built = [(t, _build_request(kind), n, kind) for t, kind, n in reqs]  # host inputs made before timing
         srv = G.Server(device=local_rank, hbm_budget=150 * 10**9, round_steps=args.serve_round,
                        precision=G.PRECISION_FP32_COMPENSATED)
@@ -676,12 +671,35 @@ def run_serve(args, rank, world, local_rank):
         per_rate.append({"rate_req_per_s": rate, "requests": len(ids), "particle_steps": moving,
                          "throughput": moving / wall, "wall_s": wall,
                          "ttc_p50_s": float(np.percentile(ttc, 50)), "ttc_p99_s": float(np.percentile(ttc, 99)),
-                         "rounds": st["rounds"], "repacks": st["repacks"]})
+                         "rounds": st["rounds"], "repacks": st["repacks"],
+                         "repack_s": st["repack_seconds"], "repack_ms_per_request":
+                             1e3 * st["repack_seconds"] / max(1, st["repack_instances"])})
         srv.close()
-    # density error of served requests against the plain FP64 path: the
-    # smallest request of each kind, re-run alone
+    # the same mix one request at a time in the plain FP64 path (each alone
+    # in its own session, back to back, the GPU busy throughout)
+    fp64 = None
+    if not args.no_fp64_compare:
+        reqs = serve_requests(rates[0], count, seed)
+        moving, t_all = 0, 0.0
+        for _, kind, n in reqs:
+            lf, meta = _build_request(kind)
+            s64 = G.Session([lf], device=local_rank)
+            s64.push()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s64.step(n, meta["cfl"])
+            torch.cuda.synchronize()
+            t_all += time.perf_counter() - t0
+            moving += meta["n_fluid"] * n
+            s64.close()
+        fp64 = {"throughput": moving / t_all, "particle_steps": moving, "seconds": t_all,
+                "served_vs_fp64_one_by_one": [r["throughput"] / (moving / t_all) for r in per_rate],
+                "sample": f"the {count} requests of the mix, each alone in the plain FP64 path, stepped "
+                          "back to back (host wall time of the steps, synchronised)"}
+    # density (and stress) error of served requests against the plain FP64
+    # path: the smallest request of each kind, re-run alone
     err = {}
-    sample = serve_requests(rates[-1], count, seed=20261203 + int(rates[-1]))
+    sample = serve_requests(rates[-1], count, seed)
     for name in ("column", "dambreak_3d"):
         cand = [(r[1][1].get("nx", 0) * r[1][1].get("ny", 0) * r[1][1].get("nz", 1), r) for r in sample
                 if r[1][0] == name]
@@ -700,12 +718,8 @@ def run_serve(args, rank, world, local_rank):
         s64.step(n, m32["cfl"])
         s64.pull(with_ghosts=False)
         s64.close()
-        a, b = lf32.systems[0], lf64.systems[0]
-        ia, ib = np.argsort(a.id), np.argsort(b.id)
-        e = {"rho": float(np.abs(a.rho[ia] - b.rho[ib]).max() / np.abs(b.rho).max())}
-        if hasattr(a, "stress"):
-            e["stress"] = float(np.abs(a.stress[ia] - b.stress[ib]).max() / np.abs(b.stress).max())
-        err[name] = dict(e, steps=n, particles=int(m32["n_fluid"]))
+        err[name] = dict(_rel_errors(lf32, lf64, m32, n), steps=n, particles=int(m32["n_fluid"]),
+                         metric=ERROR_METRIC)
     top = per_rate[-1]
     line = {
         "metric": METRIC, "value": top["throughput"], "unit": "particle-steps/s", "n_gpus": world,
@@ -714,7 +728,7 @@ def run_serve(args, rank, world, local_rank):
         "config": {"workload": "serving mix (70% 2-D DP columns 5k-200k, 30% 3-D dam breaks 50k-1M)",
                    "requests_per_rate": count, "round_steps": args.serve_round, "hbm_budget_gb": 150,
                    "parallelism": f"replicas x{world}"},
-        "serving": per_rate, "fp32c_vs_fp64": err, "e2e": None, "cpu_baseline": None,
+        "serving": per_rate, "fp64_one_by_one": fp64, "fp32c_vs_fp64": err, "e2e": None, "cpu_baseline": None,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -727,8 +741,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dambreak_3d", choices=["dambreak_3d", "dambreak_2d", "column", "batched", "serve"])
-    ap.add_argument("--serve-rates", default="10,100,500")
-    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rates", default="10,20,50,100,200,500")
+    ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-round", type=int, default=50)
     ap.add_argument("--scale", default="full", choices=["full", "small"])
     ap.add_argument("--precision", default="fp32c", choices=["fp64", "fp32c"])

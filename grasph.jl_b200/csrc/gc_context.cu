@@ -252,6 +252,11 @@ struct gc_ctx {
     int device = 0;
     size_t budget = 0, allocated = 0;
     cudaStream_t stream = nullptr;
+    // device memory: cudaMalloc/cudaFree, or (contexts a server builds) a
+    // stream-ordered pool that keeps freed memory for the next context, so
+    // building and dropping a context neither maps memory nor waits on the
+    // whole device
+    cudaMemPool_t pool = nullptr;
     std::string err;
     std::vector<HInst> inst;
     bool finalized = false;
@@ -268,6 +273,8 @@ struct gc_ctx {
     int64_t cap_keyN = 0, cap_cells = 0, cap_scan = 0;
     unsigned long long* bbox_scratch = nullptr;
     int* d_err = nullptr;
+    int* d_unsorted = nullptr;                     // a slot sort's keys were out of order
+    unsigned long long* d_sorts_in_order = nullptr;  // slot sorts that found their keys in order
     unsigned long long* d_incons = nullptr;
     int64_t* d_need = nullptr;
     int64_t* h_need = nullptr;  // pinned
@@ -379,7 +386,7 @@ int dalloc(gc_ctx* ctx, T** p, size_t count) {
     if (ctx->budget && ctx->allocated + bytes > ctx->budget)
         return seterr(ctx, GC_ERR_OOM, "device budget of %zu bytes exceeded", ctx->budget);
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes);
+    cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(&q, bytes, ctx->pool, ctx->stream) : cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return seterr(ctx, GC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
     CU(cudaMemsetAsync(q, 0, bytes, ctx->stream));
     ctx->allocated += bytes;
@@ -387,11 +394,18 @@ int dalloc(gc_ctx* ctx, T** p, size_t count) {
     return GC_OK;
 }
 
+// Device memory back to where it came from (stream-ordered into the pool).
+void dev_free(gc_ctx* ctx, void* p) {
+    if (!p) return;
+    if (ctx->pool) cudaFreeAsync(p, ctx->stream);
+    else cudaFree(p);
+}
+
 template <class T>
 void dfree(gc_ctx* ctx, T*& p, size_t count) {
     if (p) {
         ctx->alloc_epoch++;
-        cudaFree(p);
+        dev_free(ctx, p);
         size_t bytes = count * sizeof(T);
         ctx->allocated -= std::min(ctx->allocated, bytes ? bytes : 16);
         p = nullptr;
@@ -1003,6 +1017,8 @@ int finalize(gc_ctx* ctx) {
     TRY(dalloc(ctx, &ctx->bbox_scratch, (size_t)ninst * 2 * MAXD + 1));  // + block counter
     launch_bbox_reset(ctx->bbox_scratch, ninst, ctx->stream);
     TRY(dalloc(ctx, &ctx->d_err, 1));
+    TRY(dalloc(ctx, &ctx->d_unsorted, 1));
+    TRY(dalloc(ctx, &ctx->d_sorts_in_order, 1));
     TRY(dalloc(ctx, &ctx->d_incons, 1));
     TRY(dalloc(ctx, &ctx->d_total_cells, 1));
     ctx->nneed = (int)(ctx->slots.size() + ctx->ghosts.size() + ctx->inters.size());
@@ -1121,10 +1137,11 @@ int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells, const i
     GatherArgs ga{};
     if (S) {
         launch_sort_keys(S->F(F_X), S->N, S->nd, S->inst_of, nullptr, S->d_inst, ctx->key, ctx->hist, cells,
-                         ctx->d_err, ctx->stream);
+                         ctx->d_err, ctx->stream, ctx->d_unsorted);
         scan_exclusive_clear(ctx->hist, ctx->start, cells, ctx->scan_tmp, ctx->stream);
-        launch_sort_scatter(ctx->key, S->N, nullptr, ctx->start, ctx->fill, ctx->perm, ctx->stream);
-        launch_sort_fixup_clear(ctx->start, cells, total, ctx->perm, ctx->fill, ctx->stream);
+        launch_sort_scatter(ctx->key, S->N, nullptr, ctx->start, ctx->fill, ctx->perm, ctx->stream, ctx->d_unsorted);
+        launch_sort_fixup_clear(ctx->start, cells, total, ctx->perm, ctx->fill, ctx->stream, ctx->d_unsorted,
+                                ctx->d_sorts_in_order);
         for (int f = 0; f < NF; ++f)
             if (S->ncomp[f]) {
                 ga.src[ga.nf] = S->F(f);
@@ -1134,6 +1151,7 @@ int sort_particles_slot(gc_ctx* ctx, DSlot* S, DGhost* G, int64_t cells, const i
         ga.isrc[0] = S->id[S->cur];
         ga.idst[0] = S->id[S->cur ^ 1];
         ga.ni = 1;
+        ga.clear = ctx->d_unsorted;
         launch_gather_fields(ga, S->N, ctx->perm, nullptr, ctx->stream);
         S->cur ^= 1;
         S->xpk_static = false;
@@ -2553,6 +2571,7 @@ int run_steps(gc_ctx* ctx, int nsteps) {
                 ctx->graphs.emplace_back();
                 cap_err = capture_step(ctx, ctx->graphs.back());
                 if (cap_err != GC_OK) {
+                    cudaGetLastError();  // the steps continue exactly
                     ctx->graphs.pop_back();
                     break;
                 }
@@ -2636,96 +2655,98 @@ int gc_ctx_destroy(gc_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto& S : ctx->slots) {
         for (int b = 0; b < 2; ++b) {
-            for (int f = 0; f < NF; ++f) cudaFree(S.f[b][f]);
-            cudaFree(S.id[b]);
+            for (int f = 0; f < NF; ++f) dev_free(ctx, S.f[b][f]);
+            dev_free(ctx, S.id[b]);
         }
-        cudaFree(S.q0v);
-        cudaFree(S.q0rho);
-        cudaFree(S.accv);
-        cudaFree(S.accrho);
-        cudaFree(S.aux);
-        cudaFree(S.inst_of);
-        cudaFree(S.groups);
-        cudaFree(S.d_ngroups);
-        cudaFree(S.gcnt);
-        cudaFree(S.goff);
-        cudaFree(S.d_inst);
-        cudaFree(S.d_mass);
-        cudaFree(S.d_c);
-        cudaFree(S.d_massf);
-        cudaFree(S.d_cf);
-        cudaFree(S.fpk);
+        dev_free(ctx, S.q0v);
+        dev_free(ctx, S.q0rho);
+        dev_free(ctx, S.accv);
+        dev_free(ctx, S.accrho);
+        dev_free(ctx, S.aux);
+        dev_free(ctx, S.inst_of);
+        dev_free(ctx, S.groups);
+        dev_free(ctx, S.d_ngroups);
+        dev_free(ctx, S.gcnt);
+        dev_free(ctx, S.goff);
+        dev_free(ctx, S.d_inst);
+        dev_free(ctx, S.d_mass);
+        dev_free(ctx, S.d_c);
+        dev_free(ctx, S.d_massf);
+        dev_free(ctx, S.d_cf);
+        dev_free(ctx, S.fpk);
         for (auto& ch : S.d_upd)
-            for (auto* p : ch) cudaFree(p);
+            for (auto* p : ch) dev_free(ctx, p);
     }
     for (auto& G : ctx->ghosts) {
         for (int b = 0; b < 2; ++b) {
-            cudaFree(G.x[b]);
-            cudaFree(G.io[b]);
-            cudaFree(G.ib[b]);
-            cudaFree(G.ginst[b]);
+            dev_free(ctx, G.x[b]);
+            dev_free(ctx, G.io[b]);
+            dev_free(ctx, G.ib[b]);
+            dev_free(ctx, G.ginst[b]);
         }
-        cudaFree(G.normals);
-        cudaFree(G.v);
-        cudaFree(G.rho);
-        cudaFree(G.p);
-        cudaFree(G.stress);
-        cudaFree(G.aux);
-        cudaFree(G.flags);
-        cudaFree(G.pos);
-        cudaFree(G.d_count);
-        cudaFree(G.d_gh);
-        cudaFree(G.d_inst);
-        cudaFree(G.d_mass);
-        cudaFree(G.d_c);
-        cudaFree(G.fpk);
-        cudaFree(G.groups);
-        cudaFree(G.d_ngroups);
-        cudaFree(G.gcnt);
-        cudaFree(G.goff);
-        cudaFree(G.gadj);
+        dev_free(ctx, G.normals);
+        dev_free(ctx, G.v);
+        dev_free(ctx, G.rho);
+        dev_free(ctx, G.p);
+        dev_free(ctx, G.stress);
+        dev_free(ctx, G.aux);
+        dev_free(ctx, G.flags);
+        dev_free(ctx, G.pos);
+        dev_free(ctx, G.d_count);
+        dev_free(ctx, G.d_gh);
+        dev_free(ctx, G.d_inst);
+        dev_free(ctx, G.d_mass);
+        dev_free(ctx, G.d_c);
+        dev_free(ctx, G.fpk);
+        dev_free(ctx, G.groups);
+        dev_free(ctx, G.d_ngroups);
+        dev_free(ctx, G.gcnt);
+        dev_free(ctx, G.goff);
+        dev_free(ctx, G.gadj);
     }
     for (auto& V : ctx->virts) {
-        cudaFree(V.wsum);
-        cudaFree(V.wsum_alt);
-        cudaFree(V.d_vi);
+        dev_free(ctx, V.wsum);
+        dev_free(ctx, V.wsum_alt);
+        dev_free(ctx, V.d_vi);
         for (auto& chain : V.d_upd)
-            for (auto* p : chain) cudaFree(p);
+            for (auto* p : chain) dev_free(ctx, p);
     }
     for (auto& D : ctx->inters) {
-        cudaFree(D.d_gi);
-        cudaFree(D.d_gi_b);
-        for (auto* p : D.d_pi) cudaFree(p);
-        cudaFree(D.cs);
-        cudaFree(D.cs_a);
-        cudaFree(D.counts);
-        cudaFree(D.d_keep);
-        cudaFree(D.d_gi_prev);
+        dev_free(ctx, D.d_gi);
+        dev_free(ctx, D.d_gi_b);
+        for (auto* p : D.d_pi) dev_free(ctx, p);
+        dev_free(ctx, D.cs);
+        dev_free(ctx, D.cs_a);
+        dev_free(ctx, D.counts);
+        dev_free(ctx, D.d_keep);
+        dev_free(ctx, D.d_gi_prev);
     }
-    cudaFree(ctx->key);
-    cudaFree(ctx->perm);
-    cudaFree(ctx->hist);
-    cudaFree(ctx->start);
-    cudaFree(ctx->fill);
-    cudaFree(ctx->scan_tmp);
-    cudaFree(ctx->bbox_scratch);
-    cudaFree(ctx->d_err);
-    cudaFree(ctx->d_incons);
-    cudaFree(ctx->d_need);
-    cudaFree(ctx->d_total_cells);
+    dev_free(ctx, ctx->key);
+    dev_free(ctx, ctx->perm);
+    dev_free(ctx, ctx->hist);
+    dev_free(ctx, ctx->start);
+    dev_free(ctx, ctx->fill);
+    dev_free(ctx, ctx->scan_tmp);
+    dev_free(ctx, ctx->bbox_scratch);
+    dev_free(ctx, ctx->d_err);
+    dev_free(ctx, ctx->d_unsorted);
+    dev_free(ctx, ctx->d_sorts_in_order);
+    dev_free(ctx, ctx->d_incons);
+    dev_free(ctx, ctx->d_need);
+    dev_free(ctx, ctx->d_total_cells);
     if (ctx->h_need) cudaFreeHost(ctx->h_need);
-    cudaFree(ctx->d_need_max);
-    cudaFree(ctx->d_need_cap);
-    cudaFree(ctx->d_plan_args);
+    dev_free(ctx, ctx->d_need_max);
+    dev_free(ctx, ctx->d_need_cap);
+    dev_free(ctx, ctx->d_plan_args);
     if (ctx->h_need_max) cudaFreeHost(ctx->h_need_max);
     drop_graphs(ctx);
     for (auto& sn : ctx->snaps) {
-        for (int f = 0; f < NF; ++f) cudaFree(sn.f[f]);
-        cudaFree(sn.id);
+        for (int f = 0; f < NF; ++f) dev_free(ctx, sn.f[f]);
+        dev_free(ctx, sn.id);
     }
-    cudaFree(ctx->staging);
-    cudaFree(ctx->d_ioflags);
-    cudaFree(ctx->d_pairs);
+    dev_free(ctx, ctx->staging);
+    dev_free(ctx, ctx->d_ioflags);
+    dev_free(ctx, ctx->d_pairs);
     for (auto& e : ctx->ev_pool) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
@@ -2734,6 +2755,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
+    if (ctx->pool) cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GC_OK;
@@ -3549,6 +3571,11 @@ int gc_get_stats(gc_ctx* ctx, gc_stats* out) {
         TRY(hcopy(ctx, &v, ctx->d_incons, sizeof v, cudaMemcpyDeviceToHost));
         out->grid_inconsistent = (int64_t)v;
     }
+    if (ctx->d_sorts_in_order) {
+        unsigned long long v = 0;
+        TRY(hcopy(ctx, &v, ctx->d_sorts_in_order, sizeof v, cudaMemcpyDeviceToHost));
+        out->sorts_in_order = (int64_t)v;
+    }
     return GC_OK;
 }
 
@@ -3856,6 +3883,22 @@ bool ctx_same_structure(gc_ctx* a, int ia, gc_ctx* b, int ib) {
 }
 
 bool ctx_finalized(gc_ctx* c) { return c->finalized; }
+
+// Move a context to a new stream of the given priority (highest: true),
+// once its queued work is done.  Blocks of a higher-priority stream are
+// dispatched before pending blocks of others, so a context being built while
+// other contexts step does not wait behind their kernels at every sync.
+int ctx_set_priority(gc_ctx* ctx, bool highest) {
+    gc_ctx* c = ctx;
+    int least = 0, greatest = 0;
+    CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    cudaStream_t ns = nullptr;
+    CU(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, highest ? greatest : least));
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+    c->stream = ns;
+    return GC_OK;
+}
 int ctx_ninst(gc_ctx* c) { return (int)c->inst.size(); }
 
 int ctx_set_cfl(gc_ctx* c, int inst, double cfl) {
@@ -3930,46 +3973,67 @@ int64_t ctx_estimate_bytes(gc_ctx* m, int inst) {
     return b + b / 4;
 }
 
+// An instance's model without its staged field bytes (they can be hundreds
+// of MB of host memory and are read from the source where needed).
+HInst model_of(HInst& from) {
+    std::vector<HStaged> keep;
+    keep.swap(from.staged);
+    HInst out = from;
+    from.staged.swap(keep);
+    return out;
+}
+
 // A context with no device state holding one instance's model (no staged
 // fields): the structure a batch of the serving loop is keyed by.
 int ctx_model_copy(gc_ctx* m, int inst, gc_ctx** out) {
     gc_ctx* c = nullptr;
     TRY(gc_ctx_create(m->device, 0, &c));
-    c->inst.push_back(m->inst[inst]);
-    c->inst.back().staged.clear();
+    c->inst.push_back(model_of(m->inst[inst]));
     *out = c;
     return GC_OK;
 }
 
 int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pair<gc_ctx*, int>>& src,
-             gc_ctx** out, std::string* err) {
+             gc_ctx** out, std::string* err, cudaMemPool_t pool) {
     *out = nullptr;
     gc_ctx* ctx = nullptr;
     TRY(gc_ctx_create(device, budget, &ctx));
+    ctx->pool = pool;
+    if (pool) TRY(ctx_set_priority(ctx, true));
     auto fail = [&](int st) {
         if (err) *err = ctx->err;
         gc_ctx_destroy(ctx);
         return st;
     };
-    for (auto& p : src) {
-        ctx->inst.push_back(p.first->inst[p.second]);
-        ctx->inst.back().staged.clear();
-    }
+    for (auto& p : src) ctx->inst.push_back(model_of(p.first->inst[p.second]));
     int st = gc_finalize(ctx);
     if (st) return fail(st);
     st = gc_set_precision(ctx, precision);
     if (st) return fail(st);
+    // the sweep configurations a running context of this structure tuned
+    // carry over (the structure, and so the tuner's keys, are the same)
+    for (auto& p : src)
+        if (p.first->finalized && p.first->precision == precision && p.first->force_cfg < 0) {
+            for (auto& kv : p.first->tune)
+                if (kv.second.best >= 0) ctx->tune[kv.first] = kv.second;
+            break;
+        }
     // device state of instances that come from running contexts
     for (auto& p : src)
         if (p.first->finalized) cudaStreamSynchronize(p.first->stream);
-    PackSeg* d_seg = nullptr;
-    if (cudaMalloc(&d_seg, sizeof(PackSeg) * std::max<size_t>(src.size(), 1)) != cudaSuccess)
-        return fail(seterr(ctx, GC_ERR_OOM, "pack table"));
+    // every (slot, field) segment table in one upload, then the copies
+    std::vector<PackSeg> tab;
+    struct Launch {
+        size_t off, n;
+        int64_t nmax;
+        int slot, field;
+    };
+    std::vector<Launch> launches;
     for (size_t s = 0; s < ctx->slots.size(); ++s) {
         DSlot& D = ctx->slots[s];
         for (int f = -1; f < NF; ++f) {  // -1: ids
             if (f >= 0 && !D.ncomp[f]) continue;
-            std::vector<PackSeg> seg;
+            const size_t off = tab.size();
             int64_t nmax = 0;
             for (size_t k = 0; k < src.size(); ++k) {
                 gc_ctx* sc = src[k].first;
@@ -3983,25 +4047,36 @@ int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pa
                 g.dst_base = D.h_inst[k].base;
                 g.n = S.h_inst[si].n;
                 nmax = std::max(nmax, g.n);
-                seg.push_back(g);
+                tab.push_back(g);
             }
-            if (seg.empty() || nmax == 0) continue;
-            if (cudaMemcpyAsync(d_seg, seg.data(), sizeof(PackSeg) * seg.size(), cudaMemcpyHostToDevice,
-                                ctx->stream) != cudaSuccess) {
-                cudaFree(d_seg);
-                return fail(seterr(ctx, GC_ERR_CUDA, "pack table upload"));
+            if (tab.size() == off || nmax == 0) {
+                tab.resize(off);
+                continue;
             }
-            dim3 grid((unsigned)std::min<int64_t>((nmax + 255) / 256, 64), (unsigned)seg.size());
-            if (f < 0) k_pack<int32_t><<<grid, 256, 0, ctx->stream>>>(d_seg, 1, D.id[D.cur], D.N);
-            else k_pack<double><<<grid, 256, 0, ctx->stream>>>(d_seg, D.ncomp[f], D.F(f), D.N);
-            g_launches.fetch_add(1, std::memory_order_relaxed);
-            // the table is reused by the next launch: wait for this one
-            cudaStreamSynchronize(ctx->stream);
+            launches.push_back({off, tab.size() - off, nmax, (int)s, f});
         }
         for (size_t k = 0; k < src.size(); ++k)
             if (src[k].first->finalized) D.nonzero_kin[k] = src[k].first->slots[s].nonzero_kin[src[k].second];
     }
-    cudaFree(d_seg);
+    if (!tab.empty()) {
+        PackSeg* d_seg = nullptr;
+        if (dalloc(ctx, &d_seg, tab.size()) != GC_OK) return fail(GC_ERR_OOM);
+        if (cudaMemcpyAsync(d_seg, tab.data(), sizeof(PackSeg) * tab.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+            cudaSuccess) {
+            dfree(ctx, d_seg, tab.size());
+            return fail(seterr(ctx, GC_ERR_CUDA, "pack table upload"));
+        }
+        for (const Launch& L : launches) {
+            DSlot& D = ctx->slots[L.slot];
+            dim3 grid((unsigned)std::min<int64_t>((L.nmax + 255) / 256, 64), (unsigned)L.n);
+            if (L.field < 0) k_pack<int32_t><<<grid, 256, 0, ctx->stream>>>(d_seg + L.off, 1, D.id[D.cur], D.N);
+            else k_pack<double><<<grid, 256, 0, ctx->stream>>>(d_seg + L.off, D.ncomp[L.field], D.F(L.field), D.N);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+        // the host table lives until the copy has run
+        cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, d_seg, tab.size());
+    }
     st = check_launch(ctx, "pack");
     if (st) return fail(st);
     // instances that come from model contexts: their staged fields

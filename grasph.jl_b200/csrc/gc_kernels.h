@@ -35,10 +35,16 @@ void launch_bbox_fused(const double* x, int64_t N, int nd, const int32_t* inst_o
 // Per-instance key lattice from the bbox; writes total cells to *need.
 void launch_sort_plan(SysInst* inst, int ninst, int nd, int64_t* need, int* err, cudaStream_t s);
 // Flat sort key per particle + histogram.
+// `unsorted` (optional): a device flag, zero on entry, that the keys
+// kernel sets when the keys are not already non-decreasing; given to the
+// scatter and the clearing fix-up, a flag left zero makes the sort the
+// identity without the fill counters (src/Sorting.jl:176-186).  The gather
+// that follows clears it (GatherArgs::clear).
 void launch_sort_keys(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
-                      const SysInst* inst, int32_t* key, int32_t* hist, int64_t cells_cap, int* err, cudaStream_t s);
+                      const SysInst* inst, int32_t* key, int32_t* hist, int64_t cells_cap, int* err, cudaStream_t s,
+                      int* unsorted = nullptr);
 void launch_sort_scatter(const int32_t* key, int64_t N, const int64_t* count, const int32_t* start, int32_t* fill,
-                         int32_t* perm, cudaStream_t s);
+                         int32_t* perm, cudaStream_t s, const int* unsorted = nullptr);
 void launch_sort_fixup(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
                        cudaStream_t s);
 void launch_gather(const double* src, double* dst, int ncomp, int64_t N, const int32_t* perm, const int64_t* count,
@@ -46,8 +52,10 @@ void launch_gather(const double* src, double* dst, int ncomp, int64_t N, const i
 void launch_gather_i32(const int32_t* src, int32_t* dst, int64_t N, const int32_t* perm, const int64_t* count,
                        cudaStream_t s);
 // fixup that also zeroes the per-cell fill counters it has consumed
+// (with `unsorted` left zero it only counts the in-order sort)
 void launch_sort_fixup_clear(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
-                             int32_t* fill, cudaStream_t s);
+                             int32_t* fill, cudaStream_t s, const int* unsorted = nullptr,
+                             unsigned long long* in_order_count = nullptr);
 // Every carried field of a slot in one launch.
 constexpr int GATHER_MAX = 16;
 struct GatherArgs {
@@ -57,6 +65,7 @@ struct GatherArgs {
     int ncomp[GATHER_MAX];
     const int32_t* isrc[4];
     int32_t* idst[4];
+    int* clear;  // optional: a sort's order flag, zeroed by the gather
 };
 void launch_gather_fields(const GatherArgs& a, int64_t N, const int32_t* perm, const int64_t* count,
                           cudaStream_t s);

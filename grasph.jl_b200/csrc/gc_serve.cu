@@ -9,7 +9,12 @@
 // Rounds: every batch advances min(round_steps, the fewest steps any of its
 // requests still needs) steps, so a request stops exactly at its step
 // count.  Its result is then copied to host memory and the request leaves
-// the batch at the next repack.
+// the batch at the next repack.  A batch's repack runs on its own host
+// thread just before its steps, so it overlaps the other batches' steps;
+// the server's contexts draw device memory from one stream-ordered pool
+// that keeps freed memory, so a repack maps no new memory and waits on no
+// other stream, and a new context is built on a highest-priority stream so
+// its setup kernels are not queued behind the other batches' sweeps.
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -23,6 +28,8 @@
 #include <utility>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/grasph_cuda.h"
 
 namespace gc {
@@ -30,12 +37,13 @@ bool ctx_same_structure(gc_ctx* a, int ia, gc_ctx* b, int ib);
 bool ctx_finalized(gc_ctx* c);
 int ctx_ninst(gc_ctx* c);
 int ctx_set_cfl(gc_ctx* c, int inst, double cfl);
+int ctx_set_priority(gc_ctx* c, bool highest);
 int64_t ctx_particles(gc_ctx* c, int inst);
 int64_t ctx_moving_particles(gc_ctx* c, int inst);
 int64_t ctx_estimate_bytes(gc_ctx* m, int inst);
 int ctx_model_copy(gc_ctx* m, int inst, gc_ctx** out);
 int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pair<gc_ctx*, int>>& src,
-             gc_ctx** out, std::string* err);
+             gc_ctx** out, std::string* err, cudaMemPool_t pool);
 void ctx_result_fields(gc_ctx* c, int inst, std::vector<std::array<int64_t, 3>>& out);
 const char* ctx_error(gc_ctx* c);
 }  // namespace gc
@@ -87,6 +95,7 @@ struct gc_server {
     size_t used = 0;
     size_t max_batch = 0;  // estimated bytes one batch may hold (bounds a repack's peak)
     int64_t next_id = 1;
+    cudaMemPool_t pool = nullptr;  // device memory of every batch context
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     gc_serve_stats stats{};
     std::string err;
@@ -147,50 +156,99 @@ void admit(gc_server* s) {
     }
 }
 
-// Rebuild a batch's context: the requests of `live` that still run (state
+// One batch's work in a round: the repack (when requests joined or left)
+// and the steps.  The plan is made on the server's thread; `run` touches
+// only the batch's contexts, so batches run it concurrently.
+struct Job {
+    Batch* B = nullptr;
+    bool repack = false;
+    std::vector<std::pair<gc_ctx*, int>> src;  // running instances, then joining models
+    std::vector<int64_t> ids;                  // the batch's requests after the repack
+    std::vector<double> cfl;
+    int steps = 0;
+    double cfl0 = 0;
+    int pack_status = GC_OK;
+    std::string pack_err;
+    double repack_s = 0;
+};
+
+// The batch after a repack: the requests of `live` that still run (state
 // copied on the device from the old context) followed by the joining ones
 // (staged host fields).
-int repack(gc_server* s, Batch& B) {
-    if (!B.dirty && B.joining.empty()) return GC_OK;
-    std::vector<std::pair<gc_ctx*, int>> src;
-    std::vector<int64_t> ids;
-    for (size_t k = 0; k < B.live.size(); ++k)
-        if (s->reqs[B.live[k]].state == RQ_RUNNING) {
-            src.push_back({B.ctx, (int)k});
-            ids.push_back(B.live[k]);
-        }
-    for (int64_t id : B.joining) {
-        src.push_back({s->reqs[id].model, 0});
-        ids.push_back(id);
-    }
-    gc_ctx* nc = nullptr;
-    if (!src.empty()) {
-        std::string e;
-        int st = gc::ctx_pack(s->device, 0, s->precision, src, &nc, &e);
-        if (st != GC_OK) {
-            for (int64_t id : ids) {
-                Request& r = s->reqs[id];
-                r.state = RQ_FAILED;
-                r.err = "repack: " + e;
-                s->used -= std::min(s->used, (size_t)r.est);
+Job plan_round(gc_server* s, Batch& B) {
+    Job J;
+    J.B = &B;
+    J.repack = B.dirty || !B.joining.empty();
+    if (J.repack) {
+        for (size_t k = 0; k < B.live.size(); ++k)
+            if (s->reqs[B.live[k]].state == RQ_RUNNING) {
+                J.src.push_back({B.ctx, (int)k});
+                J.ids.push_back(B.live[k]);
             }
-            B.est = 0;
-            if (B.ctx) gc_ctx_destroy(B.ctx);
-            B.ctx = nullptr;
-            B.live.clear();
-            B.joining.clear();
-            B.dirty = false;
-            return serr(s, st, "repack: " + e);
+        for (int64_t id : B.joining) {
+            J.src.push_back({s->reqs[id].model, 0});
+            J.ids.push_back(id);
         }
-        for (size_t k = 0; k < ids.size(); ++k) gc::ctx_set_cfl(nc, (int)k, s->reqs[ids[k]].cfl);
+    } else {
+        J.ids = B.live;
     }
-    if (B.ctx) gc_ctx_destroy(B.ctx);
-    B.ctx = nc;
-    B.live = ids;
+    int64_t left = s->round_steps;
+    for (int64_t id : J.ids) {
+        const Request& r = s->reqs[id];
+        J.cfl.push_back(r.cfl);
+        left = std::min<int64_t>(left, r.nsteps - r.done);
+    }
+    J.steps = J.ids.empty() ? 0 : (int)std::max<int64_t>(left, 0);
+    J.cfl0 = J.cfl.empty() ? 0.0 : J.cfl[0];
+    return J;
+}
+
+// Repack (a new context replaces the old one) and step.
+void run_round(gc_server* s, Job& J) {
+    Batch& B = *J.B;
+    if (J.repack) {
+        const double t_start = s->now();
+        gc_ctx* nc = nullptr;
+        if (!J.src.empty()) {
+            J.pack_status = gc::ctx_pack(s->device, 0, s->precision, J.src, &nc, &J.pack_err, s->pool);
+            if (J.pack_status == GC_OK)
+                for (size_t k = 0; k < J.ids.size(); ++k) gc::ctx_set_cfl(nc, (int)k, J.cfl[k]);
+        }
+        if (B.ctx) gc_ctx_destroy(B.ctx);
+        B.ctx = J.pack_status == GC_OK ? nc : nullptr;
+        J.repack_s = s->now() - t_start;
+    }
+    if (B.ctx && J.steps > 0) {
+        B.last_status = gc_step(B.ctx, J.steps, J.cfl0);
+        if (B.last_status != GC_OK) B.last_err = gc_last_error(B.ctx);
+    }
+    // a new context is built and takes its first (exact, capturing) steps
+    // on a highest-priority stream, then steps at the normal priority
+    if (J.repack && B.ctx) gc::ctx_set_priority(B.ctx, false);
+}
+
+// The repack's bookkeeping, on the server's thread.
+void finish_repack(gc_server* s, Job& J) {
+    if (!J.repack) return;
+    Batch& B = *J.B;
     B.joining.clear();
     B.dirty = false;
+    if (J.pack_status != GC_OK) {
+        for (int64_t id : J.ids) {
+            Request& r = s->reqs[id];
+            r.state = RQ_FAILED;
+            r.err = "repack: " + J.pack_err;
+            s->used -= std::min(s->used, (size_t)r.est);
+        }
+        B.est = 0;
+        B.live.clear();
+        serr(s, J.pack_status, "repack: " + J.pack_err);
+        return;
+    }
+    B.live = J.ids;
     s->stats.repacks += 1;
-    return GC_OK;
+    s->stats.repack_instances += (int64_t)J.ids.size();
+    s->stats.repack_seconds += J.repack_s;
 }
 
 // After a round of `steps` steps: count them, copy finished results to the
@@ -248,6 +306,18 @@ int gc_serve_create(int device, size_t hbm_budget_bytes, int round_steps, int pr
     s->round_steps = round_steps;
     s->precision = precision;
     s->max_batch = hbm_budget_bytes ? std::max<size_t>(hbm_budget_bytes / 8, (size_t)1 << 30) : (size_t)16 << 30;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+        delete s;
+        return GC_ERR_CUDA;
+    }
+    // keep freed memory in the pool for the next repack (released when the
+    // server is destroyed)
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     *out = s;
     return GC_OK;
 }
@@ -260,6 +330,7 @@ int gc_serve_destroy(gc_server* s) {
     }
     for (auto& kv : s->reqs)
         if (kv.second.model) gc_ctx_destroy(kv.second.model);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return GC_OK;
 }
@@ -289,28 +360,22 @@ int gc_serve_pump(gc_server* s, int* ncompleted) {
     if (!s) return GC_ERR_ARG;
     int done = 0;
     admit(s);
-    for (auto& B : s->batches) repack(s, B);
+    std::vector<Job> jobs;
+    for (auto& B : s->batches)
+        if (B.ctx || !B.joining.empty()) jobs.push_back(plan_round(s, B));
+    // each batch repacks and steps on its own thread (one batch: this one)
+    if (jobs.size() == 1) {
+        run_round(s, jobs[0]);
+    } else {
+        std::vector<std::thread> th;
+        for (auto& J : jobs) th.emplace_back([s, &J] { run_round(s, J); });
+        for (auto& t : th) t.join();
+    }
     // requests that need no steps at all finish now
-    std::vector<Batch*> run;
-    std::vector<int> steps;
-    for (auto& B : s->batches) {
-        if (!B.ctx) continue;
-        int64_t left = s->round_steps;
-        for (int64_t id : B.live) left = std::min<int64_t>(left, s->reqs[id].nsteps - s->reqs[id].done);
-        run.push_back(&B);
-        steps.push_back((int)std::max<int64_t>(left, 0));
+    for (auto& J : jobs) {
+        finish_repack(s, J);
+        if (J.B->ctx) retire(s, *J.B, J.steps, &done);
     }
-    std::vector<std::thread> th;
-    for (size_t i = 0; i < run.size(); ++i) {
-        if (steps[i] == 0) continue;
-        th.emplace_back([&, i] {
-            Batch& B = *run[i];
-            B.last_status = gc_step(B.ctx, steps[i], s->reqs[B.live[0]].cfl);
-            if (B.last_status != GC_OK) B.last_err = gc_last_error(B.ctx);
-        });
-    }
-    for (auto& t : th) t.join();
-    for (size_t i = 0; i < run.size(); ++i) retire(s, *run[i], steps[i], &done);
     s->stats.rounds += 1;
     if (ncompleted) *ncompleted = done;
     return GC_OK;

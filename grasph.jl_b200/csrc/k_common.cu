@@ -279,66 +279,83 @@ void launch_bbox_reset(unsigned long long* scratch, int ninst, cudaStream_t s) {
 __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                              const int64_t* count, unsigned long long* scratch, SysInst* inst, int ninst, int* err,
                              int64_t tiles_per_block) {
-    // each block reduces a contiguous run of 256-particle tiles (as k_bbox
-    // does one), so the block counter below sees few atomics
+    // each block reduces a contiguous run of 256-particle tiles: every thread
+    // keeps the running min/max of its particles while they belong to one
+    // instance (flushing with atomics when the instance changes), and the
+    // block reduces them once at the end, so one block makes 2·nd atomics,
+    // not 2·nd per tile (ordered keys: min/max is exact in any order)
     const int64_t n = count ? *count : N;
+    int krun = -1;
+    unsigned long long amn[MAXD], amx[MAXD];
+    for (int d = 0; d < MAXD; ++d) {
+        amn[d] = ~0ull;
+        amx[d] = 0ull;
+    }
+    bool bad = false;
     for (int64_t tile = (int64_t)blockIdx.x * tiles_per_block;
          tile < (int64_t)(blockIdx.x + 1) * tiles_per_block && tile * blockDim.x < n; ++tile) {
-        int64_t g = tile * blockDim.x + threadIdx.x;
-        bool valid = g < n;
-        int k = valid ? inst_of[g] : -1;
-        unsigned long long mn[MAXD], mx[MAXD];
-        bool bad = false;
-        for (int d = 0; d < MAXD; ++d) {
-            mn[d] = ~0ull;
-            mx[d] = 0ull;
-        }
-        if (valid) {
-            for (int d = 0; d < nd; ++d) {
-                double v = x[d * N + g];
-                if (!isfinite(v)) bad = true;
-                mn[d] = mx[d] = ord_key(v);
+        const int64_t g = tile * blockDim.x + threadIdx.x;
+        if (g >= n) continue;
+        const int k = inst_of[g];
+        if (k != krun) {
+            if (krun >= 0)
+                for (int d = 0; d < nd; ++d) {
+                    atomicMin(&scratch[(krun * 2 + 0) * MAXD + d], amn[d]);
+                    atomicMax(&scratch[(krun * 2 + 1) * MAXD + d], amx[d]);
+                }
+            krun = k;
+            for (int d = 0; d < MAXD; ++d) {
+                amn[d] = ~0ull;
+                amx[d] = 0ull;
             }
         }
-        if (bad) atomicOr(err, ERR_NONFINITE);
-        __shared__ int k0;
-        if (threadIdx.x == 0) k0 = k;
+        for (int d = 0; d < nd; ++d) {
+            const double v = x[d * N + g];
+            if (!isfinite(v)) bad = true;
+            const unsigned long long key = ord_key(v);
+            amn[d] = key < amn[d] ? key : amn[d];
+            amx[d] = key > amx[d] ? key : amx[d];
+        }
+    }
+    if (bad) atomicOr(err, ERR_NONFINITE);
+    // thread 0 holds the block's first particle, so its instance is the
+    // block's whenever the block has any
+    __shared__ int k0;
+    if (threadIdx.x == 0) k0 = krun;
+    __syncthreads();
+    const int uniform = __syncthreads_and(krun < 0 || krun == k0);
+    if (uniform && k0 >= 0) {
+        __shared__ unsigned long long smn[TPB / 32][MAXD], smx[TPB / 32][MAXD];
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int d = 0; d < nd; ++d) {
+            unsigned long long a = amn[d], b = amx[d];
+            for (int o = 16; o > 0; o >>= 1) {
+                unsigned long long a2 = __shfl_down_sync(0xffffffffu, a, o);
+                unsigned long long b2 = __shfl_down_sync(0xffffffffu, b, o);
+                a = a2 < a ? a2 : a;
+                b = b2 > b ? b2 : b;
+            }
+            if (lane == 0) {
+                smn[wid][d] = a;
+                smx[wid][d] = b;
+            }
+        }
         __syncthreads();
-        int uniform = __syncthreads_and(!valid || k == k0);
-        if (uniform && k0 >= 0) {
-            __shared__ unsigned long long smn[TPB / 32][MAXD], smx[TPB / 32][MAXD];
-            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-            for (int d = 0; d < nd; ++d) {
-                unsigned long long a = mn[d], b = mx[d];
-                for (int o = 16; o > 0; o >>= 1) {
-                    unsigned long long a2 = __shfl_down_sync(0xffffffffu, a, o);
-                    unsigned long long b2 = __shfl_down_sync(0xffffffffu, b, o);
-                    a = a2 < a ? a2 : a;
-                    b = b2 > b ? b2 : b;
-                }
-                if (lane == 0) {
-                    smn[wid][d] = a;
-                    smx[wid][d] = b;
-                }
+        if (threadIdx.x < nd) {
+            const int d = threadIdx.x;
+            unsigned long long a = ~0ull, b = 0ull;
+            for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+                a = smn[w][d] < a ? smn[w][d] : a;
+                b = smx[w][d] > b ? smx[w][d] : b;
             }
-            __syncthreads();
-            if (threadIdx.x < nd) {
-                int d = threadIdx.x;
-                unsigned long long a = ~0ull, b = 0ull;
-                for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
-                    a = smn[w][d] < a ? smn[w][d] : a;
-                    b = smx[w][d] > b ? smx[w][d] : b;
-                }
-                atomicMin(&scratch[(k0 * 2 + 0) * MAXD + d], a);
-                atomicMax(&scratch[(k0 * 2 + 1) * MAXD + d], b);
-            }
-        } else if (valid) {
-            for (int d = 0; d < nd; ++d) {
-                atomicMin(&scratch[(k * 2 + 0) * MAXD + d], mn[d]);
-                atomicMax(&scratch[(k * 2 + 1) * MAXD + d], mx[d]);
-            }
+            atomicMin(&scratch[(k0 * 2 + 0) * MAXD + d], a);
+            atomicMax(&scratch[(k0 * 2 + 1) * MAXD + d], b);
         }
-        __syncthreads();  // the shared k0 and partials are reused by the next tile
+    } else if (krun >= 0) {
+        for (int d = 0; d < nd; ++d) {
+            atomicMin(&scratch[(krun * 2 + 0) * MAXD + d], amn[d]);
+            atomicMax(&scratch[(krun * 2 + 1) * MAXD + d], amx[d]);
+        }
     }
     unsigned long long* counter = scratch + (size_t)ninst * 2 * MAXD;
     __shared__ bool last;
@@ -414,57 +431,91 @@ void launch_sort_plan(SysInst* inst, int ninst, int nd, int64_t* need, int* err,
     COUNTED(1);
 }
 
+// The packed cell key of particle g (src/Sorting.jl:157-175): -1 with
+// `bad` set to the error bit when a coordinate is not finite or falls
+// outside the planned cells.
+__device__ __forceinline__ int32_t sort_key_of(const double* __restrict__ x, int64_t N, int nd,
+                                               const int32_t* __restrict__ inst_of, const SysInst* __restrict__ inst,
+                                               int64_t g, int64_t cells_cap, int* bad) {
+    const SysInst& S = inst[inst_of[g]];
+    int64_t flat = 0;
+    bool ok = true;
+    for (int d = 0; d < nd; ++d) {
+        int64_t kd;
+        if (!floor_i64(x[d * N + g] / S.sort_cutoff, &kd)) {
+            ok = false;
+            break;
+        }
+        int64_t rel = kd - S.kmin[d];
+        if (rel < 0 || rel >= S.kext[d]) ok = false;
+        flat = flat * S.kext[d] + rel;
+    }
+    flat += S.sort_cellbase;
+    if (!ok || flat < 0 || flat >= cells_cap) {
+        *bad = ok ? ERR_CAPACITY : ERR_NONFINITE;
+        return -1;
+    }
+    *bad = 0;
+    return (int32_t)flat;
+}
+
 __global__ void k_sort_keys(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                             const int64_t* count, const SysInst* __restrict__ inst, int32_t* __restrict__ key,
-                            int32_t* __restrict__ hist, int64_t cells_cap, int* err) {
+                            int32_t* __restrict__ hist, int64_t cells_cap, int* err, int* unsorted) {
     int64_t n = count ? *count : N;
+    const int lane = threadIdx.x & 31;
     // whole warps iterate together (warp-aggregated histogram)
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {
         const int64_t g = g0 + threadIdx.x;
         bool valid = g < n;
         int32_t kk = -1;
+        int bad = 0;
         if (valid) {
-            const SysInst& S = inst[inst_of[g]];
-            int64_t flat = 0;
-            bool ok = true;
-            for (int d = 0; d < nd; ++d) {
-                int64_t kd;
-                if (!floor_i64(x[d * N + g] / S.sort_cutoff, &kd)) {
-                    ok = false;
-                    break;
-                }
-                int64_t rel = kd - S.kmin[d];
-                if (rel < 0 || rel >= S.kext[d]) ok = false;
-                flat = flat * S.kext[d] + rel;
-            }
-            flat += S.sort_cellbase;
-            if (!ok || flat < 0 || flat >= cells_cap) {
-                atomicOr(err, ok ? ERR_CAPACITY : ERR_NONFINITE);
+            kk = sort_key_of(x, N, nd, inst_of, inst, g, cells_cap, &bad);
+            if (bad) {
+                atomicOr(err, bad);
                 valid = false;
-            } else {
-                kk = (int32_t)flat;
             }
             key[g] = kk;
         }
         warp_agg_inc(hist, kk, valid);
+        if (unsorted) {
+            // keys already non-decreasing (src/Sorting.jl:176-186): lane 0
+            // recomputes the key before its warp, the others take it from
+            // the lane below; an invalid key counts as out of order
+            int32_t prev = __shfl_up_sync(0xffffffffu, kk, 1);
+            if (lane == 0 && g > 0 && g < n) {
+                int pb = 0;
+                prev = sort_key_of(x, N, nd, inst_of, inst, g - 1, cells_cap, &pb);
+            }
+            const bool order_broken = g < n && (bad || (g > 0 && prev > kk));
+            if (__any_sync(0xffffffffu, order_broken) && lane == 0) atomicOr(unsorted, 1);
+        }
     }
 }
 
 void launch_sort_keys(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
-                      const SysInst* inst, int32_t* key, int32_t* hist, int64_t cells_cap, int* err, cudaStream_t s) {
+                      const SysInst* inst, int32_t* key, int32_t* hist, int64_t cells_cap, int* err, cudaStream_t s,
+                      int* unsorted) {
     if (N <= 0) return;
-    k_sort_keys<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, inst, key, hist, cells_cap, err);  // TPB % 32 == 0
+    k_sort_keys<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, inst, key, hist, cells_cap, err,
+                                        unsorted);  // TPB % 32 == 0
     COUNTED(1);
 }
 
 __global__ void k_sort_scatter(const int32_t* __restrict__ key, int64_t N, const int64_t* count,
                                const int32_t* __restrict__ start, int32_t* __restrict__ fill,
-                               int32_t* __restrict__ perm) {
+                               int32_t* __restrict__ perm, const int* unsorted) {
     int64_t n = count ? *count : N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    if (unsorted && *unsorted == 0) {
+        // keys in order: the stable sort is the identity
+        for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) perm[g] = (int32_t)g;
+        return;
+    }
     // whole warps iterate together (warp-aggregated fill counters); the
     // order inside a cell is restored by the fix-up
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {
         const int64_t g = g0 + threadIdx.x;
         const int32_t k = g < n ? key[g] : -1;
@@ -475,9 +526,9 @@ __global__ void k_sort_scatter(const int32_t* __restrict__ key, int64_t N, const
 }
 
 void launch_sort_scatter(const int32_t* key, int64_t N, const int64_t* count, const int32_t* start, int32_t* fill,
-                         int32_t* perm, cudaStream_t s) {
+                         int32_t* perm, cudaStream_t s, const int* unsorted) {
     if (N <= 0) return;
-    k_sort_scatter<<<nblk(N), TPB, 0, s>>>(key, N, count, start, fill, perm);
+    k_sort_scatter<<<nblk(N), TPB, 0, s>>>(key, N, count, start, fill, perm, unsorted);
     COUNTED(1);
 }
 
@@ -544,7 +595,13 @@ __device__ __forceinline__ void sort_segment(int32_t* __restrict__ perm, int32_t
 // sorted by source index in registers (segments of up to 32 members; a
 // larger one by an insertion sort in place).
 __global__ void k_sort_fixup_clear(const int32_t* __restrict__ start, int64_t ncells_cap, const int64_t* total_cells,
-                                   int32_t* __restrict__ perm, int32_t* __restrict__ fill) {
+                                   int32_t* __restrict__ perm, int32_t* __restrict__ fill, const int* unsorted,
+                                   unsigned long long* in_order_count) {
+    if (unsorted && *unsorted == 0) {
+        // the scatter placed nothing through the fill counters
+        if (in_order_count && blockIdx.x == 0 && threadIdx.x == 0) *in_order_count += 1ull;
+        return;
+    }
     int64_t nc = *total_cells;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc && c < ncells_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -573,9 +630,10 @@ __global__ void k_sort_fixup_clear(const int32_t* __restrict__ start, int64_t nc
 }
 
 void launch_sort_fixup_clear(const int32_t* start, int64_t ncells_cap, const int64_t* total_cells, int32_t* perm,
-                             int32_t* fill, cudaStream_t s) {
+                             int32_t* fill, cudaStream_t s, const int* unsorted, unsigned long long* in_order_count) {
     if (ncells_cap <= 0) return;
-    k_sort_fixup_clear<<<nblk(ncells_cap), TPB, 0, s>>>(start, ncells_cap, total_cells, perm, fill);
+    k_sort_fixup_clear<<<nblk(ncells_cap), TPB, 0, s>>>(start, ncells_cap, total_cells, perm, fill, unsorted,
+                                                        in_order_count);
     COUNTED(1);
 }
 
@@ -613,6 +671,9 @@ __global__ void k_gather_i32(const int32_t* __restrict__ src, int32_t* __restric
 __global__ void k_gather_fields(GatherArgs a, int64_t N, const int32_t* __restrict__ perm, const int64_t* count) {
     const int64_t n = count ? *count : N;
     const int f = blockIdx.y;
+    // the sort's order flag, read by the scatter and fix-up launched
+    // before this gather, is cleared for the next sort
+    if (a.clear && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *a.clear = 0;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         int64_t o = perm[g];
         if ((uint64_t)o >= (uint64_t)N) o = g;

@@ -14,7 +14,7 @@ from .model import (AbstractParticleSystem, ArgumentError, BasicParticleSystem, 
                     StressParticleSystem, SystemInteraction, TaitEOSUpdater, ViscoPlasticMCStressUpdater,
                     WenlandC2Kernel, XSPHPfn, ZeroFieldUpdater, is_coupled, VirtualParticleSystem,
                     InterpolateFieldFn, VirtualNormUpdater, PrescribedVelocityUpdater, ProbeParticleSystem,
-                    NeighborCountFn)
+                    NeighborCountFn, float_type)
 from .engine import (CudaBackend, GcError, Server, Session, compile_instance, download_instance, load_library,
                      time_integrate, upload_instance)
 

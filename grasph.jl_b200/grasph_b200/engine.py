@@ -52,7 +52,7 @@ class GcStats(ct.Structure):
                 ("sweep_launches", ct.c_int64), ("sweep_ms", ct.c_double),
                 ("last_status", ct.c_int32), ("pad", ct.c_int32),
                 ("graph_steps", ct.c_int64), ("rollbacks", ct.c_int64),
-                ("sweep_cfg_chosen", ct.c_int32 * 4)]
+                ("sweep_cfg_chosen", ct.c_int32 * 4), ("sorts_in_order", ct.c_int64)]
 
 
 _LIB = None
@@ -290,6 +290,10 @@ class CudaBackend:
     def set_precision(self, mode):
         self._chk(self.lib.gc_set_precision(self.ctx, mode), "gc_set_precision")
 
+    def set_profiling(self, on):
+        """Time every sweep launch with CUDA events (gc_stats.sweep_ms)."""
+        self._chk(self.lib.gc_set_profiling(self.ctx, 1 if on else 0), "gc_set_profiling")
+
     def set_graphs(self, on, sync_every=32, cap_margin=0.0):
         self._chk(self.lib.gc_set_graphs(self.ctx, 1 if on else 0, sync_every, cap_margin), "gc_set_graphs")
 
@@ -472,8 +476,13 @@ def compile_instance(backend, inst, systems, interactions, ghosts=(), gamma=0.0,
     return m
 
 
+def _wide(a):
+    """A Float32 field widened to the Float64 the library transfers."""
+    return a.astype(np.float64) if a.dtype == np.float32 else a
+
+
 def upload_instance(backend, m: InstanceMap, systems=None):
-    items = [(m.inst, m.h(ps), fid, getattr(ps, name))
+    items = [(m.inst, m.h(ps), fid, _wide(getattr(ps, name)))
              for ps in m.systems if systems is None or any(ps is q for q in systems)
              for name, fid in ps.particle_fields()]
     if hasattr(backend, "upload_many"):
@@ -484,14 +493,25 @@ def upload_instance(backend, m: InstanceMap, systems=None):
 
 
 def download_instance(backend, m: InstanceMap, with_ghosts=True, systems=None):
-    items = [(m.inst, m.h(ps), fid, getattr(ps, name))
-             for ps in m.systems if systems is None or any(ps is q for q in systems)
-             for name, fid in ps.particle_fields()]
+    items, narrow = [], []
+    for ps in m.systems:
+        if systems is not None and not any(ps is q for q in systems):
+            continue
+        for name, fid in ps.particle_fields():
+            a = getattr(ps, name)
+            if a.dtype == np.float32:
+                # downloaded in Float64, rounded to the system's Float32
+                w = np.empty(a.shape)
+                narrow.append((a, w))
+                a = w
+            items.append((m.inst, m.h(ps), fid, a))
     if hasattr(backend, "download_many"):
         backend.download_many(items)
     else:
         for inst, h, fid, a in items:
             backend.download_into(inst, h, fid, a)
+    for a, w in narrow:
+        a[...] = w
     if with_ghosts:
         for ge in m.ghosts:
             download_ghost(backend, m, ge)
@@ -528,6 +548,9 @@ def download_ghost(backend, m: InstanceMap, ge: GhostEntry):
     g.idx_original = backend.download_into(m.inst, h, C.GC_FIELD_IDX_ORIGINAL, np.zeros(n, dtype=np.int64))
     g.idx_boundary = backend.download_into(m.inst, h, C.GC_FIELD_IDX_BOUNDARY, np.zeros(n, dtype=np.int64))
     g.normals = backend.download_into(m.inst, h, C.GC_FIELD_NORMALS, np.zeros((n, nd)))
+    T = g.source.dtype
+    if T != np.float64:
+        g.x, g.v, g.rho, g.normals = (a.astype(T) for a in (g.x, g.v, g.rho, g.normals))
     for f in g.extras_fields:
         if f == "p":
             g.extras["p"] = backend.download_into(m.inst, h, C.GC_FIELD_P, np.zeros(n))
@@ -733,7 +756,8 @@ def time_integrate(integrator: LeapFrogTimeIntegrator, num_timesteps: int, print
 class ServeStats(ct.Structure):
     _fields_ = [("queued", ct.c_int64), ("running", ct.c_int64), ("batches", ct.c_int64),
                 ("rounds", ct.c_int64), ("repacks", ct.c_int64), ("particle_steps", ct.c_int64),
-                ("device_bytes_reserved", ct.c_int64)]
+                ("device_bytes_reserved", ct.c_int64), ("repack_seconds", ct.c_double),
+                ("repack_instances", ct.c_int64)]
 
 
 class Server:
@@ -782,7 +806,7 @@ class Server:
         for ps in m.systems:
             h = m.h(ps)
             for name, fid in ps.particle_fields():
-                be.stage(inst, h, fid, getattr(ps, name))
+                be.stage(inst, h, fid, _wide(getattr(ps, name)))
         req = ct.c_int64()
         st = self.lib.gc_serve_submit(self.srv, be.ctx, nsteps, cfl, ct.byref(req))
         if st != 0:
@@ -812,8 +836,11 @@ class Server:
             h = m.h(ps)
             for name, fid in ps.particle_fields():
                 a = getattr(ps, name)
-                self._chk(self.lib.gc_serve_download(self.srv, req, h, fid, a.ctypes.data, a.nbytes),
+                w = np.empty(a.shape) if a.dtype == np.float32 else a
+                self._chk(self.lib.gc_serve_download(self.srv, req, h, fid, w.ctypes.data, w.nbytes),
                           "gc_serve_download")
+                if w is not a:
+                    a[...] = w
         return lf
 
     def release(self, req):

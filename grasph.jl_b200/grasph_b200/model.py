@@ -31,6 +31,62 @@ class ArgumentError(ValueError):
     """Mirror of Julia's ``ArgumentError`` for invalid constructor input."""
 
 
+# ------------------------------------------------------------ element types
+#
+# A particle system's element type T is Float64 (default) or Float32
+# (src/Particles.jl:67,78).  Its arrays, mass and c are stored in T; kernels,
+# functors and updaters built from float32 values are specialised on
+# Float32.  The device library computes every system in the session's
+# precision from the values widened to Float64 and rounds the results back
+# to T on download.
+
+_JULIA_NAME = {np.dtype(np.float32): "Float32", np.dtype(np.float64): "Float64"}
+
+
+def _elt(dtype):
+    """`dtype` as a numpy float type (Float32 or Float64)."""
+    try:
+        d = np.dtype(dtype)
+    except TypeError:
+        d = None
+    if d not in _JULIA_NAME:
+        raise ArgumentError(f"dtype must be Float32 or Float64, got {dtype}")
+    return d.type
+
+
+def _promote(*vals):
+    """The float type Julia's `promote(float.(vals)...)` gives: Float32 when
+    every value is a float32, Float64 once any is not (integers and Python
+    floats promote to Float64)."""
+    vs = [v for v in vals if v is not None]
+    if vs and all(isinstance(v, np.float32) for v in vs):
+        return np.float32
+    return np.float64
+
+
+def _scalar(t, v):
+    """A T-typed scalar: a Python float for Float64, np.float32 for Float32."""
+    return float(v) if t is np.float64 else np.float32(v)
+
+
+def float_type(functor):
+    """The AbstractFloat type parameter a functor is specialised on, or None
+    for an unparameterised one (a function, ``nothing``, a tuple)."""
+    return getattr(functor, "_elt", None)
+
+
+def _check_functors_eltype(functors, T, label):
+    """src/Utils.jl:59-78: a functor specialised on a float type other than
+    the target's raises ArgumentError."""
+    for f in functors:
+        P = float_type(f)
+        if P is not None and P is not T:
+            raise ArgumentError(
+                f"{label} {type(f).__name__} is specialised on {_JULIA_NAME[np.dtype(P)]} "
+                f"but target expects {_JULIA_NAME[np.dtype(T)]}; construct it with "
+                f"{_JULIA_NAME[np.dtype(T)]} values")
+
+
 # ---------------------------------------------------------------- systems
 
 class AbstractParticleSystem:
@@ -50,30 +106,31 @@ class AbstractParticleSystem:
             raise ArgumentError(f"n must be positive, got {n}")
         if ndims <= 0:
             raise ArgumentError(f"ndims must be positive, got {ndims}")
+        T = _elt(dtype)
         if source_v is None:
             source_v = np.zeros(ndims)
-        source_v = np.asarray(source_v, dtype=np.float64)
+        source_v = np.asarray(source_v, dtype=T)
         if source_v.shape != (ndims,):
             raise ArgumentError(
                 f"length(source_v) = {source_v.size} must equal ndims = {ndims}")
-        if np.dtype(dtype) != np.float64:
-            raise ArgumentError("only Float64 particle systems are supported by the device library")
+        ups = state_updater if isinstance(state_updater, tuple) else (state_updater,)
+        _check_functors_eltype(ups, T, "state updater")
+        self.dtype = np.dtype(T)
         self.name = str(name)
         self.n = n
         self.ndims = ndims
         self.ns = int(ns)
-        self.mass = float(mass)
-        self.c = float(c)
+        self.mass = _scalar(T, mass)
+        self.c = _scalar(T, c)
         self.source_v = source_v
-        self.source_rho = float(source_rho)
+        self.source_rho = _scalar(T, source_rho)
         self.id = np.arange(1, n + 1, dtype=np.int64)
-        self.x = np.zeros((n, ndims))
-        self.v = np.zeros((n, ndims))
-        self.v_adjustment = np.zeros((n, ndims))
-        self.rho = np.zeros(n)
-        self.dvdt = np.zeros((n, ndims))
-        self.drhodt = np.zeros(n)
-        ups = state_updater if isinstance(state_updater, tuple) else (state_updater,)
+        self.x = np.zeros((n, ndims), T)
+        self.v = np.zeros((n, ndims), T)
+        self.v_adjustment = np.zeros((n, ndims), T)
+        self.rho = np.zeros(n, T)
+        self.dvdt = np.zeros((n, ndims), T)
+        self.drhodt = np.zeros(n, T)
         self.state_updater = ups
 
     # Fields in the order of src/Sorting.jl:15-26 (the arrays a sort permutes).
@@ -111,7 +168,7 @@ class FluidParticleSystem(AbstractParticleSystem):
 
     def __init__(self, name, n, ndims, mass, c, **kw):
         super().__init__(name, n, ndims, mass, c, **kw)
-        self.p = np.zeros(self.n)
+        self.p = np.zeros(self.n, self.dtype)
 
 
 class StressParticleSystem(AbstractParticleSystem):
@@ -126,9 +183,9 @@ class StressParticleSystem(AbstractParticleSystem):
         if ns not in (3, 4, 6):
             raise ArgumentError(f"ns must be 3, 4, or 6, got {ns}")
         super().__init__(name, n, ndims, mass, c, ns=ns, **kw)
-        self.p = np.zeros(self.n)
-        self.stress = np.zeros((self.n, ns))
-        self.strain_rate = np.zeros((self.n, ns))
+        self.p = np.zeros(self.n, self.dtype)
+        self.stress = np.zeros((self.n, ns), self.dtype)
+        self.strain_rate = np.zeros((self.n, ns), self.dtype)
 
 
 class ElastoPlasticParticleSystem(StressParticleSystem):
@@ -141,9 +198,10 @@ class ElastoPlasticParticleSystem(StressParticleSystem):
 
     def __init__(self, name, n, ndims, ns, mass, c, **kw):
         super().__init__(name, n, ndims, ns, mass, c, **kw)
-        self.vorticity = np.zeros(self.n) if self.ndims == 2 else np.zeros((self.n, 3))
-        self.strain = np.zeros((self.n, self.ns))
-        self.strain_p = np.zeros((self.n, self.ns))
+        T = self.dtype
+        self.vorticity = np.zeros(self.n, T) if self.ndims == 2 else np.zeros((self.n, 3), T)
+        self.strain = np.zeros((self.n, self.ns), T)
+        self.strain_p = np.zeros((self.n, self.ns), T)
 
 
 # --------------------------------------------------------------- wrappers
@@ -289,15 +347,30 @@ class GhostEntry:
 # ---------------------------------------------------------------- kernels
 
 class AbstractKernel:
+    """Kernel of element type T = typeof(h) (src/Kernels.jl:33): h,
+    norm_coeff and interaction_length are T values."""
+
     kind = C.GC_KERNEL_CUBIC_SPLINE
 
     def __init__(self, h: float, ndims: int = 3):
-        self.h = float(h)
+        self._elt = _promote(h)
+        self.h = _scalar(self._elt, h)
         self.ndims = int(ndims)
 
     @property
     def interaction_length(self):
-        return 2.0 * self.h
+        return _scalar(self._elt, 2.0 * self.h)
+
+    def _norm(self, v):
+        return _scalar(self._elt, v)
+
+    def _hpow(self, k):
+        """H^k in T, as Julia's literal power: H*H, H*H*H."""
+        H = self._elt(self.h)
+        r = H
+        for _ in range(k - 1):
+            r = r * H
+        return float(r)
 
 
 class CubicSplineKernel(AbstractKernel):
@@ -307,12 +380,12 @@ class CubicSplineKernel(AbstractKernel):
 
     @property
     def norm_coeff(self):
-        H = self.h
+        H = float(self.h)
         if self.ndims == 1:
-            return 2.0 / (3.0 * H)
+            return self._norm(2.0 / (3.0 * H))
         if self.ndims == 2:
-            return 10.0 / ((7.0 * math.pi) * (H * H))
-        return 1.0 / (math.pi * (H * H * H))
+            return self._norm(10.0 / ((7.0 * math.pi) * self._hpow(2)))
+        return self._norm(1.0 / (math.pi * self._hpow(3)))
 
 
 class WenlandC2Kernel(AbstractKernel):
@@ -322,10 +395,9 @@ class WenlandC2Kernel(AbstractKernel):
 
     @property
     def norm_coeff(self):
-        H = self.h
         if self.ndims == 2:
-            return 7.0 / ((64.0 * math.pi) * (H * H))
-        return 21.0 / ((256.0 * math.pi) * (H * H * H))
+            return self._norm(7.0 / ((64.0 * math.pi) * self._hpow(2)))
+        return self._norm(21.0 / ((256.0 * math.pi) * self._hpow(3)))
 
 
 # ----------------------------------------------------------- pair functors
@@ -346,15 +418,16 @@ class FluidPfn(_Pfn):
     kind = C.GC_PFN_FLUID
 
     def __init__(self, alpha, beta, h, *, sigma=2, delta=None, epsilon=None):
-        self.art_visc_alpha = float(alpha)
-        self.art_visc_beta = float(beta)
-        self.h = float(h)
+        T = self._elt = _promote(alpha, beta, h)
+        self.art_visc_alpha = _scalar(T, alpha)
+        self.art_visc_beta = _scalar(T, beta)
+        self.h = _scalar(T, h)
         self.sigma = int(sigma)
         if self.sigma not in (1, 2):
             raise ArgumentError("FluidPfn sigma must be 1 or 2 on the device path")
-        self.delta = None if delta is None else float(delta)
+        self.delta = None if delta is None else _scalar(T, delta)
         # artificial surface tension: used by the two-sided fluid x fluid form only
-        self.epsilon = None if epsilon is None else float(epsilon)
+        self.epsilon = None if epsilon is None else _scalar(T, epsilon)
 
     def params(self):
         p = super().params()
@@ -374,13 +447,14 @@ class FluidSolidPfn(_Pfn):
     kind = C.GC_PFN_FLUID_SOLID
 
     def __init__(self, alpha, beta, h, *, sigma=2, delta=None):
-        self.art_visc_alpha = float(alpha)
-        self.art_visc_beta = float(beta)
-        self.h = float(h)
+        T = self._elt = _promote(alpha, beta, h)
+        self.art_visc_alpha = _scalar(T, alpha)
+        self.art_visc_beta = _scalar(T, beta)
+        self.h = _scalar(T, h)
         self.sigma = int(sigma)
         if self.sigma not in (1, 2):
             raise ArgumentError("FluidSolidPfn sigma must be 1 or 2 on the device path")
-        self.delta = None if delta is None else float(delta)
+        self.delta = None if delta is None else _scalar(T, delta)
 
     def params(self):
         p = super().params()
@@ -396,10 +470,11 @@ class CauchyFluidPfn(_Pfn):
     kind = C.GC_PFN_CAUCHY_FLUID
 
     def __init__(self, alpha, beta, h, *, delta=None):
-        self.art_visc_alpha = float(alpha)
-        self.art_visc_beta = float(beta)
-        self.h = float(h)
-        self.delta = None if delta is None else float(delta)
+        T = self._elt = _promote(alpha, beta, h)
+        self.art_visc_alpha = _scalar(T, alpha)
+        self.art_visc_beta = _scalar(T, beta)
+        self.h = _scalar(T, h)
+        self.delta = None if delta is None else _scalar(T, delta)
 
     def params(self):
         p = super().params()
@@ -472,7 +547,8 @@ class XSPHPfn(_Pfn):
     kind = C.GC_PFN_XSPH
 
     def __init__(self, epsilon):
-        self.epsilon = float(epsilon)
+        T = self._elt = _promote(epsilon)
+        self.epsilon = _scalar(T, epsilon)
 
 
 def _pfn_kind(p):
@@ -525,9 +601,10 @@ class TaitEOSUpdater(_Updater):
 
     kind = C.GC_UPD_TAIT_EOS
 
-    def __init__(self, rho0, gamma=7.0):
-        self.rho0 = float(rho0)
-        self.gamma = float(gamma)
+    def __init__(self, rho0, gamma=None):
+        T = self._elt = _promote(rho0)
+        self.rho0 = _scalar(T, rho0)
+        self.gamma = _scalar(T, 7.0 if gamma is None else gamma)
 
     def params(self):
         p = super().params()
@@ -541,7 +618,8 @@ class LinearEOSUpdater(_Updater):
     kind = C.GC_UPD_LINEAR_EOS
 
     def __init__(self, rho0):
-        self.rho0 = float(rho0)
+        T = self._elt = _promote(rho0)
+        self.rho0 = _scalar(T, rho0)
 
     def params(self):
         p = super().params()
@@ -555,7 +633,8 @@ class ElastoPlasticStressUpdater(_Updater):
     kind = C.GC_UPD_ELASTOPLASTIC
 
     def __init__(self, E, nu, phi, psi, cohesion):
-        self.E, self.nu, self.phi, self.psi, self.cohesion = map(float, (E, nu, phi, psi, cohesion))
+        T = self._elt = _promote(E, nu, phi, psi, cohesion)
+        self.E, self.nu, self.phi, self.psi, self.cohesion = (_scalar(T, v) for v in (E, nu, phi, psi, cohesion))
 
     def params(self):
         p = super().params()
@@ -571,7 +650,9 @@ class VirtualNormUpdater(_Updater):
     _ok = {"v": C.GC_FIELD_V, "rho": C.GC_FIELD_RHO, "p": C.GC_FIELD_P, "stress": C.GC_FIELD_STRESS}
 
     def __init__(self, v_mult, *fields):
-        self.v_mult = np.asarray(v_mult, dtype=np.float64).ravel()
+        vm = np.asarray(v_mult)
+        self._elt = np.float32 if vm.dtype == np.float32 else np.float64
+        self.v_mult = vm.astype(self._elt).ravel()
         names = [str(f).lstrip(":") for f in fields]
         for n in names:
             if n not in self._ok:
@@ -597,7 +678,8 @@ class HookeLawStressUpdater(_Updater):
     kind = C.GC_UPD_HOOKE
 
     def __init__(self, E, nu):
-        self.E, self.nu = float(E), float(nu)
+        T = self._elt = _promote(E, nu)
+        self.E, self.nu = _scalar(T, E), _scalar(T, nu)
 
     def params(self):
         p = super().params()
@@ -616,8 +698,9 @@ class ViscoPlasticMCStressUpdater(_Updater):
         if not isinstance(eos, (TaitEOSUpdater, LinearEOSUpdater)):
             raise ArgumentError("ViscoPlasticMCStressUpdater: eos must be an EOS updater")
         self.eos = eos
-        self.friction_angle = float(friction_angle)
-        self.cohesion = float(cohesion)
+        T = self._elt = _promote(friction_angle, cohesion)
+        self.friction_angle = _scalar(T, friction_angle)
+        self.cohesion = _scalar(T, cohesion)
 
     def params(self):
         p = super().params()
@@ -663,6 +746,7 @@ class SystemInteraction:
             raise ArgumentError(f"velocity-adjust functor {type(vpf).__name__} has no device implementation")
         self.kernel = kernel
         self.pfns = pairwise_fn if isinstance(pairwise_fn, tuple) else (pairwise_fn,)
+        _check_functors_eltype(self.pfns, system_a.dtype.type, "pairwise functor")
         for f in self.pfns:
             if isinstance(f, XSPHPfn):
                 raise ArgumentError("XSPHPfn is a velocity-adjust functor, not a stage functor")
@@ -828,9 +912,10 @@ class LeapFrogTimeIntegrator:
         for si in self.probe_interactions:
             if not any(si.system_b is p for p in self.probes):
                 raise ArgumentError("a probe interaction's system_b must be one of `probes`")
-        self.c = max(ps.c for ps in sys_)
-        self.h = min(it.kernel.h for it in ints)
-        self.gamma = float(gamma)
+        T = sys_[0].dtype.type
+        self.c = _scalar(T, max(ps.c for ps in sys_))
+        self.h = _scalar(T, min(it.kernel.h for it in ints))
+        self.gamma = _scalar(T, gamma)
         self._device = None
 
 

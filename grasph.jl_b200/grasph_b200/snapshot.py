@@ -40,8 +40,8 @@ def _put_group(arrays, ps, prefix):
     """_write_to_group! (src/Particles.jl:720-734) under key prefix `prefix`."""
     arrays[f"{prefix}@n"] = np.int64(ps.n)
     arrays[f"{prefix}@ndims"] = np.int64(ps.ndims)
-    arrays[f"{prefix}@mass"] = np.float64(ps.mass)
-    arrays[f"{prefix}@c"] = np.float64(ps.c)
+    arrays[f"{prefix}@mass"] = ps.dtype.type(ps.mass)
+    arrays[f"{prefix}@c"] = ps.dtype.type(ps.c)
     for name, _ in ps.particle_fields():
         arrays[f"{prefix}{name}"] = np.asarray(getattr(ps, name))
 

@@ -289,11 +289,18 @@ ps_ndims(ps) = ps.ndims
 function field_io!(cl::CudaLeapFrog, ps, f::Symbol, upload::Bool)
     arr = getfield(ps, f)
     fid = GC_FIELD[f]
-    GC.@preserve arr begin
+    # the library moves Float64: a Float32 system's field goes through a
+    # widened copy, rounded back to Float32 after a download
+    wide = eltype(eltype(arr)) === Float32
+    buf = wide ? Float64.(reinterpret(Float32, arr)) : arr
+    GC.@preserve buf begin
         fn = upload ? :gc_upload_field : :gc_download_field
         st = ccall((fn, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{Cvoid}, Csize_t),
-                   cl.ctx, 0, cl.handles[ps], fid, pointer(arr), sizeof(arr))
+                   cl.ctx, 0, cl.handles[ps], fid, pointer(buf), sizeof(buf))
         check(cl.ctx, st)
+    end
+    if wide && !upload
+        reinterpret(Float32, arr) .= Float32.(buf)
     end
 end
 

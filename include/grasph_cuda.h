@@ -156,6 +156,9 @@ typedef struct gc_stats {
     int64_t rollbacks;           /* verified windows re-run exactly (a capacity
                                     was outgrown inside the window)              */
     int32_t sweep_cfg_chosen[4]; /* tuned (system, stage) sweeps per configuration */
+    int64_t sorts_in_order;      /* system sorts whose cell keys were already in
+                                    order, so the reorder was the identity
+                                    (src/Sorting.jl:176-186)                     */
 } gc_stats;
 
 /* Launch configurations of the pair sweep (block residency, staged
@@ -409,6 +412,8 @@ typedef struct gc_serve_stats {
     int64_t rounds, repacks;
     int64_t particle_steps;          /* moving particles × steps, all requests */
     int64_t device_bytes_reserved;   /* estimates of the admitted requests     */
+    double repack_seconds;           /* host time spent rebuilding batches     */
+    int64_t repack_instances;        /* requests placed by those rebuilds      */
 } gc_serve_stats;
 enum { GC_REQ_FAILED = -1, GC_REQ_QUEUED = 0, GC_REQ_RUNNING = 1, GC_REQ_DONE = 2 };
 

@@ -121,11 +121,13 @@ def _passing_block():
     return G.LeapFrogTimeIntegrator([fluid, wall], [si]), 0.2
 
 
-@pytest.mark.parametrize("graphs", [False, True])
-def test_still_wall_grid_follows_geometry_changes(graphs):
+@pytest.mark.parametrize("graphs,profiling", [(False, False), (True, False), (True, True)])
+def test_still_wall_grid_follows_geometry_changes(graphs, profiling):
     """The CSR over a wall that never moves is kept on the device while its
-    grid's geometry is unchanged and recounted when it changes: the device
-    stays with the oracle while the block slides past the wall's end."""
+    grid's geometry is unchanged and recounted when it changes (in captured
+    steps through a conditional graph node that the device switches): the
+    device stays with the oracle while the block slides past the wall's end.
+    With sweep timing on, the captured step also holds event nodes."""
     out, sessions = [], []
     for be in ("cuda", "oracle"):
         lf, cfl = _passing_block()
@@ -133,10 +135,16 @@ def test_still_wall_grid_follows_geometry_changes(graphs):
         sessions.append(s)
         if be == "cuda":
             s.backend.set_graphs(graphs, 8)
+            s.backend.set_profiling(profiling)
         s.push()
         s.step(40, cfl)
         s.pull()
         out.append(lf)
+    st = sessions[0].stats()
+    if graphs:
+        assert st["graph_steps"] > 0  # the steps were captured, not run eagerly after a failed capture
+    if profiling:
+        assert st["sweep_launches"] > 0
     fc = out[1].systems[0]
     assert fc.x[:, 0].max() > 0.3  # the block left the wall's end behind
     # per-particle scale of tests/parity.py, the state on its integrated scale

@@ -77,3 +77,49 @@ def test_budget_holds_requests_back():
     r = srv.submit(lf0, n0, meta0["cfl"])
     srv.pump()
     assert srv.poll(r)["state"] == G.Server.FAILED
+
+
+def _estimate(lf, meta, n):
+    """A request's device-memory estimate, as the server reserves it."""
+    srv = G.Server(round_steps=1, hbm_budget=10**12)
+    r = srv.submit(lf, n, meta["cfl"])
+    srv.pump()
+    est = srv.stats()["device_bytes_reserved"]
+    srv.close()
+    return est
+
+
+def test_request_waits_for_budget_then_runs():
+    """Two requests that fit the budget one at a time but not together: the
+    second stays queued while the first runs, is admitted after the first
+    finishes, and its result still equals the run alone."""
+    reqs = _requests()
+    (la, ma, na), (lb, mb, nb) = reqs[4], reqs[5]
+    ea, eb = _estimate(*_requests()[4]), _estimate(*_requests()[5])
+    assert ea > 0 and eb > 0
+    srv = G.Server(round_steps=8, hbm_budget=max(ea, eb) + min(ea, eb) // 2)
+    ra = srv.submit(la, na, ma["cfl"])
+    rb = srv.submit(lb, nb, mb["cfl"])
+    srv.pump()
+    assert srv.poll(ra)["state"] in (G.Server.RUNNING, G.Server.DONE)
+    assert srv.poll(rb)["state"] == G.Server.QUEUED
+    waited = 0
+    while srv.poll(ra)["state"] != G.Server.DONE:
+        assert srv.poll(rb)["state"] == G.Server.QUEUED
+        srv.pump()
+        waited += 1
+        assert waited < 100
+    rounds = 0
+    while srv.poll(rb)["state"] != G.Server.DONE:
+        srv.pump()
+        rounds += 1
+        assert rounds < 100
+    a, b = srv.poll(ra), srv.poll(rb)
+    assert b["t_admit"] >= a["t_done"] and waited >= 1
+    got = srv.fetch(rb)
+    ref = _alone(5, G.PRECISION_FP32_COMPENSATED)
+    for sg, sr in zip(got.systems, ref.systems):
+        for name, _ in sg.particle_fields():
+            assert np.array_equal(getattr(sg, name), getattr(sr, name), equal_nan=True), f"{sg.name}.{name}"
+    st = srv.stats()
+    assert st["repacks"] >= 2 and st["repack_seconds"] > 0.0 and st["repack_instances"] >= 2
