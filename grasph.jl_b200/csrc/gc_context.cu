@@ -2039,7 +2039,7 @@ void upload_inst_params(gc_ctx* ctx, double cfl) {
         for (auto& S : ctx->slots) {
             S.h_inst[k].dt = dt;
             S.h_inst[k].half_dt = dt / 2.0;
-            S.h_inst[k].gamma_dt = I.gamma != 0.0 ? I.gamma / dt : 0.0;
+            S.h_inst[k].gamma_dt = I.gamma != 0.0 && dt > 0.0 ? I.gamma / dt : 0.0;  // dt = 0: a frozen instance
             S.h_inst[k].sort_cutoff = 2.0 * h;
         }
     }

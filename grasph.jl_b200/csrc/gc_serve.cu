@@ -7,9 +7,14 @@
 // leave; state of the simulations that stay is copied on the device.
 //
 // Rounds: every batch advances min(round_steps, the fewest steps any of its
-// requests still needs) steps, so a request stops exactly at its step
-// count.  Its result is then copied to host memory and the request leaves
-// the batch at the next repack.  A batch's repack runs on its own host
+// running requests still needs) steps, so a request stops exactly at its
+// step count.  Its result is then copied to host memory and its instance is
+// frozen in place (time step 0) until the batch's next repack, which drops
+// it.  A batch repacks when a request failed, when no request is left
+// running, when frozen particles exceed a quarter of the batch, or when the
+// joining requests bring at least a quarter of the running particles or one
+// of them has waited JOIN_WAIT_ROUNDS rounds: joins and leaves then share
+// repacks.  A batch's repack runs on its own host
 // thread just before its steps, so it overlaps the other batches' steps;
 // the server's contexts draw device memory from one stream-ordered pool
 // that keeps freed memory, so a repack maps no new memory and waits on no
@@ -67,16 +72,19 @@ struct Request {
     double t_submit = 0, t_admit = -1, t_done = -1;
     int64_t est = 0, particles = 0, moving = 0;
     int batch = -1;
+    int waited = 0;  // rounds spent admitted but not yet packed
     std::vector<Result> result;
     std::string err;
 };
+
+constexpr int JOIN_WAIT_ROUNDS = 2;
 
 struct Batch {
     gc_ctx* proto = nullptr;  // the structure (model copy, no state)
     gc_ctx* ctx = nullptr;    // packed running context
     std::vector<int64_t> live;     // request ids, instance order of ctx
     std::vector<int64_t> joining;  // admitted, packed at the next repack
-    bool dirty = false;            // a request left
+    bool dirty = false;            // a request failed: repack at the next round
     int64_t est = 0;               // estimated bytes of live + joining requests
     int last_status = GC_OK;
     std::string last_err;
@@ -178,7 +186,27 @@ struct Job {
 Job plan_round(gc_server* s, Batch& B) {
     Job J;
     J.B = &B;
-    J.repack = B.dirty || !B.joining.empty();
+    int64_t live_p = 0, dead_p = 0, join_p = 0;
+    int nlive = 0, waited = 0;
+    for (int64_t id : B.live) {
+        const Request& r = s->reqs[id];
+        if (r.state == RQ_RUNNING) {
+            live_p += r.moving;
+            ++nlive;
+        } else {
+            dead_p += r.moving;
+        }
+    }
+    for (int64_t id : B.joining) {
+        join_p += s->reqs[id].moving;
+        waited = std::max(waited, s->reqs[id].waited);
+    }
+    const bool join_now =
+        !B.joining.empty() && (nlive == 0 || 4 * join_p >= live_p || waited >= JOIN_WAIT_ROUNDS);
+    const bool drop_now = !B.live.empty() && (nlive == 0 || 4 * dead_p > live_p + dead_p);
+    J.repack = B.dirty || join_now || drop_now;
+    if (!J.repack)
+        for (int64_t id : B.joining) s->reqs[id].waited += 1;
     if (J.repack) {
         for (size_t k = 0; k < B.live.size(); ++k)
             if (s->reqs[B.live[k]].state == RQ_RUNNING) {
@@ -193,13 +221,16 @@ Job plan_round(gc_server* s, Batch& B) {
         J.ids = B.live;
     }
     int64_t left = s->round_steps;
+    bool any = false;
     for (int64_t id : J.ids) {
         const Request& r = s->reqs[id];
         J.cfl.push_back(r.cfl);
+        if (r.state != RQ_RUNNING) continue;  // frozen in place
         left = std::min<int64_t>(left, r.nsteps - r.done);
+        if (!any) J.cfl0 = r.cfl;
+        any = true;
     }
-    J.steps = J.ids.empty() ? 0 : (int)std::max<int64_t>(left, 0);
-    J.cfl0 = J.cfl.empty() ? 0.0 : J.cfl[0];
+    J.steps = any ? (int)std::max<int64_t>(left, 0) : 0;
     return J;
 }
 
@@ -231,6 +262,13 @@ void run_round(gc_server* s, Job& J) {
 void finish_repack(gc_server* s, Job& J) {
     if (!J.repack) return;
     Batch& B = *J.B;
+    // finished requests leave the batch now: their reservation ends
+    for (int64_t id : B.live) {
+        const Request& r = s->reqs[id];
+        if (r.state != RQ_DONE) continue;
+        s->used -= std::min(s->used, (size_t)r.est);
+        B.est -= std::min(B.est, r.est);
+    }
     B.joining.clear();
     B.dirty = false;
     if (J.pack_status != GC_OK) {
@@ -252,7 +290,7 @@ void finish_repack(gc_server* s, Job& J) {
 }
 
 // After a round of `steps` steps: count them, copy finished results to the
-// host, mark the batch for a repack when a request left.
+// host and freeze their instances; a failure marks the batch for a repack.
 void retire(gc_server* s, Batch& B, int steps, int* ncompleted) {
     for (size_t k = 0; k < B.live.size(); ++k) {
         Request& r = s->reqs[B.live[k]];
@@ -284,6 +322,10 @@ void retire(gc_server* s, Batch& B, int steps, int* ncompleted) {
                 r.state = RQ_DONE;
                 r.t_done = s->now();
                 ++*ncompleted;
+                // frozen until the next repack drops it (still stepped, but
+                // with dt = 0 its state does not change)
+                gc::ctx_set_cfl(B.ctx, (int)k, 0.0);
+                continue;
             }
         }
         s->used -= std::min(s->used, (size_t)r.est);

@@ -340,11 +340,13 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
 template <int ND, int NS, int PFN, int KK>
 struct PhysF64 {
     static constexpr int NQ = 0;  // no staged copies (k_sweep only)
+    static constexpr bool BLOCKED = false;  // plain FP64 sums: nothing to merge at strip ends
     struct Own {
         OwnState<ND> o;
         double sig[NS > 0 ? NS : 1];
     };
     using AccT = Acc<ND, NS>;
+    static __device__ __forceinline__ void flush(AccT&) {}
     static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
         const int64_t N = A.aN;
 #pragma unroll
@@ -444,13 +446,13 @@ __device__ __forceinline__ void kadd(float& s, float& c, float x) {
     s = t;
 }
 
-// kadd when `on`, else nothing (a select, not a branch)
-__device__ __forceinline__ void kadd_if(float& s, float& c, float x, bool on) {
-    const float y = x - c;
-    const float t = s + y;
-    const float cn = (t - s) - y;
-    s = on ? t : s;
-    c = on ? cn : c;
+// x added to a strip's partial sum when `on`.  An explicit round-to-nearest
+// add: the compiler may not fuse it with the product that made x, which it
+// would otherwise do differently in the two sweeps (and so change bits
+// between launch configurations).
+__device__ __forceinline__ void padd_if(float& p, float x, bool on) {
+    const float t = __fadd_rn(p, x);
+    p = on ? t : p;
 }
 
 
@@ -517,12 +519,33 @@ struct PhysF32 {
             for (int d = 0; d < ND; ++d) x[d] = r.bx[d * r.bN + j];
         }
     }
+    // Per-particle sums s with Kahan compensation c, fed strip by strip: a
+    // pair's term goes into the plain FP32 partial p of its strip, and at
+    // the end of each strip p is added to s with compensation.  Both sweeps
+    // evaluate a particle's pairs of a strip in the same order and merge at
+    // the same strip ends, so every launch configuration gives the same bits.
+    static constexpr bool BLOCKED = true;
     struct AccT {
-        float dv[ND], cdv[ND];
-        float dr, cdr;
-        float sr[NS > 0 ? NS : 1], csr[NS > 0 ? NS : 1];
-        float w[3], cw[3];
+        float dv[ND], cdv[ND], pdv[ND];
+        float dr, cdr, pdr;
+        float sr[NS > 0 ? NS : 1], csr[NS > 0 ? NS : 1], psr[NS > 0 ? NS : 1];
+        float w[3], cw[3], pw[3];
     };
+    // A zero partial is skipped (a compensated add of 0 would fold c into
+    // s), so a strip a sweep does not visit merges exactly like an empty one.
+    static __device__ __forceinline__ void merge(float& s, float& c, float& p) {
+        if (p != 0.f) kadd(s, c, p);
+        p = 0.f;
+    }
+    static __device__ __forceinline__ void flush(AccT& acc) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) merge(acc.dv[d], acc.cdv[d], acc.pdv[d]);
+        merge(acc.dr, acc.cdr, acc.pdr);
+#pragma unroll
+        for (int q = 0; q < (NS > 0 ? NS : 1); ++q) merge(acc.sr[q], acc.csr[q], acc.psr[q]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) merge(acc.w[q], acc.cw[q], acc.pw[q]);
+    }
     static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
         const int64_t N = A.aN;
         float f[R];
@@ -541,13 +564,14 @@ struct PhysF32 {
     static __device__ __forceinline__ const double* xpos(const Own& w) { return w.x; }
     static __device__ __forceinline__ void init(const ForceArgs&, int64_t, AccT& acc, bool) {
 #pragma unroll
-        for (int d = 0; d < ND; ++d) acc.dv[d] = acc.cdv[d] = 0.f;
-        acc.dr = acc.cdr = 0.f;
+        for (int d = 0; d < ND; ++d) acc.dv[d] = acc.cdv[d] = acc.pdv[d] = 0.f;
+        acc.dr = acc.cdr = acc.pdr = 0.f;
 #pragma unroll
-        for (int q = 0; q < (NS > 0 ? NS : 1); ++q) acc.sr[q] = acc.csr[q] = 0.f;
+        for (int q = 0; q < (NS > 0 ? NS : 1); ++q) acc.sr[q] = acc.csr[q] = acc.psr[q] = 0.f;
 #pragma unroll
-        for (int q = 0; q < 3; ++q) acc.w[q] = acc.cw[q] = 0.f;
+        for (int q = 0; q < 3; ++q) acc.w[q] = acc.cw[q] = acc.pw[q] = 0.f;
     }
+    // (the sweeps merge every strip's partials before storing)
     static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
         // FP64 state += compensated FP32 sum (s − c)
         const int64_t N = A.aN;
@@ -709,12 +733,12 @@ struct PhysF32 {
                 sr[5] = 0.5f * (dv[1] * gx[2] + dv[2] * gx[1]);
             }
 #pragma unroll
-            for (int q2 = 0; q2 < NS; ++q2) kadd_if(acc.sr[q2], acc.csr[q2], sr[q2] * f, in);
+            for (int q2 = 0; q2 < NS; ++q2) padd_if(acc.psr[q2], sr[q2] * f, in);
             if (P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
-                kadd_if(acc.w[0], acc.cw[0], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f, in);
+                padd_if(acc.pw[0], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f, in);
                 if (ND == 3) {
-                    kadd_if(acc.w[1], acc.cw[1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f, in);
-                    kadd_if(acc.w[2], acc.cw[2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f, in);
+                    padd_if(acc.pw[1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f, in);
+                    padd_if(acc.pw[2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f, in);
                 }
             }
             return in ? 1 : 0;
@@ -739,7 +763,7 @@ struct PhysF32 {
                 const float rfj = (0.01f * ca) * ca * lj;
                 const float s = -G.f_bmass * piv;
 #pragma unroll
-                for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d] + rfj * dxf[d], in);
+                for (int d = 0; d < ND; ++d) padd_if(acc.pdv[d], s * gx[d] + rfj * dxf[d], in);
                 return in ? 1 : 0;
             }
             const float mj = (self || dyn) ? ma : G.f_bmass;
@@ -756,7 +780,7 @@ struct PhysF32 {
                 if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
                 const float s = mj * (dh - piv);
 #pragma unroll
-                for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], s * gx[d], in);
+                for (int d = 0; d < ND; ++d) padd_if(acc.pdv[d], s * gx[d], in);
             } else {
                 // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
                 float sj[NS > 0 ? NS : 1];
@@ -777,7 +801,7 @@ struct PhysF32 {
                             (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
                 }
 #pragma unroll
-                for (int d = 0; d < ND; ++d) kadd_if(acc.dv[d], acc.cdv[d], mj * (hv[d] - piv * gx[d]), in);
+                for (int d = 0; d < ND; ++d) padd_if(acc.pdv[d], mj * (hv[d] - piv * gx[d]), in);
             }
             float tail = 0.f;
             if (P.has_delta) {
@@ -785,7 +809,7 @@ struct PhysF32 {
                 const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
                 tail = psi * irhoj;
             }
-            kadd_if(acc.dr, acc.cdr, mj * (dotf<ND>(dv, gx) + tail), in);
+            padd_if(acc.pdr, mj * (dotf<ND>(dv, gx) + tail), in);
             (void)gi;
             return in ? 1 : 0;
         }
@@ -1051,6 +1075,14 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         }
                         __syncwarp();
                     }
+                    if (Phys::BLOCKED) {
+                        // the strip's pairs, then its partial sums merged
+                        accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col,
+                                                                             BT, acc);
+                        nbuf = 0;
+                        __syncwarp();
+                        Phys::flush(acc);
+                    }
                 }
                 accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col, BT, acc);
                 nbuf = 0;
@@ -1071,6 +1103,12 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                                                                                  BT, acc);
                             nbuf = 0;
                         }
+                    }
+                    if (Phys::BLOCKED) {
+                        accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col,
+                                                                             BT, acc);
+                        nbuf = 0;
+                        Phys::flush(acc);
                     }
                 }
                 accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col, BT, acc);
@@ -1240,6 +1278,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                             }
                             __syncwarp();  // every lane is done with the chunk before the next one lands
                         }
+                        Phys::flush(acc);  // the strip's partial sums
                     }
                 };
                 if (self) strips(std::integral_constant<int, BT_SELF>{});
@@ -1255,6 +1294,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                         if (self && j == gi) continue;
                         accepted += Phys::template pair<PFN>(A, r, G, P, gi, k, w, da, j, acc);
                     }
+                    Phys::flush(acc);
                 }
             }
             __syncwarp();
