@@ -481,14 +481,25 @@ __global__ void k_sort_keys(const double* __restrict__ x, int64_t N, int nd, con
         }
         warp_agg_inc(hist, kk, valid);
         if (unsorted) {
-            // keys already non-decreasing (src/Sorting.jl:176-186): lane 0
-            // recomputes the key before its warp, the others take it from
-            // the lane below; an invalid key counts as out of order
+            // keys already non-decreasing (src/Sorting.jl:176-186): each
+            // thread compares with the key before it, from the lane below,
+            // the previous warp's last lane (shared memory) or, for the
+            // block's first thread, recomputed; an invalid key counts as out
+            // of order
+            __shared__ int32_t wlast[TPB / 32];
+            const int wid = threadIdx.x >> 5;
             int32_t prev = __shfl_up_sync(0xffffffffu, kk, 1);
-            if (lane == 0 && g > 0 && g < n) {
-                int pb = 0;
-                prev = sort_key_of(x, N, nd, inst_of, inst, g - 1, cells_cap, &pb);
+            if (lane == 31) wlast[wid] = kk;
+            __syncthreads();
+            if (lane == 0) {
+                if (wid > 0) {
+                    prev = wlast[wid - 1];
+                } else if (g > 0 && g < n) {
+                    int pb = 0;
+                    prev = sort_key_of(x, N, nd, inst_of, inst, g - 1, cells_cap, &pb);
+                }
             }
+            __syncthreads();  // wlast is rewritten by the next tile
             const bool order_broken = g < n && (bad || (g > 0 && prev > kk));
             if (__any_sync(0xffffffffu, order_broken) && lane == 0) atomicOr(unsorted, 1);
         }
@@ -500,7 +511,7 @@ void launch_sort_keys(const double* x, int64_t N, int nd, const int32_t* inst_of
                       int* unsorted) {
     if (N <= 0) return;
     k_sort_keys<<<nblk(N), TPB, 0, s>>>(x, N, nd, inst_of, count, inst, key, hist, cells_cap, err,
-                                        unsorted);  // TPB % 32 == 0
+                                        unsorted);  // blockDim == TPB, a multiple of 32
     COUNTED(1);
 }
 
