@@ -3993,11 +3993,43 @@ int ctx_model_copy(gc_ctx* m, int inst, gc_ctx** out) {
     return GC_OK;
 }
 
-int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pair<gc_ctx*, int>>& src,
-             gc_ctx** out, std::string* err, cudaMemPool_t pool) {
+// A repack in two parts.  ctx_pack_plan (on the caller's thread) copies what
+// the new context needs from the sources: every instance's model, the
+// sources of their state, and the sweep configurations a running context
+// of this structure tuned.  ctx_pack_build then makes and finalizes the new
+// context and uploads the staged fields of instances that come from model
+// contexts; it reads only the plan and those models, so it may run while
+// the running sources step.  ctx_pack_fill copies the running instances'
+// device state once their sources have stopped.
+struct PackJob {
+    int precision = GC_PRECISION_FP64;
+    std::vector<HInst> models;
+    std::vector<std::pair<gc_ctx*, int>> src;  // per new instance: its source and instance there
+    std::map<int64_t, gc_ctx::Tune> tune;
+};
+
+PackJob* ctx_pack_plan(int precision, const std::vector<std::pair<gc_ctx*, int>>& src) {
+    PackJob* J = new PackJob;
+    J->precision = precision;
+    J->src = src;
+    for (auto& p : src) J->models.push_back(model_of(p.first->inst[p.second]));
+    // the sweep configurations a running context of this structure tuned
+    // carry over (the structure, and so the tuner's keys, are the same)
+    for (auto& p : src)
+        if (p.first->finalized && p.first->precision == precision && p.first->force_cfg < 0) {
+            for (auto& kv : p.first->tune)
+                if (kv.second.best >= 0) J->tune[kv.first] = kv.second;
+            break;
+        }
+    return J;
+}
+
+void ctx_pack_free(PackJob* J) { delete J; }
+
+int ctx_pack_build(PackJob* J, int device, cudaMemPool_t pool, gc_ctx** out, std::string* err) {
     *out = nullptr;
     gc_ctx* ctx = nullptr;
-    TRY(gc_ctx_create(device, budget, &ctx));
+    TRY(gc_ctx_create(device, 0, &ctx));
     ctx->pool = pool;
     if (pool) TRY(ctx_set_priority(ctx, true));
     auto fail = [&](int st) {
@@ -4005,20 +4037,32 @@ int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pa
         gc_ctx_destroy(ctx);
         return st;
     };
-    for (auto& p : src) ctx->inst.push_back(model_of(p.first->inst[p.second]));
+    ctx->inst = J->models;
     int st = gc_finalize(ctx);
     if (st) return fail(st);
-    st = gc_set_precision(ctx, precision);
+    st = gc_set_precision(ctx, J->precision);
     if (st) return fail(st);
-    // the sweep configurations a running context of this structure tuned
-    // carry over (the structure, and so the tuner's keys, are the same)
-    for (auto& p : src)
-        if (p.first->finalized && p.first->precision == precision && p.first->force_cfg < 0) {
-            for (auto& kv : p.first->tune)
-                if (kv.second.best >= 0) ctx->tune[kv.first] = kv.second;
-            break;
+    for (auto& kv : J->tune) ctx->tune[kv.first] = kv.second;
+    // instances that come from model contexts: their staged fields
+    for (size_t k = 0; k < J->src.size(); ++k) {
+        gc_ctx* sc = J->src[k].first;
+        if (sc->finalized) continue;
+        for (auto& f : sc->inst[J->src[k].second].staged) {
+            st = gc_upload_field(ctx, (int)k, f.handle, f.field, f.bytes.data(), f.bytes.size());
+            if (st) return fail(st);
         }
-    // device state of instances that come from running contexts
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    *out = ctx;
+    return GC_OK;
+}
+
+int ctx_pack_fill(PackJob* J, gc_ctx* ctx, std::string* err) {
+    auto fail = [&](int st) {
+        if (err) *err = ctx->err;
+        return st;
+    };
+    const auto& src = J->src;
     for (auto& p : src)
         if (p.first->finalized) cudaStreamSynchronize(p.first->stream);
     // every (slot, field) segment table in one upload, then the copies
@@ -4077,19 +4121,9 @@ int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pa
         cudaStreamSynchronize(ctx->stream);
         dfree(ctx, d_seg, tab.size());
     }
-    st = check_launch(ctx, "pack");
+    int st = check_launch(ctx, "pack");
     if (st) return fail(st);
-    // instances that come from model contexts: their staged fields
-    for (size_t k = 0; k < src.size(); ++k) {
-        gc_ctx* sc = src[k].first;
-        if (sc->finalized) continue;
-        for (auto& f : sc->inst[src[k].second].staged) {
-            st = gc_upload_field(ctx, (int)k, f.handle, f.field, f.bytes.data(), f.bytes.size());
-            if (st) return fail(st);
-        }
-    }
     CU(cudaStreamSynchronize(ctx->stream));
-    *out = ctx;
     return GC_OK;
 }
 

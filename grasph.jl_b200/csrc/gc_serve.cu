@@ -47,8 +47,11 @@ int64_t ctx_particles(gc_ctx* c, int inst);
 int64_t ctx_moving_particles(gc_ctx* c, int inst);
 int64_t ctx_estimate_bytes(gc_ctx* m, int inst);
 int ctx_model_copy(gc_ctx* m, int inst, gc_ctx** out);
-int ctx_pack(int device, size_t budget, int precision, const std::vector<std::pair<gc_ctx*, int>>& src,
-             gc_ctx** out, std::string* err, cudaMemPool_t pool);
+struct PackJob;
+PackJob* ctx_pack_plan(int precision, const std::vector<std::pair<gc_ctx*, int>>& src);
+int ctx_pack_build(PackJob* J, int device, cudaMemPool_t pool, gc_ctx** out, std::string* err);
+int ctx_pack_fill(PackJob* J, gc_ctx* ctx, std::string* err);
+void ctx_pack_free(PackJob* J);
 void ctx_result_fields(gc_ctx* c, int inst, std::vector<std::array<int64_t, 3>>& out);
 const char* ctx_error(gc_ctx* c);
 }  // namespace gc
@@ -85,6 +88,7 @@ struct Batch {
     std::vector<int64_t> live;     // request ids, instance order of ctx
     std::vector<int64_t> joining;  // admitted, packed at the next repack
     bool dirty = false;            // a request failed: repack at the next round
+    bool fresh = false;            // ctx is new: its first round runs on a highest-priority stream
     int64_t est = 0;               // estimated bytes of live + joining requests
     int last_status = GC_OK;
     std::string last_err;
@@ -166,33 +170,40 @@ void admit(gc_server* s) {
 
 // One batch's work in a round: the repack (when requests joined or left)
 // and the steps.  The plan is made on the server's thread; `run` touches
-// only the batch's contexts, so batches run it concurrently.
+// only the batch's contexts, so batches run it concurrently.  A batch that
+// is stepping repacks in a pipeline: its current context steps the round
+// while the new one is built and the joiners' fields uploaded on another
+// thread; after the round the staying requests' state is copied over and
+// the new context takes over (the joiners step from the next round on).
 struct Job {
     Batch* B = nullptr;
     bool repack = false;
-    std::vector<std::pair<gc_ctx*, int>> src;  // running instances, then joining models
-    std::vector<int64_t> ids;                  // the batch's requests after the repack
+    bool pipelined = false;          // the current context steps while the new one is built
+    gc::PackJob* plan = nullptr;
+    std::vector<int64_t> ids;        // the batch's requests in the new context
+    std::vector<int64_t> joiners;    // of those, the ones not yet in a context
     std::vector<double> cfl;
-    int steps = 0;
+    int steps = 0;                   // this round's steps
     double cfl0 = 0;
+    gc_ctx* nc = nullptr;            // the new context
     int pack_status = GC_OK;
     std::string pack_err;
     double repack_s = 0;
 };
 
-// The batch after a repack: the requests of `live` that still run (state
-// copied on the device from the old context) followed by the joining ones
-// (staged host fields).
 Job plan_round(gc_server* s, Batch& B) {
     Job J;
     J.B = &B;
     int64_t live_p = 0, dead_p = 0, join_p = 0;
     int nlive = 0, waited = 0;
+    int64_t left = s->round_steps;  // steps of this round over the current context's running requests
     for (int64_t id : B.live) {
         const Request& r = s->reqs[id];
         if (r.state == RQ_RUNNING) {
             live_p += r.moving;
+            if (nlive == 0) J.cfl0 = r.cfl;
             ++nlive;
+            left = std::min<int64_t>(left, r.nsteps - r.done);
         } else {
             dead_p += r.moving;
         }
@@ -207,59 +218,100 @@ Job plan_round(gc_server* s, Batch& B) {
     J.repack = B.dirty || join_now || drop_now;
     if (!J.repack)
         for (int64_t id : B.joining) s->reqs[id].waited += 1;
-    if (J.repack) {
-        for (size_t k = 0; k < B.live.size(); ++k)
-            if (s->reqs[B.live[k]].state == RQ_RUNNING) {
-                J.src.push_back({B.ctx, (int)k});
-                J.ids.push_back(B.live[k]);
-            }
-        for (int64_t id : B.joining) {
-            J.src.push_back({s->reqs[id].model, 0});
-            J.ids.push_back(id);
-        }
-    } else {
+    J.pipelined = J.repack && B.ctx && nlive > 0 && !B.dirty;
+    std::vector<std::pair<gc_ctx*, int>> src;
+    if (!J.repack) {
         J.ids = B.live;
+        J.steps = nlive > 0 ? (int)std::max<int64_t>(left, 0) : 0;
+    } else {
+        // the new context: the requests that still run after this round
+        // (pipelined) or now, then the joiners
+        if (J.pipelined) J.steps = (int)std::max<int64_t>(left, 0);
+        for (size_t k = 0; k < B.live.size(); ++k) {
+            const Request& r = s->reqs[B.live[k]];
+            if (r.state != RQ_RUNNING) continue;
+            if (J.pipelined && r.nsteps - r.done <= J.steps) continue;  // finishes in this round
+            src.push_back({B.ctx, (int)k});
+            J.ids.push_back(B.live[k]);
+        }
+        for (int64_t id : B.joining) {
+            src.push_back({s->reqs[id].model, 0});
+            J.ids.push_back(id);
+            J.joiners.push_back(id);
+        }
+        if (!J.pipelined) {
+            // a batch that is not stepping: the new context steps this round
+            left = s->round_steps;
+            bool any = false;
+            for (int64_t id : J.ids) {
+                const Request& r = s->reqs[id];
+                if (r.state != RQ_RUNNING) continue;
+                left = std::min<int64_t>(left, r.nsteps - r.done);
+                if (!any) J.cfl0 = r.cfl;
+                any = true;
+            }
+            J.steps = any ? (int)std::max<int64_t>(left, 0) : 0;
+        }
     }
-    int64_t left = s->round_steps;
-    bool any = false;
-    for (int64_t id : J.ids) {
-        const Request& r = s->reqs[id];
-        J.cfl.push_back(r.cfl);
-        if (r.state != RQ_RUNNING) continue;  // frozen in place
-        left = std::min<int64_t>(left, r.nsteps - r.done);
-        if (!any) J.cfl0 = r.cfl;
-        any = true;
-    }
-    J.steps = any ? (int)std::max<int64_t>(left, 0) : 0;
+    for (int64_t id : J.ids) J.cfl.push_back(s->reqs[id].cfl);
+    if (J.repack && !src.empty()) J.plan = gc::ctx_pack_plan(s->precision, src);
     return J;
 }
 
-// Repack (a new context replaces the old one) and step.
-void run_round(gc_server* s, Job& J) {
-    Batch& B = *J.B;
-    if (J.repack) {
-        const double t_start = s->now();
-        gc_ctx* nc = nullptr;
-        if (!J.src.empty()) {
-            J.pack_status = gc::ctx_pack(s->device, 0, s->precision, J.src, &nc, &J.pack_err, s->pool);
-            if (J.pack_status == GC_OK)
-                for (size_t k = 0; k < J.ids.size(); ++k) gc::ctx_set_cfl(nc, (int)k, J.cfl[k]);
-        }
-        if (B.ctx) gc_ctx_destroy(B.ctx);
-        B.ctx = J.pack_status == GC_OK ? nc : nullptr;
-        J.repack_s = s->now() - t_start;
+// Build the planned context (and, once its running sources have stopped,
+// fill it with their state).
+void build_new(gc_server* s, Job& J) {
+    const double t0 = s->now();
+    if (J.plan) {
+        J.pack_status = gc::ctx_pack_build(J.plan, s->device, s->pool, &J.nc, &J.pack_err);
+        if (J.pack_status == GC_OK)
+            for (size_t k = 0; k < J.ids.size(); ++k) gc::ctx_set_cfl(J.nc, (int)k, J.cfl[k]);
     }
-    if (B.ctx && J.steps > 0) {
-        B.last_status = gc_step(B.ctx, J.steps, J.cfl0);
-        if (B.last_status != GC_OK) B.last_err = gc_last_error(B.ctx);
-    }
-    // a new context is built and takes its first (exact, capturing) steps
-    // on a highest-priority stream, then steps at the normal priority
-    if (J.repack && B.ctx) gc::ctx_set_priority(B.ctx, false);
+    J.repack_s += s->now() - t0;
 }
 
-// The repack's bookkeeping, on the server's thread.
-void finish_repack(gc_server* s, Job& J) {
+void fill_new(gc_server* s, Job& J) {
+    if (!J.nc || J.pack_status != GC_OK) return;
+    const double t0 = s->now();
+    J.pack_status = gc::ctx_pack_fill(J.plan, J.nc, &J.pack_err);
+    J.repack_s += s->now() - t0;
+}
+
+void step_batch(Batch& B, const Job& J) {
+    if (!B.ctx || J.steps <= 0) return;
+    B.last_status = gc_step(B.ctx, J.steps, J.cfl0);
+    if (B.last_status != GC_OK) B.last_err = gc_last_error(B.ctx);
+    // a new context is built and takes its first (exact, capturing) steps
+    // on a highest-priority stream, then steps at the normal priority
+    if (B.fresh) {
+        gc::ctx_set_priority(B.ctx, false);
+        B.fresh = false;
+    }
+}
+
+void run_round(gc_server* s, Job& J) {
+    Batch& B = *J.B;
+    if (J.pipelined) {
+        std::thread builder([s, &J] { build_new(s, J); });
+        step_batch(B, J);
+        builder.join();
+        if (B.last_status == GC_OK) fill_new(s, J);
+        return;  // the server thread switches contexts after reading the round's results
+    }
+    if (J.repack) {
+        build_new(s, J);
+        fill_new(s, J);
+        if (B.ctx) gc_ctx_destroy(B.ctx);
+        B.ctx = J.pack_status == GC_OK ? J.nc : nullptr;
+        B.fresh = B.ctx != nullptr;
+        J.nc = nullptr;
+    }
+    step_batch(B, J);
+}
+
+// The repack's bookkeeping, on the server's thread (after the round's
+// results were read when the repack was pipelined).
+void finish_repack(gc_server* s, Job& J, bool round_ok) {
     if (!J.repack) return;
     Batch& B = *J.B;
     // finished requests leave the batch now: their reservation ends
@@ -271,6 +323,26 @@ void finish_repack(gc_server* s, Job& J) {
     }
     B.joining.clear();
     B.dirty = false;
+    if (J.pipelined) {
+        if (B.ctx) gc_ctx_destroy(B.ctx);
+        B.ctx = nullptr;
+        if (!round_ok) {
+            // the round failed (its requests with it): the joiners wait for
+            // the next round's context
+            if (J.nc) gc_ctx_destroy(J.nc);
+            J.nc = nullptr;
+            B.live.clear();
+            B.joining = J.joiners;
+            return;
+        }
+        if (J.pack_status == GC_OK) {
+            B.ctx = J.nc;
+            B.fresh = B.ctx != nullptr;
+        } else if (J.nc) {
+            gc_ctx_destroy(J.nc);
+        }
+        J.nc = nullptr;
+    }
     if (J.pack_status != GC_OK) {
         for (int64_t id : J.ids) {
             Request& r = s->reqs[id];
@@ -413,10 +485,18 @@ int gc_serve_pump(gc_server* s, int* ncompleted) {
         for (auto& J : jobs) th.emplace_back([s, &J] { run_round(s, J); });
         for (auto& t : th) t.join();
     }
-    // requests that need no steps at all finish now
     for (auto& J : jobs) {
-        finish_repack(s, J);
-        if (J.B->ctx) retire(s, *J.B, J.steps, &done);
+        if (J.pipelined) {
+            // the round ran on the current context: its results first
+            const bool ok = J.B->last_status == GC_OK;
+            retire(s, *J.B, J.steps, &done);
+            finish_repack(s, J, ok);
+        } else {
+            finish_repack(s, J, true);
+            // (requests that need no steps at all finish now)
+            if (J.B->ctx) retire(s, *J.B, J.steps, &done);
+        }
+        if (J.plan) gc::ctx_pack_free(J.plan);
     }
     s->stats.rounds += 1;
     if (ncompleted) *ncompleted = done;
