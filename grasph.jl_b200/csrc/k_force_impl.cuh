@@ -346,7 +346,15 @@ struct PhysF64 {
         double sig[NS > 0 ? NS : 1];
     };
     using AccT = Acc<ND, NS>;
-    static __device__ __forceinline__ void flush(AccT&) {}
+    static constexpr int NSUM = 1;  // (plain FP64 sums live in AccT)
+    template <class Sum>
+    static __device__ __forceinline__ void flush(AccT&, Sum&) {}
+    template <class Sum>
+    static __device__ __forceinline__ void init_sum(Sum&) {}
+    template <class Sum>
+    static __device__ __forceinline__ void store_sum(const ForceArgs& A, int64_t gi, const AccT& acc, Sum&) {
+        store(A, gi, acc);
+    }
     static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
         const int64_t N = A.aN;
 #pragma unroll
@@ -455,6 +463,23 @@ __device__ __forceinline__ void padd_if(float& p, float x, bool on) {
     p = on ? t : p;
 }
 
+// A particle's compensated sums (N components: sum s_j, compensation c_j),
+// in registers or in the warp's shared memory ([2N][32], one column per
+// lane, so a warp's accesses hit 32 different banks).
+template <int N>
+struct SumRegs {
+    float s[N], c[N];
+    __device__ __forceinline__ float& S(int j) { return s[j]; }
+    __device__ __forceinline__ float& C(int j) { return c[j]; }
+};
+template <int N>
+struct SumSmem {
+    float* b;
+    int lane;
+    __device__ __forceinline__ float& S(int j) { return b[j * 32 + lane]; }
+    __device__ __forceinline__ float& C(int j) { return b[(N + j) * 32 + lane]; }
+};
+
 
 template <int ND>
 __device__ __forceinline__ double dot_exact(const double* a, const double* b) {
@@ -520,31 +545,38 @@ struct PhysF32 {
         }
     }
     // Per-particle sums s with Kahan compensation c, fed strip by strip: a
-    // pair's term goes into the plain FP32 partial p of its strip, and at
-    // the end of each strip p is added to s with compensation.  Both sweeps
-    // evaluate a particle's pairs of a strip in the same order and merge at
-    // the same strip ends, so every launch configuration gives the same bits.
+    // pair's term goes into the plain FP32 partial p of its strip (AccT, in
+    // registers), and at the end of each strip p is added to s with
+    // compensation (the sums: registers in k_sweep, shared memory in
+    // k_sweep_stg).  Both sweeps evaluate a particle's pairs of a strip in
+    // the same order and merge at the same strip ends, so every launch
+    // configuration gives the same bits.  Components: dv/dt then dρ/dt
+    // (fluid, Cauchy and counting functors), or the strain rate then the
+    // vorticity.
     static constexpr bool BLOCKED = true;
+    static constexpr bool FLUIDLIKE = fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT;
+    static constexpr int NSX = NS > 0 ? NS : 1;
+    static constexpr int NVORT = ND == 2 ? 1 : 3;
+    static constexpr int NSUM = FLUIDLIKE ? ND + 1 : NSX + (PFN == GC_PFN_STRAIN_RATE_VORTICITY ? NVORT : 0);
+    static constexpr int IDR = ND;   // dρ/dt's component (fluid-like)
+    static constexpr int IW = NSX;   // the first vorticity component
     struct AccT {
-        float dv[ND], cdv[ND], pdv[ND];
-        float dr, cdr, pdr;
-        float sr[NS > 0 ? NS : 1], csr[NS > 0 ? NS : 1], psr[NS > 0 ? NS : 1];
-        float w[3], cw[3], pw[3];
+        float p[NSUM];
     };
     // A zero partial is skipped (a compensated add of 0 would fold c into
     // s), so a strip a sweep does not visit merges exactly like an empty one.
-    static __device__ __forceinline__ void merge(float& s, float& c, float& p) {
-        if (p != 0.f) kadd(s, c, p);
-        p = 0.f;
+    template <class Sum>
+    static __device__ __forceinline__ void flush(AccT& acc, Sum& sum) {
+#pragma unroll
+        for (int j = 0; j < NSUM; ++j) {
+            if (acc.p[j] != 0.f) kadd(sum.S(j), sum.C(j), acc.p[j]);
+            acc.p[j] = 0.f;
+        }
     }
-    static __device__ __forceinline__ void flush(AccT& acc) {
+    template <class Sum>
+    static __device__ __forceinline__ void init_sum(Sum& sum) {
 #pragma unroll
-        for (int d = 0; d < ND; ++d) merge(acc.dv[d], acc.cdv[d], acc.pdv[d]);
-        merge(acc.dr, acc.cdr, acc.pdr);
-#pragma unroll
-        for (int q = 0; q < (NS > 0 ? NS : 1); ++q) merge(acc.sr[q], acc.csr[q], acc.psr[q]);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) merge(acc.w[q], acc.cw[q], acc.pw[q]);
+        for (int j = 0; j < NSUM; ++j) sum.S(j) = sum.C(j) = 0.f;
     }
     static __device__ __forceinline__ void load(const ForceArgs& A, int64_t gi, Own& w) {
         const int64_t N = A.aN;
@@ -564,29 +596,25 @@ struct PhysF32 {
     static __device__ __forceinline__ const double* xpos(const Own& w) { return w.x; }
     static __device__ __forceinline__ void init(const ForceArgs&, int64_t, AccT& acc, bool) {
 #pragma unroll
-        for (int d = 0; d < ND; ++d) acc.dv[d] = acc.cdv[d] = acc.pdv[d] = 0.f;
-        acc.dr = acc.cdr = acc.pdr = 0.f;
-#pragma unroll
-        for (int q = 0; q < (NS > 0 ? NS : 1); ++q) acc.sr[q] = acc.csr[q] = acc.psr[q] = 0.f;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) acc.w[q] = acc.cw[q] = acc.pw[q] = 0.f;
+        for (int j = 0; j < NSUM; ++j) acc.p[j] = 0.f;
     }
     // (the sweeps merge every strip's partials before storing)
-    static __device__ __forceinline__ void store(const ForceArgs& A, int64_t gi, const AccT& acc) {
+    template <class Sum>
+    static __device__ __forceinline__ void store_sum(const ForceArgs& A, int64_t gi, const AccT&, Sum& sum) {
         // FP64 state += compensated FP32 sum (s − c)
         const int64_t N = A.aN;
-        if (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID || PFN == GC_PFN_COUNT) {
+        if (FLUIDLIKE) {
 #pragma unroll
             for (int d = 0; d < ND; ++d)
-                A.advdt[d * N + gi] = A.advdt[d * N + gi] + ((double)acc.dv[d] - (double)acc.cdv[d]);
-            A.adrhodt[gi] = A.adrhodt[gi] + ((double)acc.dr - (double)acc.cdr);
+                A.advdt[d * N + gi] = A.advdt[d * N + gi] + ((double)sum.S(d) - (double)sum.C(d));
+            A.adrhodt[gi] = A.adrhodt[gi] + ((double)sum.S(IDR) - (double)sum.C(IDR));
         } else {
 #pragma unroll
-            for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = A.asr[q * N + gi] + ((double)acc.sr[q] - (double)acc.csr[q]);
+            for (int q = 0; q < NS; ++q) A.asr[q * N + gi] = A.asr[q * N + gi] + ((double)sum.S(q) - (double)sum.C(q));
             if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
 #pragma unroll
-                for (int q = 0; q < (ND == 2 ? 1 : 3); ++q)
-                    A.avort[q * N + gi] = A.avort[q * N + gi] + ((double)acc.w[q] - (double)acc.cw[q]);
+                for (int q = 0; q < NVORT; ++q)
+                    A.avort[q * N + gi] = A.avort[q * N + gi] + ((double)sum.S(IW + q) - (double)sum.C(IW + q));
             }
         }
     }
@@ -671,8 +699,10 @@ struct PhysF32 {
         const bool in = rr < G.cutoff_sq;
         if (P2 == GC_PFN_COUNT) {
             if (!in) return 0;
-            acc.dv[0] += 1.f;
-            acc.dr += 1.f;
+            if constexpr (FLUIDLIKE) {
+                acc.p[0] += 1.f;
+                acc.p[IDR] += 1.f;
+            }
             return 1;
         }
         float dxf[ND];
@@ -733,12 +763,15 @@ struct PhysF32 {
                 sr[5] = 0.5f * (dv[1] * gx[2] + dv[2] * gx[1]);
             }
 #pragma unroll
-            for (int q2 = 0; q2 < NS; ++q2) padd_if(acc.psr[q2], sr[q2] * f, in);
-            if (P2 == GC_PFN_STRAIN_RATE_VORTICITY) {
-                padd_if(acc.pw[0], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f, in);
-                if (ND == 3) {
-                    padd_if(acc.pw[1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f, in);
-                    padd_if(acc.pw[2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f, in);
+            if constexpr (!FLUIDLIKE) {
+#pragma unroll
+                for (int q2 = 0; q2 < NS; ++q2) padd_if(acc.p[q2], sr[q2] * f, in);
+                if constexpr (P2 == GC_PFN_STRAIN_RATE_VORTICITY && PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
+                    padd_if(acc.p[IW], 0.5f * (dv[0] * gx[1] - dv[1] * gx[0]) * f, in);
+                    if (ND == 3) {
+                        padd_if(acc.p[IW + 1], 0.5f * (dv[0] * gx[2] - dv[2] * gx[0]) * f, in);
+                        padd_if(acc.p[IW + 2], 0.5f * (dv[1] * gx[2] - dv[2] * gx[1]) * f, in);
+                    }
                 }
             }
             return in ? 1 : 0;
@@ -763,7 +796,8 @@ struct PhysF32 {
                 const float rfj = (0.01f * ca) * ca * lj;
                 const float s = -G.f_bmass * piv;
 #pragma unroll
-                for (int d = 0; d < ND; ++d) padd_if(acc.pdv[d], s * gx[d] + rfj * dxf[d], in);
+                if constexpr (FLUIDLIKE)
+                    for (int d = 0; d < ND; ++d) padd_if(acc.p[d], s * gx[d] + rfj * dxf[d], in);
                 return in ? 1 : 0;
             }
             const float mj = (self || dyn) ? ma : G.f_bmass;
@@ -780,7 +814,8 @@ struct PhysF32 {
                 if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
                 const float s = mj * (dh - piv);
 #pragma unroll
-                for (int d = 0; d < ND; ++d) padd_if(acc.pdv[d], s * gx[d], in);
+                if constexpr (FLUIDLIKE)
+                    for (int d = 0; d < ND; ++d) padd_if(acc.p[d], s * gx[d], in);
             } else {
                 // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
                 float sj[NS > 0 ? NS : 1];
@@ -801,7 +836,8 @@ struct PhysF32 {
                             (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
                 }
 #pragma unroll
-                for (int d = 0; d < ND; ++d) padd_if(acc.pdv[d], mj * (hv[d] - piv * gx[d]), in);
+                if constexpr (FLUIDLIKE)
+                    for (int d = 0; d < ND; ++d) padd_if(acc.p[d], mj * (hv[d] - piv * gx[d]), in);
             }
             float tail = 0.f;
             if (P.has_delta) {
@@ -809,7 +845,7 @@ struct PhysF32 {
                 const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
                 tail = psi * irhoj;
             }
-            padd_if(acc.pdr, mj * (dotf<ND>(dv, gx) + tail), in);
+            if constexpr (FLUIDLIKE) padd_if(acc.p[IDR], mj * (dotf<ND>(dv, gx) + tail), in);
             (void)gi;
             return in ? 1 : 0;
         }
@@ -1005,6 +1041,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
         const double* ox = Phys::xpos(w);
         typename Phys::AccT acc;
         Phys::init(A, gi, acc, !COUNT_ONLY);
+        SumRegs<Phys::NSUM> sum;
+        Phys::init_sum(sum);
 
         for (int ri = 0; ri < A.nref; ++ri) {
             const InterRef& r = A.ref[ri];
@@ -1081,7 +1119,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                                                                              BT, acc);
                         nbuf = 0;
                         __syncwarp();
-                        Phys::flush(acc);
+                        Phys::flush(acc, sum);
                     }
                 }
                 accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col, BT, acc);
@@ -1108,7 +1146,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                         accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col,
                                                                              BT, acc);
                         nbuf = 0;
-                        Phys::flush(acc);
+                        Phys::flush(acc, sum);
                     }
                 }
                 accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col, BT, acc);
@@ -1117,7 +1155,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
             __syncwarp();
             if (active && r.counts) r.counts[gi] = accepted;
         }
-        if (!COUNT_ONLY && active) Phys::store(A, gi, acc);
+        if (!COUNT_ONLY && active) Phys::store_sum(A, gi, acc, sum);
         __syncwarp();
     }
 }
@@ -1130,9 +1168,9 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
 // grid and functor parameters for this warp's instance.
 constexpr int STG_GI_BYTES = SWEEP_GI_BYTES;
 constexpr int STG_PI_BYTES = SWEEP_PI_BYTES;
-template <int ND, int NQ, int CH>
+template <int ND, int NQ, int CH, int NSUM>
 __host__ __device__ constexpr int stg_warp_bytes() {
-    return NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16 + STG_GI_BYTES + STG_PI_BYTES + 16;
+    return NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16 + STG_GI_BYTES + STG_PI_BYTES + 16 + NSUM * 2 * 32 * 4;
 }
 
 
@@ -1150,7 +1188,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
     static_assert(CH % 32 == 0 && CH >= 32 && CH <= 128, "chunk of 1 to 4 batches of 32");
     constexpr int NB = CH / 32;
     constexpr int NQ = Phys::NQ;
-    constexpr int WB = stg_warp_bytes<ND, NQ, CH>();
+    constexpr int WB = stg_warp_bytes<ND, NQ, CH, Phys::NSUM>();
     extern __shared__ float4 sstg[];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -1164,6 +1202,8 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
     GridInst* gsm = reinterpret_cast<GridInst*>(wbase + NQ * CH * 16 + 32 + (ND * CH * 4 + 15) / 16 * 16);
     PfnInst* psm = reinterpret_cast<PfnInst*>(reinterpret_cast<char*>(gsm) + STG_GI_BYTES);
     float2* camsm = reinterpret_cast<float2*>(reinterpret_cast<char*>(psm) + STG_PI_BYTES);
+    // this lane's compensated sums (touched only at strip ends)
+    SumSmem<Phys::NSUM> sum{reinterpret_cast<float*>(reinterpret_cast<char*>(camsm) + 16), lane};
     const int64_t ngroups = *A.ngroups;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wg < ngroups; wg += nwarps) {
@@ -1176,6 +1216,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
         const double* ox = Phys::xpos(w);
         typename Phys::AccT acc;
         Phys::init(A, gi, acc, true);
+        Phys::init_sum(sum);
 
         for (int ri = 0; ri < A.nref; ++ri) {
             const InterRef& r = A.ref[ri];
@@ -1278,7 +1319,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                             }
                             __syncwarp();  // every lane is done with the chunk before the next one lands
                         }
-                        Phys::flush(acc);  // the strip's partial sums
+                        Phys::flush(acc, sum);  // the strip's partial sums
                     }
                 };
                 if (self) strips(std::integral_constant<int, BT_SELF>{});
@@ -1294,13 +1335,13 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                         if (self && j == gi) continue;
                         accepted += Phys::template pair<PFN>(A, r, G, P, gi, k, w, da, j, acc);
                     }
-                    Phys::flush(acc);
+                    Phys::flush(acc, sum);
                 }
             }
             __syncwarp();
             if (active && r.counts) r.counts[gi] = accepted;
         }
-        if (active) Phys::store(A, gi, acc);
+        if (active) Phys::store_sum(A, gi, acc, sum);
         __syncwarp();
     }
 }
@@ -1314,7 +1355,7 @@ static void launch_c(const ForceArgs& A, cudaStream_t s) {
     if (blocks > (int64_t)A.num_sms * cf.minb * 4) blocks = (int64_t)A.num_sms * cf.minb * 4;
     if (blocks < 1) blocks = 1;
     if constexpr (cf.stg > 0 && Phys::NQ > 0) {
-        constexpr size_t smem = (size_t)(FORCE_TPB / 32) * stg_warp_bytes<ND, Phys::NQ, cf.stg>();
+        constexpr size_t smem = (size_t)(FORCE_TPB / 32) * stg_warp_bytes<ND, Phys::NQ, cf.stg, Phys::NSUM>();
         auto kern = k_sweep_stg<Phys, ND, PFN, cf.minb, cf.stg>;
         if (smem > 48 * 1024) {
             static bool opted = false;
