@@ -77,6 +77,7 @@ struct Request {
     int batch = -1;
     int waited = 0;  // rounds spent admitted but not yet packed
     std::vector<Result> result;
+    bool result_ready = false;  // result copied to the host by its batch's thread
     std::string err;
 };
 
@@ -182,6 +183,7 @@ struct Job {
     gc::PackJob* plan = nullptr;
     std::vector<int64_t> ids;        // the batch's requests in the new context
     std::vector<int64_t> joiners;    // of those, the ones not yet in a context
+    std::vector<int64_t> stepping;   // the requests of the context that steps this round, in its instance order
     std::vector<double> cfl;
     int steps = 0;                   // this round's steps
     double cfl0 = 0;
@@ -255,7 +257,36 @@ Job plan_round(gc_server* s, Batch& B) {
     }
     for (int64_t id : J.ids) J.cfl.push_back(s->reqs[id].cfl);
     if (J.repack && !src.empty()) J.plan = gc::ctx_pack_plan(s->precision, src);
+    J.stepping = J.repack && !J.pipelined ? J.ids : B.live;
     return J;
+}
+
+// The results of the requests that finish in this round, copied to the
+// host by the batch's own thread right after its steps (so the copies
+// overlap the other batches' steps).
+void collect_results(gc_server* s, Batch& B, const Job& J) {
+    if (!B.ctx || B.last_status != GC_OK) return;
+    for (size_t k = 0; k < J.stepping.size(); ++k) {
+        Request& r = s->reqs.at(J.stepping[k]);
+        if (r.state != RQ_RUNNING || r.done + J.steps < r.nsteps) continue;
+        std::vector<std::array<int64_t, 3>> fields;
+        gc::ctx_result_fields(B.ctx, (int)k, fields);
+        r.result.clear();
+        r.result_ready = true;
+        for (auto& f : fields) {
+            Result res;
+            res.handle = (int)f[0];
+            res.field = (int)f[1];
+            res.bytes.resize((size_t)f[2]);
+            if (gc_download_field(B.ctx, (int)k, res.handle, res.field, res.bytes.data(), res.bytes.size()) !=
+                GC_OK) {
+                r.result_ready = false;
+                r.err = gc::ctx_error(B.ctx);
+                break;
+            }
+            r.result.push_back(std::move(res));
+        }
+    }
 }
 
 // Build the planned context (and, once its running sources have stopped,
@@ -294,9 +325,10 @@ void run_round(gc_server* s, Job& J) {
     if (J.pipelined) {
         std::thread builder([s, &J] { build_new(s, J); });
         step_batch(B, J);
+        collect_results(s, B, J);
         builder.join();
         if (B.last_status == GC_OK) fill_new(s, J);
-        return;  // the server thread switches contexts after reading the round's results
+        return;  // the server thread switches contexts after the round's bookkeeping
     }
     if (J.repack) {
         build_new(s, J);
@@ -307,6 +339,7 @@ void run_round(gc_server* s, Job& J) {
         J.nc = nullptr;
     }
     step_batch(B, J);
+    collect_results(s, B, J);
 }
 
 // The repack's bookkeeping, on the server's thread (after the round's
@@ -374,22 +407,8 @@ void retire(gc_server* s, Batch& B, int steps, int* ncompleted) {
             r.done += steps;
             s->stats.particle_steps += r.moving * steps;
             if (r.done < r.nsteps) continue;
-            std::vector<std::array<int64_t, 3>> fields;
-            gc::ctx_result_fields(B.ctx, (int)k, fields);
-            r.result.clear();
-            for (auto& f : fields) {
-                Result res;
-                res.handle = (int)f[0];
-                res.field = (int)f[1];
-                res.bytes.resize((size_t)f[2]);
-                if (gc_download_field(B.ctx, (int)k, res.handle, res.field, res.bytes.data(), res.bytes.size()) !=
-                    GC_OK) {
-                    r.state = RQ_FAILED;
-                    r.err = gc::ctx_error(B.ctx);
-                    break;
-                }
-                r.result.push_back(std::move(res));
-            }
+            // the batch's thread copied the result (collect_results)
+            if (!r.result_ready) r.state = RQ_FAILED;
             if (r.state != RQ_FAILED) {
                 r.state = RQ_DONE;
                 r.t_done = s->now();

@@ -762,7 +762,6 @@ struct PhysF32 {
                 sr[4] = 0.5f * (dv[0] * gx[2] + dv[2] * gx[0]);
                 sr[5] = 0.5f * (dv[1] * gx[2] + dv[2] * gx[1]);
             }
-#pragma unroll
             if constexpr (!FLUIDLIKE) {
 #pragma unroll
                 for (int q2 = 0; q2 < NS; ++q2) padd_if(acc.p[q2], sr[q2] * f, in);
@@ -795,8 +794,8 @@ struct PhysF32 {
                 const float lj = rf < G.f_ljcut ? (x6 * x6 - x6) / rrf : 0.f;
                 const float rfj = (0.01f * ca) * ca * lj;
                 const float s = -G.f_bmass * piv;
-#pragma unroll
                 if constexpr (FLUIDLIKE)
+#pragma unroll
                     for (int d = 0; d < ND; ++d) padd_if(acc.p[d], s * gx[d] + rfj * dxf[d], in);
                 return in ? 1 : 0;
             }
@@ -813,8 +812,8 @@ struct PhysF32 {
                 // |p| = |p/ρ²|·ρ² from the record
                 if (two && P.has_eps) dh -= P.f_eps * (fabsf(w.aux) * w.rho * irhoj + fabsf(auxj) * rhoj * w.irho);
                 const float s = mj * (dh - piv);
-#pragma unroll
                 if constexpr (FLUIDLIKE)
+#pragma unroll
                     for (int d = 0; d < ND; ++d) padd_if(acc.p[d], s * gx[d], in);
             } else {
                 // Cauchy stress divergence: stress_j is the own stress on a dynamic boundary
@@ -835,8 +834,8 @@ struct PhysF32 {
                     hv[2] = (w.sig[4] * gx[0] + w.sig[5] * gx[1] + w.sig[2] * gx[2]) * ci +
                             (sj[4] * gx[0] + sj[5] * gx[1] + sj[2] * gx[2]) * cj;
                 }
-#pragma unroll
                 if constexpr (FLUIDLIKE)
+#pragma unroll
                     for (int d = 0; d < ND; ++d) padd_if(acc.p[d], mj * (hv[d] - piv * gx[d]), in);
             }
             float tail = 0.f;
