@@ -6,6 +6,11 @@
 // thread.  A batch is repacked at a round boundary when requests join or
 // leave; state of the simulations that stay is copied on the device.
 //
+// A step that fails (a non-finite position, say) fails the whole batch's
+// context, whichever request caused it: the batch's running requests then
+// run again from their submitted state, each in a batch of its own, and
+// only a request that fails alone fails.
+//
 // Rounds: every batch advances min(round_steps, the fewest steps any of its
 // running requests still needs) steps, so a request stops exactly at its
 // step count.  Its result is then copied to host memory and its instance is
@@ -76,6 +81,7 @@ struct Request {
     int64_t est = 0, particles = 0, moving = 0;
     int batch = -1;
     int waited = 0;  // rounds spent admitted but not yet packed
+    bool solo = false;  // runs in a batch of its own (a retry after a batch failure)
     std::vector<Result> result;
     bool result_ready = false;  // result copied to the host by its batch's thread
     std::string err;
@@ -90,6 +96,7 @@ struct Batch {
     std::vector<int64_t> joining;  // admitted, packed at the next repack
     bool dirty = false;            // a request failed: repack at the next round
     bool fresh = false;            // ctx is new: its first round runs on a highest-priority stream
+    bool solo = false;             // holds one retried request, no other joins
     int64_t est = 0;               // estimated bytes of live + joining requests
     int last_status = GC_OK;
     std::string last_err;
@@ -127,13 +134,15 @@ int serr(gc_server* s, int code, const std::string& msg) {
 // A batch of the same structure with room for `est` more bytes, else a new
 // one.  A repack holds the old and the new context at once, so batches are
 // kept to a fraction of the budget.
-int find_batch(gc_server* s, gc_ctx* model, int64_t est) {
+int find_batch(gc_server* s, gc_ctx* model, int64_t est, bool solo) {
     for (size_t b = 0; b < s->batches.size(); ++b) {
         Batch& B = s->batches[b];
-        if (!gc::ctx_same_structure(B.proto, 0, model, 0)) continue;
-        if (B.est == 0 || (size_t)(B.est + est) <= s->max_batch) return (int)b;
+        if (B.solo != solo || !gc::ctx_same_structure(B.proto, 0, model, 0)) continue;
+        const bool empty = !B.ctx && B.live.empty() && B.joining.empty();
+        if (solo ? empty : (B.est == 0 || (size_t)(B.est + est) <= s->max_batch)) return (int)b;
     }
     Batch nb;
+    nb.solo = solo;
     if (gc::ctx_model_copy(model, 0, &nb.proto) != GC_OK) return -1;
     s->batches.push_back(nb);
     return (int)s->batches.size() - 1;
@@ -154,7 +163,7 @@ void admit(gc_server* s) {
             ++it;
             continue;
         }
-        const int b = find_batch(s, r.model, r.est);
+        const int b = find_batch(s, r.model, r.est, r.solo);
         if (b < 0) {
             ++it;
             continue;
@@ -193,6 +202,12 @@ struct Job {
     double repack_s = 0;
 };
 
+// A request of B's list still runs in B (a retried one was listed by the
+// batch whose step failed and may run elsewhere now).
+bool runs_in(gc_server* s, const Batch& B, const Request& r) {
+    return r.state == RQ_RUNNING && r.batch == (int)(&B - s->batches.data());
+}
+
 Job plan_round(gc_server* s, Batch& B) {
     Job J;
     J.B = &B;
@@ -201,7 +216,7 @@ Job plan_round(gc_server* s, Batch& B) {
     int64_t left = s->round_steps;  // steps of this round over the current context's running requests
     for (int64_t id : B.live) {
         const Request& r = s->reqs[id];
-        if (r.state == RQ_RUNNING) {
+        if (runs_in(s, B, r)) {
             live_p += r.moving;
             if (nlive == 0) J.cfl0 = r.cfl;
             ++nlive;
@@ -231,7 +246,7 @@ Job plan_round(gc_server* s, Batch& B) {
         if (J.pipelined) J.steps = (int)std::max<int64_t>(left, 0);
         for (size_t k = 0; k < B.live.size(); ++k) {
             const Request& r = s->reqs[B.live[k]];
-            if (r.state != RQ_RUNNING) continue;
+            if (!runs_in(s, B, r)) continue;
             if (J.pipelined && r.nsteps - r.done <= J.steps) continue;  // finishes in this round
             src.push_back({B.ctx, (int)k});
             J.ids.push_back(B.live[k]);
@@ -268,7 +283,7 @@ void collect_results(gc_server* s, Batch& B, const Job& J) {
     if (!B.ctx || B.last_status != GC_OK) return;
     for (size_t k = 0; k < J.stepping.size(); ++k) {
         Request& r = s->reqs.at(J.stepping[k]);
-        if (r.state != RQ_RUNNING || r.done + J.steps < r.nsteps) continue;
+        if (!runs_in(s, B, r) || r.done + J.steps < r.nsteps) continue;
         std::vector<std::array<int64_t, 3>> fields;
         gc::ctx_result_fields(B.ctx, (int)k, fields);
         r.result.clear();
@@ -397,12 +412,27 @@ void finish_repack(gc_server* s, Job& J, bool round_ok) {
 // After a round of `steps` steps: count them, copy finished results to the
 // host and freeze their instances; a failure marks the batch for a repack.
 void retire(gc_server* s, Batch& B, int steps, int* ncompleted) {
+    std::vector<int64_t> retry;
     for (size_t k = 0; k < B.live.size(); ++k) {
         Request& r = s->reqs[B.live[k]];
-        if (r.state != RQ_RUNNING) continue;
+        if (!runs_in(s, B, r)) continue;
         if (B.last_status != GC_OK) {
-            r.state = RQ_FAILED;
-            r.err = B.last_err;
+            if (!r.solo) {
+                // another request may have caused it: again, alone
+                r.solo = true;
+                r.state = RQ_QUEUED;
+                r.done = 0;
+                r.waited = 0;
+                r.batch = -1;
+                r.t_admit = -1;
+                r.result.clear();
+                r.result_ready = false;
+                retry.push_back(r.id);
+                s->stats.retries += 1;
+            } else {
+                r.state = RQ_FAILED;
+                r.err = B.last_err;
+            }
         } else {
             r.done += steps;
             s->stats.particle_steps += r.moving * steps;
@@ -423,6 +453,8 @@ void retire(gc_server* s, Batch& B, int steps, int* ncompleted) {
         B.est -= std::min(B.est, r.est);
         B.dirty = true;
     }
+    // retried requests go to the front of the queue, in their order
+    s->queue.insert(s->queue.begin(), retry.begin(), retry.end());
     B.last_status = GC_OK;
 }
 
@@ -571,7 +603,7 @@ int gc_serve_get_stats(gc_server* s, gc_serve_stats* out) {
     out->batches = 0;
     for (auto& B : s->batches) {
         if (B.ctx) out->batches += 1;
-        for (int64_t id : B.live) out->running += s->reqs[id].state == RQ_RUNNING;
+        for (int64_t id : B.live) out->running += runs_in(s, B, s->reqs[id]);
         out->running += (int64_t)B.joining.size();
     }
     out->device_bytes_reserved = (int64_t)s->used;

@@ -757,7 +757,7 @@ class ServeStats(ct.Structure):
     _fields_ = [("queued", ct.c_int64), ("running", ct.c_int64), ("batches", ct.c_int64),
                 ("rounds", ct.c_int64), ("repacks", ct.c_int64), ("particle_steps", ct.c_int64),
                 ("device_bytes_reserved", ct.c_int64), ("repack_seconds", ct.c_double),
-                ("repack_instances", ct.c_int64)]
+                ("repack_instances", ct.c_int64), ("retries", ct.c_int64)]
 
 
 class Server:

@@ -414,6 +414,9 @@ typedef struct gc_serve_stats {
     int64_t device_bytes_reserved;   /* estimates of the admitted requests     */
     double repack_seconds;           /* host time spent rebuilding batches     */
     int64_t repack_instances;        /* requests placed by those rebuilds      */
+    int64_t retries;                 /* requests run again alone, from their
+                                        submitted state, after their batch's
+                                        step failed                          */
 } gc_serve_stats;
 enum { GC_REQ_FAILED = -1, GC_REQ_QUEUED = 0, GC_REQ_RUNNING = 1, GC_REQ_DONE = 2 };
 

@@ -123,3 +123,32 @@ def test_request_waits_for_budget_then_runs():
             assert np.array_equal(getattr(sg, name), getattr(sr, name), equal_nan=True), f"{sg.name}.{name}"
     st = srv.stats()
     assert st["repacks"] >= 2 and st["repack_seconds"] > 0.0 and st["repack_instances"] >= 2
+
+
+def test_failing_request_is_retried_alone_and_isolated():
+    """A request with a non-finite position makes its batch's step fail,
+    whichever of the batch's requests caused it.  The server then runs the
+    batch's requests again from their submitted state, each in a batch of
+    its own: only the bad request fails, and the others finish with the
+    results of the same simulation run alone."""
+    reqs = _requests()[:3]  # three columns: one structure, one batch
+    bad_lf, _, _ = _requests()[1]
+    bad_lf.systems[0].x[0, 0] = np.nan
+    srv = G.Server(round_steps=8, precision=G.PRECISION_FP64, hbm_budget=2 * 10**9)
+    ids = []
+    for k, (lf, meta, n) in enumerate(reqs):
+        ids.append(srv.submit(bad_lf if k == 1 else lf, n, meta["cfl"]))
+    rounds = 0
+    while any(srv.poll(r)["state"] in (G.Server.QUEUED, G.Server.RUNNING) for r in ids):
+        srv.pump()
+        rounds += 1
+        assert rounds < 400
+    assert [srv.poll(r)["state"] for r in ids] == [G.Server.DONE, G.Server.FAILED, G.Server.DONE]
+    assert srv.stats()["retries"] >= 3
+    for k in (0, 2):
+        got = srv.fetch(ids[k])
+        ref = _alone(k, G.PRECISION_FP64)
+        for sg, sr in zip(got.systems, ref.systems):
+            for name, _ in sg.particle_fields():
+                assert np.array_equal(getattr(sg, name), getattr(sr, name), equal_nan=True), \
+                    f"request {k}: {sg.name}.{name}"
