@@ -224,6 +224,8 @@ struct DInter {
     // scan are skipped on the device when the geometry is unchanged
     int* d_keep = nullptr;          // [0] cs is current for d_gi_prev, [1] this step's grid equals it
     GridInst* d_gi_prev = nullptr;  // geometry cs was last counted on, per instance
+    int32_t* hist = nullptr;        // its own histogram (batched still grids): zero between uses
+    int64_t cap_hist = 0;
 };
 
 // One captured step: valid for the buffer parities `pre` (cur of every slot,
@@ -1033,8 +1035,14 @@ int finalize(gc_ctx* ctx) {
         ctx->inters[i].need_slot = (int64_t)(ctx->slots.size() + ctx->ghosts.size() + i);
     {
         std::vector<GridPlanArgs> pa;  // the steps' interactions; probe grids are planned at measurement
-        for (auto& D : ctx->inters)
-            if (!D.probe) pa.push_back(grid_plan_args(ctx, D));
+        for (auto& D : ctx->inters) {
+            if (D.probe) continue;
+            pa.push_back(grid_plan_args(ctx, D));
+            // the keep check of a still system_b's CSR runs in its plan (the
+            // only plan of such an interaction in a step)
+            pa.back().prev = D.d_gi_prev;
+            pa.back().keep = D.d_keep;
+        }
         ctx->nplan = (int)pa.size();
         TRY(dalloc(ctx, &ctx->d_plan_args, pa.size()));
         TRY(hcopy(ctx, ctx->d_plan_args, pa.data(), pa.size() * sizeof(GridPlanArgs), cudaMemcpyHostToDevice));
@@ -1075,7 +1083,15 @@ int ensure_inter_cells(gc_ctx* ctx, DInter& D, int64_t cells) {
         TRY(dalloc(ctx, &D.cs, (size_t)cap));
         if (D.btype != BT_SELF) TRY(dalloc(ctx, &D.cs_a, (size_t)cap));
         D.cap_cells = cap;
-        if (D.d_keep) CU(cudaMemsetAsync(D.d_keep, 0, sizeof(int), ctx->stream));  // new buffer: nothing counted
+        if (D.d_keep) {
+            // its own histogram for the batched still grids, zero between uses
+            dfree(ctx, D.hist, D.cap_hist);
+            D.cap_hist = still_hist_elems(cap);
+            TRY(dalloc(ctx, &D.hist, (size_t)D.cap_hist));
+            CU(cudaMemsetAsync(D.hist, 0, sizeof(int32_t) * D.cap_hist, ctx->stream));
+            // new buffer: nothing counted (the step's plan may already have set keep[1])
+            CU(cudaMemsetAsync(D.d_keep, 0, 2 * sizeof(int), ctx->stream));
+        }
     }
     return ensure_cells(ctx, cells);
 }
@@ -1266,18 +1282,15 @@ AParts a_parts(gc_ctx* ctx, const DInter& D) {
 }
 
 // allow_keep: system_b's positions have not changed since its CSR was last
-// counted, so an unchanged geometry keeps the CSR (decided on the device).
+// counted, so an unchanged geometry keeps the CSR (decided on the device by
+// the step's plan, keep[1]).
 int build_grid(gc_ctx* ctx, DInter& D, int64_t cells, bool allow_keep = false) {
     TRY(ensure_inter_cells(ctx, D, cells));
     DSlot& A = ctx->slots[D.a];
     const int* skip = nullptr;
     if (D.d_keep) {
-        if (allow_keep) {
-            launch_grid_keep(D.d_gi, D.d_gi_prev, ninst(ctx), A.nd, D.d_keep, ctx->stream);
-            skip = D.d_keep + 1;
-        } else {
-            CU(cudaMemsetAsync(D.d_keep, 0, sizeof(int), ctx->stream));  // counted on a geometry not recorded
-        }
+        if (allow_keep) skip = D.d_keep + 1;
+        else CU(cudaMemsetAsync(D.d_keep, 0, sizeof(int), ctx->stream));  // counted on a geometry not recorded
     }
     const double* bx;
     const int32_t* binst;
@@ -1309,6 +1322,32 @@ int build_grid(gc_ctx* ctx, DInter& D, int64_t cells, bool allow_keep = false) {
     D.grid_ver = ++ctx->grid_version;
     D.csa_ver = D.two_sided ? D.grid_ver : -1;
     return check_launch(ctx, "grid");
+}
+
+// The grids of interactions against a system_b that does not move, built
+// together: one count and one scan launch for all of them, each returning
+// at once on the device while its grid's geometry is unchanged (keep[1]).
+int build_still_grids(gc_ctx* ctx, const std::vector<DInter*>& L, const std::vector<int64_t>& need) {
+    for (size_t i0 = 0; i0 < L.size(); i0 += STILL_MAX) {
+        StillGridArgs a{};
+        a.n = (int)std::min<size_t>(STILL_MAX, L.size() - i0);
+        a.err = ctx->d_err;
+        a.incons = ctx->d_incons;
+        for (int i = 0; i < a.n; ++i) {
+            DInter& D = *L[i0 + i];
+            const int64_t cells = need[D.need_slot];
+            TRY(ensure_inter_cells(ctx, D, cells));  // sizes the histogram with the CSR
+            DSlot& B = ctx->slots[D.bslot];
+            a.nd = ctx->slots[D.a].nd;
+            a.g[i] = StillGrid{B.F(F_X), B.inst_of, B.N, D.d_gi, D.d_keep, D.hist, D.cs, cells};
+            D.grid_valid = true;
+            D.cells = cells;
+            D.grid_ver = ++ctx->grid_version;
+            D.csa_ver = -1;
+        }
+        launch_still_grids(a, ctx->stream);
+    }
+    return check_launch(ctx, "still grids");
 }
 
 // CSR of system_a's particles on a coupled interaction's grid.
@@ -1427,13 +1466,18 @@ int prepare(gc_ctx* ctx, const std::vector<char>& sort_mask) {
     }
     // grids (ghost-b plans are recomputed from the exact ghost boxes; the
     // cell count cannot exceed the planned bound)
+    std::vector<DInter*> still;
     for (auto& D : ctx->inters) {
         if (D.probe) continue;
         if (D.btype == BT_GHOST || D.ag >= 0) launch_grid_plan(grid_plan_args(ctx, D), ctx->stream);
         const bool b_still = D.d_keep && !sort_mask[D.bslot] && !ctx->slots[D.bslot].xmoves();
+        if (b_still && ctx->slots[D.bslot].N > 0 && need[D.need_slot] <= STILL_MAX_CELLS) {
+            still.push_back(&D);
+            continue;
+        }
         TRY(build_grid(ctx, D, need[D.need_slot], b_still));
     }
-    return GC_OK;
+    return build_still_grids(ctx, still, need);
 }
 
 StepArgs step_args(DSlot& S) {
@@ -2720,6 +2764,7 @@ int gc_ctx_destroy(gc_ctx* ctx) {
         dev_free(ctx, D.counts);
         dev_free(ctx, D.d_keep);
         dev_free(ctx, D.d_gi_prev);
+        dev_free(ctx, D.hist);
     }
     dev_free(ctx, ctx->key);
     dev_free(ctx, ctx->perm);

@@ -80,6 +80,12 @@ struct GridPlanArgs {
     const int64_t* bn;     // ghost-b counts per instance (nullptr otherwise)
     int64_t* need;         // total cells
     int* err;
+    // interactions whose system_b does not move (nullptr otherwise): after
+    // the plan, keep[1] = (every instance's grid equals prev) && keep[0],
+    // prev = the grid, keep[0] = 1.  keep[0] says the CSR is current for
+    // prev; keep[1] lets this step's count and scan return at once.
+    GridInst* prev;
+    int* keep;
 };
 void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s);
 // The plans of n interactions (device array of arguments), one block each.
@@ -89,9 +95,31 @@ void launch_grid_plan_all(const GridPlanArgs* d_args, int n, cudaStream_t s);
 void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                        const GridInst* gi, int32_t* hist, int64_t cells_cap, int* err,
                        unsigned long long* incons, cudaStream_t s, const int* skip = nullptr);
-// state[1] = (every instance's grid equals prev) && state[0]; prev = grid;
-// state[0] = 1 (see k_grid_keep).
-void launch_grid_keep(const GridInst* gi, GridInst* prev, int ninst, int nd, int* state, cudaStream_t s);
+// The grids of the interactions whose system_b does not move, counted and
+// scanned in one launch each: entry y of the table is interaction y's CSR,
+// counted into its own histogram (zero between uses; the scan clears it)
+// and skipped on the device while keep[1] is set.  cells <= STILL_MAX_CELLS.
+constexpr int STILL_MAX = 16;
+constexpr int64_t STILL_MAX_CELLS = 2048LL * 2048LL;
+struct StillGrid {
+    const double* x;
+    const int32_t* inst_of;
+    int64_t N;      // system_b's particles
+    const GridInst* gi;
+    const int* keep;
+    int32_t* hist;  // cells entries, then the scan's tile sums
+    int32_t* cs;    // CSR, cells + 1 entries
+    int64_t cells;
+};
+struct StillGridArgs {
+    StillGrid g[STILL_MAX];
+    int n, nd;
+    int* err;
+    unsigned long long* incons;
+};
+// Tile sums after the histogram's cells: entries of hist beyond cells.
+int64_t still_hist_elems(int64_t cells);
+void launch_still_grids(const StillGridArgs& a, cudaStream_t s);
 
 // ---------------------------------------------------------------- ghosts
 struct GhostGenArgs {

@@ -807,6 +807,27 @@ __device__ void grid_plan_block(const GridPlanArgs& a) {
             B.f_bc = fbc;
         }
     }
+    if (a.keep) {
+        // is every instance's grid the one the CSR was last counted on?
+        __shared__ int same;
+        __syncthreads();
+        if (threadIdx.x == 0) same = a.keep[0];
+        __syncthreads();
+        for (int k = threadIdx.x; k < a.ninst; k += blockDim.x) {
+            const GridInst& g = a.gi[k];
+            const GridInst& p = a.prev[k];
+            bool eq = g.cellbase == p.cellbase && g.ncells == p.ncells;
+            for (int d = 0; d < a.nd; ++d)
+                eq = eq && g.ng[d] == p.ng[d] && __double_as_longlong(g.ming[d]) == __double_as_longlong(p.ming[d]);
+            if (!eq) atomicAnd(&same, 0);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < a.ninst; k += blockDim.x) a.prev[k] = a.gi[k];
+        if (threadIdx.x == 0) {
+            a.keep[1] = same;
+            a.keep[0] = 1;
+        }
+    }
 }
 
 void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s) {
@@ -827,17 +848,19 @@ __device__ __forceinline__ bool cell_flat(const double* __restrict__ x, int64_t 
     return true;
 }
 
-__global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
-                             const int64_t* count, const GridInst* __restrict__ gi, int32_t* __restrict__ hist,
-                             int64_t cells_cap, int* err, unsigned long long* incons, const int* skip) {
-    if (skip && *skip) return;
+// Blocks bid, bid + nblocks, ... of a grid-stride pass over the particles.
+__device__ __forceinline__ void grid_count_blocks(const double* __restrict__ x, int64_t N, int nd,
+                                                  const int32_t* __restrict__ inst_of, const int64_t* count,
+                                                  const GridInst* __restrict__ gi, int32_t* __restrict__ hist,
+                                                  int64_t cells_cap, int* err, unsigned long long* incons,
+                                                  int64_t bid, int64_t nblocks) {
     int64_t n = count ? *count : N;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     // whole warps iterate together (warp-aggregated histogram; the previous
     // particle's cell comes from the neighbouring lane)
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {
+    const int64_t stride = nblocks * blockDim.x;
+    for (int64_t g0 = bid * blockDim.x; g0 < n; g0 += stride) {
         const int64_t g = g0 + threadIdx.x;
         bool valid = g < n;
         int k = -1;
@@ -869,6 +892,13 @@ __global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, co
     }
 }
 
+__global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
+                             const int64_t* count, const GridInst* __restrict__ gi, int32_t* __restrict__ hist,
+                             int64_t cells_cap, int* err, unsigned long long* incons, const int* skip) {
+    if (skip && *skip) return;
+    grid_count_blocks(x, N, nd, inst_of, count, gi, hist, cells_cap, err, incons, blockIdx.x, gridDim.x);
+}
+
 void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_of, const int64_t* count,
                        const GridInst* gi, int32_t* hist, int64_t cells_cap, int* err, unsigned long long* incons,
                        cudaStream_t s, const int* skip) {
@@ -877,34 +907,90 @@ void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_o
     COUNTED(1);
 }
 
-// Does every instance's grid of an interaction equal the one its CSR was
-// last counted on?  state[0]: that CSR is current for prev; state[1]
-// (output): equal, so the count and scan of this step may be skipped.  prev
-// takes this step's geometry.
-__global__ void k_grid_keep(const GridInst* __restrict__ gi, GridInst* __restrict__ prev, int ninst, int nd,
-                            int* state) {
-    __shared__ int same;
-    if (threadIdx.x == 0) same = state[0];
-    __syncthreads();
-    for (int k = threadIdx.x; k < ninst; k += blockDim.x) {
-        const GridInst& a = gi[k];
-        const GridInst& b = prev[k];
-        bool eq = a.cellbase == b.cellbase && a.ncells == b.ncells;
-        for (int d = 0; d < nd; ++d)
-            eq = eq && a.ng[d] == b.ng[d] && __double_as_longlong(a.ming[d]) == __double_as_longlong(b.ming[d]);
-        if (!eq) atomicAnd(&same, 0);
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < ninst; k += blockDim.x) prev[k] = gi[k];
-    if (threadIdx.x == 0) {
-        state[1] = same;
-        state[0] = 1;
+// ------------------------------------------------ still grids, batched
+// Every interaction whose system_b does not move recounts its CSR only when
+// its grid's geometry changed (keep[1], set by the plan).  Their counts and
+// scans run as one launch each over a table of interactions (blockIdx.y),
+// with a few blocks per interaction striding over the work: on the usual
+// step every block returns at once, and separate launches of one block per
+// tile would cost more in launch latency than the work they skip.
+int64_t still_hist_elems(int64_t cells) { return cells + (cells + SCAN_TILE - 1) / SCAN_TILE + 1; }
+
+__global__ void k_still_count(const __grid_constant__ StillGridArgs a) {
+    const StillGrid& g = a.g[blockIdx.y];
+    if (g.keep[1]) return;
+    grid_count_blocks(g.x, g.N, a.nd, g.inst_of, nullptr, g.gi, g.hist, g.cells, a.err, a.incons, blockIdx.x,
+                      gridDim.x);
+}
+
+// Tile sums of each histogram, after its cells.
+__global__ void k_still_scan_reduce(const __grid_constant__ StillGridArgs a) {
+    const StillGrid& g = a.g[blockIdx.y];
+    if (g.keep[1]) return;
+    const int64_t nb = (g.cells + SCAN_TILE - 1) / SCAN_TILE;
+    int32_t* bsum = g.hist + g.cells;
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const int64_t t0 = b * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
+        int32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_I; ++k)
+            if (t0 + k < g.cells) s += g.hist[t0 + k];
+        int32_t total;
+        (void)block_excl_scan(s, &total);
+        if (threadIdx.x == 0) bsum[b] = total;
     }
 }
 
-void launch_grid_keep(const GridInst* gi, GridInst* prev, int ninst, int nd, int* state, cudaStream_t s) {
-    k_grid_keep<<<1, 128, 0, s>>>(gi, prev, ninst, nd, state);
-    COUNTED(1);
+// Exclusive scan of each histogram into its CSR (cells + 1 entries), the
+// histogram cleared as it is read; each tile adds up the sums before it.
+__global__ void k_still_scan_apply(const __grid_constant__ StillGridArgs a) {
+    const StillGrid& g = a.g[blockIdx.y];
+    if (g.keep[1]) return;
+    const int64_t n = g.cells;
+    const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    const int32_t* bsum = g.hist + n;
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        int32_t off;
+        {
+            int32_t s = 0;
+            for (int64_t t = threadIdx.x; t < b; t += blockDim.x) s += bsum[t];
+            (void)block_excl_scan(s, &off);
+        }
+        const int64_t t0 = b * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
+        int32_t v[SCAN_I];
+        int32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_I; ++k) {
+            v[k] = t0 + k < n ? g.hist[t0 + k] : 0;
+            sum += v[k];
+        }
+#pragma unroll
+        for (int k = 0; k < SCAN_I; ++k)
+            if (t0 + k < n) g.hist[t0 + k] = 0;
+        int32_t total;
+        int32_t run = block_excl_scan(sum, &total) + off;
+#pragma unroll
+        for (int k = 0; k < SCAN_I; ++k) {
+            if (t0 + k < n) g.cs[t0 + k] = run;
+            run += v[k];
+        }
+        if (b == nb - 1 && threadIdx.x == 0) g.cs[n] = off + total;
+    }
+}
+
+void launch_still_grids(const StillGridArgs& a, cudaStream_t s) {
+    if (a.n <= 0) return;
+    int64_t maxN = 1, maxnb = 1;
+    for (int i = 0; i < a.n; ++i) {
+        maxN = std::max(maxN, a.g[i].N);
+        maxnb = std::max(maxnb, (a.g[i].cells + SCAN_TILE - 1) / SCAN_TILE);
+    }
+    const unsigned bc = (unsigned)std::min<int64_t>(nblk(maxN), 2 * 148);
+    const unsigned bs = (unsigned)std::min<int64_t>(maxnb, 148);
+    k_still_count<<<dim3(bc, a.n), TPB, 0, s>>>(a);
+    k_still_scan_reduce<<<dim3(bs, a.n), SCAN_T, 0, s>>>(a);
+    k_still_scan_apply<<<dim3(bs, a.n), SCAN_T, 0, s>>>(a);
+    COUNTED(3);
 }
 
 // ================================================================ ghosts

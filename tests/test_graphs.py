@@ -125,8 +125,9 @@ def _passing_block():
 def test_still_wall_grid_follows_geometry_changes(graphs, profiling):
     """The CSR over a wall that never moves is kept on the device while its
     grid's geometry is unchanged and recounted when it changes (in captured
-    steps through a conditional graph node that the device switches): the
-    device stays with the oracle while the block slides past the wall's end.
+    steps the batched count and scan return at once on a flag the step's
+    plan sets): the device stays with the oracle while the block slides past
+    the wall's end.
     With sweep timing on, the captured step also holds event nodes."""
     out, sessions = [], []
     for be in ("cuda", "oracle"):
