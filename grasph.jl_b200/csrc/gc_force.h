@@ -16,7 +16,7 @@ constexpr int FORCE_BUF = 64;   // staged-neighbour column of the counting sweep
 // (system, stage) by the tuner in gc_context.cu.
 struct ForceCfg {
     int minb, buf, unroll;
-    int stg;  // > 0: k_sweep_stg with chunks of stg candidates (FP32-compensated records)
+    int stg;  // > 0: k_sweep_stg with chunks of stg candidates (policies that stage copies; k_sweep otherwise)
 };
 constexpr int NUM_FORCE_CFG = GC_NUM_SWEEP_CONFIGS;
 constexpr ForceCfg FORCE_CFGS[NUM_FORCE_CFG] = {{4, 64, 1, 0}, {6, 64, 1, 0}, {5, 64, 1, 96}, {6, 64, 1, 96}};

@@ -106,17 +106,51 @@ struct Acc {
     double w[ND == 2 ? 1 : 3];
 };
 
-// One staged candidate j of reference r for owned particle i: the exact
-// reference test r² < (2h)² (src/Interaction.jl:546-548) on the FP64
+// Neighbour j's FP64 state, read from system_b's planar arrays ...
+struct NbGlobal {
+    const InterRef& r;
+    int64_t j;
+    __device__ __forceinline__ double x(int d) const { return r.bx[d * r.bN + j]; }
+    __device__ __forceinline__ double v(int d) const { return r.bv[d * r.bN + j]; }
+    __device__ __forceinline__ double rho() const { return r.brho[j]; }
+    __device__ __forceinline__ double aux() const { return r.baux[j]; }
+    __device__ __forceinline__ double p() const { return r.bp[j]; }
+    __device__ __forceinline__ double stress(int q) const { return r.bstress[q * r.bN + j]; }
+};
+
+// ... or from its copy staged in shared memory by PhysF64::issue: 16-byte
+// chunks q*BT of the slot, the position's components in pairs, then
+// [v, ρ, aux, p] in pairs (the functors staged there read no stress).
+template <int ND>
+struct NbSlot {
+    static constexpr int XQ = (ND + 1) / 2;
+    const float4* slot;
+    int BT;
+    __device__ __forceinline__ double x(int d) const {
+        return reinterpret_cast<const double*>(&slot[(d >> 1) * BT])[d & 1];
+    }
+    __device__ __forceinline__ double rec(int e) const {
+        return reinterpret_cast<const double*>(&slot[(XQ + (e >> 1)) * BT])[e & 1];
+    }
+    __device__ __forceinline__ double v(int d) const { return rec(d); }
+    __device__ __forceinline__ double rho() const { return rec(ND); }
+    __device__ __forceinline__ double aux() const { return rec(ND + 1); }
+    __device__ __forceinline__ double p() const { return rec(ND + 2); }
+    __device__ __forceinline__ double stress(int) const { return 0.0; }
+};
+
+// One candidate j (source nb) of reference r for owned particle i: the
+// exact reference test r² < (2h)² (src/Interaction.jl:546-548) on the FP64
 // positions, then the functor's i-side term.  Returns 1 when accepted.
-template <int ND, int NS, int PFN, int KK>
+// BTK: the system_b kind when known at compile time (-1: r.btype).
+template <int ND, int NS, int PFN, int KK, int BTK = -1, class Nb>
 __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                             const PfnInst& P, int64_t gi, int k, const OwnState<ND>& o,
-                                            const double* osig, double da, int32_t j, Acc<ND, NS>& acc) {
-    const int64_t Nb = r.bN;
+                                            const double* osig, double da, const Nb& nb, Acc<ND, NS>& acc) {
+    const int btype = BTK >= 0 ? BTK : r.btype;
     double dx[ND];
 #pragma unroll
-    for (int d = 0; d < ND; ++d) dx[d] = o.x[d] - r.bx[d * Nb + j];
+    for (int d = 0; d < ND; ++d) dx[d] = o.x[d] - nb.x(d);
     double rr = dotv<ND>(dx, dx);
     if (!(rr < G.cutoff_sq)) return 0;
     if (PFN == GC_PFN_COUNT) {
@@ -129,15 +163,15 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         // src/PairwiseFunctors.jl:424-428 from the virtual particle's side:
         // kw = w·(m_a/ρ_a[i]); f[j] += kw·f_a[i]; w_sum[j] += kw
         const double q = sqrt(rr) / G.H;
-        const double kw = kernel_w<KK>(G.knorm, q) * (G.bmass / r.brho[j]);
+        const double kw = kernel_w<KK>(G.knorm, q) * (G.bmass / nb.rho());
         if (A.imask & (1 << GC_FIELD_V)) {
 #pragma unroll
-            for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + kw * r.bv[d * Nb + j];
+            for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + kw * nb.v(d);
         }
-        if (A.imask & (1 << GC_FIELD_RHO)) acc.dr = acc.dr + kw * r.brho[j];
+        if (A.imask & (1 << GC_FIELD_RHO)) acc.dr = acc.dr + kw * nb.rho();
         if (A.imask & (1 << GC_FIELD_STRESS)) {
 #pragma unroll
-            for (int q2 = 0; q2 < NS; ++q2) acc.sr[q2] = acc.sr[q2] + kw * r.bstress[q2 * Nb + j];
+            for (int q2 = 0; q2 < NS; ++q2) acc.sr[q2] = acc.sr[q2] + kw * nb.stress(q2);
         }
         if (A.iwsum) acc.w[0] = acc.w[0] + (A.iwsum == 2 ? 1.0 : kw);  // 2: NeighborCountFn's count
         return 1;
@@ -150,11 +184,11 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         // the system_b side is this same term with the roles swapped.
         const double q = sqrt(rr) / G.H;
         const double wk = kernel_w<KK>(G.knorm, q);
-        const double den = o.rho + r.brho[j];
-        const double mj = r.btype == BT_SELF ? A.a_mass[k] : G.bmass;
+        const double den = o.rho + nb.rho();
+        const double mj = btype == BT_SELF ? A.a_mass[k] : G.bmass;
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
-            const double du = (((-P.alpha) * (o.v[d] - r.bv[d * Nb + j])) * wk) / den;
+            const double du = (((-P.alpha) * (o.v[d] - nb.v(d))) * wk) / den;
             acc.dv[d] = acc.dv[d] + du * mj;
         }
         return 1;
@@ -164,11 +198,11 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
     const double ca = A.a_c[k];
     const double mass_a = A.a_mass[k];
 
-    if (r.btype == BT_DYNAMIC) {
+    if (btype == BT_DYNAMIC) {
         // src/PairwiseFunctors.jl:53,111,222,334
         double t[ND];
 #pragma unroll
-        for (int d = 0; d < ND; ++d) t[d] = r.bx[d * Nb + j] - G.point[d];
+        for (int d = 0; d < ND; ++d) t[d] = nb.x(d) - G.point[d];
         double db = dotv<ND>(t, G.normal);
         double m = -jmin(G.beta, fabs(db / da));
         double vj[ND];
@@ -222,10 +256,10 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
     // neighbour state
     double vj[ND];
 #pragma unroll
-    for (int d = 0; d < ND; ++d) vj[d] = r.bv[d * Nb + j];
-    const double rhoj = r.brho[j];
+    for (int d = 0; d < ND; ++d) vj[d] = nb.v(d);
+    const double rhoj = nb.rho();
 
-    if (r.btype == BT_STATIC && (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID)) {
+    if (btype == BT_STATIC && (fluid_pfn<PFN>() || PFN == GC_PFN_CAUCHY_FLUID)) {
         // src/PairwiseFunctors.jl:210-219, :322-331
         double dv[ND];
 #pragma unroll
@@ -251,22 +285,22 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
             // FluidSolidPfn :494-519: the fluid's pressure on both sides; the
             // fluid is the neighbour on the system_b side
             if (G.side_b) {
-                const double pf = r.bp[j];
-                dh = P.S == 1 ? -(pf + pf) / (o.rho * rhoj) : -(r.baux[j] + pf / (o.rho * o.rho));
+                const double pf = nb.p();
+                dh = P.S == 1 ? -(pf + pf) / (o.rho * rhoj) : -(nb.aux() + pf / (o.rho * o.rho));
             } else {
                 const double pf = A.a_p[gi];
                 dh = P.S == 1 ? -(pf + pf) / (o.rho * rhoj) : -(o.aux + pf / (rhoj * rhoj));
             }
         } else {
-            dh = P.S == 1 ? -(A.a_p[gi] + r.bp[j]) / (o.rho * rhoj) : -(o.aux + r.baux[j]);
+            dh = P.S == 1 ? -(A.a_p[gi] + nb.p()) / (o.rho * rhoj) : -(o.aux + nb.aux());
         }
-        double mj = r.btype == BT_SELF ? mass_a : G.bmass;
+        double mj = btype == BT_SELF ? mass_a : G.bmass;
         if (two) {
             // dv_tmp = (dh + ast - piv)·gx, then mass_j·dv_tmp; the system_b side
             // runs this same code with the roles swapped (every factor is
             // symmetric or flips sign exactly with dx, dv and gx)
             double c = dh;
-            if (P.has_eps) c = c + P.eps * (-(fabs(A.a_p[gi]) + fabs(r.bp[j])) / (o.rho * rhoj));
+            if (P.has_eps) c = c + P.eps * (-(fabs(A.a_p[gi]) + fabs(nb.p())) / (o.rho * rhoj));
             c = c - piv;
 #pragma unroll
             for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + mj * (c * gx[d]);
@@ -290,14 +324,14 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         double dv[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) dv[d] = o.v[d] - vj[d];
-        const bool self = r.btype == BT_SELF;
+        const bool self = btype == BT_SELF;
         double cb = self ? ca : G.bc;
         double piv = art_visc<ND>(dx, dv, rr, P.h, o.rho, rhoj, P.alpha, P.beta, ca, cb);
         double sj[NS > 0 ? NS : 1];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) sj[q] = r.bstress[q * Nb + j];
+        for (int q = 0; q < NS; ++q) sj[q] = nb.stress(q);
         double hv[ND];
-        cauchy_f<ND, NS>(osig, sj, o.aux, r.baux[j], gx, hv);
+        cauchy_f<ND, NS>(osig, sj, o.aux, nb.aux(), gx, hv);
         double mj = self ? mass_a : G.bmass;
 #pragma unroll
         for (int d = 0; d < ND; ++d) acc.dv[d] = acc.dv[d] + mj * (hv[d] - piv * gx[d]);
@@ -317,7 +351,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         for (int d = 0; d < ND; ++d) dv[d] = vj[d] - o.v[d];
         double sr[NS > 0 ? NS : 1];
         strain_rate_f<ND, NS>(dv, gx, sr);
-        const double f = r.baux[j];  // mass_j / rho_j
+        const double f = nb.aux();  // mass_j / rho_j
 #pragma unroll
         for (int q = 0; q < NS; ++q) acc.sr[q] = acc.sr[q] + sr[q] * f;
         if (PFN == GC_PFN_STRAIN_RATE_VORTICITY) {
@@ -339,7 +373,6 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
 
 template <int ND, int NS, int PFN, int KK>
 struct PhysF64 {
-    static constexpr int NQ = 0;  // no staged copies (k_sweep only)
     static constexpr bool BLOCKED = false;  // plain FP64 sums: nothing to merge at strip ends
     struct Own {
         OwnState<ND> o;
@@ -441,7 +474,40 @@ struct PhysF64 {
     static __device__ __forceinline__ int pair(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                const PfnInst& P, int64_t gi, int k, const Own& w, double da,
                                                int32_t j, AccT& acc) {
-        return process_pair<ND, NS, P2, KK>(A, r, G, P, gi, k, w.o, w.sig, da, j, acc);
+        return process_pair<ND, NS, P2, KK>(A, r, G, P, gi, k, w.o, w.sig, da, NbGlobal{r, j}, acc);
+    }
+
+    // Chunk staging (k_sweep_stg) for the fluid functors: a neighbour's FP64
+    // position, then its [v, ρ, aux, p] (NbSlot's layout), copied from the
+    // planar arrays by 8-byte asynchronous copies; a dynamic boundary's
+    // term reads only the position, and p is copied only for the functor
+    // forms that read it.  The pair terms are the same expression trees on
+    // the same values as k_sweep's, so both kernels give the same bits.
+    static constexpr int NQP = (ND + 1) / 2, NQR = 3;
+    static constexpr int NQ = fluid_pfn<PFN>() ? NQP + NQR : 0;
+    static __device__ __forceinline__ void issue(const InterRef& r, const PfnInst& P, int32_t j, float4* slot,
+                                                 int BT) {
+        auto cp = [&](int e, const double* src) {  // double e of the slot
+            __pipeline_memcpy_async(reinterpret_cast<double*>(&slot[(e >> 1) * BT]) + (e & 1), src, 8);
+        };
+        const int64_t N = r.bN;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) cp(d, r.bx + d * N + j);
+        if (r.btype == BT_DYNAMIC) return;
+        constexpr int E = 2 * NQP;  // first double of the record
+#pragma unroll
+        for (int d = 0; d < ND; ++d) cp(E + d, r.bv + d * N + j);
+        cp(E + ND, r.brho + j);
+        if (r.baux) cp(E + ND + 1, r.baux + j);
+        // p: the multiphase pressure form, FluidSolidPfn's fluid side and the
+        // two-sided form's ε term
+        if (P.S == 1 || (PFN == PFN_FLUID2 && (P.fs || P.has_eps))) cp(E + ND + 2, r.bp + j);
+    }
+    template <int P2, int BTK = -1>
+    static __device__ __forceinline__ int pair_slot(const ForceArgs& A, const InterRef& r, const GridInst& G,
+                                                    const PfnInst& P, int64_t gi, int k, const Own& w, double da,
+                                                    const float4* slot, int BT, const float2*, AccT& acc) {
+        return process_pair<ND, NS, P2, KK, BTK>(A, r, G, P, gi, k, w.o, w.sig, da, NbSlot<ND>{slot, BT}, acc);
     }
 };
 
@@ -659,7 +725,8 @@ struct PhysF32 {
     // Copy of a neighbour's position and record into a shared-memory slot
     // (16-byte asynchronous copies), chunk q at slot[q*BT]; pair_slot reads it.
     static constexpr int NQP = XD / 2, NQR = R / 4, NQ = NQP + NQR;
-    static __device__ __forceinline__ void issue(const InterRef& r, int32_t j, float4* slot, int BT) {
+    static __device__ __forceinline__ void issue(const InterRef& r, const PfnInst&, int32_t j, float4* slot,
+                                                 int BT) {
         const float4* px = reinterpret_cast<const float4*>(r.bxp + (int64_t)j * XD);
 #pragma unroll
         for (int q = 0; q < NQP; ++q) __pipeline_memcpy_async(&slot[q * BT], &px[q], 16);
@@ -1230,7 +1297,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
             const int nstrips = ND == 2 ? 3 : 9;
             warp_copy(gsm, G, lane);
             warp_copy(psm, P, lane);
-            if (lane == 0) *camsm = make_float2(A.a_cf[k], A.a_massf[k]);
+            if (lane == 0 && A.a_cf) *camsm = make_float2(A.a_cf[k], A.a_massf[k]);
             __syncwarp();
             const GridInst& Gs = *gsm;
             const PfnInst& Ps = *psm;
@@ -1275,7 +1342,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                         const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
                         for (int32_t ch = u0; ch < u1; ch += CH) {
                             const int n = u1 - ch < CH ? (int)(u1 - ch) : CH;
-                            for (int i = lane; i < n; i += 32) Phys::issue(r, ch + i, slots + i, CH);
+                            for (int i = lane; i < n; i += 32) Phys::issue(r, Ps, ch + i, slots + i, CH);
                             __pipeline_commit();
                             __pipeline_wait_prior(0);
                             // this lane's staged positions -> relative FP32 coordinates

@@ -72,10 +72,13 @@ def test_capacity_overflow_rolls_back_bit_identical():
     assert st["graph_steps"] > 0
 
 
+@pytest.mark.parametrize("case", ["column", "dambreak_2d", "dambreak_3d"])
 @pytest.mark.parametrize("prec", [G.PRECISION_FP64, G.PRECISION_FP32_COMPENSATED])
-def test_sweep_configs_bit_identical(prec):
-    """Every launch configuration the autotuner picks from gives the same bits."""
-    builder, kw = CASES["column"]
+def test_sweep_configs_bit_identical(prec, case):
+    """Every launch configuration the autotuner picks from gives the same
+    bits: buffered and chunk-staged sweeps, for the stress functors of the
+    column and the fluid functors of the dam breaks (walls included)."""
+    builder, kw = CASES[case]
     ref = None
     for cfg in range(G.consts.GC_NUM_SWEEP_CONFIGS):
         lf, meta = builder(**kw)
