@@ -188,6 +188,14 @@ void scan_exclusive_clear(int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cu
     scan_impl(in, out, n, tmp, in, s, skip);
 }
 
+// Particle g's coordinates, every load issued before any value is used
+// (a loop over a run-time dimension count would otherwise wait out one
+// memory round trip per coordinate).
+__device__ __forceinline__ void load_pos(const double* __restrict__ x, int64_t N, int64_t g, int nd, double* v) {
+#pragma unroll
+    for (int d = 0; d < MAXD; ++d) v[d] = d < nd ? x[d * N + g] : 0.0;
+}
+
 // ========================================================== bounding box
 __global__ void k_bbox_reset(unsigned long long* scratch, int ninst) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -296,6 +304,8 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
          tile < (int64_t)(blockIdx.x + 1) * tiles_per_block && tile * blockDim.x < n; ++tile) {
         const int64_t g = tile * blockDim.x + threadIdx.x;
         if (g >= n) continue;
+        double xv[MAXD];
+        load_pos(x, N, g, nd, xv);
         const int k = inst_of[g];
         if (k != krun) {
             if (krun >= 0)
@@ -310,7 +320,7 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
             }
         }
         for (int d = 0; d < nd; ++d) {
-            const double v = x[d * N + g];
+            const double v = xv[d];
             if (!isfinite(v)) bad = true;
             const unsigned long long key = ord_key(v);
             amn[d] = key < amn[d] ? key : amn[d];
@@ -437,12 +447,14 @@ void launch_sort_plan(SysInst* inst, int ninst, int nd, int64_t* need, int* err,
 __device__ __forceinline__ int32_t sort_key_of(const double* __restrict__ x, int64_t N, int nd,
                                                const int32_t* __restrict__ inst_of, const SysInst* __restrict__ inst,
                                                int64_t g, int64_t cells_cap, int* bad) {
+    double xv[MAXD];
+    load_pos(x, N, g, nd, xv);
     const SysInst& S = inst[inst_of[g]];
     int64_t flat = 0;
     bool ok = true;
     for (int d = 0; d < nd; ++d) {
         int64_t kd;
-        if (!floor_i64(x[d * N + g] / S.sort_cutoff, &kd)) {
+        if (!floor_i64(xv[d] / S.sort_cutoff, &kd)) {
             ok = false;
             break;
         }
@@ -837,10 +849,12 @@ void launch_grid_plan(const GridPlanArgs& a, cudaStream_t s) {
 
 __device__ __forceinline__ bool cell_flat(const double* __restrict__ x, int64_t N, int64_t g, int nd,
                                           const GridInst& G, int64_t* flat) {
+    double xv[MAXD];
+    load_pos(x, N, g, nd, xv);
     int64_t f = 0;
     for (int d = 0; d < nd; ++d) {
         int64_t cd;
-        if (!floor_i64((x[d * N + g] - G.ming[d]) / G.cell, &cd)) return false;
+        if (!floor_i64((xv[d] - G.ming[d]) / G.cell, &cd)) return false;
         if (cd < 0 || cd >= G.ng[d]) return false;
         f = f * G.ng[d] + cd;
     }
