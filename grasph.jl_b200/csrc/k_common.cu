@@ -697,22 +697,40 @@ __global__ void k_gather_fields(GatherArgs a, int64_t N, const int32_t* __restri
     // the sort's order flag, read by the scatter and fix-up launched
     // before this gather, is cleared for the next sort
     if (a.clear && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *a.clear = 0;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
-        int64_t o = perm[g];
-        if ((uint64_t)o >= (uint64_t)N) o = g;
+    // two elements per thread (g and g + blockDim.x), their loads issued
+    // together
+    const int64_t step = (int64_t)gridDim.x * blockDim.x * 2;
+    for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x * 2 + threadIdx.x; g0 < n; g0 += step) {
+        int64_t gs[2] = {g0, g0 + blockDim.x};
+        int64_t o[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            o[e] = gs[e] < n ? perm[gs[e]] : gs[e];
+            if ((uint64_t)o[e] >= (uint64_t)N) o[e] = gs[e];
+        }
         if (f < a.nf) {
             const double* __restrict__ src = a.src[f];
             double* __restrict__ dst = a.dst[f];
             const int nc = a.ncomp[f];
-            double v[MAXS];
+            double v[2][MAXS];
 #pragma unroll
-            for (int c = 0; c < MAXS; ++c)
-                if (c < nc) v[c] = __ldg(src + c * N + o);
+            for (int e = 0; e < 2; ++e)
 #pragma unroll
-            for (int c = 0; c < MAXS; ++c)
-                if (c < nc) dst[c * N + g] = v[c];
+                for (int c = 0; c < MAXS; ++c)
+                    if (c < nc && gs[e] < n) v[e][c] = __ldg(src + c * N + o[e]);
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+#pragma unroll
+                for (int c = 0; c < MAXS; ++c)
+                    if (c < nc && gs[e] < n) dst[c * N + gs[e]] = v[e][c];
         } else {
-            a.idst[f - a.nf][g] = __ldg(a.isrc[f - a.nf] + o);
+            int32_t iv[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+                if (gs[e] < n) iv[e] = __ldg(a.isrc[f - a.nf] + o[e]);
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+                if (gs[e] < n) a.idst[f - a.nf][gs[e]] = iv[e];
         }
     }
 }
@@ -720,7 +738,7 @@ __global__ void k_gather_fields(GatherArgs a, int64_t N, const int32_t* __restri
 void launch_gather_fields(const GatherArgs& a, int64_t N, const int32_t* perm, const int64_t* count,
                           cudaStream_t s) {
     if (N <= 0 || (a.nf == 0 && a.ni == 0)) return;
-    dim3 grid((unsigned)nblk(N), (unsigned)(a.nf + a.ni));
+    dim3 grid((unsigned)nblk((N + 1) / 2), (unsigned)(a.nf + a.ni));
     k_gather_fields<<<grid, TPB, 0, s>>>(a, N, perm, count);
     COUNTED(1);
 }

@@ -19,18 +19,29 @@ static inline int ublk(int64_t n) {
 }
 
 // src/TimeIntegration.jl:158 (_halfstep_ps!) with the q0 snapshot of :220.
+// Every load comes before the first store: the fields are separate arrays,
+// but the compiler cannot know that, and would otherwise wait out a memory
+// round trip per component.
 __device__ __forceinline__ void halfstep_one(const StepArgs& a, int64_t g) {
+    double v[MAXD], dv[MAXD];
+#pragma unroll
+    for (int d = 0; d < MAXD; ++d)
+        if (d < a.nd) {
+            v[d] = a.v[d * a.N + g];
+            dv[d] = a.dvdt[d * a.N + g];
+        }
+    const double r = a.rho[g], dr = a.drhodt[g];
     const SysInst& S = a.inst[a.inst_of[g]];
     const double h = S.half_dt;
-    for (int d = 0; d < a.nd; ++d) {
-        double v = a.v[d * a.N + g];
-        a.q0v[d * a.N + g] = v;
-        a.v[d * a.N + g] = v + h * a.dvdt[d * a.N + g];
-        a.dvdt[d * a.N + g] = S.srcv[d];
-    }
-    double r = a.rho[g];
+#pragma unroll
+    for (int d = 0; d < MAXD; ++d)
+        if (d < a.nd) {
+            a.q0v[d * a.N + g] = v[d];
+            a.v[d * a.N + g] = v[d] + h * dv[d];
+            a.dvdt[d * a.N + g] = S.srcv[d];
+        }
     a.q0rho[g] = r;
-    a.rho[g] = fma(h, a.drhodt[g], r);
+    a.rho[g] = fma(h, dr, r);
     a.drhodt[g] = S.srcrho;
 }
 
@@ -52,30 +63,44 @@ __global__ void k_halfstep_fused(StepArgs a, UpdArgs u, PackArgs pk) {
     }
 }
 
-// src/TimeIntegration.jl:673-682: damping, full step, zero XSPH pass, x += dt·v.
+// src/TimeIntegration.jl:673-682: damping, full step, zero XSPH pass, x += dt·v
+// (every load before the first store, as in halfstep_one).
 __global__ void k_fullstep(StepArgs a) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const SysInst& S = a.inst[a.inst_of[g]];
         const double dt = S.dt;
-        for (int d = 0; d < a.nd; ++d) {
-            double dv = a.dvdt[d * a.N + g];
-            if (S.gamma_dt != 0.0) {
-                dv = dv - S.gamma_dt * a.v[d * a.N + g];
+        const bool damp = S.gamma_dt != 0.0;
+        double dvl[MAXD], q0[MAXD], vo[MAXD], xa[MAXD];  // xa: x, or v_adjustment with XSPH
+#pragma unroll
+        for (int d = 0; d < MAXD; ++d)
+            if (d < a.nd) {
+                dvl[d] = a.dvdt[d * a.N + g];
+                q0[d] = a.q0v[d * a.N + g];
+                vo[d] = damp ? a.v[d * a.N + g] : 0.0;
+                xa[d] = a.vadj ? a.vadj[d * a.N + g] : a.x[d * a.N + g];
+            }
+        const double q0r = a.q0rho[g], dr = a.drhodt[g];
+#pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= a.nd) continue;
+            double dv = dvl[d];
+            if (damp) {
+                dv = dv - S.gamma_dt * vo[d];
                 a.dvdt[d * a.N + g] = dv;
             }
-            double v = a.q0v[d * a.N + g] + dt * dv;
+            double v = q0[d] + dt * dv;
             if (a.vadj) {
                 // XSPH correction first half; positions move after the sweeps
-                v = v + (-1.0 * a.vadj[d * a.N + g]);
+                v = v + (-1.0 * xa[d]);
                 a.vadj[d * a.N + g] = 0.0;
                 a.v[d * a.N + g] = v;
             } else {
                 v = (v + (-1.0 * 0.0)) + 1.0 * 0.0;
                 a.v[d * a.N + g] = v;
-                a.x[d * a.N + g] = a.x[d * a.N + g] + dt * v;
+                a.x[d * a.N + g] = xa[d] + dt * v;
             }
         }
-        a.rho[g] = fma(dt, a.drhodt[g], a.q0rho[g]);
+        a.rho[g] = fma(dt, dr, q0r);
     }
 }
 
