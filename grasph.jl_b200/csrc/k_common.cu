@@ -309,7 +309,9 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
         const int k = inst_of[g];
         if (k != krun) {
             if (krun >= 0)
-                for (int d = 0; d < nd; ++d) {
+                #pragma unroll
+                for (int d = 0; d < MAXD; ++d) {
+                    if (d >= nd) break;
                     atomicMin(&scratch[(krun * 2 + 0) * MAXD + d], amn[d]);
                     atomicMax(&scratch[(krun * 2 + 1) * MAXD + d], amx[d]);
                 }
@@ -319,7 +321,9 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
                 amx[d] = 0ull;
             }
         }
-        for (int d = 0; d < nd; ++d) {
+        #pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= nd) break;
             const double v = xv[d];
             if (!isfinite(v)) bad = true;
             const unsigned long long key = ord_key(v);
@@ -337,7 +341,9 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
     if (uniform && k0 >= 0) {
         __shared__ unsigned long long smn[TPB / 32][MAXD], smx[TPB / 32][MAXD];
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        for (int d = 0; d < nd; ++d) {
+        #pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= nd) break;
             unsigned long long a = amn[d], b = amx[d];
             for (int o = 16; o > 0; o >>= 1) {
                 unsigned long long a2 = __shfl_down_sync(0xffffffffu, a, o);
@@ -362,7 +368,9 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
             atomicMax(&scratch[(k0 * 2 + 1) * MAXD + d], b);
         }
     } else if (krun >= 0) {
-        for (int d = 0; d < nd; ++d) {
+        #pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= nd) break;
             atomicMin(&scratch[(krun * 2 + 0) * MAXD + d], amn[d]);
             atomicMax(&scratch[(krun * 2 + 1) * MAXD + d], amx[d]);
         }
@@ -376,7 +384,9 @@ __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, co
     if (!last) return;
     __threadfence();
     for (int k = threadIdx.x; k < ninst; k += blockDim.x) {
-        for (int d = 0; d < nd; ++d) {
+        #pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= nd) break;
             unsigned long long a = atomicExch(&scratch[(k * 2 + 0) * MAXD + d], ~0ull);
             unsigned long long b = atomicExch(&scratch[(k * 2 + 1) * MAXD + d], 0ull);
             inst[k].bbmin[d] = a == ~0ull ? 0.0 : ord_val(a);
@@ -452,7 +462,9 @@ __device__ __forceinline__ int32_t sort_key_of(const double* __restrict__ x, int
     const SysInst& S = inst[inst_of[g]];
     int64_t flat = 0;
     bool ok = true;
-    for (int d = 0; d < nd; ++d) {
+    #pragma unroll
+    for (int d = 0; d < MAXD; ++d) {
+        if (d >= nd) break;
         int64_t kd;
         if (!floor_i64(xv[d] / S.sort_cutoff, &kd)) {
             ok = false;
@@ -775,7 +787,9 @@ __device__ void grid_plan_block(const GridPlanArgs& a) {
         GridInst& G = a.gi[k];
         const SysInst& A = a.a[k];
         double mn[MAXD], mx[MAXD];
-        for (int d = 0; d < a.nd; ++d) {
+        #pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= a.nd) break;
             mn[d] = A.bbmin[d];
             mx[d] = A.bbmax[d];
             G.mina[d] = mn[d];
@@ -784,14 +798,18 @@ __device__ void grid_plan_block(const GridPlanArgs& a) {
         if (a.b) {
             const SysInst& B = a.b[k];
             if (B.n > 0)
-                for (int d = 0; d < a.nd; ++d) {
+                #pragma unroll
+                for (int d = 0; d < MAXD; ++d) {
+                    if (d >= a.nd) break;
                     mn[d] = jmin(mn[d], B.bbmin[d]);
                     mx[d] = jmax(mx[d], B.bbmax[d]);
                 }
         }
         const double c = G.cell;
         int64_t cells = 1;
-        for (int d = 0; d < a.nd; ++d) {
+        #pragma unroll
+        for (int d = 0; d < MAXD; ++d) {
+            if (d >= a.nd) break;
             double raw = mn[d] - 2.0 * c;
             G.ming[d] = floor(raw / c) * c;
             double maxg = mx[d] + 2.0 * c;
@@ -870,7 +888,9 @@ __device__ __forceinline__ bool cell_flat(const double* __restrict__ x, int64_t 
     double xv[MAXD];
     load_pos(x, N, g, nd, xv);
     int64_t f = 0;
-    for (int d = 0; d < nd; ++d) {
+    #pragma unroll
+    for (int d = 0; d < MAXD; ++d) {
+        if (d >= nd) break;
         int64_t cd;
         if (!floor_i64((xv[d] - G.ming[d]) / G.cell, &cd)) return false;
         if (cd < 0 || cd >= G.ng[d]) return false;
@@ -1148,10 +1168,14 @@ __global__ void k_ghost_copy(int64_t cap, const int64_t* count, int nd, int ns, 
             dst[k] = src[o];
             continue;
         }
+        // loops over the compile-time bound keep sg and out in registers
         double sg[MAXS];
-        for (int q = 0; q < ns; ++q) sg[q] = src[q * Nsrc + o];
+#pragma unroll
+        for (int q = 0; q < MAXS; ++q) sg[q] = q < ns ? src[q * Nsrc + o] : 0.0;
         if (mode != GC_COPY_HOUSEHOLDER) {
-            for (int q = 0; q < ns; ++q) dst[q * cap + k] = sg[q];
+#pragma unroll
+            for (int q = 0; q < MAXS; ++q)
+                if (q < ns) dst[q * cap + k] = sg[q];
             continue;
         }
         double out[MAXS];
@@ -1178,7 +1202,9 @@ __global__ void k_ghost_copy(int64_t cap, const int64_t* count, int nd, int ns, 
             out[4] = sg[4] - 2.0 * (tx * nz + nx * tz) + 4.0 * sc * nx * nz;
             out[5] = sg[5] - 2.0 * (ty * nz + ny * tz) + 4.0 * sc * ny * nz;
         }
-        for (int q = 0; q < ns; ++q) dst[q * cap + k] = out[q];
+#pragma unroll
+        for (int q = 0; q < MAXS; ++q)
+            if (q < ns) dst[q * cap + k] = out[q];
         (void)nd;
     }
 }
