@@ -983,29 +983,43 @@ __device__ __forceinline__ void warp_zrange(const int32_t* c, bool active, int32
 // Conservative FP32 prefilter of a batch of mb <= 32 candidates against this
 // lane (coordinates relative to lane 0; rows of the batch `stride` floats
 // apart, entries past mb far away): bit t set when candidate t may be within
-// the cutoff.  Two candidates per packed FP32x2 instruction.
-template <int ND>
+// the cutoff.  Two candidates per packed FP32x2 instruction.  The chain
+// starts from −cut, so it ends at r² − cut and its sign bit is the hit: one
+// funnel shift per candidate moves it into the mask (candidates pushed from
+// last to first).  A NaN result is not guaranteed a clear sign bit, so the
+// callers mask out inactive lanes.  V4: 16-byte loads of four candidates'
+// coordinates (rows and the base 16-byte aligned).
+template <int ND, bool V4 = false>
 __device__ __forceinline__ unsigned batch_hits(const float* cb, int stride, int mb, const float* xi, float cut_f) {
     const float2 neg1 = make_float2(-1.0f, -1.0f);
+    const float2 ncut = make_float2(-cut_f, -cut_f);
     unsigned hits = 0;
     for (int t0 = 0; t0 < mb; t0 += 8) {
         unsigned h8 = 0;
 #pragma unroll
-        for (int t = 0; t < 8; t += 2) {
-            float2 rr;
-            {
-                const float2 xj = *reinterpret_cast<const float2*>(cb + t0 + t);
-                const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[0], xi[0]));
-                rr = __fmul2_rn(dd, dd);
-            }
+        for (int t = 4; t >= 0; t -= 4) {
+            float2 ra = ncut, rb = ncut;  // candidates t, t+1 and t+2, t+3
 #pragma unroll
-            for (int d = 1; d < ND; ++d) {
-                const float2 xj = *reinterpret_cast<const float2*>(cb + d * stride + t0 + t);
-                const float2 dd = __ffma2_rn(xj, neg1, make_float2(xi[d], xi[d]));
-                rr = __ffma2_rn(dd, dd, rr);
+            for (int d = 0; d < ND; ++d) {
+                const float* row = cb + d * stride + t0 + t;
+                float2 xa, xb;
+                if (V4) {
+                    const float4 q = *reinterpret_cast<const float4*>(row);
+                    xa = make_float2(q.x, q.y);
+                    xb = make_float2(q.z, q.w);
+                } else {
+                    xa = *reinterpret_cast<const float2*>(row);
+                    xb = *reinterpret_cast<const float2*>(row + 2);
+                }
+                const float2 xo = make_float2(xi[d], xi[d]);
+                const float2 da = __ffma2_rn(xa, neg1, xo), db = __ffma2_rn(xb, neg1, xo);
+                ra = __ffma2_rn(da, da, ra);
+                rb = __ffma2_rn(db, db, rb);
             }
-            if (rr.x < cut_f) h8 |= 1u << t;
-            if (rr.y < cut_f) h8 |= 2u << t;
+            h8 = __funnelshift_l(__float_as_uint(rb.y), h8, 1);
+            h8 = __funnelshift_l(__float_as_uint(rb.x), h8, 1);
+            h8 = __funnelshift_l(__float_as_uint(ra.y), h8, 1);
+            h8 = __funnelshift_l(__float_as_uint(ra.x), h8, 1);
         }
         hits |= h8 << t0;
     }
@@ -1134,7 +1148,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                 // Conservative FP32 prefilter in coordinates relative to lane 0:
                 // |rel| spans a few cells, so single-precision rounding moves r²
                 // by < 1e-5 relative; the 1e-3 margin keeps every true pair.
-                // Inactive lanes test against NaN and so accept nothing.
+                // Inactive lanes have an empty own range and accept nothing.
                 // lane 0's position, the origin of the relative coordinates,
                 // kept in the warp's shared memory rather than in registers
                 double* xref = reinterpret_cast<double*>(cand + ND * 32);
@@ -1145,7 +1159,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                 }
                 __syncwarp();
 #pragma unroll
-                for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
+                for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : 0.f;
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
                 const int64_t ngl = G.ng[L];
                 const int nstrips = ND == 2 ? 3 : 9;
@@ -1155,7 +1169,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
                     else colflat = (c0 + sidx / 3 - 1) * G.ng[1] + (c1 + sidx % 3 - 1);
                     const int64_t base = G.cellbase + colflat * ngl;
                     const int32_t u0 = r.cs[base + zlo - 1], u1 = r.cs[base + zhi + 2];
-                    const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
+                    const int32_t lo = active ? r.cs[base + c[L] - 1] : 0, hi = active ? r.cs[base + c[L] + 2] : 0;
                     for (int32_t ch = u0; ch < u1; ch += 32) {
                         if (__any_sync(FULL, nbuf > BUF - 32)) {
                             accepted += flush_all<Phys, COUNT_ONLY, UNROLL, PFN>(A, r, Gs, Ps, gi, k, w, da, nbuf, col,
@@ -1311,10 +1325,10 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                 }
                 __syncwarp();
                 // conservative FP32 prefilter relative to lane 0 (k_sweep's);
-                // inactive lanes test against NaN and accept nothing
+                // inactive lanes have an empty own range and accept nothing
                 float xi[ND];
 #pragma unroll
-                for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : __int_as_float(0x7fffffff);
+                for (int d = 0; d < ND; ++d) xi[d] = active ? (float)(ox[d] - xref[d]) : 0.f;
                 const float cut_f = (float)(G.cutoff_sq * 1.001);
                 const int64_t ngl = G.ng[L];
                 auto strip_base = [&](int s2) -> int64_t {
@@ -1338,8 +1352,9 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                         const int32_t u0 = __shfl_sync(FULL, su0, sidx), u1 = __shfl_sync(FULL, su1, sidx);
                         if (u0 >= u1) continue;  // warp-uniform
                         const int64_t base = strip_base(sidx);
-                        // this lane's own strip range [cs[z-1], cs[z+2])
-                        const int32_t lo = r.cs[base + c[L] - 1], hi = r.cs[base + c[L] + 2];
+                        // this lane's own strip range [cs[z-1], cs[z+2]) (empty when inactive)
+                        const int32_t lo = active ? r.cs[base + c[L] - 1] : 0;
+                        const int32_t hi = active ? r.cs[base + c[L] + 2] : 0;
                         for (int32_t ch = u0; ch < u1; ch += CH) {
                             const int n = u1 - ch < CH ? (int)(u1 - ch) : CH;
                             for (int i = lane; i < n; i += 32) Phys::issue(r, Ps, ch + i, slots + i, CH);
@@ -1367,20 +1382,29 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
                                 msk[b] = 0u;
                                 if (32 * b < n) {
                                     const int mb = n - 32 * b < 32 ? n - 32 * b : 32;
-                                    msk[b] = batch_hits<ND>(cand + 32 * b, CH, mb, xi, cut_f) &
+                                    msk[b] = batch_hits<ND, true>(cand + 32 * b, CH, mb, xi, cut_f) &
                                              own_allow(lo, hi, ch + 32 * b, self, gi);
                                 }
                             }
-                            // this lane's accepted candidates, from the staged copies
+                            // this lane's accepted candidates, from the staged copies, in
+                            // increasing order: msk[0] is the current batch's mask, and an
+                            // empty one shifts the later batches down
+                            int mbase = 0;
                             while (true) {
-                                int t = -1;
+                                if (msk[0] == 0u) {
 #pragma unroll
-                                for (int b = 0; b < NB; ++b)
-                                    if (t < 0 && msk[b]) {
-                                        t = 32 * b + __ffs(msk[b]) - 1;
-                                        msk[b] &= msk[b] - 1;
+                                    for (int s2 = 1; s2 < NB; ++s2) {
+                                        if (msk[0] == 0u) {
+#pragma unroll
+                                            for (int b = 0; b + 1 < NB; ++b) msk[b] = msk[b + 1];
+                                            msk[NB - 1] = 0u;
+                                            mbase += 32;
+                                        }
                                     }
-                                if (t < 0) break;
+                                    if (msk[0] == 0u) break;
+                                }
+                                const int t = mbase + __ffs(msk[0]) - 1;
+                                msk[0] &= msk[0] - 1;
                                 accepted += Phys::template pair_slot<PFN, BTK>(A, r, Gs, Ps, gi, k, w, da, slots + t, CH, camsm, acc);
                             }
                             __syncwarp();  // every lane is done with the chunk before the next one lands
