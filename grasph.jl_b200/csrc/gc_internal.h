@@ -8,6 +8,7 @@
 // Particle indices are int32 (a context holds < 2^31 particles per slot).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -52,19 +53,32 @@ struct GridInst {
     // system_b wrapper parameters (src/BoundaryParticles.jl)
     double normal[MAXD], point[MAXD], beta, ljcut;
     double bmass, bc;                  // system_b mass and sound speed
+    // FP32 copies for the FP32-compensated sweep (1/h and the kernel
+    // normalisation 16-byte aligned: the pair code reads them as one float2)
+    alignas(16) float f_invH;
+    float f_knorm;
+    float f_normal[MAXD], f_beta, f_ljcut, f_bmass, f_bc;
     int side_b;                        // 1 in the system_b-side copy of a two-sided interaction
-    // FP32 copies for the FP32-compensated sweep
-    float f_invH, f_knorm, f_normal[MAXD], f_beta, f_ljcut, f_bmass, f_bc;
 };
+static_assert(offsetof(GridInst, f_invH) % 16 == 0 && offsetof(GridInst, f_knorm) == offsetof(GridInst, f_invH) + 4,
+              "1/h and the kernel normalisation are read as one float2");
 
 // Per (interaction, stage, instance) functor parameters.
 struct PfnInst {
     double alpha, beta, h, delta, eps;
+    // FP32 copies; h2eps = 0.01·h² (the first four 16-byte aligned: the pair
+    // code reads them as one float4)
+    alignas(16) float f_h;
+    float f_h2eps, f_alpha, f_beta;
+    float f_delta, f_eps;
     int S, has_delta, has_eps;
     int two;  // FluidPfn between two fluid systems, or FluidSolidPfn (both sides written)
     int fs;   // FluidSolidPfn: system_a's (the fluid's) pressure on both sides
-    float f_alpha, f_beta, f_h, f_h2eps, f_delta, f_eps;  // FP32 copies; h2eps = 0.01·h²
 };
+static_assert(offsetof(PfnInst, f_h) % 16 == 0 && offsetof(PfnInst, f_h2eps) == offsetof(PfnInst, f_h) + 4 &&
+                  offsetof(PfnInst, f_alpha) == offsetof(PfnInst, f_h) + 8 &&
+                  offsetof(PfnInst, f_beta) == offsetof(PfnInst, f_h) + 12,
+              "h, 0.01·h², α and β are read as one float4");
 
 // Per (virtual system, instance) parameters.
 struct VirtInst {

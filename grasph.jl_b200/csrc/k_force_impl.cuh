@@ -778,8 +778,11 @@ struct PhysF32 {
         const float rrf = (float)rr;
         const float rinv = rsqrtf(rrf);
         const float rf = rrf * rinv;
-        const float q = rf * G.f_invH;
-        const float gc = kernel_dw_dq_f<KK>(G.f_knorm, q) * G.f_invH * rinv;
+        // 1/h and the kernel normalisation; h, 0.01·h², α and β: one vector load each
+        const float2 gk = *reinterpret_cast<const float2*>(&G.f_invH);
+        const float4 pv = *reinterpret_cast<const float4*>(&P.f_h);
+        const float q = rf * gk.x;
+        const float gc = kernel_dw_dq_f<KK>(gk.y, q) * gk.x * rinv;
         float gx[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) gx[d] = gc * dxf[d];
@@ -852,9 +855,9 @@ struct PhysF32 {
             float piv = 0.f;
             const float vr = dotf<ND>(dxf, dv);
             if (vr < 0.f) {
-                const float muv = __fdividef(P.f_h * vr, rrf + P.f_h2eps);
+                const float muv = __fdividef(pv.x * vr, rrf + pv.y);
                 const float mc = 0.5f * (ca + cb);
-                piv = (P.f_beta * muv - P.f_alpha * mc) * muv * 2.f * w.irho * irhoj;
+                piv = (pv.w * muv - pv.z * mc) * muv * 2.f * w.irho * irhoj;
             }
             if (bt == BT_STATIC) {
                 const float x = G.f_ljcut * rinv, x2 = x * x, x6 = x2 * x2 * x2;
@@ -908,7 +911,7 @@ struct PhysF32 {
             float tail = 0.f;
             if (P.has_delta) {
                 const float cd = two ? 0.5f * (ca + cb) : ca;
-                const float psi = 2.f * P.f_delta * cd * P.f_h * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
+                const float psi = 2.f * P.f_delta * cd * pv.x * (w.rho - rhoj) * dotf<ND>(dxf, gx) / rrf;
                 tail = psi * irhoj;
             }
             if constexpr (FLUIDLIKE) padd_if(acc.p[IDR], mj * (dotf<ND>(dv, gx) + tail), in);
@@ -994,7 +997,9 @@ __device__ __forceinline__ unsigned batch_hits(const float* cb, int stride, int 
     const float2 neg1 = make_float2(-1.0f, -1.0f);
     const float2 ncut = make_float2(-cut_f, -cut_f);
     unsigned hits = 0;
-    for (int t0 = 0; t0 < mb; t0 += 8) {
+#pragma unroll
+    for (int t0 = 0; t0 < 32; t0 += 8) {
+        if (t0 >= mb) break;  // warp-uniform
         unsigned h8 = 0;
 #pragma unroll
         for (int t = 4; t >= 0; t -= 4) {
