@@ -44,7 +44,12 @@ struct SysInst {
 
 // Per (interaction, instance) grid and system_b parameters.
 struct GridInst {
-    double H, cell, cutoff_sq, knorm;  // h, 2h, (2h)^2, kernel normalisation
+    double H, cell;                    // h, 2h
+    // (2h)^2, then the FP32 copies of 1/h and of the kernel normalisation:
+    // one 16-byte load in the FP32-compensated pair code
+    alignas(16) double cutoff_sq;
+    float f_invH, f_knorm;
+    double knorm;                      // kernel normalisation
     double ming[MAXD];                 // grid origin (src/Interaction.jl:143)
     int64_t ng[MAXD];                  // cells per dimension (:179)
     int64_t ncells, cellbase;          // this instance's cells in the packed grid
@@ -53,15 +58,13 @@ struct GridInst {
     // system_b wrapper parameters (src/BoundaryParticles.jl)
     double normal[MAXD], point[MAXD], beta, ljcut;
     double bmass, bc;                  // system_b mass and sound speed
-    // FP32 copies for the FP32-compensated sweep (1/h and the kernel
-    // normalisation 16-byte aligned: the pair code reads them as one float2)
-    alignas(16) float f_invH;
-    float f_knorm;
+    // FP32 copies for the FP32-compensated sweep
     float f_normal[MAXD], f_beta, f_ljcut, f_bmass, f_bc;
     int side_b;                        // 1 in the system_b-side copy of a two-sided interaction
 };
-static_assert(offsetof(GridInst, f_invH) % 16 == 0 && offsetof(GridInst, f_knorm) == offsetof(GridInst, f_invH) + 4,
-              "1/h and the kernel normalisation are read as one float2");
+static_assert(offsetof(GridInst, cutoff_sq) % 16 == 0 && offsetof(GridInst, f_invH) == offsetof(GridInst, cutoff_sq) + 8 &&
+                  offsetof(GridInst, f_knorm) == offsetof(GridInst, cutoff_sq) + 12,
+              "(2h)^2, 1/h and the kernel normalisation are read as one 16-byte load");
 
 // Per (interaction, stage, instance) functor parameters.
 struct PfnInst {

@@ -146,7 +146,12 @@ struct NbSlot {
 template <int ND, int NS, int PFN, int KK, int BTK = -1, class Nb>
 __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                             const PfnInst& P, int64_t gi, int k, const OwnState<ND>& o,
-                                            const double* osig, double da, const Nb& nb, Acc<ND, NS>& acc) {
+                                            const double* osig, double da, const Nb& nb, Acc<ND, NS>& acc,
+                                            const double2* cam = nullptr) {
+    // system_a's sound speed and mass: the warp's shared copy (cam) or the
+    // per-instance arrays
+    auto sound_a = [&]() { return cam ? cam->x : A.a_c[k]; };
+    auto mass_of_a = [&]() { return cam ? cam->y : A.a_mass[k]; };
     const int btype = BTK >= 0 ? BTK : r.btype;
     double dx[ND];
 #pragma unroll
@@ -185,7 +190,7 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
         const double q = sqrt(rr) / G.H;
         const double wk = kernel_w<KK>(G.knorm, q);
         const double den = o.rho + nb.rho();
-        const double mj = btype == BT_SELF ? A.a_mass[k] : G.bmass;
+        const double mj = btype == BT_SELF ? mass_of_a() : G.bmass;
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
             const double du = (((-P.alpha) * (o.v[d] - nb.v(d))) * wk) / den;
@@ -195,8 +200,8 @@ __device__ __forceinline__ int process_pair(const ForceArgs& A, const InterRef& 
     }
     double gx[ND];
     Pair<ND, NS, PFN, KK>::geom(dx, rr, G.H, G.knorm, gx);
-    const double ca = A.a_c[k];
-    const double mass_a = A.a_mass[k];
+    const double ca = sound_a();
+    const double mass_a = mass_of_a();
 
     if (btype == BT_DYNAMIC) {
         // src/PairwiseFunctors.jl:53,111,222,334
@@ -506,8 +511,13 @@ struct PhysF64 {
     template <int P2, int BTK = -1>
     static __device__ __forceinline__ int pair_slot(const ForceArgs& A, const InterRef& r, const GridInst& G,
                                                     const PfnInst& P, int64_t gi, int k, const Own& w, double da,
-                                                    const float4* slot, int BT, const float2*, AccT& acc) {
-        return process_pair<ND, NS, P2, KK, BTK>(A, r, G, P, gi, k, w.o, w.sig, da, NbSlot<ND>{slot, BT}, acc);
+                                                    const float4* slot, int BT, const float2* cam, AccT& acc) {
+        return process_pair<ND, NS, P2, KK, BTK>(A, r, G, P, gi, k, w.o, w.sig, da, NbSlot<ND>{slot, BT}, acc,
+                                                 reinterpret_cast<const double2*>(cam));
+    }
+    // system_a's sound speed and mass of instance k into the warp's 16-byte slot
+    static __device__ __forceinline__ void stage_cam(const ForceArgs& A, int k, float2* cam) {
+        if (A.a_c && A.a_mass) *reinterpret_cast<double2*>(cam) = make_double2(A.a_c[k], A.a_mass[k]);
     }
 };
 
@@ -736,6 +746,10 @@ struct PhysF32 {
             for (int q = 0; q < NQR; ++q) __pipeline_memcpy_async(&slot[(NQP + q) * BT], &pr[q], 16);
         }
     }
+    // system_a's FP32 sound speed and mass of instance k into the warp's slot
+    static __device__ __forceinline__ void stage_cam(const ForceArgs& A, int k, float2* cam) {
+        if (A.a_cf) *cam = make_float2(A.a_cf[k], A.a_massf[k]);
+    }
     // cam: system_a's (FP32) sound speed and mass of this instance; BTK: the
     // system_b kind when known at compile time (-1: r.btype)
     template <int P2, int BTK = -1>
@@ -761,9 +775,11 @@ struct PhysF32 {
 #pragma unroll
         for (int d = 0; d < ND; ++d) dx[d] = __dsub_rn(w.x[d], xj[d]);
         const double rr = dot_exact<ND>(dx, dx);
+        // (2h)^2, 1/h and the kernel normalisation: one 16-byte load
+        const int4 gq = *reinterpret_cast<const int4*>(&G.cutoff_sq);
         // the exact test decides, without a branch, whether the pair's terms
         // are added (the pair's arithmetic stays one straight-line block)
-        const bool in = rr < G.cutoff_sq;
+        const bool in = rr < __hiloint2double(gq.y, gq.x);
         if (P2 == GC_PFN_COUNT) {
             if (!in) return 0;
             if constexpr (FLUIDLIKE) {
@@ -778,11 +794,11 @@ struct PhysF32 {
         const float rrf = (float)rr;
         const float rinv = rsqrtf(rrf);
         const float rf = rrf * rinv;
-        // 1/h and the kernel normalisation; h, 0.01·h², α and β: one vector load each
-        const float2 gk = *reinterpret_cast<const float2*>(&G.f_invH);
+        // h, 0.01·h², α and β: one vector load
         const float4 pv = *reinterpret_cast<const float4*>(&P.f_h);
-        const float q = rf * gk.x;
-        const float gc = kernel_dw_dq_f<KK>(gk.y, q) * gk.x * rinv;
+        const float invh = __int_as_float(gq.z);
+        const float q = rf * invh;
+        const float gc = kernel_dw_dq_f<KK>(__int_as_float(gq.w), q) * invh * rinv;
         float gx[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) gx[d] = gc * dxf[d];
@@ -1316,7 +1332,7 @@ __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
             const int nstrips = ND == 2 ? 3 : 9;
             warp_copy(gsm, G, lane);
             warp_copy(psm, P, lane);
-            if (lane == 0 && A.a_cf) *camsm = make_float2(A.a_cf[k], A.a_massf[k]);
+            if (lane == 0) Phys::stage_cam(A, k, camsm);
             __syncwarp();
             const GridInst& Gs = *gsm;
             const PfnInst& Ps = *psm;
