@@ -50,6 +50,10 @@ TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 171.44e6, ("dambreak_3d"
 # largest per-particle error of the FP32-compensated path against plain FP64
 # after the configuration's step count: the stated tolerances on density and stress
 FP32C_TOL = {"rho": 1e-4, "stress": 1e-3}
+# what bounds the sweep, from the same ncu captures: the fraction of issue
+# slots that issued an instruction (smsp__issue_active) and the active lanes
+# per warp instruction
+ISSUE_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): (0.685, 20.94), ("dambreak_3d", "full", "fp64"): (0.624, 17.6)}
 STAGED_CONFIGS = (2, 3)  # sweep launch configurations that run the chunk-staged kernel
 
 
@@ -493,6 +497,9 @@ def run_ours(args, rank, world, local_rank):
     chosen = st1["sweep_cfg_chosen"]
     staged = max(range(len(chosen)), key=lambda c: chosen[c]) in STAGED_CONFIGS
     kname = "k_sweep_stg (fused pair sweep, chunk-staged)" if staged else "k_sweep (fused pair sweep, buffered)"
+    iss = ISSUE_PER_LAUNCH.get((args.workload, args.scale, args.precision))
+    issue = ({"slots_used": iss[0], "lanes_per_instruction": iss[1],
+              "source": "ncu capture of the benched kernel (profiles/)"} if iss and staged else None)
     roof = {"kernel": kname, "bound": "fp32" if f32 else "fp64", "achieved": achieved_tflops,
             "peak": peak.value, "unit": "TFLOP/s", "frac": achieved_tflops / peak.value,
             "peak_source": ("measured FP32 FMA issue rate (gc_measure_fp32_peak)" if f32
@@ -500,6 +507,7 @@ def run_ours(args, rank, world, local_rank):
             "flops_per_launch": flops_per_launch,
             "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, args.scale, args.precision)),
             "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_ms / ms,
+            "issue": issue,
             "hbm": {"achieved": achieved_gbs, "peak": hbm_peak, "peak_source": src, "unit": "GB/s",
                     "frac": achieved_gbs / hbm_peak, "bytes_per_launch": per_launch_bytes}}
     cpu = None
