@@ -46,14 +46,14 @@ FLUID_PAIR_FLOPS = {2: 70, 3: 86}
 WARMUP_MIN = 12  # untimed steps: 1 cold step, 8 autotuner steps (4 configurations twice), then graph capture
 # DRAM bytes (read + write) of one sweep launch from an ncu capture, keyed by
 # (workload, scale, precision); the profiles/ summaries give the commands.
-TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 171.44e6, ("dambreak_3d", "full", "fp64"): 147.16e6}
+TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 171.44e6, ("dambreak_3d", "full", "fp64"): 147.04e6}
 # largest per-particle error of the FP32-compensated path against plain FP64
 # after the configuration's step count: the stated tolerances on density and stress
 FP32C_TOL = {"rho": 1e-4, "stress": 1e-3}
 # what bounds the sweep, from the same ncu captures: the fraction of issue
 # slots that issued an instruction (smsp__issue_active) and the active lanes
 # per warp instruction
-ISSUE_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): (0.685, 20.94), ("dambreak_3d", "full", "fp64"): (0.624, 17.6)}
+ISSUE_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): (0.685, 20.94), ("dambreak_3d", "full", "fp64"): (0.625, 17.26)}
 STAGED_CONFIGS = (2, 3)  # sweep launch configurations that run the chunk-staged kernel
 
 
