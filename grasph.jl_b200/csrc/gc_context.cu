@@ -1114,6 +1114,7 @@ int bbox_slot(gc_ctx* ctx, DSlot& S) {
 // Conservative ghost extent before generation: the reflection of the source
 // bounding box's corners across every plane, padded by one cell.
 __global__ void k_ghost_bound(GhostInst* gh, const SysInst* src, SysInst* gi, int ninst, int nd, int nplanes) {
+    pdl_enter();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ninst) return;
     const SysInst& S = src[k];
@@ -1407,6 +1408,7 @@ int ensure_groups(gc_ctx* ctx, int slot, int id, bool b_side) {
 // Capacity mode: record the largest plans, and flag every plan that does
 // not fit its buffers (the window is then rolled back and re-run exactly).
 __global__ void k_need_max(const int64_t* need, int64_t* need_max, const int64_t* cap, int n, int* err) {
+    pdl_enter();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         if (need[i] > need_max[i]) need_max[i] = need[i];
         if (need[i] > cap[i]) atomicOr(err, ERR_CAPACITY);
@@ -1627,6 +1629,7 @@ int aux_mode_for(int pfn) {
 __global__ void k_xsph_ghost_add(const double* __restrict__ gadj, int64_t CAP, const int64_t* count, int nd,
                                  const int32_t* __restrict__ ginst, const GhostInst* __restrict__ gh,
                                  const SysInst* __restrict__ src, double* __restrict__ vadj, int64_t Ns, int* err) {
+    pdl_enter();
     const int64_t n = *count;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         const int k = ginst[g];
@@ -2489,6 +2492,56 @@ int ev_pair(gc_ctx* ctx, size_t i) {
     return GC_OK;
 }
 
+// A copy of a captured step whose kernel-to-kernel edges are programmatic:
+// a kernel may launch once every block of the kernel before it has passed
+// pdl_enter (where each kernel first waits for its predecessors to finish),
+// so the launches overlap the kernels before them.  Returns nullptr (the
+// step keeps its plain edges) when GC_NO_PDL is set or the copy cannot be
+// made and instantiated.
+static cudaGraph_t programmatic_copy(cudaGraph_t graph) {
+    static const bool off = [] {
+        const char* e = getenv("GC_NO_PDL");
+        return e && *e && *e != '0';
+    }();
+    if (off) return nullptr;
+    size_t ne = 0;
+    if (cudaGraphGetEdges_v2(graph, nullptr, nullptr, nullptr, &ne) != cudaSuccess || ne == 0) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::vector<cudaGraphNode_t> from(ne), to(ne);
+    std::vector<cudaGraphEdgeData> ed(ne);
+    cudaGraph_t cl = nullptr;
+    bool ok = cudaGraphGetEdges_v2(graph, from.data(), to.data(), ed.data(), &ne) == cudaSuccess &&
+              cudaGraphClone(&cl, graph) == cudaSuccess;
+    int converted = 0;
+    for (size_t i = 0; ok && i < ne; ++i) {
+        cudaGraphNodeType ta, tb;
+        ok = cudaGraphNodeGetType(from[i], &ta) == cudaSuccess && cudaGraphNodeGetType(to[i], &tb) == cudaSuccess;
+        if (!ok || ta != cudaGraphNodeTypeKernel || tb != cudaGraphNodeTypeKernel ||
+            ed[i].type != cudaGraphDependencyTypeDefault)
+            continue;
+        cudaGraphNode_t a = nullptr, b = nullptr;
+        ok = cudaGraphNodeFindInClone(&a, from[i], cl) == cudaSuccess &&
+             cudaGraphNodeFindInClone(&b, to[i], cl) == cudaSuccess;
+        cudaGraphEdgeData pe = ed[i];
+        pe.from_port = cudaGraphKernelNodePortProgrammatic;
+        pe.type = cudaGraphDependencyTypeProgrammatic;
+        ok = ok && cudaGraphRemoveDependencies_v2(cl, &a, &b, &ed[i], 1) == cudaSuccess &&
+             cudaGraphAddDependencies_v2(cl, &a, &b, &pe, 1) == cudaSuccess;
+        converted += ok ? 1 : 0;
+    }
+    cudaGraphExec_t ex = nullptr;
+    ok = ok && converted > 0 && cudaGraphInstantiate(&ex, cl, 0) == cudaSuccess;
+    if (ex) cudaGraphExecDestroy(ex);
+    if (!ok) {
+        cudaGetLastError();
+        if (cl) cudaGraphDestroy(cl);
+        return nullptr;
+    }
+    return cl;
+}
+
 // Capture one capacity-mode step into `g` (nothing runs).
 int capture_step(gc_ctx* ctx, StepGraph& g) {
     if (ctx->profiling) TRY(ev_pair(ctx, ctx->ev_used + 4 * ctx->slots.size() * (size_t)std::max(ctx->nstages, 1)));
@@ -2517,6 +2570,10 @@ int capture_step(gc_ctx* ctx, StepGraph& g) {
     }
     g.post = parity(ctx);
     set_parity(ctx, g.pre);
+    if (cudaGraph_t pg = programmatic_copy(graph)) {
+        cudaGraphDestroy(graph);
+        graph = pg;
+    }
     g.graph = graph;
     if (ev1 > ev0) {
         size_t nn = 0;
@@ -3078,6 +3135,7 @@ int gc_add_probe_interaction(gc_ctx* ctx, int inst, int sys_a, int probe, int ke
 __global__ void k_probe_mirror(double* __restrict__ xp, int64_t Np, const SysInst* __restrict__ pinst,
                                const double* __restrict__ xs, int64_t Ns, const int32_t* __restrict__ sid,
                                const int32_t* __restrict__ sinst_of, int nd) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < Ns; g += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = pinst[sinst_of[g]].base + sid[g] - 1;
         for (int d = 0; d < nd; ++d) xp[d * Np + t] = xs[d * Ns + g];
@@ -3087,6 +3145,7 @@ __global__ void k_probe_mirror(double* __restrict__ xp, int64_t Np, const SysIns
 // perm[base + id - 1] = position: the gather that puts a slot back in id order
 __global__ void k_perm_by_id(const int32_t* __restrict__ id, const int32_t* __restrict__ inst_of,
                              const SysInst* __restrict__ inst, int64_t N, int32_t* __restrict__ perm) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x)
         perm[inst[inst_of[g]].base + id[g] - 1] = (int32_t)g;
 }
@@ -3383,6 +3442,7 @@ static int resolve(gc_ctx* ctx, int inst, int handle, HandleRef* r) {
 // Nonzero test of uploaded kinematics (and of v_adjustment, which must be
 // zero) on the device: flag[k] = 1 when any of the n doubles is nonzero.
 __global__ void k_any_nonzero(const double* __restrict__ a, int64_t n, int* flag) {
+    pdl_enter();
     bool nz = false;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         nz |= a[i] != 0.0;
@@ -3916,6 +3976,7 @@ struct PackSeg {
 
 template <class T>
 __global__ void k_pack(const PackSeg* __restrict__ seg, int ncomp, T* __restrict__ dst, int64_t dst_stride) {
+    pdl_enter();
     const PackSeg S = seg[blockIdx.y];
     const T* src = (const T*)S.src;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += (int64_t)gridDim.x * blockDim.x)

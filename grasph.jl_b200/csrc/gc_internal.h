@@ -130,4 +130,17 @@ struct UpdInst {
     uint32_t zmask;
 };
 
+#ifdef __CUDACC__
+// Programmatic dependent launch.  In a captured step graph a kernel may be
+// launched while the kernel it depends on is still running; every kernel's
+// first act is therefore to wait until its predecessors have finished and
+// their memory is visible (griddepcontrol.wait, which returns at once
+// without such an edge), and only then does it let its own dependents
+// launch, so that their launch overlaps its work.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
+
 }  // namespace gc

@@ -75,6 +75,7 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* total) {
 
 __global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int32_t* __restrict__ bsum,
                               const int* skip) {
+    pdl_enter();
     if (skip && *skip) return;
     int64_t t0 = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
     int32_t s = 0;
@@ -88,6 +89,7 @@ __global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t n, int32_t
 
 __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const int32_t* __restrict__ boff,
                              int32_t* __restrict__ out, int32_t* clear, const int* skip) {
+    pdl_enter();
     if (skip && *skip) return;
     int64_t t0 = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_I;
     int32_t v[SCAN_I];
@@ -123,6 +125,7 @@ int64_t scan_tmp_elems(int64_t n) {
 // sums needs no launch of its own.
 __global__ void k_scan_apply_sums(const int32_t* __restrict__ in, int64_t n, const int32_t* __restrict__ bsum,
                                   int32_t* __restrict__ out, int32_t* clear, const int* skip) {
+    pdl_enter();
     if (skip && *skip) return;
     __shared__ int32_t off;
     {
@@ -198,6 +201,7 @@ __device__ __forceinline__ void load_pos(const double* __restrict__ x, int64_t N
 
 // ========================================================== bounding box
 __global__ void k_bbox_reset(unsigned long long* scratch, int ninst) {
+    pdl_enter();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ninst) return;
     for (int d = 0; d < MAXD; ++d) {
@@ -208,6 +212,7 @@ __global__ void k_bbox_reset(unsigned long long* scratch, int ninst) {
 
 __global__ void k_bbox(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                        const int64_t* count, unsigned long long* scratch, int* err) {
+    pdl_enter();
     int64_t n = count ? *count : N;
     int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = g < n;
@@ -267,6 +272,7 @@ __global__ void k_bbox(const double* __restrict__ x, int64_t N, int nd, const in
 }
 
 __global__ void k_bbox_finish(const unsigned long long* scratch, SysInst* inst, int ninst, int nd) {
+    pdl_enter();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ninst) return;
     for (int d = 0; d < nd; ++d) {
@@ -287,6 +293,7 @@ void launch_bbox_reset(unsigned long long* scratch, int ninst, cudaStream_t s) {
 __global__ void k_bbox_fused(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                              const int64_t* count, unsigned long long* scratch, SysInst* inst, int ninst, int* err,
                              int64_t tiles_per_block) {
+    pdl_enter();
     // each block reduces a contiguous run of 256-particle tiles: every thread
     // keeps the running min/max of its particles while they belong to one
     // instance (flushing with atomics when the instance changes), and the
@@ -415,6 +422,7 @@ void launch_bbox(const double* x, int64_t N, int nd, const int32_t* inst_of, con
 
 // ================================================================== sort
 __global__ void k_sort_plan(SysInst* inst, int ninst, int nd, int64_t* need, int* err) {
+    pdl_enter();
     for (int k = threadIdx.x; k < ninst; k += blockDim.x) {
         SysInst& S = inst[k];
         int64_t cells = S.n > 0 ? 1 : 0;
@@ -486,6 +494,7 @@ __device__ __forceinline__ int32_t sort_key_of(const double* __restrict__ x, int
 __global__ void k_sort_keys(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                             const int64_t* count, const SysInst* __restrict__ inst, int32_t* __restrict__ key,
                             int32_t* __restrict__ hist, int64_t cells_cap, int* err, int* unsorted) {
+    pdl_enter();
     int64_t n = count ? *count : N;
     const int lane = threadIdx.x & 31;
     // whole warps iterate together (warp-aggregated histogram)
@@ -542,6 +551,7 @@ void launch_sort_keys(const double* x, int64_t N, int nd, const int32_t* inst_of
 __global__ void k_sort_scatter(const int32_t* __restrict__ key, int64_t N, const int64_t* count,
                                const int32_t* __restrict__ start, int32_t* __restrict__ fill,
                                int32_t* __restrict__ perm, const int* unsorted) {
+    pdl_enter();
     int64_t n = count ? *count : N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     if (unsorted && *unsorted == 0) {
@@ -572,6 +582,7 @@ void launch_sort_scatter(const int32_t* key, int64_t N, const int64_t* count, co
 // Julia's sortperm (equal keys keep ascending original index).
 __global__ void k_sort_fixup(const int32_t* __restrict__ start, int64_t ncells_cap, const int64_t* total_cells,
                              int32_t* __restrict__ perm) {
+    pdl_enter();
     int64_t nc = *total_cells;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc && c < ncells_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -632,6 +643,7 @@ __device__ __forceinline__ void sort_segment(int32_t* __restrict__ perm, int32_t
 __global__ void k_sort_fixup_clear(const int32_t* __restrict__ start, int64_t ncells_cap, const int64_t* total_cells,
                                    int32_t* __restrict__ perm, int32_t* __restrict__ fill, const int* unsorted,
                                    unsigned long long* in_order_count) {
+    pdl_enter();
     if (unsorted && *unsorted == 0) {
         // the scatter placed nothing through the fill counters
         if (in_order_count && blockIdx.x == 0 && threadIdx.x == 0) *in_order_count += 1ull;
@@ -681,6 +693,7 @@ void launch_sort_fixup(const int32_t* start, int64_t ncells_cap, const int64_t* 
 
 __global__ void k_gather(const double* __restrict__ src, double* __restrict__ dst, int ncomp, int64_t N,
                          const int32_t* __restrict__ perm, const int64_t* count) {
+    pdl_enter();
     int64_t n = count ? *count : N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         int64_t o = perm[g];
@@ -693,6 +706,7 @@ __global__ void k_gather(const double* __restrict__ src, double* __restrict__ ds
 
 __global__ void k_gather_i32(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int64_t N,
                              const int32_t* __restrict__ perm, const int64_t* count) {
+    pdl_enter();
     int64_t n = count ? *count : N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         int64_t o = perm[g];
@@ -704,6 +718,7 @@ __global__ void k_gather_i32(const int32_t* __restrict__ src, int32_t* __restric
 // blockIdx.y picks the field (the int32 fields after the double ones), so
 // every thread has one independent gather per component.
 __global__ void k_gather_fields(GatherArgs a, int64_t N, const int32_t* __restrict__ perm, const int64_t* count) {
+    pdl_enter();
     const int64_t n = count ? *count : N;
     const int f = blockIdx.y;
     // the sort's order flag, read by the scatter and fix-up launched
@@ -773,8 +788,10 @@ void launch_gather_i32(const int32_t* src, int32_t* dst, int64_t N, const int32_
 // src/Interaction.jl:131-193: origin snapped to a multiple of the cell
 // size below min−2h, ngridx = floor((max+2h − origin)/h2) + 1.
 __device__ void grid_plan_block(const GridPlanArgs& a);
-__global__ void k_grid_plan(GridPlanArgs a) { grid_plan_block(a); }
-__global__ void k_grid_plan_all(const GridPlanArgs* __restrict__ args) { grid_plan_block(args[blockIdx.x]); }
+__global__ void k_grid_plan(GridPlanArgs a) {
+    pdl_enter(); grid_plan_block(a); }
+__global__ void k_grid_plan_all(const GridPlanArgs* __restrict__ args) {
+    pdl_enter(); grid_plan_block(args[blockIdx.x]); }
 
 void launch_grid_plan_all(const GridPlanArgs* d_args, int n, cudaStream_t s) {
     if (n <= 0) return;
@@ -947,6 +964,7 @@ __device__ __forceinline__ void grid_count_blocks(const double* __restrict__ x, 
 __global__ void k_grid_count(const double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                              const int64_t* count, const GridInst* __restrict__ gi, int32_t* __restrict__ hist,
                              int64_t cells_cap, int* err, unsigned long long* incons, const int* skip) {
+    pdl_enter();
     if (skip && *skip) return;
     grid_count_blocks(x, N, nd, inst_of, count, gi, hist, cells_cap, err, incons, blockIdx.x, gridDim.x);
 }
@@ -969,6 +987,7 @@ void launch_grid_count(const double* x, int64_t N, int nd, const int32_t* inst_o
 int64_t still_hist_elems(int64_t cells) { return cells + (cells + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
 __global__ void k_still_count(const __grid_constant__ StillGridArgs a) {
+    pdl_enter();
     const StillGrid& g = a.g[blockIdx.y];
     if (g.keep[1]) return;
     grid_count_blocks(g.x, g.N, a.nd, g.inst_of, nullptr, g.gi, g.hist, g.cells, a.err, a.incons, blockIdx.x,
@@ -977,6 +996,7 @@ __global__ void k_still_count(const __grid_constant__ StillGridArgs a) {
 
 // Tile sums of each histogram, after its cells.
 __global__ void k_still_scan_reduce(const __grid_constant__ StillGridArgs a) {
+    pdl_enter();
     const StillGrid& g = a.g[blockIdx.y];
     if (g.keep[1]) return;
     const int64_t nb = (g.cells + SCAN_TILE - 1) / SCAN_TILE;
@@ -996,6 +1016,7 @@ __global__ void k_still_scan_reduce(const __grid_constant__ StillGridArgs a) {
 // Exclusive scan of each histogram into its CSR (cells + 1 entries), the
 // histogram cleared as it is read; each tile adds up the sums before it.
 __global__ void k_still_scan_apply(const __grid_constant__ StillGridArgs a) {
+    pdl_enter();
     const StillGrid& g = a.g[blockIdx.y];
     if (g.keep[1]) return;
     const int64_t n = g.cells;
@@ -1060,6 +1081,7 @@ __device__ __forceinline__ double plane_da(const double* __restrict__ x, int64_t
 
 template <int ND>
 __global__ void k_ghost_flags(GhostGenArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.Nsrc;
          g += (int64_t)gridDim.x * blockDim.x) {
         const GhostInst& H = a.gh[a.src_inst_of[g]];
@@ -1074,6 +1096,7 @@ __global__ void k_ghost_flags(GhostGenArgs a) {
 
 template <int ND>
 __global__ void k_ghost_fill(GhostGenArgs a) {
+    pdl_enter();
     const int64_t CAP = a.Nsrc * a.nplanes;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.Nsrc;
          g += (int64_t)gridDim.x * blockDim.x) {
@@ -1099,6 +1122,7 @@ __global__ void k_ghost_fill(GhostGenArgs a) {
 }
 
 __global__ void k_ghost_ranges(GhostGenArgs a) {
+    pdl_enter();
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.ninst; k += gridDim.x * blockDim.x) {
         GhostInst& H = a.gh[k];
         int64_t v0 = H.src_base * a.nplanes, v1 = (H.src_base + H.src_n) * a.nplanes;
@@ -1131,6 +1155,7 @@ __global__ void k_ghost_kin(int64_t cap, const int64_t* count, const int32_t* __
                             const GhostInst* __restrict__ gh, const double* __restrict__ src_v,
                             const double* __restrict__ src_rho, int64_t Nsrc, double* __restrict__ gv,
                             double* __restrict__ grho) {
+    pdl_enter();
     int64_t n = *count;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         int64_t o = gh[ginst[k]].src_base + io[k] - 1;
@@ -1161,6 +1186,7 @@ __global__ void k_ghost_copy(int64_t cap, const int64_t* count, int nd, int ns, 
                              const int32_t* __restrict__ ginst, const double* __restrict__ normals,
                              const GhostInst* __restrict__ gh, int field, int mode, const double* __restrict__ src,
                              int64_t Nsrc, double* __restrict__ dst) {
+    pdl_enter();
     int64_t n = *count;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         int64_t o = gh[ginst[k]].src_base + io[k] - 1;
@@ -1221,6 +1247,7 @@ void launch_ghost_copy(int64_t cap, const int64_t* count, int nd, int ns, const 
 // Julia's AoS layout (K doubles per particle) <-> planar device fields.
 __global__ void k_aos_to_planar(const double* __restrict__ src, double* __restrict__ dst, int64_t n, int comps,
                                 int64_t N, int64_t base) {
+    pdl_enter();
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * comps;
          t += (int64_t)gridDim.x * blockDim.x) {
         int64_t i = t / comps;
@@ -1230,6 +1257,7 @@ __global__ void k_aos_to_planar(const double* __restrict__ src, double* __restri
 }
 __global__ void k_planar_to_aos(const double* __restrict__ src, double* __restrict__ dst, int64_t n, int comps,
                                 int64_t N, int64_t base) {
+    pdl_enter();
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * comps;
          t += (int64_t)gridDim.x * blockDim.x) {
         int64_t i = t / comps;
@@ -1238,10 +1266,12 @@ __global__ void k_planar_to_aos(const double* __restrict__ src, double* __restri
     }
 }
 __global__ void k_i64_to_i32(const int64_t* __restrict__ src, int32_t* __restrict__ dst, int64_t n) {
+    pdl_enter();
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
         dst[t] = (int32_t)src[t];
 }
 __global__ void k_i32_to_i64(const int32_t* __restrict__ src, int64_t* __restrict__ dst, int64_t n) {
+    pdl_enter();
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
         dst[t] = (int64_t)src[t];
 }
@@ -1275,6 +1305,7 @@ void launch_i32_to_i64(const int32_t* src, int64_t* dst, int64_t n, cudaStream_t
 
 // ===================================================== measurement helpers
 __global__ void k_sum_counts(const int32_t* __restrict__ c, int64_t n, unsigned long long* out) {
+    pdl_enter();
     unsigned long long s = 0;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
         s += (unsigned long long)c[t];
@@ -1291,6 +1322,7 @@ void launch_sum_counts(const int32_t* c, int64_t n, unsigned long long* out, cud
 
 // FP64 FMA issue rate: eight independent dependent chains per thread.
 __global__ void k_fp64_peak(double* out, int iters, double a, double b) {
+    pdl_enter();
     double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
            x7 = x0 + 7;
     for (int i = 0; i < iters; ++i) {
@@ -1313,6 +1345,7 @@ void launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStrea
 
 // FP32 FMA issue rate: eight independent dependent chains per thread.
 __global__ void k_fp32_peak(float* out, int iters, float a, float b) {
+    pdl_enter();
     float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
           x7 = x0 + 7;
     for (int i = 0; i < iters; ++i) {

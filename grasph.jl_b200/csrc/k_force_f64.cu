@@ -38,6 +38,7 @@ __device__ __forceinline__ int find_inst(const GridInst* gi, int ninst, int64_t 
 // (the grid build has flagged the overflow).
 __global__ void k_groups_count(const GridInst* __restrict__ gi, int ninst, int nd, const int32_t* __restrict__ cs,
                                int64_t ncols_cap, int64_t cells_cap, int32_t* __restrict__ cnt) {
+    pdl_enter();
     const int64_t T = gi[ninst - 1].colbase + gi[ninst - 1].ncols;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncols_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -61,6 +62,7 @@ __global__ void k_groups_count(const GridInst* __restrict__ gi, int ninst, int n
 __global__ void k_groups_fill(const GridInst* __restrict__ gi, int ninst, int nd, const int32_t* __restrict__ cs,
                               const int32_t* __restrict__ off, int64_t ncols_cap, int64_t cells_cap,
                               int2* __restrict__ groups, int64_t* ngroups) {
+    pdl_enter();
     const int64_t T = gi[ninst - 1].colbase + gi[ninst - 1].ncols;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < T && c < ncols_cap;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -97,6 +99,7 @@ void launch_groups_fill(const GridInst* gi, int ninst, int nd, const int32_t* cs
 __global__ void k_aux(int mode, int64_t N, const int64_t* count, const double* __restrict__ rho,
                       const double* __restrict__ p, const int32_t* __restrict__ inst_of, const double* mass,
                       double* __restrict__ aux) {
+    pdl_enter();
     int64_t n = count ? *count : N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
         double r = rho[g];
@@ -107,6 +110,7 @@ __global__ void k_aux(int mode, int64_t N, const int64_t* count, const double* _
 }
 
 __global__ void k_pack32(PackArgs a, const int64_t* count) {
+    pdl_enter();
     const int64_t n = count ? *count : a.N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x)
         pack_one(a, g);

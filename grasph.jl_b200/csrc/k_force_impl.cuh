@@ -1117,6 +1117,7 @@ __device__ __forceinline__ int flush_all(const ForceArgs& A, const InterRef& r, 
 
 template <class Phys, int ND, int PFN, bool COUNT_ONLY, int MINB, int BUF, int UNROLL>
 __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep(ForceArgs A) {
+    pdl_enter();
     extern __shared__ int32_t sbuf[];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -1286,6 +1287,7 @@ __host__ __device__ constexpr int stg_warp_bytes() {
 // policy's pair_data, as in k_sweep.
 template <class Phys, int ND, int PFN, int MINB, int CH>
 __global__ void __launch_bounds__(FORCE_TPB, MINB) k_sweep_stg(ForceArgs A) {
+    pdl_enter();
     static_assert(CH % 32 == 0 && CH >= 32 && CH <= 128, "chunk of 1 to 4 batches of 32");
     constexpr int NB = CH / 32;
     constexpr int NQ = Phys::NQ;

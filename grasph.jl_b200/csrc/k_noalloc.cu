@@ -46,6 +46,7 @@ constexpr int64_t NA_WORDS = NA_TAIL + NA_TAIL_BYTES / 4;
 __device__ __align__(256) int32_t g_noalloc_scratch[NA_WORDS];
 
 __global__ void k_na_init(SysInst* S, int64_t n, double cutoff, int64_t* cells, int* err) {
+    pdl_enter();
     SysInst s{};
     s.base = 0;
     s.n = n;

@@ -46,6 +46,7 @@ __device__ __forceinline__ void halfstep_one(const StepArgs& a, int64_t g) {
 }
 
 __global__ void k_halfstep(StepArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x)
         halfstep_one(a, g);
 }
@@ -56,6 +57,7 @@ __device__ __forceinline__ void update_one(const UpdArgs& a, int64_t g);
 // KIND: the updater's GC_UPD_* kind, or -1 for none
 template <int KIND>
 __global__ void k_halfstep_fused(StepArgs a, UpdArgs u, PackArgs pk) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         halfstep_one(a, g);
         if (KIND >= 0) update_one<KIND>(u, g);
@@ -66,6 +68,7 @@ __global__ void k_halfstep_fused(StepArgs a, UpdArgs u, PackArgs pk) {
 // src/TimeIntegration.jl:673-682: damping, full step, zero XSPH pass, x += dt·v
 // (every load before the first store, as in halfstep_one).
 __global__ void k_fullstep(StepArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const SysInst& S = a.inst[a.inst_of[g]];
         const double dt = S.dt;
@@ -106,6 +109,7 @@ __global__ void k_fullstep(StepArgs a) {
 
 // :434 and :684-685: v += v_adjustment, then x += dt·v.
 __global__ void k_xsph_final(StepArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const double dt = a.inst[a.inst_of[g]].dt;
         for (int d = 0; d < a.nd; ++d) {
@@ -120,6 +124,7 @@ __global__ void k_xsph_final(StepArgs a) {
 // src/TimeIntegration.jl:783-791 (_save_q0_all!, _zero_acc_all!) and, for
 // the first stage, :800 (_reset_dqdt_all!).
 __global__ void k_rk4_begin(StepArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const SysInst& S = a.inst[a.inst_of[g]];
         for (int d = 0; d < a.nd; ++d) {
@@ -135,6 +140,7 @@ __global__ void k_rk4_begin(StepArgs a) {
 
 // :802 (_rk4_advance_all!): q = q0 + (f·dt)·dqdt, then dqdt <- source.
 __global__ void k_rk4_advance(StepArgs a, double f) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const SysInst& S = a.inst[a.inst_of[g]];
         const double c = f * S.dt;
@@ -149,6 +155,7 @@ __global__ void k_rk4_advance(StepArgs a, double f) {
 
 // :814-816: damping (dvdt -= Γ/dt·v), then acc += w·dqdt.
 __global__ void k_rk4_acc(StepArgs a, double w) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const SysInst& S = a.inst[a.inst_of[g]];
         for (int d = 0; d < a.nd; ++d) {
@@ -165,6 +172,7 @@ __global__ void k_rk4_acc(StepArgs a, double w) {
 
 // :820-826: q = q0 + dt·acc, zero XSPH pass, x += dt·v.
 __global__ void k_rk4_final(StepArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x) {
         const SysInst& S = a.inst[a.inst_of[g]];
         const double dt = S.dt;
@@ -294,6 +302,7 @@ __device__ __forceinline__ void ep_update(const UpdInst& u, double dt, double* s
 // held to the registers of the stress return mappings.
 template <int KIND>
 __global__ void k_update(UpdArgs a) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.N; g += (int64_t)gridDim.x * blockDim.x)
         update_one<KIND>(a, g);
 }
@@ -426,6 +435,7 @@ bool halfstep_fuses(int kind) {
 // roundings (a fused broadcast, no contraction); PrescribedVelocityUpdater
 // (:95-97): v += prescribed_v.
 __global__ void k_virtual_update(VirtArgs a) {
+    pdl_enter();
     const int64_t N = a.N;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
         const int k = a.inst_of[g];
@@ -456,6 +466,7 @@ void launch_virtual_update(const VirtArgs& a, cudaStream_t s) {
 
 __global__ void k_virtual_advance(double* __restrict__ x, int64_t N, int nd, const int32_t* __restrict__ inst_of,
                                   const SysInst* __restrict__ inst, const VirtInst* __restrict__ vi) {
+    pdl_enter();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (int64_t)gridDim.x * blockDim.x) {
         const int k = inst_of[g];
         const double dt = inst[k].dt;
