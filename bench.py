@@ -46,7 +46,7 @@ FLUID_PAIR_FLOPS = {2: 70, 3: 86}
 WARMUP_MIN = 12  # untimed steps: 1 cold step, 8 autotuner steps (4 configurations twice), then graph capture
 # DRAM bytes (read + write) of one sweep launch from an ncu capture, keyed by
 # (workload, scale, precision); the profiles/ summaries give the commands.
-TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 171.44e6, ("dambreak_3d", "full", "fp64"): 147.04e6}
+TRAFFIC_PER_LAUNCH = {("dambreak_3d", "full", "fp32c"): 171.61e6, ("dambreak_3d", "full", "fp64"): 147.04e6}
 # largest per-particle error of the FP32-compensated path against plain FP64
 # after the configuration's step count: the stated tolerances on density and stress
 FP32C_TOL = {"rho": 1e-4, "stress": 1e-3}
